@@ -1,0 +1,334 @@
+"""Benchmark of the SIE hot path: plane-wave solves per second on the rough-slab
+workload (10 lambda x 10 lambda, ~19.5k triangles, ~29k RWG edges, plain FP64
+MLFMM + GMRES to 1e-6).
+
+One step = one GMRES solve of one right-hand side on a set-up problem (near
+field, radiation patterns and translation tables are built once, as the
+reference does for its incidence-angle loop, main.f90:450-463).  `value` times
+the device solve (inputs resident in HBM); `e2e` times the public host API with
+the right-hand side copied in from pinned memory and the currents copied out.
+
+Multi-GPU (torchrun): every rank solves its own realisation (seed = rank),
+weak scaling, no collective on the data path; timings are max-reduced.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s @1e-5 far-field err vs FP64: mixed vs plain FP64 GPU; matvec % HBM peak"
+WL = 632.8e-9
+EPS = -11.7 - 1.26j  # exp(+iwt) convention of the reference (lossy => Im < 0)
+
+WORKLOADS = {
+    # 10 lambda x 10 lambda rough slab, seed 0, corr 1 lambda, RMS 0.5 lambda, 1 lambda thick
+    "slab10": dict(length_wl=10.0, rms_wl=0.5, corr_wl=1.0, thickness_wl=1.0, cells=64, seed=0),
+    # a small case for quick checks
+    "slab4": dict(length_wl=4.0, rms_wl=0.3, corr_wl=1.0, thickness_wl=1.0, cells=24, seed=0),
+}
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for n, v in zip(names, r[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_mesh(wl_name, seed):
+    from specklesim_b200 import mesh
+    w = dict(WORKLOADS[wl_name])
+    w["seed"] = seed
+    return mesh.slab_config(w["length_wl"], WL, w["rms_wl"], w["corr_wl"], w["seed"], cells=w["cells"],
+                            thickness_wl=w["thickness_wl"])
+
+
+def matvec_bytes(g, nnz, Q, level_boxes, n_i4):
+    """Algorithmic bytes of one FP64 matvec (per right-hand side)."""
+    M, N, s = g.n_edges, g.n, 16
+    near = nnz * 3 * s + 2 * N * s              # a, b, d panels + x in + y out
+    rt = 2 * M * 4 * Q * s                      # radiation patterns, aggregate + receive
+    coeff = sum(b * 8 * Q * s * 4 for b in level_boxes)   # C, D written and read
+    sr_src = n_i4 * 8 * Q * s                   # SR source reads
+    tl = len(level_boxes) * 343 * 2 * Q * s
+    return dict(near=near, rt=rt, coeff=coeff, sr=sr_src, tl=tl, total=near + rt + coeff + sr_src + tl)
+
+
+def cpu_reference(V, T, matvecs_per_solve, threads, s_opt=250, budget_matvecs=2):
+    """The oracle (C++ restatement of the reference) timed on the host cores."""
+    from oracle.oracle import Oracle
+    o = Oracle(V, T, WL, EPS, tree_s_opt=s_opt, threads=threads)
+    t0 = time.perf_counter()
+    o.tree()
+    o.setup_fmm()
+    t_setup = time.perf_counter() - t0
+    x = np.random.default_rng(0).standard_normal(o.N) + 0j
+    ts = []
+    for _ in range(budget_matvecs):
+        t1 = time.perf_counter()
+        o.matvec(x)
+        ts.append(time.perf_counter() - t1)
+    t_mv = min(ts)
+    o.close()
+    per_solve = t_mv * matvecs_per_solve
+    return dict(value=1.0 / per_solve, unit="solves/s", cores=threads, kind="port",
+                sample=(f"oracle C++ restatement (OpenMP, {threads} threads): set-up {t_setup:.1f} s untimed, "
+                        f"{budget_matvecs} MLFMM matvecs timed ({t_mv:.3f} s each); solves/s = "
+                        f"1 / (matvec time x {matvecs_per_solve} matvecs per solve of the GPU run)"),
+                setup_s=t_setup, matvec_s=t_mv)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="slab10", choices=list(WORKLOADS))
+    ap.add_argument("--restart", type=int, default=50)
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-matvecs-per-solve", type=int, default=0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference's CPU implementation of the path (the oracle port) on the host cores
+        if rank != 0:
+            return
+        V, T = build_mesh(args.workload, 0)
+        threads = os.cpu_count() or 1
+        mps = args.reference_matvecs_per_solve or 120
+        vals = []
+        for _ in range(max(1, args.warmup and 0) + args.steps if False else 1):
+            pass
+        cb = cpu_reference(V, T, mps, threads)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload} rough slab (seed 0), ICTF, ng=3, s_opt=250, K=19",
+                       "matvecs_per_solve": mps},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from specklesim_b200 import Sie, incidence, _lib
+
+    V, T = build_mesh(args.workload, rank)
+    t0 = time.perf_counter()
+    g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local)
+    g.setup()
+    setup_s = time.perf_counter() - t0
+    lib = _lib.load()
+    stream = torch.cuda.Stream()
+    _lib.check(lib.sie_set_stream(g._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+
+    k, E = incidence(0.0, 0.0, "TM", 2)  # x-polarised normal incidence along -z
+    b_host = g.rhs_planewave(k, E)
+    N = g.n
+    dev = torch.device("cuda", local)
+    with torch.cuda.stream(stream):
+        b = torch.from_numpy(b_host.view(np.float64)).to(dev)
+        x = torch.zeros_like(b)
+    stream.synchronize()
+
+    import ctypes as C
+    cfg = _lib.SieSolverCfg()
+    lib.sie_solver_default(C.byref(cfg))
+    cfg.restart, cfg.max_iterations, cfg.tolerance = args.restart, 650, args.tol
+    st = _lib.SieStats()
+
+    def solve_dev():
+        rc = lib.sie_solve_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1, C.byref(cfg),
+                                  C.byref(st))
+        _lib.check(rc)
+
+    for _ in range(args.warmup):
+        solve_dev()
+    iters, mvs = st.iterations, st.matvecs
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = lib.sie_launch_count()
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            solve_dev()
+        e1.record(stream)
+        barrier()
+    launches = lib.sie_launch_count() - l0
+    t_dev = e0.elapsed_time(e1) / 1000.0
+    if world > 1:
+        tt = torch.tensor([t_dev], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    value = world * args.steps / t_dev
+
+    # ---- end to end through the public host API (pinned host buffers)
+    bp = torch.from_numpy(b_host.view(np.float64).copy()).pin_memory()
+    xp = torch.zeros_like(bp).pin_memory()
+    stats = (_lib.SieStats * 1)()
+    dp = C.POINTER(C.c_double)
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        _lib.check(lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg),
+                                 stats))
+    e3.record(stream)
+    barrier()
+    t_e2e = e2.elapsed_time(e3) / 1000.0
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = world * args.steps / t_e2e
+    x_e2e = xp.numpy().view(np.complex128)
+
+    # ---- matvec phases and roofline (one timed matvec)
+    y = torch.empty_like(b)
+    _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
+                                     C.c_void_p(stream.cuda_stream)))
+    for _ in range(3):
+        _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
+                                         C.c_void_p(stream.cuda_stream)))
+    tm = g.timings()
+    Q = 2 * 19 * 19 + 2
+    level_boxes, n_i4 = [], 0
+    for l in range(g.l_min, g.l_max + 1):
+        pass
+    info = getattr(g, "level_info", None)
+    peak, peak_kind = peaks()
+    phases = {k: tm[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
+    dom = max(phases, key=phases.get)
+    nnz = g.near_nnz
+    bytes_near = nnz * 3 * 16 + 2 * N * 16
+    bytes_rt = g.n_edges * 4 * Q * 16
+    dom_bytes = {"mv_near_ms": bytes_near, "mv_recv_ms": bytes_rt + 2 * N * 16,
+                 "mv_agg_ms": bytes_rt + N * 16}.get(dom, None)
+    roof = None
+    if dom_bytes:
+        ach = dom_bytes / (phases[dom] * 1e-3) / 1e9
+        roof = {"kernel": dom.replace("mv_", "").replace("_ms", ""), "bound": "hbm", "achieved": ach,
+                "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
+                "bytes_per_launch": dom_bytes, "launch_ms": phases[dom], "traffic": None}
+    mv_bytes = bytes_near + 2 * bytes_rt
+    mv_frac = mv_bytes / (tm["mv_total_ms"] * 1e-3) / 1e9 / peak
+
+    # ---- CPU baseline: the oracle on the host cores (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cb = cpu_reference(V, T, mvs, threads)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        res = b_host - g.matvec(x_e2e)
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {
+                "workload": (f"{args.workload}: rough slab {WORKLOADS[args.workload]['length_wl']} lambda, "
+                             f"lambda=632.8nm, eps=-11.7-1.26i (exp(+iwt)), seed=rank, {T.shape[0]} triangles, "
+                             f"{g.n_edges} RWG edges, ICTF, ng=3, s_opt=250, K=19, l={g.l_min}..{g.l_max}"),
+                "precision": "fp64", "solver": f"GMRES(IMGS) restart {args.restart}, tol {args.tol}",
+                "iterations": iters, "matvecs_per_solve": mvs, "setup_s": setup_s,
+                "near_nnz_blocks": nnz, "matvec_ms": tm["mv_total_ms"], "matvec_phases_ms": phases,
+                "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
+                "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
+                "l2": "inputs > L2 (near panels and radiation patterns are GBs)",
+            },
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,170 @@
+/*
+ * sie_gpu.h -- C-ABI of the B200 SIE hot path (libsiegpu.so).
+ *
+ * Drop-in boundary for SpeckleSim's surface-integral-equation matvec path:
+ * the RWG near-field impedance fill with Hänninen singularity subtraction and
+ * the MLFMM matrix-vector product that GMRES calls.  Every function returns an
+ * int status (SIE_OK = 0); sie_last_error() gives the message of the last
+ * failure on the calling thread.  Plain pointers and sizes only.
+ *
+ * Vector layout (all complex vectors): interleaved (re, im) doubles, length 2*N
+ * doubles per right-hand side with N = 2*M unknowns; element i < M is the
+ * electric coefficient J of RWG edge i and element M + i its magnetic
+ * coefficient, edges in the reference's neighbour-scan order
+ * (src/lib_sie_tri_calculation_mod.f90:865-905).  Several right-hand sides are
+ * stored one after another (column-major N x nrhs).
+ *
+ * Sign convention: exp(+i w t), Green function exp(-i k R)/(4 pi R)
+ * (src/lib_sie_tri_calculation_mod.f90:1421-1432); a lossy body therefore has a
+ * NEGATIVE imaginary relative permittivity.
+ */
+#ifndef SIE_GPU_H
+#define SIE_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SIE_OK 0
+#define SIE_ERR_ARG 1       /* bad argument (null pointer, size, option) */
+#define SIE_ERR_CUDA 2      /* a CUDA call failed or no device */
+#define SIE_ERR_STATE 3     /* call order violated (e.g. matvec before setup) */
+#define SIE_ERR_NOMEM 4     /* device or host allocation failed */
+#define SIE_ERR_MESH 5      /* mesh is not a valid triangle surface */
+#define SIE_ERR_NOCONV 6    /* GMRES did not reach the tolerance */
+#define SIE_ERR_TIMEOUT 7   /* host-side time limit reached */
+#define SIE_ERR_NONFINITE 8 /* NaN/Inf met in an input or a result */
+
+#define SIE_PMCHWT 1
+#define SIE_ICTF 3
+
+#define SIE_FP64 0  /* every step in double precision */
+#define SIE_MIXED 1 /* FP32 bulk matvec (used by the mixed-precision solver) */
+
+typedef struct sie_ctx sie_ctx;
+
+/* Module globals of the reference set before lib_sie_ml_fmm_precalculation_tri
+ * (src/lib_sie_data_container.f90:22-96, main.f90:221-241). */
+typedef struct {
+  double lambda;                   /* illumination_p%lambda [m] */
+  double eps_r1_re, eps_r1_im;     /* background relative permittivity (1, 0) */
+  double eps_r2_re, eps_r2_im;     /* body relative permittivity */
+  int formulation;                 /* SIE_ICTF (calc_p(3)=3, default) or SIE_PMCHWT */
+  int ngp;                         /* triangle rule points, ng = 3 (1,3,4,6,7,12) */
+  int tree_s_opt;                  /* tree_s_opt = 250 */
+  int truncation_number;           /* truncation_number_default = 19 */
+  int normal_convention;           /* calc_p(7): 1 or 2 */
+  int fix_itbn;                    /* 0 reproduces the IT_bn bracket of :2142 */
+  int device;                      /* CUDA device ordinal */
+  int dense;                       /* 1: no MLFMM, every pair in the near matrix */
+} sie_config;
+
+typedef struct {
+  int restart;           /* GMRES restart m (reference: restart = max_iterations) */
+  int max_iterations;    /* icntl(7) */
+  double tolerance;      /* cntl(1): backward-error tolerance */
+  int use_initial_guess; /* icntl(6); x holds the guess on entry */
+  int precision;         /* SIE_FP64: zgmres semantics on the GPU;
+                            SIE_MIXED: FP64 outer FGMRES around an FP32 inner GMRES */
+  int inner_restart;     /* SIE_MIXED: inner FP32 GMRES restart */
+  double inner_tolerance;/* SIE_MIXED: inner relative residual reduction */
+  double time_limit_s;   /* host-side wall limit, 0 = none */
+} sie_solver_cfg;
+
+typedef struct {
+  int iterations;              /* info(2) (outer iterations for SIE_MIXED) */
+  int inner_iterations;        /* SIE_MIXED: total inner iterations */
+  int matvecs;                 /* matvec applications (all precisions) */
+  int converged;               /* 1 if the backward error reached the tolerance */
+  double backward_error_arnoldi; /* last Arnoldi estimate (bea) */
+  double backward_error_true;    /* rinfo(2): ||b - Ax|| / ||b|| */
+  double seconds;              /* device time of the solve */
+} sie_stats;
+
+/* Fill *cfg with the reference defaults (ICTF, ng = 3, s_opt = 250, K = 19). */
+void sie_config_default(sie_config* cfg);
+void sie_solver_default(sie_solver_cfg* cfg);
+
+const char* sie_last_error(void);
+const char* sie_version(void);
+
+/* Replaces data_import_tri + precalculation_fn + the tree constructor
+ * (src/lib_sie_tri_mlfmm_interface.f90:59-92 up to lib_sie_constructor_tri).
+ * verts: nv x 3 doubles; tris: nt x 3 vertex indices, 0-based. */
+int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris, int nt,
+             sie_ctx** out);
+
+/* Number of RWG edges M (m_pairs) and the MLFMM levels of the tree. */
+int sie_info(const sie_ctx* ctx, int* n_edges, int* l_min, int* l_max, long long* near_nnz);
+
+/* Replaces the rest of lib_sie_ml_fmm_precalculation_tri: near-field CSR fill
+ * (precalculation_near_field_csr_tri :779-863), radiation patterns
+ * (PreCalculate_RT, lib_sie_tri_mlfmm.f90:503-539), translation tables
+ * (precalculation_LT3_TL, lib_sie_mlfmm.f90:27-82) and the Jacobi diagonal
+ * (precalculation_diagonal_element :94-109). */
+int sie_setup(sie_ctx* ctx);
+
+/* y = Z x for nrhs right-hand sides (host arrays).  Replaces the matvec
+ * callback lib_sie_ml_fmm_calculate_vector_b_tri
+ * (src/lib_sie_tri_mlfmm_interface.f90:285-319). */
+int sie_matvec(sie_ctx* ctx, const double* x, double* y, int nrhs, int precision);
+
+/* Same on device arrays (no host copies); stream may be NULL. */
+int sie_matvec_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, int precision,
+                      void* stream);
+
+/* Plane-wave right-hand sides, get_vector_b_tri + incident_field_tri_general
+ * (src/lib_sie_tri_calculation_mod.f90:391-460, 939-1002).  k_in, E_in: 3 x nrhs. */
+int sie_rhs_planewave(sie_ctx* ctx, const double* k_in, const double* E_in, int nrhs, double* b);
+
+/* Incident direction and polarisation as in kin_and_Ein_calculation
+ * (src/lib_sie_math.f90:259-293): theta, phi [rad], pol 1 = TM, 2 = TE,
+ * k_dir = calc_p(7).  Writes k_in[3], E_in[3]. */
+int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in);
+
+/* Solve Z x = b.  Replaces lib_sie_solver_gmres_run
+ * (src/lib_sie_solver_gmres_interface.f90:123-211) and the CERFACS zgmres
+ * driver (src/lib/libmath_external/src/algorithm_842/zPackgmres.f90:537-1565). */
+int sie_solve(sie_ctx* ctx, const double* b, double* x, int nrhs, const sie_solver_cfg* cfg,
+              sie_stats* stats);
+int sie_solve_device(sie_ctx* ctx, const double* d_b, double* d_x, int nrhs,
+                     const sie_solver_cfg* cfg, sie_stats* stats);
+
+/* Left Jacobi preconditioner, lib_sie_ml_fmm_preconditioner_left
+ * (src/lib_sie_tri_mlfmm_interface.f90:323-339): v2 = v1 / diag. */
+int sie_precondition_left(sie_ctx* ctx, const double* v1, double* v2);
+
+/* Scattered E and H at observation points (Integration_scattered_field_tri,
+ * src/lib_sie_tri_calculation_mod.f90:2782-2825) and the 'rcs' intensity
+ * |E|^2 4 pi |r|^2 (src/lib_sie_tri_solver_normal.f90:325-342).
+ * pts: npts x 3; E, H: npts x 3 complex (may be NULL); intensity: npts. */
+int sie_farfield(sie_ctx* ctx, const double* x, const double* pts, int npts, double* E,
+                 double* H, double* intensity);
+
+/* Introspection for parity tests. */
+int sie_get_edges(const sie_ctx* ctx, int* elem, int* corner);
+int sie_get_tree(const sie_ctx* ctx, double* D_xmin, long long* leaf_box);
+/* 2x2 blocks (D11, D12, D21, D22 complex) of arbitrary edge pairs through the
+ * fill kernels. */
+int sie_get_blocks(sie_ctx* ctx, const int* m, const int* n, int cnt, double* out);
+/* Near-field matrix entry (m, n) as stored after sie_setup (0 if not near). */
+int sie_get_near_entries(sie_ctx* ctx, const int* m, const int* n, int cnt, double* out);
+/* Radiation patterns of edges (4 x Q complex each: med1 theta, med1 phi, med2 theta, med2 phi). */
+int sie_get_rt(sie_ctx* ctx, const int* edges, int cnt, double* out);
+int sie_num_directions(const sie_ctx* ctx, int* Q);
+/* Device-side timings of the last sie_setup / sie_matvec phases [ms]. */
+int sie_get_timings(const sie_ctx* ctx, double* out, int n);
+
+/* Launch all further work of ctx on the caller's CUDA stream (NULL: back to the
+ * library's own stream). */
+int sie_set_stream(sie_ctx* ctx, void* stream);
+
+/* Number of kernels this library has launched since it was loaded. */
+unsigned long long sie_launch_count(void);
+
+int sie_free(sie_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SIE_GPU_H */

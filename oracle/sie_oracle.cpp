@@ -1,0 +1,1509 @@
+// SpeckleSim SIE hot path -- CPU ORACLE (test infrastructure only).
+//
+// This file is the parity checker for the B200 library.  It is a plain FP64 C++
+// restatement of the reference Fortran algorithm and is only ever linked by the
+// test-suite, by __graft_entry__.smoke() and by bench.py's cpu_baseline /
+// --impl reference leg.  The product library (specklesim_b200/csrc) never calls it.
+//
+// Parity status: the SIE blocks, matvec and currents have no golden vectors in the
+// reference (its SIE fixtures are missing), so those are pinned by the reference's
+// own probes restated here (K2q/K3q/K4q vs 12-point quadrature), by the dense vs
+// MLFMM cross-check and by physics (reciprocity, Mie).  The special functions and
+// GMRES are pinned against the reference's known-answer tests (tests/golden).
+//
+// Reference files (paths inside the SpeckleSim project):
+//   src/lib_sie_tri_calculation_mod.f90   near-field blocks, RHS, far field
+//   src/lib_sie_integration_points.f90    triangle rules (binary32 literals)
+//   src/lib_sie_tri_mlfmm_interface.f90   near CSR, matvec callback, MLFMM plug-ins
+//   src/lib_sie_tri_mlfmm.f90             RT, receive summation
+//   src/lib_sie_mlfmm.f90                 TL tables, k-space sampling
+//   src/lib_sie_lookup_table.f90          offset -> TL index lookup
+//   src/lib/libtree/lib/lib_tree*.f90     octree (Morton universal index)
+//   src/lib/libmlfmm/lib/lib_ml_fmm.f90   engine pass order
+//   src/lib/libmath_external/src/algorithm_842/zPackgmres.f90   GMRES
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+typedef std::complex<double> cd;
+static const double PI = 3.141592653589793238462643383279502884;  // 4*atan(1d0)
+static const cd IM(0.0, 1.0);
+
+// Unsuffixed Fortran literals are binary32 (no real-kind promotion flag in the
+// reference build); src/lib_sie_constants.f90:9-11.
+static inline double f32(double x) { return (double)(float)x; }
+static const double C0 = (double)2.99792458e+8f;
+static const double EPS0 = (double)8.854187817e-12f;
+static const double MU0 = (double)1.2566370614e-6f;
+
+struct V3 {
+  double x, y, z;
+};
+static inline V3 v3(double a, double b, double c) { return V3{a, b, c}; }
+static inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V3 operator*(V3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
+static inline V3 operator/(V3 a, double s) { return v3(a.x / s, a.y / s, a.z / s); }
+static inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) {
+  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline double vlen(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+struct C3 {
+  cd x, y, z;
+};
+static inline C3 c3zero() { return C3{0.0, 0.0, 0.0}; }
+static inline C3 operator+(C3 a, C3 b) { return C3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline C3 operator*(V3 a, cd s) { return C3{a.x * s, a.y * s, a.z * s}; }
+static inline C3 operator*(C3 a, cd s) { return C3{a.x * s, a.y * s, a.z * s}; }
+static inline cd rdot(V3 a, C3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// cross_rc (src/lib_sie_math.f90:561-572): cmplx(v1) without a kind parameter
+// rounds the real vector to binary32 before the product.
+static inline C3 cross_rc(V3 a, C3 b) {
+  double ax = f32(a.x), ay = f32(a.y), az = f32(a.z);
+  return C3{ay * b.z - az * b.y, az * b.x - ax * b.z, ax * b.y - ay * b.x};
+}
+
+// ---------------------------------------------------------------------------
+// Triangle rules, src/lib_sie_integration_points.f90:7-141 (binary32 literals).
+struct Rule {
+  int n;
+  double a[12], b[12], w[12];
+};
+static Rule make_rule(int ngp) {
+  Rule r;
+  std::memset(&r, 0, sizeof(r));
+  r.n = ngp;
+  if (ngp == 1) {
+    r.a[0] = 0.33333333333333f; r.b[0] = 0.33333333333333f; r.w[0] = 1.0f;
+  } else if (ngp == 3) {
+    const float a[3] = {0.16666666666667f, 0.16666666666667f, 0.66666666666667f};
+    const float b[3] = {0.16666666666667f, 0.66666666666667f, 0.16666666666667f};
+    for (int i = 0; i < 3; i++) { r.a[i] = a[i]; r.b[i] = b[i]; r.w[i] = 0.33333333333333f; }
+  } else if (ngp == 4) {
+    const float a[4] = {0.33333333333333f, 0.20000000000000f, 0.20000000000000f, 0.60000000000000f};
+    const float b[4] = {0.33333333333333f, 0.20000000000000f, 0.60000000000000f, 0.20000000000000f};
+    const float w[4] = {-0.56250000000000f, 0.52083333333333f, 0.52083333333333f, 0.52083333333333f};
+    for (int i = 0; i < 4; i++) { r.a[i] = a[i]; r.b[i] = b[i]; r.w[i] = w[i]; }
+  } else if (ngp == 6) {
+    const float a[6] = {0.44594849091597f, 0.44594849091597f, 0.10810301816807f,
+                        0.09157621350977f, 0.09157621350977f, 0.81684757298046f};
+    const float b[6] = {0.44594849091597f, 0.10810301816807f, 0.44594849091597f,
+                        0.09157621350977f, 0.81684757298046f, 0.09157621350977f};
+    const float w[6] = {0.22338158967801f, 0.22338158967801f, 0.22338158967801f,
+                        0.10995174365532f, 0.10995174365532f, 0.10995174365532f};
+    for (int i = 0; i < 6; i++) { r.a[i] = a[i]; r.b[i] = b[i]; r.w[i] = w[i]; }
+  } else if (ngp == 7) {
+    const float a[7] = {0.33333333333333f, 0.47014206410511f, 0.47014206410511f, 0.05971587178977f,
+                        0.10128650732346f, 0.10128650732346f, 0.79742698535309f};
+    const float b[7] = {0.33333333333333f, 0.47014206410511f, 0.05971587178977f, 0.47014206410511f,
+                        0.10128650732346f, 0.79742698535309f, 0.10128650732346f};
+    const float w[7] = {0.22500000000000f, 0.13239415278851f, 0.13239415278851f, 0.13239415278851f,
+                        0.12593918054483f, 0.12593918054483f, 0.12593918054483f};
+    for (int i = 0; i < 7; i++) { r.a[i] = a[i]; r.b[i] = b[i]; r.w[i] = w[i]; }
+  } else if (ngp == 12) {
+    const float a[12] = {0.249286745170910f, 0.249286745170910f, 0.501426509658180f,
+                         0.063089014491500f, 0.063089014491500f, 0.873821971017000f,
+                         0.310352451033780f, 0.636502499121400f, 0.053145049844820f,
+                         0.636502499121400f, 0.310352451033780f, 0.053145049844820f};
+    const float b[12] = {0.249286745170910f, 0.501426509658180f, 0.249286745170910f,
+                         0.063089014491500f, 0.873821971017000f, 0.063089014491500f,
+                         0.636502499121400f, 0.053145049844820f, 0.310352451033780f,
+                         0.310352451033780f, 0.053145049844820f, 0.636502499121400f};
+    const float w[12] = {0.116786275726380f, 0.116786275726380f, 0.116786275726380f,
+                         0.0508449063702100f, 0.0508449063702100f, 0.0508449063702100f,
+                         0.0828510756183700f, 0.0828510756183700f, 0.0828510756183700f,
+                         0.0828510756183700f, 0.0828510756183700f, 0.0828510756183700f};
+    for (int i = 0; i < 12; i++) { r.a[i] = a[i]; r.b[i] = b[i]; r.w[i] = w[i]; }
+  } else {
+    r.n = 0;
+  }
+  return r;
+}
+
+// RWG half basis (fn_rwg, src/lib_sie_type_function.f90:12-20).
+struct Fn {
+  V3 c[3];  // p1, p2 (common edge, in triangle order), pc (free vertex)
+  double area, length, df;
+  int sign;
+  V3 mid, nq;
+};
+
+// r_simplex_new, src/lib_sie_tri_calculation_mod.f90:2741-2749
+static inline V3 simplex(double a, double b, const V3* c) {
+  double w0 = 1 - a - b;
+  return v3(w0 * c[0].x + a * c[1].x + b * c[2].x, w0 * c[0].y + a * c[1].y + b * c[2].y,
+            w0 * c[0].z + a * c[1].z + b * c[2].z);
+}
+
+struct Params {
+  double lambda;
+  cd eps_r1, eps_r2;
+  int formulation;  // 1 PMCHWT, 3 ICTF
+  int ngp;
+  int s_opt;
+  int K;
+  int normal_conv;  // calc_p(7): 1 or 2
+  int fix_itbn;
+};
+
+struct Material {
+  double k0, omega, my1, my2;
+  cd k1, k2, eps1, eps2, eta1, eta2, eta_a;
+};
+
+// set_local_material_parameters_tri, src/lib_sie_tri_data_container.f90:212-224
+static Material make_material(const Params& p) {
+  Material m;
+  m.k0 = 2 * PI / p.lambda;
+  m.omega = 2 * PI * C0 / p.lambda;
+  m.my1 = MU0;
+  m.my2 = MU0;
+  m.k1 = m.k0 * std::sqrt(p.eps_r1);
+  m.k2 = m.k0 * std::sqrt(p.eps_r2);
+  m.eps1 = EPS0 * p.eps_r1;
+  m.eps2 = EPS0 * p.eps_r2;
+  m.eta1 = std::sqrt(m.my1 / m.eps1);
+  m.eta2 = std::sqrt(m.my2 / m.eps2);
+  m.eta_a = (m.eta1 + m.eta2) / 2.0;
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Hänninen singular integrals (PIER 63, 2006), lib_sie_tri_calculation_mod.f90.
+
+struct Edge {
+  V3 ps, pt;
+};
+// edge_vectors_assigned :2706-2717
+static inline void edges_of(const Fn& f, Edge e[3]) {
+  e[0].ps = f.c[2]; e[0].pt = f.c[1];
+  e[1].ps = f.c[0]; e[1].pt = f.c[2];
+  e[2].ps = f.c[1]; e[2].pt = f.c[0];
+}
+// m_vector :1048-1059
+static inline void m_vector(const Fn& f, V3 m[3]) {
+  V3 a = cross(f.nq, f.c[2] - f.c[1]);
+  m[0] = a / vlen(a);
+  V3 b = cross(f.nq, f.c[0] - f.c[2]);
+  m[1] = b / vlen(b);
+  V3 c = cross(f.nq, f.c[1] - f.c[0]);
+  m[2] = c / vlen(c);
+}
+
+// Iq_L :1074-1119 (line integrals, eq. 33)
+static double Iq_L(int q, V3 Ra, V3 p1, V3 p2) {
+  V3 s = (p2 - p1) / vlen(p2 - p1);
+  double Sp = dot(p2 - Ra, s);
+  double Sn = dot(p1 - Ra, s);
+  double Rn = vlen(Ra - p1);
+  double Rp = vlen(Ra - p2);
+  double Sum_p = Rp + Sp, Sum_n = Rn + Sn, Dif_p = Rp - Sp, Dif_n = Rn - Sn;
+  double R0 = std::sqrt(Rp * Rp - Sp * Sp);
+  double IL_n1;
+  if (R0 == 0.0) {
+    IL_n1 = std::log(Sp / Sn);
+  } else if (std::fabs(Dif_p) > std::fabs(Sum_n)) {
+    IL_n1 = std::log(Dif_n / Dif_p);
+  } else {
+    IL_n1 = std::log(Sum_p / Sum_n);
+  }
+  double IL_p1 = 0.5 * R0 * R0 * IL_n1 + 0.5 * (Sp * Rp - Sn * Rn);
+  double IL_p3 = 0.75 * R0 * R0 * IL_p1 + 0.25 * (Sp * Rp * Rp * Rp - Sn * Rn * Rn * Rn);
+  if (q == -1) return IL_n1;
+  if (q == 1) return IL_p1;
+  if (q == 3) return IL_p3;
+  double IL_p5 = (double)(5.0f / 6.0f) * R0 * R0 * IL_p3 +
+                 (double)(1.0f / 6.0f) * (Sp * std::pow(Rp, 5) - Sn * std::pow(Rn, 5));
+  return IL_p5;
+}
+
+// Iq_s :1256-1331 (surface integrals)
+static double Iq_s(int q, V3 Ra, const Fn& fn, bool self) {
+  V3 a[3];
+  for (int i = 0; i < 3; i++) a[i] = (fn.c[i] - Ra) / vlen(fn.c[i] - Ra);
+  double Is_n3 = 0.0;
+  double x = 1 + dot(a[0], a[1]) + dot(a[0], a[2]) + dot(a[1], a[2]);
+  V3 r = cross(a[1], a[2]);
+  double y = std::fabs(dot(a[0], r));
+  double Omeg = 2 * std::atan2(y, x);
+  double h = dot(fn.nq, Ra - fn.mid);
+  if (h == 0.0) {
+    Is_n3 = 0.0;
+  } else if (self) {
+    Is_n3 = 0.0;
+  } else if (Omeg <= PI && Omeg > -PI) {
+    Is_n3 = -1 / h * Omeg;
+  }  // else: the reference prints a warning and leaves Is_n3 = 0
+  V3 mr[3];
+  m_vector(fn, mr);
+  Edge e[3];
+  edges_of(fn, e);
+  double t[3], sum = 0.0;
+  for (int i = 0; i < 3; i++) {
+    t[i] = dot(mr[i], Ra - (e[i].pt + e[i].ps) / 2.0);
+    sum += t[i] * Iq_L(-1, Ra, e[i].pt, e[i].ps);
+  }
+  double Is_n1 = 1.0 * (-1 * h * h * Is_n3 - sum);
+  sum = 0.0;
+  for (int i = 0; i < 3; i++) sum += t[i] * Iq_L(1, Ra, e[i].pt, e[i].ps);
+  double Is_p1 = (double)(1.0f / 3.0f) * (1 * h * h * Is_n1 - sum);
+  if (self && q > -1) return 0.0;
+  if (q == -3) return Is_n3;
+  if (q == -1) return Is_n1;
+  return Is_p1;
+}
+
+// K2q :1333-1364
+static V3 K2q(int q, V3 Ra, const Fn& fn, bool self) {
+  double h = dot(fn.nq, Ra - fn.mid);
+  V3 mv[3];
+  m_vector(fn, mv);
+  Edge e[3];
+  edges_of(fn, e);
+  V3 sum = v3(0, 0, 0);
+  for (int i = 0; i < 3; i++) sum = sum + mv[i] * Iq_L(q + 2, Ra, e[i].ps, e[i].pt);
+  double Is = Iq_s(q, Ra, fn, self);
+  V3 rho = Ra - fn.nq * h;
+  double coef = (q == -1) ? 1.0 : (double)(1.0f / 3.0f);  // 1/(real(q)+2) in binary32
+  return (sum * coef + (rho - fn.c[2]) * Is) * fn.df * 0.5;
+}
+
+// K3q :1397-1419
+static V3 K3q(int q, V3 Ra, const Fn& fn, bool self) {
+  V3 mv[3];
+  m_vector(fn, mv);
+  Edge e[3];
+  edges_of(fn, e);
+  V3 sum = v3(0, 0, 0);
+  for (int i = 0; i < 3; i++) sum = sum + mv[i] * Iq_L(q, Ra, e[i].ps, e[i].pt);
+  double h = dot(fn.nq, Ra - fn.mid);
+  double Is = Iq_s(q - 2, Ra, fn, self);
+  return sum - fn.nq * (h * (double)q) * Is;
+}
+
+// K4q :1366-1395
+static V3 K4q(int q, V3 Ra, const Fn& fn, bool self) {
+  if (self) return v3(0, 0, 0);
+  V3 k3 = K3q(q, Ra, fn, self);
+  return cross(Ra - fn.c[2], k3) * (-fn.df * 0.5);
+}
+
+// Diver_Green :1421-1432 and Diver_Green_s :1435-1451
+static inline void green(cd k, double R, cd& G, cd& DG) {
+  cd e = std::exp(-IM * k * R);
+  DG = -(1.0 + IM * k * R) * e / (4 * PI * R * R);
+  G = e / (4 * PI * R);
+}
+static inline void green_s(cd k, double R, cd& Gs, cd& DGs) {
+  cd e = std::exp(-IM * k * R);
+  if (R == 0.0) {
+    Gs = -IM * k / (4 * PI);
+    DGs = k * k / (8 * PI);
+  } else {
+    Gs = (e - 1.0) / (4 * PI * R) + k * k * R / (8 * PI);
+    DGs = (1.0 - (1.0 + IM * k * R) * e) / (4 * PI * R * R) + k * k / (8 * PI);
+  }
+}
+
+struct Inner {
+  C3 IK, ITa, ITbn;
+  cd ITbt;
+};
+struct Outer {
+  cd Kn, Kt, Tn, Tt;
+};
+
+// tri_inner_integration :2040-2069
+static Inner inner_regular(V3 ra, const Fn& fn, const Rule& R, cd k) {
+  Inner o{c3zero(), c3zero(), c3zero(), 0.0};
+  for (int j = 0; j < R.n; j++) {
+    V3 rq = simplex(R.a[j], R.b[j], fn.c);
+    V3 rfn = (rq - fn.c[2]) * 0.5 * fn.df;
+    V3 Rv = ra - rq;
+    double Rl = vlen(Rv);
+    V3 Rn = Rv / Rl;
+    cd G, DG;
+    green(k, Rl, G, DG);
+    double trf = R.w[j] * fn.area;
+    o.IK = o.IK + cross(rfn, Rn) * (DG * trf);
+    o.ITa = o.ITa + rfn * (G * trf);
+    o.ITbn = o.ITbn + Rn * (fn.df * DG * trf);
+    o.ITbt += fn.df * G * trf;
+  }
+  return o;
+}
+
+// tri_inner_singular_integration_smooth :2071-2107
+static Inner inner_smooth(V3 ra, const Fn& fn, const Rule& R, cd k, bool self) {
+  Inner o{c3zero(), c3zero(), c3zero(), 0.0};
+  for (int j = 0; j < R.n; j++) {
+    V3 rq = simplex(R.a[j], R.b[j], fn.c);
+    V3 rfn = (rq - fn.c[2]) * 0.5 * fn.df;
+    V3 Rv = ra - rq;
+    double Rl = vlen(Rv);
+    cd Gs, DGs;
+    green_s(k, Rl, Gs, DGs);
+    double trf = R.w[j] * fn.area;
+    if (!self) {
+      V3 Rn = Rv / Rl;
+      o.IK = o.IK + cross(rfn, Rn) * (DGs * trf);
+      o.ITbn = o.ITbn + Rn * (fn.df * DGs * trf);
+    }
+    o.ITa = o.ITa + rfn * (Gs * trf);
+    o.ITbt += fn.df * Gs * trf;
+  }
+  return o;
+}
+
+// tri_inner_singular_integration_singular :2109-2145
+static Inner inner_singular(V3 ra, const Fn& fn, cd k, bool self, int fix_itbn) {
+  double Is_n1 = Iq_s(-1, ra, fn, self);
+  V3 K2n1 = K2q(-1, ra, fn, self), K3n1 = K3q(-1, ra, fn, self), K4n1 = K4q(-1, ra, fn, self);
+  double Is_p1 = Iq_s(1, ra, fn, self);
+  V3 K2p1 = K2q(1, ra, fn, self), K3p1 = K3q(1, ra, fn, self), K4p1 = K4q(1, ra, fn, self);
+  Inner o;
+  cd k2c = k * k;
+  if (self) {
+    o.IK = c3zero();
+  } else {
+    o.IK = K4n1 * cd(1 / (4 * PI)) + K4p1 * (-k2c / (8 * PI));
+  }
+  o.ITa = K2n1 * cd(1 / (4 * PI)) + K2p1 * (-k2c / (8 * PI));
+  if (!fix_itbn) {
+    // :2142  rv%IT_bn = -(fn%df/(4*PI)*K3_n1 - kd**2*fn%df/(8*PI))*K3_p1  (element-wise)
+    cd c = k2c * fn.df / (8 * PI);
+    double a = fn.df / (4 * PI);
+    o.ITbn = C3{-(a * K3n1.x - c) * K3p1.x, -(a * K3n1.y - c) * K3p1.y, -(a * K3n1.z - c) * K3p1.z};
+  } else {
+    o.ITbn = K3n1 * cd(-fn.df / (4 * PI)) + K3p1 * (k2c * fn.df / (8 * PI));
+  }
+  o.ITbt = fn.df / (4 * PI) * Is_n1 - k2c * fn.df / (8 * PI) * Is_p1;
+  return o;
+}
+
+// tri_outer_integration :2255-2302
+static Outer outer_regular(const Fn& fm, const Fn& fn, const Rule& R, int md, cd k) {
+  Outer o{0.0, 0.0, 0.0, 0.0};
+  double xnn = 0, xnt = 0;
+  for (int j = 0; j < R.n; j++) {
+    V3 ra = simplex(R.a[j], R.b[j], fm.c);
+    V3 rfm = (ra - fm.c[2]) * 0.5 * fm.df;
+    V3 rfn = (ra - fn.c[2]) * 0.5 * fn.df;
+    double trf = R.w[j] * fm.area;
+    Inner in = inner_regular(ra, fn, R, k);
+    o.Kn += rdot(rfm, cross_rc(fm.nq, in.IK)) * trf;
+    o.Kt += rdot(rfm, in.IK) * trf;
+    C3 tv = cross_rc(fm.nq, in.ITa * k + in.ITbn * (1.0 / k));
+    o.Tn += IM * trf * rdot(rfm, tv);
+    cd ts = 1.0 / k * fm.df * in.ITbt;
+    o.Tt += IM * trf * (k * rdot(rfm, in.ITa) - ts);
+    xnt -= dot(cross(fm.nq, rfm), rfn) * trf;
+    xnn -= dot(rfm, rfn) * trf;
+  }
+  double sg = (md == 1) ? -0.5 : 0.5;  // 0.5*(-1)**md
+  o.Kn += sg * f32(xnn);                // cmplx(x_nn, 0.0) is binary32
+  o.Kt += sg * f32(xnt);
+  return o;
+}
+
+// tri_outer_integration_singular :2199-2253
+static Outer outer_singular(const Fn& fm, const Fn& fn, const Rule& R, int md, cd k, bool self,
+                            int fix_itbn) {
+  Outer o{0.0, 0.0, 0.0, 0.0};
+  double xnn = 0, xnt = 0;
+  for (int j = 0; j < R.n; j++) {
+    V3 ra = simplex(R.a[j], R.b[j], fm.c);
+    V3 rfm = (ra - fm.c[2]) * 0.5 * fm.df;
+    V3 rfn = (ra - fn.c[2]) * 0.5 * fn.df;
+    double trf = R.w[j] * fm.area;
+    Inner a = inner_singular(ra, fn, k, self, fix_itbn);
+    Inner b = inner_smooth(ra, fn, R, k, self);
+    Inner in{a.IK + b.IK, a.ITa + b.ITa, a.ITbn + b.ITbn, a.ITbt + b.ITbt};
+    o.Kn += rdot(rfm, cross_rc(fm.nq, in.IK)) * trf;
+    o.Kt += rdot(rfm, in.IK) * trf;
+    C3 tv = cross_rc(fm.nq, in.ITa * k) + cross_rc(fm.nq, in.ITbn * (1.0 / k));
+    o.Tn += IM * trf * rdot(rfm, tv);
+    cd ts = 1.0 / k * fm.df * in.ITbt;
+    o.Tt += IM * trf * (k * rdot(rfm, in.ITa) - ts);
+    xnt -= dot(cross(fm.nq, rfm), rfn) * trf;
+    xnn -= dot(rfm, rfn) * trf;
+  }
+  double sg = (md == 1) ? -0.5 : 0.5;
+  o.Kn += sg * f32(xnn);
+  o.Kt += sg * f32(xnt);
+  return o;
+}
+
+// tri_outer_integration_edge_adjacent :2165-2197 (PMCHWT only)
+static cd outer_edge_adjacent(const Fn& fm, const Fn& fn, int md, cd k) {
+  Rule R = make_rule(12);
+  cd Kt = 0.0;
+  double xnt = 0;
+  for (int j = 0; j < R.n; j++) {
+    V3 ra = simplex(R.a[j], R.b[j], fm.c);
+    V3 rfm = (ra - fm.c[2]) * 0.5 * fm.df;
+    V3 rfn = (ra - fn.c[2]) * 0.5 * fn.df;
+    double trf = R.w[j] * fm.area;
+    C3 Ik = c3zero();
+    for (int i = 0; i < R.n; i++) {
+      V3 rq = simplex(R.a[i], R.b[i], fn.c);
+      V3 rfq = (rq - fn.c[2]) * 0.5 * fn.df;
+      V3 Rv = ra - rq;
+      double Rl = vlen(Rv);
+      cd G, DG;
+      green(k, Rl, G, DG);
+      Ik = Ik + cross(rfq, Rv / Rl) * (DG * (R.w[i] * fn.area));
+    }
+    Kt += rdot(rfm, Ik) * trf;
+    xnt -= dot(rfn, cross(fm.nq, rfm)) * trf;
+  }
+  double sg = (md == 1) ? -0.5 : 0.5;
+  return Kt + sg * f32(xnt);
+}
+
+// ---------------------------------------------------------------------------
+// Mesh topology.
+
+struct Mesh {
+  std::vector<V3> pts;
+  std::vector<int> tri;      // 3 per triangle, 0-based
+  std::vector<int> elem;     // 2 per edge (triangle of side 1 and side 2)
+  std::vector<int> corner;   // 2 per edge (common vertices, order of triangle side 1)
+  std::vector<V3> centroid;  // per triangle
+  std::vector<Fn> fn;        // 2 per edge
+  std::vector<V3> edge_mid;  // tree position per edge
+};
+
+// find_neighbours :865-905 + common_2 :907-928.  The O(T^2) (i<j) scan order is
+// reproduced by sorting the (i, j) pairs lexicographically.
+static void build_pairs(Mesh& m) {
+  int nt = (int)m.tri.size() / 3;
+  std::map<std::pair<int, int>, std::vector<int>> emap;
+  for (int t = 0; t < nt; t++) {
+    for (int e = 0; e < 3; e++) {
+      int a = m.tri[3 * t + e], b = m.tri[3 * t + (e + 1) % 3];
+      if (a > b) std::swap(a, b);
+      emap[{a, b}].push_back(t);
+    }
+  }
+  std::vector<std::pair<int, int>> prs;
+  for (auto& kv : emap) {
+    auto& L = kv.second;
+    std::sort(L.begin(), L.end());
+    for (size_t i = 0; i < L.size(); i++)
+      for (size_t j = i + 1; j < L.size(); j++) prs.push_back({L[i], L[j]});
+  }
+  std::sort(prs.begin(), prs.end());
+  prs.erase(std::unique(prs.begin(), prs.end()), prs.end());
+  m.elem.clear();
+  m.corner.clear();
+  for (auto& pr : prs) {
+    int i = pr.first, j = pr.second;
+    int com[3], nc = 0;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        if (m.tri[3 * i + a] == m.tri[3 * j + b] && nc < 3) com[nc++] = m.tri[3 * i + a];
+    if (nc != 2) continue;
+    m.elem.push_back(i);
+    m.elem.push_back(j);
+    m.corner.push_back(com[0]);
+    m.corner.push_back(com[1]);
+  }
+}
+
+// fn_parameter_type :1539-1586 and norm_vec_r_new :1017-1033
+static Fn make_fn(const Mesh& m, int e, int ot, int normal_conv) {
+  int t = m.elem[2 * e + ot];
+  int c1 = m.corner[2 * e], c2 = m.corner[2 * e + 1];
+  int nv = 0;
+  V3 pc{0, 0, 0};
+  for (int j = 0; j < 3; j++) {
+    int v = m.tri[3 * t + j];
+    if (v != c1 && v != c2) {
+      pc = m.pts[v];
+      nv = j + 1;
+    }
+  }
+  V3 p1, p2;
+  const int* T = &m.tri[3 * t];
+  if (nv == 1) { p1 = m.pts[T[1]]; p2 = m.pts[T[2]]; }
+  else if (nv == 2) { p1 = m.pts[T[2]]; p2 = m.pts[T[0]]; }
+  else { p1 = m.pts[T[0]]; p2 = m.pts[T[1]]; }
+  Fn f;
+  f.c[0] = p1; f.c[1] = p2; f.c[2] = pc;
+  f.length = vlen(p1 - p2);
+  f.area = 0.5 * vlen(cross(p1 - pc, p2 - pc));
+  f.sign = (ot == 0) ? 1 : -1;
+  f.df = f.sign * f.length / f.area;
+  f.mid = m.centroid[t];
+  V3 a, b;
+  if (normal_conv == 1) { a = p1 - p2; b = pc - p2; }
+  else { a = pc - p1; b = p2 - p1; }
+  V3 n = cross(a, b);
+  f.nq = n / vlen(n);
+  return f;
+}
+
+static void build_mesh(Mesh& m, const double* verts, int nv, const int* tris, int nt, int normal_conv) {
+  m.pts.resize(nv);
+  for (int i = 0; i < nv; i++) m.pts[i] = v3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+  m.tri.assign(tris, tris + 3 * nt);
+  m.centroid.resize(nt);
+  for (int t = 0; t < nt; t++) {
+    V3 a = m.pts[m.tri[3 * t]], b = m.pts[m.tri[3 * t + 1]], c = m.pts[m.tri[3 * t + 2]];
+    m.centroid[t] = (a + b + c) / 3.0;
+  }
+  build_pairs(m);
+  int M = (int)m.elem.size() / 2;
+  m.fn.resize(2 * M);
+  m.edge_mid.resize(M);
+  for (int e = 0; e < M; e++) {
+    m.fn[2 * e] = make_fn(m, e, 0, normal_conv);
+    m.fn[2 * e + 1] = make_fn(m, e, 1, normal_conv);
+    m.edge_mid[e] = (m.fn[2 * e].c[0] + m.fn[2 * e].c[1]) / 2.0;  // fn_edge_center :712-742
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Near-field 2x2 block, lib_sie_tri_get_impedance_edges :463-644.
+static void block(const Mesh& ms, const Params& P, const Material& mt, const Rule& R, int m, int n,
+                  double r_ref, cd D[4]) {
+  D[0] = D[1] = D[2] = D[3] = 0.0;
+  for (int t = 0; t < 2; t++) {
+    for (int s = 0; s < 2; s++) {
+      int p = ms.elem[2 * m + t], q = ms.elem[2 * n + s];
+      double r_ob = vlen(ms.centroid[p] - ms.centroid[q]);
+      const Fn& fm = ms.fn[2 * m + t];
+      const Fn& fn = ms.fn[2 * n + s];
+      Outer r1, r2;
+      bool singular = !(r_ob > 1.5 * r_ref);
+      bool self = (p == q);
+      if (singular) {
+        r1 = outer_singular(fm, fn, R, 1, mt.k1, self, P.fix_itbn);
+        r2 = outer_singular(fm, fn, R, 2, mt.k2, self, P.fix_itbn);
+        if (P.formulation == 1 && !self) {
+          int cnt = 0;
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+              if (ms.tri[3 * p + a] == ms.tri[3 * q + b]) cnt++;
+          if (cnt == 2) {
+            r1.Kt = outer_edge_adjacent(fm, fn, 1, mt.k1);
+            r2.Kt = outer_edge_adjacent(fm, fn, 2, mt.k2);
+          }
+        }
+      } else {
+        r1 = outer_regular(fm, fn, R, 1, mt.k1);
+        r2 = outer_regular(fm, fn, R, 2, mt.k2);
+      }
+      if (P.formulation == 1) {  // PMCHWT :1713-1769, :481-500
+        cd z1 = mt.eta1 * r1.Tt + mt.eta2 * r2.Tt;
+        cd z2 = -(r1.Kt + r2.Kt);
+        cd z3 = 1.0 / mt.eta1 * r1.Tt + 1.0 / mt.eta2 * r2.Tt;
+        D[0] += z1;
+        D[1] += z2;
+        D[2] = -D[1];
+        D[3] += z3;
+      } else {  // ICTF :1876-1919
+        D[0] += (mt.eta1 * r1.Tt + mt.eta2 * r2.Tt) / mt.eta_a;
+        D[1] += -(r1.Kt + r2.Kt) / mt.eta_a;
+        D[2] += (r1.Kt + r2.Kt) * mt.eta_a;
+        D[3] += (r1.Tt / mt.eta1 + r2.Tt / mt.eta2) * mt.eta_a;
+      }
+    }
+  }
+}
+
+static double r_ref_of(const Mesh& ms, int m) {
+  return vlen(ms.centroid[ms.elem[2 * m]] - ms.centroid[ms.elem[2 * m + 1]]);
+}
+
+// ---------------------------------------------------------------------------
+// Octree (libtree), Morton universal index with x as the most significant bit.
+
+static const int L_TH = 21;  // int(8 bytes * 8 bits / 3)
+
+static inline uint64_t morton3(uint64_t ix, uint64_t iy, uint64_t iz, int l) {
+  uint64_t n = 0;
+  for (int b = l - 1; b >= 0; b--) {
+    n = (n << 3) | (((ix >> b) & 1) << 2) | (((iy >> b) & 1) << 1) | ((iz >> b) & 1);
+  }
+  return n;
+}
+static inline void demorton3(uint64_t n, int l, int64_t& ix, int64_t& iy, int64_t& iz) {
+  ix = iy = iz = 0;
+  for (int b = 0; b < l; b++) {
+    iz |= (int64_t)((n >> (3 * b)) & 1) << b;
+    iy |= (int64_t)((n >> (3 * b + 1)) & 1) << b;
+    ix |= (int64_t)((n >> (3 * b + 2)) & 1) << b;
+  }
+}
+
+struct Tree {
+  double xmin[3], D;
+  int l_min, l_max;
+  std::vector<uint64_t> n_th;  // per element at level 21
+  std::vector<uint64_t> leaf;  // per element at l_max
+  std::vector<std::vector<uint64_t>> boxes;  // per level (index = level), sorted unique
+  std::map<uint64_t, std::vector<int>> leaf_elems;  // leaf box -> elements (ascending)
+};
+
+// lib_tree_get_scaled_element_list (lib_tree.f90:370-434) +
+// lib_tree_hf_get_coordinate_binary_number_1D_double (helper :547-629): the
+// binary coordinate is floor(f * 2^64); its top l bits are floor(f * 2^l).
+static uint64_t coord_bits(double f, int l) {
+  if (!(f > 0.0)) return 0;
+  double s = std::ldexp(f, l);
+  return (uint64_t)std::floor(s);
+}
+
+static void build_tree(const Mesh& ms, int s_opt, Tree& T) {
+  int N = (int)ms.edge_mid.size();
+  double xmax[3], Dd[3];
+  for (int d = 0; d < 3; d++) { T.xmin[d] = 1e300; xmax[d] = -1e300; }
+  for (auto& p : ms.edge_mid) {
+    double c[3] = {p.x, p.y, p.z};
+    for (int d = 0; d < 3; d++) {
+      T.xmin[d] = std::min(T.xmin[d], c[d]);
+      xmax[d] = std::max(xmax[d], c[d]);
+    }
+  }
+  for (int d = 0; d < 3; d++) Dd[d] = (xmax[d] - T.xmin[d]) * (1 + std::ldexp(1.0, -52));
+  T.D = std::max(Dd[0], std::max(Dd[1], Dd[2]));
+  T.n_th.resize(N);
+  std::vector<uint64_t> ic(3 * N);
+  for (int e = 0; e < N; e++) {
+    V3 p = ms.edge_mid[e];
+    double c[3] = {p.x, p.y, p.z};
+    for (int d = 0; d < 3; d++) ic[3 * e + d] = coord_bits((c[d] - T.xmin[d]) / T.D, L_TH);
+    T.n_th[e] = morton3(ic[3 * e], ic[3 * e + 1], ic[3 * e + 2], L_TH);
+  }
+  // lib_tree_get_level_max (lib_tree.f90:1290-1345)
+  std::vector<uint64_t> srt = T.n_th;
+  std::sort(srt.begin(), srt.end());
+  int l_max = 1;
+  for (int i = 0; i + s_opt < N; i++) {
+    uint64_t a = srt[i], b = srt[i + s_opt];
+    for (int lev = L_TH - 1; lev >= 0; lev--) {
+      int sh = 3 * (L_TH - lev);
+      if ((a >> sh) == (b >> sh)) {
+        l_max = std::max(l_max, lev + 1);
+        break;
+      }
+    }
+  }
+  T.l_max = l_max;
+  T.l_min = 2;  // 1 + floor(log2(k+1)), k = 1  (lib_tree.f90:1264-1271)
+  if (T.l_max < T.l_min) T.l_min = T.l_max;
+  T.leaf.resize(N);
+  T.leaf_elems.clear();
+  for (int e = 0; e < N; e++) {
+    T.leaf[e] = T.n_th[e] >> (3 * (L_TH - l_max));
+    T.leaf_elems[T.leaf[e]].push_back(e);
+  }
+  T.boxes.assign(l_max + 1, {});
+  for (int l = T.l_min; l <= l_max; l++) {
+    std::vector<uint64_t> v(N);
+    for (int e = 0; e < N; e++) v[e] = T.leaf[e] >> (3 * (l_max - l));
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    T.boxes[l] = v;
+  }
+}
+
+// lib_tree_hf_get_neighbour_all_xD (k = 1), self excluded.
+static std::vector<uint64_t> neighbours(uint64_t n, int l) {
+  int64_t ix, iy, iz;
+  demorton3(n, l, ix, iy, iz);
+  int64_t ub = ((int64_t)1 << l) - 1;
+  std::vector<uint64_t> r;
+  for (int dx = -1; dx <= 1; dx++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dz = -1; dz <= 1; dz++) {
+        int64_t a = ix + dx, b = iy + dy, c = iz + dz;
+        if (a < 0 || b < 0 || c < 0 || a > ub || b > ub || c > ub) continue;
+        uint64_t m = morton3(a, b, c, l);
+        if (m != n) r.push_back(m);
+      }
+  return r;
+}
+
+// lib_tree_get_domain_i4 (lib_tree.f90:1096-1245)
+static std::vector<uint64_t> domain_i4(uint64_t n, int l) {
+  std::vector<uint64_t> par = neighbours(n >> 3, l - 1);
+  par.push_back(n >> 3);
+  std::vector<uint64_t> own = neighbours(n, l);
+  own.push_back(n);
+  std::sort(own.begin(), own.end());
+  std::vector<uint64_t> r;
+  for (uint64_t p : par)
+    for (uint64_t c = 0; c < 8; c++) {
+      uint64_t ch = (p << 3) | c;
+      if (!std::binary_search(own.begin(), own.end(), ch)) r.push_back(ch);
+    }
+  std::sort(r.begin(), r.end());
+  return r;
+}
+
+static V3 box_centre(const Tree& T, uint64_t n, int l) {
+  int64_t ix, iy, iz;
+  demorton3(n, l, ix, iy, iz);
+  double s = std::ldexp(1.0, -l);
+  double c[3] = {s * (ix + 0.5), s * (iy + 0.5), s * (iz + 0.5)};
+  return v3(c[0] * T.D + T.xmin[0], c[1] * T.D + T.xmin[1], c[2] * T.D + T.xmin[2]);
+}
+
+// ---------------------------------------------------------------------------
+// Special functions for the translation operator (setup only).
+
+// Gauss-Legendre nodes on [-1,1] ascending, Newton on P_n (the reference uses
+// the Glaser-Liu-Rokhlin rule, Gauss_Quadrature_Fast.f90:424-498; both are exact
+// to rounding).
+static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  auto legendre = [n](double z, double& pn, double& dpn) {
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= n; k++) {
+      double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    pn = p1;
+    dpn = n * (z * p1 - p0) / (z * z - 1.0);
+  };
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(PI * (i + 0.75) / (n + 0.5));
+    double pn, dp;
+    int extra = 0;
+    for (int it = 0; it < 100 && extra < 2; it++) {
+      legendre(z, pn, dp);
+      double dz = pn / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-15) extra++;
+    }
+    legendre(z, pn, dp);
+    x[n - 1 - i] = z;  // ascending
+    w[n - 1 - i] = 2.0 / ((1 - z * z) * dp * dp);
+  }
+}
+
+// Spherical Hankel function of the second kind h2_n(z) = j_n(z) - i y_n(z),
+// orders 0..nmax-1 (lib_math_bessel.f90:935-990, A&S 10.1).  For real z, j_n by
+// Miller's downward recurrence and y_n upward; for complex z, h2 by the upward
+// recurrence from h2_0 = i e^{-iz}/z, h2_{-1} = e^{-iz}/z (accurate where the
+// separate j and y lose all digits to cancellation).
+static void hankel2(cd z, int nmax, std::vector<cd>& h) {
+  h.assign(nmax, 0.0);
+  if (z.imag() == 0.0) {
+    double x = z.real();
+    std::vector<double> j(nmax + 1), y(nmax + 1);
+    y[0] = -std::cos(x) / x;
+    if (nmax > 1) y[1] = -std::cos(x) / (x * x) - std::sin(x) / x;
+    for (int n = 1; n + 1 < nmax; n++) y[n + 1] = (2 * n + 1) / x * y[n] - y[n - 1];
+    int start = std::max(nmax + 20, (int)(std::fabs(x)) + 40);
+    std::vector<double> jj(start + 2, 0.0);
+    jj[start + 1] = 0.0;
+    jj[start] = 1e-300;
+    for (int n = start; n >= 1; n--) {
+      jj[n - 1] = (2 * n + 1) / x * jj[n] - jj[n + 1];
+      if (std::fabs(jj[n - 1]) > 1e250) {
+        for (int k = n - 1; k <= start + 1; k++) jj[k] *= 1e-250;
+      }
+    }
+    double j0 = std::sin(x) / x;
+    double j1 = std::sin(x) / (x * x) - std::cos(x) / x;
+    double scale = (std::fabs(j0) >= std::fabs(j1)) ? j0 / jj[0] : j1 / jj[1];
+    for (int n = 0; n < nmax; n++) h[n] = cd(jj[n] * scale, -y[n]);
+    return;
+  }
+  cd e = std::exp(-IM * z);
+  cd hm1 = e / z, h0 = IM * e / z;
+  h[0] = h0;
+  cd prev = hm1, cur = h0;
+  for (int n = 0; n + 1 < nmax; n++) {
+    cd nxt = (double)(2 * n + 1) / z * cur - prev;
+    prev = cur;
+    cur = nxt;
+    h[n + 1] = cur;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MLFMM state.
+
+struct Fmm {
+  int K, Q;
+  std::vector<V3> khat, tth, tph;
+  std::vector<double> trf;
+  // RT per edge: [e][med][comp][q], comp 0 = theta (a_nm), 1 = phi (b_nm)
+  std::vector<cd> rt;
+  // TL per level: [lvl][343][med][q]
+  std::vector<std::vector<cd>> tl;
+  std::vector<double> tl_xmin, tl_dx;
+  // near CSR (1 row per edge, 2x2 blocks)
+  std::vector<int> ia, ja;
+  std::vector<cd> a, b, c, d;
+};
+
+// Khat_and_TRF_ExtendedK, lib_sie_mlfmm.f90:190-240
+static void make_sampling(Fmm& F) {
+  int K = F.K, Ns = 2 * K * K;
+  F.Q = Ns + 2;
+  std::vector<double> xx, ww;
+  gauss_legendre(K, xx, ww);
+  F.khat.resize(F.Q);
+  F.tth.resize(F.Q);
+  F.tph.resize(F.Q);
+  F.trf.resize(F.Q);
+  double dphi = 2 * PI / (2 * K);
+  for (int j = 0; j < K; j++)
+    for (int k = 0; k < 2 * K; k++) {
+      double phi = k * dphi;
+      int i = k + j * 2 * K;
+      double st = std::sin(std::acos(xx[j]));
+      F.khat[i] = v3(st * std::cos(phi), st * std::sin(phi), xx[j]);
+      F.tth[i] = v3(xx[j] * std::cos(phi), xx[j] * std::sin(phi), -st);
+      F.tph[i] = v3(-std::sin(phi), std::cos(phi), 0.0);
+      F.trf[i] = ww[j] * dphi;
+    }
+  F.khat[Ns] = v3(0, 0, 1);
+  F.khat[Ns + 1] = v3(0, 0, -1);
+  F.tth[Ns] = F.tth[Ns + 1] = v3(1, 0, 0);
+  F.tph[Ns] = F.tph[Ns + 1] = v3(0, 1, 0);
+  F.trf[Ns] = F.trf[Ns + 1] = 0.0;
+}
+
+// PreCalculate_RT + RT_function_SCSArr_New, lib_sie_tri_mlfmm.f90:503-583
+static void make_rt(const Mesh& ms, const Material& mt, const Rule& R, const Tree& T, Fmm& F) {
+  int M = (int)ms.edge_mid.size(), Q = F.Q;
+  F.rt.assign((size_t)M * 4 * Q, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int e = 0; e < M; e++) {
+    V3 Rc = box_centre(T, T.leaf[e], T.l_max);
+    for (int ll = 0; ll < 2; ll++) {
+      const Fn& f = ms.fn[2 * e + ll];
+      double dfm = f.sign * f.length;
+      for (int i = 0; i < Q; i++) {
+        C3 sa = c3zero(), sb = c3zero();
+        for (int j = 0; j < R.n; j++) {
+          V3 Ro = simplex(R.a[j], R.b[j], f.c);
+          V3 fm = (Ro - f.c[2]) * 0.5 * dfm;
+          double tmp = dot(F.khat[i], Ro - Rc);
+          cd f1 = std::exp(-IM * mt.k1 * tmp) * R.w[j];
+          cd f2 = std::exp(-IM * mt.k2 * tmp) * R.w[j];
+          sa = sa + fm * f1;
+          sb = sb + fm * f2;
+        }
+        cd* r = &F.rt[(size_t)e * 4 * Q];
+        r[0 * Q + i] += rdot(F.tth[i], sa);  // med 1, theta
+        r[1 * Q + i] += rdot(F.tph[i], sa);  // med 1, phi
+        r[2 * Q + i] += rdot(F.tth[i], sb);  // med 2, theta
+        r[3 * Q + i] += rdot(F.tph[i], sb);  // med 2, phi
+      }
+    }
+  }
+}
+
+// precalculation_LT3_TL + PreCalc_transfer_function + TL_km_ml_fmm,
+// lib_sie_mlfmm.f90:27-188
+static void make_tl(const Material& mt, const Tree& T, Fmm& F) {
+  int Q = F.Q, K = F.K;
+  F.tl.assign(T.l_max + 1, {});
+  F.tl_xmin.assign(T.l_max + 1, 0.0);
+  F.tl_dx.assign(T.l_max + 1, 0.0);
+  for (int l = T.l_min; l <= T.l_max; l++) {
+    double dc = std::ldexp(1.0, -l) * T.D;
+    double xmn = -3 * dc, xmx = -xmn;
+    double dx = (xmx - xmn) / 6;
+    F.tl_xmin[l] = xmn;
+    F.tl_dx[l] = dx;
+    F.tl[l].assign((size_t)343 * 2 * Q, 0.0);
+    bool only_k1 = (std::fabs(mt.k2.imag()) > 0.0) && (l < T.l_max);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < 343; t++) {
+      int i = t / 49, j = (t / 7) % 7, k = t % 7;
+      if (i >= 2 && i <= 4 && j >= 2 && j <= 4 && k >= 2 && k <= 4) continue;
+      V3 r = v3(xmn + i * dx, xmn + j * dx, xmn + k * dx);
+      double rl = vlen(r);
+      V3 rh = r / rl;
+      cd kd[2] = {mt.k1, mt.k2};
+      std::vector<cd> h;
+      std::vector<double> P(K);
+      for (int med = 0; med < 2; med++) {
+        if (med == 1 && only_k1) continue;
+        hankel2(kd[med] * rl, K, h);
+        for (int q = 0; q < Q; q++) {
+          double x = dot(rh, F.khat[q]);
+          P[0] = 1.0;
+          if (K > 1) P[1] = x;
+          for (int n = 1; n + 1 < K; n++) P[n + 1] = ((2 * n + 1) * x * P[n] - n * P[n - 1]) / (n + 1);
+          cd acc = 0.0;
+          cd mi = 1.0;
+          for (int n = 1; n <= K; n++) {
+            mi *= -IM;
+            acc += h[n - 1] * mi * (double)(2 * (n - 1) + 1) * P[n - 1] * kd[med] / ((4 * PI) * (4 * PI));
+          }
+          F.tl[l][((size_t)t * 2 + med) * Q + q] = acc;
+        }
+      }
+    }
+  }
+}
+
+// LT3_get_loc + LT3_get_col_at_loc + NINT (lib_sie_lookup_table.f90:572-629):
+// the interpolated index rounds to the nearest grid offset.
+static int tl_index(const Fmm& F, int l, V3 rab) {
+  double c[3] = {rab.x, rab.y, rab.z};
+  int ix[3];
+  for (int d = 0; d < 3; d++) {
+    double fr = (c[d] - F.tl_xmin[l]) / F.tl_dx[l];
+    int r = (int)std::lround(fr);
+    if (r < 0) r = 0;
+    if (r > 6) r = 6;
+    ix[d] = r;
+  }
+  return ix[0] * 49 + ix[1] * 7 + ix[2];
+}
+
+struct Ctx {
+  Params P;
+  Material mt;
+  Rule R;
+  Mesh ms;
+  Tree T;
+  Fmm F;
+  bool have_tree = false, have_fmm = false;
+};
+
+// precalculation_near_field_csr_tri, lib_sie_tri_mlfmm_interface.f90:779-863
+static void make_near(Ctx& C) {
+  int M = (int)C.ms.edge_mid.size();
+  Fmm& F = C.F;
+  F.ia.assign(M + 1, 0);
+  std::vector<std::vector<int>> cols(M);
+  for (int m = 0; m < M; m++) {
+    uint64_t bx = C.T.leaf[m];
+    std::vector<uint64_t> nb = neighbours(bx, C.T.l_max);
+    nb.insert(nb.begin(), bx);
+    for (uint64_t b : nb) {
+      auto it = C.T.leaf_elems.find(b);
+      if (it == C.T.leaf_elems.end()) continue;
+      for (int e : it->second) cols[m].push_back(e);
+    }
+    std::sort(cols[m].begin(), cols[m].end());  // sort_edge_index
+    F.ia[m + 1] = F.ia[m] + (int)cols[m].size();
+  }
+  size_t nnz = F.ia[M];
+  F.ja.resize(nnz);
+  F.a.resize(nnz);
+  F.b.resize(nnz);
+  F.c.resize(nnz);
+  F.d.resize(nnz);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int m = 0; m < M; m++) {
+    double rr = r_ref_of(C.ms, m);
+    for (size_t j = 0; j < cols[m].size(); j++) {
+      size_t o = F.ia[m] + j;
+      F.ja[o] = cols[m][j];
+      cd D[4];
+      block(C.ms, C.P, C.mt, C.R, m, cols[m][j], rr, D);
+      F.a[o] = D[0];
+      F.b[o] = D[1];
+      F.c[o] = D[2];
+      F.d[o] = D[3];
+    }
+  }
+}
+
+// MLFMM matvec: lib_sie_ml_fmm_calculate_vector_b_tri (:285-319) through
+// lib_ml_fmm_run (lib_ml_fmm.f90:269-300) with the SIE plug-ins.
+// faithful_lookup = 1 reproduces the linear CSR search per E2 element
+// (find_elements_in_field_zcsr, lib_sie_mlfmm.f90:612-629).
+static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
+  const Fmm& F = C.F;
+  const Tree& T = C.T;
+  const Material& mt = C.mt;
+  int M = (int)C.ms.edge_mid.size(), Q = F.Q;
+  int L0 = T.l_min, L1 = T.l_max;
+  // coefficient storage per level: [box][8][Q]; item order a1 a2 a3 a4 b1 b2 b3 b4
+  std::vector<std::vector<cd>> Cc(L1 + 1), Dd(L1 + 1);
+  for (int l = L0; l <= L1; l++) {
+    Cc[l].assign(T.boxes[l].size() * 8 * Q, 0.0);
+    Dd[l].assign(T.boxes[l].size() * 8 * Q, 0.0);
+  }
+  auto bidx = [&](int l, uint64_t n) -> long {
+    auto& v = T.boxes[l];
+    auto it = std::lower_bound(v.begin(), v.end(), n);
+    if (it == v.end() || *it != n) return -1;
+    return (long)(it - v.begin());
+  };
+  // upward pass step 1: lib_sie_ml_fmm_get_C (:395-448)
+  {
+    auto& lv = T.boxes[L1];
+#pragma omp parallel for schedule(dynamic)
+    for (long bi = 0; bi < (long)lv.size(); bi++) {
+      cd* Cb = &Cc[L1][(size_t)bi * 8 * Q];
+      const std::vector<int>& el = T.leaf_elems.at(lv[bi]);
+      for (int e : el) {
+        cd xe = x[e], xh = x[e + M];
+        const cd* r = &F.rt[(size_t)e * 4 * Q];
+        for (int k = 0; k < 2; k++) {
+          for (int q = 0; q < Q; q++) {
+            cd fa = std::conj(r[(2 * k) * Q + q]);
+            cd fb = std::conj(r[(2 * k + 1) * Q + q]);
+            Cb[(0 + k) * Q + q] += fa * xe;
+            Cb[(4 + k) * Q + q] += fb * xe;
+            Cb[(2 + k) * Q + q] += fa * xh;
+            Cb[(6 + k) * Q + q] += fb * xh;
+          }
+        }
+      }
+    }
+  }
+  cd kk[2] = {mt.k1, mt.k2};
+  // upward pass step 2: translation_SS (:466-528)
+  for (int l = L1 - 1; l >= L0; l--) {
+    auto& lv = T.boxes[l];
+#pragma omp parallel for schedule(dynamic)
+    for (long bi = 0; bi < (long)lv.size(); bi++) {
+      V3 xp = box_centre(T, lv[bi], l);
+      cd* Cp = &Cc[l][(size_t)bi * 8 * Q];
+      for (uint64_t c = 0; c < 8; c++) {
+        uint64_t ch = (lv[bi] << 3) | c;
+        long ci = bidx(l + 1, ch);
+        if (ci < 0) continue;
+        V3 r = box_centre(T, ch, l + 1) - xp;
+        const cd* Cch = &Cc[l + 1][(size_t)ci * 8 * Q];
+        for (int q = 0; q < Q; q++) {
+          double tmp = dot(F.khat[q], r);
+          cd tk[2] = {std::exp(IM * mt.k1 * tmp), std::exp(IM * mt.k2 * tmp)};
+          for (int j = 0; j < 2; j++) {
+            Cp[(0 + j) * Q + q] += Cch[(0 + j) * Q + q] * tk[j];
+            Cp[(4 + j) * Q + q] += Cch[(4 + j) * Q + q] * tk[j];
+            Cp[(2 + j) * Q + q] += Cch[(2 + j) * Q + q] * tk[j];
+            Cp[(6 + j) * Q + q] += Cch[(6 + j) * Q + q] * tk[j];
+          }
+        }
+      }
+    }
+  }
+  (void)kk;
+  // downward pass step 1: translation_SR over I4 (:547-586)
+  for (int l = L0; l <= L1; l++) {
+    auto& lv = T.boxes[l];
+#pragma omp parallel for schedule(dynamic)
+    for (long bi = 0; bi < (long)lv.size(); bi++) {
+      V3 xa = box_centre(T, lv[bi], l);
+      cd* Db = &Dd[l][(size_t)bi * 8 * Q];
+      std::vector<uint64_t> i4 = domain_i4(lv[bi], l);
+      for (uint64_t sb : i4) {
+        long si = bidx(l, sb);
+        if (si < 0) continue;
+        V3 xb = box_centre(T, sb, l);
+        int ti = tl_index(F, l, xa - xb);
+        const cd* tl = &F.tl[l][(size_t)ti * 2 * Q];
+        const cd* Cs = &Cc[l][(size_t)si * 8 * Q];
+        for (int j = 0; j < 2; j++)
+          for (int q = 0; q < Q; q++) {
+            cd t = F.trf[q] * tl[j * Q + q];
+            Db[(0 + j) * Q + q] += Cs[(0 + j) * Q + q] * t;
+            Db[(4 + j) * Q + q] += Cs[(4 + j) * Q + q] * t;
+            Db[(2 + j) * Q + q] += Cs[(2 + j) * Q + q] * t;
+            Db[(6 + j) * Q + q] += Cs[(6 + j) * Q + q] * t;
+          }
+      }
+    }
+  }
+  // downward pass step 2: translation_RR (:600-655)
+  for (int l = L0 + 1; l <= L1; l++) {
+    auto& lv = T.boxes[l];
+#pragma omp parallel for schedule(dynamic)
+    for (long bi = 0; bi < (long)lv.size(); bi++) {
+      uint64_t par = lv[bi] >> 3;
+      long pi = bidx(l - 1, par);
+      if (pi < 0) continue;
+      V3 r = box_centre(T, lv[bi], l) - box_centre(T, par, l - 1);
+      cd* Db = &Dd[l][(size_t)bi * 8 * Q];
+      const cd* Dp = &Dd[l - 1][(size_t)pi * 8 * Q];
+      for (int q = 0; q < Q; q++) {
+        double tmp = dot(F.khat[q], r);
+        cd tk[2] = {std::exp(-IM * mt.k1 * tmp), std::exp(-IM * mt.k2 * tmp)};
+        for (int j = 0; j < 2; j++) {
+          Db[(0 + j) * Q + q] += Dp[(0 + j) * Q + q] * tk[j];
+          Db[(4 + j) * Q + q] += Dp[(4 + j) * Q + q] * tk[j];
+          Db[(2 + j) * Q + q] += Dp[(2 + j) * Q + q] * tk[j];
+          Db[(6 + j) * Q + q] += Dp[(6 + j) * Q + q] * tk[j];
+        }
+      }
+    }
+  }
+  // final summation: get_v_y_j (:690-751) + MLFMM_tri_summation_New (:416-497)
+  cd eps_d[2] = {mt.eps1 * IM * mt.omega, mt.eps2 * IM * mt.omega};
+  cd my_d[2] = {mt.my1 * IM * mt.omega, mt.my2 * IM * mt.omega};
+  cd kd[2] = {mt.k1 * IM, mt.k2 * IM};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int j = 0; j < M; j++) {
+    long bi = bidx(L1, T.leaf[j]);
+    const cd* D = &Dd[L1][(size_t)bi * 8 * Q];
+    const cd* r = &F.rt[(size_t)j * 4 * Q];
+    cd s1 = 0.0, s2 = 0.0;
+    for (int i = 0; i < 2; i++) {
+      const cd* fa = &r[(2 * i) * Q];
+      const cd* fb = &r[(2 * i + 1) * Q];
+      cd kh = 0.0, le = 0.0, ke = 0.0, lh = 0.0;
+      for (int q = 0; q < Q; q++) {
+        cd rka = -fb[q], rkb = fa[q];
+        le += fa[q] * D[(0 + i) * Q + q] * my_d[i] + fb[q] * D[(4 + i) * Q + q] * my_d[i];
+        ke += -rka * D[(0 + i) * Q + q] * kd[i] - rkb * D[(4 + i) * Q + q] * kd[i];
+        lh += fa[q] * D[(2 + i) * Q + q] * eps_d[i] + fb[q] * D[(6 + i) * Q + q] * eps_d[i];
+        kh += rka * D[(2 + i) * Q + q] * kd[i] + rkb * D[(6 + i) * Q + q] * kd[i];
+      }
+      s1 += kh + le;
+      s2 += ke + lh;
+    }
+    if (C.P.formulation == 3) {
+      s1 = s1 / mt.eta_a;
+      s2 = s2 * mt.eta_a;
+    }
+    // near field
+    cd n1 = 0.0, n2 = 0.0;
+    int r0 = F.ia[j], r1 = F.ia[j + 1];
+    if (faithful_lookup) {
+      // E2 order of lib_tree_get_domain_e2 with a linear search per element
+      uint64_t bx = T.leaf[j];
+      std::vector<uint64_t> nb = neighbours(bx, L1);
+      nb.insert(nb.begin(), bx);
+      for (uint64_t b : nb) {
+        auto it = T.leaf_elems.find(b);
+        if (it == T.leaf_elems.end()) continue;
+        for (int i : it->second) {
+          cd A = 0, B = 0, Cq = 0, Dq = 0;
+          for (int o = r0; o < r1; o++)
+            if (F.ja[o] == i) { A = F.a[o]; B = F.b[o]; Cq = F.c[o]; Dq = F.d[o]; }
+          n1 += A * x[i] + B * x[i + M];
+          n2 += Cq * x[i] + Dq * x[i + M];
+        }
+      }
+    } else {
+      for (int o = r0; o < r1; o++) {
+        int i = F.ja[o];
+        n1 += F.a[o] * x[i] + F.b[o] * x[i + M];
+        n2 += F.c[o] * x[i] + F.d[o] * x[i + M];
+      }
+    }
+    y[j] = n1 + s1;
+    y[j + M] = n2 + s2;
+  }
+}
+
+// get_vector_b_tri :391-460 + incident_field_tri_general :939-1002 (plane wave)
+static void rhs_planewave(const Ctx& C, const double* kin, const double* Ein, cd* b) {
+  int M = (int)C.ms.edge_mid.size();
+  const Material& mt = C.mt;
+  V3 k = v3(kin[0], kin[1], kin[2]);
+  for (int m = 0; m < M; m++) {
+    cd S1 = 0.0, S2 = 0.0;
+    for (int ot = 0; ot < 2; ot++) {
+      const Fn& f = C.ms.fn[2 * m + ot];
+      for (int i = 0; i < C.R.n; i++) {
+        V3 Ra = simplex(C.R.a[i], C.R.b[i], f.c);
+        V3 rfm = (Ra - f.c[2]) * f.df * 0.5;
+        cd ph = std::exp(-IM * (std::conj(mt.k1) * dot(k, Ra)));
+        C3 E{Ein[0] * ph, Ein[1] * ph, Ein[2] * ph};
+        C3 H{(k.y * E.z - k.z * E.y) / (mt.my1 * C0), (k.z * E.x - k.x * E.z) / (mt.my1 * C0),
+             (k.x * E.y - k.y * E.x) / (mt.my1 * C0)};
+        S1 += rdot(rfm, E) * C.R.w[i] * f.area;
+        S2 += rdot(rfm, H) * C.R.w[i] * f.area;
+      }
+    }
+    if (C.P.formulation == 3) {
+      b[m] = S1 / mt.eta_a;
+      b[m + M] = S2 * mt.eta_a;
+    } else {
+      b[m] = S1;
+      b[m + M] = S2;
+    }
+  }
+}
+
+// Integration_scattered_field_tri :2782-2825 (E and H at observation points)
+static void scattered_field(const Ctx& C, const cd* x, const double* pts, int npts, cd* E, cd* H) {
+  int M = (int)C.ms.edge_mid.size();
+  const Material& mt = C.mt;
+  Rule R = make_rule(3);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int p = 0; p < npts; p++) {
+    V3 ra = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
+    C3 Es = c3zero(), Hs = c3zero();
+    for (int m = 0; m < M; m++) {
+      for (int t = 0; t < 2; t++) {
+        const Fn& f = C.ms.fn[2 * m + t];
+        double dfm = f.sign * f.length;
+        for (int i = 0; i < R.n; i++) {
+          V3 rq = simplex(R.a[i], R.b[i], f.c);
+          V3 fm = (rq - f.c[2]) * 0.5 * dfm;
+          V3 d = ra - rq;
+          double Rn = vlen(d);
+          cd G, DG;
+          green(mt.k1, Rn, G, DG);
+          C3 gG = (d / Rn) * DG;
+          cd J = x[m], Mm = x[m + M];
+          C3 Mf = fm * Mm;
+          C3 cMg{Mf.y * gG.z - Mf.z * gG.y, Mf.z * gG.x - Mf.x * gG.z, Mf.x * gG.y - Mf.y * gG.x};
+          C3 fg{fm.y * gG.z - fm.z * gG.y, fm.z * gG.x - fm.x * gG.z, fm.x * gG.y - fm.y * gG.x};
+          cd a1 = IM * mt.omega * mt.my1 * J * G;
+          C3 Kt{a1 * fm.x - cMg.x, a1 * fm.y - cMg.y, a1 * fm.z - cMg.z};  // charge term * 0
+          double w = R.w[i];
+          Es = Es + Kt * cd(-w);
+          cd a2 = IM * mt.omega * mt.eps1 * Mm * G;
+          cd a3 = 1.0 / (IM * mt.omega * mt.my1) * Mm * dfm;
+          C3 Kh{a2 * fm.x - a3 * gG.x + J * fg.x, a2 * fm.y - a3 * gG.y + J * fg.y,
+                a2 * fm.z - a3 * gG.z + J * fg.z};
+          Hs = Hs + Kh * cd(-w);
+        }
+      }
+    }
+    E[3 * p] = Es.x; E[3 * p + 1] = Es.y; E[3 * p + 2] = Es.z;
+    H[3 * p] = Hs.x; H[3 * p + 1] = Hs.y; H[3 * p + 2] = Hs.z;
+  }
+}
+
+}  // namespace orc
+
+// ===========================================================================
+// C interface for the test harness (ctypes).
+using namespace orc;
+
+extern "C" {
+
+void* orc_create(const double* verts, int nv, const int* tris, int nt, double lambda, double er2_re,
+                 double er2_im, int formulation, int ngp, int s_opt, int K, int normal_conv,
+                 int fix_itbn) {
+  Ctx* C = new Ctx();
+  C->P.lambda = lambda;
+  C->P.eps_r1 = cd(1.0, 0.0);
+  C->P.eps_r2 = cd(er2_re, er2_im);
+  C->P.formulation = formulation;
+  C->P.ngp = ngp;
+  C->P.s_opt = s_opt;
+  C->P.K = K;
+  C->P.normal_conv = normal_conv;
+  C->P.fix_itbn = fix_itbn;
+  C->mt = make_material(C->P);
+  C->R = make_rule(ngp);
+  build_mesh(C->ms, verts, nv, tris, nt, normal_conv);
+  return C;
+}
+
+void orc_free(void* h) { delete (Ctx*)h; }
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+int orc_num_edges(void* h) { return (int)((Ctx*)h)->ms.edge_mid.size(); }
+
+void orc_edges(void* h, int* elem, int* corner) {
+  Ctx* C = (Ctx*)h;
+  std::copy(C->ms.elem.begin(), C->ms.elem.end(), elem);
+  std::copy(C->ms.corner.begin(), C->ms.corner.end(), corner);
+}
+
+// material: k0, omega, k1, k2, eps1, eps2, eta1, eta2, eta_a (complex as re,im pairs)
+void orc_material(void* h, double* out) {
+  Ctx* C = (Ctx*)h;
+  Material& m = C->mt;
+  cd v[9] = {m.k0, m.omega, m.k1, m.k2, m.eps1, m.eps2, m.eta1, m.eta2, m.eta_a};
+  for (int i = 0; i < 9; i++) { out[2 * i] = v[i].real(); out[2 * i + 1] = v[i].imag(); }
+}
+
+// 2x2 block for an explicit list of (m, n) pairs; out: 8 doubles per pair
+void orc_blocks(void* h, const int* ms, const int* ns, int cnt, double* out) {
+  Ctx* C = (Ctx*)h;
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int i = 0; i < cnt; i++) {
+    cd D[4];
+    block(C->ms, C->P, C->mt, C->R, ms[i], ns[i], r_ref_of(C->ms, ms[i]), D);
+    for (int k = 0; k < 4; k++) {
+      out[8 * i + 2 * k] = D[k].real();
+      out[8 * i + 2 * k + 1] = D[k].imag();
+    }
+  }
+}
+
+// dense N x N matrix (row-major complex, interleaved), every pair through the
+// block routine (lib_sie_tri_solver_normal_I :64-217)
+void orc_dense(void* h, double* Z) {
+  Ctx* C = (Ctx*)h;
+  int M = (int)C->ms.edge_mid.size();
+  size_t N = 2 * (size_t)M;
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int m = 0; m < M; m++) {
+    double rr = r_ref_of(C->ms, m);
+    for (int n = 0; n < M; n++) {
+      cd D[4];
+      block(C->ms, C->P, C->mt, C->R, m, n, rr, D);
+      size_t r0 = (size_t)m, r1 = (size_t)m + M, c0 = (size_t)n, c1 = (size_t)n + M;
+      cd* z = (cd*)Z;
+      z[r0 * N + c0] = D[0];
+      z[r0 * N + c1] = D[1];
+      z[r1 * N + c0] = D[2];
+      z[r1 * N + c1] = D[3];
+    }
+  }
+}
+
+int orc_tree(void* h) {
+  Ctx* C = (Ctx*)h;
+  build_tree(C->ms, C->P.s_opt, C->T);
+  C->have_tree = true;
+  return C->T.l_max;
+}
+
+// l_min, l_max, scaling D, xmin[3], leaf box of every edge
+void orc_tree_info(void* h, int* lmin_lmax, double* D_xmin, long long* leaf) {
+  Ctx* C = (Ctx*)h;
+  lmin_lmax[0] = C->T.l_min;
+  lmin_lmax[1] = C->T.l_max;
+  D_xmin[0] = C->T.D;
+  for (int d = 0; d < 3; d++) D_xmin[1 + d] = C->T.xmin[d];
+  for (size_t e = 0; e < C->T.leaf.size(); e++) leaf[e] = (long long)C->T.leaf[e];
+}
+
+int orc_num_boxes(void* h, int l) {
+  Ctx* C = (Ctx*)h;
+  if (l < C->T.l_min || l > C->T.l_max) return 0;
+  return (int)C->T.boxes[l].size();
+}
+
+void orc_boxes(void* h, int l, long long* out) {
+  Ctx* C = (Ctx*)h;
+  for (size_t i = 0; i < C->T.boxes[l].size(); i++) out[i] = (long long)C->T.boxes[l][i];
+}
+
+int orc_i4(void* h, long long n, int l, long long* out) {
+  (void)h;
+  std::vector<uint64_t> v = domain_i4((uint64_t)n, l);
+  for (size_t i = 0; i < v.size(); i++) out[i] = (long long)v[i];
+  return (int)v.size();
+}
+
+int orc_neighbours(long long n, int l, long long* out) {
+  std::vector<uint64_t> v = neighbours((uint64_t)n, l);
+  for (size_t i = 0; i < v.size(); i++) out[i] = (long long)v[i];
+  return (int)v.size();
+}
+
+// near CSR + RT + TL; returns nnz
+long long orc_setup_fmm(void* h) {
+  Ctx* C = (Ctx*)h;
+  if (!C->have_tree) build_tree(C->ms, C->P.s_opt, C->T), C->have_tree = true;
+  C->F.K = C->P.K;
+  make_sampling(C->F);
+  make_rt(C->ms, C->mt, C->R, C->T, C->F);
+  make_tl(C->mt, C->T, C->F);
+  make_near(*C);
+  C->have_fmm = true;
+  return (long long)C->F.ia.back();
+}
+
+void orc_near_csr(void* h, int* ia, int* ja, double* abcd) {
+  Ctx* C = (Ctx*)h;
+  Fmm& F = C->F;
+  std::copy(F.ia.begin(), F.ia.end(), ia);
+  std::copy(F.ja.begin(), F.ja.end(), ja);
+  for (size_t o = 0; o < F.ja.size(); o++) {
+    cd v[4] = {F.a[o], F.b[o], F.c[o], F.d[o]};
+    for (int k = 0; k < 4; k++) { abcd[8 * o + 2 * k] = v[k].real(); abcd[8 * o + 2 * k + 1] = v[k].imag(); }
+  }
+}
+
+int orc_Q(void* h) { return ((Ctx*)h)->F.Q; }
+
+// sampling: khat[3Q], theta[3Q], phi[3Q], trf[Q]
+void orc_sampling(void* h, double* kh, double* th, double* ph, double* trf) {
+  Fmm& F = ((Ctx*)h)->F;
+  for (int q = 0; q < F.Q; q++) {
+    kh[3 * q] = F.khat[q].x; kh[3 * q + 1] = F.khat[q].y; kh[3 * q + 2] = F.khat[q].z;
+    th[3 * q] = F.tth[q].x; th[3 * q + 1] = F.tth[q].y; th[3 * q + 2] = F.tth[q].z;
+    ph[3 * q] = F.tph[q].x; ph[3 * q + 1] = F.tph[q].y; ph[3 * q + 2] = F.tph[q].z;
+    trf[q] = F.trf[q];
+  }
+}
+
+void orc_rt(void* h, double* out) {
+  Fmm& F = ((Ctx*)h)->F;
+  std::memcpy(out, F.rt.data(), F.rt.size() * sizeof(cd));
+}
+
+void orc_tl(void* h, int l, double* out) {
+  Fmm& F = ((Ctx*)h)->F;
+  std::memcpy(out, F.tl[l].data(), F.tl[l].size() * sizeof(cd));
+}
+
+void orc_matvec(void* h, const double* x, double* y, int faithful_lookup) {
+  Ctx* C = (Ctx*)h;
+  matvec(*C, (const cd*)x, (cd*)y, faithful_lookup);
+}
+
+void orc_rhs(void* h, const double* kin, const double* Ein, double* b) {
+  rhs_planewave(*(Ctx*)h, kin, Ein, (cd*)b);
+}
+
+void orc_field(void* h, const double* x, const double* pts, int npts, double* E, double* H) {
+  scattered_field(*(Ctx*)h, (const cd*)x, pts, npts, (cd*)E, (cd*)H);
+}
+
+// special functions exposed for the pins
+void orc_hankel2(double zr, double zi, int n, double* out) {
+  std::vector<cd> h;
+  hankel2(cd(zr, zi), n, h);
+  for (int i = 0; i < n; i++) { out[2 * i] = h[i].real(); out[2 * i + 1] = h[i].imag(); }
+}
+
+void orc_gauss_legendre(int n, double* x, double* w) {
+  std::vector<double> xx, ww;
+  gauss_legendre(n, xx, ww);
+  for (int i = 0; i < n; i++) { x[i] = xx[i]; w[i] = ww[i]; }
+}
+
+// Hänninen pieces for the probe tests (m side tt, n side ll; 0-based)
+void orc_hanninen(void* h, int m, int tt, int n, int ll, int ia, int q, double* out) {
+  Ctx* C = (Ctx*)h;
+  const Fn& fm = C->ms.fn[2 * m + tt];
+  const Fn& fn = C->ms.fn[2 * n + ll];
+  Rule R6 = make_rule(6);
+  V3 Ra = simplex(R6.a[ia], R6.b[ia], fm.c);
+  V3 k2 = K2q(q, Ra, fn, false), k3 = K3q(q, Ra, fn, false), k4 = K4q(q, Ra, fn, false);
+  double is = Iq_s(q, Ra, fn, false);
+  double v[10] = {k2.x, k2.y, k2.z, k3.x, k3.y, k3.z, k4.x, k4.y, k4.z, is};
+  for (int i = 0; i < 10; i++) out[i] = v[i];
+  out[10] = Ra.x; out[11] = Ra.y; out[12] = Ra.z;
+}
+
+// fn table of one edge side: p1 p2 pc (9), area, length, df, mid(3), nq(3)
+void orc_fn(void* h, int e, int ot, double* out) {
+  const Fn& f = ((Ctx*)h)->ms.fn[2 * e + ot];
+  for (int i = 0; i < 3; i++) { out[3 * i] = f.c[i].x; out[3 * i + 1] = f.c[i].y; out[3 * i + 2] = f.c[i].z; }
+  out[9] = f.area; out[10] = f.length; out[11] = f.df;
+  out[12] = f.mid.x; out[13] = f.mid.y; out[14] = f.mid.z;
+  out[15] = f.nq.x; out[16] = f.nq.y; out[17] = f.nq.z;
+}
+
+}  // extern "C"

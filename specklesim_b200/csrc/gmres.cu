@@ -1,0 +1,462 @@
+// Restarted GMRES on the GPU with the semantics of the CERFACS zgmres driver
+// used by the reference (src/lib/libmath_external/src/algorithm_842/zPackgmres.f90
+// :537-1565, called through lib_math_solver_gmres_run,
+// src/lib/libmath/src/math/lib_math_solver_GMRES.f90:159-379): iterative modified
+// Gram-Schmidt (icntl(5) = 1), BLAS Givens rotations (zrotg/zrot), convergence
+// on the Arnoldi backward error ||r||/||b|| confirmed by the true residual, and
+// the recurrence for the restart residual (icntl(8) = 0).
+//
+// All vectors and the Hessenberg matrix stay on the device; the host only reads
+// a few scalars per Arnoldi step to steer the iteration.
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "sie_internal.h"
+
+namespace sie {
+
+static const int RB = 296;   // reduction blocks (2 x 148 SMs)
+static const int RT_ = 256;  // threads per reduction block
+
+struct GmState {
+  // scalars shared between the small kernels
+  double dloo2;     // sum |h|^2 of the current pass
+  double dnormw;
+  double dloo;
+  double bea;
+  double nrm;       // generic norm result
+  int reorth;
+  int pad;
+};
+
+__device__ __forceinline__ zc warp_sum(zc v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v.re += __shfl_xor_sync(0xffffffff, v.re, o);
+    v.im += __shfl_xor_sync(0xffffffff, v.im, o);
+  }
+  return v;
+}
+
+// block-wide sum, result valid in thread 0
+__device__ zc block_sum(zc v) {
+  __shared__ zc sh[32];
+  v = warp_sum(v);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  zc r = mk<double>(0, 0);
+  if (threadIdx.x < 32) {
+    r = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : mk<double>(0, 0);
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;
+}
+
+// Sum of the per-block partials in a fixed order (every block computes the same value).
+__device__ zc reduce_partials(const zc* part, int np) {
+  __shared__ zc res;
+  zc v = mk<double>(0, 0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  v = block_sum(v);
+  if (threadIdx.x == 0) res = v;
+  __syncthreads();
+  zc r = res;
+  __syncthreads();
+  return r;
+}
+
+// One fused MGS step: finish h_j = <V_j, w> from the partials of the previous
+// launch, w -= h_j V_j, and start <V_next, w> (next >= 0) or ||w||^2 (next < 0).
+__global__ void __launch_bounds__(RT_) k_mgs(zc* __restrict__ w, const zc* __restrict__ Vj,
+                                             const zc* __restrict__ Vn, const zc* part_in,
+                                             zc* part_out, int n, zc* Hcol, int j, GmState* gs) {
+  zc h = mk<double>(0, 0);
+  if (Vj) {
+    h = reduce_partials(part_in, gridDim.x);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      Hcol[j] += h;
+      gs->dloo2 += cabs2(h);
+    }
+  }
+  zc acc = mk<double>(0, 0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    zc wi = w[i];
+    if (Vj) {
+      wi = wi - h * Vj[i];
+      w[i] = wi;
+    }
+    if (Vn)
+      acc = cfma_conj(Vn[i], wi, acc);
+    else
+      acc.re += cabs2(wi);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part_out[blockIdx.x] = acc;
+}
+
+// partial dot <a, b> (or ||a||^2 when b == nullptr)
+__global__ void __launch_bounds__(RT_) k_dot(const zc* a, const zc* b, int n, zc* part_out) {
+  zc acc = mk<double>(0, 0);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (b)
+      acc = cfma_conj(a[i], b[i], acc);
+    else
+      acc.re += cabs2(a[i]);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part_out[blockIdx.x] = acc;
+}
+
+__global__ void k_norm_final(const zc* part, int np, GmState* gs) {
+  zc s = reduce_partials(part, np);
+  if (threadIdx.x == 0) gs->nrm = sqrt(s.re);
+}
+
+// end of an MGS pass: dnormw, dloo and the IMGS re-orthogonalisation test
+__global__ void k_pass_final(const zc* part, int np, GmState* gs, int northo) {
+  zc s = reduce_partials(part, np);
+  if (threadIdx.x == 0) {
+    double dnormw = sqrt(s.re);
+    double dloo = sqrt(gs->dloo2);
+    gs->dnormw = dnormw;
+    gs->dloo = dloo;
+    gs->reorth = (dnormw <= dloo && northo < 3) ? 1 : 0;
+  }
+}
+
+__global__ void k_scale_copy(const zc* w, zc* v, int n, const GmState* gs) {
+  double inv = 1.0 / gs->dnormw;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = w[i] * inv;
+}
+__global__ void k_scale_copy_s(const zc* w, zc* v, int n, double beta) {
+  double inv = 1.0 / beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = w[i] * inv;
+}
+__global__ void k_copy(const zc* a, zc* b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+__global__ void k_zero(zc* a, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    a[i] = mk<double>(0, 0);
+}
+// c = a - b
+__global__ void k_sub(const zc* a, const zc* b, zc* c, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    c[i] = a[i] - b[i];
+}
+// y = a + V(:, 0:k) coef (coef on the device)
+__global__ void k_combine(const zc* a, const zc* V, const zc* coef, int k, int n, size_t ld, zc* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    zc s = a ? a[i] : mk<double>(0, 0);
+    for (int j = 0; j < k; j++) s = cfma(V[(size_t)j * ld + i], coef[j], s);
+    y[i] = s;
+  }
+}
+
+// BLAS zrotg (reference BLAS): c real, s complex
+__device__ void zrotg(zc ca, zc cb, double& c, zc& s) {
+  double aca = sqrt(cabs2(ca));
+  if (aca == 0.0) {
+    c = 0.0;
+    s = mk<double>(1.0, 0.0);
+    return;
+  }
+  double acb = sqrt(cabs2(cb));
+  double scale = aca + acb;
+  double na = aca / scale, nb = acb / scale;
+  double norm = scale * sqrt(na * na + nb * nb);
+  zc alpha = ca / aca;
+  c = aca / norm;
+  s = alpha * conj(cb) / norm;
+}
+// BLAS zrot on one pair: x' = c x + s y ; y' = c y - conj(s) x
+__device__ __forceinline__ void zrot(zc& x, zc& y, double c, zc s) {
+  zc t = x * c + s * y;
+  y = y * c - conj(s) * x;
+  x = t;
+}
+
+// H is (m+1) x (m+1), column-major with leading dimension m+1; column m holds the rhs.
+#define HIDX(i, j) ((size_t)(j) * (m + 1) + (i))
+
+// New column jh (0-based) of H: H(jh+1, jh) = dnormw, previous rotations, new
+// rotation, rhs update, bea = |H(jh+1, m)| / bn.
+__global__ void k_givens(zc* H, int m, int jh, double* rc, zc* rs, GmState* gs, double bn) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  H[HIDX(jh + 1, jh)] = mk<double>(gs->dnormw, 0.0);
+  for (int j = 0; j < jh; j++) zrot(H[HIDX(j, jh)], H[HIDX(j + 1, jh)], rc[j], rs[j]);
+  double c;
+  zc s;
+  zrotg(H[HIDX(jh, jh)], H[HIDX(jh + 1, jh)], c, s);
+  rc[jh] = c;
+  rs[jh] = s;
+  zrot(H[HIDX(jh, m)], H[HIDX(jh + 1, m)], c, s);
+  zrot(H[HIDX(jh, jh)], H[HIDX(jh + 1, jh)], c, s);
+  H[HIDX(jh + 1, jh)] = mk<double>(0, 0);
+  gs->bea = sqrt(cabs2(H[HIDX(jh + 1, m)])) / bn;
+}
+
+// y = H(0:k, 0:k)^{-1} H(0:k, m)   (ztrsv 'U','N','N')
+__global__ void k_trsv(const zc* H, int m, int k, zc* y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int i = 0; i < k; i++) y[i] = H[HIDX(i, m)];
+  for (int i = k - 1; i >= 0; i--) {
+    y[i] = y[i] / H[HIDX(i, i)];
+    for (int j = 0; j < i; j++) y[j] = y[j] - y[i] * H[HIDX(j, i)];
+  }
+}
+
+// restart recurrence: beta = |H(m, m)|; rotations in reverse on column m
+__global__ void k_restart_rhs(zc* H, int m, const double* rc, const zc* rs, GmState* gs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  gs->nrm = sqrt(cabs2(H[HIDX(m, m)]));
+  for (int j = m - 1; j >= 0; j--) {
+    H[HIDX(j, m)] = mk<double>(0, 0);
+    zc ms = mk<double>(-rs[j].re, -rs[j].im);
+    zrot(H[HIDX(j, m)], H[HIDX(j + 1, m)], rc[j], ms);
+  }
+}
+
+__global__ void k_hinit(zc* H, int m, double beta) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > m) return;
+  H[HIDX(i, m)] = (i == 0) ? mk<double>(beta, 0) : mk<double>(0, 0);
+}
+__global__ void k_hcol_zero(zc* H, int m, int jh) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= jh) H[HIDX(i, jh)] = mk<double>(0, 0);
+}
+__global__ void k_gs_reset(GmState* gs) {
+  gs->dloo2 = 0;
+}
+
+struct Gm {
+  int n, m;
+  zc *V, *w, *r0, *xc, *y, *H, *part_a, *part_b, *rs;
+  double* rc;
+  GmState* gs;
+  GmState* hgs;  // pinned host copy
+};
+
+static int gm_alloc(sie_ctx* c, int m, Gm& g) {
+  int n = 2 * c->M;
+  size_t need = 0;
+  auto add = [&](size_t bytes) {
+    size_t o = need;
+    need += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  size_t oV = add((size_t)(m + 1) * n * sizeof(zc));
+  size_t ow = add((size_t)n * sizeof(zc));
+  size_t or0 = add((size_t)n * sizeof(zc));
+  size_t oxc = add((size_t)n * sizeof(zc));
+  size_t oy = add((size_t)(m + 1) * sizeof(zc));
+  size_t oH = add((size_t)(m + 1) * (m + 1) * sizeof(zc));
+  size_t opa = add(RB * sizeof(zc));
+  size_t opb = add(RB * sizeof(zc));
+  size_t ors = add((size_t)(m + 1) * sizeof(zc));
+  size_t orc = add((size_t)(m + 1) * sizeof(double));
+  size_t ogs = add(sizeof(GmState));
+  if (c->gm_bytes < need) {
+    if (c->d_gm) cudaFree(c->d_gm);
+    c->d_gm = nullptr;
+    c->gm_bytes = 0;
+    SIE_CUDA(cudaMalloc(&c->d_gm, need));
+    c->gm_bytes = need;
+  }
+  char* b = (char*)c->d_gm;
+  g.n = n;
+  g.m = m;
+  g.V = (zc*)(b + oV);
+  g.w = (zc*)(b + ow);
+  g.r0 = (zc*)(b + or0);
+  g.xc = (zc*)(b + oxc);
+  g.y = (zc*)(b + oy);
+  g.H = (zc*)(b + oH);
+  g.part_a = (zc*)(b + opa);
+  g.part_b = (zc*)(b + opb);
+  g.rs = (zc*)(b + ors);
+  g.rc = (double*)(b + orc);
+  g.gs = (GmState*)(b + ogs);
+  return SIE_OK;
+}
+
+static int read_gs(sie_ctx* c, Gm& g, GmState& h) {
+  SIE_CUDA(cudaMemcpyAsync(&h, g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, c->stream));
+  SIE_CUDA(cudaStreamSynchronize(c->stream));
+  return SIE_OK;
+}
+
+static int norm2(sie_ctx* c, Gm& g, const zc* a, double& out) {
+  k_dot<<<RB, RT_, 0, c->stream>>>(a, nullptr, g.n, g.part_a); sie::count_launch();
+  k_norm_final<<<1, RT_, 0, c->stream>>>(g.part_a, RB, g.gs); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  GmState h;
+  SIE_TRY(read_gs(c, g, h));
+  out = h.nrm;
+  return SIE_OK;
+}
+
+}  // namespace sie
+
+using namespace sie;
+
+
+int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solver_cfg* cfg,
+                     sie_stats* st) {
+  cudaStream_t s = c->stream;
+  int m = cfg->restart;
+  Gm g;
+  {
+    int r = gm_alloc(c, m, g);
+    if (r != SIE_OK) return r;
+  }
+  int n = g.n;
+  size_t ld = (size_t)n;
+  auto t0 = std::chrono::steady_clock::now();
+  cudaEventRecord(c->ev[12], s);
+  // internal layout: b -> d_yi (kept), x -> d_xi
+  zc* b = c->d_yi;
+  zc* x = c->d_xi;
+  int r = gather_ext_to_int(c, d_b_ext, b, 1, s);
+  if (r != SIE_OK) return r;
+  if (cfg->use_initial_guess) {
+    r = gather_ext_to_int(c, d_x_ext, x, 1, s);
+  } else {
+    k_zero<<<RB, RT_, 0, s>>>(x, n); sie::count_launch();
+  }
+  if (r != SIE_OK) return r;
+  int matvecs = 0;
+  auto matvec = [&](const zc* in, zc* out) -> int {
+    matvecs++;
+    return sie_internal_matvec(c, in, out, 1, s, false);
+  };
+  auto finish = [&](int code, int iters, double bea, double be, int conv) {
+    scatter_int_to_ext(c, x, d_x_ext, 1, s);
+    cudaEventRecord(c->ev[13], s);
+    cudaEventSynchronize(c->ev[13]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[12], c->ev[13]);
+    if (st) {
+      st->iterations = iters;
+      st->matvecs = matvecs;
+      st->converged = conv;
+      st->backward_error_arnoldi = bea;
+      st->backward_error_true = be;
+      st->seconds = ms * 1e-3;
+    }
+    return code;
+  };
+  double bn = 0;
+  r = norm2(c, g, b, bn);
+  if (r != SIE_OK) return r;
+  if (!std::isfinite(bn)) return fail(SIE_ERR_NONFINITE, "GMRES: non-finite right-hand side");
+  if (bn == 0.0) {
+    k_zero<<<RB, RT_, 0, s>>>(x, n); sie::count_launch();
+    return finish(SIE_OK, 0, 0, 0, 1);
+  }
+  // r0 = b - A x  (or b)
+  if (cfg->use_initial_guess) {
+    SIE_TRY(matvec(x, g.r0));
+    k_sub<<<RB, RT_, 0, s>>>(b, g.r0, g.w, n); sie::count_launch();
+  } else {
+    k_copy<<<RB, RT_, 0, s>>>(b, g.w, n); sie::count_launch();
+  }
+  double beta = 0;
+  r = norm2(c, g, g.w, beta);
+  if (r != SIE_OK) return r;
+  if (beta == 0.0) return finish(SIE_OK, 0, 0, 0, 1);
+  k_scale_copy_s<<<RB, RT_, 0, s>>>(g.w, g.V, n, beta); sie::count_launch();
+  int iterOut = 0, compRsd = 0;
+  double bea = 1e300, be = 1e300, trueNormRes = 0;
+  int itermax = cfg->max_iterations;
+  while (true) {
+    k_hinit<<<(m + 1 + 127) / 128, 128, 0, s>>>(g.H, m, beta); sie::count_launch();
+    int jH = 0;
+    for (; jH < m; jH++) {
+      // w = A V_jH
+      SIE_TRY(matvec(g.V + (size_t)jH * ld, g.w));
+      k_hcol_zero<<<(m + 1 + 127) / 128, 128, 0, s>>>(g.H, m, jH); sie::count_launch();
+      GmState h;
+      for (int northo = 1;; northo++) {
+        k_gs_reset<<<1, 1, 0, s>>>(g.gs); sie::count_launch();
+        // start <V_0, w>
+        k_mgs<<<RB, RT_, 0, s>>>(g.w, nullptr, g.V, nullptr, g.part_a, n, g.H + (size_t)jH * (m + 1),
+                                 0, g.gs); sie::count_launch();
+        zc* pin = g.part_a;
+        zc* pout = g.part_b;
+        for (int j = 0; j <= jH; j++) {
+          const zc* Vn = (j < jH) ? g.V + (size_t)(j + 1) * ld : nullptr;
+          k_mgs<<<RB, RT_, 0, s>>>(g.w, g.V + (size_t)j * ld, Vn, pin, pout, n,
+                                   g.H + (size_t)jH * (m + 1), j, g.gs); sie::count_launch();
+          zc* t = pin;
+          pin = pout;
+          pout = t;
+        }
+        k_pass_final<<<1, RT_, 0, s>>>(pin, RB, g.gs, northo); sie::count_launch();
+        SIE_CUDA(cudaGetLastError());
+        SIE_TRY(read_gs(c, g, h));
+        if (!std::isfinite(h.dnormw)) return fail(SIE_ERR_NONFINITE, "GMRES: non-finite Arnoldi vector");
+        if (!h.reorth) break;
+      }
+      // V_{jH+1} = w / dnormw (icntl(8) = 0 keeps m+1 basis vectors)
+      k_scale_copy<<<RB, RT_, 0, s>>>(g.w, g.V + (size_t)(jH + 1) * ld, n, g.gs); sie::count_launch();
+      k_givens<<<1, 1, 0, s>>>(g.H, m, jH, g.rc, g.rs, g.gs, bn); sie::count_launch();
+      SIE_CUDA(cudaGetLastError());
+      SIE_TRY(read_gs(c, g, h));
+      bea = h.bea;
+      int it = iterOut * m + jH + 1;
+      if (!std::isfinite(bea)) return fail(SIE_ERR_NONFINITE, "GMRES: non-finite residual estimate");
+      if (bea <= cfg->tolerance || it >= itermax) {
+        compRsd = 1;
+        // xCurrent = x + V y
+        k_trsv<<<1, 1, 0, s>>>(g.H, m, jH + 1, g.y); sie::count_launch();
+        k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, jH + 1, n, ld, g.xc); sie::count_launch();
+        // true residual
+        SIE_TRY(matvec(g.xc, g.w));
+        k_sub<<<RB, RT_, 0, s>>>(b, g.w, g.w, n); sie::count_launch();
+        r = norm2(c, g, g.w, trueNormRes);
+        if (r != SIE_OK) return r;
+        be = trueNormRes / bn;
+        if (be <= cfg->tolerance || it >= itermax) {
+          k_copy<<<RB, RT_, 0, s>>>(g.xc, x, n); sie::count_launch();
+          int conv = be <= cfg->tolerance;
+          return finish(conv ? SIE_OK : fail(SIE_ERR_NOCONV, "GMRES: no convergence"), it, bea,
+                        trueNormRes / bn, conv);
+        }
+      }
+      if (cfg->time_limit_s > 0) {
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > cfg->time_limit_s) {
+          finish(SIE_ERR_TIMEOUT, it, bea, be, 0);
+          return fail(SIE_ERR_TIMEOUT, "GMRES: time limit reached");
+        }
+      }
+    }
+    iterOut++;
+    if (bea > cfg->tolerance) {
+      k_trsv<<<1, 1, 0, s>>>(g.H, m, m, g.y); sie::count_launch();
+      k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, m, n, ld, g.xc); sie::count_launch();
+    }
+    k_copy<<<RB, RT_, 0, s>>>(g.xc, x, n); sie::count_launch();
+    if (compRsd == 1) {
+      SIE_TRY(matvec(x, g.r0));
+      k_sub<<<RB, RT_, 0, s>>>(b, g.r0, g.w, n); sie::count_launch();
+      r = norm2(c, g, g.w, beta);
+      if (r != SIE_OK) return r;
+    } else {
+      k_restart_rhs<<<1, 1, 0, s>>>(g.H, m, g.rc, g.rs, g.gs); sie::count_launch();
+      // w = V(:, 0:m+1) H(:, m)
+      k_combine<<<RB, RT_, 0, s>>>(nullptr, g.V, g.H + (size_t)m * (m + 1), m + 1, n, ld, g.w); sie::count_launch();
+      GmState h;
+      SIE_TRY(read_gs(c, g, h));
+      beta = h.nrm;
+    }
+    k_scale_copy_s<<<RB, RT_, 0, s>>>(g.w, g.V, n, beta); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+}

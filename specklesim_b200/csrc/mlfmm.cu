@@ -1,0 +1,467 @@
+// MLFMM far field on the GPU: radiation patterns, translation tables and the
+// level-synchronous upward / downward / receive passes.
+//
+// Reference: the plug-ins of src/lib_sie_tri_mlfmm_interface.f90 (get_C
+// :395-448, translation_SS :466-528, translation_SR :547-586, translation_RR
+// :600-655, get_v_y_j :690-751), MLFMM_tri_summation_New and PreCalculate_RT in
+// src/lib_sie_tri_mlfmm.f90 (:416-583), TL_km_ml_fmm in src/lib_sie_mlfmm.f90
+// (:129-188) and the pass order of src/lib/libmlfmm/lib/lib_ml_fmm.f90 (:269-1110).
+//
+// Coefficient layout per box: 8 items x Q directions, item order
+//   0,1 = theta J (k1,k2)   2,3 = theta M (k1,k2)
+//   4,5 = phi   J (k1,k2)   6,7 = phi   M (k1,k2)
+// (a_nm(1..4), b_nm(1..4) of lib_ml_fmm_coefficient).  Medium = item & 1.
+#include "sie_internal.h"
+
+namespace sie {
+
+// ---------------------------------------------------------------------------
+// Radiation pattern per edge about the centre of its leaf box
+// (RT_function_SCSArr_New :543-583): for every direction q and medium,
+//   sum_sides sum_j 0.5*sign*len*(r_j - v) exp(-i k khat.(r_j - Rc)) w_j
+// projected on theta-hat (a_nm) and phi-hat (b_nm).
+__global__ void k_rt(const FnD* fn, const double* boxc, const int* edge_box, int M, Rule R,
+                     zc k1, zc k2, const double* khat, const double* tth, const double* tph, int Q,
+                     zc* rt) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int e = blockIdx.y;
+  if (q >= Q || e >= M) return;
+  int b = edge_box[e];
+  vd Rc = mkv<double>(boxc[3 * b], boxc[3 * b + 1], boxc[3 * b + 2]);
+  vd kh = mkv<double>(khat[3 * q], khat[3 * q + 1], khat[3 * q + 2]);
+  vd th = mkv<double>(tth[3 * q], tth[3 * q + 1], tth[3 * q + 2]);
+  vd ph = mkv<double>(tph[3 * q], tph[3 * q + 1], tph[3 * q + 2]);
+  zc a1 = mk<double>(0, 0), b1 = a1, a2 = a1, b2 = a1;
+  for (int ll = 0; ll < 2; ll++) {
+    const FnD& f = fn[2 * e + ll];
+    double dfm = f.sgn * f.length;
+    zc sa[3] = {mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0)};
+    zc sb[3] = {sa[0], sa[0], sa[0]};
+    for (int j = 0; j < R.n; j++) {
+      double w0 = 1 - R.a[j] - R.b[j];
+      vd Ro = mkv<double>(w0 * f.c[0] + R.a[j] * f.c[3] + R.b[j] * f.c[6],
+                          w0 * f.c[1] + R.a[j] * f.c[4] + R.b[j] * f.c[7],
+                          w0 * f.c[2] + R.a[j] * f.c[5] + R.b[j] * f.c[8]);
+      vd fm = (Ro - mkv<double>(f.c[6], f.c[7], f.c[8])) * 0.5 * dfm;
+      double tmp = dot(kh, Ro - Rc);
+      zc f1 = cexp_mik(k1, tmp) * R.w[j];
+      zc f2 = cexp_mik(k2, tmp) * R.w[j];
+      sa[0] += f1 * fm.x;
+      sa[1] += f1 * fm.y;
+      sa[2] += f1 * fm.z;
+      sb[0] += f2 * fm.x;
+      sb[1] += f2 * fm.y;
+      sb[2] += f2 * fm.z;
+    }
+    a1 += sa[0] * th.x + sa[1] * th.y + sa[2] * th.z;
+    b1 += sa[0] * ph.x + sa[1] * ph.y + sa[2] * ph.z;
+    a2 += sb[0] * th.x + sb[1] * th.y + sb[2] * th.z;
+    b2 += sb[0] * ph.x + sb[1] * ph.y + sb[2] * ph.z;
+  }
+  zc* o = rt + (size_t)e * 4 * Q;
+  o[0 * Q + q] = a1;
+  o[1 * Q + q] = b1;
+  o[2 * Q + q] = a2;
+  o[3 * Q + q] = b2;
+}
+
+// ---------------------------------------------------------------------------
+// Spherical Hankel functions of the second kind for every TL offset and medium
+// (lib_math_hankel_spherical_2 = j - i y, lib_math_bessel.f90:935-990).
+// Real argument: j_n by Miller's downward recurrence, y_n upward.  Complex
+// argument: h2 by upward recurrence from h2_{-1} = e^{-iz}/z, h2_0 = i e^{-iz}/z.
+__device__ void hankel2_dev(zc z, int K, zc* h) {
+  if (z.im == 0.0) {
+    double x = z.re;
+    double sx, cxv;
+    sincos(x, &sx, &cxv);
+    double ym1 = -cxv / x, y0 = ym1;
+    double y1 = -cxv / (x * x) - sx / x;
+    // y_n upward
+    double yp = y0, yc = y1;
+    h[0].im = -y0;
+    if (K > 1) h[1].im = -y1;
+    for (int n = 1; n + 1 < K; n++) {
+      double yn = (2 * n + 1) / x * yc - yp;
+      yp = yc;
+      yc = yn;
+      h[n + 1].im = -yn;
+    }
+    // j_n downward (Miller), normalised on j0 or j1
+    int start = K + 20;
+    int s2 = (int)fabs(x) + 40;
+    if (s2 > start) start = s2;
+    double jn1 = 0.0, jn = 1e-300;
+    double j0v = sx / x, j1v = sx / (x * x) - cxv / x;
+    // first pass: find scale, storing the values of orders < K as we go
+    double store[64];
+    for (int n = start; n >= 1; n--) {
+      double jm = (2 * n + 1) / x * jn - jn1;
+      jn1 = jn;
+      jn = jm;
+      if (fabs(jn) > 1e250) {
+        jn *= 1e-250;
+        jn1 *= 1e-250;
+        for (int k = 0; k < K && k < 64; k++) store[k] *= 1e-250;
+      }
+      if (n - 1 < K) store[n - 1] = jn;
+      if (n < K) store[n] = jn1;
+    }
+    double sc = (fabs(j0v) >= fabs(j1v)) ? j0v / store[0] : j1v / store[1];
+    for (int n = 0; n < K; n++) h[n].re = store[n] * sc;
+    return;
+  }
+  zc mi = mk<double>(0.0, -1.0);
+  zc e = cexp(mi * z);
+  zc hm1 = e / z;
+  zc h0 = mk<double>(0.0, 1.0) * e / z;
+  h[0] = h0;
+  zc prev = hm1, cur = h0;
+  for (int n = 0; n + 1 < K; n++) {
+    zc nx = (mk<double>((double)(2 * n + 1), 0.0) / z) * cur - prev;
+    prev = cur;
+    cur = nx;
+    h[n + 1] = cur;
+  }
+}
+
+__global__ void k_hankel(double xmin, double dx, zc k1, zc k2, int K, bool only_k1, zc* hk) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 343) return;
+  int i = t / 49, j = (t / 7) % 7, k = t % 7;
+  vd r = mkv<double>(xmin + i * dx, xmin + j * dx, xmin + k * dx);
+  double rl = vlen(r);
+  zc hb[64];
+  for (int md = 0; md < 2; md++) {
+    zc* o = hk + ((size_t)t * 2 + md) * K;
+    bool excluded = (i >= 2 && i <= 4 && j >= 2 && j <= 4 && k >= 2 && k <= 4);
+    if (excluded || (md == 1 && only_k1)) {
+      for (int n = 0; n < K; n++) o[n] = mk<double>(0, 0);
+      continue;
+    }
+    zc kk = md == 0 ? k1 : k2;
+    hankel2_dev(kk * rl, K, hb);
+    for (int n = 0; n < K; n++) o[n] = hb[n];
+  }
+}
+
+// TL_km_ml_fmm (lib_sie_mlfmm.f90:129-188):
+//   TL(q) = sum_{n=1..K} h2_{n-1}(kR) (-i)^n (2n-1) P_{n-1}(rhat.khat_q) k / (4 pi)^2
+__global__ void k_tl(double xmin, double dx, const zc* hk, zc k1, zc k2, int K, int Q,
+                     const double* khat, zc* tl) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  int t = blockIdx.y;
+  if (q >= Q) return;
+  int i = t / 49, j = (t / 7) % 7, k = t % 7;
+  vd r = mkv<double>(xmin + i * dx, xmin + j * dx, xmin + k * dx);
+  double rl = vlen(r);
+  vd rh = r / rl;
+  double x = rh.x * khat[3 * q] + rh.y * khat[3 * q + 1] + rh.z * khat[3 * q + 2];
+  const double c16 = (4 * PI) * (4 * PI);
+  for (int md = 0; md < 2; md++) {
+    const zc* h = hk + ((size_t)t * 2 + md) * K;
+    zc kd = md == 0 ? k1 : k2;
+    zc acc = mk<double>(0, 0);
+    double p0 = 1.0, p1 = x;
+    zc mi = mk<double>(1.0, 0.0);
+    for (int n = 1; n <= K; n++) {
+      double P = (n == 1) ? p0 : (n == 2 ? p1 : 0.0);
+      if (n >= 3) {
+        int nn = n - 2;  // P_{nn+1} from P_nn, P_{nn-1}
+        double p2 = ((2 * nn + 1) * x * p1 - nn * p0) / (nn + 1);
+        p0 = p1;
+        p1 = p2;
+        P = p1;
+      }
+      mi = mi * mk<double>(0.0, -1.0);
+      acc += ((h[n - 1] * mi) * (double)(2 * (n - 1) + 1)) * P * kd / c16;
+    }
+    tl[((size_t)t * 2 + md) * Q + q] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Upward pass step 1 (lib_sie_ml_fmm_get_C :395-448): C = sum conj(RT) x over
+// the edges of each leaf box.  Block per leaf box, threads over directions.
+template <typename T>
+__global__ void k_aggregate(const cx<T>* __restrict__ rt, const int* box_first, const int* box_cnt,
+                            int Q, const cx<T>* __restrict__ x, cx<T>* __restrict__ C) {
+  int b = blockIdx.x;
+  int f = box_first[b], cnt = box_cnt[b];
+  for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+    cx<T> acc[8];
+    for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+    for (int e = f; e < f + cnt; e++) {
+      const cx<T>* r = rt + (size_t)e * 4 * Q;
+      cx<T> xe = x[2 * e], xh = x[2 * e + 1];
+      cx<T> ra1 = r[q], rb1 = r[Q + q], ra2 = r[2 * Q + q], rb2 = r[3 * Q + q];
+      acc[0] = cfma_conj(ra1, xe, acc[0]);
+      acc[1] = cfma_conj(ra2, xe, acc[1]);
+      acc[2] = cfma_conj(ra1, xh, acc[2]);
+      acc[3] = cfma_conj(ra2, xh, acc[3]);
+      acc[4] = cfma_conj(rb1, xe, acc[4]);
+      acc[5] = cfma_conj(rb2, xe, acc[5]);
+      acc[6] = cfma_conj(rb1, xh, acc[6]);
+      acc[7] = cfma_conj(rb2, xh, acc[7]);
+    }
+    cx<T>* o = C + (size_t)b * 8 * Q;
+    for (int i = 0; i < 8; i++) o[i * Q + q] = acc[i];
+  }
+}
+
+// Upward pass step 2 (translation_SS :466-528): parent C = sum over children
+// of C_child * exp(+i k khat.(x_child - x_parent)).  nmed = 1 skips medium 2.
+template <typename T>
+__global__ void k_ss(const cx<T>* __restrict__ Cc, const int* ch_ptr, const int* ch_idx,
+                     const int* ch_oct, const cx<T>* __restrict__ ph, int Q, int nmed,
+                     cx<T>* __restrict__ Cp) {
+  int b = blockIdx.y;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  cx<T> acc[8];
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  for (int k = ch_ptr[b]; k < ch_ptr[b + 1]; k++) {
+    int c = ch_idx[k], o = ch_oct[k];
+    const cx<T>* src = Cc + (size_t)c * 8 * Q;
+    for (int md = 0; md < nmed; md++) {
+      cx<T> p = ph[((size_t)o * 2 + md) * Q + q];
+      for (int it = md; it < 8; it += 2) acc[it] = cfma(src[it * Q + q], p, acc[it]);
+    }
+  }
+  cx<T>* out = Cp + (size_t)b * 8 * Q;
+  for (int i = 0; i < 8; i++) out[i * Q + q] = acc[i];
+}
+
+// Downward pass step 1 (translation_SR :547-586 over lib_tree_get_domain_i4):
+// D~ = sum_{I4} C_src * TRF * TL(x_box - x_src).
+template <typename T>
+__global__ void k_sr(const cx<T>* __restrict__ C, const int* i4_ptr, const int* i4_src,
+                     const int* i4_off, const cx<T>* __restrict__ tl, const T* __restrict__ trf,
+                     int Q, int nmed, cx<T>* __restrict__ D) {
+  int b = blockIdx.y;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  cx<T> acc[8];
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  T w = trf[q];
+  for (int k = i4_ptr[b]; k < i4_ptr[b + 1]; k++) {
+    int s = i4_src[k], t = i4_off[k];
+    const cx<T>* src = C + (size_t)s * 8 * Q;
+    for (int md = 0; md < nmed; md++) {
+      cx<T> f = tl[((size_t)t * 2 + md) * Q + q] * w;
+      for (int it = md; it < 8; it += 2) acc[it] = cfma(src[it * Q + q], f, acc[it]);
+    }
+  }
+  cx<T>* out = D + (size_t)b * 8 * Q;
+  for (int i = 0; i < 8; i++) out[i * Q + q] = acc[i];
+}
+
+// Downward pass step 2 (translation_RR :600-655): D += D_parent * exp(-i k khat.(x_child - x_parent)).
+template <typename T>
+__global__ void k_rr(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
+                     const cx<T>* __restrict__ ph, int Q, int nmed, cx<T>* __restrict__ D) {
+  int b = blockIdx.y;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  int p = parent[b];
+  if (p < 0) return;
+  int o = oct[b];
+  const cx<T>* src = Dp + (size_t)p * 8 * Q;
+  cx<T>* dst = D + (size_t)b * 8 * Q;
+  for (int md = 0; md < nmed; md++) {
+    cx<T> f = ph[((size_t)o * 2 + md) * Q + q];
+    for (int it = md; it < 8; it += 2) dst[it * Q + q] = cfma(src[it * Q + q], f, dst[it * Q + q]);
+  }
+}
+
+// Final summation far part (get_v_y_j :690-751 + MLFMM_tri_summation_New
+// :416-497).  Block per leaf box; D of the box in shared memory; one warp per
+// edge reduces over the directions.
+struct RecvConst {
+  zc kd[2], my_d[2], eps_d[2];
+  zc s1f, s2f;  // ICTF scaling of the two outputs
+};
+
+template <typename T>
+__global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, const int* box_cnt,
+                          const cx<T>* __restrict__ D, int Q, RecvConst rc,
+                          cx<T>* __restrict__ y) {
+  extern __shared__ unsigned char smraw[];
+  cx<T>* sD = reinterpret_cast<cx<T>*>(smraw);
+  int b = blockIdx.x;
+  const cx<T>* Db = D + (size_t)b * 8 * Q;
+  for (int i = threadIdx.x; i < 8 * Q; i += blockDim.x) sD[i] = Db[i];
+  __syncthreads();
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  int f = box_first[b], cnt = box_cnt[b];
+  for (int e = f + warp; e < f + cnt; e += nw) {
+    const cx<T>* r = rt + (size_t)e * 4 * Q;
+    // per medium: Sa = sum(fa D_i + fb D_{4+i}), Sb = sum(fb D_i - fa D_{4+i}),
+    //             Sc = sum(fa D_{2+i} + fb D_{6+i}), Sd = sum(fa D_{6+i} - fb D_{2+i})
+    cx<T> S[2][4];
+    for (int md = 0; md < 2; md++)
+      for (int k = 0; k < 4; k++) S[md][k] = mk<T>(0, 0);
+    for (int q = lane; q < Q; q += 32) {
+      for (int md = 0; md < 2; md++) {
+        cx<T> fa = r[(2 * md) * Q + q], fb = r[(2 * md + 1) * Q + q];
+        cx<T> dJt = sD[(0 + md) * Q + q], dMt = sD[(2 + md) * Q + q];
+        cx<T> dJp = sD[(4 + md) * Q + q], dMp = sD[(6 + md) * Q + q];
+        S[md][0] = cfma(fa, dJt, S[md][0]);
+        S[md][0] = cfma(fb, dJp, S[md][0]);
+        S[md][1] = cfma(fb, dJt, S[md][1]);
+        S[md][1] = cfma(-fa, dJp, S[md][1]);
+        S[md][2] = cfma(fa, dMt, S[md][2]);
+        S[md][2] = cfma(fb, dMp, S[md][2]);
+        S[md][3] = cfma(fa, dMp, S[md][3]);
+        S[md][3] = cfma(-fb, dMt, S[md][3]);
+      }
+    }
+    for (int md = 0; md < 2; md++)
+      for (int k = 0; k < 4; k++)
+        for (int o = 16; o > 0; o >>= 1) {
+          S[md][k].re += __shfl_xor_sync(0xffffffff, S[md][k].re, o);
+          S[md][k].im += __shfl_xor_sync(0xffffffff, S[md][k].im, o);
+        }
+    if (lane == 0) {
+      zc s1 = mk<double>(0, 0), s2 = s1;
+      for (int md = 0; md < 2; md++) {
+        zc Sa = mk<double>(S[md][0].re, S[md][0].im), Sb = mk<double>(S[md][1].re, S[md][1].im);
+        zc Sc = mk<double>(S[md][2].re, S[md][2].im), Sd = mk<double>(S[md][3].re, S[md][3].im);
+        s1 += rc.kd[md] * Sd + rc.my_d[md] * Sa;
+        s2 += rc.kd[md] * Sb + rc.eps_d[md] * Sc;
+      }
+      s1 = s1 * rc.s1f;
+      s2 = s2 * rc.s2f;
+      y[2 * e] += mk<T>((T)s1.re, (T)s1.im);
+      y[2 * e + 1] += mk<T>((T)s2.re, (T)s2.im);
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_zero(cx<T>* p, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = mk<T>(0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+int far_build_tables(sie_ctx* c, const double* d_boxc) {
+  cudaStream_t st = c->stream;
+  int Q = c->Q, K = c->K, M = c->M;
+  // radiation patterns
+  {
+    dim3 g((Q + 127) / 128, M);
+    k_rt<<<g, 128, 0, st>>>(c->d_fn, d_boxc, c->d_edge_box, M, c->R, c->mt.k1, c->mt.k2, c->d_khat,
+                            c->d_tth, c->d_tph, Q, c->d_rt); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  // TL tables per level
+  zc* hk = nullptr;
+  SIE_CUDA(cudaMalloc(&hk, (size_t)343 * 2 * K * sizeof(zc)));
+  for (int l = c->l_min; l <= c->l_max; l++) {
+    Level& L = c->lv[l];
+    double dc = ldexp(1.0, -l) * c->D;
+    double xmn = -3 * dc, xmx = -xmn;
+    double dx = (xmx - xmn) / 6;
+    k_hankel<<<(343 + 63) / 64, 64, 0, st>>>(xmn, dx, c->mt.k1, c->mt.k2, K, L.only_k1, hk); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+    dim3 g((Q + 127) / 128, 343);
+    k_tl<<<g, 128, 0, st>>>(xmn, dx, hk, c->mt.k1, c->mt.k2, K, Q, c->d_khat, L.tl); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  SIE_CUDA(cudaStreamSynchronize(st));
+  cudaFree(hk);
+  return SIE_OK;
+}
+
+template <typename T>
+int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
+                 cudaEvent_t* ev) {
+  int Q = c->Q;
+  int L0 = c->l_min, L1 = c->l_max;
+  bool k2c = c->mt.k2.im != 0.0;
+  int thr = 128;
+  // up 1
+  {
+    Level& L = c->lv[L1];
+    k_aggregate<T><<<L.nb, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  // up 2
+  for (int l = L1 - 1; l >= L0; l--) {
+    Level& P = c->lv[l];
+    Level& Ch = c->lv[l + 1];
+    dim3 g((Q + thr - 1) / thr, P.nb);
+    k_ss<T><<<g, thr, 0, st>>>((const cx<T>*)Ch.C, P.ch_ptr, P.ch_idx, P.ch_oct,
+                               (const cx<T>*)Ch.ph_up, Q, k2c ? 1 : 2, (cx<T>*)P.C); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  // down 1
+  for (int l = L0; l <= L1; l++) {
+    Level& L = c->lv[l];
+    dim3 g((Q + thr - 1) / thr, L.nb);
+    k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
+                               (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
+                               (cx<T>*)L.D); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  // down 2
+  for (int l = L0 + 1; l <= L1; l++) {
+    Level& L = c->lv[l];
+    Level& P = c->lv[l - 1];
+    dim3 g((Q + thr - 1) / thr, L.nb);
+    int nmed = (k2c && l < L1) ? 1 : 2;
+    // D_k2 of the parent is zero when its level only carries k1
+    if (k2c) nmed = 1;
+    k_rr<T><<<g, thr, 0, st>>>((const cx<T>*)P.D, L.parent, L.oct, (const cx<T>*)L.ph_dn, Q, nmed,
+                               (cx<T>*)L.D); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[4], st);
+  // final far summation
+  {
+    Level& L = c->lv[L1];
+    RecvConst rc;
+    zc I = mk<double>(0, 1);
+    rc.kd[0] = c->mt.k1 * I;
+    rc.kd[1] = c->mt.k2 * I;
+    rc.my_d[0] = mk<double>(0, c->mt.my1 * c->mt.omega);
+    rc.my_d[1] = mk<double>(0, c->mt.my2 * c->mt.omega);
+    rc.eps_d[0] = c->mt.eps1 * I * c->mt.omega;
+    rc.eps_d[1] = c->mt.eps2 * I * c->mt.omega;
+    if (c->cfg.formulation == SIE_ICTF) {
+      rc.s1f = mk<double>(1, 0) / c->mt.eta_a;
+      rc.s2f = c->mt.eta_a;
+    } else {
+      rc.s1f = mk<double>(1, 0);
+      rc.s2f = mk<double>(1, 0);
+    }
+    size_t smem = (size_t)8 * Q * sizeof(cx<T>);
+    k_receive<T><<<L.nb, 256, smem, st>>>(rt, c->d_box_first, c->d_box_cnt, (const cx<T>*)L.D, Q,
+                                          rc, y); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[5], st);
+  return SIE_OK;
+}
+
+int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev) {
+  return far_matvec_t<double>(c, c->d_rt, x, y, st, ev);
+}
+
+int far_prepare_kernels(sie_ctx* c) {
+  size_t smem64 = (size_t)8 * c->Q * sizeof(zc);
+  size_t smem32 = (size_t)8 * c->Q * sizeof(cc);
+  SIE_CUDA(cudaFuncSetAttribute(k_receive<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem64));
+  SIE_CUDA(cudaFuncSetAttribute(k_receive<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem32));
+  return SIE_OK;
+}
+
+}  // namespace sie

@@ -1,0 +1,1106 @@
+// C-ABI entry points, mesh/tree set-up and matvec orchestration of libsiegpu.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sie_internal.h"
+
+namespace sie {
+
+static thread_local std::string g_err = "";
+static unsigned long long g_launches = 0;
+void count_launch() { __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+
+void set_error(const std::string& msg) { g_err = msg; }
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? SIE_ERR_NOMEM : SIE_ERR_CUDA;
+}
+
+// src/lib_sie_integration_points.f90:7-141; the literals are binary32.
+Rule make_rule(int ngp) {
+  Rule r;
+  memset(&r, 0, sizeof(r));
+  r.n = ngp;
+  if (ngp == 1) {
+    r.a[0] = 0.33333333333333f;
+    r.b[0] = 0.33333333333333f;
+    r.w[0] = 1.0f;
+  } else if (ngp == 3) {
+    const float a[3] = {0.16666666666667f, 0.16666666666667f, 0.66666666666667f};
+    const float b[3] = {0.16666666666667f, 0.66666666666667f, 0.16666666666667f};
+    for (int i = 0; i < 3; i++) {
+      r.a[i] = a[i];
+      r.b[i] = b[i];
+      r.w[i] = 0.33333333333333f;
+    }
+  } else if (ngp == 4) {
+    const float a[4] = {0.33333333333333f, 0.20000000000000f, 0.20000000000000f, 0.60000000000000f};
+    const float b[4] = {0.33333333333333f, 0.20000000000000f, 0.60000000000000f, 0.20000000000000f};
+    const float w[4] = {-0.56250000000000f, 0.52083333333333f, 0.52083333333333f,
+                        0.52083333333333f};
+    for (int i = 0; i < 4; i++) {
+      r.a[i] = a[i];
+      r.b[i] = b[i];
+      r.w[i] = w[i];
+    }
+  } else if (ngp == 6) {
+    const float a[6] = {0.44594849091597f, 0.44594849091597f, 0.10810301816807f,
+                        0.09157621350977f, 0.09157621350977f, 0.81684757298046f};
+    const float b[6] = {0.44594849091597f, 0.10810301816807f, 0.44594849091597f,
+                        0.09157621350977f, 0.81684757298046f, 0.09157621350977f};
+    const float w[6] = {0.22338158967801f, 0.22338158967801f, 0.22338158967801f,
+                        0.10995174365532f, 0.10995174365532f, 0.10995174365532f};
+    for (int i = 0; i < 6; i++) {
+      r.a[i] = a[i];
+      r.b[i] = b[i];
+      r.w[i] = w[i];
+    }
+  } else if (ngp == 7) {
+    const float a[7] = {0.33333333333333f, 0.47014206410511f, 0.47014206410511f,
+                        0.05971587178977f, 0.10128650732346f, 0.10128650732346f,
+                        0.79742698535309f};
+    const float b[7] = {0.33333333333333f, 0.47014206410511f, 0.05971587178977f,
+                        0.47014206410511f, 0.10128650732346f, 0.79742698535309f,
+                        0.10128650732346f};
+    const float w[7] = {0.22500000000000f, 0.13239415278851f, 0.13239415278851f,
+                        0.13239415278851f, 0.12593918054483f, 0.12593918054483f,
+                        0.12593918054483f};
+    for (int i = 0; i < 7; i++) {
+      r.a[i] = a[i];
+      r.b[i] = b[i];
+      r.w[i] = w[i];
+    }
+  } else if (ngp == 12) {
+    const float a[12] = {0.249286745170910f, 0.249286745170910f, 0.501426509658180f,
+                         0.063089014491500f, 0.063089014491500f, 0.873821971017000f,
+                         0.310352451033780f, 0.636502499121400f, 0.053145049844820f,
+                         0.636502499121400f, 0.310352451033780f, 0.053145049844820f};
+    const float b[12] = {0.249286745170910f, 0.501426509658180f, 0.249286745170910f,
+                         0.063089014491500f, 0.873821971017000f, 0.063089014491500f,
+                         0.636502499121400f, 0.053145049844820f, 0.310352451033780f,
+                         0.310352451033780f, 0.053145049844820f, 0.636502499121400f};
+    const float w[12] = {0.116786275726380f, 0.116786275726380f, 0.116786275726380f,
+                         0.0508449063702100f, 0.0508449063702100f, 0.0508449063702100f,
+                         0.0828510756183700f, 0.0828510756183700f, 0.0828510756183700f,
+                         0.0828510756183700f, 0.0828510756183700f, 0.0828510756183700f};
+    for (int i = 0; i < 12; i++) {
+      r.a[i] = a[i];
+      r.b[i] = b[i];
+      r.w[i] = w[i];
+    }
+  } else {
+    r.n = 0;
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Morton universal index (src/lib/libtree/lib/lib_tree_helper_functions.f90:217-379,
+// 1652-1875): x is the most significant bit of every triple.
+static const int L_TH = 21;
+static inline uint64_t morton3(uint64_t ix, uint64_t iy, uint64_t iz, int l) {
+  uint64_t n = 0;
+  for (int b = l - 1; b >= 0; b--)
+    n = (n << 3) | (((ix >> b) & 1) << 2) | (((iy >> b) & 1) << 1) | ((iz >> b) & 1);
+  return n;
+}
+static inline void demorton3(uint64_t n, int l, int64_t& ix, int64_t& iy, int64_t& iz) {
+  ix = iy = iz = 0;
+  for (int b = 0; b < l; b++) {
+    iz |= (int64_t)((n >> (3 * b)) & 1) << b;
+    iy |= (int64_t)((n >> (3 * b + 1)) & 1) << b;
+    ix |= (int64_t)((n >> (3 * b + 2)) & 1) << b;
+  }
+}
+static inline uint64_t coord_bits(double f, int l) {
+  if (!(f > 0.0)) return 0;
+  return (uint64_t)std::floor(std::ldexp(f, l));
+}
+
+static void box_centre(const sie_ctx* c, uint64_t n, int l, double* out) {
+  int64_t i[3];
+  demorton3(n, l, i[0], i[1], i[2]);
+  double s = std::ldexp(1.0, -l);
+  for (int d = 0; d < 3; d++) out[d] = s * (i[d] + 0.5) * c->D + c->xmin[d];
+}
+
+static int index_of(const std::vector<uint64_t>& v, uint64_t n) {
+  auto it = std::lower_bound(v.begin(), v.end(), n);
+  if (it == v.end() || *it != n) return -1;
+  return (int)(it - v.begin());
+}
+
+// k = 1 neighbours at level l, self excluded (lib_tree_hf_get_neighbour_all_xD)
+static void neighbours(uint64_t n, int l, std::vector<uint64_t>& out) {
+  out.clear();
+  int64_t ix, iy, iz;
+  demorton3(n, l, ix, iy, iz);
+  int64_t ub = ((int64_t)1 << l) - 1;
+  for (int dx = -1; dx <= 1; dx++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dz = -1; dz <= 1; dz++) {
+        int64_t a = ix + dx, b = iy + dy, cc = iz + dz;
+        if (a < 0 || b < 0 || cc < 0 || a > ub || b > ub || cc > ub) continue;
+        uint64_t m = morton3(a, b, cc, l);
+        if (m != n) out.push_back(m);
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Mesh topology: find_neighbours (:865-905) in the order of its (i<j) scan,
+// fn_parameter_type (:1539-1586).
+static int build_mesh(sie_ctx* c) {
+  int nt = c->nt;
+  c->cent.resize(3 * (size_t)nt);
+  for (int t = 0; t < nt; t++) {
+    for (int d = 0; d < 3; d++) {
+      double a = c->verts[3 * c->tris[3 * t] + d], b = c->verts[3 * c->tris[3 * t + 1] + d],
+             e = c->verts[3 * c->tris[3 * t + 2] + d];
+      c->cent[3 * t + d] = (a + b + e) / 3.0;
+    }
+  }
+  std::unordered_map<uint64_t, std::vector<int>> emap;
+  emap.reserve((size_t)nt * 2);
+  for (int t = 0; t < nt; t++)
+    for (int e = 0; e < 3; e++) {
+      uint64_t a = (uint32_t)c->tris[3 * t + e], b = (uint32_t)c->tris[3 * t + (e + 1) % 3];
+      if (a > b) std::swap(a, b);
+      emap[(a << 32) | b].push_back(t);
+    }
+  std::vector<std::pair<int, int>> prs;
+  prs.reserve((size_t)nt * 2);
+  for (auto& kv : emap) {
+    auto& L = kv.second;
+    std::sort(L.begin(), L.end());
+    for (size_t i = 0; i < L.size(); i++)
+      for (size_t j = i + 1; j < L.size(); j++) prs.push_back({L[i], L[j]});
+  }
+  std::sort(prs.begin(), prs.end());
+  prs.erase(std::unique(prs.begin(), prs.end()), prs.end());
+  c->elem.clear();
+  c->corner.clear();
+  for (auto& pr : prs) {
+    int i = pr.first, j = pr.second;
+    int com[3], nc = 0;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++)
+        if (c->tris[3 * i + a] == c->tris[3 * j + b] && nc < 3) com[nc++] = c->tris[3 * i + a];
+    if (nc != 2) continue;
+    c->elem.push_back(i);
+    c->elem.push_back(j);
+    c->corner.push_back(com[0]);
+    c->corner.push_back(com[1]);
+  }
+  c->M = (int)c->elem.size() / 2;
+  if (c->M == 0) return fail(SIE_ERR_MESH, "mesh has no interior edge (no RWG basis)");
+  c->fn_ext.resize(2 * (size_t)c->M);
+  const double* P = c->verts.data();
+  for (int e = 0; e < c->M; e++) {
+    for (int ot = 0; ot < 2; ot++) {
+      int t = c->elem[2 * e + ot];
+      int c1 = c->corner[2 * e], c2 = c->corner[2 * e + 1];
+      int nv = 0, ipc = 0;
+      for (int j = 0; j < 3; j++) {
+        int v = c->tris[3 * t + j];
+        if (v != c1 && v != c2) {
+          ipc = v;
+          nv = j + 1;
+        }
+      }
+      const int* T = &c->tris[3 * t];
+      int i1, i2;
+      if (nv == 1) {
+        i1 = T[1];
+        i2 = T[2];
+      } else if (nv == 2) {
+        i1 = T[2];
+        i2 = T[0];
+      } else {
+        i1 = T[0];
+        i2 = T[1];
+      }
+      FnD f;
+      memset(&f, 0, sizeof(f));
+      vd p1 = mkv<double>(P[3 * i1], P[3 * i1 + 1], P[3 * i1 + 2]);
+      vd p2 = mkv<double>(P[3 * i2], P[3 * i2 + 1], P[3 * i2 + 2]);
+      vd pc = mkv<double>(P[3 * ipc], P[3 * ipc + 1], P[3 * ipc + 2]);
+      f.c[0] = p1.x; f.c[1] = p1.y; f.c[2] = p1.z;
+      f.c[3] = p2.x; f.c[4] = p2.y; f.c[5] = p2.z;
+      f.c[6] = pc.x; f.c[7] = pc.y; f.c[8] = pc.z;
+      f.length = vlen(p1 - p2);
+      f.area = 0.5 * vlen(cross(p1 - pc, p2 - pc));
+      if (!(f.area > 0.0)) return fail(SIE_ERR_MESH, "degenerate triangle " + std::to_string(t));
+      f.sgn = (ot == 0) ? 1.0 : -1.0;
+      f.df = f.sgn * f.length / f.area;
+      for (int d = 0; d < 3; d++) f.mid[d] = c->cent[3 * t + d];
+      vd a, b;
+      if (c->cfg.normal_convention == 1) {
+        a = p1 - p2;
+        b = pc - p2;
+      } else {
+        a = pc - p1;
+        b = p2 - p1;
+      }
+      vd n = cross(a, b);
+      double ln = vlen(n);
+      f.nq[0] = n.x / ln;
+      f.nq[1] = n.y / ln;
+      f.nq[2] = n.z / ln;
+      f.tri = t;
+      c->fn_ext[2 * e + ot] = f;
+    }
+  }
+  return SIE_OK;
+}
+
+// Octree of the edge midpoints (lib_tree_constructor, lib_tree.f90:176-321;
+// scaling :370-434; lib_tree_get_level_max :1290-1345).
+static int build_tree(sie_ctx* c) {
+  int M = c->M;
+  std::vector<double> pos(3 * (size_t)M);
+  for (int e = 0; e < M; e++) {
+    const FnD& f = c->fn_ext[2 * e];
+    for (int d = 0; d < 3; d++) pos[3 * e + d] = (f.c[d] + f.c[3 + d]) / 2.0;  // fn_edge_center
+  }
+  double xmax[3], Dd[3];
+  for (int d = 0; d < 3; d++) {
+    c->xmin[d] = 1e300;
+    xmax[d] = -1e300;
+  }
+  for (int e = 0; e < M; e++)
+    for (int d = 0; d < 3; d++) {
+      c->xmin[d] = std::min(c->xmin[d], pos[3 * e + d]);
+      xmax[d] = std::max(xmax[d], pos[3 * e + d]);
+    }
+  for (int d = 0; d < 3; d++) Dd[d] = (xmax[d] - c->xmin[d]) * (1 + std::ldexp(1.0, -52));
+  c->D = std::max(Dd[0], std::max(Dd[1], Dd[2]));
+  if (!(c->D > 0.0)) return fail(SIE_ERR_MESH, "all edge midpoints coincide");
+  std::vector<uint64_t> nth(M);
+  for (int e = 0; e < M; e++) {
+    uint64_t ic[3];
+    for (int d = 0; d < 3; d++) ic[d] = coord_bits((pos[3 * e + d] - c->xmin[d]) / c->D, L_TH);
+    nth[e] = morton3(ic[0], ic[1], ic[2], L_TH);
+  }
+  std::vector<uint64_t> srt = nth;
+  std::sort(srt.begin(), srt.end());
+  int s = c->cfg.tree_s_opt;
+  int l_max = 1;
+  for (long i = 0; i + s < (long)M; i++) {
+    uint64_t a = srt[i], b = srt[i + s];
+    for (int lev = L_TH - 1; lev >= 0; lev--) {
+      int sh = 3 * (L_TH - lev);
+      if ((a >> sh) == (b >> sh)) {
+        l_max = std::max(l_max, lev + 1);
+        break;
+      }
+    }
+  }
+  if (c->cfg.dense) l_max = 1;
+  c->l_max = l_max;
+  c->l_min = std::min(2, l_max);
+  c->leaf.resize(M);
+  for (int e = 0; e < M; e++) c->leaf[e] = nth[e] >> (3 * (L_TH - l_max));
+  // internal order: edges sorted by leaf box (stable)
+  c->perm.resize(M);
+  for (int e = 0; e < M; e++) c->perm[e] = e;
+  std::stable_sort(c->perm.begin(), c->perm.end(),
+                   [&](int a, int b) { return c->leaf[a] < c->leaf[b]; });
+  c->iperm.resize(M);
+  for (int i = 0; i < M; i++) c->iperm[c->perm[i]] = i;
+  c->lv.assign(l_max + 1, Level());
+  for (int l = c->l_min; l <= l_max; l++) {
+    std::vector<uint64_t> v(M);
+    for (int e = 0; e < M; e++) v[e] = c->leaf[e] >> (3 * (l_max - l));
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    c->lv[l].l = l;
+    c->lv[l].box = v;
+    c->lv[l].nb = (int)v.size();
+    c->lv[l].only_k1 = (c->mt.k2.im != 0.0) && (l < l_max);
+  }
+  // leaf boxes in internal numbering
+  NearLayout& N = c->near;
+  const std::vector<uint64_t>& lb = c->lv[l_max].box;
+  N.nbox = (int)lb.size();
+  N.box_first.assign(N.nbox, 0);
+  N.box_cnt.assign(N.nbox, 0);
+  for (int i = 0; i < M; i++) {
+    int b = index_of(lb, c->leaf[c->perm[i]]);
+    if (N.box_cnt[b] == 0) N.box_first[b] = i;
+    N.box_cnt[b]++;
+  }
+  N.nbr_ptr.assign(N.nbox + 1, 0);
+  N.nbr_box.clear();
+  N.ncols.assign(N.nbox, 0);
+  N.base.assign(N.nbox + 1, 0);
+  std::vector<uint64_t> nb;
+  for (int a = 0; a < N.nbox; a++) {
+    std::vector<int> lst;
+    if (c->cfg.dense) {
+      for (int b = 0; b < N.nbox; b++) lst.push_back(b);
+    } else {
+      neighbours(lb[a], l_max, nb);
+      lst.push_back(a);
+      for (uint64_t n : nb) {
+        int b = index_of(lb, n);
+        if (b >= 0) lst.push_back(b);
+      }
+      std::sort(lst.begin(), lst.end());
+    }
+    int nc = 0;
+    for (int b : lst) {
+      N.nbr_box.push_back(b);
+      nc += N.box_cnt[b];
+    }
+    N.nbr_ptr[a + 1] = (int)N.nbr_box.size();
+    N.ncols[a] = nc;
+    N.base[a + 1] = N.base[a] + (long long)N.box_cnt[a] * nc;
+  }
+  N.nnz = N.base[N.nbox];
+  return SIE_OK;
+}
+
+template <typename T>
+static int upload(T** d, const std::vector<T>& h) {
+  size_t n = std::max<size_t>(h.size(), 1);
+  SIE_CUDA(cudaMalloc(d, n * sizeof(T)));
+  if (!h.empty()) SIE_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return SIE_OK;
+}
+
+
+// I4 interaction lists, children and parents of every level (lib_tree_get_domain_i4,
+// lib_tree.f90:1096-1245).
+static int build_levels(sie_ctx* c) {
+  std::vector<uint64_t> par, own;
+  for (int l = c->l_min; l <= c->l_max; l++) {
+    Level& L = c->lv[l];
+    std::vector<int> i4p(L.nb + 1, 0), i4s, i4o;
+    for (int b = 0; b < L.nb; b++) {
+      uint64_t n = L.box[b];
+      if (!c->cfg.dense && l >= 1) {
+        neighbours(n >> 3, l - 1, par);
+        par.push_back(n >> 3);
+        neighbours(n, l, own);
+        own.push_back(n);
+        std::sort(own.begin(), own.end());
+        std::vector<uint64_t> cand;
+        for (uint64_t p : par)
+          for (uint64_t ch = 0; ch < 8; ch++) {
+            uint64_t m = (p << 3) | ch;
+            if (!std::binary_search(own.begin(), own.end(), m)) cand.push_back(m);
+          }
+        std::sort(cand.begin(), cand.end());
+        int64_t ax, ay, az;
+        demorton3(n, l, ax, ay, az);
+        for (uint64_t m : cand) {
+          int s = index_of(L.box, m);
+          if (s < 0) continue;
+          int64_t bx, by, bz;
+          demorton3(m, l, bx, by, bz);
+          int t = (int)((ax - bx + 3) * 49 + (ay - by + 3) * 7 + (az - bz + 3));
+          i4s.push_back(s);
+          i4o.push_back(t);
+        }
+      }
+      i4p[b + 1] = (int)i4s.size();
+    }
+    L.n_i4 = (long long)i4s.size();
+    SIE_TRY(upload(&L.i4_ptr, i4p));
+    SIE_TRY(upload(&L.i4_src, i4s));
+    SIE_TRY(upload(&L.i4_off, i4o));
+    // children at l+1
+    std::vector<int> chp(L.nb + 1, 0), chi, cho;
+    if (l < c->l_max) {
+      Level& C = c->lv[l + 1];
+      for (int b = 0; b < L.nb; b++) {
+        for (uint64_t o = 0; o < 8; o++) {
+          int ci = index_of(C.box, (L.box[b] << 3) | o);
+          if (ci >= 0) {
+            chi.push_back(ci);
+            cho.push_back((int)o);
+          }
+        }
+        chp[b + 1] = (int)chi.size();
+      }
+    }
+    SIE_TRY(upload(&L.ch_ptr, chp));
+    SIE_TRY(upload(&L.ch_idx, chi));
+    SIE_TRY(upload(&L.ch_oct, cho));
+    std::vector<int> pa(L.nb, -1), oc(L.nb, 0);
+    if (l > c->l_min) {
+      Level& P = c->lv[l - 1];
+      for (int b = 0; b < L.nb; b++) {
+        pa[b] = index_of(P.box, L.box[b] >> 3);
+        oc[b] = (int)(L.box[b] & 7);
+      }
+    }
+    SIE_TRY(upload(&L.parent, pa));
+    SIE_TRY(upload(&L.oct, oc));
+  }
+  return SIE_OK;
+}
+
+// Gauss-Legendre nodes, ascending (the reference uses the Glaser-Liu-Rokhlin
+// rule, src/Gauss_Quadrature_Fast.f90:424-498; both are exact to rounding).
+static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  auto leg = [n](double z, double& pn, double& dpn) {
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= n; k++) {
+      double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    pn = p1;
+    dpn = n * (z * p1 - p0) / (z * z - 1.0);
+  };
+  for (int i = 0; i < n; i++) {
+    double z = std::cos(PI * (i + 0.75) / (n + 0.5));
+    double pn, dp;
+    int extra = 0;
+    for (int it = 0; it < 100 && extra < 2; it++) {
+      leg(z, pn, dp);
+      double dz = pn / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-15) extra++;
+    }
+    leg(z, pn, dp);
+    x[n - 1 - i] = z;
+    w[n - 1 - i] = 2.0 / ((1 - z * z) * dp * dp);
+  }
+}
+
+// Khat_and_TRF_ExtendedK (src/lib_sie_mlfmm.f90:190-240)
+static int build_sampling(sie_ctx* c) {
+  int K = c->K, Ns = 2 * K * K, Q = Ns + 2;
+  c->Q = Q;
+  std::vector<double> xx, ww;
+  gauss_legendre(K, xx, ww);
+  std::vector<double> kh(3 * Q), th(3 * Q), ph(3 * Q), trf(Q);
+  double dphi = 2 * PI / (2 * K);
+  for (int j = 0; j < K; j++)
+    for (int k = 0; k < 2 * K; k++) {
+      double phi = k * dphi;
+      int i = k + j * 2 * K;
+      double st = std::sin(std::acos(xx[j]));
+      kh[3 * i] = st * std::cos(phi);
+      kh[3 * i + 1] = st * std::sin(phi);
+      kh[3 * i + 2] = xx[j];
+      th[3 * i] = xx[j] * std::cos(phi);
+      th[3 * i + 1] = xx[j] * std::sin(phi);
+      th[3 * i + 2] = -st;
+      ph[3 * i] = -std::sin(phi);
+      ph[3 * i + 1] = std::cos(phi);
+      ph[3 * i + 2] = 0.0;
+      trf[i] = ww[j] * dphi;
+    }
+  double pk[2][3] = {{0, 0, 1}, {0, 0, -1}};
+  for (int p = 0; p < 2; p++) {
+    int i = Ns + p;
+    for (int d = 0; d < 3; d++) kh[3 * i + d] = pk[p][d];
+    th[3 * i] = 1; th[3 * i + 1] = 0; th[3 * i + 2] = 0;
+    ph[3 * i] = 0; ph[3 * i + 1] = 1; ph[3 * i + 2] = 0;
+    trf[i] = 0.0;
+  }
+  SIE_TRY(upload(&c->d_khat, kh));
+  SIE_TRY(upload(&c->d_tth, th));
+  SIE_TRY(upload(&c->d_tph, ph));
+  SIE_TRY(upload(&c->d_trf, trf));
+  return SIE_OK;
+}
+
+static Material make_material(const sie_config& cfg) {
+  Material m;
+  auto csqrt = [](zc z) {
+    double r = std::hypot(z.re, z.im);
+    double a = std::sqrt((r + std::fabs(z.re)) / 2);
+    if (a == 0.0) return mk<double>(0, 0);
+    if (z.re >= 0) return mk<double>(a, z.im / (2 * a));
+    return mk<double>(std::fabs(z.im) / (2 * a), z.im >= 0 ? a : -a);
+  };
+  m.k0 = 2 * PI / cfg.lambda;
+  m.omega = 2 * PI * C0 / cfg.lambda;
+  m.my1 = MU0;
+  m.my2 = MU0;
+  zc er1 = mk<double>(cfg.eps_r1_re, cfg.eps_r1_im), er2 = mk<double>(cfg.eps_r2_re, cfg.eps_r2_im);
+  m.k1 = csqrt(er1) * m.k0;
+  m.k2 = csqrt(er2) * m.k0;
+  m.eps1 = er1 * EPS0;
+  m.eps2 = er2 * EPS0;
+  m.eta1 = csqrt(mk<double>(m.my1, 0) / m.eps1);
+  m.eta2 = csqrt(mk<double>(m.my2, 0) / m.eps2);
+  m.eta_a = (m.eta1 + m.eta2) * 0.5;
+  return m;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+static int ensure_work(sie_ctx* c, int nrhs) {
+  if ((size_t)nrhs <= c->work_rhs) return SIE_OK;
+  if (c->d_xi) cudaFree(c->d_xi);
+  if (c->d_yi) cudaFree(c->d_yi);
+  c->d_xi = c->d_yi = nullptr;
+  size_t n = (size_t)2 * c->M * nrhs;
+  SIE_CUDA(cudaMalloc(&c->d_xi, n * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&c->d_yi, n * sizeof(zc)));
+  c->work_rhs = nrhs;
+  return SIE_OK;
+}
+
+}  // namespace sie
+
+using namespace sie;
+
+// Device matvec on internal-layout vectors: y = Z x (one right-hand side per call).
+int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed) {
+  for (int r = 0; r < nrhs; r++) {
+    const zc* x = xi + (size_t)r * 2 * c->M;
+    zc* y = yi + (size_t)r * 2 * c->M;
+    if (timed) cudaEventRecord(c->ev[0], st);
+    SIE_TRY(near_matvec64(c, x, y, 1, false, st));
+    if (timed) cudaEventRecord(c->ev[6], st);
+    if (!c->cfg.dense) SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr));
+    if (timed) {
+      cudaEventRecord(c->ev[7], st);
+      cudaEventSynchronize(c->ev[7]);
+      float a = 0;
+      cudaEventElapsedTime(&a, c->ev[0], c->ev[7]);
+      c->tm.mv_total_ms = a;
+      cudaEventElapsedTime(&a, c->ev[0], c->ev[6]);
+      c->tm.mv_near_ms = a;
+      if (!c->cfg.dense) {
+        cudaEventElapsedTime(&a, c->ev[6], c->ev[1]);
+        c->tm.mv_agg_ms = a;
+        cudaEventElapsedTime(&a, c->ev[1], c->ev[2]);
+        c->tm.mv_ss_ms = a;
+        cudaEventElapsedTime(&a, c->ev[2], c->ev[3]);
+        c->tm.mv_sr_ms = a;
+        cudaEventElapsedTime(&a, c->ev[3], c->ev[4]);
+        c->tm.mv_rr_ms = a;
+        cudaEventElapsedTime(&a, c->ev[4], c->ev[5]);
+        c->tm.mv_recv_ms = a;
+      }
+    }
+  }
+  return SIE_OK;
+}
+
+extern "C" {
+
+void sie_config_default(sie_config* cfg) {
+  if (!cfg) return;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->lambda = 500e-9;
+  cfg->eps_r1_re = 1.0;
+  cfg->eps_r1_im = 0.0;
+  cfg->eps_r2_re = 18.392;
+  cfg->eps_r2_im = -0.4164;
+  cfg->formulation = SIE_ICTF;
+  cfg->ngp = 3;
+  cfg->tree_s_opt = 250;
+  cfg->truncation_number = 19;
+  cfg->normal_convention = 2;
+  cfg->fix_itbn = 0;
+  cfg->device = 0;
+  cfg->dense = 0;
+}
+
+void sie_solver_default(sie_solver_cfg* cfg) {
+  if (!cfg) return;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->restart = 50;
+  cfg->max_iterations = 650;
+  cfg->tolerance = 1e-6;
+  cfg->use_initial_guess = 0;
+  cfg->precision = SIE_FP64;
+  cfg->inner_restart = 30;
+  cfg->inner_tolerance = 1e-4;
+  cfg->time_limit_s = 0;
+}
+
+const char* sie_last_error(void) { return g_err.c_str(); }
+
+unsigned long long sie_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int sie_set_stream(sie_ctx* c, void* stream) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_set_stream: null context");
+  SIE_CUDA(cudaSetDevice(c->device));
+  SIE_CUDA(cudaStreamSynchronize(c->stream));
+  if (!c->own_stream) c->own_stream = c->stream;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return SIE_OK;
+}
+const char* sie_version(void) { return "specklesim_b200 0.1 (sm_100a)"; }
+
+int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris, int nt,
+             sie_ctx** out) {
+  if (!cfg || !verts || !tris || !out) return fail(SIE_ERR_ARG, "sie_init: null argument");
+  *out = nullptr;
+  if (nv < 3 || nt < 2) return fail(SIE_ERR_ARG, "sie_init: mesh too small");
+  if (!(cfg->lambda > 0)) return fail(SIE_ERR_ARG, "sie_init: lambda must be > 0");
+  if (cfg->formulation != SIE_ICTF && cfg->formulation != SIE_PMCHWT)
+    return fail(SIE_ERR_ARG, "sie_init: formulation must be SIE_ICTF or SIE_PMCHWT");
+  Rule R = make_rule(cfg->ngp);
+  if (R.n == 0) return fail(SIE_ERR_ARG, "sie_init: ngp must be one of 1,3,4,6,7,12");
+  if (cfg->truncation_number < 1 || cfg->truncation_number > 60)
+    return fail(SIE_ERR_ARG, "sie_init: truncation_number must be in 1..60");
+  if (cfg->tree_s_opt < 1) return fail(SIE_ERR_ARG, "sie_init: tree_s_opt must be >= 1");
+  for (int i = 0; i < 3 * nt; i++)
+    if (tris[i] < 0 || tris[i] >= nv) return fail(SIE_ERR_MESH, "sie_init: vertex index out of range");
+  for (int i = 0; i < 3 * nv; i++)
+    if (!std::isfinite(verts[i])) return fail(SIE_ERR_NONFINITE, "sie_init: non-finite vertex");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(SIE_ERR_CUDA, "sie_init: no CUDA device");
+  if (cfg->device < 0 || cfg->device >= ndev) return fail(SIE_ERR_ARG, "sie_init: bad device");
+  sie_ctx* c = new sie_ctx();
+  c->cfg = *cfg;
+  c->device = cfg->device;
+  c->R = R;
+  c->mt = make_material(*cfg);
+  c->K = cfg->truncation_number;
+  c->nv = nv;
+  c->nt = nt;
+  c->verts.assign(verts, verts + 3 * (size_t)nv);
+  c->tris.assign(tris, tris + 3 * (size_t)nt);
+  auto cleanup = [&](int r) {
+    sie_free(c);
+    return r;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return cleanup(fail(SIE_ERR_CUDA, "cudaSetDevice"));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(SIE_ERR_CUDA, "stream"));
+  if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(SIE_ERR_CUDA, "stream"));
+  for (int i = 0; i < 16; i++) cudaEventCreate(&c->ev[i]);
+  int r = build_mesh(c);
+  if (r != SIE_OK) return cleanup(r);
+  r = build_tree(c);
+  if (r != SIE_OK) return cleanup(r);
+  // ICTF: D21 = -eta_a^2 D12 ; PMCHWT: D21 = -D12
+  c->cfac = (cfg->formulation == SIE_ICTF) ? -(c->mt.eta_a * c->mt.eta_a) : mk<double>(-1.0, 0.0);
+  *out = c;
+  return SIE_OK;
+}
+
+int sie_info(const sie_ctx* c, int* n_edges, int* l_min, int* l_max, long long* nnz) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_info: null context");
+  if (n_edges) *n_edges = c->M;
+  if (l_min) *l_min = c->l_min;
+  if (l_max) *l_max = c->l_max;
+  if (nnz) *nnz = c->near.nnz;
+  return SIE_OK;
+}
+
+int sie_num_directions(const sie_ctx* c, int* Q) {
+  if (!c || !Q) return fail(SIE_ERR_ARG, "null argument");
+  *Q = 2 * c->K * c->K + 2;
+  return SIE_OK;
+}
+
+int sie_setup(sie_ctx* c) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_setup: null context");
+  if (c->setup_done) return SIE_OK;
+  SIE_CUDA(cudaSetDevice(c->device));
+  auto t0 = std::chrono::steady_clock::now();
+  int M = c->M;
+  // internal-order fn table and per-edge data
+  std::vector<FnD> fn(2 * (size_t)M);
+  std::vector<double> rref(M);
+  std::vector<int> ebox(M);
+  for (int i = 0; i < M; i++) {
+    int e = c->perm[i];
+    fn[2 * i] = c->fn_ext[2 * e];
+    fn[2 * i + 1] = c->fn_ext[2 * e + 1];
+    const double* a = &c->cent[3 * c->elem[2 * e]];
+    const double* b = &c->cent[3 * c->elem[2 * e + 1]];
+    rref[i] = std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) +
+                        (a[2] - b[2]) * (a[2] - b[2]));
+  }
+  for (int b = 0; b < c->near.nbox; b++)
+    for (int k = 0; k < c->near.box_cnt[b]; k++) ebox[c->near.box_first[b] + k] = b;
+  SIE_TRY(upload(&c->d_fn, fn));
+  SIE_TRY(upload(&c->d_rref, rref));
+  SIE_TRY(upload(&c->d_cent, c->cent));
+  SIE_TRY(upload(&c->d_perm, c->perm));
+  SIE_TRY(upload(&c->d_edge_box, ebox));
+  SIE_TRY(upload(&c->d_box_first, c->near.box_first));
+  SIE_TRY(upload(&c->d_box_cnt, c->near.box_cnt));
+  SIE_TRY(upload(&c->d_nbr_ptr, c->near.nbr_ptr));
+  SIE_TRY(upload(&c->d_nbr_box, c->near.nbr_box));
+  SIE_TRY(upload(&c->d_ncols, c->near.ncols));
+  SIE_TRY(upload(&c->d_base, c->near.base));
+  int* d_tv = nullptr;
+  SIE_TRY(upload(&d_tv, c->tris));
+  // near-field values
+  size_t nnz = (size_t)c->near.nnz;
+  SIE_CUDA(cudaMalloc(&c->d_na, std::max<size_t>(nnz, 1) * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&c->d_nb, std::max<size_t>(nnz, 1) * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&c->d_nd, std::max<size_t>(nnz, 1) * sizeof(zc)));
+  cudaEventRecord(c->ev[8], c->stream);
+  int r = near_fill(c, d_tv);
+  cudaEventRecord(c->ev[9], c->stream);
+  cudaFree(d_tv);
+  if (r != SIE_OK) return r;
+  SIE_TRY(diag_extract(c));
+  // far field
+  if (!c->cfg.dense) {
+    SIE_TRY(build_sampling(c));
+    SIE_TRY(build_levels(c));
+    int Q = c->Q;
+    std::vector<double> boxc(3 * (size_t)c->near.nbox);
+    for (int b = 0; b < c->near.nbox; b++)
+      box_centre(c, c->lv[c->l_max].box[b], c->l_max, &boxc[3 * b]);
+    double* d_boxc = nullptr;
+    SIE_TRY(upload(&d_boxc, boxc));
+    SIE_CUDA(cudaMalloc(&c->d_rt, (size_t)M * 4 * Q * sizeof(zc)));
+    for (int l = c->l_min; l <= c->l_max; l++) {
+      Level& L = c->lv[l];
+      SIE_CUDA(cudaMalloc(&L.C, (size_t)L.nb * 8 * Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.D, (size_t)L.nb * 8 * Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.tl, (size_t)343 * 2 * Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.ph_up, (size_t)8 * 2 * Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.ph_dn, (size_t)8 * 2 * Q * sizeof(zc)));
+      SIE_TRY(phase_tables(c, L, l));
+    }
+    cudaEventRecord(c->ev[10], c->stream);
+    r = far_build_tables(c, d_boxc);
+    cudaEventRecord(c->ev[11], c->stream);
+    cudaFree(d_boxc);
+    if (r != SIE_OK) return r;
+    SIE_TRY(far_prepare_kernels(c));
+  }
+  SIE_CUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]);
+  c->tm.fill_ms = ms;
+  if (!c->cfg.dense) {
+    cudaEventElapsedTime(&ms, c->ev[10], c->ev[11]);
+    c->tm.rt_ms = ms;
+  }
+  c->tm.setup_ms = ms_since(t0);
+  c->setup_done = true;
+  return SIE_OK;
+}
+
+int sie_matvec_device(sie_ctx* c, const double* d_x, double* d_y, int nrhs, int precision,
+                      void* stream) {
+  if (!c || !d_x || !d_y || nrhs < 1) return fail(SIE_ERR_ARG, "sie_matvec_device: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_matvec_device: sie_setup not called");
+  if (precision != SIE_FP64 && precision != SIE_MIXED)
+    return fail(SIE_ERR_ARG, "sie_matvec_device: bad precision");
+  SIE_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  SIE_TRY(ensure_work(c, nrhs));
+  SIE_TRY(gather_ext_to_int(c, (const zc*)d_x, c->d_xi, nrhs, st));
+  SIE_TRY(sie_internal_matvec(c, c->d_xi, c->d_yi, nrhs, st, true));
+  SIE_TRY(scatter_int_to_ext(c, c->d_yi, (zc*)d_y, nrhs, st));
+  SIE_CUDA(cudaStreamSynchronize(st));
+  return SIE_OK;
+}
+
+int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) {
+  if (!c || !x || !y || nrhs < 1) return fail(SIE_ERR_ARG, "sie_matvec: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_matvec: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
+  for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
+    if (!std::isfinite(x[i])) return fail(SIE_ERR_NONFINITE, "sie_matvec: non-finite input");
+  zc *dx = nullptr, *dy = nullptr;
+  SIE_CUDA(cudaMalloc(&dx, bytes));
+  SIE_CUDA(cudaMalloc(&dy, bytes));
+  int r = SIE_OK;
+  if (cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    r = fail(SIE_ERR_CUDA, "sie_matvec: H2D copy");
+  if (r == SIE_OK) r = sie_matvec_device(c, (const double*)dx, (double*)dy, nrhs, precision, c->stream);
+  if (r == SIE_OK && (cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                      cudaStreamSynchronize(c->stream) != cudaSuccess))
+    r = fail(SIE_ERR_CUDA, "sie_matvec: D2H copy");
+  cudaFree(dx);
+  cudaFree(dy);
+  return r;
+}
+
+int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in) {
+  if (!k_in || !E_in) return fail(SIE_ERR_ARG, "sie_incidence: null argument");
+  if (k_dir != 1 && k_dir != 2) return fail(SIE_ERR_ARG, "sie_incidence: k_dir must be 1 or 2");
+  double sgn = (k_dir == 1) ? 1.0 : -1.0;
+  double ep[2] = {pol == 1 ? 1.0 : 0.0, pol == 1 ? 0.0 : 1.0};
+  k_in[0] = std::sin(theta) * std::cos(phi);
+  k_in[1] = std::sin(theta) * std::sin(phi);
+  k_in[2] = sgn * std::cos(theta);
+  // field_rotation_matrix (main.f90:297-323)
+  double a = std::sin(theta), b = std::cos(theta), cc = std::sin(phi), d = std::cos(phi);
+  double Rm[3][2] = {{d * d * b + cc * cc, cc * d * (b - 1)},
+                     {cc * d * (b - 1), cc * cc * b + d * d},
+                     {a * d, a * cc}};
+  for (int i = 0; i < 3; i++) E_in[i] = Rm[i][0] * ep[0] + Rm[i][1] * ep[1];
+  return SIE_OK;
+}
+
+int sie_rhs_planewave(sie_ctx* c, const double* k_in, const double* E_in, int nrhs, double* b) {
+  if (!c || !k_in || !E_in || !b || nrhs < 1) return fail(SIE_ERR_ARG, "sie_rhs_planewave: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_rhs_planewave: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  SIE_TRY(ensure_work(c, nrhs));
+  double *dk = nullptr, *dE = nullptr;
+  zc* db = nullptr;
+  size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
+  SIE_CUDA(cudaMalloc(&dk, 3 * nrhs * sizeof(double)));
+  SIE_CUDA(cudaMalloc(&dE, 3 * nrhs * sizeof(double)));
+  SIE_CUDA(cudaMalloc(&db, bytes));
+  SIE_CUDA(cudaMemcpy(dk, k_in, 3 * nrhs * sizeof(double), cudaMemcpyHostToDevice));
+  SIE_CUDA(cudaMemcpy(dE, E_in, 3 * nrhs * sizeof(double), cudaMemcpyHostToDevice));
+  int r = rhs_planewave_dev(c, dk, dE, nrhs, c->d_yi);
+  if (r == SIE_OK) r = scatter_int_to_ext(c, c->d_yi, db, nrhs, c->stream);
+  if (r == SIE_OK && cudaMemcpy(b, db, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+    r = fail(SIE_ERR_CUDA, "sie_rhs_planewave: D2H copy");
+  cudaFree(dk);
+  cudaFree(dE);
+  cudaFree(db);
+  return r;
+}
+
+int sie_solve_device(sie_ctx* c, const double* d_b, double* d_x, int nrhs, const sie_solver_cfg* cfg,
+                     sie_stats* stats) {
+  if (!c || !d_b || !d_x || nrhs < 1 || !cfg) return fail(SIE_ERR_ARG, "sie_solve_device: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_solve_device: sie_setup not called");
+  if (cfg->restart < 1 || cfg->max_iterations < 1 || !(cfg->tolerance > 0))
+    return fail(SIE_ERR_ARG, "sie_solve_device: bad solver configuration");
+  SIE_CUDA(cudaSetDevice(c->device));
+  SIE_TRY(ensure_work(c, 1));
+  int rc_all = SIE_OK;
+  for (int r = 0; r < nrhs; r++) {
+    const zc* b = (const zc*)d_b + (size_t)r * 2 * c->M;
+    zc* x = (zc*)d_x + (size_t)r * 2 * c->M;
+    sie_stats st;
+    memset(&st, 0, sizeof(st));
+    int rc = gmres_solve(c, b, x, cfg, &st);
+    if (stats) stats[r] = st;
+    if (rc != SIE_OK && rc != SIE_ERR_NOCONV) return rc;
+    if (rc == SIE_ERR_NOCONV) rc_all = rc;
+  }
+  return rc_all;
+}
+
+int sie_solve(sie_ctx* c, const double* b, double* x, int nrhs, const sie_solver_cfg* cfg,
+              sie_stats* stats) {
+  if (!c || !b || !x || nrhs < 1 || !cfg) return fail(SIE_ERR_ARG, "sie_solve: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_solve: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
+    if (!std::isfinite(b[i])) return fail(SIE_ERR_NONFINITE, "sie_solve: non-finite right-hand side");
+  size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
+  zc *db = nullptr, *dx = nullptr;
+  SIE_CUDA(cudaMalloc(&db, bytes));
+  SIE_CUDA(cudaMalloc(&dx, bytes));
+  SIE_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (cfg->use_initial_guess) SIE_CUDA(cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  int r = sie_solve_device(c, (const double*)db, (double*)dx, nrhs, cfg, stats);
+  if ((r == SIE_OK || r == SIE_ERR_NOCONV) &&
+      (cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+       cudaStreamSynchronize(c->stream) != cudaSuccess))
+    r = fail(SIE_ERR_CUDA, "sie_solve: D2H copy");
+  cudaFree(db);
+  cudaFree(dx);
+  return r;
+}
+
+int sie_farfield(sie_ctx* c, const double* x, const double* pts, int npts, double* E, double* H,
+                 double* intensity) {
+  if (!c || !x || !pts || npts < 1) return fail(SIE_ERR_ARG, "sie_farfield: bad argument");
+  SIE_CUDA(cudaSetDevice(c->device));
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_farfield: sie_setup not called");
+  SIE_TRY(ensure_work(c, 1));
+  size_t bytes = (size_t)2 * c->M * sizeof(zc);
+  zc *dx = nullptr, *dE = nullptr, *dH = nullptr;
+  double *dp = nullptr, *dI = nullptr;
+  SIE_CUDA(cudaMalloc(&dx, bytes));
+  SIE_CUDA(cudaMalloc(&dp, 3 * (size_t)npts * sizeof(double)));
+  SIE_CUDA(cudaMalloc(&dE, 3 * (size_t)npts * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&dH, 3 * (size_t)npts * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&dI, (size_t)npts * sizeof(double)));
+  SIE_CUDA(cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice));
+  SIE_CUDA(cudaMemcpy(dp, pts, 3 * (size_t)npts * sizeof(double), cudaMemcpyHostToDevice));
+  int r = gather_ext_to_int(c, dx, c->d_xi, 1, c->stream);
+  if (r == SIE_OK) r = farfield_dev(c, c->d_xi, dp, npts, dE, dH, dI);
+  if (r == SIE_OK) {
+    cudaStreamSynchronize(c->stream);
+    if (E) cudaMemcpy(E, dE, 3 * (size_t)npts * sizeof(zc), cudaMemcpyDeviceToHost);
+    if (H) cudaMemcpy(H, dH, 3 * (size_t)npts * sizeof(zc), cudaMemcpyDeviceToHost);
+    if (intensity) cudaMemcpy(intensity, dI, (size_t)npts * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) r = cuda_fail(e, "sie_farfield copies");
+  }
+  cudaFree(dx);
+  cudaFree(dp);
+  cudaFree(dE);
+  cudaFree(dH);
+  cudaFree(dI);
+  return r;
+}
+
+int sie_get_edges(const sie_ctx* c, int* elem, int* corner) {
+  if (!c || !elem || !corner) return fail(SIE_ERR_ARG, "sie_get_edges: null argument");
+  std::copy(c->elem.begin(), c->elem.end(), elem);
+  std::copy(c->corner.begin(), c->corner.end(), corner);
+  return SIE_OK;
+}
+
+int sie_get_tree(const sie_ctx* c, double* D_xmin, long long* leaf) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_get_tree: null context");
+  if (D_xmin) {
+    D_xmin[0] = c->D;
+    for (int d = 0; d < 3; d++) D_xmin[1 + d] = c->xmin[d];
+  }
+  if (leaf)
+    for (int e = 0; e < c->M; e++) leaf[e] = (long long)c->leaf[e];
+  return SIE_OK;
+}
+
+int sie_get_blocks(sie_ctx* c, const int* m, const int* n, int cnt, double* out) {
+  if (!c || !m || !n || !out || cnt < 1) return fail(SIE_ERR_ARG, "sie_get_blocks: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_get_blocks: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  std::vector<int> mi(cnt), ni(cnt);
+  for (int i = 0; i < cnt; i++) {
+    if (m[i] < 0 || m[i] >= c->M || n[i] < 0 || n[i] >= c->M)
+      return fail(SIE_ERR_ARG, "sie_get_blocks: edge index out of range");
+    mi[i] = c->iperm[m[i]];
+    ni[i] = c->iperm[n[i]];
+  }
+  int *dm = nullptr, *dn = nullptr, *dtv = nullptr;
+  zc* dout = nullptr;
+  SIE_TRY(upload(&dm, mi));
+  SIE_TRY(upload(&dn, ni));
+  SIE_TRY(upload(&dtv, c->tris));
+  SIE_CUDA(cudaMalloc(&dout, (size_t)cnt * 3 * sizeof(zc)));
+  int r = near_blocks_list(c, dtv, dm, dn, cnt, dout);
+  std::vector<zc> h((size_t)cnt * 3);
+  if (r == SIE_OK) {
+    cudaStreamSynchronize(c->stream);
+    if (cudaMemcpy(h.data(), dout, h.size() * sizeof(zc), cudaMemcpyDeviceToHost) != cudaSuccess)
+      r = fail(SIE_ERR_CUDA, "sie_get_blocks: copy");
+  }
+  cudaFree(dm);
+  cudaFree(dn);
+  cudaFree(dtv);
+  cudaFree(dout);
+  if (r != SIE_OK) return r;
+  for (int i = 0; i < cnt; i++) {
+    zc a = h[3 * i], b = h[3 * i + 1], d = h[3 * i + 2];
+    zc cc = c->cfac * b;
+    zc v[4] = {a, b, cc, d};
+    for (int k = 0; k < 4; k++) {
+      out[8 * i + 2 * k] = v[k].re;
+      out[8 * i + 2 * k + 1] = v[k].im;
+    }
+  }
+  return SIE_OK;
+}
+
+int sie_get_near_entries(sie_ctx* c, const int* m, const int* n, int cnt, double* out) {
+  if (!c || !m || !n || !out || cnt < 1) return fail(SIE_ERR_ARG, "sie_get_near_entries: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_get_near_entries: sie_setup not called");
+  const NearLayout& N = c->near;
+  std::vector<long long> idx(cnt, -1);
+  std::vector<int> ebox(c->M);
+  for (int b = 0; b < N.nbox; b++)
+    for (int k = 0; k < N.box_cnt[b]; k++) ebox[N.box_first[b] + k] = b;
+  for (int i = 0; i < cnt; i++) {
+    if (m[i] < 0 || m[i] >= c->M || n[i] < 0 || n[i] >= c->M)
+      return fail(SIE_ERR_ARG, "sie_get_near_entries: edge index out of range");
+    int mi = c->iperm[m[i]], ni = c->iperm[n[i]];
+    int A = ebox[mi], B = ebox[ni];
+    int col = 0;
+    bool found = false;
+    for (int k = N.nbr_ptr[A]; k < N.nbr_ptr[A + 1]; k++) {
+      int bb = N.nbr_box[k];
+      if (bb == B) {
+        col += ni - N.box_first[B];
+        found = true;
+        break;
+      }
+      col += N.box_cnt[bb];
+    }
+    if (found) idx[i] = N.base[A] + (long long)(mi - N.box_first[A]) * N.ncols[A] + col;
+  }
+  for (int i = 0; i < cnt; i++) {
+    zc v[3] = {mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0)};
+    if (idx[i] >= 0) {
+      SIE_CUDA(cudaMemcpy(&v[0], c->d_na + idx[i], sizeof(zc), cudaMemcpyDeviceToHost));
+      SIE_CUDA(cudaMemcpy(&v[1], c->d_nb + idx[i], sizeof(zc), cudaMemcpyDeviceToHost));
+      SIE_CUDA(cudaMemcpy(&v[2], c->d_nd + idx[i], sizeof(zc), cudaMemcpyDeviceToHost));
+    }
+    zc cc = c->cfac * v[1];
+    if (idx[i] < 0) cc = mk<double>(0, 0);
+    zc w[4] = {v[0], v[1], cc, v[2]};
+    for (int k = 0; k < 4; k++) {
+      out[8 * i + 2 * k] = w[k].re;
+      out[8 * i + 2 * k + 1] = w[k].im;
+    }
+  }
+  return SIE_OK;
+}
+
+int sie_get_rt(sie_ctx* c, const int* edges, int cnt, double* out) {
+  if (!c || !edges || !out || cnt < 1) return fail(SIE_ERR_ARG, "sie_get_rt: bad argument");
+  if (!c->setup_done || !c->d_rt) return fail(SIE_ERR_STATE, "sie_get_rt: no radiation patterns");
+  size_t per = (size_t)4 * c->Q;
+  for (int i = 0; i < cnt; i++) {
+    if (edges[i] < 0 || edges[i] >= c->M) return fail(SIE_ERR_ARG, "sie_get_rt: edge out of range");
+    int ei = c->iperm[edges[i]];
+    SIE_CUDA(cudaMemcpy(out + 2 * per * i, c->d_rt + per * ei, per * sizeof(zc), cudaMemcpyDeviceToHost));
+  }
+  return SIE_OK;
+}
+
+int sie_get_timings(const sie_ctx* c, double* out, int n) {
+  if (!c || !out) return fail(SIE_ERR_ARG, "sie_get_timings: null argument");
+  double v[11] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
+                  c->tm.mv_near_ms, c->tm.mv_agg_ms, c->tm.mv_ss_ms, c->tm.mv_sr_ms,
+                  c->tm.mv_rr_ms, c->tm.mv_recv_ms, 0.0};
+  for (int i = 0; i < n && i < 11; i++) out[i] = v[i];
+  return SIE_OK;
+}
+
+int sie_free(sie_ctx* c) {
+  if (!c) return SIE_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
+                  c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_na,
+                  c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
+                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_xi, c->d_yi, c->d_gm};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& L : c->lv) {
+    void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.i4_ptr, L.i4_src, L.i4_off,
+                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct};
+    for (void* p : lp)
+      if (p) cudaFree(p);
+  }
+  for (int i = 0; i < 16; i++)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  else if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
+  delete c;
+  return SIE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,201 @@
+// Internal state of the B200 SIE library (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "cplx.cuh"
+#include "../../include/sie_gpu.h"
+
+namespace sie {
+
+// Unsuffixed Fortran literals of the reference are binary32
+// (src/lib_sie_constants.f90:9-11, no real-kind promotion in the build).
+static const double C0 = (double)2.99792458e+8f;
+static const double EPS0 = (double)8.854187817e-12f;
+static const double MU0 = (double)1.2566370614e-6f;
+static const double PI = 3.141592653589793238462643383279502884;
+
+void set_error(const std::string& msg);
+// number of kernels launched by this library since load (for the bench's launch count)
+void count_launch();
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define SIE_TRY(x)               \
+  do {                           \
+    int _r = (x);                \
+    if (_r != SIE_OK) return _r; \
+  } while (0)
+
+#define SIE_CUDA(call)                                      \
+  do {                                                      \
+    cudaError_t _e = (call);                                \
+    if (_e != cudaSuccess) return sie::cuda_fail(_e, #call); \
+  } while (0)
+
+// Triangle quadrature rule (src/lib_sie_integration_points.f90:7-141).
+struct Rule {
+  int n;
+  double a[12], b[12], w[12];
+};
+Rule make_rule(int ngp);
+
+// Half RWG basis of one edge side (fn_rwg, src/lib_sie_type_function.f90:12-20).
+struct FnD {
+  double c[9];  // p1, p2, pc
+  double area, length, df, sgn;
+  double mid[3], nq[3];
+  int tri;
+  int pad;
+};
+
+struct Material {
+  double k0, omega, my1, my2;
+  zc k1, k2, eps1, eps2, eta1, eta2, eta_a;
+};
+
+// Device copy of everything the fill kernels need.
+struct FillArgs {
+  const FnD* fn;        // 2 per internal edge
+  const double* rref;   // per internal edge
+  const double* cent;   // 3 per triangle
+  Material mt;
+  Rule R;
+  int formulation;
+  int fix_itbn;
+};
+
+// Near-field matrix laid out per leaf box A: rows = edges of A (internal order),
+// columns = edges of the present boxes of E2(A) (self + neighbours, ascending
+// box index) -- a dense (|A| x |E2(A)|) panel of 2x2 complex blocks.
+struct NearLayout {
+  int nbox;
+  std::vector<int> box_first, box_cnt;   // leaf boxes in internal edge numbering
+  std::vector<int> nbr_ptr, nbr_box;     // E2 box lists per leaf box
+  std::vector<int> ncols;                // columns per leaf box
+  std::vector<long long> base;           // value offset of the panel of box A
+  long long nnz;
+};
+
+struct Level {
+  int l = 0;
+  int nb = 0;
+  std::vector<uint64_t> box;  // Morton indices, ascending
+  // device
+  zc* C = nullptr;            // nb x 8 x Q
+  zc* D = nullptr;            // nb x 8 x Q
+  zc* tl = nullptr;           // 343 x 2 x Q
+  zc* ph_up = nullptr;        // 8 octants x 2 media x Q  exp(+i k khat.(x_child - x_parent))
+  zc* ph_dn = nullptr;        // 8 octants x 2 media x Q  exp(-i k khat.(x_child - x_parent))
+  int* i4_ptr = nullptr;      // nb + 1
+  int* i4_src = nullptr;      // source box index (same level)
+  int* i4_off = nullptr;      // TL offset index 0..342
+  int* ch_ptr = nullptr;      // children (level l+1) per box: nb + 1
+  int* ch_idx = nullptr;
+  int* ch_oct = nullptr;
+  int* parent = nullptr;      // parent index (level l-1) per box, -1 if none
+  int* oct = nullptr;         // octant of the box in its parent
+  bool only_k1 = false;       // TL for k2 is zero at this level
+  long long n_i4 = 0;
+};
+
+struct Timings {
+  double fill_ms = 0, rt_ms = 0, tl_ms = 0, setup_ms = 0;
+  double mv_total_ms = 0, mv_near_ms = 0, mv_agg_ms = 0, mv_ss_ms = 0, mv_sr_ms = 0,
+         mv_rr_ms = 0, mv_recv_ms = 0;
+};
+
+}  // namespace sie
+
+struct sie_ctx {
+  sie_config cfg;
+  sie::Material mt;
+  sie::Rule R;
+  int device = 0;
+  cudaStream_t stream = nullptr, stream2 = nullptr;
+  cudaStream_t own_stream = nullptr;  // the library's stream when the caller set its own
+  cudaEvent_t ev[16];
+
+  // mesh (reference order)
+  int nv = 0, nt = 0, M = 0;
+  std::vector<double> verts;
+  std::vector<int> tris;
+  std::vector<int> elem, corner;  // 2 per edge (reference order)
+  std::vector<double> cent;       // 3 per triangle
+  std::vector<sie::FnD> fn_ext;   // 2 per edge, reference order
+  // tree
+  double D = 0, xmin[3] = {0, 0, 0};
+  int l_min = 0, l_max = 0;
+  std::vector<uint64_t> leaf;     // per edge (reference order)
+  std::vector<int> perm;          // internal -> reference edge index
+  std::vector<int> iperm;         // reference -> internal
+  sie::NearLayout near;
+  std::vector<sie::Level> lv;     // index = level
+  int K = 0, Q = 0;
+  bool setup_done = false;
+
+  // device arrays
+  sie::FnD* d_fn = nullptr;       // internal order
+  double* d_rref = nullptr;
+  double* d_cent = nullptr;
+  int* d_perm = nullptr;
+  int* d_box_first = nullptr;     // leaf boxes
+  int* d_box_cnt = nullptr;
+  int* d_nbr_ptr = nullptr;
+  int* d_nbr_box = nullptr;
+  int* d_ncols = nullptr;
+  long long* d_base = nullptr;
+  int* d_edge_box = nullptr;      // leaf box of each internal edge
+  // near values: ICTF / PMCHWT store (a, b, d), c = cfac * b
+  zc* d_na = nullptr;
+  zc* d_nb = nullptr;
+  zc* d_nd = nullptr;
+  cc* d_na32 = nullptr;
+  cc* d_nb32 = nullptr;
+  cc* d_nd32 = nullptr;
+  zc cfac;
+  zc* d_diag = nullptr;           // Jacobi diagonal, internal interleaved (J, M)
+  // far field
+  double* d_khat = nullptr;       // 3 x Q
+  double* d_tth = nullptr;
+  double* d_tph = nullptr;
+  double* d_trf = nullptr;
+  zc* d_rt = nullptr;             // internal edge x 4 x Q
+  cc* d_rt32 = nullptr;
+  // work vectors (internal layout, interleaved J/M per edge)
+  zc* d_xi = nullptr;
+  zc* d_yi = nullptr;
+  size_t work_rhs = 0;
+  // solver workspace
+  void* d_gm = nullptr;
+  size_t gm_bytes = 0;
+
+  sie::Timings tm;
+};
+
+// Functions shared between the translation units of the library.
+namespace sie {
+int near_fill(sie_ctx* c, int* d_tri_verts);
+int near_blocks_list(sie_ctx* c, int* d_tri_verts, const int* d_m, const int* d_n, int cnt,
+                     zc* d_out);
+int near_matvec64(sie_ctx* c, const zc* x, zc* y, int nrhs, bool accum, cudaStream_t st);
+int near_matvec32(sie_ctx* c, const cc* x, cc* y, int nrhs, bool accum, cudaStream_t st);
+int near_to_f32(sie_ctx* c);
+int far_build_tables(sie_ctx* c, const double* d_boxc);
+int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev);
+int far_prepare_kernels(sie_ctx* c);
+int gather_ext_to_int(sie_ctx* c, const zc* ext, zc* in, int nrhs, cudaStream_t st);
+int scatter_int_to_ext(sie_ctx* c, const zc* in, zc* ext, int nrhs, cudaStream_t st);
+int phase_tables(sie_ctx* c, Level& L, int l);
+int diag_extract(sie_ctx* c);
+int jacobi_apply(sie_ctx* c, const zc* v1, zc* v2, cudaStream_t st);
+int rhs_planewave_dev(sie_ctx* c, const double* d_k, const double* d_E, int nrhs, zc* d_b_int);
+int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
+                 double* d_I);
+int gmres_solve(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
+}  // namespace sie
+
+int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed);

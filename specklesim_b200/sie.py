@@ -1,0 +1,191 @@
+"""Python host side of the B200 SIE path: a thin object over the C-ABI.
+
+`Sie` owns one GPU context (one mesh, one material, one MLFMM set-up).  All
+compute goes through libsiegpu.so; nothing here evaluates the operator on the
+CPU.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import SieConfig, SieError, SieSolverCfg, SieStats, check, dptr, iptr, lptr
+
+FORMULATIONS = {"PMCHWT": _lib.SIE_PMCHWT, "ICTF": _lib.SIE_ICTF}
+PRECISIONS = {"fp64": _lib.SIE_FP64, "mixed": _lib.SIE_MIXED}
+
+
+def incidence(theta, phi, pol="TM", k_dir=2):
+    """k_in and E_in of kin_and_Ein_calculation (src/lib_sie_math.f90:259-293)."""
+    lib = _lib.load()
+    k = np.zeros(3)
+    e = np.zeros(3)
+    check(lib.sie_incidence(float(theta), float(phi), 1 if pol == "TM" else 2, int(k_dir), dptr(k), dptr(e)))
+    return k, e
+
+
+class Sie:
+    def __init__(self, verts, tris, wavelength, eps_r2, eps_r1=1.0, formulation="ICTF", ngp=3,
+                 tree_s_opt=250, truncation_number=19, normal_convention=2, fix_itbn=False,
+                 device=0, dense=False):
+        lib = _lib.load()
+        cfg = SieConfig()
+        lib.sie_config_default(C.byref(cfg))
+        cfg.lambda_ = float(wavelength)
+        e1, e2 = complex(eps_r1), complex(eps_r2)
+        cfg.eps_r1_re, cfg.eps_r1_im = e1.real, e1.imag
+        cfg.eps_r2_re, cfg.eps_r2_im = e2.real, e2.imag
+        cfg.formulation = FORMULATIONS[formulation] if isinstance(formulation, str) else int(formulation)
+        cfg.ngp = int(ngp)
+        cfg.tree_s_opt = int(tree_s_opt)
+        cfg.truncation_number = int(truncation_number)
+        cfg.normal_convention = int(normal_convention)
+        cfg.fix_itbn = int(bool(fix_itbn))
+        cfg.device = int(device)
+        cfg.dense = int(bool(dense))
+        self.cfg = cfg
+        v = np.ascontiguousarray(verts, dtype=np.float64)
+        t = np.ascontiguousarray(tris, dtype=np.int32)
+        self._h = C.c_void_p()
+        check(lib.sie_init(C.byref(cfg), dptr(v), v.shape[0], iptr(t), t.shape[0], C.byref(self._h)))
+        self._lib = lib
+        m, l0, l1, nnz = C.c_int(), C.c_int(), C.c_int(), C.c_longlong()
+        check(lib.sie_info(self._h, C.byref(m), C.byref(l0), C.byref(l1), C.byref(nnz)))
+        self.n_edges = m.value
+        self.l_min, self.l_max = l0.value, l1.value
+        self.near_nnz = nnz.value
+        self._setup = False
+
+    # --- set-up -----------------------------------------------------------
+    def setup(self):
+        if not self._setup:
+            check(self._lib.sie_setup(self._h))
+            self._setup = True
+        return self
+
+    @property
+    def n(self):
+        return 2 * self.n_edges
+
+    # --- operator -----------------------------------------------------------
+    def matvec(self, x, precision="fp64"):
+        x = _lib.as_c128(x)
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        xx = np.ascontiguousarray(x.reshape(self.n, nrhs).T)
+        y = np.zeros_like(xx)
+        check(self._lib.sie_matvec(self._h, dptr(xx.view(np.float64)), dptr(y.view(np.float64)), nrhs,
+                                   PRECISIONS[precision]))
+        y = y.T
+        return y[:, 0] if x.ndim == 1 else y
+
+    def matvec_device(self, d_x, d_y, nrhs=1, precision="fp64", stream=0):
+        """Device-pointer matvec (torch tensors' data_ptr() or raw addresses)."""
+        check(self._lib.sie_matvec_device(self._h, C.c_void_p(d_x), C.c_void_p(d_y), nrhs,
+                                          PRECISIONS[precision], C.c_void_p(stream)))
+
+    def rhs_planewave(self, k_in, E_in):
+        k = np.ascontiguousarray(np.atleast_2d(k_in), dtype=np.float64)
+        e = np.ascontiguousarray(np.atleast_2d(E_in), dtype=np.float64)
+        nrhs = k.shape[0]
+        b = np.zeros((nrhs, self.n), dtype=np.complex128)
+        check(self._lib.sie_rhs_planewave(self._h, dptr(k), dptr(e), nrhs, dptr(b.view(np.float64))))
+        return b[0] if np.ndim(k_in) == 1 else b.T
+
+    def solve(self, b, restart=50, max_iterations=650, tolerance=1e-6, x0=None, precision="fp64",
+              inner_restart=30, inner_tolerance=1e-4, time_limit_s=0.0, raise_on_noconv=True):
+        lib = self._lib
+        b = _lib.as_c128(b)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bb = np.ascontiguousarray(b.reshape(self.n, nrhs).T)
+        x = np.zeros_like(bb) if x0 is None else np.ascontiguousarray(_lib.as_c128(x0).reshape(self.n, nrhs).T)
+        cfg = SieSolverCfg()
+        lib.sie_solver_default(C.byref(cfg))
+        cfg.restart, cfg.max_iterations, cfg.tolerance = int(restart), int(max_iterations), float(tolerance)
+        cfg.use_initial_guess = int(x0 is not None)
+        cfg.precision = PRECISIONS[precision]
+        cfg.inner_restart, cfg.inner_tolerance = int(inner_restart), float(inner_tolerance)
+        cfg.time_limit_s = float(time_limit_s)
+        stats = (SieStats * nrhs)()
+        code = lib.sie_solve(self._h, dptr(bb.view(np.float64)), dptr(x.view(np.float64)), nrhs,
+                             C.byref(cfg), stats)
+        if code != _lib.SIE_OK and not (code == _lib.SIE_ERR_NOCONV and not raise_on_noconv):
+            check(code)
+        st = [{f: getattr(s, f) for f, _ in SieStats._fields_} for s in stats]
+        x = x.T
+        return (x[:, 0], st[0]) if b.ndim == 1 else (x, st)
+
+    def precondition_left(self, v1):
+        v1 = _lib.as_c128(v1)
+        v2 = np.zeros_like(v1)
+        check(self._lib.sie_precondition_left(self._h, dptr(v1.view(np.float64)), dptr(v2.view(np.float64))))
+        return v2
+
+    def farfield(self, x, pts):
+        x = _lib.as_c128(x)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        npts = p.shape[0]
+        E = np.zeros((npts, 3), np.complex128)
+        H = np.zeros((npts, 3), np.complex128)
+        I = np.zeros(npts)
+        check(self._lib.sie_farfield(self._h, dptr(x.view(np.float64)), dptr(p), npts,
+                                     dptr(E.view(np.float64)), dptr(H.view(np.float64)), dptr(I)))
+        return E, H, I
+
+    # --- introspection ------------------------------------------------------
+    def edges(self):
+        e = np.zeros(2 * self.n_edges, np.int32)
+        c = np.zeros(2 * self.n_edges, np.int32)
+        check(self._lib.sie_get_edges(self._h, iptr(e), iptr(c)))
+        return e.reshape(-1, 2), c.reshape(-1, 2)
+
+    def tree(self):
+        d = np.zeros(4)
+        leaf = np.zeros(self.n_edges, np.int64)
+        check(self._lib.sie_get_tree(self._h, dptr(d), lptr(leaf)))
+        return d[0], d[1:], leaf
+
+    def blocks(self, m, n):
+        m = np.ascontiguousarray(m, np.int32)
+        n = np.ascontiguousarray(n, np.int32)
+        out = np.zeros((len(m), 4), np.complex128)
+        check(self._lib.sie_get_blocks(self._h, iptr(m), iptr(n), len(m), dptr(out.view(np.float64))))
+        return out
+
+    def near_entries(self, m, n):
+        m = np.ascontiguousarray(m, np.int32)
+        n = np.ascontiguousarray(n, np.int32)
+        out = np.zeros((len(m), 4), np.complex128)
+        check(self._lib.sie_get_near_entries(self._h, iptr(m), iptr(n), len(m), dptr(out.view(np.float64))))
+        return out
+
+    def rt(self, edges):
+        e = np.ascontiguousarray(edges, np.int32)
+        q = C.c_int()
+        check(self._lib.sie_num_directions(self._h, C.byref(q)))
+        out = np.zeros((len(e), 4, q.value), np.complex128)
+        check(self._lib.sie_get_rt(self._h, iptr(e), len(e), dptr(out.view(np.float64))))
+        return out
+
+    def timings(self):
+        v = np.zeros(11)
+        check(self._lib.sie_get_timings(self._h, dptr(v), 11))
+        keys = ["fill_ms", "rt_tl_ms", "setup_ms", "mv_total_ms", "mv_near_ms", "mv_agg_ms",
+                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms"]
+        return dict(zip(keys, v[:10]))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sie_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -1,0 +1,63 @@
+"""Extract the reference's own known-answer vectors into small JSON fixtures.
+
+Run in a container that has the reference source tree (read as text only):
+    python tests/golden/make_golden.py /path/to/SpeckleSim
+Writes tests/golden/hankel2_x2.json and tests/golden/gmres_tridiag.json.
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def fnum(s):
+    return float(s.replace("_8", "").replace("d", "e").replace("D", "e"))
+
+
+def hankel(ref):
+    path = os.path.join(ref, "src/lib/libmath/src/math/lib_math_bessel.f90")
+    src = open(path).read().splitlines()
+    start = next(i for i, l in enumerate(src) if "function test_lib_math_bessel_spherical_third_kind_2_real" in l)
+    end = next(i for i in range(start + 1, len(src)) if "end function test_lib_math_bessel_spherical_third_kind_2_real" in src[i])
+    vals = {}
+    pat = re.compile(r"ground_truth_y\((\d+)\)\s*=\s*cmplx\(([^,]+),\s*([+-]?\s*[^,]+),\s*kind=8\)")
+    for i in range(start, end):
+        m = pat.search(src[i])
+        if m:
+            vals[int(m.group(1))] = (fnum(m.group(2).strip()), fnum(m.group(3).replace(" ", "")))
+    x = None
+    for i in range(start, end):
+        m = re.search(r"double precision :: x = ([0-9.]+)", src[i])
+        if m:
+            x = float(m.group(1))
+    n = max(vals)
+    return {
+        "source": f"src/lib/libmath/src/math/lib_math_bessel.f90:{start + 1}-{end + 1} "
+                  "(test_lib_math_bessel_spherical_third_kind_2_real; values from sageMath)",
+        "x": x, "orders": list(range(n)),
+        "re": [vals[i + 1][0] for i in range(n)], "im": [vals[i + 1][1] for i in range(n)],
+        "tolerance_log": 1e-13,
+    }
+
+
+def gmres(ref):
+    path = os.path.join(ref, "src/lib/libmath/src/math/lib_math_solver_GMRES.f90")
+    src = open(path).read()
+    assert "a(i,i) = dcmplx(4.d0, 0.d0)" in src and "dcmplx(-2.d0, 1.d0)" in src
+    line = src[: src.index("subroutine GMRES_test")].count("\n") + 1
+    return {
+        "source": f"src/lib/libmath/src/math/lib_math_solver_GMRES.f90:{line} (GMRES_test)",
+        "n": 100, "diag": [4.0, 0.0], "offdiag": [-2.0, 1.0], "restart": 60,
+        "solution": "all ones", "rhs": "A @ ones",
+    }
+
+
+if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    with open(os.path.join(HERE, "hankel2_x2.json"), "w") as f:
+        json.dump(hankel(ref), f, indent=1)
+    with open(os.path.join(HERE, "gmres_tridiag.json"), "w") as f:
+        json.dump(gmres(ref), f, indent=1)
+    print("ok")

@@ -1,0 +1,54 @@
+"""The C-ABI library loads and exports every entry point of include/sie_gpu.h (CPU)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "sie_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(sie_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_exports_match_header(gpu_lib):
+    from specklesim_b200 import _lib
+    names = header_functions()
+    assert set(names) == set(_lib.EXPORTS)
+    for n in names:
+        assert hasattr(gpu_lib, n), n
+
+
+def test_defaults_and_incidence(gpu_lib):
+    from specklesim_b200 import _lib
+    cfg = _lib.SieConfig()
+    gpu_lib.sie_config_default(C.byref(cfg))
+    assert cfg.formulation == _lib.SIE_ICTF and cfg.ngp == 3 and cfg.tree_s_opt == 250
+    assert cfg.truncation_number == 19
+    k = np.zeros(3)
+    e = np.zeros(3)
+    # theta = 0, phi = 0, TM, against z: k = (0,0,-1), E = (1,0,0) (main.f90:246-295)
+    assert gpu_lib.sie_incidence(0.0, 0.0, 1, 2, _lib.dptr(k), _lib.dptr(e)) == 0
+    assert np.allclose(k, [0, 0, -1]) and np.allclose(e, [1, 0, 0])
+    # the rotation of field_rotation_matrix keeps E transverse for k against z
+    assert gpu_lib.sie_incidence(0.3, 0.7, 2, 2, _lib.dptr(k), _lib.dptr(e)) == 0
+    assert abs(np.dot(k, e)) < 1e-15
+
+
+def test_argument_errors_without_device(gpu_lib):
+    from specklesim_b200 import _lib
+    cfg = _lib.SieConfig()
+    gpu_lib.sie_config_default(C.byref(cfg))
+    h = C.c_void_p()
+    v = np.zeros((3, 3))
+    t = np.array([[0, 1, 5]], np.int32)
+    # bad vertex index / too small mesh are rejected before any device work
+    assert gpu_lib.sie_init(C.byref(cfg), _lib.dptr(v), 3, _lib.iptr(t), 1, C.byref(h)) == _lib.SIE_ERR_ARG
+    cfg.ngp = 5
+    t2 = np.array([[0, 1, 2], [0, 2, 1]], np.int32)
+    assert gpu_lib.sie_init(C.byref(cfg), _lib.dptr(v), 3, _lib.iptr(t2), 2, C.byref(h)) == _lib.SIE_ERR_ARG
+    assert b"ngp" in gpu_lib.sie_last_error()
+    assert gpu_lib.sie_matvec(None, None, None, 1, 0) == _lib.SIE_ERR_ARG

@@ -1,0 +1,178 @@
+"""CUDA path vs the CPU oracle, through the C-ABI (needs a B200)."""
+import numpy as np
+import pytest
+
+from tests import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a - b)) / np.linalg.norm(np.ravel(b))
+
+
+@pytest.fixture(scope="module")
+def slab_pair(oracle_lib, gpu_lib):
+    from specklesim_b200 import Sie
+    V, T = P.slab(cells=16, length_wl=4.0, seed=3)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_DIELECTRIC, tree_s_opt=60, threads=8)
+    info = o.tree()
+    o.setup_fmm()
+    g = Sie(V, T, P.WL, P.EPS_DIELECTRIC, tree_s_opt=60).setup()
+    yield o, info, g
+    g.close()
+
+
+@pytest.fixture(scope="module")
+def metal_pair(oracle_lib, gpu_lib):
+    from specklesim_b200 import Sie
+    V, T = P.slab(cells=16, length_wl=4.0, seed=5)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, tree_s_opt=60, threads=8)
+    info = o.tree()
+    o.setup_fmm()
+    g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=60).setup()
+    yield o, info, g
+    g.close()
+
+
+def test_edges_and_tree_exact(slab_pair):
+    o, info, g = slab_pair
+    e1, c1 = o.edges()
+    e2, c2 = g.edges()
+    assert np.array_equal(e1, e2) and np.array_equal(c1, c2)
+    D, xmin, leaf = g.tree()
+    assert g.l_max == info["l_max"] and g.l_min == info["l_min"]
+    assert D == info["D"] and np.array_equal(xmin, info["xmin"])
+    assert np.array_equal(leaf, info["leaf"])
+    assert g.near_nnz == o.nnz
+
+
+def _pairs(o, rng, n=400):
+    m = rng.integers(0, o.M, n)
+    nn = rng.integers(0, o.M, n)
+    # self, edge-adjacent and close pairs exercise the singular branch
+    e, _ = o.edges()
+    m2 = np.arange(0, o.M, max(1, o.M // 100))
+    return np.concatenate([m, m2, m2]), np.concatenate([nn, m2, (m2 + 1) % o.M])
+
+
+@pytest.mark.parametrize("which", ["slab_pair", "metal_pair"])
+def test_blocks_match_oracle(which, request):
+    o, _, g = request.getfixturevalue(which)
+    rng = np.random.default_rng(0)
+    m, n = _pairs(o, rng)
+    a = g.blocks(m, n)
+    b = o.blocks(m, n)
+    scale = np.abs(b).max(axis=1, keepdims=True)
+    err = np.abs(a - b) / scale
+    assert err.max() < 1e-9, err.max()
+
+
+def test_near_matrix_matches_oracle_csr(slab_pair):
+    o, _, g = slab_pair
+    ia, ja, v = o.near_csr()
+    rows = np.arange(0, o.M, 13)
+    mm = np.concatenate([np.full(ia[r + 1] - ia[r], r) for r in rows])
+    nn = np.concatenate([ja[ia[r]:ia[r + 1]] for r in rows])
+    vv = np.concatenate([v[ia[r]:ia[r + 1]] for r in rows])
+    got = g.near_entries(mm, nn)
+    scale = np.abs(vv).max(axis=1, keepdims=True)
+    assert (np.abs(got - vv) / scale).max() < 1e-9
+
+
+def test_radiation_patterns_match_oracle(slab_pair):
+    o, _, g = slab_pair
+    edges = np.arange(0, o.M, 17)
+    a = g.rt(edges)
+    b = o.rt()[edges]
+    assert rel(a, b) < 1e-12
+
+
+@pytest.mark.parametrize("which", ["slab_pair", "metal_pair"])
+def test_matvec_matches_oracle(which, request):
+    o, _, g = request.getfixturevalue(which)
+    x = P.random_x(o.N, seed=4)
+    y_gpu = g.matvec(x)
+    y_orc = o.matvec(x)
+    assert rel(y_gpu, y_orc) < 1e-10
+
+
+def test_matvec_two_rhs_columns(slab_pair):
+    o, _, g = slab_pair
+    X = np.stack([P.random_x(o.N, seed=7), P.random_x(o.N, seed=8)], axis=1)
+    Y = g.matvec(X)
+    for j in range(2):
+        assert rel(Y[:, j], o.matvec(X[:, j])) < 1e-10
+
+
+def test_rhs_matches_oracle(slab_pair):
+    from specklesim_b200 import incidence
+    o, _, g = slab_pair
+    k, E = incidence(0.2, 0.5, "TE", 2)
+    b1 = g.rhs_planewave(k, E)
+    b2 = o.rhs(k, E)
+    assert rel(b1, b2) < 1e-13
+
+
+def test_solve_matches_oracle_gmres(metal_pair, oracle_lib):
+    """GPU GMRES (IMGS + Givens) against the zgmres restatement driving the oracle matvec."""
+    from specklesim_b200 import incidence
+    o, _, g = metal_pair
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b = o.rhs(k, E)
+    x_o, info = oracle_lib.zgmres(o.matvec, b, 30, 1e-6, 400)
+    x_g, st = g.solve(b, restart=30, max_iterations=400, tolerance=1e-6)
+    assert st["converged"] and info["converged"]
+    assert abs(st["iterations"] - info["iterations"]) <= 1
+    assert rel(x_g, x_o) < 1e-6
+    r = b - o.matvec(x_g)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-6
+
+
+def test_farfield_matches_oracle(slab_pair):
+    o, _, g = slab_pair
+    x = P.random_x(o.N, seed=9)
+    th = np.linspace(0.05, 1.4, 7)
+    pts = 5.0 * np.stack([np.sin(th), 0 * th, np.cos(th)], axis=1)
+    E1, H1, I1 = g.farfield(x, pts)
+    E2, H2, I2 = o.field(x, pts)
+    assert rel(E1, E2) < 1e-11 and rel(H1, H2) < 1e-11 and rel(I1, I2) < 1e-10
+
+
+def test_dense_mode_matches_oracle_dense(oracle_lib, gpu_lib):
+    from specklesim_b200 import Sie
+    V, T = P.sphere(1)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL)
+    Z = o.dense()
+    g = Sie(V, T, P.WL, P.EPS_METAL, dense=True).setup()
+    x = P.random_x(o.N, seed=3)
+    assert rel(g.matvec(x), Z @ x) < 1e-10
+    g.close()
+
+
+def test_error_paths(gpu_lib):
+    from specklesim_b200 import Sie, SieError
+    from specklesim_b200 import _lib
+    V, T = P.sphere(1)
+    g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=20)
+    with pytest.raises(SieError) as e:
+        g.matvec(np.ones(g.n, complex))  # before set-up
+    assert e.value.code == _lib.SIE_ERR_STATE
+    g.setup()
+    bad = np.ones(g.n, complex)
+    bad[3] = np.nan
+    with pytest.raises(SieError) as e:
+        g.matvec(bad)
+    assert e.value.code == _lib.SIE_ERR_NONFINITE
+    with pytest.raises(SieError) as e:
+        g.solve(np.ones(g.n, complex), restart=5, max_iterations=3, tolerance=1e-14)
+    assert e.value.code == _lib.SIE_ERR_NOCONV
+    x, st = g.solve(np.ones(g.n, complex), restart=5, max_iterations=3, tolerance=1e-14,
+                    raise_on_noconv=False)
+    assert not st["converged"] and st["iterations"] == 3
+    g.close()
+    T2 = T.copy()
+    T2[0, 0] = 10 ** 6
+    with pytest.raises(SieError) as e:
+        Sie(V, T2, P.WL, P.EPS_METAL)
+    assert e.value.code == _lib.SIE_ERR_MESH

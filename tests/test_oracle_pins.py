@@ -1,0 +1,61 @@
+"""The oracle pinned against the reference's own known-answer tests (CPU)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_hankel2_known_answers(oracle_lib):
+    """lib_math_bessel.f90: test_lib_math_bessel_spherical_third_kind_2_real (x = 2,
+    orders 0..40, |log(value) - log(truth)| <= 1e-13 for Re and Im)."""
+    g = json.load(open(os.path.join(GOLD, "hankel2_x2.json")))
+    h = oracle_lib.hankel2(g["x"], len(g["re"]))
+    re, im = np.array(g["re"]), np.array(g["im"])
+    # orders 0 (negative imaginary part) compared on the magnitude like the reference
+    assert np.all(np.abs(np.log(np.abs(h.real)) - np.log(np.abs(re))) <= 1e-13)
+    assert np.all(np.abs(np.log(np.abs(h.imag)) - np.log(np.abs(im))) <= 1e-13)
+    assert np.all(np.sign(h.real) == np.sign(re)) and np.all(np.sign(h.imag) == np.sign(im))
+
+
+@pytest.mark.parametrize("z", [3.7 + 0.0j, 12.0 + 0.0j, 25.3 + 0.0j, 5.0 - 0.3j, 9.0 - 1.0j])
+def test_hankel2_vs_scipy(oracle_lib, z):
+    from scipy.special import spherical_jn, spherical_yn
+    n = np.arange(19)
+    ref = spherical_jn(n, z) - 1j * spherical_yn(n, z)
+    h = oracle_lib.hankel2(z, 19)
+    assert np.allclose(h, ref, rtol=1e-11, atol=0)
+
+
+def test_hankel2_lossy_argument_is_accurate(oracle_lib):
+    """For k2 R with a large negative imaginary part, h2 = i^(n+1) e^{-iz}/z * poly(1/z)
+    is tiny; the upward recurrence keeps its relative accuracy (A&S 10.1.17)."""
+    from math import factorial
+    z = 3.0 - 40.0j
+    h = oracle_lib.hankel2(z, 12)
+    for n in range(12):
+        s = sum(factorial(n + k) / (factorial(k) * factorial(n - k)) / (2j * z) ** k for k in range(n + 1))
+        exact = 1j ** (n + 1) * np.exp(-1j * z) / z * s
+        assert abs(h[n] - exact) <= 1e-12 * abs(exact)
+
+
+@pytest.mark.parametrize("n", [3, 7, 19, 33])
+def test_gauss_legendre(oracle_lib, n):
+    x, w = oracle_lib.gauss_legendre(n)
+    xr, wr = np.polynomial.legendre.leggauss(n)
+    assert np.allclose(x, xr, atol=1e-14) and np.allclose(w, wr, atol=1e-14)
+
+
+def test_gmres_tridiagonal_all_ones(oracle_lib):
+    """lib_math_solver_GMRES.f90 GMRES_test: 100 x 100, diagonal 4, off-diagonals
+    -2+i, b = A * ones, restart 60; the solution is the all-ones vector."""
+    g = json.load(open(os.path.join(GOLD, "gmres_tridiag.json")))
+    n = g["n"]
+    A = np.diag(np.full(n, complex(*g["diag"]))) + np.diag(np.full(n - 1, complex(*g["offdiag"])), 1) \
+        + np.diag(np.full(n - 1, complex(*g["offdiag"])), -1)
+    b = A @ np.ones(n)
+    x, info = oracle_lib.zgmres(lambda v: A @ v, b, g["restart"], 1e-13, 1000)
+    assert info["converged"]
+    assert np.allclose(x, np.ones(n), atol=1e-9)

@@ -1,0 +1,164 @@
+"""The oracle's SIE pieces against the reference's own probes and against each
+other (CPU).  The reference ships no SIE golden vectors, so these are the pins."""
+import numpy as np
+import pytest
+
+from tests import problems as P
+
+A12 = [0.249286745170910, 0.249286745170910, 0.501426509658180, 0.063089014491500, 0.063089014491500,
+       0.873821971017000, 0.310352451033780, 0.636502499121400, 0.053145049844820, 0.636502499121400,
+       0.310352451033780, 0.053145049844820]
+B12 = [0.249286745170910, 0.501426509658180, 0.249286745170910, 0.063089014491500, 0.873821971017000,
+       0.063089014491500, 0.636502499121400, 0.053145049844820, 0.310352451033780, 0.310352451033780,
+       0.053145049844820, 0.636502499121400]
+W12 = [0.116786275726380] * 3 + [0.0508449063702100] * 3 + [0.0828510756183700] * 6
+
+
+@pytest.fixture(scope="module")
+def sph(oracle_lib):
+    V, T = P.sphere(2)
+    return oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, tree_s_opt=30)
+
+
+@pytest.mark.parametrize("m,tt,n,ll", [(0, 1, 11, 0), (5, 0, 40, 1), (17, 1, 90, 0)])
+@pytest.mark.parametrize("q", [-1, 1])
+def test_hanninen_vs_12pt_quadrature(sph, m, tt, n, ll, q):
+    """Mirrors test_K2q / test_K3q / test_K4q (lib_sie_tri_calculation_mod.f90:1121-1254):
+    analytic integrals vs a 12-point rule on a well-separated pair."""
+    h = sph.hanninen(m, tt, n, ll, 2, q)
+    fn = sph.fn(n, ll)
+    c, Ra = fn["c"], h["Ra"]
+    K2 = np.zeros(3); K3 = np.zeros(3); K4 = np.zeros(3); Is = 0.0
+    for a, b, w in zip(A12, B12, W12):
+        rq = (1 - a - b) * c[0] + a * c[1] + b * c[2]
+        rfn = 0.5 * (rq - c[2]) * fn["df"]
+        R = Ra - rq
+        Rl = np.linalg.norm(R)
+        wa = w * fn["area"]
+        K2 += Rl ** q * rfn * wa                         # K2q = int R^q f_n
+        K3 += q * Rl ** (q - 2) * R * wa                 # K3q = int grad' R^q  (sign: -grad)
+        K4 += -q * Rl ** (q - 2) * np.cross(R, rfn) * wa  # K4q = -(int grad R^q x f_n)
+        Is += Rl ** q * wa
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel(h["K2"], K2) < 1e-6
+    assert rel(h["K3"], -K3) < 1e-6
+    assert rel(h["K4"], K4) < 1e-6
+    assert abs(h["Is"] - Is) < 1e-6 * abs(Is)
+
+
+def test_edge_tables_follow_pair_scan(sph):
+    """find_neighbours (:865-905): pairs (i < j) in scan order; the corners are the
+    common vertices in the order of triangle i."""
+    elem, corner = sph.edges()
+    assert np.all(elem[:, 0] < elem[:, 1])
+    order = np.lexsort((elem[:, 1], elem[:, 0]))
+    assert np.array_equal(order, np.arange(len(elem)))
+    T = sph.t
+    for e in range(0, len(elem), 37):
+        ti = list(T[elem[e, 0]])
+        assert ti.index(corner[e, 0]) < ti.index(corner[e, 1])
+        assert corner[e, 0] in T[elem[e, 1]] and corner[e, 1] in T[elem[e, 1]]
+
+
+def test_self_block_symmetries(sph):
+    """ICTF: D21 = -eta_a^2 D12 for every block (both come from Kt1 + Kt2)."""
+    mat = sph.material()
+    m = np.arange(0, 400, 7)
+    n = (m * 13 + 5) % sph.M
+    B = sph.blocks(np.concatenate([m, m]), np.concatenate([n, m]))
+    scale = np.abs(B[:, 2]).max()
+    assert np.allclose(B[:, 2], -mat["eta_a"] ** 2 * B[:, 1], rtol=1e-12, atol=1e-12 * scale)
+    assert np.all(np.isfinite(B))
+
+
+@pytest.fixture(scope="module")
+def slab_fmm(oracle_lib):
+    V, T = P.slab(cells=16, length_wl=4.0, seed=3)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_DIELECTRIC, tree_s_opt=60, threads=8)
+    info = o.tree()
+    o.setup_fmm()
+    return o, info
+
+
+def test_tree_levels(slab_fmm):
+    o, info = slab_fmm
+    assert info["l_max"] >= 3 and info["l_min"] == 2
+    # every leaf box holds at most s_opt edges (definition of l_max)
+    _, cnt = np.unique(info["leaf"], return_counts=True)
+    assert cnt.max() <= 60
+
+
+def _demorton(n, l):
+    ix = iy = iz = 0
+    for b in range(l):
+        iz |= ((n >> (3 * b)) & 1) << b
+        iy |= ((n >> (3 * b + 1)) & 1) << b
+        ix |= ((n >> (3 * b + 2)) & 1) << b
+    return np.array([ix, iy, iz])
+
+
+def test_mlfmm_passes_match_pairwise_expansion(slab_fmm):
+    """The level-synchronous upward / SR / downward passes reproduce, for every far
+    pair, RT_m(x - x_A) * TRF * TL_l(x_A - x_B) * conj(RT_n)(x - x_B) evaluated
+    directly at the level l where box(n) is in I4(box(m)) (the only approximation
+    of lib_ml_fmm_run is that translation; SS/RR at constant K are exact shifts)."""
+    o, info = slab_fmm
+    mat = o.material()
+    kh, th, ph, w = o.sampling()
+    RT = o.rt()
+    L1, L0, D, xmin = info["l_max"], info["l_min"], info["D"], info["xmin"]
+    leaf = info["leaf"]
+    TL = {l: o.tl(l) for l in range(L0, L1 + 1)}
+    k = [mat["k1"], mat["k2"]]
+    centre = lambda n, l: (_demorton(n, l) + 0.5) * 2.0 ** -l * D + xmin
+    x = P.random_x(o.N, seed=1)
+    y = o.matvec(x)
+    ia, ja, v = o.near_csr()
+    MU0 = float(np.float32(1.2566370614e-6))
+    for m in [5, o.M // 3, o.M - 7]:
+        near = v[ia[m]:ia[m + 1]]
+        cols = ja[ia[m]:ia[m + 1]]
+        yJ = near[:, 0] @ x[cols] + near[:, 1] @ x[cols + o.M]
+        yM = near[:, 2] @ x[cols] + near[:, 3] @ x[cols + o.M]
+        colset = set(cols.tolist())
+        s1 = s2 = 0
+        for n in range(o.M):
+            if n in colset:
+                continue
+            # level of the interaction: the finest level where the boxes are not adjacent
+            for l in range(L1, L0 - 1, -1):
+                a, b = leaf[m] >> (3 * (L1 - l)), leaf[n] >> (3 * (L1 - l))
+                d = _demorton(a, l) - _demorton(b, l)
+                pa, pb = _demorton(a >> 3, l - 1), _demorton(b >> 3, l - 1)
+                if np.max(np.abs(d)) >= 2 and np.max(np.abs(pa - pb)) <= 1:
+                    break
+            t = (d[0] + 3) * 49 + (d[1] + 3) * 7 + (d[2] + 3)
+            xa, xb = centre(a, l), centre(b, l)
+            ca, cb = centre(leaf[m], L1), centre(leaf[n], L1)
+            for med in range(2):
+                tl = TL[l][t, med]
+                if not np.any(tl):
+                    continue
+                sh_m = np.exp(-1j * k[med] * (kh @ (ca - xa)))     # RR chain of the receiver
+                sh_n = np.exp(1j * k[med] * (kh @ (cb - xb)))      # SS chain of the source
+                fa, fb = RT[m, 2 * med] * sh_m, RT[m, 2 * med + 1] * sh_m
+                Dt = np.conj(RT[n, 2 * med]) * sh_n * w * tl
+                Dp = np.conj(RT[n, 2 * med + 1]) * sh_n * w * tl
+                xJ, xM = x[n], x[n + o.M]
+                kd = 1j * k[med]
+                myd = 1j * mat["omega"] * MU0
+                epsd = (mat["eps1"], mat["eps2"])[med] * 1j * mat["omega"]
+                s1 += myd * np.sum(fa * Dt + fb * Dp) * xJ + kd * np.sum(-fb * Dt + fa * Dp) * xM
+                s2 += kd * np.sum(fb * Dt - fa * Dp) * xJ + epsd * np.sum(fa * Dt + fb * Dp) * xM
+        yJ += s1 / mat["eta_a"]
+        yM += s2 * mat["eta_a"]
+        assert abs(yJ - y[m]) <= 1e-9 * abs(yJ)
+        assert abs(yM - y[m + o.M]) <= 1e-9 * abs(yM)
+
+
+def test_faithful_csr_lookup_equals_fast(slab_fmm):
+    """The O(row^2) lookup of find_elements_in_field_zcsr gives the same product."""
+    o, _ = slab_fmm
+    x = P.random_x(o.N, seed=2)
+    a, b = o.matvec(x), o.matvec(x, faithful_lookup=True)
+    assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(a)
