@@ -37,6 +37,11 @@ WORKLOADS = {
 }
 
 
+# matvecs of one budgeted FP64 solve on the GPU (650 Arnoldi steps + the final true
+# residual); the CPU arm times matvecs and multiplies by this count
+MATVECS_PER_SOLVE = {"slab10": 651, "slab4": 651}
+
+
 def peaks():
     try:
         d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -147,6 +152,7 @@ def main():
     ap.add_argument("--workload", default="slab10", choices=list(WORKLOADS))
     ap.add_argument("--restart", type=int, default=50)
     ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--max-iterations", type=int, default=650)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-matvecs-per-solve", type=int, default=0)
     args = ap.parse_args()
@@ -161,10 +167,7 @@ def main():
             return
         V, T = build_mesh(args.workload, 0)
         threads = os.cpu_count() or 1
-        mps = args.reference_matvecs_per_solve or 120
-        vals = []
-        for _ in range(max(1, args.warmup and 0) + args.steps if False else 1):
-            pass
+        mps = args.reference_matvecs_per_solve or MATVECS_PER_SOLVE[args.workload]
         cb = cpu_reference(V, T, mps, threads)
         line = {
             "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
@@ -208,17 +211,18 @@ def main():
     import ctypes as C
     cfg = _lib.SieSolverCfg()
     lib.sie_solver_default(C.byref(cfg))
-    cfg.restart, cfg.max_iterations, cfg.tolerance = args.restart, 650, args.tol
+    cfg.restart, cfg.max_iterations, cfg.tolerance = args.restart, args.max_iterations, args.tol
     st = _lib.SieStats()
 
     def solve_dev():
         rc = lib.sie_solve_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1, C.byref(cfg),
                                   C.byref(st))
-        _lib.check(rc)
+        if rc != _lib.SIE_ERR_NOCONV:  # the budgeted solve ends like the reference's info(1) = -4
+            _lib.check(rc)
 
     for _ in range(args.warmup):
         solve_dev()
-    iters, mvs = st.iterations, st.matvecs
+    iters, mvs, conv, be = st.iterations, st.matvecs, st.converged, st.backward_error_true
 
     def barrier():
         if world > 1:
@@ -252,8 +256,9 @@ def main():
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for _ in range(args.steps):
-        _lib.check(lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg),
-                                 stats))
+        rc = lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg), stats)
+        if rc != _lib.SIE_ERR_NOCONV:
+            _lib.check(rc)
     e3.record(stream)
     barrier()
     t_e2e = e2.elapsed_time(e3) / 1000.0
@@ -273,10 +278,6 @@ def main():
                                          C.c_void_p(stream.cuda_stream)))
     tm = g.timings()
     Q = 2 * 19 * 19 + 2
-    level_boxes, n_i4 = [], 0
-    for l in range(g.l_min, g.l_max + 1):
-        pass
-    info = getattr(g, "level_info", None)
     peak, peak_kind = peaks()
     phases = {k: tm[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
     dom = max(phases, key=phases.get)
@@ -312,7 +313,8 @@ def main():
                              f"lambda=632.8nm, eps=-11.7-1.26i (exp(+iwt)), seed=rank, {T.shape[0]} triangles, "
                              f"{g.n_edges} RWG edges, ICTF, ng=3, s_opt=250, K=19, l={g.l_min}..{g.l_max}"),
                 "precision": "fp64", "solver": f"GMRES(IMGS) restart {args.restart}, tol {args.tol}",
-                "iterations": iters, "matvecs_per_solve": mvs, "setup_s": setup_s,
+                "iterations": iters, "matvecs_per_solve": mvs, "converged": bool(conv),
+                "backward_error": be, "max_iterations": args.max_iterations, "setup_s": setup_s,
                 "near_nnz_blocks": nnz, "matvec_ms": tm["mv_total_ms"], "matvec_phases_ms": phases,
                 "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
                 "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
