@@ -184,29 +184,34 @@ __global__ void k_tl(double xmin, double dx, const zc* hk, zc k1, zc k2, int K, 
 // Upward pass step 1 (lib_sie_ml_fmm_get_C :395-448): C = sum conj(RT) x over
 // the edges of each leaf box.  Block per leaf box, threads over directions.
 template <typename T>
-__global__ void k_aggregate(const cx<T>* __restrict__ rt, const int* box_first, const int* box_cnt,
-                            int Q, const cx<T>* __restrict__ x, cx<T>* __restrict__ C) {
-  int b = blockIdx.x;
+__global__ void __launch_bounds__(128) k_aggregate(const cx<T>* __restrict__ rt,
+                                                   const int* box_first, const int* box_cnt,
+                                                   int Q, const cx<T>* __restrict__ x,
+                                                   cx<T>* __restrict__ C) {
+  int b = blockIdx.y;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
   int f = box_first[b], cnt = box_cnt[b];
-  for (int q = threadIdx.x; q < Q; q += blockDim.x) {
-    cx<T> acc[8];
-    for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
-    for (int e = f; e < f + cnt; e++) {
-      const cx<T>* r = rt + (size_t)e * 4 * Q;
-      cx<T> xe = x[2 * e], xh = x[2 * e + 1];
-      cx<T> ra1 = r[q], rb1 = r[Q + q], ra2 = r[2 * Q + q], rb2 = r[3 * Q + q];
-      acc[0] = cfma_conj(ra1, xe, acc[0]);
-      acc[1] = cfma_conj(ra2, xe, acc[1]);
-      acc[2] = cfma_conj(ra1, xh, acc[2]);
-      acc[3] = cfma_conj(ra2, xh, acc[3]);
-      acc[4] = cfma_conj(rb1, xe, acc[4]);
-      acc[5] = cfma_conj(rb2, xe, acc[5]);
-      acc[6] = cfma_conj(rb1, xh, acc[6]);
-      acc[7] = cfma_conj(rb2, xh, acc[7]);
-    }
-    cx<T>* o = C + (size_t)b * 8 * Q;
-    for (int i = 0; i < 8; i++) o[i * Q + q] = acc[i];
+  cx<T> acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+#pragma unroll 2
+  for (int e = f; e < f + cnt; e++) {
+    const cx<T>* r = rt + (size_t)e * 4 * Q;
+    cx<T> xe = x[2 * e], xh = x[2 * e + 1];
+    cx<T> ra1 = r[q], rb1 = r[Q + q], ra2 = r[2 * Q + q], rb2 = r[3 * Q + q];
+    acc[0] = cfma_conj(ra1, xe, acc[0]);
+    acc[1] = cfma_conj(ra2, xe, acc[1]);
+    acc[2] = cfma_conj(ra1, xh, acc[2]);
+    acc[3] = cfma_conj(ra2, xh, acc[3]);
+    acc[4] = cfma_conj(rb1, xe, acc[4]);
+    acc[5] = cfma_conj(rb2, xe, acc[5]);
+    acc[6] = cfma_conj(rb1, xh, acc[6]);
+    acc[7] = cfma_conj(rb2, xh, acc[7]);
   }
+  cx<T>* o = C + (size_t)b * 8 * Q;
+#pragma unroll
+  for (int i = 0; i < 8; i++) o[i * Q + q] = acc[i];
 }
 
 // Upward pass step 2 (translation_SS :466-528): parent C = sum over children
@@ -256,6 +261,153 @@ __global__ void k_sr(const cx<T>* __restrict__ C, const int* i4_ptr, const int* 
   for (int i = 0; i < 8; i++) out[i * Q + q] = acc[i];
 }
 
+// The same translation organised by sibling groups: the 8 children of one parent
+// P share the candidate sources, the (up to) 216 children of the 27 boxes around
+// P; a source is in I4 of sibling o exactly when their offset has a component of
+// magnitude >= 2.  Every source coefficient is read once per group instead of once
+// per target.  One thread per (group, direction); NI items of medium md per pass.
+template <typename T, int NI>
+__global__ void __launch_bounds__(128) k_sr_group(const cx<T>* __restrict__ C,
+                                                  const int* __restrict__ grp_sib,
+                                                  const int* __restrict__ grp_src,
+                                                  const cx<T>* __restrict__ tl,
+                                                  const T* __restrict__ trf, int Q, int md,
+                                                  int item0, int zero_other,
+                                                  cx<T>* __restrict__ D) {
+  __shared__ int s_sib[8];
+  __shared__ int s_src[216];
+  int g = blockIdx.y;
+  for (int i = threadIdx.x; i < 216; i += blockDim.x) s_src[i] = grp_src[(size_t)g * 216 + i];
+  if (threadIdx.x < 8) s_sib[threadIdx.x] = grp_sib[(size_t)g * 8 + threadIdx.x];
+  __syncthreads();
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  cx<T> acc[8][NI];
+#pragma unroll
+  for (int o = 0; o < 8; o++)
+#pragma unroll
+    for (int i = 0; i < NI; i++) acc[o][i] = mk<T>(0, 0);
+  const cx<T>* tlq = tl + (size_t)md * Q + q;  // + t * 2 * Q
+  for (int d = 0; d < 27; d++) {
+    int dx = d / 9 - 1, dy = (d / 3) % 3 - 1, dz = d % 3 - 1;
+    for (int c = 0; c < 8; c++) {
+      int s = s_src[d * 8 + c];
+      if (s < 0) continue;
+      const cx<T>* src = C + (size_t)s * 8 * Q + q;
+      cx<T> cs[NI];
+#pragma unroll
+      for (int i = 0; i < NI; i++) cs[i] = src[(size_t)(md + 2 * (item0 + i)) * Q];
+      int bx = (c >> 2) & 1, by = (c >> 1) & 1, bz = c & 1;
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        if (s_sib[o] < 0) continue;
+        int ox = ((o >> 2) & 1) - bx - 2 * dx;
+        int oy = ((o >> 1) & 1) - by - 2 * dy;
+        int oz = (o & 1) - bz - 2 * dz;
+        if (ox > -2 && ox < 2 && oy > -2 && oy < 2 && oz > -2 && oz < 2) continue;
+        int t = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+        cx<T> f = tlq[(size_t)t * 2 * Q];
+#pragma unroll
+        for (int i = 0; i < NI; i++) acc[o][i] = cfma(cs[i], f, acc[o][i]);
+      }
+    }
+  }
+  T w = trf[q];
+#pragma unroll
+  for (int o = 0; o < 8; o++) {
+    int b = s_sib[o];
+    if (b < 0) continue;
+    cx<T>* out = D + (size_t)b * 8 * Q + q;
+#pragma unroll
+    for (int i = 0; i < NI; i++) out[(size_t)(md + 2 * (item0 + i)) * Q] = acc[o][i] * w;
+    if (zero_other) {
+#pragma unroll
+      for (int i = 0; i < NI; i++) out[(size_t)((1 - md) + 2 * (item0 + i)) * Q] = mk<T>(0, 0);
+    }
+  }
+}
+
+// Sibling-group SR with the translation table of a tile of SR_TQ directions staged in
+// shared memory (343 offsets x SR_TQ), so each (source, sibling) pair costs one
+// shared-memory read of TL instead of an L2 read.  Block = SR_GB groups x SR_TQ
+// directions; all four items of medium md in one pass.
+#define SR_TQ 16
+#define SR_GB 8
+template <typename T>
+__global__ void __launch_bounds__(SR_TQ* SR_GB) k_sr_group_tl(
+    const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
+    int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
+    int zero_other, cx<T>* __restrict__ D) {
+  extern __shared__ unsigned char smraw[];
+  cx<T>* sTL = reinterpret_cast<cx<T>*>(smraw);                  // [343][SR_TQ]
+  int* s_src = reinterpret_cast<int*>(sTL + 343 * SR_TQ);         // [SR_GB][216]
+  int* s_sib = s_src + SR_GB * 216;                               // [SR_GB][8]
+  int q0 = blockIdx.x * SR_TQ;
+  int g0 = blockIdx.y * SR_GB;
+  int tid = threadIdx.x;
+  for (int i = tid; i < 343 * SR_TQ; i += blockDim.x) {
+    int t = i / SR_TQ, j = i - t * SR_TQ;
+    int q = q0 + j;
+    sTL[i] = (q < Q) ? tl[((size_t)t * 2 + md) * Q + q] : mk<T>(0, 0);
+  }
+  for (int i = tid; i < SR_GB * 216; i += blockDim.x) {
+    int g = g0 + i / 216;
+    s_src[i] = (g < ngrp) ? grp_src[(size_t)g * 216 + (i % 216)] : -1;
+  }
+  for (int i = tid; i < SR_GB * 8; i += blockDim.x) {
+    int g = g0 + i / 8;
+    s_sib[i] = (g < ngrp) ? grp_sib[(size_t)g * 8 + (i % 8)] : -1;
+  }
+  __syncthreads();
+  int gi = tid / SR_TQ, qi = tid - gi * SR_TQ;
+  int q = q0 + qi;
+  if (q >= Q || g0 + gi >= ngrp) return;
+  const int* src_l = s_src + gi * 216;
+  const int* sib_l = s_sib + gi * 8;
+  cx<T> acc[8][4];
+#pragma unroll
+  for (int o = 0; o < 8; o++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc[o][i] = mk<T>(0, 0);
+  for (int d = 0; d < 27; d++) {
+    int dx = d / 9 - 1, dy = (d / 3) % 3 - 1, dz = d % 3 - 1;
+    for (int c = 0; c < 8; c++) {
+      int s = src_l[d * 8 + c];
+      if (s < 0) continue;
+      const cx<T>* src = C + (size_t)s * 8 * Q + q;
+      cx<T> cs[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) cs[i] = src[(size_t)(md + 2 * i) * Q];
+      int bx = (c >> 2) & 1, by = (c >> 1) & 1, bz = c & 1;
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        if (sib_l[o] < 0) continue;
+        int ox = ((o >> 2) & 1) - bx - 2 * dx;
+        int oy = ((o >> 1) & 1) - by - 2 * dy;
+        int oz = (o & 1) - bz - 2 * dz;
+        if (ox > -2 && ox < 2 && oy > -2 && oy < 2 && oz > -2 && oz < 2) continue;
+        int t = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+        cx<T> f = sTL[t * SR_TQ + qi];
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[o][i] = cfma(cs[i], f, acc[o][i]);
+      }
+    }
+  }
+  T w = trf[q];
+#pragma unroll
+  for (int o = 0; o < 8; o++) {
+    int b = sib_l[o];
+    if (b < 0) continue;
+    cx<T>* out = D + (size_t)b * 8 * Q + q;
+#pragma unroll
+    for (int i = 0; i < 4; i++) out[(size_t)(md + 2 * i) * Q] = acc[o][i] * w;
+    if (zero_other) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) out[(size_t)((1 - md) + 2 * i) * Q] = mk<T>(0, 0);
+    }
+  }
+}
+
 // Downward pass step 2 (translation_RR :600-655): D += D_parent * exp(-i k khat.(x_child - x_parent)).
 template <typename T>
 __global__ void k_rr(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
@@ -301,7 +453,9 @@ __global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, co
     cx<T> S[2][4];
     for (int md = 0; md < 2; md++)
       for (int k = 0; k < 4; k++) S[md][k] = mk<T>(0, 0);
+#pragma unroll 3
     for (int q = lane; q < Q; q += 32) {
+#pragma unroll
       for (int md = 0; md < 2; md++) {
         cx<T> fa = r[(2 * md) * Q + q], fb = r[(2 * md + 1) * Q + q];
         cx<T> dJt = sD[(0 + md) * Q + q], dMt = sD[(2 + md) * Q + q];
@@ -386,7 +540,8 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
   // up 1
   {
     Level& L = c->lv[L1];
-    k_aggregate<T><<<L.nb, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    dim3 g((Q + 127) / 128, L.nb);
+    k_aggregate<T><<<g, 128, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[1], st);
@@ -403,10 +558,31 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
   // down 1
   for (int l = L0; l <= L1; l++) {
     Level& L = c->lv[l];
-    dim3 g((Q + thr - 1) / thr, L.nb);
-    k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
-                               (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
-                               (cx<T>*)L.D); sie::count_launch();
+    if (c->sr_mode == 0) {
+      dim3 g((Q + thr - 1) / thr, L.nb);
+      k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
+                                 (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
+                                 (cx<T>*)L.D); sie::count_launch();
+    } else if (c->sr_mode == 2) {
+      dim3 g((Q + SR_TQ - 1) / SR_TQ, (L.ngrp + SR_GB - 1) / SR_GB);
+      size_t smem = (size_t)343 * SR_TQ * sizeof(cx<T>) + (size_t)SR_GB * (216 + 8) * sizeof(int);
+      int nmed = L.only_k1 ? 1 : 2;
+      for (int md = 0; md < nmed; md++) {
+        k_sr_group_tl<T><<<g, SR_TQ * SR_GB, smem, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
+                                                          L.ngrp, (const cx<T>*)L.tl,
+                                                          (const T*)c->d_trf, Q, md, nmed == 1,
+                                                          (cx<T>*)L.D); sie::count_launch();
+      }
+    } else {
+      dim3 g((Q + thr - 1) / thr, L.ngrp);
+      int nmed = L.only_k1 ? 1 : 2;
+      for (int md = 0; md < nmed; md++)
+        for (int i0 = 0; i0 < 4; i0 += 2) {
+          k_sr_group<T, 2><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
+                                              (const cx<T>*)L.tl, (const T*)c->d_trf, Q, md, i0,
+                                              nmed == 1, (cx<T>*)L.D); sie::count_launch();
+        }
+    }
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[3], st);
@@ -461,6 +637,12 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)smem64));
   SIE_CUDA(cudaFuncSetAttribute(k_receive<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem32));
+  size_t sr64 = (size_t)343 * SR_TQ * sizeof(zc) + (size_t)SR_GB * (216 + 8) * sizeof(int);
+  size_t sr32 = (size_t)343 * SR_TQ * sizeof(cc) + (size_t)SR_GB * (216 + 8) * sizeof(int);
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_group_tl<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr64));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_group_tl<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr32));
   return SIE_OK;
 }
 

@@ -419,6 +419,29 @@ static int build_levels(sie_ctx* c) {
     SIE_TRY(upload(&L.i4_ptr, i4p));
     SIE_TRY(upload(&L.i4_src, i4s));
     SIE_TRY(upload(&L.i4_off, i4o));
+    // sibling groups: parents at level l-1 and the children of their 27 neighbours
+    {
+      std::vector<uint64_t> parents;
+      for (uint64_t n : L.box) parents.push_back(n >> 3);
+      parents.erase(std::unique(parents.begin(), parents.end()), parents.end());
+      std::vector<int> gs(parents.size() * 8, -1), gsrc(parents.size() * 216, -1);
+      int64_t ub = (l >= 1) ? (((int64_t)1 << (l - 1)) - 1) : 0;
+      for (size_t g = 0; g < parents.size(); g++) {
+        uint64_t P = parents[g];
+        for (int o = 0; o < 8; o++) gs[g * 8 + o] = index_of(L.box, (P << 3) | (uint64_t)o);
+        int64_t px, py, pz;
+        demorton3(P, l - 1, px, py, pz);
+        for (int d = 0; d < 27; d++) {
+          int64_t a = px + d / 9 - 1, b = py + (d / 3) % 3 - 1, cc = pz + d % 3 - 1;
+          if (l < 1 || a < 0 || b < 0 || cc < 0 || a > ub || b > ub || cc > ub) continue;
+          uint64_t Pn = morton3(a, b, cc, l - 1);
+          for (int ch = 0; ch < 8; ch++) gsrc[g * 216 + d * 8 + ch] = index_of(L.box, (Pn << 3) | (uint64_t)ch);
+        }
+      }
+      L.ngrp = (int)parents.size();
+      SIE_TRY(upload(&L.grp_sib, gs));
+      SIE_TRY(upload(&L.grp_src, gsrc));
+    }
     // children at l+1
     std::vector<int> chp(L.nb + 1, 0), chi, cho;
     if (l < c->l_max) {
@@ -693,6 +716,8 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (r != SIE_OK) return cleanup(r);
   // ICTF: D21 = -eta_a^2 D12 ; PMCHWT: D21 = -D12
   c->cfac = (cfg->formulation == SIE_ICTF) ? -(c->mt.eta_a * c->mt.eta_a) : mk<double>(-1.0, 0.0);
+  // kernel variant of the SR translation (tuning knob; both give the same sums)
+  if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(2, atoi(e)));
   *out = c;
   return SIE_OK;
 }
@@ -1090,7 +1115,7 @@ int sie_free(sie_ctx* c) {
     if (p) cudaFree(p);
   for (auto& L : c->lv) {
     void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.i4_ptr, L.i4_src, L.i4_off,
-                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct};
+                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src};
     for (void* p : lp)
       if (p) cudaFree(p);
   }

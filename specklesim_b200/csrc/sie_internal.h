@@ -100,6 +100,10 @@ struct Level {
   int* oct = nullptr;         // octant of the box in its parent
   bool only_k1 = false;       // TL for k2 is zero at this level
   long long n_i4 = 0;
+  // sibling groups (children of one parent at level l-1) for the SR translation
+  int ngrp = 0;
+  int* grp_sib = nullptr;     // ngrp x 8 box indices (-1: absent)
+  int* grp_src = nullptr;     // ngrp x 27 x 8 candidate source box indices (-1: absent)
 };
 
 struct Timings {
@@ -136,6 +140,9 @@ struct sie_ctx {
   std::vector<sie::Level> lv;     // index = level
   int K = 0, Q = 0;
   bool setup_done = false;
+  // SR kernel: 0 one thread per (target box, direction); 1 sibling groups;
+  // 2 sibling groups with the translation table staged in shared memory
+  int sr_mode = 2;
 
   // device arrays
   sie::FnD* d_fn = nullptr;       // internal order
