@@ -1,0 +1,220 @@
+! ISO_C_BINDING shim: the public procedures of the reference module
+! lib_sie_tri_mlfmm_interface (src/lib_sie_tri_mlfmm_interface.f90:18-26) with the
+! B200 library (include/sie_gpu.h) behind them.  Compile this file in place of the
+! reference module; lib_sie_solver_gmres_interface and main.f90 link unchanged, and
+! the GMRES driver keeps calling the same callbacks (lib_sie_solver_gmres_interface.f90:60-80).
+!
+! Module globals read here are the reference's own (lib_sie_data_container,
+! lib_sie_tri_data_container): struc_tri, m_pairs, illumination_p, eps_r1, eps_r2,
+! calc_p, pre_types, ng, tree_s_opt, truncation_number_default, x_initial,
+! simulation_data.  A non-zero status prints the library's message and stops, which is
+! how the reference reports errors.
+!
+! Not compiled in this repository's test-suite: the build image has no Fortran compiler.
+! The C entry points it binds are exercised through ctypes by tests/test_gpu_parity.py.
+
+module sie_gpu_c
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: SIE_OK = 0
+  integer(c_int), parameter :: SIE_ERR_NOCONV = 6
+  integer(c_int), parameter :: SIE_PMCHWT = 1
+  integer(c_int), parameter :: SIE_ICTF = 3
+  integer(c_int), parameter :: SIE_FP64 = 0
+
+  type, bind(C) :: sie_config
+    real(c_double) :: lambda
+    real(c_double) :: eps_r1_re, eps_r1_im
+    real(c_double) :: eps_r2_re, eps_r2_im
+    integer(c_int) :: formulation
+    integer(c_int) :: ngp
+    integer(c_int) :: tree_s_opt
+    integer(c_int) :: truncation_number
+    integer(c_int) :: normal_convention
+    integer(c_int) :: fix_itbn
+    integer(c_int) :: device
+    integer(c_int) :: dense
+  end type sie_config
+
+  interface
+    subroutine sie_config_default(cfg) bind(C, name="sie_config_default")
+      import :: sie_config
+      type(sie_config), intent(out) :: cfg
+    end subroutine
+    function sie_last_error() bind(C, name="sie_last_error") result(p)
+      import :: c_ptr
+      type(c_ptr) :: p
+    end function
+    function sie_init(cfg, verts, nv, tris, nt, ctx) bind(C, name="sie_init") result(rc)
+      import :: c_int, c_double, c_ptr, sie_config
+      type(sie_config), intent(in) :: cfg
+      real(c_double), intent(in) :: verts(*)
+      integer(c_int), value :: nv
+      integer(c_int), intent(in) :: tris(*)
+      integer(c_int), value :: nt
+      type(c_ptr), intent(out) :: ctx
+      integer(c_int) :: rc
+    end function
+    function sie_setup(ctx) bind(C, name="sie_setup") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int) :: rc
+    end function
+    function sie_matvec(ctx, x, y, nrhs, precision) bind(C, name="sie_matvec") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, x, y
+      integer(c_int), value :: nrhs, precision
+      integer(c_int) :: rc
+    end function
+    function sie_rhs_planewave(ctx, k_in, e_in, nrhs, b) bind(C, name="sie_rhs_planewave") result(rc)
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: k_in(3), e_in(3)
+      integer(c_int), value :: nrhs
+      type(c_ptr), value :: b
+      integer(c_int) :: rc
+    end function
+    function sie_precondition_left(ctx, v1, v2) bind(C, name="sie_precondition_left") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, v1, v2
+      integer(c_int) :: rc
+    end function
+    function sie_free(ctx) bind(C, name="sie_free") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int) :: rc
+    end function
+  end interface
+
+contains
+
+  subroutine sie_check(rc, what)
+    integer(c_int), intent(in) :: rc
+    character(len=*), intent(in) :: what
+    character(kind=c_char), pointer :: msg(:)
+    integer :: n
+    if (rc == SIE_OK) return
+    call c_f_pointer(sie_last_error(), msg, [1024])
+    n = 0
+    do while (n < 1024)
+      if (msg(n + 1) == c_null_char) exit
+      n = n + 1
+    end do
+    print *, 'B200 SIE library: ', what, ' failed (status ', rc, '): ', msg(1:n)
+    stop
+  end subroutine sie_check
+
+end module sie_gpu_c
+
+
+module lib_sie_tri_mlfmm_interface
+  use iso_c_binding
+  use sie_gpu_c
+  use lib_sie_data_container
+  use lib_sie_tri_data_container
+  implicit none
+  private
+
+  public :: lib_sie_ml_fmm_calculate_vector_b_tri
+  public :: lib_sie_ml_fmm_get_vector_b_tri
+  public :: lib_sie_ml_fmm_get_init_vector_x_tri
+  public :: lib_sie_ml_fmm_precalculation_tri
+  public :: lib_sie_ml_fmm_run_tri
+  public :: lib_sie_ml_fmm_save_vector_x_tri
+  public :: run_MLFMM_one_forward_tri
+  public :: lib_sie_ml_fmm_preconditioner_left
+
+  type(c_ptr), save :: m_ctx = c_null_ptr
+
+contains
+
+  ! lib_sie_ml_fmm_precalculation_tri (:59-92): mesh, tree, near field, RT, TL, diagonal.
+  subroutine lib_sie_ml_fmm_precalculation_tri()
+    type(sie_config) :: cfg
+    real(c_double), allocatable :: verts(:)
+    integer(c_int), allocatable :: tris(:)
+    integer :: i, nv, nt
+    nv = size(struc_tri%points)
+    nt = size(struc_tri%elements)
+    allocate(verts(3 * nv), tris(3 * nt))
+    do i = 1, nv
+      verts(3 * i - 2:3 * i) = struc_tri%points(i)%point
+    end do
+    do i = 1, nt
+      tris(3 * i - 2:3 * i) = struc_tri%elements(i)%corners(1:3) - 1
+    end do
+    call sie_config_default(cfg)
+    cfg%lambda = illumination_p%lambda
+    cfg%eps_r1_re = real(eps_r1, c_double)
+    cfg%eps_r1_im = aimag(eps_r1)
+    cfg%eps_r2_re = real(eps_r2, c_double)
+    cfg%eps_r2_im = aimag(eps_r2)
+    cfg%formulation = SIE_ICTF
+    if (pre_types%formulation == 'PMCHWT') cfg%formulation = SIE_PMCHWT
+    cfg%ngp = ng
+    cfg%tree_s_opt = tree_s_opt
+    cfg%truncation_number = truncation_number_default
+    cfg%normal_convention = calc_p(7)
+    if (c_associated(m_ctx)) call sie_check(sie_free(m_ctx), 'sie_free')
+    call sie_check(sie_init(cfg, verts, nv, tris, nt, m_ctx), 'sie_init')
+    call sie_check(sie_setup(m_ctx), 'sie_setup')
+  end subroutine lib_sie_ml_fmm_precalculation_tri
+
+  subroutine run_MLFMM_one_forward_tri()
+    call lib_sie_ml_fmm_precalculation_tri()
+    call lib_sie_ml_fmm_run_tri()
+  end subroutine run_MLFMM_one_forward_tri
+
+  ! lib_sie_ml_fmm_run_tri (:164-188): one forward product with the initial vector.
+  subroutine lib_sie_ml_fmm_run_tri()
+    double complex, dimension(:), allocatable :: x, b
+    call lib_sie_ml_fmm_get_init_vector_x_tri(x)
+    allocate(b(2 * m_pairs))
+    call lib_sie_ml_fmm_calculate_vector_b_tri(x, b)
+  end subroutine lib_sie_ml_fmm_run_tri
+
+  ! lib_sie_ml_fmm_get_init_vector_x_tri (:190-239), file branch disabled as in the reference.
+  subroutine lib_sie_ml_fmm_get_init_vector_x_tri(vector_x)
+    double complex, dimension(:), allocatable, intent(inout) :: vector_x
+    if (allocated(vector_x)) deallocate(vector_x)
+    allocate(vector_x(2 * m_pairs))
+    vector_x = x_initial
+  end subroutine lib_sie_ml_fmm_get_init_vector_x_tri
+
+  ! lib_sie_ml_fmm_save_vector_x_tri (:241-261)
+  subroutine lib_sie_ml_fmm_save_vector_x_tri(vector_x)
+    double complex, dimension(:), allocatable, intent(in) :: vector_x
+    double complex, dimension(:), allocatable :: buffer_x
+    allocate(buffer_x(size(vector_x)))
+    buffer_x = vector_x
+    call move_alloc(buffer_x, simulation_data%vector_x)
+  end subroutine lib_sie_ml_fmm_save_vector_x_tri
+
+  ! lib_sie_ml_fmm_get_vector_b_tri (:263-276): plane-wave right-hand side.
+  subroutine lib_sie_ml_fmm_get_vector_b_tri(vector_b)
+    double complex, dimension(:), allocatable, target, intent(inout) :: vector_b
+    if (allocated(vector_b)) deallocate(vector_b)
+    allocate(vector_b(2 * m_pairs))
+    call sie_check(sie_rhs_planewave(m_ctx, illumination_p%k_in, illumination_p%E_in, 1_c_int, &
+                                     c_loc(vector_b)), 'sie_rhs_planewave')
+  end subroutine lib_sie_ml_fmm_get_vector_b_tri
+
+  ! lib_sie_ml_fmm_calculate_vector_b_tri (:285-319): the GMRES matvec callback.
+  subroutine lib_sie_ml_fmm_calculate_vector_b_tri(vector_x, vector_b)
+    double complex, dimension(:), allocatable, target, intent(in) :: vector_x
+    double complex, dimension(:), allocatable, target, intent(inout) :: vector_b
+    call sie_check(sie_matvec(m_ctx, c_loc(vector_x), c_loc(vector_b), 1_c_int, SIE_FP64), &
+                   'sie_matvec')
+  end subroutine lib_sie_ml_fmm_calculate_vector_b_tri
+
+  ! lib_sie_ml_fmm_preconditioner_left (:323-339)
+  subroutine lib_sie_ml_fmm_preconditioner_left(vector_1, vector_2)
+    double complex, dimension(:), allocatable, target, intent(in) :: vector_1
+    double complex, dimension(:), allocatable, target, intent(out) :: vector_2
+    allocate(vector_2(size(vector_1)))
+    call sie_check(sie_precondition_left(m_ctx, c_loc(vector_1), c_loc(vector_2)), &
+                   'sie_precondition_left')
+  end subroutine lib_sie_ml_fmm_preconditioner_left
+
+end module lib_sie_tri_mlfmm_interface
