@@ -162,6 +162,24 @@ int sie_set_stream(sie_ctx* ctx, void* stream);
 /* Number of kernels this library has launched since it was loaded. */
 unsigned long long sie_launch_count(void);
 
+/* Largest mesh (RWG edges) sie_farfield_device_noalloc accepts. */
+#define SIE_NOALLOC_MAX_EDGES 131072
+
+/* sie_farfield on device buffers, allocating no device memory.  No counterpart
+ * in the reference (its field evaluation, Integration_scattered_field_tri in
+ * src/lib_sie_tri_calculation_mod.f90:2782-2825, runs on the host).
+ * d_x: 2M complex currents in the sie_farfield layout; d_pts: npts x 3;
+ * d_E, d_H: npts x 3 complex; d_I: npts (none may be NULL).  The work is queued
+ * on `stream` (NULL: the context's stream) and the call returns without waiting;
+ * the outputs are valid once that stream has reached it.
+ * Scratch: one library-wide device array of 2 x SIE_NOALLOC_MAX_EDGES complex
+ * values per GPU; meshes with more edges get SIE_ERR_ARG.  Calls that may run at
+ * the same time on one GPU (other streams, other threads, other contexts) share
+ * that array and race: order them on one stream.  The first call on each GPU
+ * looks the array up (cudaGetSymbolAddress); make it before any stream capture. */
+int sie_farfield_device_noalloc(sie_ctx* ctx, const double* d_x, const double* d_pts, int npts,
+                                double* d_E, double* d_H, double* d_I, void* stream);
+
 int sie_free(sie_ctx* ctx);
 
 #ifdef __cplusplus

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsiegpu.so")
 
 SIE_OK = 0
+SIE_NOALLOC_MAX_EDGES = 131072
 SIE_ERR_ARG = 1
 SIE_ERR_CUDA = 2
 SIE_ERR_STATE = 3
@@ -74,6 +75,7 @@ EXPORTS = [
     "sie_incidence", "sie_solve", "sie_solve_device", "sie_precondition_left", "sie_farfield",
     "sie_get_edges", "sie_get_tree", "sie_get_blocks", "sie_get_near_entries", "sie_get_rt",
     "sie_num_directions", "sie_get_timings", "sie_set_stream", "sie_launch_count", "sie_free",
+    "sie_farfield_device_noalloc",
 ]
 
 _lib = None
@@ -118,6 +120,7 @@ def load(path=None):
         "sie_set_stream": (C.c_int, [vp, vp]),
         "sie_launch_count": (C.c_ulonglong, []),
         "sie_free": (C.c_int, [vp]),
+        "sie_farfield_device_noalloc": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -131,6 +131,13 @@ class Sie:
                                      dptr(E.view(np.float64)), dptr(H.view(np.float64)), dptr(I)))
         return E, H, I
 
+    def farfield_device_noalloc(self, d_x, d_pts, npts, d_E, d_H, d_I, stream=0):
+        """Far field on device buffers (raw addresses) with no device allocation; the
+        work is queued on `stream` and not waited for."""
+        check(self._lib.sie_farfield_device_noalloc(
+            self._h, C.c_void_p(d_x), C.c_void_p(d_pts), int(npts), C.c_void_p(d_E),
+            C.c_void_p(d_H), C.c_void_p(d_I), C.c_void_p(stream)))
+
     # --- introspection ------------------------------------------------------
     def edges(self):
         e = np.zeros(2 * self.n_edges, np.int32)
