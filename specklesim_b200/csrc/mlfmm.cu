@@ -408,6 +408,113 @@ __global__ void __launch_bounds__(SR_TQ* SR_GB) k_sr_group_tl(
   }
 }
 
+// Sibling-group SR, one warp per group.  A warp covers SRW_QT directions x 2 item
+// halves of one sibling group, so every branch on the group's data is warp-uniform.
+// Per block: the TL tile of SRW_QT directions (343 offsets) and the offset table
+// (216 source slots x 8 siblings -> TL index, -1 inside the near zone) sit in shared
+// memory; each warp compacts its group's present sources into a list and streams the
+// two coefficients of its item half for the next source while it applies the current
+// one to the 8 siblings.
+#define SRW_QT 16
+#define SRW_GB 8
+template <typename T>
+__global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp(
+    const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
+    int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
+    int zero_other, cx<T>* __restrict__ D) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sTL = reinterpret_cast<cx<T>*>(smraw);                         // [343][SRW_QT]
+  short* s_tix = reinterpret_cast<short*>(sTL + 343 * SRW_QT);          // [216][8]
+  int* s_list = reinterpret_cast<int*>(s_tix + 216 * 8);                // [SRW_GB][216]
+  const int q0 = blockIdx.x * SRW_QT;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 343 * SRW_QT; i += blockDim.x) {
+    int t = i / SRW_QT, j = i - t * SRW_QT;
+    int q = q0 + j;
+    sTL[i] = (q < Q) ? tl[((size_t)t * 2 + md) * Q + q] : mk<T>(0, 0);
+  }
+  for (int i = tid; i < 216 * 8; i += blockDim.x) {
+    int dc = i >> 3, o = i & 7;
+    int d = dc >> 3, c = dc & 7;
+    int ox = ((o >> 2) & 1) - ((c >> 2) & 1) - 2 * (d / 9 - 1);
+    int oy = ((o >> 1) & 1) - ((c >> 1) & 1) - 2 * ((d / 3) % 3 - 1);
+    int oz = (o & 1) - (c & 1) - 2 * (d % 3 - 1);
+    bool nearz = ox > -2 && ox < 2 && oy > -2 && oy < 2 && oz > -2 && oz < 2;
+    s_tix[i] = nearz ? (short)-1 : (short)((ox + 3) * 49 + (oy + 3) * 7 + (oz + 3));
+  }
+  __syncthreads();
+  const int w = tid >> 5, lane = tid & 31;
+  const int g = blockIdx.y * SRW_GB + w;
+  if (g >= ngrp) return;
+  // sibling boxes (lanes 0..7) and their presence mask
+  int sib = (lane < 8) ? grp_sib[(size_t)g * 8 + lane] : -1;
+  const unsigned smask = __ballot_sync(0xffffffffu, sib >= 0) & 0xffu;
+  // compact list of present sources: (box << 8) | slot
+  int* lst = s_list + w * 216;
+  int cnt = 0;
+  for (int base = 0; base < 216; base += 32) {
+    int dc = base + lane;
+    int s = (dc < 216) ? grp_src[(size_t)g * 216 + dc] : -1;
+    unsigned bal = __ballot_sync(0xffffffffu, s >= 0);
+    if (s >= 0) lst[cnt + __popc(bal & ((1u << lane) - 1u))] = (s << 8) | dc;
+    cnt += __popc(bal);
+  }
+  __syncwarp();
+  const int ih = lane >> 4, qi = lane & 15;
+  const int q = q0 + qi;
+  const bool qok = q < Q;
+  const cx<T>* Cq = C + (qok ? q : 0);
+  const int it0 = md + 4 * ih, it1 = it0 + 2;
+  cx<T> acc[8][2];
+#pragma unroll
+  for (int o = 0; o < 8; o++) acc[o][0] = acc[o][1] = mk<T>(0, 0);
+  if (cnt > 0) {
+    int e = lst[0];
+    size_t sb = (size_t)(e >> 8) * 8;
+    cx<T> n0 = Cq[(sb + it0) * Q], n1 = Cq[(sb + it1) * Q];
+    for (int i = 0; i < cnt; i++) {
+      const cx<T> c0 = n0, c1 = n1;
+      const int dc = e & 255;
+      if (i + 1 < cnt) {
+        e = lst[i + 1];
+        sb = (size_t)(e >> 8) * 8;
+        n0 = Cq[(sb + it0) * Q];
+        n1 = Cq[(sb + it1) * Q];
+      }
+      const int4 tv = *reinterpret_cast<const int4*>(s_tix + dc * 8);
+      const int tw[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        int t = (o & 1) ? (tw[o >> 1] >> 16) : (int)(short)(tw[o >> 1] & 0xffff);
+        if (t >= 0 && ((smask >> o) & 1u)) {
+          cx<T> f = sTL[t * SRW_QT + qi];
+          acc[o][0] = cfma(c0, f, acc[o][0]);
+          acc[o][1] = cfma(c1, f, acc[o][1]);
+        }
+      }
+    }
+  }
+  const T wq = trf[qok ? q : 0];
+#pragma unroll
+  for (int o = 0; o < 8; o++) {
+    int b = __shfl_sync(0xffffffffu, sib, o);
+    if (b < 0 || !qok) continue;
+    cx<T>* out = D + (size_t)b * 8 * Q + q;
+    out[(size_t)it0 * Q] = acc[o][0] * wq;
+    out[(size_t)it1 * Q] = acc[o][1] * wq;
+    if (zero_other) {
+      out[(size_t)(it0 ^ 1) * Q] = mk<T>(0, 0);
+      out[(size_t)(it1 ^ 1) * Q] = mk<T>(0, 0);
+    }
+  }
+}
+
+template <typename T>
+static size_t sr_warp_smem() {
+  return (size_t)343 * SRW_QT * sizeof(cx<T>) + (size_t)216 * 8 * sizeof(short) +
+         (size_t)SRW_GB * 216 * sizeof(int);
+}
+
 // Downward pass step 2 (translation_RR :600-655): D += D_parent * exp(-i k khat.(x_child - x_parent)).
 template <typename T>
 __global__ void k_rr(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
@@ -563,6 +670,14 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
                                  (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
                                  (cx<T>*)L.D); sie::count_launch();
+    } else if (c->sr_mode == 3 && L.nb < (1 << 23)) {  // source box and slot share one int
+      dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
+      int nmed = L.only_k1 ? 1 : 2;
+      for (int md = 0; md < nmed; md++) {
+        k_sr_warp<T><<<g, 32 * SRW_GB, sr_warp_smem<T>(), st>>>(
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
+            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+      }
     } else if (c->sr_mode == 2) {
       dim3 g((Q + SR_TQ - 1) / SR_TQ, (L.ngrp + SR_GB - 1) / SR_GB);
       size_t smem = (size_t)343 * SR_TQ * sizeof(cx<T>) + (size_t)SR_GB * (216 + 8) * sizeof(int);
@@ -643,6 +758,10 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)sr64));
   SIE_CUDA(cudaFuncSetAttribute(k_sr_group_tl<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sr32));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_smem<double>()));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_smem<float>()));
   return SIE_OK;
 }
 

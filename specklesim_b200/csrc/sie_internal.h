@@ -141,8 +141,9 @@ struct sie_ctx {
   int K = 0, Q = 0;
   bool setup_done = false;
   // SR kernel: 0 one thread per (target box, direction); 1 sibling groups;
-  // 2 sibling groups with the translation table staged in shared memory
-  int sr_mode = 2;
+  // 2 sibling groups with the translation table staged in shared memory;
+  // 3 one warp per sibling group (compacted source lists, prefetched coefficients)
+  int sr_mode = 3;
 
   // device arrays
   sie::FnD* d_fn = nullptr;       // internal order
