@@ -75,6 +75,10 @@ SIE_HD cx<T> cfma_conj(cx<T> a, cx<T> b, cx<T> c) {
   return mk<T>(fma(a.re, b.re, fma(a.im, b.im, c.re)), fma(a.re, b.im, fma(-a.im, b.re, c.im)));
 }
 
+// widen to complex128
+SIE_HD zc cvt_z(zc a) { return a; }
+SIE_HD zc cvt_z(cc a) { return mk<double>((double)a.re, (double)a.im); }
+
 // exp(i * t) for real t
 SIE_HD zc cexpi(double t) {
   double s, c;

@@ -214,6 +214,49 @@ __global__ void __launch_bounds__(128) k_aggregate(const cx<T>* __restrict__ rt,
   for (int i = 0; i < 8; i++) o[i * Q + q] = acc[i];
 }
 
+// Same sum with a block per (leaf box, 32 directions): the 8 warps take every 8th edge
+// of the box, so each box's radiation patterns stream through 8 independent load
+// chains; the partial sums meet in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) k_aggregate_eg(const cx<T>* __restrict__ rt,
+                                                      const int* box_first, const int* box_cnt,
+                                                      int Q, const cx<T>* __restrict__ x,
+                                                      cx<T>* __restrict__ C) {
+  __shared__ cx<T> red[8][8][33];
+  const int b = blockIdx.y;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = blockIdx.x * 32 + lane;
+  const bool qok = q < Q;
+  const int f = box_first[b], cnt = box_cnt[b];
+  cx<T> acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  if (qok) {
+#pragma unroll 2
+    for (int e = f + w; e < f + cnt; e += 8) {
+      const cx<T>* r = rt + (size_t)e * 4 * Q + q;
+      cx<T> xe = x[2 * e], xh = x[2 * e + 1];
+      cx<T> ra1 = r[0], rb1 = r[Q], ra2 = r[2 * Q], rb2 = r[3 * Q];
+      acc[0] = cfma_conj(ra1, xe, acc[0]);
+      acc[1] = cfma_conj(ra2, xe, acc[1]);
+      acc[2] = cfma_conj(ra1, xh, acc[2]);
+      acc[3] = cfma_conj(ra2, xh, acc[3]);
+      acc[4] = cfma_conj(rb1, xe, acc[4]);
+      acc[5] = cfma_conj(rb2, xe, acc[5]);
+      acc[6] = cfma_conj(rb1, xh, acc[6]);
+      acc[7] = cfma_conj(rb2, xh, acc[7]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) red[w][i][lane] = acc[i];
+  __syncthreads();
+  // warp w now owns item w
+  cx<T> s = red[0][w][lane];
+#pragma unroll
+  for (int k = 1; k < 8; k++) s += red[k][w][lane];
+  if (qok) C[((size_t)b * 8 + w) * Q + q] = s;
+}
+
 // Upward pass step 2 (translation_SS :466-528): parent C = sum over children
 // of C_child * exp(+i k khat.(x_child - x_parent)).  nmed = 1 skips medium 2.
 template <typename T>
@@ -599,6 +642,89 @@ __global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, co
   }
 }
 
+// Receive over work chunks of at most 32 edges of one leaf box.  The eight D items of
+// the box are first folded, per medium, into the four vectors the two outputs need:
+//   s1 = sum_q fa (my D_Jt + kd D_Mp) + fb (my D_Jp - kd D_Mt)
+//   s2 = sum_q fa (eps D_Mt - kd D_Jp) + fb (kd D_Jt + eps D_Mp)
+// (the same sums as k_receive, regrouped), scaled by the formulation factors.  Each warp
+// then streams the radiation patterns of two edges at a time against them.
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_receive_chunk(const cx<T>* __restrict__ rt,
+                                                          const int4* __restrict__ chunks,
+                                                          const cx<T>* __restrict__ D, int Q,
+                                                          RecvConst rc, cx<T>* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sU = reinterpret_cast<cx<T>*>(smraw);  // [md][A1, B1, A2, B2][Q]
+  const int4 ch = chunks[blockIdx.x];
+  const int b = ch.x, f = ch.y, cnt = ch.z;
+  const cx<T>* Db = D + (size_t)b * 8 * Q;
+  for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+#pragma unroll
+    for (int md = 0; md < 2; md++) {
+      zc dJt = cvt_z(Db[(0 + md) * Q + q]), dMt = cvt_z(Db[(2 + md) * Q + q]);
+      zc dJp = cvt_z(Db[(4 + md) * Q + q]), dMp = cvt_z(Db[(6 + md) * Q + q]);
+      zc A1 = (rc.my_d[md] * dJt + rc.kd[md] * dMp) * rc.s1f;
+      zc B1 = (rc.my_d[md] * dJp - rc.kd[md] * dMt) * rc.s1f;
+      zc A2 = (rc.eps_d[md] * dMt - rc.kd[md] * dJp) * rc.s2f;
+      zc B2 = (rc.kd[md] * dJt + rc.eps_d[md] * dMp) * rc.s2f;
+      cx<T>* u = sU + (size_t)md * 4 * Q + q;
+      u[0] = mk<T>((T)A1.re, (T)A1.im);
+      u[Q] = mk<T>((T)B1.re, (T)B1.im);
+      u[2 * Q] = mk<T>((T)A2.re, (T)A2.im);
+      u[3 * Q] = mk<T>((T)B2.re, (T)B2.im);
+    }
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e0 = f + 2 * warp; e0 < f + cnt; e0 += 16) {
+    const bool two = e0 + 1 < f + cnt;
+    const cx<T>* r0 = rt + (size_t)e0 * 4 * Q;
+    const cx<T>* r1 = two ? r0 + 4 * Q : r0;
+    cx<T> s[2][2];
+    s[0][0] = s[0][1] = s[1][0] = s[1][1] = mk<T>(0, 0);
+#pragma unroll 2
+    for (int q = lane; q < Q; q += 32) {
+      cx<T> u[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) u[k] = sU[k * Q + q];
+      cx<T> a0[4], a1[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        a0[k] = r0[k * Q + q];
+        a1[k] = r1[k * Q + q];
+      }
+#pragma unroll
+      for (int md = 0; md < 2; md++) {
+        // rows of RT: 2 md = theta (fa), 2 md + 1 = phi (fb)
+        s[0][0] = cfma(a0[2 * md], u[4 * md + 0], s[0][0]);
+        s[0][0] = cfma(a0[2 * md + 1], u[4 * md + 1], s[0][0]);
+        s[0][1] = cfma(a0[2 * md], u[4 * md + 2], s[0][1]);
+        s[0][1] = cfma(a0[2 * md + 1], u[4 * md + 3], s[0][1]);
+        s[1][0] = cfma(a1[2 * md], u[4 * md + 0], s[1][0]);
+        s[1][0] = cfma(a1[2 * md + 1], u[4 * md + 1], s[1][0]);
+        s[1][1] = cfma(a1[2 * md], u[4 * md + 2], s[1][1]);
+        s[1][1] = cfma(a1[2 * md + 1], u[4 * md + 3], s[1][1]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int k = 0; k < 2; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          s[j][k].re += __shfl_xor_sync(0xffffffffu, s[j][k].re, o);
+          s[j][k].im += __shfl_xor_sync(0xffffffffu, s[j][k].im, o);
+        }
+    if (lane < 4) {
+      int j = lane >> 1, k = lane & 1;
+      if (j == 0 || two) {
+        cx<T> v = (j == 0) ? (k == 0 ? s[0][0] : s[0][1]) : (k == 0 ? s[1][0] : s[1][1]);
+        y[2 * (e0 + j) + k] += v;
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void k_zero(cx<T>* p, size_t n) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -647,8 +773,13 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
   // up 1
   {
     Level& L = c->lv[L1];
-    dim3 g((Q + 127) / 128, L.nb);
-    k_aggregate<T><<<g, 128, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    if (c->agg_mode == 1) {
+      dim3 g((Q + 31) / 32, L.nb);
+      k_aggregate_eg<T><<<g, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    } else {
+      dim3 g((Q + 127) / 128, L.nb);
+      k_aggregate<T><<<g, 128, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    }
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[1], st);
@@ -733,8 +864,13 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       rc.s2f = mk<double>(1, 0);
     }
     size_t smem = (size_t)8 * Q * sizeof(cx<T>);
-    k_receive<T><<<L.nb, 256, smem, st>>>(rt, c->d_box_first, c->d_box_cnt, (const cx<T>*)L.D, Q,
-                                          rc, y); sie::count_launch();
+    if (c->recv_mode == 1) {
+      k_receive_chunk<T><<<c->n_rchunk, 256, smem, st>>>(rt, (const int4*)c->d_rchunk,
+                                                         (const cx<T>*)L.D, Q, rc, y); sie::count_launch();
+    } else {
+      k_receive<T><<<L.nb, 256, smem, st>>>(rt, c->d_box_first, c->d_box_cnt, (const cx<T>*)L.D, Q,
+                                            rc, y); sie::count_launch();
+    }
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[5], st);
@@ -751,6 +887,10 @@ int far_prepare_kernels(sie_ctx* c) {
   SIE_CUDA(cudaFuncSetAttribute(k_receive<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem64));
   SIE_CUDA(cudaFuncSetAttribute(k_receive<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem32));
+  SIE_CUDA(cudaFuncSetAttribute(k_receive_chunk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem64));
+  SIE_CUDA(cudaFuncSetAttribute(k_receive_chunk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem32));
   size_t sr64 = (size_t)343 * SR_TQ * sizeof(zc) + (size_t)SR_GB * (216 + 8) * sizeof(int);
   size_t sr32 = (size_t)343 * SR_TQ * sizeof(cc) + (size_t)SR_GB * (216 + 8) * sizeof(int);

@@ -718,6 +718,8 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   c->cfac = (cfg->formulation == SIE_ICTF) ? -(c->mt.eta_a * c->mt.eta_a) : mk<double>(-1.0, 0.0);
   // kernel variant of the SR translation (tuning knob; both give the same sums)
   if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(3, atoi(e)));
+  if (const char* e = getenv("SIE_RECV_MODE")) c->recv_mode = std::max(0, std::min(1, atoi(e)));
+  if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
   *out = c;
   return SIE_OK;
 }
@@ -793,6 +795,19 @@ int sie_setup(sie_ctx* c) {
     double* d_boxc = nullptr;
     SIE_TRY(upload(&d_boxc, boxc));
     SIE_CUDA(cudaMalloc(&c->d_rt, (size_t)M * 4 * Q * sizeof(zc)));
+    {
+      // receive work units: at most 32 edges of one leaf box
+      std::vector<int> ch;
+      for (int b = 0; b < c->near.nbox; b++)
+        for (int k = 0; k < c->near.box_cnt[b]; k += 32) {
+          ch.push_back(b);
+          ch.push_back(c->near.box_first[b] + k);
+          ch.push_back(std::min(32, c->near.box_cnt[b] - k));
+          ch.push_back(0);
+        }
+      c->n_rchunk = (int)(ch.size() / 4);
+      SIE_TRY(upload(&c->d_rchunk, ch));
+    }
     for (int l = c->l_min; l <= c->l_max; l++) {
       Level& L = c->lv[l];
       SIE_CUDA(cudaMalloc(&L.C, (size_t)L.nb * 8 * Q * sizeof(zc)));
@@ -1108,7 +1123,7 @@ int sie_free(sie_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
-                  c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_na,
+                  c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_xi, c->d_yi, c->d_gm};
   for (void* p : ptrs)

@@ -144,6 +144,10 @@ struct sie_ctx {
   // 2 sibling groups with the translation table staged in shared memory;
   // 3 one warp per sibling group (compacted source lists, prefetched coefficients)
   int sr_mode = 3;
+  // receive: 0 one block per leaf box; 1 chunks of <= 32 edges with pre-combined D
+  int recv_mode = 1;
+  // aggregate: 0 one thread per (box, direction); 1 eight edge groups per block
+  int agg_mode = 1;
 
   // device arrays
   sie::FnD* d_fn = nullptr;       // internal order
@@ -157,6 +161,8 @@ struct sie_ctx {
   int* d_ncols = nullptr;
   long long* d_base = nullptr;
   int* d_edge_box = nullptr;      // leaf box of each internal edge
+  int* d_rchunk = nullptr;        // receive chunks: (box, first edge, count, 0) per chunk
+  int n_rchunk = 0;
   // near values: ICTF / PMCHWT store (a, b, d), c = cfac * b
   zc* d_na = nullptr;
   zc* d_nb = nullptr;
