@@ -560,8 +560,95 @@ __global__ void __launch_bounds__(256) k_near_spmv(PanelArgs P, const cx<T>* __r
   }
 }
 
+// Near product over work chunks of at most 32 rows of one leaf box A.  All rows of A
+// share the panel's columns, so the chunk first gathers x of those columns into shared
+// memory (J, M per column) and then streams the a, b, d rows against it: every lane
+// walks the whole concatenated column range, with no partial warps at box seams.
+template <typename T, bool ACCUM>
+__global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __restrict__ va,
+                                                    const cx<T>* __restrict__ vb,
+                                                    const cx<T>* __restrict__ vd_,
+                                                    const int4* __restrict__ chunks, int M,
+                                                    cx<T> cfac, const cx<T>* __restrict__ x,
+                                                    cx<T>* __restrict__ y, int nrhs) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [ncols][J, M]
+  const int4 ch = chunks[blockIdx.x];
+  const int A = ch.x, f = ch.y, cnt = ch.z;
+  const int nc = P.ncols[A];
+  const long long base = P.base[A] + (long long)(f - P.box_first[A]) * nc;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k0 = P.nbr_ptr[A], k1 = P.nbr_ptr[A + 1];
+  for (int r = 0; r < nrhs; r++) {
+    const cx<T>* xr = x + (size_t)r * 2 * M;
+    if (r > 0) __syncthreads();
+    int col0 = 0;
+    for (int k = k0; k < k1; k++) {
+      const int B = P.nbr_box[k];
+      const int c = P.box_cnt[B], fb = P.box_first[B];
+      for (int j = threadIdx.x; j < 2 * c; j += blockDim.x) xs[2 * col0 + j] = xr[2 * fb + j];
+      col0 += c;
+    }
+    __syncthreads();
+    for (int row = warp; row < cnt; row += 8) {
+      const long long o = base + (long long)row * nc;
+      cx<T> sJ = mk<T>(0, 0), sM = mk<T>(0, 0), tM = mk<T>(0, 0);
+#pragma unroll 4
+      for (int j = lane; j < nc; j += 32) {
+        cx<T> a = va[o + j], b = vb[o + j], d = vd_[o + j];
+        cx<T> xj = xs[2 * j], xm = xs[2 * j + 1];
+        sJ = cfma(a, xj, sJ);
+        sJ = cfma(b, xm, sJ);
+        tM = cfma(b, xj, tM);
+        sM = cfma(d, xm, sM);
+      }
+      sM = cfma(cfac, tM, sM);
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) {
+        sJ.re += __shfl_xor_sync(0xffffffffu, sJ.re, s);
+        sJ.im += __shfl_xor_sync(0xffffffffu, sJ.im, s);
+        sM.re += __shfl_xor_sync(0xffffffffu, sM.re, s);
+        sM.im += __shfl_xor_sync(0xffffffffu, sM.im, s);
+      }
+      if (lane == 0) {
+        cx<T>* yr = y + (size_t)r * 2 * M + 2 * (f + row);
+        if (ACCUM) {
+          yr[0] += sJ;
+          yr[1] += sM;
+        } else {
+          yr[0] = sJ;
+          yr[1] = sM;
+        }
+      }
+    }
+  }
+}
+
 // -------------------------------------------------------------------------
 // host wrappers
+
+// Shared memory the chunked near product needs; 0 if the widest panel does not fit.
+template <typename T>
+static size_t near_panel_smem(const sie_ctx* c) {
+  size_t s = (size_t)c->ncols_max * 2 * sizeof(cx<T>);
+  return s <= (size_t)200 * 1024 ? std::max<size_t>(s, 16) : 0;
+}
+
+int near_prepare_kernels(sie_ctx* c) {
+  if (size_t s = near_panel_smem<double>(c)) {
+    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<double, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<double, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+  }
+  if (size_t s = near_panel_smem<float>(c)) {
+    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<float, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<float, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+  }
+  return SIE_OK;
+}
 
 PanelArgs panel_args(sie_ctx* c) {
   PanelArgs P;
@@ -656,6 +743,17 @@ template <typename T>
 int near_matvec_t(sie_ctx* c, const cx<T>* va, const cx<T>* vb, const cx<T>* vdd, cx<T> cfac,
                   const cx<T>* x, cx<T>* y, int nrhs, bool accum, cudaStream_t st) {
   PanelArgs P = panel_args(c);
+  size_t smem = near_panel_smem<T>(c);
+  if (c->near_mode == 1 && smem && c->n_rchunk > 0) {
+    const int4* ch = (const int4*)c->d_rchunk;
+    if (accum) {
+      k_near_panel<T, true><<<c->n_rchunk, 256, smem, st>>>(P, va, vb, vdd, ch, c->M, cfac, x, y, nrhs); sie::count_launch();
+    } else {
+      k_near_panel<T, false><<<c->n_rchunk, 256, smem, st>>>(P, va, vb, vdd, ch, c->M, cfac, x, y, nrhs); sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+    return SIE_OK;
+  }
   long long threads = (long long)c->M * 32;
   unsigned g = (unsigned)((threads + 255) / 256);
   if (accum) {

@@ -720,6 +720,7 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(3, atoi(e)));
   if (const char* e = getenv("SIE_RECV_MODE")) c->recv_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
+  if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));
   *out = c;
   return SIE_OK;
 }
@@ -767,6 +768,22 @@ int sie_setup(sie_ctx* c) {
   SIE_TRY(upload(&c->d_edge_box, ebox));
   SIE_TRY(upload(&c->d_box_first, c->near.box_first));
   SIE_TRY(upload(&c->d_box_cnt, c->near.box_cnt));
+  {
+    // work units of the near-panel product and of the far-field receive: at most 32
+    // edges (rows) of one leaf box
+    std::vector<int> ch;
+    for (int b = 0; b < c->near.nbox; b++)
+      for (int k = 0; k < c->near.box_cnt[b]; k += 32) {
+        ch.push_back(b);
+        ch.push_back(c->near.box_first[b] + k);
+        ch.push_back(std::min(32, c->near.box_cnt[b] - k));
+        ch.push_back(0);
+      }
+    c->n_rchunk = (int)(ch.size() / 4);
+    SIE_TRY(upload(&c->d_rchunk, ch));
+    c->ncols_max = 0;
+    for (int b = 0; b < c->near.nbox; b++) c->ncols_max = std::max(c->ncols_max, c->near.ncols[b]);
+  }
   SIE_TRY(upload(&c->d_nbr_ptr, c->near.nbr_ptr));
   SIE_TRY(upload(&c->d_nbr_box, c->near.nbr_box));
   SIE_TRY(upload(&c->d_ncols, c->near.ncols));
@@ -783,6 +800,7 @@ int sie_setup(sie_ctx* c) {
   cudaEventRecord(c->ev[9], c->stream);
   cudaFree(d_tv);
   if (r != SIE_OK) return r;
+  SIE_TRY(near_prepare_kernels(c));
   SIE_TRY(diag_extract(c));
   // far field
   if (!c->cfg.dense) {
@@ -795,19 +813,6 @@ int sie_setup(sie_ctx* c) {
     double* d_boxc = nullptr;
     SIE_TRY(upload(&d_boxc, boxc));
     SIE_CUDA(cudaMalloc(&c->d_rt, (size_t)M * 4 * Q * sizeof(zc)));
-    {
-      // receive work units: at most 32 edges of one leaf box
-      std::vector<int> ch;
-      for (int b = 0; b < c->near.nbox; b++)
-        for (int k = 0; k < c->near.box_cnt[b]; k += 32) {
-          ch.push_back(b);
-          ch.push_back(c->near.box_first[b] + k);
-          ch.push_back(std::min(32, c->near.box_cnt[b] - k));
-          ch.push_back(0);
-        }
-      c->n_rchunk = (int)(ch.size() / 4);
-      SIE_TRY(upload(&c->d_rchunk, ch));
-    }
     for (int l = c->l_min; l <= c->l_max; l++) {
       Level& L = c->lv[l];
       SIE_CUDA(cudaMalloc(&L.C, (size_t)L.nb * 8 * Q * sizeof(zc)));

@@ -163,6 +163,9 @@ struct sie_ctx {
   int* d_edge_box = nullptr;      // leaf box of each internal edge
   int* d_rchunk = nullptr;        // receive chunks: (box, first edge, count, 0) per chunk
   int n_rchunk = 0;
+  int ncols_max = 0;              // widest near panel (columns)
+  // near product: 0 one warp per row; 1 chunks of rows with the panel's x in shared memory
+  int near_mode = 1;
   // near values: ICTF / PMCHWT store (a, b, d), c = cfac * b
   zc* d_na = nullptr;
   zc* d_nb = nullptr;
@@ -198,6 +201,7 @@ int near_blocks_list(sie_ctx* c, int* d_tri_verts, const int* d_m, const int* d_
 int near_matvec64(sie_ctx* c, const zc* x, zc* y, int nrhs, bool accum, cudaStream_t st);
 int near_matvec32(sie_ctx* c, const cc* x, cc* y, int nrhs, bool accum, cudaStream_t st);
 int near_to_f32(sie_ctx* c);
+int near_prepare_kernels(sie_ctx* c);
 int far_build_tables(sie_ctx* c, const double* d_boxc);
 int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev);
 int far_prepare_kernels(sie_ctx* c);
