@@ -27,6 +27,9 @@ struct GmState {
   double bea;
   double nrm;       // generic norm result
   int reorth;
+  int passes;       // MGS passes of the last Arnoldi step
+  unsigned bar_count, bar_gen;  // grid barrier of the fused Arnoldi kernel
+  int bar_err;      // set if a grid barrier wait gave up
   int pad;
 };
 
@@ -63,6 +66,23 @@ __device__ zc reduce_partials(const zc* part, int np) {
   if (threadIdx.x == 0) res = v;
   __syncthreads();
   zc r = res;
+  __syncthreads();
+  return r;
+}
+
+// Same, reading the partials from L2 (they were written by other SMs inside the same
+// kernel, so an L1 line from an earlier use of the buffer may be stale).
+__device__ zc reduce_partials_l2(const zc* part, int np) {
+  __shared__ zc res2;
+  zc v = mk<double>(0, 0);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    double2 t = __ldcg(reinterpret_cast<const double2*>(part) + i);
+    v += mk<double>(t.x, t.y);
+  }
+  v = block_sum(v);
+  if (threadIdx.x == 0) res2 = v;
+  __syncthreads();
+  zc r = res2;
   __syncthreads();
   return r;
 }
@@ -200,6 +220,113 @@ __global__ void k_givens(zc* H, int m, int jh, double* rc, zc* rs, GmState* gs, 
   gs->bea = sqrt(cabs2(H[HIDX(jh + 1, m)])) / bn;
 }
 
+// Grid-wide barrier of the fused Arnoldi kernel.  The kernel is launched cooperatively,
+// so all its blocks are resident; the wait is still bounded: a block that sees no
+// progress for about a second records the failure in bar_err and stops waiting, later
+// barriers then pass straight through, and the host reports the error.
+__device__ void grid_bar(GmState* gs, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &gs->bar_gen;
+    volatile int* err = &gs->bar_err;
+    if (*err == 0) {
+      unsigned g = *gen;
+      __threadfence();
+      unsigned arrived = atomicAdd(&gs->bar_count, 1u) + 1u;
+      if (arrived == nblocks) {
+        atomicExch(&gs->bar_count, 0u);
+        __threadfence();
+        atomicAdd(&gs->bar_gen, 1u);
+      } else {
+        long long it = 0;
+        while (*gen == g && *err == 0) {
+          if (++it > (1LL << 24)) {
+            atomicExch(&gs->bar_err, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// One Arnoldi step after the matvec, fused: iterative modified Gram-Schmidt of w
+// against V(:, 0:jH) (passes repeated while dnormw <= dloo, at most 3), H(:, jH),
+// V(:, jH+1) = w / dnormw, and the Givens update of column jH with the Arnoldi
+// backward error.  Every block reduces the per-block partials in the same order, so
+// all blocks see the same h_j and take the same re-orthogonalisation decision.
+__global__ void __launch_bounds__(512) k_arnoldi(zc* __restrict__ w, zc* __restrict__ V, size_t ld,
+                                                 int n, int jH, zc* H, int m, double* rc, zc* rs,
+                                                 zc* part, GmState* gs, double bn) {
+  const unsigned nb = gridDim.x;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  zc* Hc = H + (size_t)jH * (m + 1);
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i <= jH; i += blockDim.x) Hc[i] = mk<double>(0, 0);
+  int buf = 0, pass = 1;
+  double dnormw = 0, dloo = 0;
+  for (;; pass++) {
+    double dloo2 = 0;
+    zc acc = mk<double>(0, 0);
+    for (int i = t0; i < n; i += stride) acc = cfma_conj(V[i], w[i], acc);
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) __stcg(reinterpret_cast<double2*>(part) + buf * nb + blockIdx.x, make_double2(acc.re, acc.im));
+    grid_bar(gs, nb);
+    for (int j = 0; j <= jH; j++) {
+      const zc h = reduce_partials_l2(part + buf * nb, nb);
+      buf ^= 1;
+      if (blockIdx.x == 0 && threadIdx.x == 0) Hc[j] += h;
+      dloo2 += cabs2(h);
+      const zc* Vj = V + (size_t)j * ld;
+      acc = mk<double>(0, 0);
+      if (j < jH) {
+        const zc* Vn = Vj + ld;
+        for (int i = t0; i < n; i += stride) {
+          zc wi = w[i] - h * Vj[i];
+          w[i] = wi;
+          acc = cfma_conj(Vn[i], wi, acc);
+        }
+      } else {
+        for (int i = t0; i < n; i += stride) {
+          zc wi = w[i] - h * Vj[i];
+          w[i] = wi;
+          acc.re += cabs2(wi);
+        }
+      }
+      acc = block_sum(acc);
+      if (threadIdx.x == 0) __stcg(reinterpret_cast<double2*>(part) + buf * nb + blockIdx.x, make_double2(acc.re, acc.im));
+      grid_bar(gs, nb);
+    }
+    const zc s2 = reduce_partials_l2(part + buf * nb, nb);
+    buf ^= 1;
+    dnormw = sqrt(s2.re);
+    dloo = sqrt(dloo2);
+    if (!(dnormw <= dloo && pass < 3)) break;
+  }
+  zc* Vnew = V + (size_t)(jH + 1) * ld;
+  const double inv = 1.0 / dnormw;
+  for (int i = t0; i < n; i += stride) Vnew[i] = w[i] * inv;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    gs->dnormw = dnormw;
+    gs->dloo = dloo;
+    gs->passes = pass;
+    H[HIDX(jH + 1, jH)] = mk<double>(dnormw, 0.0);
+    for (int j = 0; j < jH; j++) zrot(H[HIDX(j, jH)], H[HIDX(j + 1, jH)], rc[j], rs[j]);
+    double c;
+    zc sn;
+    zrotg(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    rc[jH] = c;
+    rs[jH] = sn;
+    zrot(H[HIDX(jH, m)], H[HIDX(jH + 1, m)], c, sn);
+    zrot(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    H[HIDX(jH + 1, jH)] = mk<double>(0, 0);
+    gs->bea = sqrt(cabs2(H[HIDX(jH + 1, m)])) / bn;
+  }
+}
+
 // y = H(0:k, 0:k)^{-1} H(0:k, m)   (ztrsv 'U','N','N')
 __global__ void k_trsv(const zc* H, int m, int k, zc* y) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -234,12 +361,15 @@ __global__ void k_gs_reset(GmState* gs) {
   gs->dloo2 = 0;
 }
 
+static const int AR_MAXB = 1024;  // largest grid of the fused Arnoldi kernel
+
 struct Gm {
   int n, m;
-  zc *V, *w, *r0, *xc, *y, *H, *part_a, *part_b, *rs;
+  zc *V, *w, *r0, *xc, *y, *H, *part_a, *part_b, *part2, *rs;
   double* rc;
   GmState* gs;
-  GmState* hgs;  // pinned host copy
+  GmState* hgs;  // pinned host copies of gs, one slot per Arnoldi step parity
+  int ar_blocks; // grid of the fused Arnoldi kernel
 };
 
 static int gm_alloc(sie_ctx* c, int m, Gm& g) {
@@ -261,12 +391,21 @@ static int gm_alloc(sie_ctx* c, int m, Gm& g) {
   size_t ors = add((size_t)(m + 1) * sizeof(zc));
   size_t orc = add((size_t)(m + 1) * sizeof(double));
   size_t ogs = add(sizeof(GmState));
+  size_t op2 = add((size_t)2 * AR_MAXB * sizeof(zc));
   if (c->gm_bytes < need) {
     if (c->d_gm) cudaFree(c->d_gm);
     c->d_gm = nullptr;
     c->gm_bytes = 0;
     SIE_CUDA(cudaMalloc(&c->d_gm, need));
+    SIE_CUDA(cudaMemset(c->d_gm, 0, need));
     c->gm_bytes = need;
+  }
+  if (!c->h_gm) SIE_CUDA(cudaHostAlloc(&c->h_gm, 2 * sizeof(GmState), cudaHostAllocDefault));
+  if (c->ar_blocks == 0) {
+    int per_sm = 0, nsm = 0;
+    SIE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arnoldi, 512, 0));
+    SIE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    c->ar_blocks = std::max(1, std::min(AR_MAXB, std::min(per_sm, 2) * nsm));
   }
   char* b = (char*)c->d_gm;
   g.n = n;
@@ -282,6 +421,9 @@ static int gm_alloc(sie_ctx* c, int m, Gm& g) {
   g.rs = (zc*)(b + ors);
   g.rc = (double*)(b + orc);
   g.gs = (GmState*)(b + ogs);
+  g.part2 = (zc*)(b + op2);
+  g.hgs = (GmState*)c->h_gm;
+  g.ar_blocks = std::max(1, std::min(c->ar_blocks, (n + 511) / 512));
   return SIE_OK;
 }
 
@@ -318,6 +460,8 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
   int n = g.n;
   size_t ld = (size_t)n;
   auto t0 = std::chrono::steady_clock::now();
+  // grid barrier state (bar_count, bar_gen, bar_err) starts clean for every solve
+  SIE_CUDA(cudaMemsetAsync(&g.gs->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), s));
   cudaEventRecord(c->ev[12], s);
   // internal layout: b -> d_yi (kept), x -> d_xi
   zc* b = c->d_yi;
@@ -374,68 +518,89 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
   int iterOut = 0, compRsd = 0;
   double bea = 1e300, be = 1e300, trueNormRes = 0;
   int itermax = cfg->max_iterations;
+  // The scalars of Arnoldi step jH are copied to pinned slot jH & 1 and marked by
+  // event ev[14 + (jH & 1)].  The host enqueues step jH + 1 before it reads step jH,
+  // so the GPU never waits for the host.  A step enqueued after the one that ends the
+  // solve only touches w, V(:, jH+2), H(:, jH+1) and rows jH+1.. of the right-hand
+  // column, none of which the final update reads.
+  auto post = [&](int jH) -> int {
+    SIE_CUDA(cudaMemcpyAsync(&g.hgs[jH & 1], g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    SIE_CUDA(cudaEventRecord(c->ev[14 + (jH & 1)], s));
+    return SIE_OK;
+  };
+  auto arnoldi = [&](int jH) -> int {
+    size_t ldv = ld;
+    int nn = n, jj = jH, mm = m;
+    double bnv = bn;
+    void* args[] = {&g.w, &g.V, &ldv, &nn, &jj, &g.H, &mm, &g.rc, &g.rs, &g.part2, &g.gs, &bnv};
+    SIE_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi, dim3(g.ar_blocks), dim3(512), args, 0, s));
+    sie::count_launch();
+    return SIE_OK;
+  };
+  // Decide step p once its scalars are on the host: 1 = the solve ends (x final),
+  // 0 = go on; negative = error code.
+  int end_code = SIE_OK;
+  auto decide = [&](int p) -> int {
+    SIE_CUDA(cudaEventSynchronize(c->ev[14 + (p & 1)]));
+    GmState h = g.hgs[p & 1];
+    if (h.bar_err) return -fail(SIE_ERR_CUDA, "GMRES: a grid barrier of the Arnoldi step timed out");
+    if (!std::isfinite(h.dnormw)) return -fail(SIE_ERR_NONFINITE, "GMRES: non-finite Arnoldi vector");
+    bea = h.bea;
+    if (!std::isfinite(bea)) return -fail(SIE_ERR_NONFINITE, "GMRES: non-finite residual estimate");
+    int it = iterOut * m + p + 1;
+    if (bea <= cfg->tolerance || it >= itermax) {
+      compRsd = 1;
+      // xCurrent = x + V y
+      k_trsv<<<1, 1, 0, s>>>(g.H, m, p + 1, g.y); sie::count_launch();
+      k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, p + 1, n, ld, g.xc); sie::count_launch();
+      // true residual
+      int rr = matvec(g.xc, g.w);
+      if (rr != SIE_OK) return -rr;
+      k_sub<<<RB, RT_, 0, s>>>(b, g.w, g.w, n); sie::count_launch();
+      rr = norm2(c, g, g.w, trueNormRes);
+      if (rr != SIE_OK) return -rr;
+      be = trueNormRes / bn;
+      if (be <= cfg->tolerance || it >= itermax) {
+        k_copy<<<RB, RT_, 0, s>>>(g.xc, x, n); sie::count_launch();
+        int conv = be <= cfg->tolerance;
+        end_code = finish(conv ? SIE_OK : fail(SIE_ERR_NOCONV, "GMRES: no convergence"), it, bea,
+                          trueNormRes / bn, conv);
+        return 1;
+      }
+    }
+    return 0;
+  };
   while (true) {
     k_hinit<<<(m + 1 + 127) / 128, 128, 0, s>>>(g.H, m, beta); sie::count_launch();
-    int jH = 0;
-    for (; jH < m; jH++) {
-      // w = A V_jH
+    int pending = -1;
+    for (int jH = 0; jH < m; jH++) {
+      // w = A V_jH, then the fused orthogonalisation / Givens step
       SIE_TRY(matvec(g.V + (size_t)jH * ld, g.w));
-      k_hcol_zero<<<(m + 1 + 127) / 128, 128, 0, s>>>(g.H, m, jH); sie::count_launch();
-      GmState h;
-      for (int northo = 1;; northo++) {
-        k_gs_reset<<<1, 1, 0, s>>>(g.gs); sie::count_launch();
-        // start <V_0, w>
-        k_mgs<<<RB, RT_, 0, s>>>(g.w, nullptr, g.V, nullptr, g.part_a, n, g.H + (size_t)jH * (m + 1),
-                                 0, g.gs); sie::count_launch();
-        zc* pin = g.part_a;
-        zc* pout = g.part_b;
-        for (int j = 0; j <= jH; j++) {
-          const zc* Vn = (j < jH) ? g.V + (size_t)(j + 1) * ld : nullptr;
-          k_mgs<<<RB, RT_, 0, s>>>(g.w, g.V + (size_t)j * ld, Vn, pin, pout, n,
-                                   g.H + (size_t)jH * (m + 1), j, g.gs); sie::count_launch();
-          zc* t = pin;
-          pin = pout;
-          pout = t;
-        }
-        k_pass_final<<<1, RT_, 0, s>>>(pin, RB, g.gs, northo); sie::count_launch();
-        SIE_CUDA(cudaGetLastError());
-        SIE_TRY(read_gs(c, g, h));
-        if (!std::isfinite(h.dnormw)) return fail(SIE_ERR_NONFINITE, "GMRES: non-finite Arnoldi vector");
-        if (!h.reorth) break;
-      }
-      // V_{jH+1} = w / dnormw (icntl(8) = 0 keeps m+1 basis vectors)
-      k_scale_copy<<<RB, RT_, 0, s>>>(g.w, g.V + (size_t)(jH + 1) * ld, n, g.gs); sie::count_launch();
-      k_givens<<<1, 1, 0, s>>>(g.H, m, jH, g.rc, g.rs, g.gs, bn); sie::count_launch();
+      SIE_TRY(arnoldi(jH));
+      SIE_TRY(post(jH));
       SIE_CUDA(cudaGetLastError());
-      SIE_TRY(read_gs(c, g, h));
-      bea = h.bea;
-      int it = iterOut * m + jH + 1;
-      if (!std::isfinite(bea)) return fail(SIE_ERR_NONFINITE, "GMRES: non-finite residual estimate");
-      if (bea <= cfg->tolerance || it >= itermax) {
-        compRsd = 1;
-        // xCurrent = x + V y
-        k_trsv<<<1, 1, 0, s>>>(g.H, m, jH + 1, g.y); sie::count_launch();
-        k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, jH + 1, n, ld, g.xc); sie::count_launch();
-        // true residual
-        SIE_TRY(matvec(g.xc, g.w));
-        k_sub<<<RB, RT_, 0, s>>>(b, g.w, g.w, n); sie::count_launch();
-        r = norm2(c, g, g.w, trueNormRes);
-        if (r != SIE_OK) return r;
-        be = trueNormRes / bn;
-        if (be <= cfg->tolerance || it >= itermax) {
-          k_copy<<<RB, RT_, 0, s>>>(g.xc, x, n); sie::count_launch();
-          int conv = be <= cfg->tolerance;
-          return finish(conv ? SIE_OK : fail(SIE_ERR_NOCONV, "GMRES: no convergence"), it, bea,
-                        trueNormRes / bn, conv);
-        }
+      if (pending >= 0) {
+        int d = decide(pending);
+        if (d < 0) return -d;
+        if (d == 1) return end_code;
       }
+      pending = jH;
+      if (iterOut * m + jH + 1 >= itermax) break;  // the budget ends with this step
       if (cfg->time_limit_s > 0) {
         double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (el > cfg->time_limit_s) {
-          finish(SIE_ERR_TIMEOUT, it, bea, be, 0);
+          int d = decide(pending);
+          if (d < 0) return -d;
+          if (d == 1) return end_code;
+          finish(SIE_ERR_TIMEOUT, iterOut * m + jH + 1, bea, be, 0);
           return fail(SIE_ERR_TIMEOUT, "GMRES: time limit reached");
         }
       }
+    }
+    {
+      int d = decide(pending);
+      if (d < 0) return -d;
+      if (d == 1) return end_code;
     }
     iterOut++;
     if (bea > cfg->tolerance) {

@@ -1139,6 +1139,7 @@ int sie_free(sie_ctx* c) {
     for (void* p : lp)
       if (p) cudaFree(p);
   }
+  if (c->h_gm) cudaFreeHost(c->h_gm);
   for (int i = 0; i < 16; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);

@@ -189,6 +189,8 @@ struct sie_ctx {
   // solver workspace
   void* d_gm = nullptr;
   size_t gm_bytes = 0;
+  void* h_gm = nullptr;           // pinned host slots for the solver's scalars
+  int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
 
   sie::Timings tm;
 };
