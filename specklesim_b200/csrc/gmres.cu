@@ -12,6 +12,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "sie_internal.h"
 
 namespace sie {
@@ -327,6 +329,263 @@ __global__ void __launch_bounds__(512) k_arnoldi(zc* __restrict__ w, zc* __restr
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident variant of the fused Arnoldi step for n <= 148 x 512 x 8.  Each
+// thread keeps EPT elements of w in registers for the whole step.  A global reduction is
+// one all-to-all exchange: every block publishes its partial in its own slot of the
+// round's buffer with a round tag, and every block reads all slots in the same order,
+// so all blocks get bit-identical sums with no separate barrier.  The next basis
+// column is loaded while the exchange is in flight.
+struct __align__(32) ArSlot {
+  double re, im;
+  unsigned tag;
+  unsigned pad[3];
+};
+static const int AR_THREADS = 512;
+
+__device__ zc ar_allreduce(zc v, ArSlot* slots, unsigned round, unsigned tag, int nb, GmState* gs) {
+  __shared__ zc bc;
+  v = block_sum(v);
+  ArSlot* buf = slots + (size_t)(round & 1u) * nb;
+  if (threadIdx.x == 0) {
+    __stcg(&buf[blockIdx.x].re, v.re);
+    __stcg(&buf[blockIdx.x].im, v.im);
+    __threadfence();
+    atomicExch(&buf[blockIdx.x].tag, tag);
+  }
+  if (threadIdx.x < 32) {
+    zc acc = mk<double>(0, 0);
+    for (int i = threadIdx.x; i < nb; i += 32) {
+      volatile unsigned* pt = &buf[i].tag;
+      long long it = 0;
+      while (*pt != tag) {
+        if (*(volatile int*)&gs->bar_err) break;
+        if (++it > (1LL << 22)) {
+          atomicExch(&gs->bar_err, 1);
+          break;
+        }
+      }
+      __threadfence();
+      acc += mk<double>(__ldcg(&buf[i].re), __ldcg(&buf[i].im));
+    }
+    acc = warp_sum(acc);
+    if (threadIdx.x == 0) bc = acc;
+  }
+  __syncthreads();
+  zc r = bc;
+  __syncthreads();
+  return r;
+}
+
+template <int EPT>
+__global__ void __launch_bounds__(AR_THREADS, 1) k_arnoldi_reg(
+    zc* __restrict__ w, zc* __restrict__ V, size_t ld, int n, int jH, zc* H, int m, double* rc,
+    zc* rs, ArSlot* slots, unsigned epoch, GmState* gs, double bn) {
+  const int nb = gridDim.x;
+  const int i0 = blockIdx.x * AR_THREADS + threadIdx.x, stride = nb * AR_THREADS;
+  zc wr[EPT], vr[EPT], vn[EPT];
+#pragma unroll
+  for (int e = 0; e < EPT; e++) {
+    int i = i0 + e * stride;
+    wr[e] = i < n ? w[i] : mk<double>(0, 0);
+  }
+  zc* Hc = H + (size_t)jH * (m + 1);
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i <= jH; i += blockDim.x) Hc[i] = mk<double>(0, 0);
+  unsigned round = 0;
+  auto tag = [&]() { return (epoch << 12) | (round & 4095u); };
+  int pass = 1;
+  double dnormw = 0, dloo = 0;
+  for (;; pass++) {
+    double dloo2 = 0;
+    zc acc = mk<double>(0, 0);
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+      int i = i0 + e * stride;
+      double2 t = i < n ? __ldcg(reinterpret_cast<const double2*>(V) + i) : make_double2(0.0, 0.0);
+      vr[e] = mk<double>(t.x, t.y);
+      acc = cfma_conj(vr[e], wr[e], acc);
+    }
+    for (int j = 0; j <= jH; j++) {
+      if (j < jH) {
+        const double2* Vn = reinterpret_cast<const double2*>(V + (size_t)(j + 1) * ld);
+#pragma unroll
+        for (int e = 0; e < EPT; e++) {
+          int i = i0 + e * stride;
+          double2 t = i < n ? __ldcg(Vn + i) : make_double2(0.0, 0.0);
+          vn[e] = mk<double>(t.x, t.y);
+        }
+      }
+      const zc h = ar_allreduce(acc, slots, round, tag(), nb, gs);
+      round++;
+      if (blockIdx.x == 0 && threadIdx.x == 0) Hc[j] += h;
+      dloo2 += cabs2(h);
+      acc = mk<double>(0, 0);
+#pragma unroll
+      for (int e = 0; e < EPT; e++) {
+        wr[e] = wr[e] - h * vr[e];
+        if (j < jH) {
+          acc = cfma_conj(vn[e], wr[e], acc);
+          vr[e] = vn[e];
+        } else {
+          acc.re += cabs2(wr[e]);
+        }
+      }
+    }
+    const zc s2 = ar_allreduce(acc, slots, round, tag(), nb, gs);
+    round++;
+    dnormw = sqrt(s2.re);
+    dloo = sqrt(dloo2);
+    if (!(dnormw <= dloo && pass < 3)) break;
+  }
+  const double inv = 1.0 / dnormw;
+  zc* Vnew = V + (size_t)(jH + 1) * ld;
+#pragma unroll
+  for (int e = 0; e < EPT; e++) {
+    int i = i0 + e * stride;
+    if (i < n) {
+      w[i] = wr[e];
+      Vnew[i] = wr[e] * inv;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    gs->dnormw = dnormw;
+    gs->dloo = dloo;
+    gs->passes = pass;
+    H[HIDX(jH + 1, jH)] = mk<double>(dnormw, 0.0);
+    for (int j = 0; j < jH; j++) zrot(H[HIDX(j, jH)], H[HIDX(j + 1, jH)], rc[j], rs[j]);
+    double c;
+    zc sn;
+    zrotg(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    rc[jH] = c;
+    rs[jH] = sn;
+    zrot(H[HIDX(jH, m)], H[HIDX(jH + 1, m)], c, sn);
+    zrot(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    H[HIDX(jH + 1, jH)] = mk<double>(0, 0);
+    gs->bea = sqrt(cabs2(H[HIDX(jH + 1, m)])) / bn;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Single-cluster variant for n <= 16 x 512 x 8: one thread-block cluster of up to 16
+// CTAs (co-scheduled by the hardware) runs the whole Arnoldi step with w in registers.
+// A global reduction is: block sum -> own shared-memory slot -> cluster barrier ->
+// warp 0 reads the slots of all CTAs through distributed shared memory in rank order,
+// so every CTA forms the same sum.  The next basis column is loaded before the barrier.
+static const int CL_THREADS = 512;
+
+// First half of a cluster reduction: block sum, publish it in this CTA's slot, arrive.
+__device__ __forceinline__ void cl_publish(zc v, zc* slot, int buf) {
+  v = block_sum(v);
+  if (threadIdx.x == 0) slot[buf] = v;
+  cooperative_groups::this_cluster().barrier_arrive();
+}
+// Second half: wait, sum the slots of all CTAs in rank order (warp 0), broadcast.
+__device__ __forceinline__ zc cl_collect(zc* slot, zc* bc, int buf) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  cl.barrier_wait();
+  if (threadIdx.x < 32) {
+    const unsigned nr = cl.num_blocks();
+    zc a = mk<double>(0, 0);
+    if (threadIdx.x < nr) a = *cl.map_shared_rank(slot + buf, threadIdx.x);
+    a = warp_sum(a);
+    if (threadIdx.x == 0) bc[buf] = a;
+  }
+  __syncthreads();
+  return bc[buf];
+}
+
+template <int EPT>
+__global__ void __launch_bounds__(CL_THREADS, 1) k_arnoldi_cl(
+    zc* __restrict__ w, zc* __restrict__ V, size_t ld, int n, int jH, zc* H, int m, double* rc,
+    zc* rs, GmState* gs, double bn) {
+  __shared__ zc slot[2], bc[2];
+  const int nb = gridDim.x;
+  const int i0 = blockIdx.x * CL_THREADS + threadIdx.x, stride = nb * CL_THREADS;
+  zc wr[EPT], vr[EPT], vn[EPT];
+#pragma unroll
+  for (int e = 0; e < EPT; e++) {
+    int i = i0 + e * stride;
+    wr[e] = i < n ? w[i] : mk<double>(0, 0);
+  }
+  zc* Hc = H + (size_t)jH * (m + 1);
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i <= jH; i += blockDim.x) Hc[i] = mk<double>(0, 0);
+  int buf = 0, pass = 1;
+  double dnormw = 0, dloo = 0;
+  for (;; pass++) {
+    double dloo2 = 0;
+    zc acc = mk<double>(0, 0);
+#pragma unroll
+    for (int e = 0; e < EPT; e++) {
+      int i = i0 + e * stride;
+      vr[e] = i < n ? V[i] : mk<double>(0, 0);
+      acc = cfma_conj(vr[e], wr[e], acc);
+    }
+    for (int j = 0; j <= jH; j++) {
+      cl_publish(acc, slot, buf);
+      if (j < jH) {  // the next column streams in while the cluster barrier completes
+        const zc* Vn = V + (size_t)(j + 1) * ld;
+#pragma unroll
+        for (int e = 0; e < EPT; e++) {
+          int i = i0 + e * stride;
+          vn[e] = i < n ? Vn[i] : mk<double>(0, 0);
+        }
+      }
+      const zc h = cl_collect(slot, bc, buf);
+      buf ^= 1;
+      if (blockIdx.x == 0 && threadIdx.x == 0) Hc[j] += h;
+      dloo2 += cabs2(h);
+      acc = mk<double>(0, 0);
+#pragma unroll
+      for (int e = 0; e < EPT; e++) {
+        wr[e] = wr[e] - h * vr[e];
+        if (j < jH) {
+          acc = cfma_conj(vn[e], wr[e], acc);
+          vr[e] = vn[e];
+        } else {
+          acc.re += cabs2(wr[e]);
+        }
+      }
+    }
+    cl_publish(acc, slot, buf);
+    const zc s2 = cl_collect(slot, bc, buf);
+    buf ^= 1;
+    dnormw = sqrt(s2.re);
+    dloo = sqrt(dloo2);
+    if (!(dnormw <= dloo && pass < 3)) break;
+  }
+  const double inv = 1.0 / dnormw;
+  zc* Vnew = V + (size_t)(jH + 1) * ld;
+#pragma unroll
+  for (int e = 0; e < EPT; e++) {
+    int i = i0 + e * stride;
+    if (i < n) {
+      w[i] = wr[e];
+      Vnew[i] = wr[e] * inv;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    gs->dnormw = dnormw;
+    gs->dloo = dloo;
+    gs->passes = pass;
+    H[HIDX(jH + 1, jH)] = mk<double>(dnormw, 0.0);
+    for (int j = 0; j < jH; j++) zrot(H[HIDX(j, jH)], H[HIDX(j + 1, jH)], rc[j], rs[j]);
+    double c;
+    zc sn;
+    zrotg(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    rc[jH] = c;
+    rs[jH] = sn;
+    zrot(H[HIDX(jH, m)], H[HIDX(jH + 1, m)], c, sn);
+    zrot(H[HIDX(jH, jH)], H[HIDX(jH + 1, jH)], c, sn);
+    H[HIDX(jH + 1, jH)] = mk<double>(0, 0);
+    gs->bea = sqrt(cabs2(H[HIDX(jH + 1, m)])) / bn;
+  }
+  // no CTA may leave while another still reads its slots
+  cooperative_groups::this_cluster().sync();
+}
+
 // y = H(0:k, 0:k)^{-1} H(0:k, m)   (ztrsv 'U','N','N')
 __global__ void k_trsv(const zc* H, int m, int k, zc* y) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -370,7 +629,53 @@ struct Gm {
   GmState* gs;
   GmState* hgs;  // pinned host copies of gs, one slot per Arnoldi step parity
   int ar_blocks; // grid of the fused Arnoldi kernel
+  ArSlot* slots; // exchange slots of the register-resident Arnoldi kernel (2 x AR_MAXB)
+  int reg_ept, reg_blocks;  // its elements per thread and grid (0: not usable)
+  int cl_ept, cl_size;      // single-cluster Arnoldi kernel (0: not usable)
 };
+
+template <int EPT>
+static int cl_setup(int cs, cudaStream_t s, bool& ok) {
+  ok = false;
+  if (cs > 8)
+    SIE_CUDA(cudaFuncSetAttribute(k_arnoldi_cl<EPT>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(cs);
+  lc.blockDim = dim3(CL_THREADS);
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  int nclus = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclus, k_arnoldi_cl<EPT>, &lc) != cudaSuccess) {
+    cudaGetLastError();
+    return SIE_OK;
+  }
+  ok = nclus >= 1;
+  return SIE_OK;
+}
+
+template <int EPT>
+static int cl_launch(int cs, cudaStream_t s, zc* w, zc* V, size_t ld, int n, int jH, zc* H, int m,
+                     double* rc, zc* rs, GmState* gs, double bn) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(cs);
+  lc.blockDim = dim3(CL_THREADS);
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  SIE_CUDA(cudaLaunchKernelEx(&lc, k_arnoldi_cl<EPT>, w, V, ld, n, jH, H, m, rc, rs, gs, bn));
+  return SIE_OK;
+}
 
 static int gm_alloc(sie_ctx* c, int m, Gm& g) {
   int n = 2 * c->M;
@@ -392,6 +697,7 @@ static int gm_alloc(sie_ctx* c, int m, Gm& g) {
   size_t orc = add((size_t)(m + 1) * sizeof(double));
   size_t ogs = add(sizeof(GmState));
   size_t op2 = add((size_t)2 * AR_MAXB * sizeof(zc));
+  size_t osl = add((size_t)2 * AR_MAXB * sizeof(ArSlot));
   if (c->gm_bytes < need) {
     if (c->d_gm) cudaFree(c->d_gm);
     c->d_gm = nullptr;
@@ -422,6 +728,40 @@ static int gm_alloc(sie_ctx* c, int m, Gm& g) {
   g.rc = (double*)(b + orc);
   g.gs = (GmState*)(b + ogs);
   g.part2 = (zc*)(b + op2);
+  g.slots = (ArSlot*)(b + osl);
+  // register-resident Arnoldi kernel: the fewest elements per thread that keep the grid
+  // at <= 32 blocks, else 8 per thread on up to one block per SM
+  g.cl_ept = g.cl_size = 0;
+  {
+    const int epts[4] = {1, 2, 4, 8};
+    for (int k = 0; k < 4 && !g.cl_ept; k++) {
+      int cs = (n + CL_THREADS * epts[k] - 1) / (CL_THREADS * epts[k]);
+      if (cs > 16) continue;
+      bool ok = false;
+      int r = epts[k] == 1 ? cl_setup<1>(cs, c->stream, ok)
+              : epts[k] == 2 ? cl_setup<2>(cs, c->stream, ok)
+              : epts[k] == 4 ? cl_setup<4>(cs, c->stream, ok)
+                             : cl_setup<8>(cs, c->stream, ok);
+      if (r != SIE_OK) return r;
+      if (ok) {
+        g.cl_ept = epts[k];
+        g.cl_size = cs;
+      }
+    }
+  }
+  g.reg_ept = g.reg_blocks = 0;
+  if (m <= 1300) {
+    int nsm = 0;
+    SIE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    const int epts[4] = {1, 2, 4, 8};
+    for (int k = 0; k < 4 && !g.reg_ept; k++) {
+      int nbk = (n + AR_THREADS * epts[k] - 1) / (AR_THREADS * epts[k]);
+      if (nbk <= 32 || (epts[k] == 8 && nbk <= nsm)) {
+        g.reg_ept = epts[k];
+        g.reg_blocks = nbk;
+      }
+    }
+  }
   g.hgs = (GmState*)c->h_gm;
   g.ar_blocks = std::max(1, std::min(c->ar_blocks, (n + 511) / 512));
   return SIE_OK;
@@ -460,6 +800,7 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
   int n = g.n;
   size_t ld = (size_t)n;
   auto t0 = std::chrono::steady_clock::now();
+  c->tm.gm_passes = c->tm.gm_steps = 0;
   // grid barrier state (bar_count, bar_gen, bar_err) starts clean for every solve
   SIE_CUDA(cudaMemsetAsync(&g.gs->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), s));
   cudaEventRecord(c->ev[12], s);
@@ -532,8 +873,26 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
     size_t ldv = ld;
     int nn = n, jj = jH, mm = m;
     double bnv = bn;
-    void* args[] = {&g.w, &g.V, &ldv, &nn, &jj, &g.H, &mm, &g.rc, &g.rs, &g.part2, &g.gs, &bnv};
-    SIE_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi, dim3(g.ar_blocks), dim3(512), args, 0, s));
+    if (g.cl_ept && c->arnoldi_mode == 2) {
+      int rr = g.cl_ept == 1 ? cl_launch<1>(g.cl_size, s, g.w, g.V, ldv, nn, jj, g.H, mm, g.rc, g.rs, g.gs, bnv)
+               : g.cl_ept == 2 ? cl_launch<2>(g.cl_size, s, g.w, g.V, ldv, nn, jj, g.H, mm, g.rc, g.rs, g.gs, bnv)
+               : g.cl_ept == 4 ? cl_launch<4>(g.cl_size, s, g.w, g.V, ldv, nn, jj, g.H, mm, g.rc, g.rs, g.gs, bnv)
+                               : cl_launch<8>(g.cl_size, s, g.w, g.V, ldv, nn, jj, g.H, mm, g.rc, g.rs, g.gs, bnv);
+      if (rr != SIE_OK) return rr;
+    } else if (g.reg_ept && c->arnoldi_mode >= 1) {
+      unsigned epoch = c->ar_epoch;
+      c->ar_epoch = (c->ar_epoch + 1) & 0xFFFFFu;
+      if (c->ar_epoch == 0) c->ar_epoch = 1;
+      void* args[] = {&g.w, &g.V, &ldv, &nn, &jj, &g.H, &mm, &g.rc, &g.rs, &g.slots, &epoch, &g.gs, &bnv};
+      const void* fn = g.reg_ept == 1 ? (const void*)k_arnoldi_reg<1>
+                       : g.reg_ept == 2 ? (const void*)k_arnoldi_reg<2>
+                       : g.reg_ept == 4 ? (const void*)k_arnoldi_reg<4>
+                                        : (const void*)k_arnoldi_reg<8>;
+      SIE_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.reg_blocks), dim3(AR_THREADS), args, 0, s));
+    } else {
+      void* args[] = {&g.w, &g.V, &ldv, &nn, &jj, &g.H, &mm, &g.rc, &g.rs, &g.part2, &g.gs, &bnv};
+      SIE_CUDA(cudaLaunchCooperativeKernel((const void*)k_arnoldi, dim3(g.ar_blocks), dim3(512), args, 0, s));
+    }
     sie::count_launch();
     return SIE_OK;
   };
@@ -543,6 +902,8 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
   auto decide = [&](int p) -> int {
     SIE_CUDA(cudaEventSynchronize(c->ev[14 + (p & 1)]));
     GmState h = g.hgs[p & 1];
+    c->tm.gm_passes += h.passes;
+    c->tm.gm_steps += 1;
     if (h.bar_err) return -fail(SIE_ERR_CUDA, "GMRES: a grid barrier of the Arnoldi step timed out");
     if (!std::isfinite(h.dnormw)) return -fail(SIE_ERR_NONFINITE, "GMRES: non-finite Arnoldi vector");
     bea = h.bea;

@@ -374,7 +374,7 @@ template <typename T>
 static int upload(T** d, const std::vector<T>& h) {
   size_t n = std::max<size_t>(h.size(), 1);
   SIE_CUDA(cudaMalloc(d, n * sizeof(T)));
-  if (!h.empty()) SIE_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!h.empty()) SIE_CUDA(h2d(*d, h.data(), h.size() * sizeof(T)));
   return SIE_OK;
 }
 
@@ -721,6 +721,7 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (const char* e = getenv("SIE_RECV_MODE")) c->recv_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));
+  if (const char* e = getenv("SIE_ARNOLDI_MODE")) c->arnoldi_mode = std::max(0, std::min(2, atoi(e)));
   *out = c;
   return SIE_OK;
 }
@@ -908,11 +909,12 @@ int sie_rhs_planewave(sie_ctx* c, const double* k_in, const double* E_in, int nr
   SIE_CUDA(cudaMalloc(&dk, 3 * nrhs * sizeof(double)));
   SIE_CUDA(cudaMalloc(&dE, 3 * nrhs * sizeof(double)));
   SIE_CUDA(cudaMalloc(&db, bytes));
-  SIE_CUDA(cudaMemcpy(dk, k_in, 3 * nrhs * sizeof(double), cudaMemcpyHostToDevice));
-  SIE_CUDA(cudaMemcpy(dE, E_in, 3 * nrhs * sizeof(double), cudaMemcpyHostToDevice));
+  SIE_CUDA(h2d(dk, k_in, 3 * nrhs * sizeof(double)));
+  SIE_CUDA(h2d(dE, E_in, 3 * nrhs * sizeof(double)));
   int r = rhs_planewave_dev(c, dk, dE, nrhs, c->d_yi);
   if (r == SIE_OK) r = scatter_int_to_ext(c, c->d_yi, db, nrhs, c->stream);
-  if (r == SIE_OK && cudaMemcpy(b, db, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (r == SIE_OK && (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+                      cudaMemcpy(b, db, bytes, cudaMemcpyDeviceToHost) != cudaSuccess))
     r = fail(SIE_ERR_CUDA, "sie_rhs_planewave: D2H copy");
   cudaFree(dk);
   cudaFree(dE);
@@ -979,8 +981,8 @@ int sie_farfield(sie_ctx* c, const double* x, const double* pts, int npts, doubl
   SIE_CUDA(cudaMalloc(&dE, 3 * (size_t)npts * sizeof(zc)));
   SIE_CUDA(cudaMalloc(&dH, 3 * (size_t)npts * sizeof(zc)));
   SIE_CUDA(cudaMalloc(&dI, (size_t)npts * sizeof(double)));
-  SIE_CUDA(cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice));
-  SIE_CUDA(cudaMemcpy(dp, pts, 3 * (size_t)npts * sizeof(double), cudaMemcpyHostToDevice));
+  SIE_CUDA(h2d(dx, x, bytes));
+  SIE_CUDA(h2d(dp, pts, 3 * (size_t)npts * sizeof(double)));
   int r = gather_ext_to_int(c, dx, c->d_xi, 1, c->stream);
   if (r == SIE_OK) r = farfield_dev(c, c->d_xi, dp, npts, dE, dH, dI);
   if (r == SIE_OK) {
@@ -1118,7 +1120,8 @@ int sie_get_timings(const sie_ctx* c, double* out, int n) {
   if (!c || !out) return fail(SIE_ERR_ARG, "sie_get_timings: null argument");
   double v[11] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
                   c->tm.mv_near_ms, c->tm.mv_agg_ms, c->tm.mv_ss_ms, c->tm.mv_sr_ms,
-                  c->tm.mv_rr_ms, c->tm.mv_recv_ms, 0.0};
+                  c->tm.mv_rr_ms, c->tm.mv_recv_ms,
+                  c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0};
   for (int i = 0; i < n && i < 11; i++) out[i] = v[i];
   return SIE_OK;
 }

@@ -24,6 +24,15 @@ void count_launch();
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
+// Host-to-device copy that has landed when it returns.  A plain cudaMemcpy from pageable
+// memory may return while its DMA is still in flight, and the library's kernels run on
+// a stream that does not wait for the legacy default stream.
+inline cudaError_t h2d(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(cudaStreamLegacy);
+}
+
 #define SIE_TRY(x)               \
   do {                           \
     int _r = (x);                \
@@ -110,6 +119,7 @@ struct Timings {
   double fill_ms = 0, rt_ms = 0, tl_ms = 0, setup_ms = 0;
   double mv_total_ms = 0, mv_near_ms = 0, mv_agg_ms = 0, mv_ss_ms = 0, mv_sr_ms = 0,
          mv_rr_ms = 0, mv_recv_ms = 0;
+  double gm_passes = 0, gm_steps = 0;  // MGS passes and Arnoldi steps of the last solve
 };
 
 }  // namespace sie
@@ -191,6 +201,10 @@ struct sie_ctx {
   size_t gm_bytes = 0;
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
+  unsigned ar_epoch = 1;          // launch counter tagging the Arnoldi exchange rounds
+  // Arnoldi step: 0 grid-barrier kernel; 1 register-resident kernel with tagged exchanges;
+  // 2 one thread-block cluster (falls back to 1, then 0, when the vector is too long)
+  int arnoldi_mode = 2;
 
   sie::Timings tm;
 };

@@ -87,7 +87,7 @@ int diag_extract(sie_ctx* c) {
   }
   long long* d_idx = nullptr;
   SIE_CUDA(cudaMalloc(&d_idx, idx.size() * sizeof(long long)));
-  SIE_CUDA(cudaMemcpy(d_idx, idx.data(), idx.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  SIE_CUDA(h2d(d_idx, idx.data(), idx.size() * sizeof(long long)));
   SIE_CUDA(cudaMalloc(&c->d_diag, 2 * (size_t)c->M * sizeof(zc)));
   k_diag<<<(c->M + 255) / 256, 256, 0, c->stream>>>(c->d_na, c->d_nd, d_idx, c->M, c->d_diag); sie::count_launch();
   SIE_CUDA(cudaGetLastError());
@@ -256,7 +256,7 @@ extern "C" int sie_precondition_left(sie_ctx* c, const double* v1, double* v2) {
   SIE_CUDA(cudaMalloc(&d1, bytes));
   SIE_CUDA(cudaMalloc(&d2, bytes));
   SIE_CUDA(cudaMalloc(&e1, bytes));
-  SIE_CUDA(cudaMemcpy(e1, v1, bytes, cudaMemcpyHostToDevice));
+  SIE_CUDA(h2d(e1, v1, bytes));
   int r = gather_ext_to_int(c, e1, d1, 1, c->stream);
   if (r == SIE_OK) r = jacobi_apply(c, d1, d2, c->stream);
   if (r == SIE_OK) r = scatter_int_to_ext(c, d2, e1, 1, c->stream);

@@ -177,8 +177,8 @@ class Sie:
         v = np.zeros(11)
         check(self._lib.sie_get_timings(self._h, dptr(v), 11))
         keys = ["fill_ms", "rt_tl_ms", "setup_ms", "mv_total_ms", "mv_near_ms", "mv_agg_ms",
-                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms"]
-        return dict(zip(keys, v[:10]))
+                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step"]
+        return dict(zip(keys, v))
 
     def close(self):
         if getattr(self, "_h", None):

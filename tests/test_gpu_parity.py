@@ -138,6 +138,23 @@ def test_rhs_matches_oracle(slab_pair):
     assert rel(b1, b2) < 1e-13
 
 
+def test_host_copies_are_ordered_in_later_contexts(gpu_lib):
+    """Right-hand sides and far fields from host buffers come out the same in every
+    context of a process (host copies complete before the library's stream uses them)."""
+    from specklesim_b200 import Sie, incidence
+    V, T = P.sphere(1)
+    k, E = incidence(0.3, 0.2, "TE", 2)
+    pts = 5.0 * np.array([[0.1, 0.2, 0.97], [0.5, -0.3, 0.81]])
+    outs = []
+    for _ in range(3):
+        g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=20).setup()
+        b = g.rhs_planewave(k, E)
+        outs.append((b, g.farfield(b, pts)[2]))
+        g.close()
+    for b, I in outs[1:]:
+        assert np.array_equal(b, outs[0][0]) and np.array_equal(I, outs[0][1])
+
+
 def test_solve_fixed_budget_matches_oracle_gmres(metal_pair, oracle_lib):
     """GPU GMRES (IMGS + Givens, two restarts) against the zgmres restatement driving the
     oracle matvec, on the metallic slab where both stop at the iteration budget
@@ -152,6 +169,25 @@ def test_solve_fixed_budget_matches_oracle_gmres(metal_pair, oracle_lib):
     assert st["iterations"] == info["iterations"] == 45
     assert rel(x_g, x_o) < 1e-7, rel(x_g, x_o)
     assert abs(st["backward_error_true"] - info["be"]) <= 1e-7 * info["be"]
+
+
+def test_arnoldi_kernel_variants_agree(gpu_lib, monkeypatch):
+    """The grid-barrier, tagged-exchange and single-cluster Arnoldi kernels run the same
+    IMGS steps; only the order of the partial sums differs."""
+    from specklesim_b200 import Sie, incidence
+    V, T = P.slab(cells=24, length_wl=6.0, seed=3)
+    xs = []
+    for mode in ("0", "1", "2"):
+        monkeypatch.setenv("SIE_ARNOLDI_MODE", mode)
+        g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=100).setup()
+        k, E = incidence(0.0, 0.0, "TM", 2)
+        b = g.rhs_planewave(k, E)
+        x, st = g.solve(b, restart=20, max_iterations=45, tolerance=1e-12, raise_on_noconv=False)
+        assert st["iterations"] == 45
+        xs.append(x)
+        g.close()
+    for x in xs[1:]:
+        assert rel(x, xs[0]) < 1e-9, rel(x, xs[0])
 
 
 def test_solve_converges_like_oracle(oracle_lib, gpu_lib):
