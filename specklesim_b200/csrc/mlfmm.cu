@@ -558,6 +558,108 @@ static size_t sr_warp_smem() {
          (size_t)SRW_GB * 216 * sizeof(int);
 }
 
+// Branch-free form of k_sr_warp.  The TL tile gets a zero row (index 343) that every
+// pair inside the near zone points to, and absent siblings accumulate into registers
+// that are never stored, so the loop over the 8 siblings has no branches: its 8 TL
+// reads and 16 complex FMAs can all be in flight together.  Source slots inside the
+// parent itself (all siblings, all near) are dropped when the list is compacted.
+template <typename T>
+__global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_bf(
+    const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
+    int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
+    int zero_other, cx<T>* __restrict__ D) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sTL = reinterpret_cast<cx<T>*>(smraw);                         // [344][SRW_QT]
+  short* s_tix = reinterpret_cast<short*>(sTL + 344 * SRW_QT);          // [216][8]
+  int* s_list = reinterpret_cast<int*>(s_tix + 216 * 8);                // [SRW_GB][216]
+  const int q0 = blockIdx.x * SRW_QT;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 344 * SRW_QT; i += blockDim.x) {
+    int t = i / SRW_QT, j = i - t * SRW_QT;
+    int q = q0 + j;
+    sTL[i] = (t < 343 && q < Q) ? tl[((size_t)t * 2 + md) * Q + q] : mk<T>(0, 0);
+  }
+  for (int i = tid; i < 216 * 8; i += blockDim.x) {
+    int dc = i >> 3, o = i & 7;
+    int d = dc >> 3, c = dc & 7;
+    int ox = ((o >> 2) & 1) - ((c >> 2) & 1) - 2 * (d / 9 - 1);
+    int oy = ((o >> 1) & 1) - ((c >> 1) & 1) - 2 * ((d / 3) % 3 - 1);
+    int oz = (o & 1) - (c & 1) - 2 * (d % 3 - 1);
+    bool nearz = ox > -2 && ox < 2 && oy > -2 && oy < 2 && oz > -2 && oz < 2;
+    s_tix[i] = nearz ? (short)343 : (short)((ox + 3) * 49 + (oy + 3) * 7 + (oz + 3));
+  }
+  __syncthreads();
+  const int w = tid >> 5, lane = tid & 31;
+  const int g = blockIdx.y * SRW_GB + w;
+  if (g >= ngrp) return;
+  int sib = (lane < 8) ? grp_sib[(size_t)g * 8 + lane] : -1;
+  int* lst = s_list + w * 216;
+  int cnt = 0;
+  for (int base = 0; base < 216; base += 32) {
+    int dc = base + lane;
+    int s = (dc < 216 && (dc >> 3) != 13) ? grp_src[(size_t)g * 216 + dc] : -1;
+    unsigned bal = __ballot_sync(0xffffffffu, s >= 0);
+    if (s >= 0) lst[cnt + __popc(bal & ((1u << lane) - 1u))] = (s << 8) | dc;
+    cnt += __popc(bal);
+  }
+  __syncwarp();
+  const int ih = lane >> 4, qi = lane & 15;
+  const int q = q0 + qi;
+  const bool qok = q < Q;
+  const cx<T>* Cq = C + (qok ? q : 0);
+  const int it0 = md + 4 * ih, it1 = it0 + 2;
+  cx<T> acc[8][2];
+#pragma unroll
+  for (int o = 0; o < 8; o++) acc[o][0] = acc[o][1] = mk<T>(0, 0);
+  if (cnt > 0) {
+    int e = lst[0];
+    size_t sb = (size_t)(e >> 8) * 8;
+    cx<T> n0 = Cq[(sb + it0) * Q], n1 = Cq[(sb + it1) * Q];
+    for (int i = 0; i < cnt; i++) {
+      const cx<T> c0 = n0, c1 = n1;
+      const int dc = e & 255;
+      if (i + 1 < cnt) {
+        e = lst[i + 1];
+        sb = (size_t)(e >> 8) * 8;
+        n0 = Cq[(sb + it0) * Q];
+        n1 = Cq[(sb + it1) * Q];
+      }
+      const int4 tv = *reinterpret_cast<const int4*>(s_tix + dc * 8);
+      const int tw[4] = {tv.x, tv.y, tv.z, tv.w};
+      cx<T> f[8];
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        int t = (o & 1) ? (tw[o >> 1] >> 16) : (tw[o >> 1] & 0xffff);
+        f[o] = sTL[t * SRW_QT + qi];
+      }
+#pragma unroll
+      for (int o = 0; o < 8; o++) {
+        acc[o][0] = cfma(c0, f[o], acc[o][0]);
+        acc[o][1] = cfma(c1, f[o], acc[o][1]);
+      }
+    }
+  }
+  const T wq = trf[qok ? q : 0];
+#pragma unroll
+  for (int o = 0; o < 8; o++) {
+    int b = __shfl_sync(0xffffffffu, sib, o);
+    if (b < 0 || !qok) continue;
+    cx<T>* out = D + (size_t)b * 8 * Q + q;
+    out[(size_t)it0 * Q] = acc[o][0] * wq;
+    out[(size_t)it1 * Q] = acc[o][1] * wq;
+    if (zero_other) {
+      out[(size_t)(it0 ^ 1) * Q] = mk<T>(0, 0);
+      out[(size_t)(it1 ^ 1) * Q] = mk<T>(0, 0);
+    }
+  }
+}
+
+template <typename T>
+static size_t sr_warp_bf_smem() {
+  return (size_t)344 * SRW_QT * sizeof(cx<T>) + (size_t)216 * 8 * sizeof(short) +
+         (size_t)SRW_GB * 216 * sizeof(int);
+}
+
 // Downward pass step 2 (translation_RR :600-655): D += D_parent * exp(-i k khat.(x_child - x_parent)).
 template <typename T>
 __global__ void k_rr(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
@@ -801,7 +903,15 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
                                  (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
                                  (cx<T>*)L.D); sie::count_launch();
-    } else if (c->sr_mode == 3 && L.nb < (1 << 23)) {  // source box and slot share one int
+    } else if (c->sr_mode == 4 && L.nb < (1 << 23)) {
+      dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
+      int nmed = L.only_k1 ? 1 : 2;
+      for (int md = 0; md < nmed; md++) {
+        k_sr_warp_bf<T><<<g, 32 * SRW_GB, sr_warp_bf_smem<T>(), st>>>(
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
+            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+      }
+    } else if (c->sr_mode >= 3 && L.nb < (1 << 23)) {  // source box and slot share one int
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
@@ -902,6 +1012,10 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)sr_warp_smem<double>()));
   SIE_CUDA(cudaFuncSetAttribute(k_sr_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sr_warp_smem<float>()));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_bf_smem<double>()));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_bf_smem<float>()));
   return SIE_OK;
 }
 
