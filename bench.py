@@ -108,15 +108,81 @@ def build_mesh(wl_name, seed):
                             thickness_wl=w["thickness_wl"])
 
 
-def matvec_bytes(g, nnz, Q, level_boxes, n_i4):
-    """Algorithmic bytes of one FP64 matvec (per right-hand side)."""
+def level_stats(g):
+    """Boxes per MLFMM level and I4 (far-interaction) pairs per level, from the leaf Morton
+    indices the library reports (the I4 rule: children of the parent's neighbours that are
+    not neighbours themselves)."""
+    _, _, leaf = g.tree()
+    out = []
+    for l in range(g.l_min, g.l_max + 1):
+        boxes = np.unique(leaf >> (3 * (g.l_max - l)))
+        coords = np.stack([demorton(boxes, l, k) for k in range(3)], axis=1)
+        have = {tuple(c) for c in coords}
+        n_i4 = 0
+        for c in coords:
+            p = c // 2
+            for d in np.ndindex(3, 3, 3):
+                pn = p + np.array(d) - 1
+                for ch in np.ndindex(2, 2, 2):
+                    s = 2 * pn + np.array(ch)
+                    if np.max(np.abs(s - c)) > 1 and tuple(s) in have:
+                        n_i4 += 1
+        out.append((l, len(boxes), n_i4))
+    return out
+
+
+def demorton(b, l, axis):
+    """Coordinate `axis` (0 = x, most significant) of Morton indices b at level l."""
+    v = np.zeros_like(b)
+    for bit in range(l):
+        v |= ((b >> (3 * bit + 2 - axis)) & 1) << bit
+    return v
+
+
+def matvec_algorithmic(g, Q):
+    """Algorithmic DRAM bytes of one FP64 matvec, and the FP64 flops of its SR step.
+    Bytes: near panels (a, b, d: 48 B per 2x2 block), radiation patterns read by the
+    aggregate and the receive, x in and y out, C and D of every level written and read.
+    The SR source coefficients are read from L2 (each level's C fits), so they are not
+    DRAM bytes.  SR flops: 4 complex multiply-adds = 32 real flops per (I4 pair,
+    direction, medium); medium 2 only on the leaf level (k2 complex)."""
     M, N, s = g.n_edges, g.n, 16
-    near = nnz * 3 * s + 2 * N * s              # a, b, d panels + x in + y out
-    rt = 2 * M * 4 * Q * s                      # radiation patterns, aggregate + receive
-    coeff = sum(b * 8 * Q * s * 4 for b in level_boxes)   # C, D written and read
-    sr_src = n_i4 * 8 * Q * s                   # SR source reads
-    tl = len(level_boxes) * 343 * 2 * Q * s
-    return dict(near=near, rt=rt, coeff=coeff, sr=sr_src, tl=tl, total=near + rt + coeff + sr_src + tl)
+    st = level_stats(g)
+    near = g.near_nnz * 3 * s
+    rt = 2 * M * 4 * Q * s
+    xy = 2 * N * s
+    coeff = sum(nb * 8 * Q * s * 4 for _, nb, _ in st)
+    sr_flops = sum(ni4 * Q * 32 * (2 if l == g.l_max else 1) for l, _, ni4 in st)
+    return dict(near=near, rt=rt, xy=xy, coeff=coeff, total=near + rt + xy + coeff, sr_flops=sr_flops,
+                levels=st)
+
+
+def fp64_dgemm_tflops(dev):
+    """FP64 denominator measured on this GPU: best of 5 torch float64 matmuls (cuBLAS DGEMM)."""
+    import torch
+    a = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
+    b = torch.randn(4096, 4096, dtype=torch.float64, device=dev)
+    best = 0.0
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * 4096 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
+def committed_traffic():
+    """DRAM bytes (read + write) of one matvec's kernels from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "matvec_dram_traffic_slab10.md")
+    try:
+        for line in open(p):
+            if line.startswith("total_dram_bytes_per_matvec:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def cpu_reference(V, T, matvecs_per_solve, threads, s_opt=250, budget_matvecs=2):
@@ -280,20 +346,33 @@ def main():
     Q = 2 * 19 * 19 + 2
     peak, peak_kind = peaks()
     phases = {k: tm[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
-    dom = max(phases, key=phases.get)
-    nnz = g.near_nnz
-    bytes_near = nnz * 3 * 16 + 2 * N * 16
-    bytes_rt = g.n_edges * 4 * Q * 16
-    dom_bytes = {"mv_near_ms": bytes_near, "mv_recv_ms": bytes_rt + 2 * N * 16,
-                 "mv_agg_ms": bytes_rt + N * 16}.get(dom, None)
-    roof = None
-    if dom_bytes:
-        ach = dom_bytes / (phases[dom] * 1e-3) / 1e9
-        roof = {"kernel": dom.replace("mv_", "").replace("_ms", ""), "bound": "hbm", "achieved": ach,
-                "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
-                "bytes_per_launch": dom_bytes, "launch_ms": phases[dom], "traffic": None}
-    mv_bytes = bytes_near + 2 * bytes_rt
-    mv_frac = mv_bytes / (tm["mv_total_ms"] * 1e-3) / 1e9 / peak
+    mvb = matvec_algorithmic(g, Q)
+    mv_ms = tm["mv_total_ms"]
+    ach = mvb["total"] / (mv_ms * 1e-3) / 1e9
+    # The hot-path unit is one MLFMM matvec (near panels + aggregate + SS + SR + RR +
+    # receive), HBM-bound as a whole; the per-phase entries give each kernel's own bound.
+    fp64_peak = fp64_dgemm_tflops(dev)
+    ph_rows = {
+        "near": ("hbm", mvb["near"], phases["mv_near_ms"]),
+        "aggregate": ("hbm", mvb["rt"] / 2 + N * 16, phases["mv_agg_ms"]),
+        "receive": ("hbm", mvb["rt"] / 2 + 2 * N * 16, phases["mv_recv_ms"]),
+        "sr": ("fp64", mvb["sr_flops"], phases["mv_sr_ms"]),
+    }
+    per_phase = {}
+    for k, (bound, units, ms) in ph_rows.items():
+        if bound == "hbm":
+            a = units / (ms * 1e-3) / 1e9
+            per_phase[k] = {"bound": "hbm", "achieved": a, "unit": "GB/s", "frac": a / peak, "ms": ms}
+        else:
+            a = units / (ms * 1e-3) / 1e12
+            per_phase[k] = {"bound": "fp64", "achieved": a, "unit": "TFLOP/s", "peak": fp64_peak,
+                            "peak_source": "measured here: torch float64 matmul (cuBLAS DGEMM) 4096^3",
+                            "frac": a / fp64_peak if fp64_peak else None, "ms": ms}
+    roof = {"kernel": "one MLFMM matvec (all phases)", "bound": "hbm", "achieved": ach, "peak": peak,
+            "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "bytes_per_launch": mvb["total"], "launch_ms": mv_ms, "traffic": committed_traffic(),
+            "per_phase": per_phase}
+    mv_frac = ach / peak
 
     # ---- CPU baseline: the oracle on the host cores (rank 0, N = 1)
     cpu = None

@@ -654,6 +654,132 @@ __global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_bf(
   }
 }
 
+// Sibling-group SR over the present siblings only.  The TL offset index is linear in the
+// two octants: t = T0(source slot) + off(target octant), with
+//   T0 = (3 - c_x - 2 d_x) 49 + (3 - c_y - 2 d_y) 7 + (3 - c_z - 2 d_z),
+//   off = o_x 49 + o_y 7 + o_z,
+// and TL is exactly zero on the 27 near offsets (they are excluded when TL is built), so
+// the loop over the NS present siblings needs neither a table nor a branch.  NS is a
+// template parameter; each warp dispatches on its group's sibling count.
+template <typename T, int NS>
+__device__ __forceinline__ void sr_ns_body(const int* lst, int cnt, const cx<T>* Cq, int it0, int it1,
+                                           const cx<T>* sTL, int qi, const int* sibc, const int* offc,
+                                           bool qok, T wq, int Q, int q, int zero_other,
+                                           cx<T>* __restrict__ D) {
+  int off[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) off[k] = offc[k] * SRW_QT + qi;
+  cx<T> acc[NS][2];
+#pragma unroll
+  for (int k = 0; k < NS; k++) acc[k][0] = acc[k][1] = mk<T>(0, 0);
+  if (cnt > 0) {
+    int e = lst[0];
+    size_t sb = (size_t)(e >> 9) * 8;
+    cx<T> n0 = Cq[(sb + it0) * Q], n1 = Cq[(sb + it1) * Q];
+    for (int i = 0; i < cnt; i++) {
+      const cx<T> c0 = n0, c1 = n1;
+      const int t0 = (e & 511) * SRW_QT;
+      if (i + 1 < cnt) {
+        e = lst[i + 1];
+        sb = (size_t)(e >> 9) * 8;
+        n0 = Cq[(sb + it0) * Q];
+        n1 = Cq[(sb + it1) * Q];
+      }
+      cx<T> f[NS];
+#pragma unroll
+      for (int k = 0; k < NS; k++) f[k] = sTL[t0 + off[k]];
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        acc[k][0] = cfma(c0, f[k], acc[k][0]);
+        acc[k][1] = cfma(c1, f[k], acc[k][1]);
+      }
+    }
+  }
+  if (!qok) return;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    cx<T>* out = D + (size_t)sibc[k] * 8 * Q + q;
+    out[(size_t)it0 * Q] = acc[k][0] * wq;
+    out[(size_t)it1 * Q] = acc[k][1] * wq;
+    if (zero_other) {
+      out[(size_t)(it0 ^ 1) * Q] = mk<T>(0, 0);
+      out[(size_t)(it1 ^ 1) * Q] = mk<T>(0, 0);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_ns(
+    const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
+    int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
+    int zero_other, cx<T>* __restrict__ D) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sTL = reinterpret_cast<cx<T>*>(smraw);                  // [343][SRW_QT]
+  int* s_list = reinterpret_cast<int*>(sTL + 343 * SRW_QT);      // [SRW_GB][216]
+  int* s_sib = s_list + SRW_GB * 216;                            // [SRW_GB][8] present boxes
+  int* s_off = s_sib + SRW_GB * 8;                               // [SRW_GB][8] their octant offsets
+  const int q0 = blockIdx.x * SRW_QT;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 343 * SRW_QT; i += blockDim.x) {
+    int t = i / SRW_QT, j = i - t * SRW_QT;
+    int q = q0 + j;
+    sTL[i] = (q < Q) ? tl[((size_t)t * 2 + md) * Q + q] : mk<T>(0, 0);
+  }
+  __syncthreads();
+  const int w = tid >> 5, lane = tid & 31;
+  const int g = blockIdx.y * SRW_GB + w;
+  if (g >= ngrp) return;
+  // present siblings, compacted in octant order
+  int sib = (lane < 8) ? grp_sib[(size_t)g * 8 + lane] : -1;
+  const unsigned smask = __ballot_sync(0xffffffffu, sib >= 0) & 0xffu;
+  const int ns = __popc(smask);
+  if (sib >= 0) {
+    int k = __popc(smask & ((1u << lane) - 1u));
+    s_sib[w * 8 + k] = sib;
+    s_off[w * 8 + k] = ((lane >> 2) & 1) * 49 + ((lane >> 1) & 1) * 7 + (lane & 1);
+  }
+  // present sources outside the parent itself: (box << 9) | T0
+  int* lst = s_list + w * 216;
+  int cnt = 0;
+  for (int base = 0; base < 216; base += 32) {
+    int dc = base + lane;
+    int d = dc >> 3, c = dc & 7;
+    int s = (dc < 216 && d != 13) ? grp_src[(size_t)g * 216 + dc] : -1;
+    unsigned bal = __ballot_sync(0xffffffffu, s >= 0);
+    if (s >= 0) {
+      int t0 = (3 - ((c >> 2) & 1) - 2 * (d / 9 - 1)) * 49 + (3 - ((c >> 1) & 1) - 2 * ((d / 3) % 3 - 1)) * 7 +
+               (3 - (c & 1) - 2 * (d % 3 - 1));
+      lst[cnt + __popc(bal & ((1u << lane) - 1u))] = (s << 9) | t0;
+    }
+    cnt += __popc(bal);
+  }
+  __syncwarp();
+  const int ih = lane >> 4, qi = lane & 15;
+  const int q = q0 + qi;
+  const bool qok = q < Q;
+  const cx<T>* Cq = C + (qok ? q : 0);
+  const int it0 = md + 4 * ih, it1 = it0 + 2;
+  const T wq = trf[qok ? q : 0];
+  const int* sibc = s_sib + w * 8;
+  const int* offc = s_off + w * 8;
+  switch (ns) {
+    case 1: sr_ns_body<T, 1>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 2: sr_ns_body<T, 2>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 3: sr_ns_body<T, 3>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 4: sr_ns_body<T, 4>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 5: sr_ns_body<T, 5>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 6: sr_ns_body<T, 6>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 7: sr_ns_body<T, 7>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 8: sr_ns_body<T, 8>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    default: break;
+  }
+}
+
+template <typename T>
+static size_t sr_warp_ns_smem() {
+  return (size_t)343 * SRW_QT * sizeof(cx<T>) + (size_t)SRW_GB * (216 + 16) * sizeof(int);
+}
+
 template <typename T>
 static size_t sr_warp_bf_smem() {
   return (size_t)344 * SRW_QT * sizeof(cx<T>) + (size_t)216 * 8 * sizeof(short) +
@@ -903,7 +1029,15 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
                                  (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
                                  (cx<T>*)L.D); sie::count_launch();
-    } else if (c->sr_mode == 4 && L.nb < (1 << 23)) {
+    } else if (c->sr_mode == 5 && L.nb < (1 << 22)) {  // source box and T0 share one int
+      dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
+      int nmed = L.only_k1 ? 1 : 2;
+      for (int md = 0; md < nmed; md++) {
+        k_sr_warp_ns<T><<<g, 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
+            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+      }
+    } else if (c->sr_mode >= 4 && L.nb < (1 << 23)) {
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
@@ -1014,6 +1148,10 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)sr_warp_smem<float>()));
   SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sr_warp_bf_smem<double>()));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_ns<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_ns_smem<double>()));
+  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_ns<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sr_warp_ns_smem<float>()));
   SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sr_warp_bf_smem<float>()));
   return SIE_OK;

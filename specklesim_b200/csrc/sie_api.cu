@@ -717,7 +717,7 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   // ICTF: D21 = -eta_a^2 D12 ; PMCHWT: D21 = -D12
   c->cfac = (cfg->formulation == SIE_ICTF) ? -(c->mt.eta_a * c->mt.eta_a) : mk<double>(-1.0, 0.0);
   // kernel variant of the SR translation (tuning knob; both give the same sums)
-  if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(4, atoi(e)));
+  if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(5, atoi(e)));
   if (const char* e = getenv("SIE_RECV_MODE")) c->recv_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));

@@ -153,8 +153,9 @@ struct sie_ctx {
   // SR kernel: 0 one thread per (target box, direction); 1 sibling groups;
   // 2 sibling groups with the translation table staged in shared memory;
   // 3 one warp per sibling group (compacted source lists, prefetched coefficients);
-  // 4 the same without branches in the sibling loop (zero TL row for near pairs)
-  int sr_mode = 4;
+  // 4 the same without branches in the sibling loop (zero TL row for near pairs);
+  // 5 present siblings only, TL index linear in the two octants
+  int sr_mode = 5;
   // receive: 0 one block per leaf box; 1 chunks of <= 32 edges with pre-combined D
   int recv_mode = 1;
   // aggregate: 0 one thread per (box, direction); 1 eight edge groups per block

@@ -112,7 +112,7 @@ def test_sr_kernel_variants_agree(gpu_lib, monkeypatch):
     V, T = P.slab(cells=24, length_wl=6.0, seed=3)
     x = P.random_x(2 * 7000, seed=1)
     ys = []
-    for mode in ("0", "1", "2", "3", "4"):
+    for mode in ("0", "1", "2", "3", "4", "5"):
         monkeypatch.setenv("SIE_SR_MODE", mode)
         g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=100).setup()
         ys.append(g.matvec(x[:g.n]))
