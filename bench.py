@@ -394,7 +394,8 @@ def main():
                 "precision": "fp64", "solver": f"GMRES(IMGS) restart {args.restart}, tol {args.tol}",
                 "iterations": iters, "matvecs_per_solve": mvs, "converged": bool(conv),
                 "backward_error": be, "max_iterations": args.max_iterations, "setup_s": setup_s,
-                "near_nnz_blocks": nnz, "matvec_ms": tm["mv_total_ms"], "matvec_phases_ms": phases,
+                "near_nnz_blocks": g.near_nnz, "matvec_ms": tm["mv_total_ms"], "matvec_phases_ms": phases,
+                "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],
                 "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
                 "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
                 "l2": "inputs > L2 (near panels and radiation patterns are GBs)",
