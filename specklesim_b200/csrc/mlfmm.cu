@@ -11,6 +11,8 @@
 //   0,1 = theta J (k1,k2)   2,3 = theta M (k1,k2)
 //   4,5 = phi   J (k1,k2)   6,7 = phi   M (k1,k2)
 // (a_nm(1..4), b_nm(1..4) of lib_ml_fmm_coefficient).  Medium = item & 1.
+#include <algorithm>
+
 #include "sie_internal.h"
 
 namespace sie {
@@ -991,6 +993,20 @@ int far_build_tables(sie_ctx* c, const double* d_boxc) {
   return SIE_OK;
 }
 
+// Tables of the precision the pass runs in.
+template <typename T> static const cx<T>* tlp(const Level& L);
+template <> const zc* tlp<double>(const Level& L) { return L.tl; }
+template <> const cc* tlp<float>(const Level& L) { return L.tl32; }
+template <typename T> static const cx<T>* php_up(const Level& L);
+template <> const zc* php_up<double>(const Level& L) { return L.ph_up; }
+template <> const cc* php_up<float>(const Level& L) { return L.ph_up32; }
+template <typename T> static const cx<T>* php_dn(const Level& L);
+template <> const zc* php_dn<double>(const Level& L) { return L.ph_dn; }
+template <> const cc* php_dn<float>(const Level& L) { return L.ph_dn32; }
+template <typename T> static const T* trfp(const sie_ctx* c);
+template <> const double* trfp<double>(const sie_ctx* c) { return c->d_trf; }
+template <> const float* trfp<float>(const sie_ctx* c) { return c->d_trf32; }
+
 template <typename T>
 int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
                  cudaEvent_t* ev) {
@@ -1017,7 +1033,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     Level& Ch = c->lv[l + 1];
     dim3 g((Q + thr - 1) / thr, P.nb);
     k_ss<T><<<g, thr, 0, st>>>((const cx<T>*)Ch.C, P.ch_ptr, P.ch_idx, P.ch_oct,
-                               (const cx<T>*)Ch.ph_up, Q, k2c ? 1 : 2, (cx<T>*)P.C); sie::count_launch();
+                               php_up<T>(Ch), Q, k2c ? 1 : 2, (cx<T>*)P.C); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[2], st);
@@ -1027,31 +1043,31 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     if (c->sr_mode == 0) {
       dim3 g((Q + thr - 1) / thr, L.nb);
       k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
-                                 (const cx<T>*)L.tl, (const T*)c->d_trf, Q, L.only_k1 ? 1 : 2,
+                                 tlp<T>(L), trfp<T>(c), Q, L.only_k1 ? 1 : 2,
                                  (cx<T>*)L.D); sie::count_launch();
     } else if (c->sr_mode == 5 && L.nb < (1 << 22)) {  // source box and T0 share one int
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
         k_sr_warp_ns<T><<<g, 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
-            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
-            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
+            trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
     } else if (c->sr_mode >= 4 && L.nb < (1 << 23)) {
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
         k_sr_warp_bf<T><<<g, 32 * SRW_GB, sr_warp_bf_smem<T>(), st>>>(
-            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
-            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
+            trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
     } else if (c->sr_mode >= 3 && L.nb < (1 << 23)) {  // source box and slot share one int
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
         k_sr_warp<T><<<g, 32 * SRW_GB, sr_warp_smem<T>(), st>>>(
-            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, (const cx<T>*)L.tl,
-            (const T*)c->d_trf, Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
+            trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
     } else if (c->sr_mode == 2) {
       dim3 g((Q + SR_TQ - 1) / SR_TQ, (L.ngrp + SR_GB - 1) / SR_GB);
@@ -1059,8 +1075,8 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
         k_sr_group_tl<T><<<g, SR_TQ * SR_GB, smem, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
-                                                          L.ngrp, (const cx<T>*)L.tl,
-                                                          (const T*)c->d_trf, Q, md, nmed == 1,
+                                                          L.ngrp, tlp<T>(L),
+                                                          trfp<T>(c), Q, md, nmed == 1,
                                                           (cx<T>*)L.D); sie::count_launch();
       }
     } else {
@@ -1069,7 +1085,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       for (int md = 0; md < nmed; md++)
         for (int i0 = 0; i0 < 4; i0 += 2) {
           k_sr_group<T, 2><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
-                                              (const cx<T>*)L.tl, (const T*)c->d_trf, Q, md, i0,
+                                              tlp<T>(L), trfp<T>(c), Q, md, i0,
                                               nmed == 1, (cx<T>*)L.D); sie::count_launch();
         }
     }
@@ -1084,7 +1100,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     int nmed = (k2c && l < L1) ? 1 : 2;
     // D_k2 of the parent is zero when its level only carries k1
     if (k2c) nmed = 1;
-    k_rr<T><<<g, thr, 0, st>>>((const cx<T>*)P.D, L.parent, L.oct, (const cx<T>*)L.ph_dn, Q, nmed,
+    k_rr<T><<<g, thr, 0, st>>>((const cx<T>*)P.D, L.parent, L.oct, php_dn<T>(L), Q, nmed,
                                (cx<T>*)L.D); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
@@ -1125,34 +1141,81 @@ int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* e
   return far_matvec_t<double>(c, c->d_rt, x, y, st, ev);
 }
 
+int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev) {
+  return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev);
+}
+
+__global__ void k_trf_f32(const double* a, float* b, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+// complex64 copies of everything the FP32 product reads (once per context).  The
+// coefficient buffers C and D of every level are shared with the FP64 product: a
+// complex64 pass uses the first half of each.
+int make_f32_tables(sie_ctx* c) {
+  if (c->f32_ready) return SIE_OK;
+  cudaStream_t st = c->stream;
+  size_t nnz = (size_t)std::max<long long>(c->near.nnz, 1);
+  SIE_CUDA(cudaMalloc(&c->d_na32, nnz * sizeof(cc)));
+  SIE_CUDA(cudaMalloc(&c->d_nb32, nnz * sizeof(cc)));
+  SIE_CUDA(cudaMalloc(&c->d_nd32, nnz * sizeof(cc)));
+  SIE_TRY(near_to_f32(c));
+  if (!c->cfg.dense) {
+    int Q = c->Q;
+    size_t nrt = (size_t)c->M * 4 * Q;
+    SIE_CUDA(cudaMalloc(&c->d_rt32, nrt * sizeof(cc)));
+    SIE_TRY(to_c64(c->d_rt, c->d_rt32, nrt, st));
+    SIE_CUDA(cudaMalloc(&c->d_trf32, (size_t)Q * sizeof(float)));
+    k_trf_f32<<<(Q + 255) / 256, 256, 0, st>>>(c->d_trf, c->d_trf32, Q); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+    for (int l = c->l_min; l <= c->l_max; l++) {
+      Level& L = c->lv[l];
+      size_t ntl = (size_t)343 * 2 * Q, nph = (size_t)8 * 2 * Q;
+      SIE_CUDA(cudaMalloc(&L.tl32, ntl * sizeof(cc)));
+      SIE_CUDA(cudaMalloc(&L.ph_up32, nph * sizeof(cc)));
+      SIE_CUDA(cudaMalloc(&L.ph_dn32, nph * sizeof(cc)));
+      SIE_TRY(to_c64(L.tl, L.tl32, ntl, st));
+      SIE_TRY(to_c64(L.ph_up, L.ph_up32, nph, st));
+      SIE_TRY(to_c64(L.ph_dn, L.ph_dn32, nph, st));
+    }
+  }
+  size_t n = (size_t)2 * c->M;
+  SIE_CUDA(cudaMalloc(&c->d_xi32, n * sizeof(cc)));
+  SIE_CUDA(cudaMalloc(&c->d_yi32, n * sizeof(cc)));
+  SIE_CUDA(cudaStreamSynchronize(st));
+  c->f32_ready = true;
+  return SIE_OK;
+}
+
 int far_prepare_kernels(sie_ctx* c) {
   size_t smem64 = (size_t)8 * c->Q * sizeof(zc);
   size_t smem32 = (size_t)8 * c->Q * sizeof(cc);
-  SIE_CUDA(cudaFuncSetAttribute(k_receive<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_receive<double>,
                                 (int)smem64));
-  SIE_CUDA(cudaFuncSetAttribute(k_receive<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_receive<float>,
                                 (int)smem32));
-  SIE_CUDA(cudaFuncSetAttribute(k_receive_chunk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_receive_chunk<double>,
                                 (int)smem64));
-  SIE_CUDA(cudaFuncSetAttribute(k_receive_chunk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_receive_chunk<float>,
                                 (int)smem32));
   size_t sr64 = (size_t)343 * SR_TQ * sizeof(zc) + (size_t)SR_GB * (216 + 8) * sizeof(int);
   size_t sr32 = (size_t)343 * SR_TQ * sizeof(cc) + (size_t)SR_GB * (216 + 8) * sizeof(int);
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_group_tl<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_group_tl<double>,
                                 (int)sr64));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_group_tl<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_group_tl<float>,
                                 (int)sr32));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp<double>,
                                 (int)sr_warp_smem<double>()));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp<float>,
                                 (int)sr_warp_smem<float>()));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp_bf<double>,
                                 (int)sr_warp_bf_smem<double>()));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_ns<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp_ns<double>,
                                 (int)sr_warp_ns_smem<double>()));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_ns<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp_ns<float>,
                                 (int)sr_warp_ns_smem<float>()));
-  SIE_CUDA(cudaFuncSetAttribute(k_sr_warp_bf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SIE_CUDA(raise_smem(k_sr_warp_bf<float>,
                                 (int)sr_warp_bf_smem<float>()));
   return SIE_OK;
 }

@@ -636,16 +636,12 @@ static size_t near_panel_smem(const sie_ctx* c) {
 
 int near_prepare_kernels(sie_ctx* c) {
   if (size_t s = near_panel_smem<double>(c)) {
-    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<double, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
-    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<double, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+    SIE_CUDA(raise_smem(k_near_panel<double, true>, s));
+    SIE_CUDA(raise_smem(k_near_panel<double, false>, s));
   }
   if (size_t s = near_panel_smem<float>(c)) {
-    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<float, true>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
-    SIE_CUDA(cudaFuncSetAttribute(k_near_panel<float, false>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+    SIE_CUDA(raise_smem(k_near_panel<float, true>, s));
+    SIE_CUDA(raise_smem(k_near_panel<float, false>, s));
   }
   return SIE_OK;
 }

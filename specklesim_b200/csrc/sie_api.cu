@@ -589,6 +589,29 @@ static int ensure_work(sie_ctx* c, int nrhs) {
 using namespace sie;
 
 // Device matvec on internal-layout vectors: y = Z x (one right-hand side per call).
+// Phase times of the product just queued (events 0, 6, 1..5 recorded by the passes).
+static void record_phase_times(sie_ctx* c, cudaStream_t st) {
+  cudaEventRecord(c->ev[7], st);
+  cudaEventSynchronize(c->ev[7]);
+  float a = 0;
+  cudaEventElapsedTime(&a, c->ev[0], c->ev[7]);
+  c->tm.mv_total_ms = a;
+  cudaEventElapsedTime(&a, c->ev[0], c->ev[6]);
+  c->tm.mv_near_ms = a;
+  if (!c->cfg.dense) {
+    cudaEventElapsedTime(&a, c->ev[6], c->ev[1]);
+    c->tm.mv_agg_ms = a;
+    cudaEventElapsedTime(&a, c->ev[1], c->ev[2]);
+    c->tm.mv_ss_ms = a;
+    cudaEventElapsedTime(&a, c->ev[2], c->ev[3]);
+    c->tm.mv_sr_ms = a;
+    cudaEventElapsedTime(&a, c->ev[3], c->ev[4]);
+    c->tm.mv_rr_ms = a;
+    cudaEventElapsedTime(&a, c->ev[4], c->ev[5]);
+    c->tm.mv_recv_ms = a;
+  }
+}
+
 int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed) {
   for (int r = 0; r < nrhs; r++) {
     const zc* x = xi + (size_t)r * 2 * c->M;
@@ -597,28 +620,17 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
     SIE_TRY(near_matvec64(c, x, y, 1, false, st));
     if (timed) cudaEventRecord(c->ev[6], st);
     if (!c->cfg.dense) SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr));
-    if (timed) {
-      cudaEventRecord(c->ev[7], st);
-      cudaEventSynchronize(c->ev[7]);
-      float a = 0;
-      cudaEventElapsedTime(&a, c->ev[0], c->ev[7]);
-      c->tm.mv_total_ms = a;
-      cudaEventElapsedTime(&a, c->ev[0], c->ev[6]);
-      c->tm.mv_near_ms = a;
-      if (!c->cfg.dense) {
-        cudaEventElapsedTime(&a, c->ev[6], c->ev[1]);
-        c->tm.mv_agg_ms = a;
-        cudaEventElapsedTime(&a, c->ev[1], c->ev[2]);
-        c->tm.mv_ss_ms = a;
-        cudaEventElapsedTime(&a, c->ev[2], c->ev[3]);
-        c->tm.mv_sr_ms = a;
-        cudaEventElapsedTime(&a, c->ev[3], c->ev[4]);
-        c->tm.mv_rr_ms = a;
-        cudaEventElapsedTime(&a, c->ev[4], c->ev[5]);
-        c->tm.mv_recv_ms = a;
-      }
-    }
+    if (timed) record_phase_times(c, st);
   }
+  return SIE_OK;
+}
+
+int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool timed) {
+  if (timed) cudaEventRecord(c->ev[0], st);
+  SIE_TRY(near_matvec32(c, x, y, 1, false, st));
+  if (timed) cudaEventRecord(c->ev[6], st);
+  if (!c->cfg.dense) SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr));
+  if (timed) record_phase_times(c, st);
   return SIE_OK;
 }
 
@@ -853,7 +865,18 @@ int sie_matvec_device(sie_ctx* c, const double* d_x, double* d_y, int nrhs, int 
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   SIE_TRY(ensure_work(c, nrhs));
   SIE_TRY(gather_ext_to_int(c, (const zc*)d_x, c->d_xi, nrhs, st));
-  SIE_TRY(sie_internal_matvec(c, c->d_xi, c->d_yi, nrhs, st, true));
+  if (precision == SIE_MIXED) {
+    // complex64 product: tables and vectors in FP32, result widened back to FP64
+    SIE_TRY(make_f32_tables(c));
+    size_t n = (size_t)2 * c->M;
+    for (int r = 0; r < nrhs; r++) {
+      SIE_TRY(to_c64(c->d_xi + r * n, c->d_xi32, n, st));
+      SIE_TRY(sie_internal_matvec32(c, c->d_xi32, c->d_yi32, st, r == nrhs - 1));
+      SIE_TRY(to_c128(c->d_yi32, c->d_yi + r * n, n, st));
+    }
+  } else {
+    SIE_TRY(sie_internal_matvec(c, c->d_xi, c->d_yi, nrhs, st, true));
+  }
   SIE_TRY(scatter_int_to_ext(c, c->d_yi, (zc*)d_y, nrhs, st));
   SIE_CUDA(cudaStreamSynchronize(st));
   return SIE_OK;
@@ -1133,11 +1156,11 @@ int sie_free(sie_ctx* c) {
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
-                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_xi, c->d_yi, c->d_gm};
+                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {
-    void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.i4_ptr, L.i4_src, L.i4_off,
+    void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.tl32, L.ph_up32, L.ph_dn32, L.i4_ptr, L.i4_src, L.i4_off,
                   L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src};
     for (void* p : lp)
       if (p) cudaFree(p);

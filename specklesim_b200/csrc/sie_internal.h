@@ -33,6 +33,18 @@ inline cudaError_t h2d(void* dst, const void* src, size_t bytes) {
   return cudaStreamSynchronize(cudaStreamLegacy);
 }
 
+// Allow kernel fn up to `bytes` of dynamic shared memory.  The limit is a property of the
+// function for the whole process, shared by every context, so it is only ever raised:
+// lowering it for one mesh would make another context's launches fail.
+template <typename F>
+inline cudaError_t raise_smem(F* fn, size_t bytes) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, (const void*)fn);
+  if (e != cudaSuccess) return e;
+  if ((int)bytes <= a.maxDynamicSharedSizeBytes) return cudaSuccess;
+  return cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 #define SIE_TRY(x)               \
   do {                           \
     int _r = (x);                \
@@ -113,6 +125,10 @@ struct Level {
   int ngrp = 0;
   int* grp_sib = nullptr;     // ngrp x 8 box indices (-1: absent)
   int* grp_src = nullptr;     // ngrp x 27 x 8 candidate source box indices (-1: absent)
+  // complex64 copies for the FP32 matvec (made on first use)
+  cc* tl32 = nullptr;
+  cc* ph_up32 = nullptr;
+  cc* ph_dn32 = nullptr;
 };
 
 struct Timings {
@@ -194,6 +210,10 @@ struct sie_ctx {
   double* d_trf = nullptr;
   zc* d_rt = nullptr;             // internal edge x 4 x Q
   cc* d_rt32 = nullptr;
+  float* d_trf32 = nullptr;
+  bool f32_ready = false;         // complex64 tables made
+  cc* d_xi32 = nullptr;           // FP32 work vectors (internal layout)
+  cc* d_yi32 = nullptr;
   // work vectors (internal layout, interleaved J/M per edge)
   zc* d_xi = nullptr;
   zc* d_yi = nullptr;
@@ -201,6 +221,10 @@ struct sie_ctx {
   // solver workspace
   void* d_gm = nullptr;
   size_t gm_bytes = 0;
+  void* d_gm32 = nullptr;         // inner FP32 GMRES workspace (mixed precision)
+  size_t gm32_bytes = 0;
+  void* d_gmz = nullptr;          // flexible GMRES directions Z (mixed precision)
+  size_t gmz_bytes = 0;
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
   unsigned ar_epoch = 1;          // launch counter tagging the Arnoldi exchange rounds
@@ -222,7 +246,12 @@ int near_to_f32(sie_ctx* c);
 int near_prepare_kernels(sie_ctx* c);
 int far_build_tables(sie_ctx* c, const double* d_boxc);
 int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev);
+int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev);
 int far_prepare_kernels(sie_ctx* c);
+// complex64 copies of the near panels, radiation patterns, TL and phase tables
+int make_f32_tables(sie_ctx* c);
+int to_c64(const zc* in, cc* out, size_t n, cudaStream_t st);
+int to_c128(const cc* in, zc* out, size_t n, cudaStream_t st);
 int gather_ext_to_int(sie_ctx* c, const zc* ext, zc* in, int nrhs, cudaStream_t st);
 int scatter_int_to_ext(sie_ctx* c, const zc* in, zc* ext, int nrhs, cudaStream_t st);
 int phase_tables(sie_ctx* c, Level& L, int l);
@@ -232,6 +261,9 @@ int rhs_planewave_dev(sie_ctx* c, const double* d_k, const double* d_E, int nrhs
 int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
                  double* d_I);
 int gmres_solve(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
+int fgmres_mixed(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
 }  // namespace sie
 
 int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed);
+// the same product with complex64 tables and vectors
+int sie_internal_matvec32(sie_ctx* c, const cc* xi, cc* yi, cudaStream_t st, bool timed);

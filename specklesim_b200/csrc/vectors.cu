@@ -1,6 +1,7 @@
 // Layout conversion, right-hand sides, Jacobi diagonal, translation phases and
 // the scattered-field evaluation.
 #include <vector>
+#include <algorithm>
 
 #include "sie_internal.h"
 
@@ -227,6 +228,28 @@ __global__ void k_field(const FnD* fn, const zc* x, int M, Material mt, const do
 int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
                  double* d_I) {
   k_field<<<npts, 256, 0, c->stream>>>(c->d_fn, d_x_int, c->M, c->mt, d_pts, npts, d_E, d_H, d_I); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+__global__ void k_z2c(const zc* a, cc* b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = mk<float>((float)a[i].re, (float)a[i].im);
+}
+__global__ void k_c2z(const cc* a, zc* b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = mk<double>((double)a[i].re, (double)a[i].im);
+}
+
+int to_c64(const zc* in, cc* out, size_t n, cudaStream_t st) {
+  unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_z2c<<<std::max(g, 1u), 256, 0, st>>>(in, out, n); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+int to_c128(const cc* in, zc* out, size_t n, cudaStream_t st) {
+  unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_c2z<<<std::max(g, 1u), 256, 0, st>>>(in, out, n); sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }

@@ -259,3 +259,49 @@ def test_error_paths(gpu_lib):
     with pytest.raises(SieError) as e:
         Sie(V, T2, P.WL, P.EPS_METAL)
     assert e.value.code == _lib.SIE_ERR_MESH
+
+
+def test_mixed_matvec_close_to_fp64(metal_pair):
+    """The complex64 product stays within the FP32 rounding amplified by the cancellation
+    of the K = 19 translations (~1e4 on these 0.75-lambda boxes, measured 4e-5)."""
+    _, _, g = metal_pair
+    x = P.random_x(g.n, seed=5)
+    y64 = g.matvec(x)
+    y32 = g.matvec(x, precision="mixed")
+    assert rel(y32, y64) < 2e-4, rel(y32, y64)
+
+
+def test_mixed_solve_matches_fp64_farfield(slab_pair):
+    """FP64 flexible GMRES around FP32 inner GMRES reaches the FP64 tolerance on the true
+    residual; its currents and far-field intensities agree with the plain FP64 solve."""
+    from specklesim_b200 import incidence
+    _, _, g = slab_pair
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b = g.rhs_planewave(k, E)
+    x64, s64 = g.solve(b, restart=50, max_iterations=2000, tolerance=1e-8)
+    xm, sm = g.solve(b, restart=10, max_iterations=60, tolerance=1e-8, precision="mixed",
+                     inner_restart=30, inner_tolerance=1e-2)
+    assert sm["converged"] and sm["backward_error_true"] <= 1e-8
+    assert sm["inner_iterations"] > sm["iterations"]
+    th = np.linspace(0.05, 1.4, 9)
+    pts = 5.0 * np.stack([np.sin(th), 0 * th, np.cos(th)], axis=1)
+    I64 = g.farfield(x64, pts)[2]
+    Im = g.farfield(xm, pts)[2]
+    assert rel(Im, I64) < 1e-5, rel(Im, I64)
+    assert rel(xm, x64) < 1e-5, rel(xm, x64)
+
+
+def test_later_small_context_keeps_earlier_context_working(gpu_lib):
+    """Kernel launch limits are process-wide: setting up a small mesh after a large one
+    must not break the large context's products."""
+    from specklesim_b200 import Sie
+    V, T = P.slab(cells=24, length_wl=6.0, seed=3)
+    big = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=100).setup()
+    x = P.random_x(big.n, seed=2)
+    y0 = big.matvec(x)
+    Vs, Ts = P.sphere(1)
+    small = Sie(Vs, Ts, P.WL, P.EPS_METAL, tree_s_opt=20).setup()
+    small.matvec(P.random_x(small.n, seed=3))
+    assert np.array_equal(big.matvec(x), y0)
+    small.close()
+    big.close()
