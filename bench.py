@@ -173,6 +173,50 @@ def fp64_dgemm_tflops(dev):
     return best
 
 
+EPS_CONVERGING = 2.25 - 0.01j
+
+
+def hemisphere_grid(n=128, r=5.0):
+    """The 128 x 128 (theta, phi) grid over the upper hemisphere at r = 5 m."""
+    th = (np.arange(n) + 0.5) * (0.5 * np.pi / n)
+    ph = (np.arange(n) + 0.5) * (2 * np.pi / n)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    return r * np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], axis=-1).reshape(-1, 3)
+
+
+def mixed_vs_fp64(V, T, tol):
+    """Solves/s of the mixed-precision solver (FP64 flexible GMRES around FP32 GMRES)
+    against the plain FP64 GMRES, both to the same backward error, and the relative error
+    of the mixed far-field intensity on the 128 x 128 hemisphere grid.  The slab mesh of
+    the workload with a dielectric body: the metallic ICTF system stalls in both
+    precisions, so it gives no equal-accuracy comparison."""
+    from specklesim_b200 import Sie, incidence
+    g = Sie(V, T, WL, EPS_CONVERGING, tree_s_opt=250, truncation_number=19).setup()
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b = g.rhs_planewave(k, E)
+    pts = hemisphere_grid()
+    x64, s64 = g.solve(b, restart=50, max_iterations=4000, tolerance=tol, raise_on_noconv=False)
+    xm, sm = g.solve(b, restart=10, max_iterations=100, tolerance=tol, precision="mixed",
+                     inner_restart=30, inner_tolerance=1e-2, raise_on_noconv=False)
+    xm, sm = g.solve(b, restart=10, max_iterations=100, tolerance=tol, precision="mixed",
+                     inner_restart=30, inner_tolerance=1e-2, raise_on_noconv=False)
+    I64 = g.farfield(x64, pts)[2]
+    Im = g.farfield(xm, pts)[2]
+    g.close()
+    return {
+        "workload": f"same slab mesh, eps = {EPS_CONVERGING} (converging), tolerance {tol}",
+        "fp64": {"solves_per_s": 1.0 / s64["seconds"], "iterations": s64["iterations"],
+                 "backward_error": s64["backward_error_true"], "converged": bool(s64["converged"])},
+        "mixed": {"solves_per_s": 1.0 / sm["seconds"], "outer_iterations": sm["iterations"],
+                  "inner_iterations": sm["inner_iterations"], "backward_error": sm["backward_error_true"],
+                  "converged": bool(sm["converged"]), "inner": "GMRES(30) FP32 to 1e-2, outer FGMRES(10) FP64"},
+        "speedup": s64["seconds"] / sm["seconds"],
+        "farfield_rel_err_vs_fp64": float(np.linalg.norm(Im - I64) / np.linalg.norm(I64)),
+        "currents_rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
+        "farfield_points": int(pts.shape[0]),
+    }
+
+
 def committed_traffic():
     """DRAM bytes (read + write) of one matvec's kernels from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "matvec_dram_traffic_slab10.md")
@@ -220,6 +264,7 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--max-iterations", type=int, default=650)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--reference-matvecs-per-solve", type=int, default=0)
     args = ap.parse_args()
 
@@ -374,6 +419,11 @@ def main():
             "per_phase": per_phase}
     mv_frac = ach / peak
 
+    # ---- mixed precision against plain FP64 at equal tolerance (rank 0, N = 1)
+    mixed = None
+    if rank == 0 and world == 1 and not args.no_mixed:
+        mixed = mixed_vs_fp64(V, T, args.tol)
+
     # ---- CPU baseline: the oracle on the host cores (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -398,6 +448,7 @@ def main():
                 "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],
                 "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
                 "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
+                "mixed_vs_fp64": mixed,
                 "l2": "inputs > L2 (near panels and radiation patterns are GBs)",
             },
             "roofline": roof,
