@@ -305,3 +305,41 @@ def test_later_small_context_keeps_earlier_context_working(gpu_lib):
     assert np.array_equal(big.matvec(x), y0)
     small.close()
     big.close()
+
+
+@pytest.mark.parametrize("formulation,ngp", [("PMCHWT", 3), ("ICTF", 7), ("PMCHWT", 7)])
+def test_other_formulations_and_rules(oracle_lib, gpu_lib, formulation, ngp):
+    """PMCHWT (with the 12-point edge-adjacent Kt of edge_adjacent_tri) and the 7-point
+    rule of the small-sphere configuration: blocks and matvec against the oracle."""
+    from specklesim_b200 import Sie
+    V, T = P.slab(cells=16, length_wl=4.0, seed=3)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, formulation=formulation, ngp=ngp,
+                          tree_s_opt=60, threads=8)
+    o.tree()
+    o.setup_fmm()
+    g = Sie(V, T, P.WL, P.EPS_METAL, formulation=formulation, ngp=ngp, tree_s_opt=60).setup()
+    rng = np.random.default_rng(1)
+    m, n = _pairs(o, rng, 200)
+    a, b = g.blocks(m, n), o.blocks(m, n)
+    scale = np.abs(b).max(axis=1, keepdims=True)
+    assert (np.abs(a - b) / scale).max() < 1e-9
+    x = P.random_x(o.N, seed=6)
+    assert rel(g.matvec(x), o.matvec(x)) < 1e-9
+    g.close()
+
+
+def test_dense_small_sphere_ngp7_solves_like_dense_oracle(oracle_lib, gpu_lib):
+    """The small-sphere configuration in miniature: dense path (no MLFMM), 7-point rule,
+    metal, GMRES to 1e-6 against a direct solve of the oracle's dense matrix."""
+    from specklesim_b200 import Sie, incidence
+    V, T = P.sphere(2)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, ngp=7)
+    Z = o.dense()
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b = o.rhs(k, E)
+    x_direct = np.linalg.solve(Z, b)
+    g = Sie(V, T, P.WL, P.EPS_METAL, ngp=7, dense=True).setup()
+    x, st = g.solve(b, restart=50, max_iterations=2000, tolerance=1e-10, raise_on_noconv=False)
+    assert st["backward_error_true"] < 1e-8
+    assert rel(x, x_direct) < 1e-6, rel(x, x_direct)
+    g.close()
