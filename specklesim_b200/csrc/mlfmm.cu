@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_bf(
 // and TL is exactly zero on the 27 near offsets (they are excluded when TL is built), so
 // the loop over the NS present siblings needs neither a table nor a branch.  NS is a
 // template parameter; each warp dispatches on its group's sibling count.
-template <typename T, int NS>
+template <typename T, int NS, int PD>
 __device__ __forceinline__ void sr_ns_body(const int* lst, int cnt, const cx<T>* Cq, int it0, int it1,
                                            const cx<T>* sTL, int qi, const int* sibc, const int* offc,
                                            bool qok, T wq, int Q, int q, int zero_other,
@@ -674,27 +674,36 @@ __device__ __forceinline__ void sr_ns_body(const int* lst, int cnt, const cx<T>*
   cx<T> acc[NS][2];
 #pragma unroll
   for (int k = 0; k < NS; k++) acc[k][0] = acc[k][1] = mk<T>(0, 0);
-  if (cnt > 0) {
-    int e = lst[0];
-    size_t sb = (size_t)(e >> 9) * 8;
-    cx<T> n0 = Cq[(sb + it0) * Q], n1 = Cq[(sb + it1) * Q];
-    for (int i = 0; i < cnt; i++) {
-      const cx<T> c0 = n0, c1 = n1;
-      const int t0 = (e & 511) * SRW_QT;
-      if (i + 1 < cnt) {
-        e = lst[i + 1];
-        sb = (size_t)(e >> 9) * 8;
-        n0 = Cq[(sb + it0) * Q];
-        n1 = Cq[(sb + it1) * Q];
-      }
-      cx<T> f[NS];
+  // coefficients of the next PD sources stay in flight in registers
+  cx<T> p0[PD], p1[PD];
 #pragma unroll
-      for (int k = 0; k < NS; k++) f[k] = sTL[t0 + off[k]];
+  for (int d = 0; d < PD; d++) {
+    if (d < cnt) {
+      size_t sb = (size_t)(lst[d] >> 9) * 8;
+      p0[d] = Cq[(sb + it0) * Q];
+      p1[d] = Cq[(sb + it1) * Q];
+    }
+  }
+  for (int i = 0; i < cnt; i++) {
+    const cx<T> c0 = p0[0], c1 = p1[0];
+    const int t0 = (lst[i] & 511) * SRW_QT;
 #pragma unroll
-      for (int k = 0; k < NS; k++) {
-        acc[k][0] = cfma(c0, f[k], acc[k][0]);
-        acc[k][1] = cfma(c1, f[k], acc[k][1]);
-      }
+    for (int d = 0; d + 1 < PD; d++) {
+      p0[d] = p0[d + 1];
+      p1[d] = p1[d + 1];
+    }
+    if (i + PD < cnt) {
+      size_t sb = (size_t)(lst[i + PD] >> 9) * 8;
+      p0[PD - 1] = Cq[(sb + it0) * Q];
+      p1[PD - 1] = Cq[(sb + it1) * Q];
+    }
+    cx<T> f[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) f[k] = sTL[t0 + off[k]];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      acc[k][0] = cfma(c0, f[k], acc[k][0]);
+      acc[k][1] = cfma(c1, f[k], acc[k][1]);
     }
   }
   if (!qok) return;
@@ -710,7 +719,7 @@ __device__ __forceinline__ void sr_ns_body(const int* lst, int cnt, const cx<T>*
   }
 }
 
-template <typename T>
+template <typename T, int PD>
 __global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_ns(
     const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
     int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
@@ -765,14 +774,14 @@ __global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_warp_ns(
   const int* sibc = s_sib + w * 8;
   const int* offc = s_off + w * 8;
   switch (ns) {
-    case 1: sr_ns_body<T, 1>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 2: sr_ns_body<T, 2>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 3: sr_ns_body<T, 3>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 4: sr_ns_body<T, 4>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 5: sr_ns_body<T, 5>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 6: sr_ns_body<T, 6>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 7: sr_ns_body<T, 7>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
-    case 8: sr_ns_body<T, 8>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 1: sr_ns_body<T, 1, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 2: sr_ns_body<T, 2, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 3: sr_ns_body<T, 3, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 4: sr_ns_body<T, 4, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 5: sr_ns_body<T, 5, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 6: sr_ns_body<T, 6, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 7: sr_ns_body<T, 7, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
+    case 8: sr_ns_body<T, 8, PD>(lst, cnt, Cq, it0, it1, sTL, qi, sibc, offc, qok, wq, Q, q, zero_other, D); break;
     default: break;
   }
 }
@@ -781,6 +790,7 @@ template <typename T>
 static size_t sr_warp_ns_smem() {
   return (size_t)343 * SRW_QT * sizeof(cx<T>) + (size_t)SRW_GB * (216 + 16) * sizeof(int);
 }
+
 
 template <typename T>
 static size_t sr_warp_bf_smem() {
@@ -1049,7 +1059,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
       int nmed = L.only_k1 ? 1 : 2;
       for (int md = 0; md < nmed; md++) {
-        k_sr_warp_ns<T><<<g, 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
+        k_sr_warp_ns<T, 1><<<g, 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
             (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
             trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
@@ -1211,9 +1221,9 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)sr_warp_smem<float>()));
   SIE_CUDA(raise_smem(k_sr_warp_bf<double>,
                                 (int)sr_warp_bf_smem<double>()));
-  SIE_CUDA(raise_smem(k_sr_warp_ns<double>,
+  SIE_CUDA(raise_smem(k_sr_warp_ns<double, 1>,
                                 (int)sr_warp_ns_smem<double>()));
-  SIE_CUDA(raise_smem(k_sr_warp_ns<float>,
+  SIE_CUDA(raise_smem(k_sr_warp_ns<float, 1>,
                                 (int)sr_warp_ns_smem<float>()));
   SIE_CUDA(raise_smem(k_sr_warp_bf<float>,
                                 (int)sr_warp_bf_smem<float>()));
