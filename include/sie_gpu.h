@@ -130,6 +130,12 @@ int sie_solve(sie_ctx* ctx, const double* b, double* x, int nrhs, const sie_solv
 int sie_solve_device(sie_ctx* ctx, const double* d_b, double* d_x, int nrhs,
                      const sie_solver_cfg* cfg, sie_stats* stats);
 
+/* Direct solve of the dense system, the reference's normal solver
+ * (lib_sie_tri_solver_normal_I, src/lib_sie_tri_solver_normal.f90:64-217, with ZGESV in
+ * solver_LU, src/lib_sie_math.f90:649-676).  Needs a context set up with dense = 1; the
+ * LU factors are made on the first call and kept for later right-hand sides. */
+int sie_solve_direct(sie_ctx* ctx, const double* b, double* x, int nrhs);
+
 /* Left Jacobi preconditioner, lib_sie_ml_fmm_preconditioner_left
  * (src/lib_sie_tri_mlfmm_interface.f90:323-339): v2 = v1 / diag. */
 int sie_precondition_left(sie_ctx* ctx, const double* v1, double* v2);

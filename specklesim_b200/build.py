@@ -44,7 +44,7 @@ def build(force=False, verbose=False):
     if not force and not needs_build():
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + sources()
+    cmd = [_nvcc()] + NVCC_FLAGS + ["-o", tmp] + sources() + ["-lcusolver"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

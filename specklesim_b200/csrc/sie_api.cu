@@ -1156,7 +1156,7 @@ int sie_free(sie_ctx* c) {
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
-                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz};
+                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {

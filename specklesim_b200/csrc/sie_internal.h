@@ -225,6 +225,8 @@ struct sie_ctx {
   size_t gm32_bytes = 0;
   void* d_gmz = nullptr;          // flexible GMRES directions Z (mixed precision)
   size_t gmz_bytes = 0;
+  void* d_lu = nullptr;           // dense LU factors (column-major N x N, internal order)
+  int* d_piv = nullptr;           // pivots (N) + info
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
   unsigned ar_epoch = 1;          // launch counter tagging the Arnoldi exchange rounds

@@ -114,6 +114,16 @@ class Sie:
         x = x.T
         return (x[:, 0], st[0]) if b.ndim == 1 else (x, st)
 
+    def solve_direct(self, b):
+        """LU solve of the dense system (context made with dense=True)."""
+        b = _lib.as_c128(b)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bb = np.ascontiguousarray(b.reshape(self.n, nrhs).T)
+        x = np.zeros_like(bb)
+        check(self._lib.sie_solve_direct(self._h, dptr(bb.view(np.float64)), dptr(x.view(np.float64)), nrhs))
+        x = x.T
+        return x[:, 0] if b.ndim == 1 else x
+
     def precondition_left(self, v1):
         v1 = _lib.as_c128(v1)
         v2 = np.zeros_like(v1)

@@ -46,3 +46,27 @@ def test_pp_tt_roundtrip(tmp_path):
     V2, T2 = mesh.read_pp_tt(pp, tt)
     assert np.array_equal(T, T2) and np.allclose(V, V2, rtol=0, atol=0)
     assert open(tt).readline().split() == [str(i + 1) for i in T[0]]
+
+
+def test_currents_file_format_and_roundtrip(tmp_path):
+    from specklesim_b200 import io
+    assert io.fortran_es(1.234567890123e-3) == " 1.234567890123E-03"
+    assert io.fortran_es(-9.5e-104) == "-9.500000000000-104"
+    assert io.fortran_es(0.0) == " 0.000000000000E+00"
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(12) * 1e-3 + 1j * rng.standard_normal(12)
+    x[3] = 1e-120 - 2e-130j
+    p = tmp_path / "Result_SEH_tri_ICTF.txt"
+    io.write_currents(p, 80, x)
+    lines = p.read_text().splitlines()
+    assert len(lines) == 2 + 12 and len(lines[2]) == 2 * (19 + 5)
+    n_el, m, y = io.read_currents(p)
+    assert n_el == 80 and m == 6
+    assert np.allclose(y, x, rtol=1e-12, atol=0)
+
+
+def test_iteration_log_format(tmp_path):
+    from specklesim_b200 import io
+    p = tmp_path / "iteration_error.txt"
+    io.write_iteration_log(p, [0.5, 1.25e-3])
+    assert p.read_text().splitlines()[1] == "         2      1.250000000000E-03     "
