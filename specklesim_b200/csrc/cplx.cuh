@@ -75,6 +75,24 @@ SIE_HD cx<T> cfma_conj(cx<T> a, cx<T> b, cx<T> c) {
   return mk<T>(fma(a.re, b.re, fma(a.im, b.im, c.re)), fma(a.re, b.im, fma(-a.im, b.re, c.im)));
 }
 
+// Loads of data that is streamed once per product (near panels, radiation patterns):
+// marked evict-first in L2 and not kept in L1, so they do not push the level
+// coefficients, which the translation kernels re-read many times, out of L2.
+__device__ __forceinline__ unsigned long long l2_evict_first_policy() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ cx<double> ld_stream(const cx<double>* a, unsigned long long pol) {
+  double r, i;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+               : "=d"(r), "=d"(i)
+               : "l"(a), "l"(pol));
+  return mk<double>(r, i);
+}
+// complex64 streams: a plain load measured faster (8-byte accesses)
+__device__ __forceinline__ cx<float> ld_stream(const cx<float>* a, unsigned long long) { return *a; }
+
 // widen to complex128
 SIE_HD zc cvt_z(zc a) { return a; }
 SIE_HD zc cvt_z(cc a) { return mk<double>((double)a.re, (double)a.im); }

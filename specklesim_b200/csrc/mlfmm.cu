@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(256) k_aggregate_eg(const cx<T>* __restrict__ 
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = blockIdx.x * 32 + lane;
   const bool qok = q < Q;
+  const unsigned long long pol = l2_evict_first_policy();
   const int f = box_first[b], cnt = box_cnt[b];
   cx<T> acc[8];
 #pragma unroll
@@ -238,7 +239,8 @@ __global__ void __launch_bounds__(256) k_aggregate_eg(const cx<T>* __restrict__ 
     for (int e = f + w; e < f + cnt; e += 8) {
       const cx<T>* r = rt + (size_t)e * 4 * Q + q;
       cx<T> xe = x[2 * e], xh = x[2 * e + 1];
-      cx<T> ra1 = r[0], rb1 = r[Q], ra2 = r[2 * Q], rb2 = r[3 * Q];
+      cx<T> ra1 = ld_stream(r, pol), rb1 = ld_stream(r + Q, pol), ra2 = ld_stream(r + 2 * Q, pol),
+            rb2 = ld_stream(r + 3 * Q, pol);
       acc[0] = cfma_conj(ra1, xe, acc[0]);
       acc[1] = cfma_conj(ra2, xe, acc[1]);
       acc[2] = cfma_conj(ra1, xh, acc[2]);
@@ -915,6 +917,7 @@ __global__ void __launch_bounds__(256, 2) k_receive_chunk(const cx<T>* __restric
     }
   }
   __syncthreads();
+  const unsigned long long pol = l2_evict_first_policy();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int e0 = f + 2 * warp; e0 < f + cnt; e0 += 16) {
     const bool two = e0 + 1 < f + cnt;
@@ -930,8 +933,8 @@ __global__ void __launch_bounds__(256, 2) k_receive_chunk(const cx<T>* __restric
       cx<T> a0[4], a1[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        a0[k] = r0[k * Q + q];
-        a1[k] = r1[k * Q + q];
+        a0[k] = ld_stream(r0 + k * Q + q, pol);
+        a1[k] = ld_stream(r1 + k * Q + q, pol);
       }
 #pragma unroll
       for (int md = 0; md < 2; md++) {

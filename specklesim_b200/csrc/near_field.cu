@@ -577,6 +577,7 @@ __global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __
   const int A = ch.x, f = ch.y, cnt = ch.z;
   const int nc = P.ncols[A];
   const long long base = P.base[A] + (long long)(f - P.box_first[A]) * nc;
+  const unsigned long long pol = l2_evict_first_policy();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k0 = P.nbr_ptr[A], k1 = P.nbr_ptr[A + 1];
   for (int r = 0; r < nrhs; r++) {
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __
       cx<T> sJ = mk<T>(0, 0), sM = mk<T>(0, 0), tM = mk<T>(0, 0);
 #pragma unroll 4
       for (int j = lane; j < nc; j += 32) {
-        cx<T> a = va[o + j], b = vb[o + j], d = vd_[o + j];
+        cx<T> a = ld_stream(va + o + j, pol), b = ld_stream(vb + o + j, pol), d = ld_stream(vd_ + o + j, pol);
         cx<T> xj = xs[2 * j], xm = xs[2 * j + 1];
         sJ = cfma(a, xj, sJ);
         sJ = cfma(b, xm, sJ);
