@@ -24,9 +24,9 @@ namespace sie {
 // projected on theta-hat (a_nm) and phi-hat (b_nm).
 __global__ void k_rt(const FnD* fn, const double* boxc, const int* edge_box, int M, Rule R,
                      zc k1, zc k2, const double* khat, const double* tth, const double* tph, int Q,
-                     zc* rt) {
+                     zc* rt, int e0) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  int e = blockIdx.y;
+  int e = e0 + blockIdx.y;
   if (q >= Q || e >= M) return;
   int b = edge_box[e];
   vd Rc = mkv<double>(boxc[3 * b], boxc[3 * b + 1], boxc[3 * b + 2]);
@@ -982,9 +982,12 @@ int far_build_tables(sie_ctx* c, const double* d_boxc) {
   int Q = c->Q, K = c->K, M = c->M;
   // radiation patterns
   {
-    dim3 g((Q + 127) / 128, M);
-    k_rt<<<g, 128, 0, st>>>(c->d_fn, d_boxc, c->d_edge_box, M, c->R, c->mt.k1, c->mt.k2, c->d_khat,
-                            c->d_tth, c->d_tph, Q, c->d_rt); sie::count_launch();
+    // one launch per 65,535 edges (the grid's y limit)
+    for (int e0 = 0; e0 < M; e0 += 65535) {
+      dim3 g((Q + 127) / 128, std::min(65535, M - e0));
+      k_rt<<<g, 128, 0, st>>>(c->d_fn, d_boxc, c->d_edge_box, M, c->R, c->mt.k1, c->mt.k2, c->d_khat,
+                              c->d_tth, c->d_tph, Q, c->d_rt, e0); sie::count_launch();
+    }
     SIE_CUDA(cudaGetLastError());
   }
   // TL tables per level
