@@ -1025,7 +1025,7 @@ template <> const float* trfp<float>(const sie_ctx* c) { return c->d_trf32; }
 
 template <typename T>
 int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
-                 cudaEvent_t* ev) {
+                 cudaEvent_t* ev, cudaEvent_t wait_recv) {
   int Q = c->Q;
   int L0 = c->l_min, L1 = c->l_max;
   bool k2c = c->mt.k2.im != 0.0;
@@ -1121,6 +1121,8 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[4], st);
+  // the receive adds into y, which the near product (possibly on another stream) writes
+  if (wait_recv) SIE_CUDA(cudaStreamWaitEvent(st, wait_recv, 0));
   // final far summation
   {
     Level& L = c->lv[L1];
@@ -1153,12 +1155,14 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
   return SIE_OK;
 }
 
-int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev) {
-  return far_matvec_t<double>(c, c->d_rt, x, y, st, ev);
+int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev,
+                 cudaEvent_t wait_recv) {
+  return far_matvec_t<double>(c, c->d_rt, x, y, st, ev, wait_recv);
 }
 
-int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev) {
-  return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev);
+int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
+                 cudaEvent_t wait_recv) {
+  return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev, wait_recv);
 }
 
 __global__ void k_trf_f32(const double* a, float* b, int n) {

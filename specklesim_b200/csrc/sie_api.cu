@@ -599,7 +599,7 @@ static void record_phase_times(sie_ctx* c, cudaStream_t st) {
   cudaEventElapsedTime(&a, c->ev[0], c->ev[6]);
   c->tm.mv_near_ms = a;
   if (!c->cfg.dense) {
-    cudaEventElapsedTime(&a, c->ev[6], c->ev[1]);
+    cudaEventElapsedTime(&a, c->overlap_near ? c->ev[0] : c->ev[6], c->ev[1]);
     c->tm.mv_agg_ms = a;
     cudaEventElapsedTime(&a, c->ev[1], c->ev[2]);
     c->tm.mv_ss_ms = a;
@@ -617,9 +617,20 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
     const zc* x = xi + (size_t)r * 2 * c->M;
     zc* y = yi + (size_t)r * 2 * c->M;
     if (timed) cudaEventRecord(c->ev[0], st);
-    SIE_TRY(near_matvec64(c, x, y, 1, false, st));
-    if (timed) cudaEventRecord(c->ev[6], st);
-    if (!c->cfg.dense) SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr));
+    if (!c->cfg.dense && c->overlap_near) {
+      // the HBM-bound near product on stream2 overlaps the latency-bound translations;
+      // the receive waits for it because both write y
+      SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+      SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+      SIE_TRY(near_matvec64(c, x, y, 1, false, c->stream2));
+      if (timed) cudaEventRecord(c->ev[6], c->stream2);
+      SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+      SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr, c->ev_join));
+    } else {
+      SIE_TRY(near_matvec64(c, x, y, 1, false, st));
+      if (timed) cudaEventRecord(c->ev[6], st);
+      if (!c->cfg.dense) SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr));
+    }
     if (timed) record_phase_times(c, st);
   }
   return SIE_OK;
@@ -627,9 +638,18 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
 
 int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool timed) {
   if (timed) cudaEventRecord(c->ev[0], st);
-  SIE_TRY(near_matvec32(c, x, y, 1, false, st));
-  if (timed) cudaEventRecord(c->ev[6], st);
-  if (!c->cfg.dense) SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr));
+  if (!c->cfg.dense && c->overlap_near) {
+    SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+    SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+    SIE_TRY(near_matvec32(c, x, y, 1, false, c->stream2));
+    if (timed) cudaEventRecord(c->ev[6], c->stream2);
+    SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+    SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr, c->ev_join));
+  } else {
+    SIE_TRY(near_matvec32(c, x, y, 1, false, st));
+    if (timed) cudaEventRecord(c->ev[6], st);
+    if (!c->cfg.dense) SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr));
+  }
   if (timed) record_phase_times(c, st);
   return SIE_OK;
 }
@@ -722,6 +742,8 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess)
     return cleanup(fail(SIE_ERR_CUDA, "stream"));
   for (int i = 0; i < 16; i++) cudaEventCreate(&c->ev[i]);
+  cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
   int r = build_mesh(c);
   if (r != SIE_OK) return cleanup(r);
   r = build_tree(c);
@@ -734,6 +756,7 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_ARNOLDI_MODE")) c->arnoldi_mode = std::max(0, std::min(2, atoi(e)));
+  if (const char* e = getenv("SIE_OVERLAP")) c->overlap_near = atoi(e) != 0;
   *out = c;
   return SIE_OK;
 }
@@ -1168,6 +1191,8 @@ int sie_free(sie_ctx* c) {
   if (c->h_gm) cudaFreeHost(c->h_gm);
   for (int i = 0; i < 16; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   else if (c->stream) cudaStreamDestroy(c->stream);
   if (c->stream2) cudaStreamDestroy(c->stream2);

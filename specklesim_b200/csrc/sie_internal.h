@@ -148,6 +148,9 @@ struct sie_ctx {
   cudaStream_t stream = nullptr, stream2 = nullptr;
   cudaStream_t own_stream = nullptr;  // the library's stream when the caller set its own
   cudaEvent_t ev[16];
+  // the near-field product runs on stream2 next to the far-field passes
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int overlap_near = 1;
 
   // mesh (reference order)
   int nv = 0, nt = 0, M = 0;
@@ -247,8 +250,11 @@ int near_matvec32(sie_ctx* c, const cc* x, cc* y, int nrhs, bool accum, cudaStre
 int near_to_f32(sie_ctx* c);
 int near_prepare_kernels(sie_ctx* c);
 int far_build_tables(sie_ctx* c, const double* d_boxc);
-int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev);
-int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev);
+// far-field passes; wait_recv (may be null) is waited for before the receive adds into y
+int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev,
+                 cudaEvent_t wait_recv = nullptr);
+int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
+                 cudaEvent_t wait_recv = nullptr);
 int far_prepare_kernels(sie_ctx* c);
 // complex64 copies of the near panels, radiation patterns, TL and phase tables
 int make_f32_tables(sie_ctx* c);
