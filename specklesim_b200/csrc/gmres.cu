@@ -1134,18 +1134,30 @@ static int inner_gmres32(sie_ctx* c, Gm32& g, const cc* r, cc* z, double tol, in
   }
   k_scale_t<float><<<RB, RT_, 0, s>>>(r, g.V, n, 1.0 / beta); sie::count_launch();
   k_hinit<<<(m + 1 + 127) / 128, 128, 0, s>>>(g.H, m, beta); sie::count_launch();
+  // As in the FP64 solver, the scalars of step j go to pinned slot j & 1 and are read
+  // one step late, so the GPU never waits for the host; a step queued after the one
+  // that meets the tolerance is not used by the update below.
+  GmState* slots = (GmState*)c->h_gm;
   int k = 0;
-  for (int j = 0; j < m; j++) {
+  auto check = [&](int p, bool& stop) -> int {
+    SIE_CUDA(cudaEventSynchronize(c->ev[14 + (p & 1)]));
+    const GmState hp = slots[p & 1];
+    if (hp.bar_err) return fail(SIE_ERR_CUDA, "inner GMRES: a grid barrier timed out");
+    if (!std::isfinite(hp.dnormw) || !std::isfinite(hp.bea))
+      return fail(SIE_ERR_NONFINITE, "inner GMRES: non-finite Arnoldi vector");
+    k = p + 1;
+    stop = hp.bea <= tol || hp.dnormw == 0.0;
+    return SIE_OK;
+  };
+  bool stop = false;
+  for (int j = 0; j < m && !stop; j++) {
     SIE_TRY(sie_internal_matvec32(c, g.V + (size_t)j * ld, g.w, s, false));
     mvs++;
     SIE_TRY(arnoldi_launch32(g, j, beta, s));
-    SIE_CUDA(cudaMemcpyAsync(&h, g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
-    SIE_CUDA(cudaStreamSynchronize(s));
-    if (h.bar_err) return fail(SIE_ERR_CUDA, "inner GMRES: a grid barrier timed out");
-    if (!std::isfinite(h.dnormw) || !std::isfinite(h.bea))
-      return fail(SIE_ERR_NONFINITE, "inner GMRES: non-finite Arnoldi vector");
-    k = j + 1;
-    if (h.bea <= tol || h.dnormw == 0.0) break;
+    SIE_CUDA(cudaMemcpyAsync(&slots[j & 1], g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
+    SIE_CUDA(cudaEventRecord(c->ev[14 + (j & 1)], s));
+    if (j > 0) SIE_TRY(check(j - 1, stop));
+    if (!stop && j == m - 1) SIE_TRY(check(j, stop));
   }
   k_trsv<<<1, 1, 0, s>>>(g.H, m, k, g.y); sie::count_launch();
   k_combine_t<float><<<RB, RT_, 0, s>>>(g.V, ld, g.y, k, n, z); sie::count_launch();
