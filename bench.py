@@ -85,18 +85,20 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
+        sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in self.rows:
             try:
                 sm.append(float(r[0]))
                 mx.append(float(r[1]))
+                pw.append(float(r[2]))
                 for n, v in zip(names, r[3:7]):
                     if v.lower() == "active":
                         reasons.add(n)
             except Exception:
                 pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w": statistics.median(pw) if pw else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -365,13 +367,14 @@ def main():
     dp = C.POINTER(C.c_double)
     barrier()
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        rc = lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg), stats)
-        if rc != _lib.SIE_ERR_NOCONV:
-            _lib.check(rc)
-    e3.record(stream)
-    barrier()
+    with ClockSampler(local) as clk_e2e:
+        e2.record(stream)
+        for _ in range(args.steps):
+            rc = lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg), stats)
+            if rc != _lib.SIE_ERR_NOCONV:
+                _lib.check(rc)
+        e3.record(stream)
+        barrier()
     t_e2e = e2.elapsed_time(e3) / 1000.0
     if world > 1:
         tt = torch.tensor([t_e2e], device=dev)
@@ -453,7 +456,8 @@ def main():
             },
             "roofline": roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16,
+                    "clocks": clk_e2e.summary()},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }

@@ -572,6 +572,23 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Device staging for the host-buffer entry points (input and output halves), kept per
+// context and only grown: a cudaMalloc/cudaFree pair per call costs a device-wide
+// synchronisation and, measured on the slab workload, up to ~0.1 s per solve.
+static int io_buffers(sie_ctx* c, size_t bytes, zc** in, zc** out) {
+  size_t half = (bytes + 255) & ~(size_t)255;
+  if (c->io_bytes < 2 * half) {
+    if (c->d_io) cudaFree(c->d_io);
+    c->d_io = nullptr;
+    c->io_bytes = 0;
+    SIE_CUDA(cudaMalloc(&c->d_io, 2 * half));
+    c->io_bytes = 2 * half;
+  }
+  *in = (zc*)c->d_io;
+  *out = (zc*)((char*)c->d_io + c->io_bytes / 2);
+  return SIE_OK;
+}
+
 static int ensure_work(sie_ctx* c, int nrhs) {
   if ((size_t)nrhs <= c->work_rhs) return SIE_OK;
   if (c->d_xi) cudaFree(c->d_xi);
@@ -913,8 +930,7 @@ int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) 
   for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
     if (!std::isfinite(x[i])) return fail(SIE_ERR_NONFINITE, "sie_matvec: non-finite input");
   zc *dx = nullptr, *dy = nullptr;
-  SIE_CUDA(cudaMalloc(&dx, bytes));
-  SIE_CUDA(cudaMalloc(&dy, bytes));
+  SIE_TRY(io_buffers(c, bytes, &dx, &dy));
   int r = SIE_OK;
   if (cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
     r = fail(SIE_ERR_CUDA, "sie_matvec: H2D copy");
@@ -922,8 +938,6 @@ int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) 
   if (r == SIE_OK && (cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
                       cudaStreamSynchronize(c->stream) != cudaSuccess))
     r = fail(SIE_ERR_CUDA, "sie_matvec: D2H copy");
-  cudaFree(dx);
-  cudaFree(dy);
   return r;
 }
 
@@ -999,8 +1013,7 @@ int sie_solve(sie_ctx* c, const double* b, double* x, int nrhs, const sie_solver
     if (!std::isfinite(b[i])) return fail(SIE_ERR_NONFINITE, "sie_solve: non-finite right-hand side");
   size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
   zc *db = nullptr, *dx = nullptr;
-  SIE_CUDA(cudaMalloc(&db, bytes));
-  SIE_CUDA(cudaMalloc(&dx, bytes));
+  SIE_TRY(io_buffers(c, bytes, &db, &dx));
   SIE_CUDA(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, c->stream));
   if (cfg->use_initial_guess) SIE_CUDA(cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream));
   int r = sie_solve_device(c, (const double*)db, (double*)dx, nrhs, cfg, stats);
@@ -1008,8 +1021,6 @@ int sie_solve(sie_ctx* c, const double* b, double* x, int nrhs, const sie_solver
       (cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
        cudaStreamSynchronize(c->stream) != cudaSuccess))
     r = fail(SIE_ERR_CUDA, "sie_solve: D2H copy");
-  cudaFree(db);
-  cudaFree(dx);
   return r;
 }
 
@@ -1179,7 +1190,7 @@ int sie_free(sie_ctx* c) {
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
-                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv};
+                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {

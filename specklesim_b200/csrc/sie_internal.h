@@ -228,6 +228,8 @@ struct sie_ctx {
   size_t gm32_bytes = 0;
   void* d_gmz = nullptr;          // flexible GMRES directions Z (mixed precision)
   size_t gmz_bytes = 0;
+  void* d_io = nullptr;           // staging of the host-buffer entry points (two halves)
+  size_t io_bytes = 0;
   void* d_lu = nullptr;           // dense LU factors (column-major N x N, internal order)
   int* d_piv = nullptr;           // pivots (N) + info
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
