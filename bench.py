@@ -393,7 +393,21 @@ def main():
     tm = g.timings()
     Q = 2 * 19 * 19 + 2
     peak, peak_kind = peaks()
-    phases = {k: tm[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
+    # The product above runs the near panels on a second stream beside the translations,
+    # so its per-phase events overlap. Each phase's own duration comes from a second
+    # context on the same mesh whose product runs the phases one after another.
+    os.environ["SIE_OVERLAP"] = "0"
+    try:
+        gs = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local).setup()
+    finally:
+        del os.environ["SIE_OVERLAP"]
+    for _ in range(4):
+        _lib.check(lib.sie_matvec_device(gs._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
+                                         C.c_void_p(stream.cuda_stream)))
+    tms = gs.timings()
+    gs.close()
+    phases = {k: tms[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
+    phases["serial_total_ms"] = tms["mv_total_ms"]
     mvb = matvec_algorithmic(g, Q)
     mv_ms = tm["mv_total_ms"]
     ach = mvb["total"] / (mv_ms * 1e-3) / 1e9
@@ -447,7 +461,9 @@ def main():
                 "precision": "fp64", "solver": f"GMRES(IMGS) restart {args.restart}, tol {args.tol}",
                 "iterations": iters, "matvecs_per_solve": mvs, "converged": bool(conv),
                 "backward_error": be, "max_iterations": args.max_iterations, "setup_s": setup_s,
-                "near_nnz_blocks": g.near_nnz, "matvec_ms": tm["mv_total_ms"], "matvec_phases_ms": phases,
+                "near_nnz_blocks": g.near_nnz, "matvec_ms": tm["mv_total_ms"],
+                "matvec_phases_ms": phases, "matvec_phases_note": "phases timed one after another; "
+                "matvec_ms runs the near panels concurrently with the translations",
                 "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],
                 "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
                 "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),

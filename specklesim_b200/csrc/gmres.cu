@@ -1284,4 +1284,468 @@ int fgmres_mixed(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solver_cf
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched mixed-precision solve: R systems Z x_r = b_r of one matrix advance in lockstep,
+// so each product is one batched matvec that reads the near panels, radiation patterns
+// and translation tables once for all R vectors.  Outer FP64 flexible GMRES and inner
+// complex64 GMRES as in fgmres_mixed.  Each new Krylov vector of the batch is
+// orthogonalised by classical Gram-Schmidt applied twice (CGS2): one reduction per pass
+// for all basis columns at once, where modified Gram-Schmidt needs one per column.  The
+// inner cycle runs its fixed number of steps with no host synchronisation; a system that
+// meets the inner tolerance earlier keeps the solution of that step.  Per-system
+// scalars live on the device; the host reads them once per outer step.
+
+static const int BNB = 64;     // blocks per system in the batched vector kernels
+static const int BJG = 8;      // basis columns per reduction sweep
+static const int BJMAX = 64;   // largest basis (restart + 1) of the batched solver
+
+struct BState {
+  double beta;    // norm of the cycle's starting vector
+  double bn;      // norm the Arnoldi residual estimate is relative to
+  double bea;     // that estimate at the last step the system took
+  double dnormw;
+  int k;          // steps of the cycle that the update uses
+  int done;       // met its tolerance, broke down, or was frozen at the cycle start
+  int pad[2];
+};
+
+// Block sums of BJG complex values (256 threads); the results land in out[0 .. BJG-1].
+__device__ void block_sum_g(zc* v, zc* sh, zc* out) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < BJG; j++) v[j] = warp_sum(v[j]);
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < BJG; j++) sh[w * BJG + j] = v[j];
+  __syncthreads();
+  if (threadIdx.x < BJG) {
+    zc s = mk<double>(0, 0);
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sh[k * BJG + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// Partial dots <V_j, w> (j < ncol) over this block's elements of one system.
+template <typename VT>
+__device__ void bdots_chunk(const cx<VT>* Vr, size_t ldj, const cx<VT>* wr, int n, int ncol, zc* pr) {
+  __shared__ zc sh[8 * BJG], res[BJG];
+  for (int j0 = 0; j0 < ncol; j0 += BJG) {
+    zc acc[BJG];
+#pragma unroll
+    for (int jj = 0; jj < BJG; jj++) acc[jj] = mk<double>(0, 0);
+    for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) {
+      const zc wi = cvt_z(wr[i]);
+#pragma unroll
+      for (int jj = 0; jj < BJG; jj++)
+        if (j0 + jj < ncol) acc[jj] = cfma_conj(cvt_z(Vr[(size_t)(j0 + jj) * ldj + i]), wi, acc[jj]);
+    }
+    block_sum_g(acc, sh, res);
+    if (threadIdx.x < BJG && j0 + (int)threadIdx.x < ncol) pr[j0 + threadIdx.x] = res[threadIdx.x];
+  }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(RT_) k_bdots(const cx<VT>* __restrict__ V, size_t ldj,
+                                               const cx<VT>* __restrict__ w, int n, int ncol, zc* part,
+                                               int ldp) {
+  const int r = blockIdx.y;
+  bdots_chunk<VT>(V + (size_t)r * n, ldj, w + (size_t)r * n, n, ncol,
+                  part + ((size_t)r * BNB + blockIdx.x) * ldp);
+}
+
+// One CGS pass: h = the sum of the partial dots in a fixed order (every block of the
+// system forms the same h), H(:, hcol) = h (add = 0) or += h, w -= V h; then the partial
+// dots of the new w (next = 0) or its partial squared norm (next = 1).
+template <typename VT>
+__global__ void __launch_bounds__(RT_) k_bupdate(const cx<VT>* __restrict__ V, size_t ldj, cx<VT>* w, int n,
+                                                 int ncol, const zc* part_in, zc* part_out, int ldp, zc* H,
+                                                 int m, int hcol, int add, int next) {
+  __shared__ zc h[BJMAX];
+  const int r = blockIdx.y;
+  for (int j = threadIdx.x; j < ncol; j += blockDim.x) {
+    zc s = mk<double>(0, 0);
+    const zc* p = part_in + (size_t)r * BNB * ldp + j;
+    for (int b = 0; b < BNB; b++) s += p[(size_t)b * ldp];
+    h[j] = s;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    zc* Hc = H + (size_t)r * (m + 1) * (m + 1) + (size_t)hcol * (m + 1);
+    for (int j = threadIdx.x; j < ncol; j += blockDim.x) Hc[j] = add ? Hc[j] + h[j] : h[j];
+  }
+  cx<VT>* wr = w + (size_t)r * n;
+  const cx<VT>* Vr = V + (size_t)r * n;
+  double nrm = 0;
+  for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) {
+    zc wi = cvt_z(wr[i]);
+    for (int j = 0; j < ncol; j++) wi = wi - h[j] * cvt_z(Vr[(size_t)j * ldj + i]);
+    const cx<VT> wn = narrow<VT>(wi);
+    wr[i] = wn;
+    nrm += cabs2(cvt_z(wn));
+  }
+  zc* pr = part_out + ((size_t)r * BNB + blockIdx.x) * ldp;
+  if (next) {
+    const zc v = block_sum(mk<double>(nrm, 0));
+    if (threadIdx.x == 0) pr[0] = v;
+    return;
+  }
+  // each thread reads back only the elements it wrote above
+  bdots_chunk<VT>(Vr, ldj, wr, n, ncol, pr);
+}
+
+// Partial squared norms of the R vectors a_r.
+template <typename VT>
+__global__ void __launch_bounds__(RT_) k_bnorm(const cx<VT>* a, int n, zc* part, int ldp) {
+  const int r = blockIdx.y;
+  const cx<VT>* ar = a + (size_t)r * n;
+  double s = 0;
+  for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) s += cabs2(cvt_z(ar[i]));
+  const zc v = block_sum(mk<double>(s, 0));
+  if (threadIdx.x == 0) part[((size_t)r * BNB + blockIdx.x) * ldp] = v;
+}
+
+// Start of a cycle: beta_r = ||src_r||, V_0 = src_r / beta_r, H(:, m) = beta_r e_1.
+// set_bn: the Arnoldi estimate is relative to beta (inner solve); otherwise to the bn the
+// state already holds.  frozen[r] != 0 marks a system that takes no step in this cycle.
+template <typename VS, typename VT>
+__global__ void __launch_bounds__(RT_) k_binit(const cx<VS>* src, int n, const zc* part, int ldp,
+                                               cx<VT>* V0, zc* H, int m, BState* st, int set_bn,
+                                               const int* frozen) {
+  __shared__ double sb;
+  const int r = blockIdx.y;
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int b = 0; b < BNB; b++) s += part[((size_t)r * BNB + b) * ldp].re;
+    sb = sqrt(s);
+  }
+  __syncthreads();
+  const double beta = sb;
+  const double inv = beta > 0 ? 1.0 / beta : 0.0;
+  const cx<VS>* sr = src + (size_t)r * n;
+  cx<VT>* vr = V0 + (size_t)r * n;
+  for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) vr[i] = narrow<VT>(cvt_z(sr[i]) * inv);
+  if (blockIdx.x == 0) {
+    zc* Hr = H + (size_t)r * (m + 1) * (m + 1);
+    for (int i = threadIdx.x; i <= m; i += blockDim.x) Hr[HIDX(i, m)] = mk<double>(i == 0 ? beta : 0.0, 0.0);
+    if (threadIdx.x == 0) {
+      BState& S = st[r];
+      S.beta = beta;
+      if (set_bn) S.bn = beta;
+      S.k = 0;
+      S.dnormw = 0;
+      S.bea = S.bn > 0 ? beta / S.bn : 0.0;
+      S.done = (beta == 0.0) || (frozen && frozen[r]);
+    }
+  }
+}
+
+// End of a step: dnormw = ||w||, V_{jcol+1} = w / dnormw, the Givens update of column jcol
+// and the residual estimate; a system stops counting steps once it meets tol.
+template <typename VT>
+__global__ void __launch_bounds__(RT_) k_bfinish(cx<VT>* V, size_t ldj, const cx<VT>* w, int n, int jcol,
+                                                 const zc* part, int ldp, zc* H, int m, double* rc, zc* rs,
+                                                 BState* st, double tol) {
+  __shared__ double sdn;
+  const int r = blockIdx.y;
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int b = 0; b < BNB; b++) s += part[((size_t)r * BNB + b) * ldp].re;
+    sdn = sqrt(s);
+  }
+  __syncthreads();
+  const double dn = sdn;
+  const double inv = dn > 0 ? 1.0 / dn : 0.0;
+  cx<VT>* vn = V + (size_t)(jcol + 1) * ldj + (size_t)r * n;
+  const cx<VT>* wr = w + (size_t)r * n;
+  for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) vn[i] = narrow<VT>(cvt_z(wr[i]) * inv);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    zc* Hr = H + (size_t)r * (m + 1) * (m + 1);
+    double* rcr = rc + (size_t)r * (m + 1);
+    zc* rsr = rs + (size_t)r * (m + 1);
+    Hr[HIDX(jcol + 1, jcol)] = mk<double>(dn, 0.0);
+    for (int j = 0; j < jcol; j++) zrot(Hr[HIDX(j, jcol)], Hr[HIDX(j + 1, jcol)], rcr[j], rsr[j]);
+    double cr;
+    zc sn;
+    zrotg(Hr[HIDX(jcol, jcol)], Hr[HIDX(jcol + 1, jcol)], cr, sn);
+    rcr[jcol] = cr;
+    rsr[jcol] = sn;
+    zrot(Hr[HIDX(jcol, m)], Hr[HIDX(jcol + 1, m)], cr, sn);
+    zrot(Hr[HIDX(jcol, jcol)], Hr[HIDX(jcol + 1, jcol)], cr, sn);
+    Hr[HIDX(jcol + 1, jcol)] = mk<double>(0, 0);
+    BState& S = st[r];
+    S.dnormw = dn;
+    if (!S.done) {
+      const double bea = S.bn > 0 ? sqrt(cabs2(Hr[HIDX(jcol + 1, m)])) / S.bn : 0.0;
+      S.bea = bea;
+      S.k = jcol + 1;
+      if (bea <= tol || dn == 0.0 || !isfinite(bea)) S.done = 1;
+    }
+  }
+}
+
+// y_r = H_r(0:k, 0:k)^{-1} H_r(0:k, m) with k = the system's step count.
+__global__ void k_btrsv(const zc* H, int m, const BState* st, zc* y) {
+  if (threadIdx.x != 0) return;
+  const int r = blockIdx.x;
+  const zc* Hr = H + (size_t)r * (m + 1) * (m + 1);
+  zc* yr = y + (size_t)r * (m + 1);
+  const int k = st[r].k;
+  for (int i = 0; i < k; i++) yr[i] = Hr[HIDX(i, m)];
+  for (int i = k - 1; i >= 0; i--) {
+    yr[i] = yr[i] / Hr[HIDX(i, i)];
+    for (int j = 0; j < i; j++) yr[j] = yr[j] - yr[i] * Hr[HIDX(j, i)];
+  }
+}
+
+// out_r (+)= sum_{j < k_r} y_r[j] V_j
+template <typename VT, typename VO>
+__global__ void __launch_bounds__(RT_) k_bcombine(const cx<VT>* __restrict__ V, size_t ldj, const zc* y, int ly,
+                                                  const BState* st, int n, cx<VO>* out, int add) {
+  const int r = blockIdx.y;
+  const int k = st[r].k;
+  const zc* yr = y + (size_t)r * ly;
+  cx<VO>* orr = out + (size_t)r * n;
+  for (int i = blockIdx.x * RT_ + threadIdx.x; i < n; i += BNB * RT_) {
+    zc s = add ? cvt_z(orr[i]) : mk<double>(0, 0);
+    for (int j = 0; j < k; j++) s = cfma(cvt_z(V[(size_t)j * ldj + (size_t)r * n + i]), yr[j], s);
+    orr[i] = narrow<VO>(s);
+  }
+}
+
+struct GmB {
+  int n, R, mi, mo, ldp;
+  size_t ldj;         // R * n: one basis column of the batch
+  cc *V32, *w32, *r32, *z32;
+  zc *Hi, *rsi, *yi, *W, *Zb, *w64, *x, *b, *r0, *Ho, *rso, *yo, *pA, *pB;
+  double *rci, *rco;
+  BState *sti, *sto;
+  int* fin;
+};
+
+static int gmb_alloc(sie_ctx* c, int R, int mi, int mo, GmB& g) {
+  const int n = 2 * c->M;
+  size_t need = 0;
+  auto add = [&](size_t bytes) {
+    size_t o = need;
+    need += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t vr = (size_t)R * n;
+  const int ldp = BJMAX;
+  size_t oV32 = add((mi + 1) * vr * sizeof(cc)), ow32 = add(vr * sizeof(cc)), or32 = add(vr * sizeof(cc)),
+         oz32 = add(vr * sizeof(cc));
+  size_t oHi = add((size_t)R * (mi + 1) * (mi + 1) * sizeof(zc)), orsi = add((size_t)R * (mi + 1) * sizeof(zc)),
+         oyi = add((size_t)R * (mi + 1) * sizeof(zc)), orci = add((size_t)R * (mi + 1) * sizeof(double));
+  size_t oW = add((mo + 1) * vr * sizeof(zc)), oZ = add(mo * vr * sizeof(zc)), ow64 = add(vr * sizeof(zc)),
+         ox = add(vr * sizeof(zc)), ob = add(vr * sizeof(zc)), or0 = add(vr * sizeof(zc));
+  size_t oHo = add((size_t)R * (mo + 1) * (mo + 1) * sizeof(zc)), orso = add((size_t)R * (mo + 1) * sizeof(zc)),
+         oyo = add((size_t)R * (mo + 1) * sizeof(zc)), orco = add((size_t)R * (mo + 1) * sizeof(double));
+  size_t opA = add((size_t)R * BNB * ldp * sizeof(zc)), opB = add((size_t)R * BNB * ldp * sizeof(zc));
+  size_t osti = add(R * sizeof(BState)), osto = add(R * sizeof(BState)), ofin = add(R * sizeof(int));
+  if (c->gmb_bytes < need) {
+    if (c->d_gmb) cudaFree(c->d_gmb);
+    c->d_gmb = nullptr;
+    c->gmb_bytes = 0;
+    SIE_CUDA(cudaMalloc(&c->d_gmb, need));
+    c->gmb_bytes = need;
+  }
+  SIE_CUDA(cudaMemsetAsync(c->d_gmb, 0, need, c->stream));
+  if (!c->h_gmb)
+    SIE_CUDA(cudaHostAlloc(&c->h_gmb, SIE_BATCH_MAX * (sizeof(BState) + sizeof(int)), cudaHostAllocDefault));
+  char* p = (char*)c->d_gmb;
+  g.n = n;
+  g.R = R;
+  g.mi = mi;
+  g.mo = mo;
+  g.ldp = ldp;
+  g.ldj = vr;
+  g.V32 = (cc*)(p + oV32);
+  g.w32 = (cc*)(p + ow32);
+  g.r32 = (cc*)(p + or32);
+  g.z32 = (cc*)(p + oz32);
+  g.Hi = (zc*)(p + oHi);
+  g.rsi = (zc*)(p + orsi);
+  g.yi = (zc*)(p + oyi);
+  g.rci = (double*)(p + orci);
+  g.W = (zc*)(p + oW);
+  g.Zb = (zc*)(p + oZ);
+  g.w64 = (zc*)(p + ow64);
+  g.x = (zc*)(p + ox);
+  g.b = (zc*)(p + ob);
+  g.r0 = (zc*)(p + or0);
+  g.Ho = (zc*)(p + oHo);
+  g.rso = (zc*)(p + orso);
+  g.yo = (zc*)(p + oyo);
+  g.rco = (double*)(p + orco);
+  g.pA = (zc*)(p + opA);
+  g.pB = (zc*)(p + opB);
+  g.sti = (BState*)(p + osti);
+  g.sto = (BState*)(p + osto);
+  g.fin = (int*)(p + ofin);
+  return SIE_OK;
+}
+
+// One Arnoldi step of the batch after the product w = A V_j: CGS2 against V_0..V_j, then
+// the new basis column and the Givens update.
+template <typename VT>
+static int barnoldi(cx<VT>* V, size_t ldj, cx<VT>* w, int n, int R, int j, zc* pA, zc* pB, int ldp, zc* H,
+                    int m, double* rc, zc* rs, BState* st, double tol, cudaStream_t s) {
+  dim3 g(BNB, R);
+  k_bdots<VT><<<g, RT_, 0, s>>>(V, ldj, w, n, j + 1, pA, ldp); sie::count_launch();
+  k_bupdate<VT><<<g, RT_, 0, s>>>(V, ldj, w, n, j + 1, pA, pB, ldp, H, m, j, 0, 0); sie::count_launch();
+  k_bupdate<VT><<<g, RT_, 0, s>>>(V, ldj, w, n, j + 1, pB, pA, ldp, H, m, j, 1, 1); sie::count_launch();
+  k_bfinish<VT><<<g, RT_, 0, s>>>(V, ldj, w, n, j, pA, ldp, H, m, rc, rs, st, tol); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+// One inner cycle for all R systems: z_r ~ A32^{-1} rhs_r (complex64, internal layout).
+static int inner_batch32(sie_ctx* c, GmB& g, double tol) {
+  cudaStream_t s = c->stream;
+  const int n = g.n, R = g.R, mi = g.mi;
+  dim3 grid(BNB, R);
+  k_bnorm<float><<<grid, RT_, 0, s>>>(g.r32, n, g.pA, g.ldp); sie::count_launch();
+  k_binit<float, float><<<grid, RT_, 0, s>>>(g.r32, n, g.pA, g.ldp, g.V32, g.Hi, mi, g.sti, 1, nullptr);
+  sie::count_launch();
+  for (int j = 0; j < mi; j++) {
+    SIE_TRY(sie_internal_matvec_b32(c, g.V32 + (size_t)j * g.ldj, g.w32, R, s));
+    SIE_TRY(barnoldi<float>(g.V32, g.ldj, g.w32, n, R, j, g.pA, g.pB, g.ldp, g.Hi, mi, g.rci, g.rsi, g.sti, tol, s));
+  }
+  k_btrsv<<<R, 32, 0, s>>>(g.Hi, mi, g.sti, g.yi); sie::count_launch();
+  k_bcombine<float, float><<<grid, RT_, 0, s>>>(g.V32, g.ldj, g.yi, mi + 1, g.sti, n, g.z32, 0);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+int fgmres_mixed_batch(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, int R, const sie_solver_cfg* cfg,
+                       sie_stats* stats) {
+  cudaStream_t s = c->stream;
+  const int mo = cfg->restart, mi = cfg->inner_restart;
+  if (R < 1 || R > SIE_BATCH_MAX) return fail(SIE_ERR_ARG, "batched solve: bad batch size");
+  if (mi < 1 || mi + 1 > BJMAX || mo + 1 > BJMAX || !(cfg->inner_tolerance > 0))
+    return fail(SIE_ERR_ARG, "batched solve: restarts must be 1..63");
+  SIE_TRY(make_f32_tables(c));
+  GmB g;
+  SIE_TRY(gmb_alloc(c, R, mi, mo, g));
+  const int n = g.n;
+  const size_t vr = (size_t)R * n;
+  dim3 grid(BNB, R);
+  BState* hst = (BState*)c->h_gmb;
+  int* hfin = (int*)(hst + SIE_BATCH_MAX);
+  cudaEventRecord(c->ev[12], s);
+  SIE_TRY(gather_ext_to_int(c, d_b_ext, g.b, R, s));
+  if (cfg->use_initial_guess) SIE_TRY(gather_ext_to_int(c, d_x_ext, g.x, R, s));
+  // ||b_r|| into sto[r].bn (the outer estimate is relative to it)
+  k_bnorm<double><<<grid, RT_, 0, s>>>(g.b, n, g.pA, g.ldp); sie::count_launch();
+  k_binit<double, double><<<grid, RT_, 0, s>>>(g.b, n, g.pA, g.ldp, g.W, g.Ho, mo, g.sto, 1, nullptr);
+  sie::count_launch();
+  SIE_CUDA(cudaMemcpyAsync(hst, g.sto, R * sizeof(BState), cudaMemcpyDeviceToHost, s));
+  SIE_CUDA(cudaStreamSynchronize(s));
+  std::vector<double> bn(R), be(R, 1e300), bea(R, 1e300);
+  std::vector<int> its(R, 0), conv(R, 0), mv(R, 0);
+  for (int r = 0; r < R; r++) {
+    bn[r] = hst[r].beta;
+    if (!std::isfinite(bn[r])) return fail(SIE_ERR_NONFINITE, "batched solve: non-finite right-hand side");
+    hfin[r] = bn[r] == 0.0;  // x = 0 solves it
+    if (hfin[r]) conv[r] = 1, be[r] = bea[r] = 0;
+  }
+  int it = 0;
+  auto finish = [&](int code) {
+    scatter_int_to_ext(c, g.x, d_x_ext, R, s);
+    cudaEventRecord(c->ev[13], s);
+    cudaEventSynchronize(c->ev[13]);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[12], c->ev[13]);
+    if (stats)
+      for (int r = 0; r < R; r++) {
+        stats[r].iterations = its[r];
+        stats[r].inner_iterations = its[r] * mi;
+        stats[r].matvecs = mv[r];
+        stats[r].converged = conv[r];
+        stats[r].backward_error_arnoldi = bea[r];
+        stats[r].backward_error_true = be[r];
+        stats[r].seconds = ms * 1e-3;
+      }
+    return code;
+  };
+  bool first = true;
+  while (true) {
+    // r0 = b - A x in FP64 for the whole batch, then the cycle's start vectors
+    if (first && !cfg->use_initial_guess) {
+      k_copy<<<RB, RT_, 0, s>>>(g.b, g.w64, (int)vr); sie::count_launch();
+    } else {
+      SIE_TRY(sie_internal_matvec_b(c, g.x, g.r0, R, s));
+      for (int r = 0; r < R; r++)
+        if (!hfin[r]) mv[r]++;
+      k_sub<<<RB, RT_, 0, s>>>(g.b, g.r0, g.w64, (int)vr); sie::count_launch();
+    }
+    first = false;
+    SIE_CUDA(cudaMemcpyAsync(g.fin, hfin, R * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_bnorm<double><<<grid, RT_, 0, s>>>(g.w64, n, g.pA, g.ldp); sie::count_launch();
+    k_binit<double, double><<<grid, RT_, 0, s>>>(g.w64, n, g.pA, g.ldp, g.W, g.Ho, mo, g.sto, 0, g.fin);
+    sie::count_launch();
+    SIE_CUDA(cudaMemcpyAsync(hst, g.sto, R * sizeof(BState), cudaMemcpyDeviceToHost, s));
+    SIE_CUDA(cudaStreamSynchronize(s));
+    bool all = true, frozen_changed = false;
+    for (int r = 0; r < R; r++) {
+      if (hfin[r]) continue;
+      if (!std::isfinite(hst[r].beta)) return finish(fail(SIE_ERR_NONFINITE, "batched solve: non-finite residual"));
+      be[r] = hst[r].beta / bn[r];
+      if (be[r] <= cfg->tolerance) {
+        hfin[r] = 1;
+        conv[r] = 1;
+        frozen_changed = true;
+      } else {
+        all = false;
+      }
+    }
+    if (all) return finish(SIE_OK);
+    if (it >= cfg->max_iterations) return finish(fail(SIE_ERR_NOCONV, "batched solve: no convergence"));
+    if (frozen_changed) {  // systems that just converged take no further steps
+      SIE_CUDA(cudaMemcpyAsync(g.fin, hfin, R * sizeof(int), cudaMemcpyHostToDevice, s));
+      k_binit<double, double><<<grid, RT_, 0, s>>>(g.w64, n, g.pA, g.ldp, g.W, g.Ho, mo, g.sto, 0, g.fin);
+      sie::count_launch();
+    }
+    for (int j = 0; j < mo; j++) {
+      SIE_TRY(to_c64(g.W + (size_t)j * g.ldj, g.r32, vr, s));
+      SIE_TRY(inner_batch32(c, g, cfg->inner_tolerance));
+      SIE_TRY(to_c128(g.z32, g.Zb + (size_t)j * g.ldj, vr, s));
+      SIE_TRY(sie_internal_matvec_b(c, g.Zb + (size_t)j * g.ldj, g.w64, R, s));
+      SIE_TRY(barnoldi<double>(g.W, g.ldj, g.w64, n, R, j, g.pA, g.pB, g.ldp, g.Ho, mo, g.rco, g.rso, g.sto,
+                               cfg->tolerance, s));
+      it++;
+      SIE_CUDA(cudaMemcpyAsync(hst, g.sto, R * sizeof(BState), cudaMemcpyDeviceToHost, s));
+      SIE_CUDA(cudaStreamSynchronize(s));
+      bool alldone = true;
+      for (int r = 0; r < R; r++) {
+        if (hfin[r]) continue;
+        its[r]++;
+        mv[r] += mi + 1;
+        if (!std::isfinite(hst[r].bea)) return finish(fail(SIE_ERR_NONFINITE, "batched solve: non-finite Arnoldi vector"));
+        bea[r] = hst[r].bea;
+        if (!hst[r].done) alldone = false;
+      }
+      if (alldone || it >= cfg->max_iterations) break;
+      if (cfg->time_limit_s > 0) {
+        float el = 0;
+        cudaEventRecord(c->ev[13], s);
+        cudaEventSynchronize(c->ev[13]);
+        cudaEventElapsedTime(&el, c->ev[12], c->ev[13]);
+        if (el * 1e-3 > cfg->time_limit_s) {
+          finish(SIE_ERR_TIMEOUT);
+          return fail(SIE_ERR_TIMEOUT, "batched solve: time limit reached");
+        }
+      }
+    }
+    // x_r += Z_r y_r over the steps each system took
+    k_btrsv<<<R, 32, 0, s>>>(g.Ho, mo, g.sto, g.yo); sie::count_launch();
+    k_bcombine<double, double><<<grid, RT_, 0, s>>>(g.Zb, g.ldj, g.yo, mo + 1, g.sto, n, g.x, 1);
+    sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+}
+
 }  // namespace sie

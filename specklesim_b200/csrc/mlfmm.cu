@@ -975,6 +975,372 @@ __global__ void k_zero(cx<T>* p, size_t n) {
 }
 
 // ---------------------------------------------------------------------------
+// Batches of R right-hand sides.  Vector r sits at x + r * 2M (internal layout) and the
+// level coefficients of box b hold R x 8 items, [b][r][item][Q], so item r * 8 + i has
+// medium i & 1 as in the single product.  Every radiation pattern, translation table
+// and phase factor read from memory is applied to all R vectors.
+
+#define AGB_E 16  // edges per shared-memory tile of the batched aggregate
+
+// C_box[r] = sum_e conj(RT_e) x_e[r]: block per (leaf box, 32 directions) with one warp per
+// vector (8 or 16 warps); the radiation patterns of AGB_E edges and their R x (J, M)
+// coefficients are staged in shared memory and read by every warp.
+template <typename T>
+__global__ void __launch_bounds__(512) k_agg_b(const cx<T>* __restrict__ rt, const int* box_first,
+                                               const int* box_cnt, int Q, const cx<T>* __restrict__ x,
+                                               int M, int R, cx<T>* __restrict__ C) {
+  __shared__ cx<T> srt[AGB_E][4][32];
+  __shared__ cx<T> sx[AGB_E][2][16];
+  const int b = blockIdx.y, q0 = blockIdx.x * 32;
+  const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = q0 + lane;
+  const int f = box_first[b], cnt = box_cnt[b];
+  const size_t ldx = (size_t)2 * M;
+  constexpr bool split = sizeof(T) == 4;  // FP32: a fresh partial per tile, short chains
+  cx<T> acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  for (int e0 = 0; e0 < cnt; e0 += AGB_E) {
+    const int ne = min(AGB_E, cnt - e0);
+    for (int i = threadIdx.x; i < ne * 128; i += blockDim.x) {
+      const int e = i >> 7, k = (i >> 5) & 3, j = i & 31;
+      srt[e][k][j] = (q0 + j < Q) ? rt[(size_t)(f + e0 + e) * 4 * Q + (size_t)k * Q + q0 + j] : mk<T>(0, 0);
+    }
+    for (int i = threadIdx.x; i < ne * 2 * R; i += blockDim.x) {
+      const int e = i / (2 * R), rem = i - e * 2 * R;
+      sx[e][rem & 1][rem >> 1] = x[(size_t)(rem >> 1) * ldx + 2 * (f + e0 + e) + (rem & 1)];
+    }
+    __syncthreads();
+    if (r < R) {
+      cx<T> pt[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) pt[i] = split ? mk<T>(0, 0) : acc[i];
+      for (int e = 0; e < ne; e++) {
+        const cx<T> ra1 = srt[e][0][lane], rb1 = srt[e][1][lane], ra2 = srt[e][2][lane], rb2 = srt[e][3][lane];
+        const cx<T> xe = sx[e][0][r], xh = sx[e][1][r];
+        pt[0] = cfma_conj(ra1, xe, pt[0]);
+        pt[1] = cfma_conj(ra2, xe, pt[1]);
+        pt[2] = cfma_conj(ra1, xh, pt[2]);
+        pt[3] = cfma_conj(ra2, xh, pt[3]);
+        pt[4] = cfma_conj(rb1, xe, pt[4]);
+        pt[5] = cfma_conj(rb2, xe, pt[5]);
+        pt[6] = cfma_conj(rb1, xh, pt[6]);
+        pt[7] = cfma_conj(rb2, xh, pt[7]);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++) acc[i] = split ? acc[i] + pt[i] : pt[i];
+    }
+    __syncthreads();
+  }
+  if (q >= Q || r >= R) return;
+  cx<T>* o = C + ((size_t)b * R + r) * 8 * Q + q;
+#pragma unroll
+  for (int i = 0; i < 8; i++) o[(size_t)i * Q] = acc[i];
+}
+
+// SS of a batch: thread per (direction, parent box, vector r).
+template <typename T>
+__global__ void k_ss_b(const cx<T>* __restrict__ Cc, const int* ch_ptr, const int* ch_idx,
+                       const int* ch_oct, const cx<T>* __restrict__ ph, int Q, int nmed, int R,
+                       cx<T>* __restrict__ Cp) {
+  const int b = blockIdx.y, r = blockIdx.z;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  cx<T> acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  for (int k = ch_ptr[b]; k < ch_ptr[b + 1]; k++) {
+    const int c = ch_idx[k], o = ch_oct[k];
+    const cx<T>* src = Cc + ((size_t)c * R + r) * 8 * Q + q;
+#pragma unroll
+    for (int md = 0; md < 2; md++) {
+      if (md < nmed) {
+        const cx<T> p = ph[((size_t)o * 2 + md) * Q + q];
+#pragma unroll
+        for (int it = 0; it < 8; it += 2) acc[it + md] = cfma(src[(size_t)(it + md) * Q], p, acc[it + md]);
+      }
+    }
+  }
+  cx<T>* out = Cp + ((size_t)b * R + r) * 8 * Q + q;
+#pragma unroll
+  for (int i = 0; i < 8; i++) out[(size_t)i * Q] = acc[i];
+}
+
+// RR of a batch: D_child[r] += D_parent[r] * exp(-i k khat.(x_child - x_parent)).
+template <typename T>
+__global__ void k_rr_b(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
+                       const cx<T>* __restrict__ ph, int Q, int nmed, int R, cx<T>* __restrict__ D) {
+  const int b = blockIdx.y, r = blockIdx.z;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  const int p = parent[b];
+  if (p < 0) return;
+  const int o = oct[b];
+  const cx<T>* src = Dp + ((size_t)p * R + r) * 8 * Q + q;
+  cx<T>* dst = D + ((size_t)b * R + r) * 8 * Q + q;
+  for (int md = 0; md < nmed; md++) {
+    const cx<T> f = ph[((size_t)o * 2 + md) * Q + q];
+#pragma unroll
+    for (int it = 0; it < 8; it += 2)
+      dst[(size_t)(it + md) * Q] = cfma(src[(size_t)(it + md) * Q], f, dst[(size_t)(it + md) * Q]);
+  }
+}
+
+// SR of a batch over the present siblings of one group (the k_sr_warp_ns scheme).  For
+// each source the NS translation factors are read from shared memory once and applied to
+// RC vectors, items it0 and it0 + 2 of each; ni = 8 R items per box.
+template <typename T, int NS, int RC>
+__device__ __forceinline__ void sr_nsb_body(const int* lst, int cnt, const cx<T>* Cq, int ni, int it0,
+                                            const cx<T>* sTL, int qi, const int* sibc, const int* offc,
+                                            bool qok, T wq, int Q, int zero_other,
+                                            cx<T>* __restrict__ Dq) {
+  int off[NS];
+#pragma unroll
+  for (int k = 0; k < NS; k++) off[k] = offc[k] * SRW_QT + qi;
+  cx<T> acc[RC][NS][2];
+#pragma unroll
+  for (int rc = 0; rc < RC; rc++)
+#pragma unroll
+    for (int k = 0; k < NS; k++) acc[rc][k][0] = acc[rc][k][1] = mk<T>(0, 0);
+  for (int i = 0; i < cnt; i++) {
+    const int s = lst[i];
+    const size_t sb = (size_t)(s >> 9) * ni + it0;
+    const int t0 = (s & 511) * SRW_QT;
+    cx<T> c0[RC], c1[RC];
+#pragma unroll
+    for (int rc = 0; rc < RC; rc++) {
+      c0[rc] = Cq[(sb + 8 * rc) * Q];
+      c1[rc] = Cq[(sb + 8 * rc + 2) * Q];
+    }
+    cx<T> f[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) f[k] = sTL[t0 + off[k]];
+#pragma unroll
+    for (int rc = 0; rc < RC; rc++)
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        acc[rc][k][0] = cfma(c0[rc], f[k], acc[rc][k][0]);
+        acc[rc][k][1] = cfma(c1[rc], f[k], acc[rc][k][1]);
+      }
+  }
+  if (!qok) return;
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    cx<T>* out = Dq + (size_t)sibc[k] * ni * Q;
+#pragma unroll
+    for (int rc = 0; rc < RC; rc++) {
+      const int i0 = it0 + 8 * rc;
+      out[(size_t)i0 * Q] = acc[rc][k][0] * wq;
+      out[(size_t)(i0 + 2) * Q] = acc[rc][k][1] * wq;
+      if (zero_other) {
+        out[(size_t)(i0 ^ 1) * Q] = mk<T>(0, 0);
+        out[(size_t)((i0 + 2) ^ 1) * Q] = mk<T>(0, 0);
+      }
+    }
+  }
+}
+
+template <typename T, int RC>
+__global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_ns_b(
+    const cx<T>* __restrict__ C, const int* __restrict__ grp_sib, const int* __restrict__ grp_src,
+    int ngrp, const cx<T>* __restrict__ tl, const T* __restrict__ trf, int Q, int md,
+    int zero_other, int R, cx<T>* __restrict__ D) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sTL = reinterpret_cast<cx<T>*>(smraw);                  // [343][SRW_QT]
+  int* s_list = reinterpret_cast<int*>(sTL + 343 * SRW_QT);      // [SRW_GB][216]
+  int* s_sib = s_list + SRW_GB * 216;                            // [SRW_GB][8]
+  int* s_off = s_sib + SRW_GB * 8;                               // [SRW_GB][8]
+  const int q0 = blockIdx.x * SRW_QT;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 343 * SRW_QT; i += blockDim.x) {
+    const int t = i / SRW_QT, j = i - t * SRW_QT;
+    const int q = q0 + j;
+    sTL[i] = (q < Q) ? tl[((size_t)t * 2 + md) * Q + q] : mk<T>(0, 0);
+  }
+  __syncthreads();
+  const int w = tid >> 5, lane = tid & 31;
+  const int g = blockIdx.y * SRW_GB + w;
+  if (g >= ngrp) return;
+  const int sib = (lane < 8) ? grp_sib[(size_t)g * 8 + lane] : -1;
+  const unsigned smask = __ballot_sync(0xffffffffu, sib >= 0) & 0xffu;
+  const int ns = __popc(smask);
+  if (sib >= 0) {
+    const int k = __popc(smask & ((1u << lane) - 1u));
+    s_sib[w * 8 + k] = sib;
+    s_off[w * 8 + k] = ((lane >> 2) & 1) * 49 + ((lane >> 1) & 1) * 7 + (lane & 1);
+  }
+  int* lst = s_list + w * 216;
+  int cnt = 0;
+  for (int base = 0; base < 216; base += 32) {
+    const int dc = base + lane;
+    const int d = dc >> 3, c = dc & 7;
+    const int s = (dc < 216 && d != 13) ? grp_src[(size_t)g * 216 + dc] : -1;
+    const unsigned bal = __ballot_sync(0xffffffffu, s >= 0);
+    if (s >= 0) {
+      const int t0 = (3 - ((c >> 2) & 1) - 2 * (d / 9 - 1)) * 49 + (3 - ((c >> 1) & 1) - 2 * ((d / 3) % 3 - 1)) * 7 +
+                     (3 - (c & 1) - 2 * (d % 3 - 1));
+      lst[cnt + __popc(bal & ((1u << lane) - 1u))] = (s << 9) | t0;
+    }
+    cnt += __popc(bal);
+  }
+  __syncwarp();
+  const int ih = lane >> 4, qi = lane & 15;
+  const int q = q0 + qi;
+  const bool qok = q < Q;
+  const cx<T>* Cq = C + (qok ? q : 0);
+  cx<T>* Dq = D + (qok ? q : 0);
+  const T wq = trf[qok ? q : 0];
+  const int* sibc = s_sib + w * 8;
+  const int* offc = s_off + w * 8;
+  const int ni = 8 * R;
+  // blockIdx.z picks the RC vectors: the slowest grid dimension, so the blocks resident at
+  // any time read the coefficients of only RC vectors, a slice that stays in L2 while the
+  // ~27 sibling groups around each source box read it
+  const int it0 = md + 4 * ih + 8 * (blockIdx.z * RC);
+  switch (ns) {
+    case 1: sr_nsb_body<T, 1, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 2: sr_nsb_body<T, 2, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 3: sr_nsb_body<T, 3, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 4: sr_nsb_body<T, 4, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 5: sr_nsb_body<T, 5, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 6: sr_nsb_body<T, 6, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 7: sr_nsb_body<T, 7, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    case 8: sr_nsb_body<T, 8, RC>(lst, cnt, Cq, ni, it0, sTL, qi, sibc, offc, qok, wq, Q, zero_other, Dq); break;
+    default: break;
+  }
+}
+
+// Receive of a batch as a small complex GEMM per chunk of <= 32 edges of one leaf box:
+//   y[r][e][o] += sum over (medium md, row ab, direction q) of RT[e][2 md + ab][q] U[r][md][o][ab][q]
+// with U the folded D of k_receive_chunk (A1, B1 for o = 0; A2, B2 for o = 1).  The block
+// is 4 direction groups x 64 threads; thread (eq, rp) of a group owns edges 4 eq .. 4 eq + 3
+// and vectors 2 rp, 2 rp + 1 (both outputs): 16 accumulators, 16 shared-memory reads per
+// 32 complex FMAs.  Tiles of QT directions of RT ([row][q][edge]) and of U ([k][q][r]) are
+// staged per step; the four groups take every fourth direction of a tile and their sums
+// meet in shared memory at the end.
+template <typename T> struct RecvTile { static const int QT = sizeof(T) == 4 ? 32 : 16; };
+
+template <typename T>
+static size_t recv_g_smem() {
+  const int QT = RecvTile<T>::QT;
+  size_t tiles = ((size_t)4 * QT * 33 + (size_t)8 * QT * 17) * sizeof(cx<T>);
+  size_t red = (size_t)4 * 32 * 16 * 2 * sizeof(cx<T>);
+  return std::max(tiles, red);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_recv_g(const cx<T>* __restrict__ rt, const int4* __restrict__ chunks,
+                                                const cx<T>* __restrict__ D, int Q, RecvConst rc, int M, int R,
+                                                cx<T>* __restrict__ y) {
+  constexpr int QT = RecvTile<T>::QT;
+  constexpr bool split = sizeof(T) == 4;  // FP32: a fresh partial per tile keeps chains short
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* sRT = reinterpret_cast<cx<T>*>(smraw);  // [4 rows][QT][33 edges]
+  cx<T>* sU = sRT + 4 * QT * 33;                  // [8 = md, o, ab][QT][17 vectors]
+  const int4 ch = chunks[blockIdx.x];
+  const int b = ch.x, f = ch.y, cnt = ch.z;
+  const int tid = threadIdx.x, kg = tid >> 6, t = tid & 63;
+  const int eq = t >> 3, rp = t & 7;
+  cx<T> acc[4][2][2];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int jr = 0; jr < 2; jr++) acc[j][jr][0] = acc[j][jr][1] = mk<T>(0, 0);
+  for (int q0 = 0; q0 < Q; q0 += QT) {
+    for (int i = tid; i < 32 * 4 * QT; i += 256) {
+      const int e = i / (4 * QT), rem = i - e * 4 * QT, row = rem / QT, qq = rem - row * QT;
+      const int q = q0 + qq;
+      sRT[(row * QT + qq) * 33 + e] =
+          (e < cnt && q < Q) ? rt[(size_t)(f + e) * 4 * Q + (size_t)row * Q + q] : mk<T>(0, 0);
+    }
+    for (int i = tid; i < 16 * 2 * QT; i += 256) {
+      const int r = i / (2 * QT), rem = i - r * 2 * QT, md = rem / QT, qq = rem - md * QT;
+      const int q = q0 + qq;
+      cx<T> u0 = mk<T>(0, 0), u1 = u0, u2 = u0, u3 = u0;
+      if (r < R && q < Q) {
+        // folded in FP64 as in k_receive_chunk: the sums over directions cancel heavily
+        const cx<T>* Db = D + ((size_t)b * R + r) * 8 * Q + q;
+        const zc dJt = cvt_z(Db[(size_t)(0 + md) * Q]), dMt = cvt_z(Db[(size_t)(2 + md) * Q]);
+        const zc dJp = cvt_z(Db[(size_t)(4 + md) * Q]), dMp = cvt_z(Db[(size_t)(6 + md) * Q]);
+        const zc m_ = md ? rc.my_d[1] : rc.my_d[0], k_ = md ? rc.kd[1] : rc.kd[0], e_ = md ? rc.eps_d[1] : rc.eps_d[0];
+        const zc A1 = (m_ * dJt + k_ * dMp) * rc.s1f, B1 = (m_ * dJp - k_ * dMt) * rc.s1f;
+        const zc A2 = (e_ * dMt - k_ * dJp) * rc.s2f, B2 = (k_ * dJt + e_ * dMp) * rc.s2f;
+        u0 = mk<T>((T)A1.re, (T)A1.im);
+        u1 = mk<T>((T)B1.re, (T)B1.im);
+        u2 = mk<T>((T)A2.re, (T)A2.im);
+        u3 = mk<T>((T)B2.re, (T)B2.im);
+      }
+      cx<T>* u = sU + ((size_t)(md * 4) * QT + qq) * 17 + r;
+      u[0] = u0;
+      u[(size_t)QT * 17] = u1;
+      u[(size_t)2 * QT * 17] = u2;
+      u[(size_t)3 * QT * 17] = u3;
+    }
+    __syncthreads();
+    cx<T> pt[4][2][2];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int jr = 0; jr < 2; jr++)
+#pragma unroll
+        for (int o = 0; o < 2; o++) pt[j][jr][o] = split ? mk<T>(0, 0) : acc[j][jr][o];
+#pragma unroll 2
+    for (int qq = kg; qq < QT; qq += 4) {
+#pragma unroll
+      for (int md = 0; md < 2; md++) {
+        cx<T> a[4][2], u[2][2][2];
+#pragma unroll
+        for (int ab = 0; ab < 2; ab++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) a[j][ab] = sRT[((2 * md + ab) * QT + qq) * 33 + 4 * eq + j];
+#pragma unroll
+        for (int o = 0; o < 2; o++)
+#pragma unroll
+          for (int ab = 0; ab < 2; ab++)
+#pragma unroll
+            for (int jr = 0; jr < 2; jr++) u[jr][o][ab] = sU[((md * 4 + o * 2 + ab) * QT + qq) * 17 + 2 * rp + jr];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+          for (int jr = 0; jr < 2; jr++)
+#pragma unroll
+            for (int o = 0; o < 2; o++) {
+              pt[j][jr][o] = cfma(a[j][0], u[jr][o][0], pt[j][jr][o]);
+              pt[j][jr][o] = cfma(a[j][1], u[jr][o][1], pt[j][jr][o]);
+            }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int jr = 0; jr < 2; jr++)
+#pragma unroll
+        for (int o = 0; o < 2; o++) acc[j][jr][o] = split ? acc[j][jr][o] + pt[j][jr][o] : pt[j][jr][o];
+    __syncthreads();
+  }
+  // the four direction groups' partial sums: red[kg][e][r][o]
+  cx<T>* red = sRT;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int jr = 0; jr < 2; jr++)
+#pragma unroll
+      for (int o = 0; o < 2; o++) red[(((size_t)kg * 32 + 4 * eq + j) * 16 + 2 * rp + jr) * 2 + o] = acc[j][jr][o];
+  __syncthreads();
+  const size_t ldy = (size_t)2 * M;
+  for (int i = tid; i < 32 * 16 * 2; i += 256) {
+    const int e = i >> 5, r = (i >> 1) & 15, o = i & 1;
+    if (e < cnt && r < R) {
+      cx<T> s = red[i];
+      s += red[1024 + i];
+      s += red[2048 + i];
+      s += red[3072 + i];
+      y[(size_t)r * ldy + 2 * (f + e) + o] += s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 
 int far_build_tables(sie_ctx* c, const double* d_boxc) {
@@ -1022,6 +1388,27 @@ template <> const cc* php_dn<float>(const Level& L) { return L.ph_dn32; }
 template <typename T> static const T* trfp(const sie_ctx* c);
 template <> const double* trfp<double>(const sie_ctx* c) { return c->d_trf; }
 template <> const float* trfp<float>(const sie_ctx* c) { return c->d_trf32; }
+
+// Factors of the final far summation (MLFMM_tri_summation_New,
+// lib_sie_tri_mlfmm.f90:416-497) and the ICTF output scaling (:486-488).
+static RecvConst recv_const(const sie_ctx* c) {
+  RecvConst rc;
+  zc I = mk<double>(0, 1);
+  rc.kd[0] = c->mt.k1 * I;
+  rc.kd[1] = c->mt.k2 * I;
+  rc.my_d[0] = mk<double>(0, c->mt.my1 * c->mt.omega);
+  rc.my_d[1] = mk<double>(0, c->mt.my2 * c->mt.omega);
+  rc.eps_d[0] = c->mt.eps1 * I * c->mt.omega;
+  rc.eps_d[1] = c->mt.eps2 * I * c->mt.omega;
+  if (c->cfg.formulation == SIE_ICTF) {
+    rc.s1f = mk<double>(1, 0) / c->mt.eta_a;
+    rc.s2f = c->mt.eta_a;
+  } else {
+    rc.s1f = mk<double>(1, 0);
+    rc.s2f = mk<double>(1, 0);
+  }
+  return rc;
+}
 
 template <typename T>
 int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
@@ -1126,21 +1513,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
   // final far summation
   {
     Level& L = c->lv[L1];
-    RecvConst rc;
-    zc I = mk<double>(0, 1);
-    rc.kd[0] = c->mt.k1 * I;
-    rc.kd[1] = c->mt.k2 * I;
-    rc.my_d[0] = mk<double>(0, c->mt.my1 * c->mt.omega);
-    rc.my_d[1] = mk<double>(0, c->mt.my2 * c->mt.omega);
-    rc.eps_d[0] = c->mt.eps1 * I * c->mt.omega;
-    rc.eps_d[1] = c->mt.eps2 * I * c->mt.omega;
-    if (c->cfg.formulation == SIE_ICTF) {
-      rc.s1f = mk<double>(1, 0) / c->mt.eta_a;
-      rc.s2f = c->mt.eta_a;
-    } else {
-      rc.s1f = mk<double>(1, 0);
-      rc.s2f = mk<double>(1, 0);
-    }
+    const RecvConst rc = recv_const(c);
     size_t smem = (size_t)8 * Q * sizeof(cx<T>);
     if (c->recv_mode == 1) {
       k_receive_chunk<T><<<c->n_rchunk, 256, smem, st>>>(rt, (const int4*)c->d_rchunk,
@@ -1163,6 +1536,97 @@ int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* e
 int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
                  cudaEvent_t wait_recv) {
   return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev, wait_recv);
+}
+
+// Batched coefficient buffers of every level, grown to R vectors of type T.
+template <typename T>
+static int ensure_batch_coeffs(sie_ctx* c, int R) {
+  for (int l = c->l_min; l <= c->l_max; l++) {
+    Level& L = c->lv[l];
+    size_t need = (size_t)L.nb * 8 * R * c->Q * sizeof(cx<T>);
+    if (L.cdb_bytes >= need) continue;
+    if (L.Cb) cudaFree(L.Cb);
+    if (L.Db) cudaFree(L.Db);
+    L.Cb = L.Db = nullptr;
+    L.cdb_bytes = 0;
+    SIE_CUDA(cudaMalloc(&L.Cb, need));
+    SIE_CUDA(cudaMalloc(&L.Db, need));
+    L.cdb_bytes = need;
+  }
+  return SIE_OK;
+}
+
+template <typename T>
+static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, int R,
+                          cudaStream_t st) {
+  if (R < 1 || R > SIE_BATCH_MAX) return fail(SIE_ERR_ARG, "batched far product: bad batch size");
+  SIE_TRY(ensure_batch_coeffs<T>(c, R));
+  const int Q = c->Q, L0 = c->l_min, L1 = c->l_max, M = c->M;
+  const bool k2c = c->mt.k2.im != 0.0;
+  const int thr = 128;
+  {
+    Level& L = c->lv[L1];
+    dim3 g((Q + 31) / 32, L.nb);
+    k_agg_b<T><<<g, R <= 8 ? 256 : 512, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, M, R, (cx<T>*)L.Cb);
+    sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  for (int l = L1 - 1; l >= L0; l--) {
+    Level& P = c->lv[l];
+    Level& Ch = c->lv[l + 1];
+    dim3 g((Q + thr - 1) / thr, P.nb, R);
+    k_ss_b<T><<<g, thr, 0, st>>>((const cx<T>*)Ch.Cb, P.ch_ptr, P.ch_idx, P.ch_oct, php_up<T>(Ch), Q,
+                                 k2c ? 1 : 2, R, (cx<T>*)P.Cb); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  for (int l = L0; l <= L1; l++) {
+    Level& L = c->lv[l];
+    if (L.nb >= (1 << 22)) return fail(SIE_ERR_ARG, "batched far product: too many boxes on a level");
+    const unsigned gx = (Q + SRW_QT - 1) / SRW_QT, gy = (L.ngrp + SRW_GB - 1) / SRW_GB;
+    const int nmed = L.only_k1 ? 1 : 2;
+    for (int md = 0; md < nmed; md++) {
+      // two vectors per source read in FP32; one in FP64, whose accumulators are twice as wide
+      bool done = false;
+      if constexpr (sizeof(T) == 4) {
+        if (R % 2 == 0) {
+          k_sr_ns_b<T, 2><<<dim3(gx, gy, R / 2), 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
+              (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(c), Q, md, nmed == 1, R,
+              (cx<T>*)L.Db);
+          done = true;
+        }
+      }
+      if (!done)
+        k_sr_ns_b<T, 1><<<dim3(gx, gy, R), 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
+            (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(c), Q, md, nmed == 1, R,
+            (cx<T>*)L.Db);
+      sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+  }
+  for (int l = L0 + 1; l <= L1; l++) {
+    Level& L = c->lv[l];
+    Level& P = c->lv[l - 1];
+    dim3 g((Q + thr - 1) / thr, L.nb, R);
+    k_rr_b<T><<<g, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), Q, k2c ? 1 : 2, R,
+                                 (cx<T>*)L.Db); sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  {
+    Level& L = c->lv[L1];
+    k_recv_g<T><<<c->n_rchunk, 256, recv_g_smem<T>(), st>>>(rt, (const int4*)c->d_rchunk, (const cx<T>*)L.Db,
+                                                             Q, recv_const(c), M, R, y);
+    sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  return SIE_OK;
+}
+
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
+  return far_matvec_b_t<double>(c, c->d_rt, x, y, R, st);
+}
+
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st) {
+  return far_matvec_b_t<float>(c, c->d_rt32, x, y, R, st);
 }
 
 __global__ void k_trf_f32(const double* a, float* b, int n) {
@@ -1237,6 +1701,11 @@ int far_prepare_kernels(sie_ctx* c) {
                                 (int)sr_warp_ns_smem<float>()));
   SIE_CUDA(raise_smem(k_sr_warp_bf<float>,
                                 (int)sr_warp_bf_smem<float>()));
+  SIE_CUDA(raise_smem(k_sr_ns_b<double, 1>, sr_warp_ns_smem<double>()));
+  SIE_CUDA(raise_smem(k_sr_ns_b<float, 1>, sr_warp_ns_smem<float>()));
+  SIE_CUDA(raise_smem(k_sr_ns_b<float, 2>, sr_warp_ns_smem<float>()));
+  SIE_CUDA(raise_smem(k_recv_g<double>, recv_g_smem<double>()));
+  SIE_CUDA(raise_smem(k_recv_g<float>, recv_g_smem<float>()));
   return SIE_OK;
 }
 

@@ -625,8 +625,94 @@ __global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __
   }
 }
 
+// Near product of a batch of R vectors: block per (chunk of <= 32 rows of box A, group of
+// RG vectors).  The chunk gathers x of the panel's columns for its RG vectors into shared
+// memory ([vector][J, M][column], so consecutive lanes read consecutive words), then each
+// warp streams rows of the panel once and applies every value to all RG vectors.  The
+// groups of one chunk are adjacent blocks and mostly read the panel rows from L2.
+template <typename T, int RG>
+__global__ void __launch_bounds__(256) k_near_b(PanelArgs P, const cx<T>* __restrict__ va,
+                                                const cx<T>* __restrict__ vb,
+                                                const cx<T>* __restrict__ vd_,
+                                                const int4* __restrict__ chunks, int ngr, int M,
+                                                cx<T> cfac, const cx<T>* __restrict__ x, int R,
+                                                cx<T>* __restrict__ y) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [RG][J, M][ncols]
+  const int ci = blockIdx.x / ngr, g = blockIdx.x - ci * ngr;
+  const int4 ch = chunks[ci];
+  const int A = ch.x, f = ch.y, cnt = ch.z;
+  const int nc = P.ncols[A];
+  const long long base = P.base[A] + (long long)(f - P.box_first[A]) * nc;
+  const int r0 = g * RG, nr = min(RG, R - r0);
+  const size_t ldx = (size_t)2 * M;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int col0 = 0;
+  for (int k = P.nbr_ptr[A]; k < P.nbr_ptr[A + 1]; k++) {
+    const int B = P.nbr_box[k];
+    const int c = P.box_cnt[B], fb = P.box_first[B];
+    for (int j = threadIdx.x; j < 2 * RG * c; j += blockDim.x) {
+      const int rr = j / (2 * c), rem = j - rr * 2 * c;
+      const int col = rem >> 1, h = rem & 1;
+      xs[((size_t)rr * 2 + h) * nc + col0 + col] =
+          rr < nr ? x[(size_t)(r0 + rr) * ldx + 2 * (fb + col) + h] : mk<T>(0, 0);
+    }
+    col0 += c;
+  }
+  __syncthreads();
+  for (int row = warp; row < cnt; row += 8) {
+    const long long o = base + (long long)row * nc;
+    cx<T> sJ[RG], sM[RG], tM[RG];
+#pragma unroll
+    for (int rr = 0; rr < RG; rr++) sJ[rr] = sM[rr] = tM[rr] = mk<T>(0, 0);
+#pragma unroll 2
+    for (int j = lane; j < nc; j += 32) {
+      const cx<T> a = va[o + j], b = vb[o + j], d = vd_[o + j];
+#pragma unroll
+      for (int rr = 0; rr < RG; rr++) {
+        const cx<T> xj = xs[(size_t)(2 * rr) * nc + j], xm = xs[(size_t)(2 * rr + 1) * nc + j];
+        sJ[rr] = cfma(a, xj, sJ[rr]);
+        sJ[rr] = cfma(b, xm, sJ[rr]);
+        tM[rr] = cfma(b, xj, tM[rr]);
+        sM[rr] = cfma(d, xm, sM[rr]);
+      }
+    }
+#pragma unroll
+    for (int rr = 0; rr < RG; rr++) {
+      sM[rr] = cfma(cfac, tM[rr], sM[rr]);
+#pragma unroll
+      for (int s = 16; s > 0; s >>= 1) {
+        sJ[rr].re += __shfl_xor_sync(0xffffffffu, sJ[rr].re, s);
+        sJ[rr].im += __shfl_xor_sync(0xffffffffu, sJ[rr].im, s);
+        sM[rr].re += __shfl_xor_sync(0xffffffffu, sM[rr].re, s);
+        sM[rr].im += __shfl_xor_sync(0xffffffffu, sM[rr].im, s);
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int rr = 0; rr < RG; rr++) {
+        if (rr < nr) {
+          cx<T>* yr = y + (size_t)(r0 + rr) * ldx + 2 * (f + row);
+          yr[0] = sJ[rr];
+          yr[1] = sM[rr];
+        }
+      }
+    }
+  }
+}
+
 // -------------------------------------------------------------------------
 // host wrappers
+
+// vectors per block of the batched near product
+template <typename T> struct NearGroup { static const int RG = sizeof(T) == 4 ? 4 : 2; };
+
+// Shared memory of the batched near product; 0 if the widest panel does not fit.
+template <typename T>
+static size_t near_b_smem(const sie_ctx* c) {
+  size_t s = (size_t)c->ncols_max * 2 * NearGroup<T>::RG * sizeof(cx<T>);
+  return s <= (size_t)200 * 1024 ? std::max<size_t>(s, 16) : 0;
+}
 
 // Shared memory the chunked near product needs; 0 if the widest panel does not fit.
 template <typename T>
@@ -644,6 +730,8 @@ int near_prepare_kernels(sie_ctx* c) {
     SIE_CUDA(raise_smem(k_near_panel<float, true>, s));
     SIE_CUDA(raise_smem(k_near_panel<float, false>, s));
   }
+  if (size_t s = near_b_smem<double>(c)) SIE_CUDA(raise_smem(k_near_b<double, NearGroup<double>::RG>, s));
+  if (size_t s = near_b_smem<float>(c)) SIE_CUDA(raise_smem(k_near_b<float, NearGroup<float>::RG>, s));
   return SIE_OK;
 }
 
@@ -768,6 +856,30 @@ int near_matvec64(sie_ctx* c, const zc* x, zc* y, int nrhs, bool accum, cudaStre
 int near_matvec32(sie_ctx* c, const cc* x, cc* y, int nrhs, bool accum, cudaStream_t st) {
   cc cf = mk<float>((float)c->cfac.re, (float)c->cfac.im);
   return near_matvec_t<float>(c, c->d_na32, c->d_nb32, c->d_nd32, cf, x, y, nrhs, accum, st);
+}
+
+// Batched near product (writes y); panels too wide for the batched kernel's shared memory
+// take the one-vector-at-a-time product.
+template <typename T>
+static int near_matvec_b_t(sie_ctx* c, const cx<T>* va, const cx<T>* vb, const cx<T>* vdd, cx<T> cfac,
+                           const cx<T>* x, cx<T>* y, int R, cudaStream_t st) {
+  const size_t smem = near_b_smem<T>(c);
+  if (!smem || c->n_rchunk < 1) return near_matvec_t<T>(c, va, vb, vdd, cfac, x, y, R, false, st);
+  const int RG = NearGroup<T>::RG;
+  const int ngr = (R + RG - 1) / RG;
+  k_near_b<T, NearGroup<T>::RG><<<(unsigned)c->n_rchunk * ngr, 256, smem, st>>>(
+      panel_args(c), va, vb, vdd, (const int4*)c->d_rchunk, ngr, c->M, cfac, x, R, y);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
+  return near_matvec_b_t<double>(c, c->d_na, c->d_nb, c->d_nd, c->cfac, x, y, R, st);
+}
+int near_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st) {
+  cc cf = mk<float>((float)c->cfac.re, (float)c->cfac.im);
+  return near_matvec_b_t<float>(c, c->d_na32, c->d_nb32, c->d_nd32, cf, x, y, R, st);
 }
 
 }  // namespace sie

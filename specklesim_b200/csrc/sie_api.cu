@@ -601,6 +601,20 @@ static int ensure_work(sie_ctx* c, int nrhs) {
   return SIE_OK;
 }
 
+// complex64 vectors of a batched mixed-precision product
+int ensure_batch32(sie_ctx* c, int nrhs) {
+  if ((size_t)nrhs <= c->b32_rhs) return SIE_OK;
+  if (c->d_xb32) cudaFree(c->d_xb32);
+  if (c->d_yb32) cudaFree(c->d_yb32);
+  c->d_xb32 = c->d_yb32 = nullptr;
+  c->b32_rhs = 0;
+  size_t n = (size_t)2 * c->M * nrhs;
+  SIE_CUDA(cudaMalloc(&c->d_xb32, n * sizeof(cc)));
+  SIE_CUDA(cudaMalloc(&c->d_yb32, n * sizeof(cc)));
+  c->b32_rhs = nrhs;
+  return SIE_OK;
+}
+
 }  // namespace sie
 
 using namespace sie;
@@ -668,6 +682,28 @@ int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool 
     if (!c->cfg.dense) SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr));
   }
   if (timed) record_phase_times(c, st);
+  return SIE_OK;
+}
+
+// Batched products: the near panels write y, the far passes add into it.  Batches larger
+// than SIE_BATCH_MAX go in slices.
+int sie_internal_matvec_b(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
+  const size_t n = (size_t)2 * c->M;
+  for (int r0 = 0; r0 < R; r0 += SIE_BATCH_MAX) {
+    const int nr = std::min(SIE_BATCH_MAX, R - r0);
+    SIE_TRY(near_matvec_b64(c, x + r0 * n, y + r0 * n, nr, st));
+    if (!c->cfg.dense) SIE_TRY(far_matvec_b64(c, x + r0 * n, y + r0 * n, nr, st));
+  }
+  return SIE_OK;
+}
+
+int sie_internal_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st) {
+  const size_t n = (size_t)2 * c->M;
+  for (int r0 = 0; r0 < R; r0 += SIE_BATCH_MAX) {
+    const int nr = std::min(SIE_BATCH_MAX, R - r0);
+    SIE_TRY(near_matvec_b32(c, x + r0 * n, y + r0 * n, nr, st));
+    if (!c->cfg.dense) SIE_TRY(far_matvec_b32(c, x + r0 * n, y + r0 * n, nr, st));
+  }
   return SIE_OK;
 }
 
@@ -905,6 +941,27 @@ int sie_matvec_device(sie_ctx* c, const double* d_x, double* d_y, int nrhs, int 
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   SIE_TRY(ensure_work(c, nrhs));
   SIE_TRY(gather_ext_to_int(c, (const zc*)d_x, c->d_xi, nrhs, st));
+  if (nrhs > 1) {
+    // the vectors go through the product together: one read of the tables per batch
+    cudaEventRecord(c->ev[0], st);
+    if (precision == SIE_MIXED) {
+      SIE_TRY(make_f32_tables(c));
+      SIE_TRY(ensure_batch32(c, nrhs));
+      size_t n = (size_t)2 * c->M * nrhs;
+      SIE_TRY(to_c64(c->d_xi, c->d_xb32, n, st));
+      SIE_TRY(sie_internal_matvec_b32(c, c->d_xb32, c->d_yb32, nrhs, st));
+      SIE_TRY(to_c128(c->d_yb32, c->d_yi, n, st));
+    } else {
+      SIE_TRY(sie_internal_matvec_b(c, c->d_xi, c->d_yi, nrhs, st));
+    }
+    cudaEventRecord(c->ev[7], st);
+    SIE_TRY(scatter_int_to_ext(c, c->d_yi, (zc*)d_y, nrhs, st));
+    SIE_CUDA(cudaStreamSynchronize(st));
+    float a = 0;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[7]);
+    c->tm.mv_total_ms = a;
+    return SIE_OK;
+  }
   if (precision == SIE_MIXED) {
     // complex64 product: tables and vectors in FP32, result widened back to FP64
     SIE_TRY(make_f32_tables(c));
@@ -991,6 +1048,17 @@ int sie_solve_device(sie_ctx* c, const double* d_b, double* d_x, int nrhs, const
   SIE_CUDA(cudaSetDevice(c->device));
   SIE_TRY(ensure_work(c, 1));
   int rc_all = SIE_OK;
+  if (cfg->precision == SIE_MIXED && nrhs > 1) {
+    // right-hand sides in batches: one batched product per step for the whole batch
+    for (int r0 = 0; r0 < nrhs; r0 += SIE_BATCH_MAX) {
+      const int nr = std::min(SIE_BATCH_MAX, nrhs - r0);
+      const size_t off = (size_t)r0 * 2 * c->M;
+      int rc = fgmres_mixed_batch(c, (const zc*)d_b + off, (zc*)d_x + off, nr, cfg, stats ? stats + r0 : nullptr);
+      if (rc != SIE_OK && rc != SIE_ERR_NOCONV) return rc;
+      if (rc == SIE_ERR_NOCONV) rc_all = rc;
+    }
+    return rc_all;
+  }
   for (int r = 0; r < nrhs; r++) {
     const zc* b = (const zc*)d_b + (size_t)r * 2 * c->M;
     zc* x = (zc*)d_x + (size_t)r * 2 * c->M;
@@ -1190,16 +1258,18 @@ int sie_free(sie_ctx* c) {
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
-                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io};
+                  c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
+                  c->d_xb32, c->d_yb32, c->d_gmb};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {
     void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.tl32, L.ph_up32, L.ph_dn32, L.i4_ptr, L.i4_src, L.i4_off,
-                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src};
+                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src, L.Cb, L.Db};
     for (void* p : lp)
       if (p) cudaFree(p);
   }
   if (c->h_gm) cudaFreeHost(c->h_gm);
+  if (c->h_gmb) cudaFreeHost(c->h_gmb);
   for (int i = 0; i < 16; i++)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);

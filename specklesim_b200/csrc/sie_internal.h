@@ -129,6 +129,10 @@ struct Level {
   cc* tl32 = nullptr;
   cc* ph_up32 = nullptr;
   cc* ph_dn32 = nullptr;
+  // coefficients of a batch of R right-hand sides: nb x R x 8 x Q (made on first use)
+  void* Cb = nullptr;
+  void* Db = nullptr;
+  size_t cdb_bytes = 0;
 };
 
 struct Timings {
@@ -217,6 +221,9 @@ struct sie_ctx {
   bool f32_ready = false;         // complex64 tables made
   cc* d_xi32 = nullptr;           // FP32 work vectors (internal layout)
   cc* d_yi32 = nullptr;
+  cc* d_xb32 = nullptr;           // FP32 vectors of a batched product (b32_rhs of each)
+  cc* d_yb32 = nullptr;
+  size_t b32_rhs = 0;
   // work vectors (internal layout, interleaved J/M per edge)
   zc* d_xi = nullptr;
   zc* d_yi = nullptr;
@@ -228,11 +235,14 @@ struct sie_ctx {
   size_t gm32_bytes = 0;
   void* d_gmz = nullptr;          // flexible GMRES directions Z (mixed precision)
   size_t gmz_bytes = 0;
+  void* d_gmb = nullptr;          // batched mixed-precision solver workspace
+  size_t gmb_bytes = 0;
   void* d_io = nullptr;           // staging of the host-buffer entry points (two halves)
   size_t io_bytes = 0;
   void* d_lu = nullptr;           // dense LU factors (column-major N x N, internal order)
   int* d_piv = nullptr;           // pivots (N) + info
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
+  void* h_gmb = nullptr;          // pinned host copy of the batched solver's per-system state
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
   unsigned ar_epoch = 1;          // launch counter tagging the Arnoldi exchange rounds
   // Arnoldi step: 0 grid-barrier kernel; 1 register-resident kernel with tagged exchanges;
@@ -258,6 +268,15 @@ int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* e
 int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
                  cudaEvent_t wait_recv = nullptr);
 int far_prepare_kernels(sie_ctx* c);
+// Products of a batch of R right-hand sides (internal layout, vector r at offset r * 2M).
+// The near product writes y; the far product adds into it.
+int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
+int near_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
+// largest batch one launch sequence carries (larger batches go in slices)
+static const int SIE_BATCH_MAX = 16;
+int ensure_batch32(sie_ctx* c, int nrhs);
 // complex64 copies of the near panels, radiation patterns, TL and phase tables
 int make_f32_tables(sie_ctx* c);
 int to_c64(const zc* in, cc* out, size_t n, cudaStream_t st);
@@ -272,8 +291,14 @@ int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, z
                  double* d_I);
 int gmres_solve(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
 int fgmres_mixed(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
+// R systems with the same matrix solved together (R <= SIE_BATCH_MAX)
+int fgmres_mixed_batch(sie_ctx* c, const zc* d_b, zc* d_x, int R, const sie_solver_cfg* cfg,
+                       sie_stats* st);
 }  // namespace sie
 
 int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed);
 // the same product with complex64 tables and vectors
 int sie_internal_matvec32(sie_ctx* c, const cc* xi, cc* yi, cudaStream_t st, bool timed);
+// batched products of R vectors (internal layout, stride 2M; sliced by SIE_BATCH_MAX)
+int sie_internal_matvec_b(sie_ctx* c, const zc* xi, zc* yi, int R, cudaStream_t st);
+int sie_internal_matvec_b32(sie_ctx* c, const cc* xi, cc* yi, int R, cudaStream_t st);
