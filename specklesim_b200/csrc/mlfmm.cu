@@ -982,60 +982,66 @@ __global__ void k_zero(cx<T>* p, size_t n) {
 
 #define AGB_E 16  // edges per shared-memory tile of the batched aggregate
 
-// C_box[r] = sum_e conj(RT_e) x_e[r]: block per (leaf box, 32 directions) with one warp per
-// vector (8 or 16 warps); the radiation patterns of AGB_E edges and their R x (J, M)
-// coefficients are staged in shared memory and read by every warp.
-template <typename T>
-__global__ void __launch_bounds__(512) k_agg_b(const cx<T>* __restrict__ rt, const int* box_first,
+// C_box[r] = sum_e conj(RT_e) x_e[r]: block per (leaf box, 32 directions); the radiation
+// patterns of AGB_E edges and their R x (J, M) coefficients are staged in shared memory,
+// and warp w accumulates vectors w, w + 8, ... (RPW of them).
+template <typename T, int RPW>
+__global__ void __launch_bounds__(256) k_agg_b(const cx<T>* __restrict__ rt, const int* box_first,
                                                const int* box_cnt, int Q, const cx<T>* __restrict__ x,
                                                int M, int R, cx<T>* __restrict__ C) {
   __shared__ cx<T> srt[AGB_E][4][32];
-  __shared__ cx<T> sx[AGB_E][2][16];
+  __shared__ cx<T> sx[AGB_E][2][8 * RPW];
   const int b = blockIdx.y, q0 = blockIdx.x * 32;
-  const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int q = q0 + lane;
   const int f = box_first[b], cnt = box_cnt[b];
   const size_t ldx = (size_t)2 * M;
-  constexpr bool split = sizeof(T) == 4;  // FP32: a fresh partial per tile, short chains
-  cx<T> acc[8];
+  cx<T> acc[RPW][8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) acc[i] = mk<T>(0, 0);
+  for (int rr = 0; rr < RPW; rr++)
+#pragma unroll
+    for (int i = 0; i < 8; i++) acc[rr][i] = mk<T>(0, 0);
   for (int e0 = 0; e0 < cnt; e0 += AGB_E) {
     const int ne = min(AGB_E, cnt - e0);
-    for (int i = threadIdx.x; i < ne * 128; i += blockDim.x) {
+    for (int i = threadIdx.x; i < ne * 128; i += 256) {
       const int e = i >> 7, k = (i >> 5) & 3, j = i & 31;
       srt[e][k][j] = (q0 + j < Q) ? rt[(size_t)(f + e0 + e) * 4 * Q + (size_t)k * Q + q0 + j] : mk<T>(0, 0);
     }
-    for (int i = threadIdx.x; i < ne * 2 * R; i += blockDim.x) {
+    for (int i = threadIdx.x; i < ne * 2 * R; i += 256) {
       const int e = i / (2 * R), rem = i - e * 2 * R;
       sx[e][rem & 1][rem >> 1] = x[(size_t)(rem >> 1) * ldx + 2 * (f + e0 + e) + (rem & 1)];
     }
     __syncthreads();
-    if (r < R) {
-      cx<T> pt[8];
+    for (int e = 0; e < ne; e++) {
+      const cx<T> ra1 = srt[e][0][lane], rb1 = srt[e][1][lane], ra2 = srt[e][2][lane], rb2 = srt[e][3][lane];
 #pragma unroll
-      for (int i = 0; i < 8; i++) pt[i] = split ? mk<T>(0, 0) : acc[i];
-      for (int e = 0; e < ne; e++) {
-        const cx<T> ra1 = srt[e][0][lane], rb1 = srt[e][1][lane], ra2 = srt[e][2][lane], rb2 = srt[e][3][lane];
-        const cx<T> xe = sx[e][0][r], xh = sx[e][1][r];
-        pt[0] = cfma_conj(ra1, xe, pt[0]);
-        pt[1] = cfma_conj(ra2, xe, pt[1]);
-        pt[2] = cfma_conj(ra1, xh, pt[2]);
-        pt[3] = cfma_conj(ra2, xh, pt[3]);
-        pt[4] = cfma_conj(rb1, xe, pt[4]);
-        pt[5] = cfma_conj(rb2, xe, pt[5]);
-        pt[6] = cfma_conj(rb1, xh, pt[6]);
-        pt[7] = cfma_conj(rb2, xh, pt[7]);
+      for (int rr = 0; rr < RPW; rr++) {
+        const int r = w + 8 * rr;
+        if (r < R) {
+          const cx<T> xe = sx[e][0][r], xh = sx[e][1][r];
+          acc[rr][0] = cfma_conj(ra1, xe, acc[rr][0]);
+          acc[rr][1] = cfma_conj(ra2, xe, acc[rr][1]);
+          acc[rr][2] = cfma_conj(ra1, xh, acc[rr][2]);
+          acc[rr][3] = cfma_conj(ra2, xh, acc[rr][3]);
+          acc[rr][4] = cfma_conj(rb1, xe, acc[rr][4]);
+          acc[rr][5] = cfma_conj(rb2, xe, acc[rr][5]);
+          acc[rr][6] = cfma_conj(rb1, xh, acc[rr][6]);
+          acc[rr][7] = cfma_conj(rb2, xh, acc[rr][7]);
+        }
       }
-#pragma unroll
-      for (int i = 0; i < 8; i++) acc[i] = split ? acc[i] + pt[i] : pt[i];
     }
     __syncthreads();
   }
-  if (q >= Q || r >= R) return;
-  cx<T>* o = C + ((size_t)b * R + r) * 8 * Q + q;
+  if (q >= Q) return;
 #pragma unroll
-  for (int i = 0; i < 8; i++) o[(size_t)i * Q] = acc[i];
+  for (int rr = 0; rr < RPW; rr++) {
+    const int r = w + 8 * rr;
+    if (r < R) {
+      cx<T>* o = C + ((size_t)b * R + r) * 8 * Q + q;
+#pragma unroll
+      for (int i = 0; i < 8; i++) o[(size_t)i * Q] = acc[rr][i];
+    }
+  }
 }
 
 // SS of a batch: thread per (direction, parent box, vector r).
@@ -1066,23 +1072,56 @@ __global__ void k_ss_b(const cx<T>* __restrict__ Cc, const int* ch_ptr, const in
   for (int i = 0; i < 8; i++) out[(size_t)i * Q] = acc[i];
 }
 
-// RR of a batch: D_child[r] += D_parent[r] * exp(-i k khat.(x_child - x_parent)).
+// Fold of the eight D items of one (box, vector, direction) into the eight values the
+// receive multiplies the radiation patterns by: per medium A1, B1 (first output) and
+// A2, B2 (second output), as in k_receive_chunk, in FP64.  out[md * 4 + {A1, B1, A2, B2}].
+__device__ __forceinline__ void recv_fold(const zc d[8], const RecvConst& rc, zc u[8]) {
+#pragma unroll
+  for (int md = 0; md < 2; md++) {
+    const zc dJt = d[0 + md], dMt = d[2 + md], dJp = d[4 + md], dMp = d[6 + md];
+    u[md * 4 + 0] = (rc.my_d[md] * dJt + rc.kd[md] * dMp) * rc.s1f;
+    u[md * 4 + 1] = (rc.my_d[md] * dJp - rc.kd[md] * dMt) * rc.s1f;
+    u[md * 4 + 2] = (rc.eps_d[md] * dMt - rc.kd[md] * dJp) * rc.s2f;
+    u[md * 4 + 3] = (rc.kd[md] * dJt + rc.eps_d[md] * dMp) * rc.s2f;
+  }
+}
+
+// RR of a batch: D_child[r] += D_parent[r] * exp(-i k khat.(x_child - x_parent)).  On the
+// leaf level (fold = 1) the result is folded in place for the receive (recv_fold).
 template <typename T>
 __global__ void k_rr_b(const cx<T>* __restrict__ Dp, const int* parent, const int* oct,
-                       const cx<T>* __restrict__ ph, int Q, int nmed, int R, cx<T>* __restrict__ D) {
+                       const cx<T>* __restrict__ ph, int Q, int nmed, int R, int fold, RecvConst rc,
+                       cx<T>* __restrict__ D) {
   const int b = blockIdx.y, r = blockIdx.z;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= Q) return;
   const int p = parent[b];
-  if (p < 0) return;
-  const int o = oct[b];
-  const cx<T>* src = Dp + ((size_t)p * R + r) * 8 * Q + q;
   cx<T>* dst = D + ((size_t)b * R + r) * 8 * Q + q;
-  for (int md = 0; md < nmed; md++) {
-    const cx<T> f = ph[((size_t)o * 2 + md) * Q + q];
+  cx<T> d[8];
 #pragma unroll
-    for (int it = 0; it < 8; it += 2)
-      dst[(size_t)(it + md) * Q] = cfma(src[(size_t)(it + md) * Q], f, dst[(size_t)(it + md) * Q]);
+  for (int i = 0; i < 8; i++) d[i] = dst[(size_t)i * Q];
+  if (p >= 0) {
+    const int o = oct[b];
+    const cx<T>* src = Dp + ((size_t)p * R + r) * 8 * Q + q;
+#pragma unroll
+    for (int md = 0; md < 2; md++) {
+      if (md < nmed) {
+        const cx<T> f = ph[((size_t)o * 2 + md) * Q + q];
+#pragma unroll
+        for (int it = 0; it < 8; it += 2) d[it + md] = cfma(src[(size_t)(it + md) * Q], f, d[it + md]);
+      }
+    }
+  }
+  if (fold) {
+    zc dz[8], u[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) dz[i] = cvt_z(d[i]);
+    recv_fold(dz, rc, u);
+#pragma unroll
+    for (int i = 0; i < 8; i++) dst[(size_t)i * Q] = mk<T>((T)u[i].re, (T)u[i].im);
+  } else if (p >= 0) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) dst[(size_t)i * Q] = d[i];
   }
 }
 
@@ -1212,71 +1251,86 @@ __global__ void __launch_bounds__(32 * SRW_GB, 2) k_sr_ns_b(
 
 // Receive of a batch as a small complex GEMM per chunk of <= 32 edges of one leaf box:
 //   y[r][e][o] += sum over (medium md, row ab, direction q) of RT[e][2 md + ab][q] U[r][md][o][ab][q]
-// with U the folded D of k_receive_chunk (A1, B1 for o = 0; A2, B2 for o = 1).  The block
-// is 4 direction groups x 64 threads; thread (eq, rp) of a group owns edges 4 eq .. 4 eq + 3
-// and vectors 2 rp, 2 rp + 1 (both outputs): 16 accumulators, 16 shared-memory reads per
-// 32 complex FMAs.  Tiles of QT directions of RT ([row][q][edge]) and of U ([k][q][r]) are
-// staged per step; the four groups take every fourth direction of a tile and their sums
-// meet in shared memory at the end.
-template <typename T> struct RecvTile { static const int QT = sizeof(T) == 4 ? 32 : 16; };
+// with U the folded leaf coefficients (recv_fold, written by the leaf RR).  The block is 4
+// direction groups x 64 threads; thread (eq, rp) of a group owns edges eq, eq + 8, eq + 16,
+// eq + 24 and vectors 2 rp, 2 rp + 1 (both outputs): 16 accumulators, 16 shared-memory
+// reads per 32 complex FMAs.  Tiles of QT directions of RT ([row][edge][q]) and U
+// ([k][r][q]) stream in by asynchronous copies into two buffers, the next tile loading
+// while the current one is used; the padded rows keep a warp's reads on distinct banks.
+// The four groups take every fourth direction of a tile and their sums meet in shared
+// memory at the end.
+template <typename T> struct RecvTile { static const int QT = 16; };
 
 template <typename T>
 static size_t recv_g_smem() {
-  const int QT = RecvTile<T>::QT;
-  size_t tiles = ((size_t)4 * QT * 33 + (size_t)8 * QT * 17) * sizeof(cx<T>);
+  const int QT = RecvTile<T>::QT, QP = QT + 2;
+  size_t tiles = (size_t)2 * (4 * 32 + 8 * 16) * QP * sizeof(cx<T>);
   size_t red = (size_t)4 * 32 * 16 * 2 * sizeof(cx<T>);
   return std::max(tiles, red);
 }
 
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, int bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_recv_g(const cx<T>* __restrict__ rt, const int4* __restrict__ chunks,
-                                                const cx<T>* __restrict__ D, int Q, RecvConst rc, int M, int R,
+                                                const cx<T>* __restrict__ U, int Q, int M, int R,
                                                 cx<T>* __restrict__ y) {
-  constexpr int QT = RecvTile<T>::QT;
-  constexpr bool split = sizeof(T) == 4;  // FP32: a fresh partial per tile keeps chains short
+  constexpr int QT = RecvTile<T>::QT, QP = QT + 2;
+  constexpr int EPC = 16 / (int)sizeof(cx<T>);   // directions per 16-byte piece
+  constexpr int PPR = QT / EPC;                   // pieces per tile row
+  constexpr int BUF = (4 * 32 + 8 * 16) * QP;     // complex values per buffer
+  constexpr bool split = sizeof(T) == 4;          // FP32: a fresh partial per tile
   extern __shared__ __align__(16) unsigned char smraw[];
-  cx<T>* sRT = reinterpret_cast<cx<T>*>(smraw);  // [4 rows][QT][33 edges]
-  cx<T>* sU = sRT + 4 * QT * 33;                  // [8 = md, o, ab][QT][17 vectors]
+  cx<T>* sm = reinterpret_cast<cx<T>*>(smraw);    // [2][sRT 4 x 32 x QP, sU 8 x 16 x QP]
   const int4 ch = chunks[blockIdx.x];
   const int b = ch.x, f = ch.y, cnt = ch.z;
   const int tid = threadIdx.x, kg = tid >> 6, t = tid & 63;
-  const int eq = t >> 3, rp = t & 7;
+  const int eq = t & 7, rp = t >> 3;
+  const cx<T>* Ub = U + (size_t)b * R * 8 * Q;
+  auto stage = [&](int q0, int buf) {
+    cx<T>* sRT = sm + buf * BUF;
+    cx<T>* sU = sRT + 4 * 32 * QP;
+    for (int i = tid; i < 4 * 32 * PPR; i += 256) {  // RT rows (row, edge)
+      const int row = i / (32 * PPR), rem = i - row * 32 * PPR, e = rem / PPR, part = rem - e * PPR;
+      const int qs = q0 + part * EPC;
+      const int bytes = e < cnt ? max(0, min(16, (Q - qs) * (int)sizeof(cx<T>))) : 0;
+      const cx<T>* src = bytes > 0 ? rt + (size_t)(f + e) * 4 * Q + (size_t)row * Q + qs : rt;
+      cp_async16(sRT + (row * 32 + e) * QP + part * EPC, src, bytes);
+    }
+    for (int i = tid; i < 8 * 16 * PPR; i += 256) {  // U rows (k, vector)
+      const int k = i / (16 * PPR), rem = i - k * 16 * PPR, r = rem / PPR, part = rem - r * PPR;
+      const int qs = q0 + part * EPC;
+      const int bytes = r < R ? max(0, min(16, (Q - qs) * (int)sizeof(cx<T>))) : 0;
+      const cx<T>* src = bytes > 0 ? Ub + ((size_t)r * 8 + k) * Q + qs : Ub;
+      cp_async16(sU + (k * 16 + r) * QP + part * EPC, src, bytes);
+    }
+    cp_async_commit();
+  };
   cx<T> acc[4][2][2];
 #pragma unroll
   for (int j = 0; j < 4; j++)
 #pragma unroll
     for (int jr = 0; jr < 2; jr++) acc[j][jr][0] = acc[j][jr][1] = mk<T>(0, 0);
-  for (int q0 = 0; q0 < Q; q0 += QT) {
-    for (int i = tid; i < 32 * 4 * QT; i += 256) {
-      const int e = i / (4 * QT), rem = i - e * 4 * QT, row = rem / QT, qq = rem - row * QT;
-      const int q = q0 + qq;
-      sRT[(row * QT + qq) * 33 + e] =
-          (e < cnt && q < Q) ? rt[(size_t)(f + e) * 4 * Q + (size_t)row * Q + q] : mk<T>(0, 0);
-    }
-    for (int i = tid; i < 16 * 2 * QT; i += 256) {
-      const int r = i / (2 * QT), rem = i - r * 2 * QT, md = rem / QT, qq = rem - md * QT;
-      const int q = q0 + qq;
-      cx<T> u0 = mk<T>(0, 0), u1 = u0, u2 = u0, u3 = u0;
-      if (r < R && q < Q) {
-        // folded in FP64 as in k_receive_chunk: the sums over directions cancel heavily
-        const cx<T>* Db = D + ((size_t)b * R + r) * 8 * Q + q;
-        const zc dJt = cvt_z(Db[(size_t)(0 + md) * Q]), dMt = cvt_z(Db[(size_t)(2 + md) * Q]);
-        const zc dJp = cvt_z(Db[(size_t)(4 + md) * Q]), dMp = cvt_z(Db[(size_t)(6 + md) * Q]);
-        const zc m_ = md ? rc.my_d[1] : rc.my_d[0], k_ = md ? rc.kd[1] : rc.kd[0], e_ = md ? rc.eps_d[1] : rc.eps_d[0];
-        const zc A1 = (m_ * dJt + k_ * dMp) * rc.s1f, B1 = (m_ * dJp - k_ * dMt) * rc.s1f;
-        const zc A2 = (e_ * dMt - k_ * dJp) * rc.s2f, B2 = (k_ * dJt + e_ * dMp) * rc.s2f;
-        u0 = mk<T>((T)A1.re, (T)A1.im);
-        u1 = mk<T>((T)B1.re, (T)B1.im);
-        u2 = mk<T>((T)A2.re, (T)A2.im);
-        u3 = mk<T>((T)B2.re, (T)B2.im);
-      }
-      cx<T>* u = sU + ((size_t)(md * 4) * QT + qq) * 17 + r;
-      u[0] = u0;
-      u[(size_t)QT * 17] = u1;
-      u[(size_t)2 * QT * 17] = u2;
-      u[(size_t)3 * QT * 17] = u3;
+  const int ntile = (Q + QT - 1) / QT;
+  stage(0, 0);
+  for (int tt = 0; tt < ntile; tt++) {
+    if (tt + 1 < ntile) {
+      stage((tt + 1) * QT, (tt + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
+    const cx<T>* sRT = sm + (tt & 1) * BUF;
+    const cx<T>* sU = sRT + 4 * 32 * QP;
     cx<T> pt[4][2][2];
 #pragma unroll
     for (int j = 0; j < 4; j++)
@@ -1292,13 +1346,13 @@ __global__ void __launch_bounds__(256) k_recv_g(const cx<T>* __restrict__ rt, co
 #pragma unroll
         for (int ab = 0; ab < 2; ab++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) a[j][ab] = sRT[((2 * md + ab) * QT + qq) * 33 + 4 * eq + j];
+          for (int j = 0; j < 4; j++) a[j][ab] = sRT[((2 * md + ab) * 32 + eq + 8 * j) * QP + qq];
 #pragma unroll
         for (int o = 0; o < 2; o++)
 #pragma unroll
           for (int ab = 0; ab < 2; ab++)
 #pragma unroll
-            for (int jr = 0; jr < 2; jr++) u[jr][o][ab] = sU[((md * 4 + o * 2 + ab) * QT + qq) * 17 + 2 * rp + jr];
+            for (int jr = 0; jr < 2; jr++) u[jr][o][ab] = sU[((md * 4 + o * 2 + ab) * 16 + 2 * rp + jr) * QP + qq];
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
@@ -1316,16 +1370,17 @@ __global__ void __launch_bounds__(256) k_recv_g(const cx<T>* __restrict__ rt, co
       for (int jr = 0; jr < 2; jr++)
 #pragma unroll
         for (int o = 0; o < 2; o++) acc[j][jr][o] = split ? acc[j][jr][o] + pt[j][jr][o] : pt[j][jr][o];
-    __syncthreads();
+    __syncthreads();  // the buffer is refilled by the next iteration's copies
   }
   // the four direction groups' partial sums: red[kg][e][r][o]
-  cx<T>* red = sRT;
+  cx<T>* red = sm;
 #pragma unroll
   for (int j = 0; j < 4; j++)
 #pragma unroll
     for (int jr = 0; jr < 2; jr++)
 #pragma unroll
-      for (int o = 0; o < 2; o++) red[(((size_t)kg * 32 + 4 * eq + j) * 16 + 2 * rp + jr) * 2 + o] = acc[j][jr][o];
+      for (int o = 0; o < 2; o++)
+        red[(((size_t)kg * 32 + eq + 8 * j) * 16 + 2 * rp + jr) * 2 + o] = acc[j][jr][o];
   __syncthreads();
   const size_t ldy = (size_t)2 * M;
   for (int i = tid; i < 32 * 16 * 2; i += 256) {
@@ -1567,7 +1622,10 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
   {
     Level& L = c->lv[L1];
     dim3 g((Q + 31) / 32, L.nb);
-    k_agg_b<T><<<g, R <= 8 ? 256 : 512, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, M, R, (cx<T>*)L.Cb);
+    if (R <= 8)
+      k_agg_b<T, 1><<<g, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, M, R, (cx<T>*)L.Cb);
+    else
+      k_agg_b<T, 2><<<g, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, M, R, (cx<T>*)L.Cb);
     sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
@@ -1603,18 +1661,21 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
     }
     SIE_CUDA(cudaGetLastError());
   }
-  for (int l = L0 + 1; l <= L1; l++) {
+  // RR down to the leaves; the leaf level's kernel also folds D for the receive (with a
+  // single level there is no RR, and the same kernel only folds: every parent is absent)
+  const RecvConst rcn = recv_const(c);
+  for (int l = (L1 > L0 ? L0 + 1 : L1); l <= L1; l++) {
     Level& L = c->lv[l];
-    Level& P = c->lv[l - 1];
+    Level& P = c->lv[l > L0 ? l - 1 : l];
     dim3 g((Q + thr - 1) / thr, L.nb, R);
     k_rr_b<T><<<g, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), Q, k2c ? 1 : 2, R,
-                                 (cx<T>*)L.Db); sie::count_launch();
+                                 l == L1, rcn, (cx<T>*)L.Db); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   {
     Level& L = c->lv[L1];
     k_recv_g<T><<<c->n_rchunk, 256, recv_g_smem<T>(), st>>>(rt, (const int4*)c->d_rchunk, (const cx<T>*)L.Db,
-                                                             Q, recv_const(c), M, R, y);
+                                                             Q, M, R, y);
     sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
