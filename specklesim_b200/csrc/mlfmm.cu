@@ -1613,7 +1613,7 @@ static int ensure_batch_coeffs(sie_ctx* c, int R) {
 
 template <typename T>
 static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, int R,
-                          cudaStream_t st) {
+                          cudaStream_t st, cudaEvent_t wait_recv) {
   if (R < 1 || R > SIE_BATCH_MAX) return fail(SIE_ERR_ARG, "batched far product: bad batch size");
   SIE_TRY(ensure_batch_coeffs<T>(c, R));
   const int Q = c->Q, L0 = c->l_min, L1 = c->l_max, M = c->M;
@@ -1672,6 +1672,8 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
                                  l == L1, rcn, (cx<T>*)L.Db); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
+  // the receive adds into y, which the near product (possibly on another stream) writes
+  if (wait_recv) SIE_CUDA(cudaStreamWaitEvent(st, wait_recv, 0));
   {
     Level& L = c->lv[L1];
     k_recv_g<T><<<c->n_rchunk, 256, recv_g_smem<T>(), st>>>(rt, (const int4*)c->d_rchunk, (const cx<T>*)L.Db,
@@ -1682,12 +1684,12 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
   return SIE_OK;
 }
 
-int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
-  return far_matvec_b_t<double>(c, c->d_rt, x, y, R, st);
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv) {
+  return far_matvec_b_t<double>(c, c->d_rt, x, y, R, st, wait_recv);
 }
 
-int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st) {
-  return far_matvec_b_t<float>(c, c->d_rt32, x, y, R, st);
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv) {
+  return far_matvec_b_t<float>(c, c->d_rt32, x, y, R, st, wait_recv);
 }
 
 __global__ void k_trf_f32(const double* a, float* b, int n) {

@@ -685,26 +685,34 @@ int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool 
   return SIE_OK;
 }
 
-// Batched products: the near panels write y, the far passes add into it.  Batches larger
-// than SIE_BATCH_MAX go in slices.
-int sie_internal_matvec_b(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
+// Batched products: the near panels write y, the far passes add into it.  As in the
+// one-vector product, the near panels run on stream2 beside the translations and the
+// receive waits for them.  Batches larger than SIE_BATCH_MAX go in slices.
+template <typename T, typename NF, typename FF>
+static int matvec_b_t(sie_ctx* c, const cx<T>* x, cx<T>* y, int R, cudaStream_t st, NF near, FF far) {
   const size_t n = (size_t)2 * c->M;
   for (int r0 = 0; r0 < R; r0 += SIE_BATCH_MAX) {
     const int nr = std::min(SIE_BATCH_MAX, R - r0);
-    SIE_TRY(near_matvec_b64(c, x + r0 * n, y + r0 * n, nr, st));
-    if (!c->cfg.dense) SIE_TRY(far_matvec_b64(c, x + r0 * n, y + r0 * n, nr, st));
+    if (!c->cfg.dense && c->overlap_near) {
+      SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+      SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+      SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, c->stream2));
+      SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+      SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, c->ev_join));
+    } else {
+      SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, st));
+      if (!c->cfg.dense) SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, nullptr));
+    }
   }
   return SIE_OK;
 }
 
+int sie_internal_matvec_b(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {
+  return matvec_b_t<double>(c, x, y, R, st, near_matvec_b64, far_matvec_b64);
+}
+
 int sie_internal_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st) {
-  const size_t n = (size_t)2 * c->M;
-  for (int r0 = 0; r0 < R; r0 += SIE_BATCH_MAX) {
-    const int nr = std::min(SIE_BATCH_MAX, R - r0);
-    SIE_TRY(near_matvec_b32(c, x + r0 * n, y + r0 * n, nr, st));
-    if (!c->cfg.dense) SIE_TRY(far_matvec_b32(c, x + r0 * n, y + r0 * n, nr, st));
-  }
-  return SIE_OK;
+  return matvec_b_t<float>(c, x, y, R, st, near_matvec_b32, far_matvec_b32);
 }
 
 extern "C" {

@@ -272,8 +272,8 @@ int far_prepare_kernels(sie_ctx* c);
 // The near product writes y; the far product adds into it.
 int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
 int near_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
-int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
-int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
 // largest batch one launch sequence carries (larger batches go in slices)
 static const int SIE_BATCH_MAX = 16;
 int ensure_batch32(sie_ctx* c, int nrhs);
