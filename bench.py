@@ -204,6 +204,7 @@ def mixed_vs_fp64(V, T, tol):
                      inner_restart=30, inner_tolerance=1e-2, raise_on_noconv=False)
     I64 = g.farfield(x64, pts)[2]
     Im = g.farfield(xm, pts)[2]
+    batched = batched_mixed(g, pts, tol)
     g.close()
     return {
         "workload": f"same slab mesh, eps = {EPS_CONVERGING} (converging), tolerance {tol}",
@@ -216,6 +217,42 @@ def mixed_vs_fp64(V, T, tol):
         "farfield_rel_err_vs_fp64": float(np.linalg.norm(Im - I64) / np.linalg.norm(I64)),
         "currents_rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
         "farfield_points": int(pts.shape[0]),
+        "batched": batched,
+    }
+
+
+def batched_mixed(g, pts, tol, fp64_sample=4):
+    """The 16 plane waves of the batching form (theta 0/10/20/30 deg x phi 0/90 deg x TE/TM)
+    solved together by the batched mixed-precision solver, against plain FP64 GMRES solves
+    of the first `fp64_sample` of them one at a time (FP64 time per solve = mean over the
+    sample).  Errors: currents and 128 x 128 far-field intensity of the sampled columns."""
+    from specklesim_b200 import incidence
+    incs = [incidence(np.deg2rad(t), np.deg2rad(p), pol, 2)
+            for t in (0, 10, 20, 30) for p in (0, 90) for pol in ("TM", "TE")]
+    B = np.stack([g.rhs_planewave(k, E) for k, E in incs], axis=1)
+    kw = dict(restart=10, max_iterations=100, tolerance=tol, precision="mixed", inner_restart=60,
+              inner_tolerance=1e-2, raise_on_noconv=False)
+    Xb, sb = g.solve(B[:, :2], **kw)  # warm-up (allocation of the batch workspace)
+    Xb, sb = g.solve(B, **kw)
+    t_batch = sb[0]["seconds"]
+    t64, ferr, cerr = [], [], []
+    for j in range(fp64_sample):
+        x64, s64 = g.solve(B[:, j], restart=50, max_iterations=4000, tolerance=tol, raise_on_noconv=False)
+        t64.append(s64["seconds"])
+        I64 = g.farfield(x64, pts)[2]
+        Ib = g.farfield(Xb[:, j], pts)[2]
+        ferr.append(float(np.linalg.norm(Ib - I64) / np.linalg.norm(I64)))
+        cerr.append(float(np.linalg.norm(Xb[:, j] - x64) / np.linalg.norm(x64)))
+    per64 = float(np.mean(t64))
+    return {
+        "rhs": B.shape[1], "seconds": t_batch, "solves_per_s": B.shape[1] / t_batch,
+        "fp64_seconds_per_solve": per64, "fp64_sample": fp64_sample,
+        "speedup_vs_fp64": per64 / (t_batch / B.shape[1]),
+        "outer_iterations_max": max(s["iterations"] for s in sb),
+        "backward_error_max": max(s["backward_error_true"] for s in sb),
+        "converged": all(bool(s["converged"]) for s in sb),
+        "farfield_rel_err_vs_fp64_max": max(ferr), "currents_rel_err_vs_fp64_max": max(cerr),
+        "inner": "lockstep GMRES(60) complex64 to 1e-2 on one batched product per step, outer FGMRES(10) FP64",
     }
 
 
