@@ -104,7 +104,8 @@ int sie_info(const sie_ctx* ctx, int* n_edges, int* l_min, int* l_max, long long
  * (precalculation_diagonal_element :94-109). */
 int sie_setup(sie_ctx* ctx);
 
-/* y = Z x for nrhs right-hand sides (host arrays).  Replaces the matvec
+/* y = Z x for nrhs right-hand sides (host arrays, stride 2M); nrhs > 1 goes through the
+ * product in batches of up to 16 vectors that share every read of the tables.  Replaces the matvec
  * callback lib_sie_ml_fmm_calculate_vector_b_tri
  * (src/lib_sie_tri_mlfmm_interface.f90:285-319). */
 int sie_matvec(sie_ctx* ctx, const double* x, double* y, int nrhs, int precision);
@@ -122,7 +123,10 @@ int sie_rhs_planewave(sie_ctx* ctx, const double* k_in, const double* E_in, int 
  * k_dir = calc_p(7).  Writes k_in[3], E_in[3]. */
 int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in);
 
-/* Solve Z x = b.  Replaces lib_sie_solver_gmres_run
+/* Solve Z x = b for nrhs right-hand sides (stride 2M).  With precision SIE_FP64 each is
+ * solved in turn with zgmres semantics; with SIE_MIXED and nrhs > 1 they are solved in
+ * batches of up to 16 that advance in lockstep, one batched product per step (restart
+ * and inner_restart at most 63 there).  Replaces lib_sie_solver_gmres_run
  * (src/lib_sie_solver_gmres_interface.f90:123-211) and the CERFACS zgmres
  * driver (src/lib/libmath_external/src/algorithm_842/zPackgmres.f90:537-1565). */
 int sie_solve(sie_ctx* ctx, const double* b, double* x, int nrhs, const sie_solver_cfg* cfg,
