@@ -114,6 +114,15 @@ int sie_matvec(sie_ctx* ctx, const double* x, double* y, int nrhs, int precision
 int sie_matvec_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, int precision,
                       void* stream);
 
+/* Conjugate-transpose product y = Z^H x in FP64 for nrhs vectors (stride 2M), the operator
+ * of the adjoint solve Z^H lambda = dJ/dI* that a far-field gradient needs.  The reference
+ * has no adjoint; this is the exact transpose of the product sie_matvec applies (near
+ * panels transposed; far field A^T (pi T pi) R^T with pi the khat -> -khat permutation of
+ * the k-space sampling), so <Z^H u, v> = <u, Z v> to rounding. */
+int sie_matvec_adjoint(sie_ctx* ctx, const double* x, double* y, int nrhs);
+/* Same on device arrays; stream may be NULL. */
+int sie_matvec_adjoint_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, void* stream);
+
 /* Plane-wave right-hand sides, get_vector_b_tri + incident_field_tri_general
  * (src/lib_sie_tri_calculation_mod.f90:391-460, 939-1002).  k_in, E_in: 3 x nrhs. */
 int sie_rhs_planewave(sie_ctx* ctx, const double* k_in, const double* E_in, int nrhs, double* b);

@@ -1465,26 +1465,14 @@ static RecvConst recv_const(const sie_ctx* c) {
   return rc;
 }
 
+// The translation passes between the leaf aggregate and the receive: SS up the tree, SR on
+// every level, RR down, from the level coefficients C to the leaf D (events 2, 3, 4).
 template <typename T>
-int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
-                 cudaEvent_t* ev, cudaEvent_t wait_recv) {
-  int Q = c->Q;
-  int L0 = c->l_min, L1 = c->l_max;
-  bool k2c = c->mt.k2.im != 0.0;
-  int thr = 128;
-  // up 1
-  {
-    Level& L = c->lv[L1];
-    if (c->agg_mode == 1) {
-      dim3 g((Q + 31) / 32, L.nb);
-      k_aggregate_eg<T><<<g, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
-    } else {
-      dim3 g((Q + 127) / 128, L.nb);
-      k_aggregate<T><<<g, 128, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
-    }
-    SIE_CUDA(cudaGetLastError());
-  }
-  if (ev) cudaEventRecord(ev[1], st);
+static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev) {
+  const int Q = c->Q;
+  const int L0 = c->l_min, L1 = c->l_max;
+  const bool k2c = c->mt.k2.im != 0.0;
+  const int thr = 128;
   // up 2
   for (int l = L1 - 1; l >= L0; l--) {
     Level& P = c->lv[l];
@@ -1563,6 +1551,30 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[4], st);
+  return SIE_OK;
+}
+
+template <typename T>
+int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
+                 cudaEvent_t* ev, cudaEvent_t wait_recv) {
+  int Q = c->Q;
+  int L0 = c->l_min, L1 = c->l_max;
+  bool k2c = c->mt.k2.im != 0.0;
+  int thr = 128;
+  // up 1
+  {
+    Level& L = c->lv[L1];
+    if (c->agg_mode == 1) {
+      dim3 g((Q + 31) / 32, L.nb);
+      k_aggregate_eg<T><<<g, 256, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    } else {
+      dim3 g((Q + 127) / 128, L.nb);
+      k_aggregate<T><<<g, 128, 0, st>>>(rt, c->d_box_first, c->d_box_cnt, Q, x, (cx<T>*)L.C); sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  SIE_TRY(far_translate_t<T>(c, st, ev));
   // the receive adds into y, which the near product (possibly on another stream) writes
   if (wait_recv) SIE_CUDA(cudaStreamWaitEvent(st, wait_recv, 0));
   // final far summation
@@ -1580,6 +1592,113 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[5], st);
+  return SIE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Transpose of the far product, Z_far^T = A^T (pi T pi) R^T.  A is the leaf aggregate, R the
+// receive (fold of D, then the sum against the radiation patterns), T the translation
+// passes, and pi the direction permutation q -> q' with khat_q' = -khat_q.  The transpose
+// of a step that multiplies by a function of khat (SS, SR, RR phases and TL) is the same
+// step at -khat: SS^T = pi RR pi, RR^T = pi SS pi, SR^T = pi SR pi, so T^T = pi T pi and
+// the translation passes run unchanged between the two permutations.
+
+// R^T then pi: per (leaf box, direction) C[b][i][pi(q)] = Fold^T(sum_e RT_e(q) y_e).
+__global__ void k_adj_in(const zc* __restrict__ rt, const int* box_first, const int* box_cnt, int Q,
+                         const zc* __restrict__ y, const int* __restrict__ qperm, RecvConst rc,
+                         zc* __restrict__ C) {
+  const int b = blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  zc U[2][2][2];  // [md][o][ab]: o = output of the receive, ab = theta / phi row
+#pragma unroll
+  for (int md = 0; md < 2; md++) U[md][0][0] = U[md][0][1] = U[md][1][0] = U[md][1][1] = mk<double>(0, 0);
+  const int f = box_first[b], cnt = box_cnt[b];
+  for (int e = f; e < f + cnt; e++) {
+    const zc* r = rt + (size_t)e * 4 * Q + q;
+    const zc y0 = y[2 * e], y1 = y[2 * e + 1];
+#pragma unroll
+    for (int md = 0; md < 2; md++)
+#pragma unroll
+      for (int ab = 0; ab < 2; ab++) {
+        const zc v = r[(size_t)(2 * md + ab) * Q];
+        U[md][0][ab] = cfma(v, y0, U[md][0][ab]);
+        U[md][1][ab] = cfma(v, y1, U[md][1][ab]);
+      }
+  }
+  // transpose of the fold (A1, B1, A2, B2) = F (dJt, dMt, dJp, dMp) of the receive
+  zc d[8];
+#pragma unroll
+  for (int md = 0; md < 2; md++) {
+    const zc A1 = U[md][0][0], B1 = U[md][0][1], A2 = U[md][1][0], B2 = U[md][1][1];
+    d[0 + md] = rc.s1f * rc.my_d[md] * A1 + rc.s2f * rc.kd[md] * B2;
+    d[2 + md] = rc.s2f * rc.eps_d[md] * A2 - rc.s1f * rc.kd[md] * B1;
+    d[4 + md] = rc.s1f * rc.my_d[md] * B1 - rc.s2f * rc.kd[md] * A2;
+    d[6 + md] = rc.s1f * rc.kd[md] * A1 + rc.s2f * rc.eps_d[md] * B2;
+  }
+  zc* o = C + (size_t)b * 8 * Q + qperm[q];
+#pragma unroll
+  for (int i = 0; i < 8; i++) o[(size_t)i * Q] = d[i];
+}
+
+// pi then A^T: x_e[J] = sum_q conj(RT) of the J items of D[b][.][pi(q)], the same for M.
+// Block per leaf box; D of the box, permuted, in shared memory; one warp per edge.
+__global__ void k_adj_out(const zc* __restrict__ rt, const int* box_first, const int* box_cnt, int Q,
+                          const zc* __restrict__ D, const int* __restrict__ qperm, zc* __restrict__ x) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  zc* sD = reinterpret_cast<zc*>(smraw);  // [8][Q], direction q holds D at pi(q)
+  const int b = blockIdx.x;
+  const zc* Db = D + (size_t)b * 8 * Q;
+  for (int i = threadIdx.x; i < 8 * Q; i += blockDim.x) {
+    const int it = i / Q, q = i - it * Q;
+    sD[i] = Db[(size_t)it * Q + qperm[q]];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int f = box_first[b], cnt = box_cnt[b];
+  for (int e = f + warp; e < f + cnt; e += nw) {
+    const zc* r = rt + (size_t)e * 4 * Q;
+    zc sJ = mk<double>(0, 0), sM = sJ;
+    for (int q = lane; q < Q; q += 32) {
+      const zc ra1 = r[q], rb1 = r[Q + q], ra2 = r[2 * Q + q], rb2 = r[3 * Q + q];
+      sJ = cfma_conj(ra1, sD[0 * Q + q], sJ);
+      sJ = cfma_conj(ra2, sD[1 * Q + q], sJ);
+      sJ = cfma_conj(rb1, sD[4 * Q + q], sJ);
+      sJ = cfma_conj(rb2, sD[5 * Q + q], sJ);
+      sM = cfma_conj(ra1, sD[2 * Q + q], sM);
+      sM = cfma_conj(ra2, sD[3 * Q + q], sM);
+      sM = cfma_conj(rb1, sD[6 * Q + q], sM);
+      sM = cfma_conj(rb2, sD[7 * Q + q], sM);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sJ.re += __shfl_xor_sync(0xffffffffu, sJ.re, o);
+      sJ.im += __shfl_xor_sync(0xffffffffu, sJ.im, o);
+      sM.re += __shfl_xor_sync(0xffffffffu, sM.re, o);
+      sM.im += __shfl_xor_sync(0xffffffffu, sM.im, o);
+    }
+    if (lane == 0) {
+      x[2 * e] += sJ;
+      x[2 * e + 1] += sM;
+    }
+  }
+}
+
+// y += Z_far^T x (FP64, internal layout); uses the one-vector level buffers C and D.
+int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
+  const int Q = c->Q, L1 = c->l_max;
+  Level& L = c->lv[L1];
+  {
+    dim3 g((Q + 127) / 128, L.nb);
+    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, x, c->d_qperm, recv_const(c), L.C);
+    sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  SIE_TRY(far_translate_t<double>(c, st, nullptr));
+  k_adj_out<<<L.nb, 256, (size_t)8 * Q * sizeof(zc), st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, L.D,
+                                                           c->d_qperm, y);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }
 
@@ -1768,6 +1887,7 @@ int far_prepare_kernels(sie_ctx* c) {
   SIE_CUDA(raise_smem(k_sr_ns_b<float, 1>, sr_warp_ns_smem<float>()));
   SIE_CUDA(raise_smem(k_sr_ns_b<float, 2>, sr_warp_ns_smem<float>()));
   SIE_CUDA(raise_smem(k_recv_g<double>, recv_g_smem<double>()));
+  SIE_CUDA(raise_smem(k_adj_out, (size_t)8 * c->Q * sizeof(zc)));
   SIE_CUDA(raise_smem(k_recv_g<float>, recv_g_smem<float>()));
   return SIE_OK;
 }

@@ -701,6 +701,48 @@ __global__ void __launch_bounds__(256) k_near_b(PanelArgs P, const cx<T>* __rest
   }
 }
 
+// Transposed near product y = Z_near^T x (FP64, writes y).  Block per (leaf box B,
+// 128 of its edges n): for every box A of E2(B) (E2 is symmetric, so B is in E2(A) and
+// its edges are a column range of A's panel) it sums the 2 x 2 blocks of column n over the
+// rows of A, transposed: y_J[n] += a x_J[m] + cfac b x_M[m], y_M[n] += b x_J[m] + d x_M[m].
+// Consecutive threads read consecutive columns of each panel row.
+__global__ void __launch_bounds__(128) k_near_T(PanelArgs P, const zc* __restrict__ va,
+                                                const zc* __restrict__ vb, const zc* __restrict__ vd_,
+                                                zc cfac, const zc* __restrict__ x, zc* __restrict__ y) {
+  const int B = blockIdx.y;
+  const int fB = P.box_first[B], cB = P.box_cnt[B];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x * blockDim.x >= cB) return;
+  zc sJ = mk<double>(0, 0), sM = sJ;
+  for (int k = P.nbr_ptr[B]; k < P.nbr_ptr[B + 1]; k++) {
+    const int A = P.nbr_box[k];
+    // column offset of B's edges in A's panel: the boxes of E2(A) before B
+    int col0 = 0;
+    for (int kk = P.nbr_ptr[A]; kk < P.nbr_ptr[A + 1]; kk++) {
+      const int Bp = P.nbr_box[kk];
+      if (Bp == B) break;
+      col0 += P.box_cnt[Bp];
+    }
+    const int fA = P.box_first[A], cA = P.box_cnt[A], nc = P.ncols[A];
+    if (j < cB) {
+      const long long base = P.base[A] + col0 + j;
+      for (int m = 0; m < cA; m++) {
+        const long long o = base + (long long)m * nc;
+        const zc a = va[o], b = vb[o], d = vd_[o];
+        const zc xj = x[2 * (fA + m)], xm = x[2 * (fA + m) + 1];
+        sJ = cfma(a, xj, sJ);
+        sJ = cfma(cfac * b, xm, sJ);
+        sM = cfma(b, xj, sM);
+        sM = cfma(d, xm, sM);
+      }
+    }
+  }
+  if (j < cB) {
+    y[2 * (fB + j)] = sJ;
+    y[2 * (fB + j) + 1] = sM;
+  }
+}
+
 // -------------------------------------------------------------------------
 // host wrappers
 
@@ -869,6 +911,16 @@ static int near_matvec_b_t(sie_ctx* c, const cx<T>* va, const cx<T>* vb, const c
   const int ngr = (R + RG - 1) / RG;
   k_near_b<T, NearGroup<T>::RG><<<(unsigned)c->n_rchunk * ngr, 256, smem, st>>>(
       panel_args(c), va, vb, vdd, (const int4*)c->d_rchunk, ngr, c->M, cfac, x, R, y);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+int near_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
+  int cmax = 1;
+  for (int b = 0; b < c->near.nbox; b++) cmax = std::max(cmax, c->near.box_cnt[b]);
+  dim3 g((cmax + 127) / 128, c->near.nbox);
+  k_near_T<<<g, 128, 0, st>>>(panel_args(c), c->d_na, c->d_nb, c->d_nd, c->cfac, x, y);
   sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;

@@ -537,6 +537,18 @@ static int build_sampling(sie_ctx* c) {
     ph[3 * i] = 0; ph[3 * i + 1] = 1; ph[3 * i + 2] = 0;
     trf[i] = 0.0;
   }
+  // direction of -khat for every direction (used by the transposed product): theta ->
+  // pi - theta is Gauss node K-1-j, phi -> phi + pi is k + K, and the two poles swap
+  std::vector<int> qp(Q);
+  for (int j = 0; j < K; j++)
+    for (int k = 0; k < 2 * K; k++) qp[k + j * 2 * K] = (k + K) % (2 * K) + (K - 1 - j) * 2 * K;
+  qp[Ns] = Ns + 1;
+  qp[Ns + 1] = Ns;
+  for (int i = 0; i < Q; i++)
+    for (int d = 0; d < 3; d++)
+      if (std::fabs(kh[3 * qp[i] + d] + kh[3 * i + d]) > 1e-12)
+        return fail(SIE_ERR_STATE, "k-space sampling is not symmetric under khat -> -khat");
+  SIE_TRY(upload(&c->d_qperm, qp));
   SIE_TRY(upload(&c->d_khat, kh));
   SIE_TRY(upload(&c->d_tth, th));
   SIE_TRY(upload(&c->d_tph, ph));
@@ -704,6 +716,25 @@ static int matvec_b_t(sie_ctx* c, const cx<T>* x, cx<T>* y, int R, cudaStream_t 
       if (!c->cfg.dense) SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, nullptr));
     }
   }
+  return SIE_OK;
+}
+
+__global__ void k_conj_inplace(zc* a, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    a[i].im = -a[i].im;
+}
+
+// y = Z^H x = conj(Z^T conj(x)); x is conjugated in place and back.  The transposed near
+// panels write y, the transposed far passes add into it.
+int sie_internal_matvec_adj(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
+  const size_t n = (size_t)2 * c->M;
+  zc* xw = const_cast<zc*>(x);
+  k_conj_inplace<<<296, 256, 0, st>>>(xw, n); sie::count_launch();
+  SIE_TRY(near_matvec_adj64(c, x, y, st));
+  if (!c->cfg.dense) SIE_TRY(far_matvec_adj64(c, x, y, st));
+  k_conj_inplace<<<296, 256, 0, st>>>(xw, n); sie::count_launch();
+  k_conj_inplace<<<296, 256, 0, st>>>(y, n); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }
 
@@ -1006,6 +1037,39 @@ int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) 
   return r;
 }
 
+int sie_matvec_adjoint_device(sie_ctx* c, const double* d_x, double* d_y, int nrhs, void* stream) {
+  if (!c || !d_x || !d_y || nrhs < 1) return fail(SIE_ERR_ARG, "sie_matvec_adjoint_device: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_matvec_adjoint_device: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  SIE_TRY(ensure_work(c, nrhs));
+  SIE_TRY(gather_ext_to_int(c, (const zc*)d_x, c->d_xi, nrhs, st));
+  const size_t n = (size_t)2 * c->M;
+  for (int r = 0; r < nrhs; r++) SIE_TRY(sie_internal_matvec_adj(c, c->d_xi + r * n, c->d_yi + r * n, st));
+  SIE_TRY(scatter_int_to_ext(c, c->d_yi, (zc*)d_y, nrhs, st));
+  SIE_CUDA(cudaStreamSynchronize(st));
+  return SIE_OK;
+}
+
+int sie_matvec_adjoint(sie_ctx* c, const double* x, double* y, int nrhs) {
+  if (!c || !x || !y || nrhs < 1) return fail(SIE_ERR_ARG, "sie_matvec_adjoint: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_matvec_adjoint: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
+  for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
+    if (!std::isfinite(x[i])) return fail(SIE_ERR_NONFINITE, "sie_matvec_adjoint: non-finite input");
+  zc *dx = nullptr, *dy = nullptr;
+  SIE_TRY(io_buffers(c, bytes, &dx, &dy));
+  int r = SIE_OK;
+  if (cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    r = fail(SIE_ERR_CUDA, "sie_matvec_adjoint: H2D copy");
+  if (r == SIE_OK) r = sie_matvec_adjoint_device(c, (const double*)dx, (double*)dy, nrhs, c->stream);
+  if (r == SIE_OK && (cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+                      cudaStreamSynchronize(c->stream) != cudaSuccess))
+    r = fail(SIE_ERR_CUDA, "sie_matvec_adjoint: D2H copy");
+  return r;
+}
+
 int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in) {
   if (!k_in || !E_in) return fail(SIE_ERR_ARG, "sie_incidence: null argument");
   if (k_dir != 1 && k_dir != 2) return fail(SIE_ERR_ARG, "sie_incidence: k_dir must be 1 or 2");
@@ -1267,7 +1331,7 @@ int sie_free(sie_ctx* c) {
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
-                  c->d_xb32, c->d_yb32, c->d_gmb};
+                  c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {

@@ -215,6 +215,7 @@ struct sie_ctx {
   double* d_tth = nullptr;
   double* d_tph = nullptr;
   double* d_trf = nullptr;
+  int* d_qperm = nullptr;         // direction q' with khat_q' = -khat_q, per direction q
   zc* d_rt = nullptr;             // internal edge x 4 x Q
   cc* d_rt32 = nullptr;
   float* d_trf32 = nullptr;
@@ -274,6 +275,10 @@ int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
 int near_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
 int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
 int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
+// transposed products (y = Z^T x, FP64, internal layout): the near one writes y, the far
+// one adds into it
+int near_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st);
+int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st);
 // largest batch one launch sequence carries (larger batches go in slices)
 static const int SIE_BATCH_MAX = 16;
 int ensure_batch32(sie_ctx* c, int nrhs);
@@ -301,4 +306,6 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
 int sie_internal_matvec32(sie_ctx* c, const cc* xi, cc* yi, cudaStream_t st, bool timed);
 // batched products of R vectors (internal layout, stride 2M; sliced by SIE_BATCH_MAX)
 int sie_internal_matvec_b(sie_ctx* c, const zc* xi, zc* yi, int R, cudaStream_t st);
+// y = Z^H x for one vector (internal layout)
+int sie_internal_matvec_adj(sie_ctx* c, const zc* xi, zc* yi, cudaStream_t st);
 int sie_internal_matvec_b32(sie_ctx* c, const cc* xi, cc* yi, int R, cudaStream_t st);

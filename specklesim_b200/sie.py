@@ -78,6 +78,16 @@ class Sie:
         y = y.T
         return y[:, 0] if x.ndim == 1 else y
 
+    def matvec_adjoint(self, x):
+        """y = Z^H x (FP64), the operator of the adjoint solve."""
+        x = _lib.as_c128(x)
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        xx = np.ascontiguousarray(x.reshape(self.n, nrhs).T)
+        y = np.zeros_like(xx)
+        check(self._lib.sie_matvec_adjoint(self._h, dptr(xx.view(np.float64)), dptr(y.view(np.float64)), nrhs))
+        y = y.T
+        return y[:, 0] if x.ndim == 1 else y
+
     def matvec_device(self, d_x, d_y, nrhs=1, precision="fp64", stream=0):
         """Device-pointer matvec (torch tensors' data_ptr() or raw addresses)."""
         check(self._lib.sie_matvec_device(self._h, C.c_void_p(d_x), C.c_void_p(d_y), nrhs,
