@@ -123,6 +123,20 @@ int sie_matvec_adjoint(sie_ctx* ctx, const double* x, double* y, int nrhs);
 /* Same on device arrays; stream may be NULL. */
 int sie_matvec_adjoint_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, void* stream);
 
+/* Shape gradient of the far-field objective J = sum_o |E(r_o)|^2 4 pi |r_o|^2 (the intensity
+ * of sie_farfield summed over the npts points pts) with respect to the z coordinate of
+ * every mesh vertex, at the solution x of Z x = b for the plane wave (k_in, E_in) of
+ * sie_rhs_planewave.  No counterpart in the reference.  It solves the adjoint system
+ * Z^H lambda = dJ/dx* with FP64 GMRES (cfg: restart, iterations, tolerance; its stats in
+ * *stats) and returns dJ/dz = 2 Re sum_o E_o^H dE_o/dz + 2 Re lambda^H (db/dz - dZ/dz x):
+ * the near blocks, radiation patterns and right-hand side are recomputed on the device
+ * with each vertex moved by +-1e-6 lambda, the field factors (whose observation points are
+ * far away) by +-1e-4 lambda (central differences), the tree and the near/far split held
+ * fixed.  dJdz: nv doubles; J (may be NULL): the objective.
+ * Returns SIE_ERR_NOCONV (with the gradient filled in) if the adjoint solve stops short. */
+int sie_grad(sie_ctx* ctx, const double* x, const double* k_in, const double* E_in, const double* pts,
+             int npts, const sie_solver_cfg* cfg, double* dJdz, double* J, sie_stats* stats);
+
 /* Plane-wave right-hand sides, get_vector_b_tri + incident_field_tri_general
  * (src/lib_sie_tri_calculation_mod.f90:391-460, 939-1002).  k_in, E_in: 3 x nrhs. */
 int sie_rhs_planewave(sie_ctx* ctx, const double* k_in, const double* E_in, int nrhs, double* b);

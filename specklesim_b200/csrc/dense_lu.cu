@@ -114,3 +114,20 @@ extern "C" int sie_solve_direct(sie_ctx* c, const double* b, double* x, int nrhs
   cudaFree(dint);
   return rc;
 }
+
+// Z^H y = g in place on one internal-layout vector with the LU factors (adjoint solve of
+// the shape gradient on a dense context).
+int sie::lu_solve_adjoint(sie_ctx* c, zc* d_int) {
+  SIE_TRY(lu_factor(c));
+  int n = 2 * c->M;
+  cusolverDnHandle_t h = nullptr;
+  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) return fail(SIE_ERR_CUDA, "cusolverDnCreate");
+  int rc = SIE_OK;
+  if (cusolverDnSetStream(h, c->stream) != CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnZgetrs(h, CUBLAS_OP_C, n, 1, (const cuDoubleComplex*)c->d_lu, n, c->d_piv,
+                       (cuDoubleComplex*)d_int, n, c->d_piv + n) != CUSOLVER_STATUS_SUCCESS)
+    rc = fail(SIE_ERR_CUDA, "cusolverDnZgetrs (adjoint)");
+  cusolverDnDestroy(h);
+  if (rc == SIE_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "adjoint LU solve");
+  return rc;
+}

@@ -14,6 +14,7 @@
 #include <algorithm>
 
 #include "sie_internal.h"
+#include "geom.cuh"
 
 namespace sie {
 
@@ -22,6 +23,42 @@ namespace sie {
 // (RT_function_SCSArr_New :543-583): for every direction q and medium,
 //   sum_sides sum_j 0.5*sign*len*(r_j - v) exp(-i k khat.(r_j - Rc)) w_j
 // projected on theta-hat (a_nm) and phi-hat (b_nm).
+// Radiation pattern of one edge in one direction: medium 1 theta, phi, medium 2 theta, phi.
+__device__ __forceinline__ void rt_edge_q(const FnD& f0, const FnD& f1, vd Rc, vd kh, vd th, vd ph,
+                                          const Rule& R, zc k1, zc k2, zc out[4]) {
+  zc a1 = mk<double>(0, 0), b1 = a1, a2 = a1, b2 = a1;
+  for (int ll = 0; ll < 2; ll++) {
+    const FnD& f = ll ? f1 : f0;
+    double dfm = f.sgn * f.length;
+    zc sa[3] = {mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0)};
+    zc sb[3] = {sa[0], sa[0], sa[0]};
+    for (int j = 0; j < R.n; j++) {
+      double w0 = 1 - R.a[j] - R.b[j];
+      vd Ro = mkv<double>(w0 * f.c[0] + R.a[j] * f.c[3] + R.b[j] * f.c[6],
+                          w0 * f.c[1] + R.a[j] * f.c[4] + R.b[j] * f.c[7],
+                          w0 * f.c[2] + R.a[j] * f.c[5] + R.b[j] * f.c[8]);
+      vd fm = (Ro - mkv<double>(f.c[6], f.c[7], f.c[8])) * 0.5 * dfm;
+      double tmp = dot(kh, Ro - Rc);
+      zc e1 = cexp_mik(k1, tmp) * R.w[j];
+      zc e2 = cexp_mik(k2, tmp) * R.w[j];
+      sa[0] += e1 * fm.x;
+      sa[1] += e1 * fm.y;
+      sa[2] += e1 * fm.z;
+      sb[0] += e2 * fm.x;
+      sb[1] += e2 * fm.y;
+      sb[2] += e2 * fm.z;
+    }
+    a1 += sa[0] * th.x + sa[1] * th.y + sa[2] * th.z;
+    b1 += sa[0] * ph.x + sa[1] * ph.y + sa[2] * ph.z;
+    a2 += sb[0] * th.x + sb[1] * th.y + sb[2] * th.z;
+    b2 += sb[0] * ph.x + sb[1] * ph.y + sb[2] * ph.z;
+  }
+  out[0] = a1;
+  out[1] = b1;
+  out[2] = a2;
+  out[3] = b2;
+}
+
 __global__ void k_rt(const FnD* fn, const double* boxc, const int* edge_box, int M, Rule R,
                      zc k1, zc k2, const double* khat, const double* tth, const double* tph, int Q,
                      zc* rt, int e0) {
@@ -33,38 +70,13 @@ __global__ void k_rt(const FnD* fn, const double* boxc, const int* edge_box, int
   vd kh = mkv<double>(khat[3 * q], khat[3 * q + 1], khat[3 * q + 2]);
   vd th = mkv<double>(tth[3 * q], tth[3 * q + 1], tth[3 * q + 2]);
   vd ph = mkv<double>(tph[3 * q], tph[3 * q + 1], tph[3 * q + 2]);
-  zc a1 = mk<double>(0, 0), b1 = a1, a2 = a1, b2 = a1;
-  for (int ll = 0; ll < 2; ll++) {
-    const FnD& f = fn[2 * e + ll];
-    double dfm = f.sgn * f.length;
-    zc sa[3] = {mk<double>(0, 0), mk<double>(0, 0), mk<double>(0, 0)};
-    zc sb[3] = {sa[0], sa[0], sa[0]};
-    for (int j = 0; j < R.n; j++) {
-      double w0 = 1 - R.a[j] - R.b[j];
-      vd Ro = mkv<double>(w0 * f.c[0] + R.a[j] * f.c[3] + R.b[j] * f.c[6],
-                          w0 * f.c[1] + R.a[j] * f.c[4] + R.b[j] * f.c[7],
-                          w0 * f.c[2] + R.a[j] * f.c[5] + R.b[j] * f.c[8]);
-      vd fm = (Ro - mkv<double>(f.c[6], f.c[7], f.c[8])) * 0.5 * dfm;
-      double tmp = dot(kh, Ro - Rc);
-      zc f1 = cexp_mik(k1, tmp) * R.w[j];
-      zc f2 = cexp_mik(k2, tmp) * R.w[j];
-      sa[0] += f1 * fm.x;
-      sa[1] += f1 * fm.y;
-      sa[2] += f1 * fm.z;
-      sb[0] += f2 * fm.x;
-      sb[1] += f2 * fm.y;
-      sb[2] += f2 * fm.z;
-    }
-    a1 += sa[0] * th.x + sa[1] * th.y + sa[2] * th.z;
-    b1 += sa[0] * ph.x + sa[1] * ph.y + sa[2] * ph.z;
-    a2 += sb[0] * th.x + sb[1] * th.y + sb[2] * th.z;
-    b2 += sb[0] * ph.x + sb[1] * ph.y + sb[2] * ph.z;
-  }
+  zc o4[4];
+  rt_edge_q(fn[2 * e], fn[2 * e + 1], Rc, kh, th, ph, R, k1, k2, o4);
   zc* o = rt + (size_t)e * 4 * Q;
-  o[0 * Q + q] = a1;
-  o[1 * Q + q] = b1;
-  o[2 * Q + q] = a2;
-  o[3 * Q + q] = b2;
+  o[0 * Q + q] = o4[0];
+  o[1 * Q + q] = o4[1];
+  o[2 * Q + q] = o4[2];
+  o[3 * Q + q] = o4[3];
 }
 
 // ---------------------------------------------------------------------------
@@ -1558,9 +1570,7 @@ template <typename T>
 int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
                  cudaEvent_t* ev, cudaEvent_t wait_recv) {
   int Q = c->Q;
-  int L0 = c->l_min, L1 = c->l_max;
-  bool k2c = c->mt.k2.im != 0.0;
-  int thr = 128;
+  int L1 = c->l_max;
   // up 1
   {
     Level& L = c->lv[L1];
@@ -1697,6 +1707,119 @@ int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
   SIE_TRY(far_translate_t<double>(c, st, nullptr));
   k_adj_out<<<L.nb, 256, (size_t)8 * Q * sizeof(zc), st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, L.D,
                                                            c->d_qperm, y);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+// Far part of the shape gradient.  With the leaf fields U (the folded D of the forward
+// product on I, what the receive multiplies the patterns by) and C~ (the leaf
+// coefficients of the transposed chain on conj(lambda), read at pi(q)):
+//   lambda^H dZ_far I = sum_e [ sum_q dRT_e . (conj(lambda_e) U) + sum_q C~ . conj(dRT_e) I_e ].
+// Block per (edge, vertex slot): the edge's 4 x Q patterns are differentiated by central
+// differences with that vertex moved by +-h, and -2 Re(...) goes to grad[vertex].
+__global__ void __launch_bounds__(256) k_grad_far(const SideV* __restrict__ sv, const FnD* __restrict__ fn,
+                                                  const double* __restrict__ V, int normal_convention, double h,
+                                                  Rule R, zc k1, zc k2, const double* khat, const double* tth,
+                                                  const double* tph, const double* boxc, const int* edge_box,
+                                                  int Q, const zc* __restrict__ U, const zc* __restrict__ Da,
+                                                  const int* __restrict__ qperm, const zc* __restrict__ lam,
+                                                  const zc* __restrict__ I, double* grad) {
+  const int e = blockIdx.x, slot = blockIdx.y;
+  const int v = edge_vertex(sv, e, slot);
+  const int b = edge_box[e];
+  const vd Rc = mkv<double>(boxc[3 * b], boxc[3 * b + 1], boxc[3 * b + 2]);
+  FnD fp[2], fmn[2];
+  for (int ll = 0; ll < 2; ll++) {
+    fp[ll] = side_fn(sv[2 * e + ll], fn[2 * e + ll].sgn, V, normal_convention, v, h);
+    fmn[ll] = side_fn(sv[2 * e + ll], fn[2 * e + ll].sgn, V, normal_convention, v, -h);
+  }
+  const zc lJ = conj(lam[2 * e]), lM = conj(lam[2 * e + 1]), iJ = I[2 * e], iM = I[2 * e + 1];
+  const zc* Ub = U + (size_t)b * 8 * Q;
+  const zc* Db = Da + (size_t)b * 8 * Q;
+  const double inv = 0.5 / h;
+  zc acc = mk<double>(0, 0);
+  for (int q = threadIdx.x; q < Q; q += blockDim.x) {
+    const vd kh = mkv<double>(khat[3 * q], khat[3 * q + 1], khat[3 * q + 2]);
+    const vd th = mkv<double>(tth[3 * q], tth[3 * q + 1], tth[3 * q + 2]);
+    const vd ph = mkv<double>(tph[3 * q], tph[3 * q + 1], tph[3 * q + 2]);
+    zc rp[4], rm[4], d[4];
+    rt_edge_q(fp[0], fp[1], Rc, kh, th, ph, R, k1, k2, rp);
+    rt_edge_q(fmn[0], fmn[1], Rc, kh, th, ph, R, k1, k2, rm);
+    for (int k = 0; k < 4; k++) d[k] = (rp[k] - rm[k]) * inv;
+    // receive side: rows 2 md + ab against the folded U (index md * 4 + o * 2 + ab)
+    for (int md = 0; md < 2; md++)
+      for (int ab = 0; ab < 2; ab++)
+        acc += d[2 * md + ab] * (lJ * Ub[(size_t)(md * 4 + ab) * Q + q] + lM * Ub[(size_t)(md * 4 + 2 + ab) * Q + q]);
+    // aggregate side: items of C = sum conj(RT) x (0: a1 J, 1: a2 J, 2: a1 M, 3: a2 M,
+    // 4: b1 J, 5: b2 J, 6: b1 M, 7: b2 M)
+    const int qq = qperm[q];
+    const zc c0 = Db[0 * (size_t)Q + qq], c1 = Db[1 * (size_t)Q + qq], c2 = Db[2 * (size_t)Q + qq],
+             c3 = Db[3 * (size_t)Q + qq], c4 = Db[4 * (size_t)Q + qq], c5 = Db[5 * (size_t)Q + qq],
+             c6 = Db[6 * (size_t)Q + qq], c7 = Db[7 * (size_t)Q + qq];
+    acc += conj(d[0]) * (c0 * iJ + c2 * iM) + conj(d[2]) * (c1 * iJ + c3 * iM) +
+           conj(d[1]) * (c4 * iJ + c6 * iM) + conj(d[3]) * (c5 * iJ + c7 * iM);
+  }
+  __shared__ double red[2][8];
+  double re = acc.re;
+  for (int o = 16; o > 0; o >>= 1) re += __shfl_xor_sync(0xffffffffu, re, o);
+  if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = re;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[0][w];
+    atomicAdd(grad + v, -2.0 * s);
+  }
+}
+
+// D of the leaf level folded in place (recv_fold), one-vector layout [box][8][Q].
+__global__ void k_fold_leaf(zc* D, int nb, int Q, RecvConst rc) {
+  const int b = blockIdx.y, q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q || b >= nb) return;
+  zc* d = D + (size_t)b * 8 * Q + q;
+  zc in[8], u[8];
+  for (int i = 0; i < 8; i++) in[i] = d[(size_t)i * Q];
+  recv_fold(in, rc, u);
+  for (int i = 0; i < 8; i++) d[(size_t)i * Q] = u[i];
+}
+
+__global__ void k_conj_copy(const zc* a, zc* b, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = conj(a[i]);
+}
+
+// ws: 2 x (leaf boxes x 8 x Q) + 2M complex128.
+int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, void* ws, cudaStream_t st) {
+  const int Q = c->Q, L1 = c->l_max;
+  Level& L = c->lv[L1];
+  const size_t nl = (size_t)L.nb * 8 * Q;
+  zc* U = (zc*)ws;
+  zc* Da = U + nl;
+  zc* lc = Da + nl;
+  const RecvConst rc = recv_const(c);
+  // forward: leaf D of the product on I, folded
+  {
+    dim3 g((Q + 31) / 32, L.nb);
+    k_aggregate_eg<double><<<g, 256, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, I, L.C);
+    sie::count_launch();
+    SIE_TRY(far_translate_t<double>(c, st, nullptr));
+    SIE_CUDA(cudaMemcpyAsync(U, L.D, nl * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    k_fold_leaf<<<dim3((Q + 127) / 128, L.nb), 128, 0, st>>>(U, L.nb, Q, rc);
+    sie::count_launch();
+  }
+  // transposed chain on conj(lambda)
+  {
+    k_conj_copy<<<296, 256, 0, st>>>(lam, lc, (size_t)2 * c->M);
+    sie::count_launch();
+    dim3 g((Q + 127) / 128, L.nb);
+    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, lc, c->d_qperm, rc, L.C);
+    sie::count_launch();
+    SIE_TRY(far_translate_t<double>(c, st, nullptr));
+    SIE_CUDA(cudaMemcpyAsync(Da, L.D, nl * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+  }
+  k_grad_far<<<dim3(c->M, 4), 256, 0, st>>>((const SideV*)c->d_side, c->d_fn, c->d_vert, c->cfg.normal_convention,
+                                            h, c->R, c->mt.k1, c->mt.k2, c->d_khat, c->d_tth, c->d_tph, c->d_boxc,
+                                            c->d_edge_box, Q, U, Da, c->d_qperm, lam, I, grad);
   sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;

@@ -7,6 +7,7 @@
 #include <cub/cub.cuh>
 
 #include "sie_internal.h"
+#include "geom.cuh"
 
 namespace sie {
 
@@ -183,7 +184,7 @@ __device__ KT outer_regular(const FnD& fm, const FnD& fn, const FillArgs& A) {
     }
     xnt -= dot(cross(nqm, rfm), rfa) * trf;
   }
-  double xf = f32(xnt);  // cmplx(x_nt, 0.0) is binary32
+  double xf = A.smooth ? xnt : f32(xnt);  // cmplx(x_nt, 0.0) is binary32
   r.Kt[0] += mk<double>(-0.5 * xf, 0.0);
   r.Kt[1] += mk<double>(0.5 * xf, 0.0);
   return r;
@@ -258,7 +259,7 @@ __device__ KT outer_singular(const FnD& fm, const FnD& fn, bool self, const Fill
     }
     xnt -= dot(cross(nqm, rfm), rfa) * trf;
   }
-  double xf = f32(xnt);
+  double xf = A.smooth ? xnt : f32(xnt);
   r.Kt[0] += mk<double>(-0.5 * xf, 0.0);
   r.Kt[1] += mk<double>(0.5 * xf, 0.0);
   return r;
@@ -266,7 +267,7 @@ __device__ KT outer_singular(const FnD& fm, const FnD& fn, bool self, const Fill
 
 // tri_outer_integration_edge_adjacent (:2165-2197), PMCHWT only: Kt with a
 // 12-point rule on both triangles.
-__device__ zc outer_edge_adjacent(const FnD& fm, const FnD& fn, int md, zc k) {
+__device__ zc outer_edge_adjacent(const FnD& fm, const FnD& fn, int md, zc k, bool smooth) {
   const float ra12[12] = {0.249286745170910f, 0.249286745170910f, 0.501426509658180f,
                           0.063089014491500f, 0.063089014491500f, 0.873821971017000f,
                           0.310352451033780f, 0.636502499121400f, 0.053145049844820f,
@@ -304,7 +305,7 @@ __device__ zc outer_edge_adjacent(const FnD& fm, const FnD& fn, int md, zc k) {
     Kt += (Ik[0] * rfm.x + Ik[1] * rfm.y + Ik[2] * rfm.z) * trf;
     xnt -= dot(rfa, cross(nqm, rfm)) * trf;
   }
-  double xf = f32(xnt);
+  double xf = smooth ? xnt : f32(xnt);
   return Kt + mk<double>((md == 1 ? -0.5 : 0.5) * xf, 0.0);
 }
 
@@ -334,10 +335,9 @@ __device__ __forceinline__ bool pair_singular(int m, int n, int t, int s, const 
   return !(r_ob > 1.5 * A.rref[m]);
 }
 
-__device__ KT singular_pair(int m, int n, int t, int s, int p, int q, const FillArgs& A,
-                            const int* tri_verts) {
-  const FnD& fm = A.fn[2 * m + t];
-  const FnD& fn = A.fn[2 * n + s];
+// Singular (t, s) term of triangles p, q with the sides given explicitly.
+__device__ KT singular_pair_f(const FnD& fm, const FnD& fn, int p, int q, const FillArgs& A,
+                              const int* tri_verts) {
   bool self = (p == q);
   KT r = outer_singular(fm, fn, self, A);
   if (A.formulation == SIE_PMCHWT && !self) {
@@ -345,11 +345,16 @@ __device__ KT singular_pair(int m, int n, int t, int s, int p, int q, const Fill
     for (int a = 0; a < 3; a++)
       for (int b = 0; b < 3; b++) cnt += (tri_verts[3 * p + a] == tri_verts[3 * q + b]);
     if (cnt == 2) {
-      r.Kt[0] = outer_edge_adjacent(fm, fn, 1, A.mt.k1);
-      r.Kt[1] = outer_edge_adjacent(fm, fn, 2, A.mt.k2);
+      r.Kt[0] = outer_edge_adjacent(fm, fn, 1, A.mt.k1, A.smooth);
+      r.Kt[1] = outer_edge_adjacent(fm, fn, 2, A.mt.k2, A.smooth);
     }
   }
   return r;
+}
+
+__device__ KT singular_pair(int m, int n, int t, int s, int p, int q, const FillArgs& A,
+                            const int* tri_verts) {
+  return singular_pair_f(A.fn[2 * m + t], A.fn[2 * n + s], p, q, A, tri_verts);
 }
 
 // -------------------------------------------------------------------------
@@ -743,6 +748,69 @@ __global__ void __launch_bounds__(128) k_near_T(PanelArgs P, const zc* __restric
   }
 }
 
+// Near part of the shape gradient: for every near block (m, n) and triangle pair (t, s),
+// the z derivative of the (t, s) term with respect to each vertex of the two triangles, by
+// central differences of the term rebuilt with that vertex moved by +-h (same quadrature
+// and the same singular / regular choice as the fill), contracted as -2 Re(conj(lambda_m)
+// dZ_mn I_n) into grad[vertex].
+__global__ void __launch_bounds__(128) k_grad_near(PanelArgs P, FillArgs A, const int* tri_verts,
+                                                   const SideV* __restrict__ sv, const double* __restrict__ V,
+                                                   int normal_convention, double h, long long nnz,
+                                                   const zc* __restrict__ lam, const zc* __restrict__ I,
+                                                   zc cfac, double* grad) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= 4 * nnz) return;
+  const long long idx = it >> 2;
+  const int t = (int)(it >> 1) & 1, s = (int)it & 1;
+  int m, n, B;
+  panel_mn(idx, P, m, n, B);
+  int p, q;
+  const bool sing = pair_singular(m, n, t, s, A, p, q);
+  const SideV sm = sv[2 * m + t], sn = sv[2 * n + s];
+  const double sgm = A.fn[2 * m + t].sgn, sgn = A.fn[2 * n + s].sgn;
+  const zc lJ = conj(lam[2 * m]), lM = conj(lam[2 * m + 1]), iJ = I[2 * n], iM = I[2 * n + 1];
+  const int vs[6] = {sm.t0, sm.t1, sm.t2, sn.t0, sn.t1, sn.t2};
+  for (int k = 0; k < 6; k++) {
+    const int v = vs[k];
+    bool dup = false;
+    for (int j = 0; j < k; j++) dup |= (vs[j] == v);
+    if (dup) continue;
+    zc ab[2][3];
+    for (int pm = 0; pm < 2; pm++) {
+      const double dz = pm ? -h : h;
+      const FnD fm = side_fn(sm, sgm, V, normal_convention, v, dz);
+      const FnD fn = side_fn(sn, sgn, V, normal_convention, v, dz);
+      const KT r = sing ? singular_pair_f(fm, fn, p, q, A, tri_verts) : outer_regular(fm, fn, A);
+      zc a = mk<double>(0, 0), b = a, d = a;
+      combine(r, A, a, b, d);
+      ab[pm][0] = a;
+      ab[pm][1] = b;
+      ab[pm][2] = d;
+    }
+    const double inv = 0.5 / h;
+    const zc da = (ab[0][0] - ab[1][0]) * inv, db = (ab[0][1] - ab[1][1]) * inv, dd = (ab[0][2] - ab[1][2]) * inv;
+    const zc val = lJ * (da * iJ + db * iM) + lM * (cfac * db * iJ + dd * iM);
+    atomicAdd(grad + v, -2.0 * val.re);
+  }
+}
+
+PanelArgs panel_args(sie_ctx* c);
+FillArgs fill_args(sie_ctx* c);
+
+int grad_near(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, cudaStream_t st) {
+  const long long nnz = c->near.nnz;
+  const long long work = 4 * nnz;
+  FillArgs A = fill_args(c);
+  A.smooth = 1;  // differentiate the x_nt term without its binary32 rounding (a staircase)
+  k_grad_near<<<(unsigned)((work + 127) / 128), 128, 0, st>>>(panel_args(c), A, c->d_tri_verts,
+                                                              (const SideV*)c->d_side, c->d_vert,
+                                                              c->cfg.normal_convention, h, nnz, lam, I, c->cfac,
+                                                              grad);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
 // -------------------------------------------------------------------------
 // host wrappers
 
@@ -798,6 +866,7 @@ FillArgs fill_args(sie_ctx* c) {
   A.R = c->R;
   A.formulation = c->cfg.formulation;
   A.fix_itbn = c->cfg.fix_itbn;
+  A.smooth = 0;
   return A;
 }
 

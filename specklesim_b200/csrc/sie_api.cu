@@ -204,6 +204,7 @@ static int build_mesh(sie_ctx* c) {
   c->M = (int)c->elem.size() / 2;
   if (c->M == 0) return fail(SIE_ERR_MESH, "mesh has no interior edge (no RWG basis)");
   c->fn_ext.resize(2 * (size_t)c->M);
+  c->side_v.resize(16 * (size_t)c->M);
   const double* P = c->verts.data();
   for (int e = 0; e < c->M; e++) {
     for (int ot = 0; ot < 2; ot++) {
@@ -258,6 +259,9 @@ static int build_mesh(sie_ctx* c) {
       f.nq[2] = n.z / ln;
       f.tri = t;
       c->fn_ext[2 * e + ot] = f;
+      const int* tv = &c->tris[3 * t];
+      const int sv[8] = {i1, i2, ipc, t, tv[0], tv[1], tv[2], 0};
+      for (int k = 0; k < 8; k++) c->side_v[8 * (2 * (size_t)e + ot) + k] = sv[k];
     }
   }
   return SIE_OK;
@@ -656,6 +660,11 @@ static void record_phase_times(sie_ctx* c, cudaStream_t st) {
 }
 
 int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t st, bool timed) {
+  if (c->op_adjoint) {  // the solver is running the adjoint system Z^H lambda = g
+    for (int r = 0; r < nrhs; r++)
+      SIE_TRY(sie_internal_matvec_adj(c, xi + (size_t)r * 2 * c->M, yi + (size_t)r * 2 * c->M, st));
+    return SIE_OK;
+  }
   for (int r = 0; r < nrhs; r++) {
     const zc* x = xi + (size_t)r * 2 * c->M;
     zc* y = yi + (size_t)r * 2 * c->M;
@@ -938,8 +947,8 @@ int sie_setup(sie_ctx* c) {
     std::vector<double> boxc(3 * (size_t)c->near.nbox);
     for (int b = 0; b < c->near.nbox; b++)
       box_centre(c, c->lv[c->l_max].box[b], c->l_max, &boxc[3 * b]);
-    double* d_boxc = nullptr;
-    SIE_TRY(upload(&d_boxc, boxc));
+    SIE_TRY(upload(&c->d_boxc, boxc));
+    const double* d_boxc = c->d_boxc;
     SIE_CUDA(cudaMalloc(&c->d_rt, (size_t)M * 4 * Q * sizeof(zc)));
     for (int l = c->l_min; l <= c->l_max; l++) {
       Level& L = c->lv[l];
@@ -953,7 +962,6 @@ int sie_setup(sie_ctx* c) {
     cudaEventRecord(c->ev[10], c->stream);
     r = far_build_tables(c, d_boxc);
     cudaEventRecord(c->ev[11], c->stream);
-    cudaFree(d_boxc);
     if (r != SIE_OK) return r;
     SIE_TRY(far_prepare_kernels(c));
   }
@@ -1164,6 +1172,114 @@ int sie_solve(sie_ctx* c, const double* b, double* x, int nrhs, const sie_solver
   return r;
 }
 
+// Gradient tables (once per context): side vertex ids in internal order, vertex
+// coordinates and triangle vertices.
+static int grad_tables(sie_ctx* c) {
+  if (c->d_side) return SIE_OK;
+  std::vector<int> sv(16 * (size_t)c->M);
+  for (int i = 0; i < c->M; i++) {
+    const int e = c->perm[i];
+    for (int k = 0; k < 16; k++) sv[16 * (size_t)i + k] = c->side_v[16 * (size_t)e + k];
+  }
+  SIE_TRY(upload(&c->d_vert, c->verts));
+  SIE_TRY(upload(&c->d_tri_verts, c->tris));
+  SIE_TRY(upload(&c->d_side, sv));
+  return SIE_OK;
+}
+
+int sie_grad(sie_ctx* c, const double* x, const double* k_in, const double* E_in, const double* pts, int npts,
+             const sie_solver_cfg* cfg, double* dJdz, double* J, sie_stats* stats) {
+  if (!c || !x || !k_in || !E_in || !pts || npts < 1 || !cfg || !dJdz)
+    return fail(SIE_ERR_ARG, "sie_grad: bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_grad: sie_setup not called");
+  SIE_CUDA(cudaSetDevice(c->device));
+  SIE_TRY(grad_tables(c));
+  cudaStream_t st = c->stream;
+  const size_t n = (size_t)2 * c->M;
+  const size_t nl = c->cfg.dense ? 0 : (size_t)c->lv[c->l_max].nb * 8 * c->Q;
+  // workspace: x, g, lambda (internal and external), E, H, I, pts, plane wave, grad, far part
+  size_t need = 0;
+  auto add = [&](size_t bytes) {
+    size_t o = need;
+    need += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t ox = add(n * sizeof(zc)), oxe = add(n * sizeof(zc)), og = add(n * sizeof(zc)),
+               oge = add(n * sizeof(zc)), ol = add(n * sizeof(zc)), ole = add(n * sizeof(zc)),
+               oE = add(3 * (size_t)npts * sizeof(zc)), oH = add(3 * (size_t)npts * sizeof(zc)),
+               oI = add((size_t)npts * sizeof(double)), op = add(3 * (size_t)npts * sizeof(double)),
+               ok = add(6 * sizeof(double)), ogr = add((size_t)c->nv * sizeof(double)),
+               ofar = add((2 * nl + n) * sizeof(zc));
+  if (c->grad_ws_bytes < need) {
+    if (c->d_grad_ws) cudaFree(c->d_grad_ws);
+    c->d_grad_ws = nullptr;
+    c->grad_ws_bytes = 0;
+    SIE_CUDA(cudaMalloc(&c->d_grad_ws, need));
+    c->grad_ws_bytes = need;
+  }
+  char* w = (char*)c->d_grad_ws;
+  zc *xi = (zc*)(w + ox), *xe = (zc*)(w + oxe), *gi = (zc*)(w + og), *ge = (zc*)(w + oge);
+  zc *li = (zc*)(w + ol), *le = (zc*)(w + ole), *dE = (zc*)(w + oE), *dH = (zc*)(w + oH);
+  double *dI = (double*)(w + oI), *dp = (double*)(w + op), *dk = (double*)(w + ok), *dg = (double*)(w + ogr);
+  SIE_CUDA(h2d(xe, x, n * sizeof(zc)));
+  SIE_CUDA(h2d(dp, pts, 3 * (size_t)npts * sizeof(double)));
+  SIE_CUDA(h2d(dk, k_in, 3 * sizeof(double)));
+  SIE_CUDA(h2d(dk + 3, E_in, 3 * sizeof(double)));
+  SIE_TRY(gather_ext_to_int(c, xe, xi, 1, st));
+  // objective and the adjoint right-hand side dJ/dI*
+  SIE_TRY(farfield_dev(c, xi, dp, npts, dE, dH, dI));
+  SIE_TRY(field_adjoint_rhs(c, dE, dp, npts, gi, st));
+  SIE_TRY(scatter_int_to_ext(c, gi, ge, 1, st));
+  SIE_CUDA(cudaStreamSynchronize(st));
+  if (J) {
+    std::vector<double> I(npts);
+    SIE_CUDA(cudaMemcpy(I.data(), dI, (size_t)npts * sizeof(double), cudaMemcpyDeviceToHost));
+    double s = 0;
+    for (double v : I) s += v;
+    *J = s;
+  }
+  // adjoint solve Z^H lambda = g (FP64 GMRES on the conjugate-transpose product)
+  sie_solver_cfg acfg = *cfg;
+  acfg.precision = SIE_FP64;
+  acfg.use_initial_guess = 0;
+  sie_stats ast;
+  memset(&ast, 0, sizeof(ast));
+  SIE_TRY(ensure_work(c, 1));
+  int rc = SIE_OK;
+  if (c->cfg.dense) {  // the LU factors give the adjoint solution directly
+    SIE_CUDA(cudaMemcpyAsync(li, gi, n * sizeof(zc), cudaMemcpyDeviceToDevice, st));
+    SIE_TRY(lu_solve_adjoint(c, li));
+    ast.converged = 1;
+  } else {
+    c->op_adjoint = 1;
+    rc = gmres_solve(c, ge, le, &acfg, &ast);
+    c->op_adjoint = 0;
+    if (rc != SIE_OK && rc != SIE_ERR_NOCONV) {
+      if (stats) *stats = ast;
+      return rc;
+    }
+    SIE_TRY(gather_ext_to_int(c, le, li, 1, st));
+  }
+  if (stats) *stats = ast;
+  // dJ/dz = explicit far-field term + 2 Re lambda^H (db - dZ I)
+  const double h = 1e-6 * c->cfg.lambda;
+  // SIE_GRAD_PARTS (bit mask, default all): 1 field factors, 2 right-hand side, 4 near
+  // blocks, 8 far field -- for checking the terms one at a time
+  int parts = 15;
+  if (const char* e = getenv("SIE_GRAD_PARTS")) parts = atoi(e);
+  SIE_CUDA(cudaMemsetAsync(dg, 0, (size_t)c->nv * sizeof(double), st));
+  // the observation points are metres away (~1e7 lambda), so their distances carry an
+  // absolute rounding of ~1e-16 m: the field factors take a step of 1e-4 lambda, where
+  // the phase difference is well above that noise (truncation error ~(k h)^2 = 4e-7)
+  if (parts & 1) SIE_TRY(grad_field(c, dE, dp, npts, xi, 1e-4 * c->cfg.lambda, dg, st));
+  if (parts & 2) SIE_TRY(grad_rhs(c, li, dk, dk + 3, h, dg, st));
+  if (parts & 4) SIE_TRY(grad_near(c, li, xi, h, dg, st));
+  if ((parts & 8) && !c->cfg.dense) SIE_TRY(grad_far(c, li, xi, h, dg, w + ofar, st));
+  SIE_CUDA(cudaStreamSynchronize(st));
+  SIE_CUDA(cudaMemcpy(dJdz, dg, (size_t)c->nv * sizeof(double), cudaMemcpyDeviceToHost));
+  return rc;
+}
+
 int sie_farfield(sie_ctx* c, const double* x, const double* pts, int npts, double* E, double* H,
                  double* intensity) {
   if (!c || !x || !pts || npts < 1) return fail(SIE_ERR_ARG, "sie_farfield: bad argument");
@@ -1331,7 +1447,8 @@ int sie_free(sie_ctx* c) {
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
-                  c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm};
+                  c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
+                  c->d_grad_ws, c->d_tri_verts};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {

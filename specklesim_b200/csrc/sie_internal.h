@@ -87,6 +87,7 @@ struct FillArgs {
   Rule R;
   int formulation;
   int fix_itbn;
+  int smooth;  // 1: x_nt kept in FP64 (shape gradient), 0: rounded to binary32 as the reference
 };
 
 // Near-field matrix laid out per leaf box A: rows = edges of A (internal order),
@@ -163,6 +164,7 @@ struct sie_ctx {
   std::vector<int> elem, corner;  // 2 per edge (reference order)
   std::vector<double> cent;       // 3 per triangle
   std::vector<sie::FnD> fn_ext;   // 2 per edge, reference order
+  std::vector<int> side_v;        // 8 per edge side (p1, p2, pc, tri, triangle's vertices, 0)
   // tree
   double D = 0, xmin[3] = {0, 0, 0};
   int l_min = 0, l_max = 0;
@@ -216,6 +218,15 @@ struct sie_ctx {
   double* d_tph = nullptr;
   double* d_trf = nullptr;
   int* d_qperm = nullptr;         // direction q' with khat_q' = -khat_q, per direction q
+  double* d_boxc = nullptr;       // leaf box centres (3 per leaf box)
+  // gradient (made on the first sie_grad call): side vertex ids in internal order, the
+  // vertex coordinates, and the workspace
+  int* d_side = nullptr;
+  double* d_vert = nullptr;
+  int* d_tri_verts = nullptr;
+  void* d_grad_ws = nullptr;
+  size_t grad_ws_bytes = 0;
+  int op_adjoint = 0;             // the solver's products apply Z^H (adjoint solve)
   zc* d_rt = nullptr;             // internal edge x 4 x Q
   cc* d_rt32 = nullptr;
   float* d_trf32 = nullptr;
@@ -279,6 +290,14 @@ int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaE
 // one adds into it
 int near_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st);
 int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st);
+// shape gradient pieces (grad: one double per mesh vertex, accumulated with atomics)
+int grad_near(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, cudaStream_t st);
+int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, void* ws, cudaStream_t st);
+int grad_rhs(sie_ctx* c, const zc* lam, const double* kin, const double* Ein, double h, double* grad,
+             cudaStream_t st);
+int field_adjoint_rhs(sie_ctx* c, const zc* E, const double* pts, int npts, zc* g, cudaStream_t st);
+int grad_field(sie_ctx* c, const zc* E, const double* pts, int npts, const zc* I, double h, double* grad,
+               cudaStream_t st);
 // largest batch one launch sequence carries (larger batches go in slices)
 static const int SIE_BATCH_MAX = 16;
 int ensure_batch32(sie_ctx* c, int nrhs);
@@ -296,6 +315,8 @@ int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, z
                  double* d_I);
 int gmres_solve(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
 int fgmres_mixed(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
+// Z^H y = g in place (dense contexts, LU factors made on first use)
+int lu_solve_adjoint(sie_ctx* c, zc* d_int);
 // R systems with the same matrix solved together (R <= SIE_BATCH_MAX)
 int fgmres_mixed_batch(sie_ctx* c, const zc* d_b, zc* d_x, int R, const sie_solver_cfg* cfg,
                        sie_stats* st);

@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "sie_internal.h"
+#include "geom.cuh"
 
 namespace sie {
 
@@ -98,17 +99,14 @@ int diag_extract(sie_ctx* c) {
 }
 
 // get_vector_b_tri (:391-460) + incident_field_tri_general (:939-1002), plane wave
-__global__ void k_rhs(const FnD* fn, int M, Rule R, Material mt, int formulation, const double* kin,
-                      const double* Ein, int nrhs, zc* b) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)M * nrhs) return;
-  int r = (int)(i / M), e = (int)(i % M);
-  vd k = mkv<double>(kin[3 * r], kin[3 * r + 1], kin[3 * r + 2]);
-  double E0[3] = {Ein[3 * r], Ein[3 * r + 1], Ein[3 * r + 2]};
+// Right-hand side of one edge for one plane wave (get_vector_b_tri :391-460): the J and M
+// rows, ICTF-scaled.
+__device__ __forceinline__ void rhs_edge(const FnD& f0, const FnD& f1, const Rule& R, const Material& mt,
+                                         int formulation, vd k, const double E0[3], zc& bJ, zc& bM) {
   zc S1 = mk<double>(0, 0), S2 = S1;
   double hc = mt.my1 * C0;
   for (int ot = 0; ot < 2; ot++) {
-    const FnD& f = fn[2 * e + ot];
+    const FnD& f = ot ? f1 : f0;
     for (int j = 0; j < R.n; j++) {
       double w0 = 1 - R.a[j] - R.b[j];
       vd Ra = mkv<double>(w0 * f.c[0] + R.a[j] * f.c[3] + R.b[j] * f.c[6],
@@ -125,14 +123,24 @@ __global__ void k_rhs(const FnD* fn, int M, Rule R, Material mt, int formulation
       S2 += (H[0] * rfm.x + H[1] * rfm.y + H[2] * rfm.z) * wa;
     }
   }
-  zc* o = b + (size_t)r * 2 * M;
   if (formulation == SIE_ICTF) {
-    o[2 * e] = S1 / mt.eta_a;
-    o[2 * e + 1] = S2 * mt.eta_a;
+    bJ = S1 / mt.eta_a;
+    bM = S2 * mt.eta_a;
   } else {
-    o[2 * e] = S1;
-    o[2 * e + 1] = S2;
+    bJ = S1;
+    bM = S2;
   }
+}
+
+__global__ void k_rhs(const FnD* fn, int M, Rule R, Material mt, int formulation, const double* kin,
+                      const double* Ein, int nrhs, zc* b) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)M * nrhs) return;
+  int r = (int)(i / M), e = (int)(i % M);
+  vd k = mkv<double>(kin[3 * r], kin[3 * r + 1], kin[3 * r + 2]);
+  double E0[3] = {Ein[3 * r], Ein[3 * r + 1], Ein[3 * r + 2]};
+  zc* o = b + (size_t)r * 2 * M;
+  rhs_edge(fn[2 * e], fn[2 * e + 1], R, mt, formulation, k, E0, o[2 * e], o[2 * e + 1]);
 }
 
 int rhs_planewave_dev(sie_ctx* c, const double* d_k, const double* d_E, int nrhs, zc* d_b_int) {
@@ -262,6 +270,145 @@ __global__ void k_jacobi(const zc* v1, const zc* diag, int n, zc* v2) {
 int jacobi_apply(sie_ctx* c, const zc* v1, zc* v2, cudaStream_t st) {
   int n = 2 * c->M;
   k_jacobi<<<(n + 255) / 256, 256, 0, st>>>(v1, c->d_diag, n, v2); sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Far-field objective J = sum_o w_o |E(r_o)|^2, w_o = 4 pi |r_o|^2 (the intensity of
+// k_field), and the pieces of its shape gradient that live on single edges.
+
+// E(r_o) = sum_e FJ_e J_e + FM_e M_e: the per-edge field factors of k_field
+// (Integration_scattered_field_tri :2782-2825, the scalar-potential term multiplied by 0).
+__device__ __forceinline__ void field_factors(const FnD& f0, const FnD& f1, vd ra, const Material& mt, zc FJ[3],
+                                              zc FM[3]) {
+  const float ra3[3] = {0.16666666666667f, 0.16666666666667f, 0.66666666666667f};
+  const float rb3[3] = {0.16666666666667f, 0.66666666666667f, 0.16666666666667f};
+  const double w3 = (double)0.33333333333333f;
+  const zc iwm = mk<double>(0, mt.omega * mt.my1);
+  for (int d = 0; d < 3; d++) FJ[d] = FM[d] = mk<double>(0, 0);
+  for (int t = 0; t < 2; t++) {
+    const FnD& f = t ? f1 : f0;
+    double dfm = f.sgn * f.length;
+    for (int i = 0; i < 3; i++) {
+      double a = ra3[i], b = rb3[i], w0 = 1 - a - b;
+      vd rq = mkv<double>(w0 * f.c[0] + a * f.c[3] + b * f.c[6], w0 * f.c[1] + a * f.c[4] + b * f.c[7],
+                          w0 * f.c[2] + a * f.c[5] + b * f.c[8]);
+      vd fm = (rq - mkv<double>(f.c[6], f.c[7], f.c[8])) * 0.5 * dfm;
+      vd dv = ra - rq;
+      double R = vlen(dv);
+      zc ex = cexp_mik(mt.k1, R);
+      zc ikR = mk<double>(-mt.k1.im * R, mt.k1.re * R);
+      zc G = ex * (1.0 / (4 * PI * R));
+      zc DG = -((mk<double>(1, 0) + ikR) * ex) * (1.0 / (4 * PI * R * R));
+      zc gg[3] = {DG * (dv.x / R), DG * (dv.y / R), DG * (dv.z / R)};
+      double fv[3] = {fm.x, fm.y, fm.z};
+      zc fxg[3] = {fv[1] * gg[2] - fv[2] * gg[1], fv[2] * gg[0] - fv[0] * gg[2], fv[0] * gg[1] - fv[1] * gg[0]};
+      zc a1 = iwm * G;
+      for (int d = 0; d < 3; d++) {
+        FJ[d] -= a1 * fv[d] * w3;
+        FM[d] += fxg[d] * w3;
+      }
+    }
+  }
+}
+
+// g = dJ/dI* = sum_o w_o F_o^H E_o, the right-hand side of the adjoint solve (internal layout).
+__global__ void k_field_adjoint_rhs(const FnD* fn, int M, Material mt, const zc* E, const double* pts, int npts,
+                                    zc* g) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M) return;
+  zc gJ = mk<double>(0, 0), gM = gJ;
+  for (int o = 0; o < npts; o++) {
+    const vd ra = mkv<double>(pts[3 * o], pts[3 * o + 1], pts[3 * o + 2]);
+    const double w = 4 * PI * dot(ra, ra);
+    zc FJ[3], FM[3];
+    field_factors(fn[2 * e], fn[2 * e + 1], ra, mt, FJ, FM);
+    for (int d = 0; d < 3; d++) {
+      gJ += conj(FJ[d]) * E[3 * o + d] * w;
+      gM += conj(FM[d]) * E[3 * o + d] * w;
+    }
+  }
+  g[2 * e] = gJ;
+  g[2 * e + 1] = gM;
+}
+
+// Explicit term 2 Re sum_o w_o E_o^H dF_o I per (edge, vertex slot), central differences.
+__global__ void k_grad_field(const SideV* sv, const FnD* fn, const double* V, int normal_convention, double h,
+                             int M, Material mt, const zc* E, const double* pts, int npts, const zc* I,
+                             double* grad) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= 4LL * M) return;
+  const int e = (int)(it >> 2), slot = (int)(it & 3);
+  const int v = edge_vertex(sv, e, slot);
+  FnD fp[2], fmn[2];
+  for (int ll = 0; ll < 2; ll++) {
+    fp[ll] = side_fn(sv[2 * e + ll], fn[2 * e + ll].sgn, V, normal_convention, v, h);
+    fmn[ll] = side_fn(sv[2 * e + ll], fn[2 * e + ll].sgn, V, normal_convention, v, -h);
+  }
+  const zc iJ = I[2 * e], iM = I[2 * e + 1];
+  const double inv = 0.5 / h;
+  zc acc = mk<double>(0, 0);
+  for (int o = 0; o < npts; o++) {
+    const vd ra = mkv<double>(pts[3 * o], pts[3 * o + 1], pts[3 * o + 2]);
+    const double w = 4 * PI * dot(ra, ra);
+    zc FJp[3], FMp[3], FJm[3], FMm[3];
+    field_factors(fp[0], fp[1], ra, mt, FJp, FMp);
+    field_factors(fmn[0], fmn[1], ra, mt, FJm, FMm);
+    for (int d = 0; d < 3; d++)
+      acc += conj(E[3 * o + d]) * (((FJp[d] - FJm[d]) * iJ + (FMp[d] - FMm[d]) * iM) * (inv * w));
+  }
+  atomicAdd(grad + v, 2.0 * acc.re);
+}
+
+// 2 Re(lambda^H db) per (edge, vertex slot), central differences of the plane-wave rows.
+__global__ void k_grad_rhs(const SideV* sv, const FnD* fn, const double* V, int normal_convention, double h,
+                           int M, Rule R, Material mt, int formulation, const double* kin, const double* Ein,
+                           const zc* lam, double* grad) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= 4LL * M) return;
+  const int e = (int)(it >> 2), slot = (int)(it & 3);
+  const int v = edge_vertex(sv, e, slot);
+  const vd k = mkv<double>(kin[0], kin[1], kin[2]);
+  const double E0[3] = {Ein[0], Ein[1], Ein[2]};
+  zc bp[2], bm[2];
+  FnD f0 = side_fn(sv[2 * e], fn[2 * e].sgn, V, normal_convention, v, h);
+  FnD f1 = side_fn(sv[2 * e + 1], fn[2 * e + 1].sgn, V, normal_convention, v, h);
+  rhs_edge(f0, f1, R, mt, formulation, k, E0, bp[0], bp[1]);
+  f0 = side_fn(sv[2 * e], fn[2 * e].sgn, V, normal_convention, v, -h);
+  f1 = side_fn(sv[2 * e + 1], fn[2 * e + 1].sgn, V, normal_convention, v, -h);
+  rhs_edge(f0, f1, R, mt, formulation, k, E0, bm[0], bm[1]);
+  const double inv = 0.5 / h;
+  const zc val = conj(lam[2 * e]) * ((bp[0] - bm[0]) * inv) + conj(lam[2 * e + 1]) * ((bp[1] - bm[1]) * inv);
+  atomicAdd(grad + v, 2.0 * val.re);
+}
+
+int field_adjoint_rhs(sie_ctx* c, const zc* E, const double* pts, int npts, zc* g, cudaStream_t st) {
+  k_field_adjoint_rhs<<<(c->M + 127) / 128, 128, 0, st>>>(c->d_fn, c->M, c->mt, E, pts, npts, g);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+int grad_field(sie_ctx* c, const zc* E, const double* pts, int npts, const zc* I, double h, double* grad,
+               cudaStream_t st) {
+  const long long n = 4LL * c->M;
+  k_grad_field<<<(unsigned)((n + 127) / 128), 128, 0, st>>>((const SideV*)c->d_side, c->d_fn, c->d_vert,
+                                                            c->cfg.normal_convention, h, c->M, c->mt, E, pts,
+                                                            npts, I, grad);
+  sie::count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+int grad_rhs(sie_ctx* c, const zc* lam, const double* kin, const double* Ein, double h, double* grad,
+             cudaStream_t st) {
+  const long long n = 4LL * c->M;
+  k_grad_rhs<<<(unsigned)((n + 127) / 128), 128, 0, st>>>((const SideV*)c->d_side, c->d_fn, c->d_vert,
+                                                          c->cfg.normal_convention, h, c->M, c->R, c->mt,
+                                                          c->cfg.formulation, kin, Ein, lam, grad);
+  sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }

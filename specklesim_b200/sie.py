@@ -52,6 +52,7 @@ class Sie:
         m, l0, l1, nnz = C.c_int(), C.c_int(), C.c_int(), C.c_longlong()
         check(lib.sie_info(self._h, C.byref(m), C.byref(l0), C.byref(l1), C.byref(nnz)))
         self.n_edges = m.value
+        self.nv = v.shape[0]
         self.l_min, self.l_max = l0.value, l1.value
         self.near_nnz = nnz.value
         self._setup = False
@@ -87,6 +88,27 @@ class Sie:
         check(self._lib.sie_matvec_adjoint(self._h, dptr(xx.view(np.float64)), dptr(y.view(np.float64)), nrhs))
         y = y.T
         return y[:, 0] if x.ndim == 1 else y
+
+    def grad(self, x, k_in, E_in, pts, restart=50, max_iterations=2000, tolerance=1e-10,
+             raise_on_noconv=True):
+        """Objective J = sum of far-field intensities at pts for the solution x of the plane
+        wave (k_in, E_in), and dJ/dz of every mesh vertex (adjoint solve in FP64)."""
+        lib = self._lib
+        x = np.ascontiguousarray(_lib.as_c128(x))
+        k = np.ascontiguousarray(k_in, dtype=np.float64)
+        e = np.ascontiguousarray(E_in, dtype=np.float64)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        cfg = SieSolverCfg()
+        lib.sie_solver_default(C.byref(cfg))
+        cfg.restart, cfg.max_iterations, cfg.tolerance = int(restart), int(max_iterations), float(tolerance)
+        g = np.zeros(self.nv)
+        J = C.c_double()
+        st = SieStats()
+        code = lib.sie_grad(self._h, dptr(x.view(np.float64)), dptr(k), dptr(e), dptr(p), p.shape[0],
+                            C.byref(cfg), dptr(g), C.byref(J), C.byref(st))
+        if code != _lib.SIE_OK and not (code == _lib.SIE_ERR_NOCONV and not raise_on_noconv):
+            check(code)
+        return J.value, g, {f: getattr(st, f) for f, _ in SieStats._fields_}
 
     def matvec_device(self, d_x, d_y, nrhs=1, precision="fp64", stream=0):
         """Device-pointer matvec (torch tensors' data_ptr() or raw addresses)."""
