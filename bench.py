@@ -256,6 +256,31 @@ def batched_mixed(g, pts, tol, fp64_sample=4):
     }
 
 
+def gradient_timing(tol):
+    """One shape gradient in the differentiation form's setting: slab10 with seed 2 and the
+    metal, 256 observation directions in a 20-degree cone around specular.  ICTF on this
+    slab stalls in GMRES, so the forward and the adjoint solves both run the reference's
+    budget (restart 50, 650 iterations); the time is sie_grad's wall time (adjoint solve
+    plus the derivative kernels over all vertices)."""
+    from specklesim_b200 import Sie, incidence
+    from specklesim_b200.shape import cone_points
+    V, T = build_mesh("slab10", 2)
+    g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19).setup()
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    x, _ = g.solve(g.rhs_planewave(k, E), restart=50, max_iterations=650, tolerance=tol, raise_on_noconv=False)
+    pts = cone_points(256, [0, 0, 1], 20.0, seed=2)
+    kw = dict(restart=50, max_iterations=650, tolerance=tol, raise_on_noconv=False)
+    g.grad(x, k, E, pts[:8], **kw)  # warm-up: gradient tables and workspace
+    t0 = time.perf_counter()
+    J, dz, st = g.grad(x, k, E, pts, **kw)
+    t = time.perf_counter() - t0
+    g.close()
+    return {"workload": "slab10 seed 2, eps -11.7-1.26i, 256 directions in a 20-degree cone around specular",
+            "vertices": int(len(V)), "seconds": t, "adjoint_solve_seconds": st["seconds"],
+            "adjoint_iterations": st["iterations"], "derivative_kernels_seconds": t - st["seconds"],
+            "objective": J}
+
+
 def committed_traffic():
     """DRAM bytes (read + write) of one matvec's kernels from the committed ncu summary."""
     p = os.path.join(ROOT, "profiles", "matvec_dram_traffic_slab10.md")
@@ -475,8 +500,10 @@ def main():
 
     # ---- mixed precision against plain FP64 at equal tolerance (rank 0, N = 1)
     mixed = None
+    grad = None
     if rank == 0 and world == 1 and not args.no_mixed:
         mixed = mixed_vs_fp64(V, T, args.tol)
+        grad = gradient_timing(args.tol)
 
     # ---- CPU baseline: the oracle on the host cores (rank 0, N = 1)
     cpu = None
@@ -504,7 +531,7 @@ def main():
                 "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],
                 "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
                 "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
-                "mixed_vs_fp64": mixed,
+                "mixed_vs_fp64": mixed, "shape_gradient": grad,
                 "l2": "inputs > L2 (near panels and radiation patterns are GBs)",
             },
             "roofline": roof,
