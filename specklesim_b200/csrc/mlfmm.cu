@@ -1568,7 +1568,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev) {
 
 template <typename T>
 int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStream_t st,
-                 cudaEvent_t* ev, cudaEvent_t wait_recv) {
+                 cudaEvent_t* ev, cudaEvent_t wait_recv, const std::function<int()>* after_agg) {
   int Q = c->Q;
   int L1 = c->l_max;
   // up 1
@@ -1584,6 +1584,7 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[1], st);
+  if (after_agg) SIE_TRY((*after_agg)());
   SIE_TRY(far_translate_t<T>(c, st, ev));
   // the receive adds into y, which the near product (possibly on another stream) writes
   if (wait_recv) SIE_CUDA(cudaStreamWaitEvent(st, wait_recv, 0));
@@ -1826,13 +1827,13 @@ int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, voi
 }
 
 int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev,
-                 cudaEvent_t wait_recv) {
-  return far_matvec_t<double>(c, c->d_rt, x, y, st, ev, wait_recv);
+                 cudaEvent_t wait_recv, const std::function<int()>* after_agg) {
+  return far_matvec_t<double>(c, c->d_rt, x, y, st, ev, wait_recv, after_agg);
 }
 
 int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
-                 cudaEvent_t wait_recv) {
-  return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev, wait_recv);
+                 cudaEvent_t wait_recv, const std::function<int()>* after_agg) {
+  return far_matvec_t<float>(c, c->d_rt32, x, y, st, ev, wait_recv, after_agg);
 }
 
 // Batched coefficient buffers of every level, grown to R vectors of type T.
@@ -1855,7 +1856,7 @@ static int ensure_batch_coeffs(sie_ctx* c, int R) {
 
 template <typename T>
 static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, int R,
-                          cudaStream_t st, cudaEvent_t wait_recv) {
+                          cudaStream_t st, cudaEvent_t wait_recv, const std::function<int()>* after_agg) {
   if (R < 1 || R > SIE_BATCH_MAX) return fail(SIE_ERR_ARG, "batched far product: bad batch size");
   SIE_TRY(ensure_batch_coeffs<T>(c, R));
   const int Q = c->Q, L0 = c->l_min, L1 = c->l_max, M = c->M;
@@ -1871,6 +1872,7 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
     sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
+  if (after_agg) SIE_TRY((*after_agg)());
   for (int l = L1 - 1; l >= L0; l--) {
     Level& P = c->lv[l];
     Level& Ch = c->lv[l + 1];
@@ -1926,12 +1928,14 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
   return SIE_OK;
 }
 
-int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv) {
-  return far_matvec_b_t<double>(c, c->d_rt, x, y, R, st, wait_recv);
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv,
+                   const std::function<int()>* after_agg) {
+  return far_matvec_b_t<double>(c, c->d_rt, x, y, R, st, wait_recv, after_agg);
 }
 
-int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv) {
-  return far_matvec_b_t<float>(c, c->d_rt32, x, y, R, st, wait_recv);
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv,
+                   const std::function<int()>* after_agg) {
+  return far_matvec_b_t<float>(c, c->d_rt32, x, y, R, st, wait_recv, after_agg);
 }
 
 __global__ void k_trf_f32(const double* a, float* b, int n) {

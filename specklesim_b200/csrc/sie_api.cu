@@ -670,14 +670,20 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
     zc* y = yi + (size_t)r * 2 * c->M;
     if (timed) cudaEventRecord(c->ev[0], st);
     if (!c->cfg.dense && c->overlap_near) {
-      // the HBM-bound near product on stream2 overlaps the latency-bound translations;
+      // the HBM-bound near product on stream2 overlaps the latency-bound translations
+      // (mode 2: forked after the HBM-bound aggregate, so the two do not share bandwidth);
       // the receive waits for it because both write y
-      SIE_CUDA(cudaEventRecord(c->ev_fork, st));
-      SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
-      SIE_TRY(near_matvec64(c, x, y, 1, false, c->stream2));
-      if (timed) cudaEventRecord(c->ev[6], c->stream2);
-      SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
-      SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr, c->ev_join));
+      const std::function<int()> fork = [&]() -> int {
+        SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+        SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+        SIE_TRY(near_matvec64(c, x, y, 1, false, c->stream2));
+        if (timed) cudaEventRecord(c->ev[6], c->stream2);
+        SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+        return SIE_OK;
+      };
+      if (c->overlap_near == 1) SIE_TRY(fork());
+      SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr, c->ev_join,
+                           c->overlap_near == 2 ? &fork : nullptr));
     } else {
       SIE_TRY(near_matvec64(c, x, y, 1, false, st));
       if (timed) cudaEventRecord(c->ev[6], st);
@@ -691,12 +697,17 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
 int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool timed) {
   if (timed) cudaEventRecord(c->ev[0], st);
   if (!c->cfg.dense && c->overlap_near) {
-    SIE_CUDA(cudaEventRecord(c->ev_fork, st));
-    SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
-    SIE_TRY(near_matvec32(c, x, y, 1, false, c->stream2));
-    if (timed) cudaEventRecord(c->ev[6], c->stream2);
-    SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
-    SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr, c->ev_join));
+    const std::function<int()> fork = [&]() -> int {
+      SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+      SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+      SIE_TRY(near_matvec32(c, x, y, 1, false, c->stream2));
+      if (timed) cudaEventRecord(c->ev[6], c->stream2);
+      SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+      return SIE_OK;
+    };
+    if (c->overlap_near == 1) SIE_TRY(fork());
+    SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr, c->ev_join,
+                         c->overlap_near == 2 ? &fork : nullptr));
   } else {
     SIE_TRY(near_matvec32(c, x, y, 1, false, st));
     if (timed) cudaEventRecord(c->ev[6], st);
@@ -715,14 +726,18 @@ static int matvec_b_t(sie_ctx* c, const cx<T>* x, cx<T>* y, int R, cudaStream_t 
   for (int r0 = 0; r0 < R; r0 += SIE_BATCH_MAX) {
     const int nr = std::min(SIE_BATCH_MAX, R - r0);
     if (!c->cfg.dense && c->overlap_near) {
-      SIE_CUDA(cudaEventRecord(c->ev_fork, st));
-      SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
-      SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, c->stream2));
-      SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
-      SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, c->ev_join));
+      const std::function<int()> fork = [&]() -> int {
+        SIE_CUDA(cudaEventRecord(c->ev_fork, st));
+        SIE_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+        SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, c->stream2));
+        SIE_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+        return SIE_OK;
+      };
+      if (c->overlap_near == 1) SIE_TRY(fork());
+      SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, c->ev_join, c->overlap_near == 2 ? &fork : nullptr));
     } else {
       SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, st));
-      if (!c->cfg.dense) SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, nullptr));
+      if (!c->cfg.dense) SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, nullptr, nullptr));
     }
   }
   return SIE_OK;
@@ -857,7 +872,7 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_ARNOLDI_MODE")) c->arnoldi_mode = std::max(0, std::min(2, atoi(e)));
-  if (const char* e = getenv("SIE_OVERLAP")) c->overlap_near = atoi(e) != 0;
+  if (const char* e = getenv("SIE_OVERLAP")) c->overlap_near = std::max(0, std::min(2, atoi(e)));
   *out = c;
   return SIE_OK;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -155,7 +156,9 @@ struct sie_ctx {
   cudaEvent_t ev[16];
   // the near-field product runs on stream2 next to the far-field passes
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  int overlap_near = 1;
+  // near product on stream2: 0 no (sequential), 1 forked at the start of the product,
+  // 2 forked once the leaf aggregate is queued, beside the translations only
+  int overlap_near = 2;
 
   // mesh (reference order)
   int nv = 0, nt = 0, M = 0;
@@ -275,17 +278,20 @@ int near_to_f32(sie_ctx* c);
 int near_prepare_kernels(sie_ctx* c);
 int far_build_tables(sie_ctx* c, const double* d_boxc);
 // far-field passes; wait_recv (may be null) is waited for before the receive adds into y
+// after_agg (may be null) is called once the leaf aggregate is queued
 int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* ev,
-                 cudaEvent_t wait_recv = nullptr);
+                 cudaEvent_t wait_recv = nullptr, const std::function<int()>* after_agg = nullptr);
 int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
-                 cudaEvent_t wait_recv = nullptr);
+                 cudaEvent_t wait_recv = nullptr, const std::function<int()>* after_agg = nullptr);
 int far_prepare_kernels(sie_ctx* c);
 // Products of a batch of R right-hand sides (internal layout, vector r at offset r * 2M).
 // The near product writes y; the far product adds into it.
 int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
 int near_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st);
-int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
-int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr);
+int far_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr,
+                   const std::function<int()>* after_agg = nullptr);
+int far_matvec_b32(sie_ctx* c, const cc* x, cc* y, int R, cudaStream_t st, cudaEvent_t wait_recv = nullptr,
+                   const std::function<int()>* after_agg = nullptr);
 // transposed products (y = Z^T x, FP64, internal layout): the near one writes y, the far
 // one adds into it
 int near_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st);
