@@ -1614,34 +1614,54 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
 // step at -khat: SS^T = pi RR pi, RR^T = pi SS pi, SR^T = pi SR pi, so T^T = pi T pi and
 // the translation passes run unchanged between the two permutations.
 
-// R^T then pi: per (leaf box, direction) C[b][i][pi(q)] = Fold^T(sum_e RT_e(q) y_e).
-__global__ void k_adj_in(const zc* __restrict__ rt, const int* box_first, const int* box_cnt, int Q,
-                         const zc* __restrict__ y, const int* __restrict__ qperm, RecvConst rc,
-                         zc* __restrict__ C) {
+// R^T then pi: per (leaf box, direction) C[b][i][pi(q)] = Fold^T(sum_e RT_e(q) y_e).  Block
+// per (leaf box, 32 directions); the 8 warps take every 8th edge of the box (as
+// k_aggregate_eg) and their partial sums meet in shared memory.
+__global__ void __launch_bounds__(256) k_adj_in(const zc* __restrict__ rt, const int* box_first, const int* box_cnt,
+                                                int Q, const zc* __restrict__ y, const int* __restrict__ qperm,
+                                                RecvConst rc, zc* __restrict__ C) {
+  __shared__ zc red[8][8][33];
+  __shared__ zc sum[8][32];
   const int b = blockIdx.y;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= Q) return;
-  zc U[2][2][2];  // [md][o][ab]: o = output of the receive, ab = theta / phi row
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = blockIdx.x * 32 + lane;
+  const bool qok = q < Q;
+  const unsigned long long pol = l2_evict_first_policy();
+  zc U[8];  // index md * 4 + o * 2 + ab: o = output of the receive, ab = theta / phi row
 #pragma unroll
-  for (int md = 0; md < 2; md++) U[md][0][0] = U[md][0][1] = U[md][1][0] = U[md][1][1] = mk<double>(0, 0);
+  for (int i = 0; i < 8; i++) U[i] = mk<double>(0, 0);
   const int f = box_first[b], cnt = box_cnt[b];
-  for (int e = f; e < f + cnt; e++) {
-    const zc* r = rt + (size_t)e * 4 * Q + q;
-    const zc y0 = y[2 * e], y1 = y[2 * e + 1];
+  if (qok) {
+    for (int e = f + w; e < f + cnt; e += 8) {
+      const zc* r = rt + (size_t)e * 4 * Q + q;
+      const zc y0 = y[2 * e], y1 = y[2 * e + 1];
 #pragma unroll
-    for (int md = 0; md < 2; md++)
+      for (int md = 0; md < 2; md++)
 #pragma unroll
-      for (int ab = 0; ab < 2; ab++) {
-        const zc v = r[(size_t)(2 * md + ab) * Q];
-        U[md][0][ab] = cfma(v, y0, U[md][0][ab]);
-        U[md][1][ab] = cfma(v, y1, U[md][1][ab]);
-      }
+        for (int ab = 0; ab < 2; ab++) {
+          const zc v = ld_stream(r + (size_t)(2 * md + ab) * Q, pol);
+          U[md * 4 + ab] = cfma(v, y0, U[md * 4 + ab]);
+          U[md * 4 + 2 + ab] = cfma(v, y1, U[md * 4 + 2 + ab]);
+        }
+    }
   }
+#pragma unroll
+  for (int i = 0; i < 8; i++) red[w][i][lane] = U[i];
+  __syncthreads();
+  {  // warp w sums value w over the 8 edge groups
+    zc s = red[0][w][lane];
+#pragma unroll
+    for (int k = 1; k < 8; k++) s += red[k][w][lane];
+    sum[w][lane] = s;
+  }
+  __syncthreads();
+  if (w != 0 || !qok) return;
   // transpose of the fold (A1, B1, A2, B2) = F (dJt, dMt, dJp, dMp) of the receive
   zc d[8];
 #pragma unroll
   for (int md = 0; md < 2; md++) {
-    const zc A1 = U[md][0][0], B1 = U[md][0][1], A2 = U[md][1][0], B2 = U[md][1][1];
+    const zc A1 = sum[md * 4 + 0][lane], B1 = sum[md * 4 + 1][lane];
+    const zc A2 = sum[md * 4 + 2][lane], B2 = sum[md * 4 + 3][lane];
     d[0 + md] = rc.s1f * rc.my_d[md] * A1 + rc.s2f * rc.kd[md] * B2;
     d[2 + md] = rc.s2f * rc.eps_d[md] * A2 - rc.s1f * rc.kd[md] * B1;
     d[4 + md] = rc.s1f * rc.my_d[md] * B1 - rc.s2f * rc.kd[md] * A2;
@@ -1652,45 +1672,58 @@ __global__ void k_adj_in(const zc* __restrict__ rt, const int* box_first, const 
   for (int i = 0; i < 8; i++) o[(size_t)i * Q] = d[i];
 }
 
-// pi then A^T: x_e[J] = sum_q conj(RT) of the J items of D[b][.][pi(q)], the same for M.
-// Block per leaf box; D of the box, permuted, in shared memory; one warp per edge.
-__global__ void k_adj_out(const zc* __restrict__ rt, const int* box_first, const int* box_cnt, int Q,
-                          const zc* __restrict__ D, const int* __restrict__ qperm, zc* __restrict__ x) {
+// pi then A^T over chunks of <= 32 edges (as k_receive_chunk): the box's D, permuted, in
+// shared memory; each warp streams the radiation patterns of two edges at a time.
+//   x_e[J] = sum_q conj(RT) of the J items of D[b][.][pi(q)], the same for M.
+__global__ void __launch_bounds__(256, 2) k_adj_out(const zc* __restrict__ rt, const int4* __restrict__ chunks,
+                                                    int Q, const zc* __restrict__ D, const int* __restrict__ qperm,
+                                                    zc* __restrict__ x) {
   extern __shared__ __align__(16) unsigned char smraw[];
   zc* sD = reinterpret_cast<zc*>(smraw);  // [8][Q], direction q holds D at pi(q)
-  const int b = blockIdx.x;
+  const int4 ch = chunks[blockIdx.x];
+  const int b = ch.x, f = ch.y, cnt = ch.z;
   const zc* Db = D + (size_t)b * 8 * Q;
   for (int i = threadIdx.x; i < 8 * Q; i += blockDim.x) {
     const int it = i / Q, q = i - it * Q;
     sD[i] = Db[(size_t)it * Q + qperm[q]];
   }
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int f = box_first[b], cnt = box_cnt[b];
-  for (int e = f + warp; e < f + cnt; e += nw) {
-    const zc* r = rt + (size_t)e * 4 * Q;
-    zc sJ = mk<double>(0, 0), sM = sJ;
+  const unsigned long long pol = l2_evict_first_policy();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e0 = f + 2 * warp; e0 < f + cnt; e0 += 16) {
+    const bool two = e0 + 1 < f + cnt;
+    const zc* r0 = rt + (size_t)e0 * 4 * Q;
+    const zc* r1 = two ? r0 + 4 * Q : r0;
+    zc s[2][2];
+    s[0][0] = s[0][1] = s[1][0] = s[1][1] = mk<double>(0, 0);
     for (int q = lane; q < Q; q += 32) {
-      const zc ra1 = r[q], rb1 = r[Q + q], ra2 = r[2 * Q + q], rb2 = r[3 * Q + q];
-      sJ = cfma_conj(ra1, sD[0 * Q + q], sJ);
-      sJ = cfma_conj(ra2, sD[1 * Q + q], sJ);
-      sJ = cfma_conj(rb1, sD[4 * Q + q], sJ);
-      sJ = cfma_conj(rb2, sD[5 * Q + q], sJ);
-      sM = cfma_conj(ra1, sD[2 * Q + q], sM);
-      sM = cfma_conj(ra2, sD[3 * Q + q], sM);
-      sM = cfma_conj(rb1, sD[6 * Q + q], sM);
-      sM = cfma_conj(rb2, sD[7 * Q + q], sM);
+      zc g[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) g[k] = sD[k * Q + q];
+      zc a0[4], a1[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        a0[k] = ld_stream(r0 + k * Q + q, pol);
+        a1[k] = ld_stream(r1 + k * Q + q, pol);
+      }
+      // rows: 0 a1 (medium 1 theta), 1 b1, 2 a2, 3 b2; items J: 0 a1, 1 a2, 4 b1, 5 b2; M: 2, 3, 6, 7
+      s[0][0] = cfma_conj(a0[0], g[0], cfma_conj(a0[2], g[1], cfma_conj(a0[1], g[4], cfma_conj(a0[3], g[5], s[0][0]))));
+      s[0][1] = cfma_conj(a0[0], g[2], cfma_conj(a0[2], g[3], cfma_conj(a0[1], g[6], cfma_conj(a0[3], g[7], s[0][1]))));
+      s[1][0] = cfma_conj(a1[0], g[0], cfma_conj(a1[2], g[1], cfma_conj(a1[1], g[4], cfma_conj(a1[3], g[5], s[1][0]))));
+      s[1][1] = cfma_conj(a1[0], g[2], cfma_conj(a1[2], g[3], cfma_conj(a1[1], g[6], cfma_conj(a1[3], g[7], s[1][1]))));
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sJ.re += __shfl_xor_sync(0xffffffffu, sJ.re, o);
-      sJ.im += __shfl_xor_sync(0xffffffffu, sJ.im, o);
-      sM.re += __shfl_xor_sync(0xffffffffu, sM.re, o);
-      sM.im += __shfl_xor_sync(0xffffffffu, sM.im, o);
-    }
-    if (lane == 0) {
-      x[2 * e] += sJ;
-      x[2 * e + 1] += sM;
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int k = 0; k < 2; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          s[j][k].re += __shfl_xor_sync(0xffffffffu, s[j][k].re, o);
+          s[j][k].im += __shfl_xor_sync(0xffffffffu, s[j][k].im, o);
+        }
+    if (lane < 4) {
+      const int j = lane >> 1, k = lane & 1;
+      if (j == 0 || two) x[2 * (e0 + j) + k] += (j == 0) ? (k == 0 ? s[0][0] : s[0][1]) : (k == 0 ? s[1][0] : s[1][1]);
     }
   }
 }
@@ -1700,14 +1733,14 @@ int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
   const int Q = c->Q, L1 = c->l_max;
   Level& L = c->lv[L1];
   {
-    dim3 g((Q + 127) / 128, L.nb);
-    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, x, c->d_qperm, recv_const(c), L.C);
+    dim3 g((Q + 31) / 32, L.nb);
+    k_adj_in<<<g, 256, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, x, c->d_qperm, recv_const(c), L.C);
     sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   SIE_TRY(far_translate_t<double>(c, st, nullptr));
-  k_adj_out<<<L.nb, 256, (size_t)8 * Q * sizeof(zc), st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, L.D,
-                                                           c->d_qperm, y);
+  k_adj_out<<<c->n_rchunk, 256, (size_t)8 * Q * sizeof(zc), st>>>(c->d_rt, (const int4*)c->d_rchunk, Q, L.D,
+                                                                  c->d_qperm, y);
   sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
@@ -1812,8 +1845,8 @@ int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, voi
   {
     k_conj_copy<<<296, 256, 0, st>>>(lam, lc, (size_t)2 * c->M);
     sie::count_launch();
-    dim3 g((Q + 127) / 128, L.nb);
-    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, lc, c->d_qperm, rc, L.C);
+    dim3 g((Q + 31) / 32, L.nb);
+    k_adj_in<<<g, 256, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, lc, c->d_qperm, rc, L.C);
     sie::count_launch();
     SIE_TRY(far_translate_t<double>(c, st, nullptr));
     SIE_CUDA(cudaMemcpyAsync(Da, L.D, nl * sizeof(zc), cudaMemcpyDeviceToDevice, st));

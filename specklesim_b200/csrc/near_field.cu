@@ -706,46 +706,31 @@ __global__ void __launch_bounds__(256) k_near_b(PanelArgs P, const cx<T>* __rest
   }
 }
 
-// Transposed near product y = Z_near^T x (FP64, writes y).  Block per (leaf box B,
-// 128 of its edges n): for every box A of E2(B) (E2 is symmetric, so B is in E2(A) and
-// its edges are a column range of A's panel) it sums the 2 x 2 blocks of column n over the
-// rows of A, transposed: y_J[n] += a x_J[m] + cfac b x_M[m], y_M[n] += b x_J[m] + d x_M[m].
-// Consecutive threads read consecutive columns of each panel row.
-__global__ void __launch_bounds__(128) k_near_T(PanelArgs P, const zc* __restrict__ va,
-                                                const zc* __restrict__ vb, const zc* __restrict__ vd_,
-                                                zc cfac, const zc* __restrict__ x, zc* __restrict__ y) {
-  const int B = blockIdx.y;
-  const int fB = P.box_first[B], cB = P.box_cnt[B];
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (blockIdx.x * blockDim.x >= cB) return;
-  zc sJ = mk<double>(0, 0), sM = sJ;
-  for (int k = P.nbr_ptr[B]; k < P.nbr_ptr[B + 1]; k++) {
-    const int A = P.nbr_box[k];
-    // column offset of B's edges in A's panel: the boxes of E2(A) before B
-    int col0 = 0;
-    for (int kk = P.nbr_ptr[A]; kk < P.nbr_ptr[A + 1]; kk++) {
-      const int Bp = P.nbr_box[kk];
-      if (Bp == B) break;
-      col0 += P.box_cnt[Bp];
-    }
-    const int fA = P.box_first[A], cA = P.box_cnt[A], nc = P.ncols[A];
-    if (j < cB) {
-      const long long base = P.base[A] + col0 + j;
-      for (int m = 0; m < cA; m++) {
-        const long long o = base + (long long)m * nc;
-        const zc a = va[o], b = vb[o], d = vd_[o];
-        const zc xj = x[2 * (fA + m)], xm = x[2 * (fA + m) + 1];
-        sJ = cfma(a, xj, sJ);
-        sJ = cfma(cfac * b, xm, sJ);
-        sM = cfma(b, xj, sM);
-        sM = cfma(d, xm, sM);
-      }
-    }
+// Transposed near panels, made once for the adjoint product.  E2 is symmetric, so the
+// transposed matrix has the forward panels' layout: element (row n, column m) of box B's
+// panel is Z[m, n], found in the panel of box(m) at row m and at the column of n, which
+// lies in the column range of B there.  The 2 x 2 block [[a, b], [cfac b, d]] transposes
+// to [[a, cfac b], [b, d]]; stored as (a, cfac b, d), the forward product kernels apply it
+// with cfac replaced by 1 / cfac.
+__global__ void k_transpose_panels(PanelArgs P, const int* __restrict__ edge_box, long long nnz,
+                                   const zc* __restrict__ va, const zc* __restrict__ vb,
+                                   const zc* __restrict__ vd_, zc cfac, zc* __restrict__ ta,
+                                   zc* __restrict__ tb, zc* __restrict__ td) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nnz) return;
+  int n, m, B;
+  panel_mn(idx, P, n, m, B);  // transposed panel of box B: row edge n, column edge m
+  const int Bm = edge_box[m];
+  int col0 = 0;
+  for (int k = P.nbr_ptr[Bm]; k < P.nbr_ptr[Bm + 1]; k++) {
+    const int Bp = P.nbr_box[k];
+    if (Bp == B) break;
+    col0 += P.box_cnt[Bp];
   }
-  if (j < cB) {
-    y[2 * (fB + j)] = sJ;
-    y[2 * (fB + j) + 1] = sM;
-  }
+  const long long src = P.base[Bm] + (long long)(m - P.box_first[Bm]) * P.ncols[Bm] + col0 + (n - P.box_first[B]);
+  ta[idx] = va[src];
+  tb[idx] = cfac * vb[src];
+  td[idx] = vd_[src];
 }
 
 // Near part of the shape gradient: for every near block (m, n) and triangle pair (t, s),
@@ -986,13 +971,20 @@ static int near_matvec_b_t(sie_ctx* c, const cx<T>* va, const cx<T>* vb, const c
 }
 
 int near_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
-  int cmax = 1;
-  for (int b = 0; b < c->near.nbox; b++) cmax = std::max(cmax, c->near.box_cnt[b]);
-  dim3 g((cmax + 127) / 128, c->near.nbox);
-  k_near_T<<<g, 128, 0, st>>>(panel_args(c), c->d_na, c->d_nb, c->d_nd, c->cfac, x, y);
-  sie::count_launch();
-  SIE_CUDA(cudaGetLastError());
-  return SIE_OK;
+  const long long nnz = c->near.nnz;
+  if (!c->d_naT) {
+    const size_t bytes = (size_t)std::max<long long>(nnz, 1) * sizeof(zc);
+    SIE_CUDA(cudaMalloc(&c->d_naT, bytes));
+    SIE_CUDA(cudaMalloc(&c->d_nbT, bytes));
+    SIE_CUDA(cudaMalloc(&c->d_ndT, bytes));
+    k_transpose_panels<<<(unsigned)((nnz + 255) / 256), 256, 0, st>>>(panel_args(c), c->d_edge_box, nnz, c->d_na,
+                                                                      c->d_nb, c->d_nd, c->cfac, c->d_naT,
+                                                                      c->d_nbT, c->d_ndT);
+    sie::count_launch();
+    SIE_CUDA(cudaGetLastError());
+  }
+  const zc inv = mk<double>(1.0, 0.0) / c->cfac;
+  return near_matvec_t<double>(c, c->d_naT, c->d_nbT, c->d_ndT, inv, x, y, 1, false, st);
 }
 
 int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st) {

@@ -1463,7 +1463,7 @@ int sie_free(sie_ctx* c) {
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
-                  c->d_grad_ws, c->d_tri_verts};
+                  c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->lv) {

@@ -210,6 +210,9 @@ struct sie_ctx {
   zc* d_na = nullptr;
   zc* d_nb = nullptr;
   zc* d_nd = nullptr;
+  zc* d_naT = nullptr;            // transposed panels (adjoint product, made on first use)
+  zc* d_nbT = nullptr;
+  zc* d_ndT = nullptr;
   cc* d_na32 = nullptr;
   cc* d_nb32 = nullptr;
   cc* d_nd32 = nullptr;
