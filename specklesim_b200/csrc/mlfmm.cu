@@ -1614,54 +1614,35 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
 // step at -khat: SS^T = pi RR pi, RR^T = pi SS pi, SR^T = pi SR pi, so T^T = pi T pi and
 // the translation passes run unchanged between the two permutations.
 
-// R^T then pi: per (leaf box, direction) C[b][i][pi(q)] = Fold^T(sum_e RT_e(q) y_e).  Block
-// per (leaf box, 32 directions); the 8 warps take every 8th edge of the box (as
-// k_aggregate_eg) and their partial sums meet in shared memory.
-__global__ void __launch_bounds__(256) k_adj_in(const zc* __restrict__ rt, const int* box_first, const int* box_cnt,
-                                                int Q, const zc* __restrict__ y, const int* __restrict__ qperm,
-                                                RecvConst rc, zc* __restrict__ C) {
-  __shared__ zc red[8][8][33];
-  __shared__ zc sum[8][32];
+// R^T then pi: per (leaf box, direction) C[b][i][pi(q)] = Fold^T(sum_e RT_e(q) y_e); thread per
+// (direction, leaf box).  (An 8-edge-group block as in k_aggregate_eg measured slower here.)
+__global__ void k_adj_in(const zc* __restrict__ rt, const int* box_first, const int* box_cnt, int Q,
+                         const zc* __restrict__ y, const int* __restrict__ qperm, RecvConst rc,
+                         zc* __restrict__ C) {
   const int b = blockIdx.y;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int q = blockIdx.x * 32 + lane;
-  const bool qok = q < Q;
-  const unsigned long long pol = l2_evict_first_policy();
-  zc U[8];  // index md * 4 + o * 2 + ab: o = output of the receive, ab = theta / phi row
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= Q) return;
+  zc U[2][2][2];  // [md][o][ab]: o = output of the receive, ab = theta / phi row
 #pragma unroll
-  for (int i = 0; i < 8; i++) U[i] = mk<double>(0, 0);
+  for (int md = 0; md < 2; md++) U[md][0][0] = U[md][0][1] = U[md][1][0] = U[md][1][1] = mk<double>(0, 0);
   const int f = box_first[b], cnt = box_cnt[b];
-  if (qok) {
-    for (int e = f + w; e < f + cnt; e += 8) {
-      const zc* r = rt + (size_t)e * 4 * Q + q;
-      const zc y0 = y[2 * e], y1 = y[2 * e + 1];
+  for (int e = f; e < f + cnt; e++) {
+    const zc* r = rt + (size_t)e * 4 * Q + q;
+    const zc y0 = y[2 * e], y1 = y[2 * e + 1];
 #pragma unroll
-      for (int md = 0; md < 2; md++)
+    for (int md = 0; md < 2; md++)
 #pragma unroll
-        for (int ab = 0; ab < 2; ab++) {
-          const zc v = ld_stream(r + (size_t)(2 * md + ab) * Q, pol);
-          U[md * 4 + ab] = cfma(v, y0, U[md * 4 + ab]);
-          U[md * 4 + 2 + ab] = cfma(v, y1, U[md * 4 + 2 + ab]);
-        }
-    }
+      for (int ab = 0; ab < 2; ab++) {
+        const zc v = r[(size_t)(2 * md + ab) * Q];
+        U[md][0][ab] = cfma(v, y0, U[md][0][ab]);
+        U[md][1][ab] = cfma(v, y1, U[md][1][ab]);
+      }
   }
-#pragma unroll
-  for (int i = 0; i < 8; i++) red[w][i][lane] = U[i];
-  __syncthreads();
-  {  // warp w sums value w over the 8 edge groups
-    zc s = red[0][w][lane];
-#pragma unroll
-    for (int k = 1; k < 8; k++) s += red[k][w][lane];
-    sum[w][lane] = s;
-  }
-  __syncthreads();
-  if (w != 0 || !qok) return;
   // transpose of the fold (A1, B1, A2, B2) = F (dJt, dMt, dJp, dMp) of the receive
   zc d[8];
 #pragma unroll
   for (int md = 0; md < 2; md++) {
-    const zc A1 = sum[md * 4 + 0][lane], B1 = sum[md * 4 + 1][lane];
-    const zc A2 = sum[md * 4 + 2][lane], B2 = sum[md * 4 + 3][lane];
+    const zc A1 = U[md][0][0], B1 = U[md][0][1], A2 = U[md][1][0], B2 = U[md][1][1];
     d[0 + md] = rc.s1f * rc.my_d[md] * A1 + rc.s2f * rc.kd[md] * B2;
     d[2 + md] = rc.s2f * rc.eps_d[md] * A2 - rc.s1f * rc.kd[md] * B1;
     d[4 + md] = rc.s1f * rc.my_d[md] * B1 - rc.s2f * rc.kd[md] * A2;
@@ -1733,8 +1714,8 @@ int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
   const int Q = c->Q, L1 = c->l_max;
   Level& L = c->lv[L1];
   {
-    dim3 g((Q + 31) / 32, L.nb);
-    k_adj_in<<<g, 256, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, x, c->d_qperm, recv_const(c), L.C);
+    dim3 g((Q + 127) / 128, L.nb);
+    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, x, c->d_qperm, recv_const(c), L.C);
     sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
@@ -1845,8 +1826,8 @@ int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, voi
   {
     k_conj_copy<<<296, 256, 0, st>>>(lam, lc, (size_t)2 * c->M);
     sie::count_launch();
-    dim3 g((Q + 31) / 32, L.nb);
-    k_adj_in<<<g, 256, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, lc, c->d_qperm, rc, L.C);
+    dim3 g((Q + 127) / 128, L.nb);
+    k_adj_in<<<g, 128, 0, st>>>(c->d_rt, c->d_box_first, c->d_box_cnt, Q, lc, c->d_qperm, rc, L.C);
     sie::count_launch();
     SIE_TRY(far_translate_t<double>(c, st, nullptr));
     SIE_CUDA(cudaMemcpyAsync(Da, L.D, nl * sizeof(zc), cudaMemcpyDeviceToDevice, st));
