@@ -114,6 +114,13 @@ int sie_matvec(sie_ctx* ctx, const double* x, double* y, int nrhs, int precision
 int sie_matvec_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, int precision,
                       void* stream);
 
+/* Operator of the SIE_MIXED solver's inner complex64 products: another context set up on
+ * the same mesh with the same tree (e.g. a lower truncation number, a cheaper
+ * preconditioner operator); NULL restores ctx itself.  The outer FP64 products, and so the
+ * solution's accuracy, stay those of ctx.  No counterpart in the reference.  The caller
+ * keeps `inner` alive while it is linked. */
+int sie_set_inner_operator(sie_ctx* ctx, sie_ctx* inner);
+
 /* Conjugate-transpose product y = Z^H x in FP64 for nrhs vectors (stride 2M), the operator
  * of the adjoint solve Z^H lambda = dJ/dI* that a far-field gradient needs.  The reference
  * has no adjoint; this is the exact transpose of the product sie_matvec applies (near

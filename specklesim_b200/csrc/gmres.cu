@@ -1151,7 +1151,7 @@ static int inner_gmres32(sie_ctx* c, Gm32& g, const cc* r, cc* z, double tol, in
   };
   bool stop = false;
   for (int j = 0; j < m && !stop; j++) {
-    SIE_TRY(sie_internal_matvec32(c, g.V + (size_t)j * ld, g.w, s, false));
+    SIE_TRY(sie_internal_matvec32(c->inner ? c->inner : c, g.V + (size_t)j * ld, g.w, s, false));
     mvs++;
     SIE_TRY(arnoldi_launch32(g, j, beta, s));
     SIE_CUDA(cudaMemcpyAsync(&slots[j & 1], g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
@@ -1171,6 +1171,7 @@ int fgmres_mixed(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solver_cf
   if (cfg->inner_restart < 1 || !(cfg->inner_tolerance > 0))
     return fail(SIE_ERR_ARG, "mixed solve: bad inner solver settings");
   SIE_TRY(make_f32_tables(c));
+  if (c->inner) SIE_TRY(make_f32_tables(c->inner));
   int m = cfg->restart;
   Gm g;
   SIE_TRY(gm_alloc(c, m, g));
@@ -1610,7 +1611,7 @@ static int inner_batch32(sie_ctx* c, GmB& g, double tol) {
   k_binit<float, float><<<grid, RT_, 0, s>>>(g.r32, n, g.pA, g.ldp, g.V32, g.Hi, mi, g.sti, 1, nullptr);
   sie::count_launch();
   for (int j = 0; j < mi; j++) {
-    SIE_TRY(sie_internal_matvec_b32(c, g.V32 + (size_t)j * g.ldj, g.w32, R, s));
+    SIE_TRY(sie_internal_matvec_b32(c->inner ? c->inner : c, g.V32 + (size_t)j * g.ldj, g.w32, R, s));
     SIE_TRY(barnoldi<float>(g.V32, g.ldj, g.w32, n, R, j, g.pA, g.pB, g.ldp, g.Hi, mi, g.rci, g.rsi, g.sti, tol, s));
   }
   k_btrsv<<<R, 32, 0, s>>>(g.Hi, mi, g.sti, g.yi); sie::count_launch();
@@ -1628,6 +1629,7 @@ int fgmres_mixed_batch(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, int R, const 
   if (mi < 1 || mi + 1 > BJMAX || mo + 1 > BJMAX || !(cfg->inner_tolerance > 0))
     return fail(SIE_ERR_ARG, "batched solve: restarts must be 1..63");
   SIE_TRY(make_f32_tables(c));
+  if (c->inner) SIE_TRY(make_f32_tables(c->inner));
   GmB g;
   SIE_TRY(gmb_alloc(c, R, mi, mo, g));
   const int n = g.n;

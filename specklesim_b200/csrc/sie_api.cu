@@ -1060,6 +1060,18 @@ int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) 
   return r;
 }
 
+int sie_set_inner_operator(sie_ctx* c, sie_ctx* inner) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_set_inner_operator: null context");
+  if (inner) {
+    if (!c->setup_done || !inner->setup_done) return fail(SIE_ERR_STATE, "sie_set_inner_operator: sie_setup not called");
+    if (inner == c || inner->M != c->M || inner->perm != c->perm || inner->device != c->device)
+      return fail(SIE_ERR_ARG, "sie_set_inner_operator: needs a different context on the same mesh, tree and device");
+    if (inner->inner) return fail(SIE_ERR_ARG, "sie_set_inner_operator: the inner context has an inner operator itself");
+  }
+  c->inner = inner;
+  return SIE_OK;
+}
+
 int sie_matvec_adjoint_device(sie_ctx* c, const double* d_x, double* d_y, int nrhs, void* stream) {
   if (!c || !d_x || !d_y || nrhs < 1) return fail(SIE_ERR_ARG, "sie_matvec_adjoint_device: bad argument");
   if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_matvec_adjoint_device: sie_setup not called");

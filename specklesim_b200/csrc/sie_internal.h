@@ -233,6 +233,7 @@ struct sie_ctx {
   void* d_grad_ws = nullptr;
   size_t grad_ws_bytes = 0;
   int op_adjoint = 0;             // the solver's products apply Z^H (adjoint solve)
+  sie_ctx* inner = nullptr;       // operator of the mixed solver's inner products (null: this one)
   zc* d_rt = nullptr;             // internal edge x 4 x Q
   cc* d_rt32 = nullptr;
   float* d_trf32 = nullptr;

@@ -79,6 +79,12 @@ class Sie:
         y = y.T
         return y[:, 0] if x.ndim == 1 else y
 
+    def set_inner_operator(self, other):
+        """Inner complex64 products of the mixed solver through `other` (a context on the
+        same mesh and tree, e.g. with a lower truncation number); None restores this one."""
+        check(self._lib.sie_set_inner_operator(self._h, other._h if other is not None else None))
+        self._inner = other  # keep it alive while linked
+
     def matvec_adjoint(self, x):
         """y = Z^H x (FP64), the operator of the adjoint solve."""
         x = _lib.as_c128(x)

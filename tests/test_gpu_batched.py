@@ -128,3 +128,34 @@ def test_batched_overlap_gives_the_same_product(gpu_lib, monkeypatch):
         g.close()
     for o in out[1:]:
         assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
+
+
+def test_batched_mixed_solve_with_cheaper_inner_operator(diel, gpu_lib):
+    """Inner complex64 products through a K = 12 context on the same mesh: the outer FP64
+    products are unchanged, so the solutions still reach the FP64 tolerance and agree with
+    one-at-a-time FP64 solves."""
+    from specklesim_b200 import Sie, SieError, incidence
+    g = diel
+    V, T = P.slab(cells=24, length_wl=6.0, seed=3)
+    gi = Sie(V, T, P.WL, P.EPS_DIELECTRIC, tree_s_opt=100, truncation_number=12).setup()
+    other = Sie(*P.sphere(sub=1), P.WL, P.EPS_DIELECTRIC).setup()
+    try:
+        with pytest.raises(SieError):
+            g.set_inner_operator(other)  # a different mesh
+        g.set_inner_operator(gi)
+        inc = [incidence(np.deg2rad(t), 0.0, "TM", 2) for t in (0, 20, 30)]
+        B = np.stack([g.rhs_planewave(k, E) for k, E in inc], axis=1)
+        X, st = g.solve(B, restart=10, max_iterations=60, tolerance=1e-8, precision="mixed",
+                        inner_restart=30, inner_tolerance=1e-2)
+        x1, s1 = g.solve(B[:, 1], restart=10, max_iterations=60, tolerance=1e-8, precision="mixed",
+                         inner_restart=30, inner_tolerance=1e-2)
+        g.set_inner_operator(None)
+        assert s1["converged"] and s1["backward_error_true"] <= 1e-8
+        for j in range(B.shape[1]):
+            assert st[j]["converged"] and st[j]["backward_error_true"] <= 1e-8
+            x64, _ = g.solve(B[:, j], restart=50, max_iterations=3000, tolerance=1e-8)
+            assert rel(X[:, j], x64) < 1e-5, (j, rel(X[:, j], x64))
+    finally:
+        g.set_inner_operator(None)
+        gi.close()
+        other.close()
