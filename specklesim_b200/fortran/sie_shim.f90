@@ -37,6 +37,27 @@ module sie_gpu_c
     integer(c_int) :: dense
   end type sie_config
 
+  type, bind(C) :: sie_solver_cfg
+    integer(c_int) :: restart
+    integer(c_int) :: max_iterations
+    real(c_double) :: tolerance
+    integer(c_int) :: use_initial_guess
+    integer(c_int) :: precision
+    integer(c_int) :: inner_restart
+    real(c_double) :: inner_tolerance
+    real(c_double) :: time_limit_s
+  end type sie_solver_cfg
+
+  type, bind(C) :: sie_stats
+    integer(c_int) :: iterations
+    integer(c_int) :: inner_iterations
+    integer(c_int) :: matvecs
+    integer(c_int) :: converged
+    real(c_double) :: backward_error_arnoldi
+    real(c_double) :: backward_error_true
+    real(c_double) :: seconds
+  end type sie_stats
+
   interface
     subroutine sie_config_default(cfg) bind(C, name="sie_config_default")
       import :: sie_config
@@ -78,6 +99,33 @@ module sie_gpu_c
     function sie_precondition_left(ctx, v1, v2) bind(C, name="sie_precondition_left") result(rc)
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx, v1, v2
+      integer(c_int) :: rc
+    end function
+    subroutine sie_solver_default(cfg) bind(C, name="sie_solver_default")
+      import :: sie_solver_cfg
+      type(sie_solver_cfg), intent(out) :: cfg
+    end subroutine
+    function sie_matvec_adjoint(ctx, x, y, nrhs) bind(C, name="sie_matvec_adjoint") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, x, y
+      integer(c_int), value :: nrhs
+      integer(c_int) :: rc
+    end function
+    function sie_grad(ctx, x, k_in, e_in, pts, npts, cfg, dJdz, J, stats) bind(C, name="sie_grad") result(rc)
+      import :: c_int, c_double, c_ptr, sie_solver_cfg, sie_stats
+      type(c_ptr), value :: ctx, x
+      real(c_double), intent(in) :: k_in(3), e_in(3)
+      type(c_ptr), value :: pts
+      integer(c_int), value :: npts
+      type(sie_solver_cfg), intent(in) :: cfg
+      type(c_ptr), value :: dJdz
+      real(c_double), intent(out) :: J
+      type(sie_stats), intent(out) :: stats
+      integer(c_int) :: rc
+    end function
+    function sie_set_inner_operator(ctx, inner) bind(C, name="sie_set_inner_operator") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, inner
       integer(c_int) :: rc
     end function
     function sie_free(ctx) bind(C, name="sie_free") result(rc)
@@ -124,6 +172,10 @@ module lib_sie_tri_mlfmm_interface
   public :: lib_sie_ml_fmm_save_vector_x_tri
   public :: run_MLFMM_one_forward_tri
   public :: lib_sie_ml_fmm_preconditioner_left
+  ! additions with no counterpart in the reference module: the adjoint product and the
+  ! shape gradient of the far-field intensity
+  public :: lib_sie_ml_fmm_adjoint_tri
+  public :: lib_sie_ml_fmm_grad_z_tri
 
   type(c_ptr), save :: m_ctx = c_null_ptr
 
@@ -216,5 +268,37 @@ contains
     call sie_check(sie_precondition_left(m_ctx, c_loc(vector_1), c_loc(vector_2)), &
                    'sie_precondition_left')
   end subroutine lib_sie_ml_fmm_preconditioner_left
+
+  ! vector_y = Z^H vector_x (FP64), the operator of an adjoint solve
+  subroutine lib_sie_ml_fmm_adjoint_tri(vector_x, vector_y)
+    double complex, dimension(:), allocatable, target, intent(in) :: vector_x
+    double complex, dimension(:), allocatable, target, intent(inout) :: vector_y
+    call sie_check(sie_matvec_adjoint(m_ctx, c_loc(vector_x), c_loc(vector_y), 1_c_int), &
+                   'sie_matvec_adjoint')
+  end subroutine lib_sie_ml_fmm_adjoint_tri
+
+  ! dJ/dz of every vertex for J = sum of far-field intensities at the points pts(3, npts),
+  ! at the solution vector_x of the plane wave (k_in, e_in); adjoint solve with FP64 GMRES
+  ! (restart, max_iterations, tolerance)
+  subroutine lib_sie_ml_fmm_grad_z_tri(vector_x, k_in, e_in, pts, restart, max_iterations, tolerance, &
+                                       dJdz, J)
+    double complex, dimension(:), allocatable, target, intent(in) :: vector_x
+    real(c_double), intent(in) :: k_in(3), e_in(3)
+    real(c_double), dimension(:, :), allocatable, target, intent(in) :: pts
+    integer, intent(in) :: restart, max_iterations
+    double precision, intent(in) :: tolerance
+    real(c_double), dimension(:), allocatable, target, intent(inout) :: dJdz
+    double precision, intent(out) :: J
+    type(sie_solver_cfg) :: cfg
+    type(sie_stats) :: st
+    integer(c_int) :: rc
+    call sie_solver_default(cfg)
+    cfg%restart = restart
+    cfg%max_iterations = max_iterations
+    cfg%tolerance = tolerance
+    rc = sie_grad(m_ctx, c_loc(vector_x), k_in, e_in, c_loc(pts), int(size(pts, 2), c_int), cfg, &
+                  c_loc(dJdz), J, st)
+    if (rc /= SIE_ERR_NOCONV) call sie_check(rc, 'sie_grad')
+  end subroutine lib_sie_ml_fmm_grad_z_tri
 
 end module lib_sie_tri_mlfmm_interface
