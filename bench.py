@@ -396,6 +396,8 @@ def main():
     g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local)
     g.setup()
     setup_s = time.perf_counter() - t0
+    # kernel variants picked for this mesh by the library's autotuner (same product)
+    tune_before, tune_after, tune_modes = g.autotune("fp64")
     lib = _lib.load()
     stream = torch.cuda.Stream()
     _lib.check(lib.sie_set_stream(g._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
@@ -552,6 +554,7 @@ def main():
                 "iterations": iters, "matvecs_per_solve": mvs, "converged": bool(conv),
                 "backward_error": be, "max_iterations": args.max_iterations, "setup_s": setup_s,
                 "near_nnz_blocks": g.near_nnz, "matvec_ms": tm["mv_total_ms"],
+                "autotune": {"matvec_ms_before": tune_before, "matvec_ms_after": tune_after, "variants": tune_modes},
                 "matvec_phases_ms": phases, "matvec_phases_note": "phases timed one after another; "
                 "matvec_ms runs the near panels concurrently with the translations",
                 "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],

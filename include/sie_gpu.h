@@ -114,6 +114,14 @@ int sie_matvec(sie_ctx* ctx, const double* x, double* y, int nrhs, int precision
 int sie_matvec_device(sie_ctx* ctx, const double* d_x, double* d_y, int nrhs, int precision,
                       void* stream);
 
+/* Autotuner: times the product of the given precision on this context's mesh with each
+ * kernel variant (near panels, aggregate, SR translation, receive, and where the near
+ * product forks beside the far passes), one knob at a time, and keeps the fastest.  All
+ * variants compute the same product (to the last bits of summation order).  ms[0], ms[1]
+ * (may be NULL): device time of one product before and after; modes[5] (may be NULL): the
+ * chosen near, aggregate, SR, receive and fork variants.  No counterpart in the reference. */
+int sie_autotune(sie_ctx* ctx, int precision, double* ms, int* modes);
+
 /* Operator of the SIE_MIXED solver's inner complex64 products: another context set up on
  * the same mesh with the same tree (e.g. a lower truncation number, a cheaper
  * preconditioner operator); NULL restores ctx itself.  The outer FP64 products, and so the

@@ -76,7 +76,7 @@ EXPORTS = [
     "sie_get_edges", "sie_get_tree", "sie_get_blocks", "sie_get_near_entries", "sie_get_rt",
     "sie_num_directions", "sie_get_timings", "sie_set_stream", "sie_launch_count", "sie_free",
     "sie_farfield_device_noalloc", "sie_solve_direct", "sie_matvec_adjoint", "sie_matvec_adjoint_device",
-    "sie_grad", "sie_set_inner_operator",
+    "sie_grad", "sie_set_inner_operator", "sie_autotune",
 ]
 
 _lib = None
@@ -125,6 +125,7 @@ def load(path=None):
         "sie_solve_direct": (C.c_int, [vp, dp, dp, C.c_int]),
         "sie_matvec_adjoint": (C.c_int, [vp, dp, dp, C.c_int]),
         "sie_set_inner_operator": (C.c_int, [vp, vp]),
+        "sie_autotune": (C.c_int, [vp, C.c_int, dp, ip]),
         "sie_matvec_adjoint_device": (C.c_int, [vp, vp, vp, C.c_int, vp]),
         "sie_grad": (C.c_int, [vp, dp, dp, dp, dp, C.c_int, C.POINTER(SieSolverCfg), dp, dp,
                                C.POINTER(SieStats)]),

@@ -1060,6 +1060,65 @@ int sie_matvec(sie_ctx* c, const double* x, double* y, int nrhs, int precision) 
   return r;
 }
 
+// Minimum over `reps` products (after two warm-up ones) of the device time of one product
+// of the given precision on fixed vectors.
+static int time_product(sie_ctx* c, int precision, int reps, double& ms) {
+  cudaStream_t st = c->stream;
+  ms = 1e300;
+  for (int i = 0; i < reps + 2; i++) {
+    cudaEventRecord(c->ev[8], st);
+    if (precision == SIE_MIXED)
+      SIE_TRY(sie_internal_matvec32(c, c->d_xi32, c->d_yi32, st, false));
+    else
+      SIE_TRY(sie_internal_matvec(c, c->d_xi, c->d_yi, 1, st, false));
+    cudaEventRecord(c->ev[9], st);
+    SIE_CUDA(cudaEventSynchronize(c->ev[9]));
+    float a = 0;
+    cudaEventElapsedTime(&a, c->ev[8], c->ev[9]);
+    if (i >= 2) ms = std::min(ms, (double)a);
+  }
+  return SIE_OK;
+}
+
+int sie_autotune(sie_ctx* c, int precision, double* ms, int* modes) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_autotune: null context");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_autotune: sie_setup not called");
+  if (precision != SIE_FP64 && precision != SIE_MIXED) return fail(SIE_ERR_ARG, "sie_autotune: bad precision");
+  SIE_CUDA(cudaSetDevice(c->device));
+  SIE_TRY(ensure_work(c, 1));
+  if (precision == SIE_MIXED) SIE_TRY(make_f32_tables(c));
+  const size_t n = (size_t)2 * c->M;
+  // fixed finite inputs (the values do not change the work)
+  SIE_CUDA(cudaMemsetAsync(c->d_xi, 0x3f, n * sizeof(zc), c->stream));
+  if (precision == SIE_MIXED) SIE_CUDA(cudaMemsetAsync(c->d_xi32, 0x3f, n * sizeof(cc), c->stream));
+  // coordinate descent over the variant knobs, each at its best value so far
+  int* knob[5] = {&c->near_mode, &c->agg_mode, &c->sr_mode, &c->recv_mode, &c->overlap_near};
+  const int lo[5] = {0, 0, 1, 0, 0}, hi[5] = {1, 1, 5, 1, 2};
+  double best = 0;
+  SIE_TRY(time_product(c, precision, 5, best));
+  if (ms) ms[0] = best;
+  for (int k = 0; k < 5; k++) {
+    if (c->cfg.dense && k > 0) break;  // a dense context has no far passes
+    const int keep = *knob[k];
+    int arg = keep;
+    for (int v = lo[k]; v <= hi[k]; v++) {
+      if (v == keep) continue;
+      *knob[k] = v;
+      double t = 0;
+      SIE_TRY(time_product(c, precision, 5, t));
+      if (t < best) {
+        best = t;
+        arg = v;
+      }
+    }
+    *knob[k] = arg;
+  }
+  if (ms) ms[1] = best;
+  if (modes)
+    for (int k = 0; k < 5; k++) modes[k] = *knob[k];
+  return SIE_OK;
+}
+
 int sie_set_inner_operator(sie_ctx* c, sie_ctx* inner) {
   if (!c) return fail(SIE_ERR_ARG, "sie_set_inner_operator: null context");
   if (inner) {

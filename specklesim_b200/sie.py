@@ -79,6 +79,15 @@ class Sie:
         y = y.T
         return y[:, 0] if x.ndim == 1 else y
 
+    def autotune(self, precision="fp64"):
+        """Pick the fastest kernel variants for this mesh; returns the product's device time
+        before and after [ms] and the chosen variants."""
+        ms = np.zeros(2)
+        modes = np.zeros(5, dtype=np.int32)
+        check(self._lib.sie_autotune(self._h, PRECISIONS[precision], dptr(ms), iptr(modes)))
+        names = ["near", "aggregate", "sr", "receive", "overlap"]
+        return ms[0], ms[1], dict(zip(names, modes.tolist()))
+
     def set_inner_operator(self, other):
         """Inner complex64 products of the mixed solver through `other` (a context on the
         same mesh and tree, e.g. with a lower truncation number); None restores this one."""

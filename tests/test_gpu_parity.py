@@ -377,3 +377,18 @@ def test_direct_dense_solve_matches_oracle(oracle_lib, gpu_lib):
     x1 = g.solve_direct(B[:, 1])
     assert rel(x1, X[:, 1]) < 1e-8
     g.close()
+
+
+def test_autotune_keeps_the_product(gpu_lib):
+    """The autotuner only picks among variants that compute the same product."""
+    from specklesim_b200 import Sie
+    V, T = P.slab(cells=24, length_wl=6.0, seed=3)
+    g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=100).setup()
+    x = P.random_x(g.n, seed=11)
+    y0 = g.matvec(x)
+    before, after, modes = g.autotune("fp64")
+    assert after <= before and 1 <= modes["sr"] <= 5 and 0 <= modes["overlap"] <= 2
+    assert rel(g.matvec(x), y0) < 1e-13
+    g.autotune("mixed")
+    assert rel(g.matvec(x, precision="mixed"), y0) < 2e-4
+    g.close()
