@@ -202,7 +202,8 @@ int sie_get_rt(sie_ctx* ctx, const int* edges, int cnt, double* out);
 int sie_num_directions(const sie_ctx* ctx, int* Q);
 /* Device-side timings of the last sie_setup / sie_matvec phases [ms]:
  * fill, RT+TL, set-up, matvec total, near, aggregate, SS, SR, RR, receive; then
- * out[10] = mean Gram-Schmidt passes per Arnoldi step of the last solve. */
+ * out[10] = mean Gram-Schmidt passes per Arnoldi step of the last solve; out[11] = inner
+ * cycles of the last batched mixed solve replayed from their captured CUDA graph. */
 int sie_get_timings(const sie_ctx* ctx, double* out, int n);
 
 /* Launch all further work of ctx on the caller's CUDA stream (NULL: back to the

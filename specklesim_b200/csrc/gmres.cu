@@ -1621,8 +1621,66 @@ static int inner_batch32(sie_ctx* c, GmB& g, double tol) {
   return SIE_OK;
 }
 
+// The inner cycle of the batch as a CUDA graph: every launch of one cycle (about 17 per
+// inner step) is captured once per solve and replayed for the later outer steps.  Its
+// pointers and scalars are fixed for the solve (input r32, output z32, the basis, the
+// tables).  The first cycle runs uncaptured, so the lazily made buffers of the batched
+// products exist before the capture; a capture that fails falls back to plain launches.
+struct InnerGraph {
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels = 0;
+  bool tried = false;
+  ~InnerGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+static int inner_cycle(sie_ctx* c, GmB& g, double tol, InnerGraph& ig, bool first) {
+  cudaStream_t s = c->stream;
+  if (ig.exec) {
+    SIE_CUDA(cudaGraphLaunch(ig.exec, s));
+    count_launches(ig.kernels);
+    c->tm.graph_replays += 1;
+    return SIE_OK;
+  }
+  const char* ge = getenv("SIE_GRAPH");
+  const bool enabled = !(ge && atoi(ge) == 0);
+  if (first || ig.tried || !enabled) return inner_batch32(c, g, tol);
+  ig.tried = true;
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    const int r = inner_batch32(c, g, tol);
+    const cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (r == SIE_OK && e == cudaSuccess && graph &&
+        cudaGraphInstantiate(&ig.exec, graph, 0) == cudaSuccess) {
+      size_t nn = 0;
+      cudaGraphGetNodes(graph, nullptr, &nn);
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (nn) cudaGraphGetNodes(graph, nodes.data(), &nn);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ig.kernels++;
+      }
+    } else {
+      ig.exec = nullptr;
+    }
+    if (graph) cudaGraphDestroy(graph);
+  }
+  cudaGetLastError();  // a failed capture leaves no sticky error; fall back to launches
+  if (ig.exec) {
+    SIE_CUDA(cudaGraphLaunch(ig.exec, s));
+    count_launches(ig.kernels);
+    c->tm.graph_replays += 1;
+    return SIE_OK;
+  }
+  return inner_batch32(c, g, tol);
+}
+
 int fgmres_mixed_batch(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, int R, const sie_solver_cfg* cfg,
                        sie_stats* stats) {
+  InnerGraph ig;
+  bool first_cycle = true;
+  c->tm.graph_replays = 0;
   cudaStream_t s = c->stream;
   const int mo = cfg->restart, mi = cfg->inner_restart;
   if (R < 1 || R > SIE_BATCH_MAX) return fail(SIE_ERR_ARG, "batched solve: bad batch size");
@@ -1713,7 +1771,8 @@ int fgmres_mixed_batch(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, int R, const 
     }
     for (int j = 0; j < mo; j++) {
       SIE_TRY(to_c64(g.W + (size_t)j * g.ldj, g.r32, vr, s));
-      SIE_TRY(inner_batch32(c, g, cfg->inner_tolerance));
+      SIE_TRY(inner_cycle(c, g, cfg->inner_tolerance, ig, first_cycle));
+      first_cycle = false;
       SIE_TRY(to_c128(g.z32, g.Zb + (size_t)j * g.ldj, vr, s));
       SIE_TRY(sie_internal_matvec_b(c, g.Zb + (size_t)j * g.ldj, g.w64, R, s));
       SIE_TRY(barnoldi<double>(g.W, g.ldj, g.w64, n, R, j, g.pA, g.pB, g.ldp, g.Ho, mo, g.rco, g.rso, g.sto,

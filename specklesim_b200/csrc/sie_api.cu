@@ -15,6 +15,7 @@ namespace sie {
 static thread_local std::string g_err = "";
 static unsigned long long g_launches = 0;
 void count_launch() { __atomic_add_fetch(&g_launches, 1ULL, __ATOMIC_RELAXED); }
+void count_launches(unsigned long long n) { __atomic_add_fetch(&g_launches, n, __ATOMIC_RELAXED); }
 
 void set_error(const std::string& msg) { g_err = msg; }
 int fail(int code, const std::string& msg) {
@@ -1517,11 +1518,11 @@ int sie_get_rt(sie_ctx* c, const int* edges, int cnt, double* out) {
 
 int sie_get_timings(const sie_ctx* c, double* out, int n) {
   if (!c || !out) return fail(SIE_ERR_ARG, "sie_get_timings: null argument");
-  double v[11] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
+  double v[12] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
                   c->tm.mv_near_ms, c->tm.mv_agg_ms, c->tm.mv_ss_ms, c->tm.mv_sr_ms,
                   c->tm.mv_rr_ms, c->tm.mv_recv_ms,
-                  c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0};
-  for (int i = 0; i < n && i < 11; i++) out[i] = v[i];
+                  c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0, c->tm.graph_replays};
+  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
   return SIE_OK;
 }
 

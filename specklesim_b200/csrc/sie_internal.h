@@ -22,6 +22,7 @@ static const double PI = 3.141592653589793238462643383279502884;
 void set_error(const std::string& msg);
 // number of kernels launched by this library since load (for the bench's launch count)
 void count_launch();
+void count_launches(unsigned long long n);  // kernels of a replayed CUDA graph
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
@@ -142,6 +143,7 @@ struct Timings {
   double mv_total_ms = 0, mv_near_ms = 0, mv_agg_ms = 0, mv_ss_ms = 0, mv_sr_ms = 0,
          mv_rr_ms = 0, mv_recv_ms = 0;
   double gm_passes = 0, gm_steps = 0;  // MGS passes and Arnoldi steps of the last solve
+  double graph_replays = 0;            // inner cycles replayed from a CUDA graph, last batched solve
 };
 
 }  // namespace sie

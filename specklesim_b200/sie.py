@@ -231,10 +231,10 @@ class Sie:
         return out
 
     def timings(self):
-        v = np.zeros(11)
-        check(self._lib.sie_get_timings(self._h, dptr(v), 11))
+        v = np.zeros(12)
+        check(self._lib.sie_get_timings(self._h, dptr(v), 12))
         keys = ["fill_ms", "rt_tl_ms", "setup_ms", "mv_total_ms", "mv_near_ms", "mv_agg_ms",
-                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step"]
+                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step", "graph_replays"]
         return dict(zip(keys, v))
 
     def close(self):
