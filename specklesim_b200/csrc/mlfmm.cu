@@ -1480,7 +1480,8 @@ static RecvConst recv_const(const sie_ctx* c) {
 // The translation passes between the leaf aggregate and the receive: SS up the tree, SR on
 // every level, RR down, from the level coefficients C to the leaf D (events 2, 3, 4).
 template <typename T>
-static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev) {
+static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
+                           const std::function<int()>* after_ss = nullptr) {
   const int Q = c->Q;
   const int L0 = c->l_min, L1 = c->l_max;
   const bool k2c = c->mt.k2.im != 0.0;
@@ -1495,6 +1496,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev) {
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[2], st);
+  if (after_ss) SIE_TRY((*after_ss)());
   // down 1
   for (int l = L0; l <= L1; l++) {
     Level& L = c->lv[l];
@@ -1584,8 +1586,9 @@ int far_matvec_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y, cudaStre
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[1], st);
-  if (after_agg) SIE_TRY((*after_agg)());
-  SIE_TRY(far_translate_t<T>(c, st, ev));
+  const bool at_sr = c->overlap_near == 3;  // the hook runs once the SS passes are queued
+  if (after_agg && !at_sr) SIE_TRY((*after_agg)());
+  SIE_TRY(far_translate_t<T>(c, st, ev, at_sr ? after_agg : nullptr));
   // the receive adds into y, which the near product (possibly on another stream) writes
   if (wait_recv) SIE_CUDA(cudaStreamWaitEvent(st, wait_recv, 0));
   // final far summation

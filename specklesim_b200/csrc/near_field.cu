@@ -569,8 +569,8 @@ __global__ void __launch_bounds__(256) k_near_spmv(PanelArgs P, const cx<T>* __r
 // share the panel's columns, so the chunk first gathers x of those columns into shared
 // memory (J, M per column) and then streams the a, b, d rows against it: every lane
 // walks the whole concatenated column range, with no partial warps at box seams.
-template <typename T, bool ACCUM>
-__global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __restrict__ va,
+template <typename T, bool ACCUM, int NW = 8>
+__global__ void __launch_bounds__(32 * NW) k_near_panel(PanelArgs P, const cx<T>* __restrict__ va,
                                                     const cx<T>* __restrict__ vb,
                                                     const cx<T>* __restrict__ vd_,
                                                     const int4* __restrict__ chunks, int M,
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(256) k_near_panel(PanelArgs P, const cx<T>* __
       col0 += c;
     }
     __syncthreads();
-    for (int row = warp; row < cnt; row += 8) {
+    for (int row = warp; row < cnt; row += NW) {
       const long long o = base + (long long)row * nc;
       cx<T> sJ = mk<T>(0, 0), sM = mk<T>(0, 0), tM = mk<T>(0, 0);
 #pragma unroll 4
@@ -820,10 +820,14 @@ int near_prepare_kernels(sie_ctx* c) {
   if (size_t s = near_panel_smem<double>(c)) {
     SIE_CUDA(raise_smem(k_near_panel<double, true>, s));
     SIE_CUDA(raise_smem(k_near_panel<double, false>, s));
+    SIE_CUDA(raise_smem(k_near_panel<double, true, 4>, s));
+    SIE_CUDA(raise_smem(k_near_panel<double, false, 4>, s));
   }
   if (size_t s = near_panel_smem<float>(c)) {
     SIE_CUDA(raise_smem(k_near_panel<float, true>, s));
     SIE_CUDA(raise_smem(k_near_panel<float, false>, s));
+    SIE_CUDA(raise_smem(k_near_panel<float, true, 4>, s));
+    SIE_CUDA(raise_smem(k_near_panel<float, false, 4>, s));
   }
   if (size_t s = near_b_smem<double>(c)) SIE_CUDA(raise_smem(k_near_b<double, NearGroup<double>::RG>, s));
   if (size_t s = near_b_smem<float>(c)) SIE_CUDA(raise_smem(k_near_b<float, NearGroup<float>::RG>, s));
@@ -925,6 +929,16 @@ int near_matvec_t(sie_ctx* c, const cx<T>* va, const cx<T>* vb, const cx<T>* vdd
                   const cx<T>* x, cx<T>* y, int nrhs, bool accum, cudaStream_t st) {
   PanelArgs P = panel_args(c);
   size_t smem = near_panel_smem<T>(c);
+  if (c->near_mode == 2 && smem && c->n_rchunk > 0) {
+    const int4* ch = (const int4*)c->d_rchunk;
+    if (accum) {
+      k_near_panel<T, true, 4><<<c->n_rchunk, 128, smem, st>>>(P, va, vb, vdd, ch, c->M, cfac, x, y, nrhs); sie::count_launch();
+    } else {
+      k_near_panel<T, false, 4><<<c->n_rchunk, 128, smem, st>>>(P, va, vb, vdd, ch, c->M, cfac, x, y, nrhs); sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+    return SIE_OK;
+  }
   if (c->near_mode == 1 && smem && c->n_rchunk > 0) {
     const int4* ch = (const int4*)c->d_rchunk;
     if (accum) {

@@ -444,8 +444,28 @@ static int build_levels(sie_ctx* c) {
         }
       }
       L.ngrp = (int)parents.size();
-      SIE_TRY(upload(&L.grp_sib, gs));
-      SIE_TRY(upload(&L.grp_src, gsrc));
+      // descending work, stable: the SR kernels give each warp one group, and a block
+      // lasts as long as its heaviest warp.  Every box has one group, and a group writes
+      // only its own boxes, so the order changes no result.
+      std::vector<int> cost(L.ngrp), ord(L.ngrp);
+      for (int g = 0; g < L.ngrp; g++) {
+        int ns = 0, cnt = 0;
+        for (int o = 0; o < 8; o++) ns += gs[(size_t)g * 8 + o] >= 0;
+        for (int dc = 0; dc < 216; dc++) cnt += (dc >> 3) != 13 && gsrc[(size_t)g * 216 + dc] >= 0;
+        cost[g] = ns * cnt;
+        ord[g] = g;
+      }
+      std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+      std::vector<int> gs2(gs.size()), gsrc2(gsrc.size());
+      L.grp_cost.resize(L.ngrp);
+      for (int g = 0; g < L.ngrp; g++) {
+        std::copy(gs.begin() + (size_t)ord[g] * 8, gs.begin() + (size_t)ord[g] * 8 + 8, gs2.begin() + (size_t)g * 8);
+        std::copy(gsrc.begin() + (size_t)ord[g] * 216, gsrc.begin() + (size_t)ord[g] * 216 + 216,
+                  gsrc2.begin() + (size_t)g * 216);
+        L.grp_cost[g] = cost[ord[g]];
+      }
+      SIE_TRY(upload(&L.grp_sib, gs2));
+      SIE_TRY(upload(&L.grp_src, gsrc2));
     }
     // children at l+1
     std::vector<int> chp(L.nb + 1, 0), chi, cho;
@@ -684,7 +704,7 @@ int sie_internal_matvec(sie_ctx* c, const zc* xi, zc* yi, int nrhs, cudaStream_t
       };
       if (c->overlap_near == 1) SIE_TRY(fork());
       SIE_TRY(far_matvec64(c, x, y, st, timed ? c->ev : nullptr, c->ev_join,
-                           c->overlap_near == 2 ? &fork : nullptr));
+                           c->overlap_near >= 2 ? &fork : nullptr));
     } else {
       SIE_TRY(near_matvec64(c, x, y, 1, false, st));
       if (timed) cudaEventRecord(c->ev[6], st);
@@ -708,7 +728,7 @@ int sie_internal_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, bool 
     };
     if (c->overlap_near == 1) SIE_TRY(fork());
     SIE_TRY(far_matvec32(c, x, y, st, timed ? c->ev : nullptr, c->ev_join,
-                         c->overlap_near == 2 ? &fork : nullptr));
+                         c->overlap_near >= 2 ? &fork : nullptr));
   } else {
     SIE_TRY(near_matvec32(c, x, y, 1, false, st));
     if (timed) cudaEventRecord(c->ev[6], st);
@@ -735,7 +755,7 @@ static int matvec_b_t(sie_ctx* c, const cx<T>* x, cx<T>* y, int R, cudaStream_t 
         return SIE_OK;
       };
       if (c->overlap_near == 1) SIE_TRY(fork());
-      SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, c->ev_join, c->overlap_near == 2 ? &fork : nullptr));
+      SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, c->ev_join, c->overlap_near >= 2 ? &fork : nullptr));
     } else {
       SIE_TRY(near(c, x + r0 * n, y + r0 * n, nr, st));
       if (!c->cfg.dense) SIE_TRY(far(c, x + r0 * n, y + r0 * n, nr, st, nullptr, nullptr));
@@ -871,9 +891,9 @@ int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris
   if (const char* e = getenv("SIE_SR_MODE")) c->sr_mode = std::max(0, std::min(5, atoi(e)));
   if (const char* e = getenv("SIE_RECV_MODE")) c->recv_mode = std::max(0, std::min(1, atoi(e)));
   if (const char* e = getenv("SIE_AGG_MODE")) c->agg_mode = std::max(0, std::min(1, atoi(e)));
-  if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(1, atoi(e)));
+  if (const char* e = getenv("SIE_NEAR_MODE")) c->near_mode = std::max(0, std::min(2, atoi(e)));
   if (const char* e = getenv("SIE_ARNOLDI_MODE")) c->arnoldi_mode = std::max(0, std::min(2, atoi(e)));
-  if (const char* e = getenv("SIE_OVERLAP")) c->overlap_near = std::max(0, std::min(2, atoi(e)));
+  if (const char* e = getenv("SIE_OVERLAP")) c->overlap_near = std::max(0, std::min(3, atoi(e)));
   *out = c;
   return SIE_OK;
 }
@@ -1094,7 +1114,7 @@ int sie_autotune(sie_ctx* c, int precision, double* ms, int* modes) {
   if (precision == SIE_MIXED) SIE_CUDA(cudaMemsetAsync(c->d_xi32, 0x3f, n * sizeof(cc), c->stream));
   // coordinate descent over the variant knobs, each at its best value so far
   int* knob[5] = {&c->near_mode, &c->agg_mode, &c->sr_mode, &c->recv_mode, &c->overlap_near};
-  const int lo[5] = {0, 0, 1, 0, 0}, hi[5] = {1, 1, 5, 1, 2};
+  const int lo[5] = {0, 0, 1, 0, 0}, hi[5] = {2, 1, 5, 1, 3};
   double best = 0;
   SIE_TRY(time_product(c, precision, 5, best));
   if (ms) ms[0] = best;

@@ -128,6 +128,9 @@ struct Level {
   int ngrp = 0;
   int* grp_sib = nullptr;     // ngrp x 8 box indices (-1: absent)
   int* grp_src = nullptr;     // ngrp x 27 x 8 candidate source box indices (-1: absent)
+  // present siblings x present sources outside the parent, per group; the groups are
+  // stored in descending order of it, so that the warps of one block get equal work
+  std::vector<int> grp_cost;
   // complex64 copies for the FP32 matvec (made on first use)
   cc* tl32 = nullptr;
   cc* ph_up32 = nullptr;
@@ -159,7 +162,8 @@ struct sie_ctx {
   // the near-field product runs on stream2 next to the far-field passes
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // near product on stream2: 0 no (sequential), 1 forked at the start of the product,
-  // 2 forked once the leaf aggregate is queued, beside the translations only
+  // 2 forked once the leaf aggregate is queued, beside the translations only, 3 forked
+  // once the SS passes are queued, beside the SR and RR passes
   int overlap_near = 2;
 
   // mesh (reference order)
@@ -206,7 +210,8 @@ struct sie_ctx {
   int* d_rchunk = nullptr;        // receive chunks: (box, first edge, count, 0) per chunk
   int n_rchunk = 0;
   int ncols_max = 0;              // widest near panel (columns)
-  // near product: 0 one warp per row; 1 chunks of rows with the panel's x in shared memory
+  // near product: 0 one warp per row; 1 chunks of rows with the panel's x in shared memory;
+  // 2 the same with 4-warp blocks, of which one fits on an SM beside two SR blocks
   int near_mode = 1;
   // near values: ICTF / PMCHWT store (a, b, d), c = cfac * b
   zc* d_na = nullptr;

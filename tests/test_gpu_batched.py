@@ -120,7 +120,7 @@ def test_batched_overlap_gives_the_same_product(gpu_lib, monkeypatch):
     from specklesim_b200 import Sie
     V, T = P.slab(cells=24, length_wl=6.0, seed=3)
     out = []
-    for ov in ("0", "1", "2"):
+    for ov in ("0", "1", "2", "3"):
         monkeypatch.setenv("SIE_OVERLAP", ov)
         g = Sie(V, T, P.WL, P.EPS_METAL, tree_s_opt=100).setup()
         X = _columns(g.n, 6, 400)
