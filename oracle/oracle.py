@@ -73,6 +73,7 @@ def lib():
             "orc_field": (None, [vp, dp, dp, C.c_int, dp, dp]),
             "orc_hankel2": (None, [C.c_double, C.c_double, C.c_int, dp]),
             "orc_gauss_legendre": (None, [C.c_int, dp, dp]),
+            "orc_lagrange_interp": (None, [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]),
             "orc_hanninen": (None, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp]),
             "orc_fn": (None, [vp, C.c_int, C.c_int, dp]),
         }
@@ -243,6 +244,20 @@ def gauss_legendre(n):
     x, w = np.zeros(n), np.zeros(n)
     lib().orc_gauss_legendre(int(n), _d(x), _d(w))
     return x, w
+
+
+def lagrange_interp(p, k_from, k_to, fa, fb):
+    """Local Lagrange interpolation of one (theta, phi) far-field pattern pair from the
+    K = k_from sampling to K = k_to (Lagrange_Interpolation_New, lib_sie_mlfmm.f90:268-390;
+    stencil of 2p x 2p points, p = 3 in the reference).  fa, fb: 2 k_from^2 + 2 complex
+    values in the sampling order of `Oracle.sampling`, the last two being the +z and -z
+    poles, which hold the Cartesian x and y components.  Returns (ga, gb)."""
+    qf, qt = 2 * k_from * k_from + 2, 2 * k_to * k_to + 2
+    a = np.ascontiguousarray(np.asarray(fa, dtype=np.complex128).reshape(qf)).view(np.float64)
+    b = np.ascontiguousarray(np.asarray(fb, dtype=np.complex128).reshape(qf)).view(np.float64)
+    ga, gb = np.zeros(2 * qt), np.zeros(2 * qt)
+    lib().orc_lagrange_interp(int(p), int(k_from), int(k_to), _d(a), _d(b), _d(ga), _d(gb))
+    return ga.view(np.complex128), gb.view(np.complex128)
 
 
 # ---------------------------------------------------------------------------

@@ -9,7 +9,9 @@
 // reference (its SIE fixtures are missing), so those are pinned by the reference's
 // own probes restated here (K2q/K3q/K4q vs 12-point quadrature), by the dense vs
 // MLFMM cross-check and by physics (reciprocity, Mie).  The special functions and
-// GMRES are pinned against the reference's known-answer tests (tests/golden).
+// GMRES are pinned against the reference's known-answer tests (tests/golden).  The
+// k-space Lagrange interpolation (level-dependent K, dormant at the reference's
+// defaults) is pinned only by its mathematics: parity unpinned.
 //
 // Reference files (paths inside the SpeckleSim project):
 //   src/lib_sie_tri_calculation_mod.f90   near-field blocks, RHS, far field
@@ -885,6 +887,123 @@ static void make_sampling(Fmm& F) {
   F.trf[Ns] = F.trf[Ns + 1] = 0.0;
 }
 
+// Level-dependent K: local Lagrange interpolation of one far-field pattern from the
+// K_m sampling to the K_n sampling (Lagrange_Interpolation_New, lib_sie_mlfmm.f90:268-390),
+// for one (theta, phi) component pair: Fa, Fb hold Q_m = 2 K_m^2 + 2 values in the
+// sampling order of make_sampling, the last two being the +z and -z poles, where the
+// pair holds the Cartesian (x, y) components (the reference's transfer vectors there).
+// The translation passes call it on the child grid before the SS phase shift
+// (lib_sie_tri_mlfmm_interface.f90:490-507) and, with K_n < K_m, after the RR phase
+// shift on the parent grid (:622-640).  The arithmetic keeps the reference's order and
+// types where they decide a stencil or a branch: the stencil base is computed in binary32
+// ((it-1.0)/K_n*K_m with a default-real literal), and the extended phi grid is
+// -2 pi + dphi (k-1), compared against 0 and 2 pi as computed.
+//
+// Extended grid (theta_phi_extended :573-610, Sorting_theta_phi_LenReduced_Arr_New
+// :414-493): rows are theta nodes u = -p .. K_m + p + 1 (u = 0 the -z pole at theta =
+// pi, u = K_m + 1 the +z pole at theta = 0), columns phi nodes -p .. 2 K_m + p.  The pole
+// rows are the Cartesian pole values projected on theta-hat / phi-hat of the column's
+// phi; rows past a pole are the reflection through it at phi + pi with both components
+// negated; columns past 0 or 2 pi wrap.  Weights (Lagrange_Interpolation_Weights
+// :392-412): the 2p-point Lagrange basis over the extended nodes around the target.
+static void lagrange_interp(int p, int Km, int Kn, const cd* Fa, const cd* Fb, cd* Ga, cd* Gb) {
+  std::vector<double> xm, wm, xn, wn;
+  gauss_legendre(Km, xm, wm);
+  gauss_legendre(Kn, xn, wn);
+  // theta_phi_extended: a_theta from 2 pi down to -pi, a_phi from -2 pi up to 4 pi
+  const int mph = 3 * (2 * Km);
+  const double dphi = 6 * PI / mph;
+  std::vector<double> at(3 * Km + 2), ap(mph);
+  for (int j = 1; j <= Km; j++) {
+    at[j - 1] = 2 * PI - std::acos(xm[Km - j]);
+    at[j + Km] = std::acos(xm[j - 1]);
+    at[2 * Km + 1 + j] = -std::acos(xm[Km - j]);
+  }
+  at[Km] = PI;
+  at[2 * Km + 1] = 0.0;
+  for (int k = 0; k < mph; k++) ap[k] = -2 * PI + dphi * k;
+  // ff_out for the two channels (0: theta component, 1: phi component)
+  const int nth = Km + 2 * p + 2, nph = 2 * Km + 2 * p + 1, KnL = 2 * Km;
+  std::vector<cd> ff((size_t)2 * nth * nph, cd(0.0, 0.0));
+  auto F = [&](int ch, int r, int c) -> cd& { return ff[((size_t)ch * nth + r) * nph + c]; };
+  const int Nsm = 2 * Km * Km;
+  const cd fx0 = Fa[Nsm], fy0 = Fb[Nsm], fxpi = Fa[Nsm + 1], fypi = Fb[Nsm + 1];
+  for (int c = 0; c < nph; c++) {
+    const double ph = ap[c + KnL - p];
+    const double ct = std::cos(ph), st = std::sin(ph);
+    F(0, p, c) = -(ct * fxpi + st * fypi);      // theta = pi
+    F(0, Km + p + 1, c) = ct * fx0 + st * fy0;  // theta = 0
+    F(1, p, c) = -st * fxpi + ct * fypi;
+    F(1, Km + p + 1, c) = -st * fx0 + ct * fy0;
+  }
+  for (int i = 0; i < Km; i++)
+    for (int j = 0; j < 2 * Km; j++) {
+      F(0, p + 1 + i, p + j) = Fa[(size_t)i * 2 * Km + j];
+      F(1, p + 1 + i, p + j) = Fb[(size_t)i * 2 * Km + j];
+    }
+  for (int r = 0; r < nth; r++) {
+    const double xt = at[r + 1 - p + Km];
+    for (int c = 0; c < nph; c++) {
+      const double xp = ap[c - p + KnL];
+      int rs = -1, cs = -1;
+      if (xt < 0.0) {
+        rs = 2 * Km + 2 * p + 2 - r;
+        if (xp < PI && xp >= 0.0) cs = c + Km;
+        else if (xp < 2 * PI && xp >= PI) cs = c - Km;
+      } else if (xt >= PI) {
+        rs = 2 * p - r;
+        if (xp < PI && xp >= 0.0) cs = c + Km;
+        else if (xp < 2 * PI && xp >= PI) cs = c - Km;
+      }
+      if (cs >= 0)
+        for (int ch = 0; ch < 2; ch++) F(ch, r, c) = -F(ch, rs, cs);
+    }
+  }
+  for (int r = 0; r < nth; r++)
+    for (int c = 0; c < nph; c++) {
+      const double xp = ap[c - p + KnL];
+      if (xp >= 2 * PI)
+        for (int ch = 0; ch < 2; ch++) F(ch, r, c) = F(ch, r, c - KnL);
+      else if (xp < 0)
+        for (int ch = 0; ch < 2; ch++) F(ch, r, c) = F(ch, r, c + KnL);
+    }
+  // Lagrange_Interpolation_Weights: nodes ext[K_arr + t - p .. K_arr + t + p - 1]
+  auto weights = [p](double x, int t, int karr, const std::vector<double>& ext, std::vector<double>& wk) {
+    const double* xx = ext.data() + karr + t - p;
+    for (int j = 0; j < 2 * p; j++) {
+      wk[j] = 1.0;
+      for (int m = 0; m < 2 * p; m++)
+        if (m != j) wk[j] = (x - xx[m]) / (xx[j] - xx[m]) * wk[j];
+    }
+  };
+  std::vector<double> wt(2 * p), wp(2 * p);
+  for (int it = 1; it <= Kn; it++) {
+    const double theta = std::acos(xn[it - 1]);
+    const int t = (int)std::floor(((float)it - 1.0f) / (float)Kn * (float)Km) + 1;
+    weights(theta, t, Km, at, wt);
+    for (int jp = 1; jp <= 2 * Kn; jp++) {
+      const double phi = (double)((jp - 1) * 2) * PI / (2 * Kn);
+      const int s = (int)std::floor(((float)jp - 1.0f) / (float)Kn * (float)Km) + 1;
+      weights(phi, s, 2 * Km, ap, wp);
+      cd ga(0.0, 0.0), gb(0.0, 0.0);
+      for (int i = 0; i < 2 * p; i++)
+        for (int j = 0; j < 2 * p; j++) {
+          const double w = wp[j] * wt[i];
+          ga += w * F(0, t + i, s + j);
+          gb += w * F(1, t + i, s + j);
+        }
+      const size_t o = (size_t)(it - 1) * 2 * Kn + (jp - 1);
+      Ga[o] = ga;
+      Gb[o] = gb;
+    }
+  }
+  const int Nsn = 2 * Kn * Kn;
+  for (int k = 0; k < 2; k++) {
+    Ga[Nsn + k] = Fa[Nsm + k];
+    Gb[Nsn + k] = Fb[Nsm + k];
+  }
+}
+
 // PreCalculate_RT + RT_function_SCSArr_New, lib_sie_tri_mlfmm.f90:503-583
 static void make_rt(const Mesh& ms, const Material& mt, const Rule& R, const Tree& T, Fmm& F) {
   int M = (int)ms.edge_mid.size(), Q = F.Q;
@@ -1475,6 +1594,12 @@ void orc_hankel2(double zr, double zi, int n, double* out) {
   std::vector<cd> h;
   hankel2(cd(zr, zi), n, h);
   for (int i = 0; i < n; i++) { out[2 * i] = h[i].real(); out[2 * i + 1] = h[i].imag(); }
+}
+
+// Lagrange interpolation of one (theta, phi) pattern pair between samplings (complex
+// values interleaved re, im; 2 K^2 + 2 each)
+void orc_lagrange_interp(int p, int Km, int Kn, const double* Fa, const double* Fb, double* Ga, double* Gb) {
+  lagrange_interp(p, Km, Kn, (const cd*)Fa, (const cd*)Fb, (cd*)Ga, (cd*)Gb);
 }
 
 void orc_gauss_legendre(int n, double* x, double* w) {
