@@ -63,6 +63,8 @@ def lib():
             "orc_i4": (C.c_int, [vp, C.c_longlong, C.c_int, lp]),
             "orc_neighbours": (C.c_int, [C.c_longlong, C.c_int, lp]),
             "orc_setup_fmm": (C.c_longlong, [vp]),
+            "orc_set_level_k": (None, [vp, ip, C.c_int]),
+            "orc_level_Q": (C.c_int, [vp, C.c_int]),
             "orc_near_csr": (None, [vp, ip, ip, dp]),
             "orc_Q": (C.c_int, [vp]),
             "orc_sampling": (None, [vp, dp, dp, dp, dp]),
@@ -171,8 +173,21 @@ class Oracle:
         k = lib().orc_i4(self.h, int(n), int(level), _l(out))
         return out[:k]
 
+    def set_level_truncation(self, k_by_level):
+        """Truncation number per tree level ({level: K}; levels left out keep the
+        context's K), the reference's truncation_number(l)%n.  Call before setup_fmm.
+        A level whose K differs from its parent's takes the interpolation branches of SS
+        and RR (lib_sie_tri_mlfmm_interface.f90:486-507, :622-640)."""
+        n = max(k_by_level) + 1
+        arr = np.zeros(n, np.int32)
+        for l, k in k_by_level.items():
+            arr[l] = int(k)
+        lib().orc_set_level_k(self.h, _i(arr), n)
+
     def setup_fmm(self):
         self.nnz = lib().orc_setup_fmm(self.h)
+        if self.nnz < 0:
+            raise ValueError("truncation numbers must not grow from a level to its children")
         self.Q = lib().orc_Q(self.h)
         return self.nnz
 
@@ -195,7 +210,7 @@ class Oracle:
         return out
 
     def tl(self, level):
-        out = np.zeros((343, 2, self.Q), np.complex128)
+        out = np.zeros((343, 2, lib().orc_level_Q(self.h, int(level))), np.complex128)
         lib().orc_tl(self.h, int(level), _d(out.view(np.float64)))
         return out
 

@@ -158,6 +158,10 @@ struct Params {
   int K;
   int normal_conv;  // calc_p(7): 1 or 2
   int fix_itbn;
+  // truncation_number(l)%n per level (index = level; 0 or absent: K).  The reference
+  // fills it with K on every level (Truncation_number_calculation,
+  // lib_sie_mlfmm.f90:694-699); other values take its interpolation branches.
+  std::vector<int> level_K;
 };
 
 struct Material {
@@ -845,10 +849,18 @@ static void hankel2(cd z, int nmax, std::vector<cd>& h) {
 // ---------------------------------------------------------------------------
 // MLFMM state.
 
-struct Fmm {
-  int K, Q;
+// k-space sampling of one truncation number
+struct Samp {
+  int K = 0, Q = 0;
   std::vector<V3> khat, tth, tph;
   std::vector<double> trf;
+};
+
+struct Fmm {
+  int K, Q;  // the leaf level's sampling (RT, aggregate, receive)
+  std::vector<V3> khat, tth, tph;
+  std::vector<double> trf;
+  std::vector<Samp> sl;  // sampling per level (index = level)
   // RT per edge: [e][med][comp][q], comp 0 = theta (a_nm), 1 = phi (b_nm)
   std::vector<cd> rt;
   // TL per level: [lvl][343][med][q]
@@ -860,8 +872,9 @@ struct Fmm {
 };
 
 // Khat_and_TRF_ExtendedK, lib_sie_mlfmm.f90:190-240
-static void make_sampling(Fmm& F) {
-  int K = F.K, Ns = 2 * K * K;
+static void make_samp(int K, Samp& F) {
+  F.K = K;
+  int Ns = 2 * K * K;
   F.Q = Ns + 2;
   std::vector<double> xx, ww;
   gauss_legendre(K, xx, ww);
@@ -885,6 +898,20 @@ static void make_sampling(Fmm& F) {
   F.tth[Ns] = F.tth[Ns + 1] = v3(1, 0, 0);
   F.tph[Ns] = F.tph[Ns + 1] = v3(0, 1, 0);
   F.trf[Ns] = F.trf[Ns + 1] = 0.0;
+}
+
+// Samplings of every level; the leaf level's is also F's own (RT and the leaf passes).
+static void make_sampling(Fmm& F, const std::vector<int>& Kl) {
+  F.sl.assign(Kl.size(), Samp());
+  for (size_t l = 0; l < Kl.size(); l++)
+    if (Kl[l] > 0) make_samp(Kl[l], F.sl[l]);
+  const Samp& S = F.sl.back();
+  F.K = S.K;
+  F.Q = S.Q;
+  F.khat = S.khat;
+  F.tth = S.tth;
+  F.tph = S.tph;
+  F.trf = S.trf;
 }
 
 // Level-dependent K: local Lagrange interpolation of one far-field pattern from the
@@ -1038,11 +1065,12 @@ static void make_rt(const Mesh& ms, const Material& mt, const Rule& R, const Tre
 // precalculation_LT3_TL + PreCalc_transfer_function + TL_km_ml_fmm,
 // lib_sie_mlfmm.f90:27-188
 static void make_tl(const Material& mt, const Tree& T, Fmm& F) {
-  int Q = F.Q, K = F.K;
   F.tl.assign(T.l_max + 1, {});
   F.tl_xmin.assign(T.l_max + 1, 0.0);
   F.tl_dx.assign(T.l_max + 1, 0.0);
   for (int l = T.l_min; l <= T.l_max; l++) {
+    const Samp& S = F.sl[l];
+    const int Q = S.Q, K = S.K;
     double dc = std::ldexp(1.0, -l) * T.D;
     double xmn = -3 * dc, xmx = -xmn;
     double dx = (xmx - xmn) / 6;
@@ -1064,7 +1092,7 @@ static void make_tl(const Material& mt, const Tree& T, Fmm& F) {
         if (med == 1 && only_k1) continue;
         hankel2(kd[med] * rl, K, h);
         for (int q = 0; q < Q; q++) {
-          double x = dot(rh, F.khat[q]);
+          double x = dot(rh, S.khat[q]);
           P[0] = 1.0;
           if (K > 1) P[1] = x;
           for (int n = 1; n + 1 < K; n++) P[n + 1] = ((2 * n + 1) * x * P[n] - n * P[n - 1]) / (n + 1);
@@ -1156,12 +1184,21 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
   const Material& mt = C.mt;
   int M = (int)C.ms.edge_mid.size(), Q = F.Q;
   int L0 = T.l_min, L1 = T.l_max;
-  // coefficient storage per level: [box][8][Q]; item order a1 a2 a3 a4 b1 b2 b3 b4
+  // coefficient storage per level: [box][8][Q_l]; item order a1 a2 a3 a4 b1 b2 b3 b4
+  // (theta items 0..3 and their phi items 4..7)
   std::vector<std::vector<cd>> Cc(L1 + 1), Dd(L1 + 1);
   for (int l = L0; l <= L1; l++) {
-    Cc[l].assign(T.boxes[l].size() * 8 * Q, 0.0);
-    Dd[l].assign(T.boxes[l].size() * 8 * Q, 0.0);
+    Cc[l].assign(T.boxes[l].size() * 8 * F.sl[l].Q, 0.0);
+    Dd[l].assign(T.boxes[l].size() * 8 * F.sl[l].Q, 0.0);
   }
+  // the 8 items of one box from the K_from sampling to K_to (Lagrange_Interpolation_New
+  // on the (a_nm, b_nm) pair of each item, lib_sie_mlfmm.f90:268-390, p = 3)
+  auto interp8 = [](int Kf, int Kt, const cd* in, cd* out) {
+    const int qf = 2 * Kf * Kf + 2, qt = 2 * Kt * Kt + 2;
+    for (int i = 0; i < 4; i++)
+      lagrange_interp(3, Kf, Kt, in + (size_t)i * qf, in + (size_t)(i + 4) * qf, out + (size_t)i * qt,
+                      out + (size_t)(i + 4) * qt);
+  };
   auto bidx = [&](int l, uint64_t n) -> long {
     auto& v = T.boxes[l];
     auto it = std::lower_bound(v.begin(), v.end(), n);
@@ -1192,21 +1229,30 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
     }
   }
   cd kk[2] = {mt.k1, mt.k2};
-  // upward pass step 2: translation_SS (:466-528)
+  // upward pass step 2: translation_SS (:466-528); a child level with a lower
+  // truncation number is interpolated to the parent's sampling first (:486-507)
   for (int l = L1 - 1; l >= L0; l--) {
     auto& lv = T.boxes[l];
+    const Samp& S = F.sl[l];
+    const int Q = S.Q, Kc = F.sl[l + 1].K, Qc = F.sl[l + 1].Q;
+    const bool up = S.K > Kc;
 #pragma omp parallel for schedule(dynamic)
     for (long bi = 0; bi < (long)lv.size(); bi++) {
       V3 xp = box_centre(T, lv[bi], l);
       cd* Cp = &Cc[l][(size_t)bi * 8 * Q];
+      std::vector<cd> tmpc(up ? (size_t)8 * Q : 0);
       for (uint64_t c = 0; c < 8; c++) {
         uint64_t ch = (lv[bi] << 3) | c;
         long ci = bidx(l + 1, ch);
         if (ci < 0) continue;
         V3 r = box_centre(T, ch, l + 1) - xp;
-        const cd* Cch = &Cc[l + 1][(size_t)ci * 8 * Q];
+        const cd* Cch = &Cc[l + 1][(size_t)ci * 8 * Qc];
+        if (up) {
+          interp8(Kc, S.K, Cch, tmpc.data());
+          Cch = tmpc.data();
+        }
         for (int q = 0; q < Q; q++) {
-          double tmp = dot(F.khat[q], r);
+          double tmp = dot(S.khat[q], r);
           cd tk[2] = {std::exp(IM * mt.k1 * tmp), std::exp(IM * mt.k2 * tmp)};
           for (int j = 0; j < 2; j++) {
             Cp[(0 + j) * Q + q] += Cch[(0 + j) * Q + q] * tk[j];
@@ -1222,6 +1268,8 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
   // downward pass step 1: translation_SR over I4 (:547-586)
   for (int l = L0; l <= L1; l++) {
     auto& lv = T.boxes[l];
+    const int Q = F.sl[l].Q;
+    const std::vector<double>& trf = F.sl[l].trf;
 #pragma omp parallel for schedule(dynamic)
     for (long bi = 0; bi < (long)lv.size(); bi++) {
       V3 xa = box_centre(T, lv[bi], l);
@@ -1236,7 +1284,7 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
         const cd* Cs = &Cc[l][(size_t)si * 8 * Q];
         for (int j = 0; j < 2; j++)
           for (int q = 0; q < Q; q++) {
-            cd t = F.trf[q] * tl[j * Q + q];
+            cd t = trf[q] * tl[j * Q + q];
             Db[(0 + j) * Q + q] += Cs[(0 + j) * Q + q] * t;
             Db[(4 + j) * Q + q] += Cs[(4 + j) * Q + q] * t;
             Db[(2 + j) * Q + q] += Cs[(2 + j) * Q + q] * t;
@@ -1245,9 +1293,37 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
       }
     }
   }
-  // downward pass step 2: translation_RR (:600-655)
+  // downward pass step 2: translation_RR (:600-655).  For a child level with a lower
+  // truncation number, the shift runs on the parent's sampling (:622-636) and the
+  // result goes to the child's sampling by anterpolation, the transpose of the SS
+  // interpolation, where the reference calls the interpolation itself (:638-640).
+  // D carries the TRF weights of its own level (SR above), so the parent's far sum
+  // sum_q w_q R^(p)(q) D^(p)(q), with R^(p) = I R^(c) (the receiving pattern
+  // interpolated), equals sum_q' R^(c)(q') [I^T (w D^(p))](q'), the child's sum.
+  // Interpolating the weighted D instead is not accurate: D = C TL has the bandwidth of
+  // C plus K, more than the child's sampling resolves.
   for (int l = L0 + 1; l <= L1; l++) {
     auto& lv = T.boxes[l];
+    const Samp& S = F.sl[l];
+    const Samp& Sp = F.sl[l - 1];
+    const int Q = S.Q, Qp = Sp.Q;
+    const bool down = S.K < Sp.K;
+    // interpolation matrix child -> parent, [2 Qp][2 Qc] (a then b values), by columns
+    std::vector<double> Im;
+    if (down) {
+      Im.assign((size_t)4 * Qp * Q, 0.0);
+      std::vector<cd> ea(Q), eb(Q), ga(Qp), gb(Qp);
+      for (int j = 0; j < 2 * Q; j++) {
+        std::fill(ea.begin(), ea.end(), cd(0.0, 0.0));
+        std::fill(eb.begin(), eb.end(), cd(0.0, 0.0));
+        (j < Q ? ea[j] : eb[j - Q]) = 1.0;
+        lagrange_interp(3, S.K, Sp.K, ea.data(), eb.data(), ga.data(), gb.data());
+        for (int i = 0; i < Qp; i++) {
+          Im[(size_t)i * 2 * Q + j] = ga[i].real();
+          Im[(size_t)(i + Qp) * 2 * Q + j] = gb[i].real();
+        }
+      }
+    }
 #pragma omp parallel for schedule(dynamic)
     for (long bi = 0; bi < (long)lv.size(); bi++) {
       uint64_t par = lv[bi] >> 3;
@@ -1255,9 +1331,31 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
       if (pi < 0) continue;
       V3 r = box_centre(T, lv[bi], l) - box_centre(T, par, l - 1);
       cd* Db = &Dd[l][(size_t)bi * 8 * Q];
-      const cd* Dp = &Dd[l - 1][(size_t)pi * 8 * Q];
+      const cd* Dp = &Dd[l - 1][(size_t)pi * 8 * Qp];
+      if (down) {
+        std::vector<cd> sh((size_t)8 * Qp), it((size_t)8 * Q);
+        for (int q = 0; q < Qp; q++) {
+          double tmp = dot(Sp.khat[q], r);
+          cd tk[2] = {std::exp(-IM * mt.k1 * tmp), std::exp(-IM * mt.k2 * tmp)};
+          for (int j = 0; j < 2; j++)
+            for (int o = 0; o < 8; o += 2) sh[(size_t)(o + j) * Qp + q] = Dp[(size_t)(o + j) * Qp + q] * tk[j];
+        }
+        // I^T on each (a, b) item pair
+        for (int p = 0; p < 4; p++) {
+          const cd* pa = &sh[(size_t)p * Qp];
+          const cd* pb = &sh[(size_t)(p + 4) * Qp];
+          for (int j = 0; j < 2 * Q; j++) {
+            cd acc(0.0, 0.0);
+            for (int i = 0; i < Qp; i++)
+              acc += Im[(size_t)i * 2 * Q + j] * pa[i] + Im[(size_t)(i + Qp) * 2 * Q + j] * pb[i];
+            it[(size_t)(j < Q ? p : p + 4) * Q + (j < Q ? j : j - Q)] = acc;
+          }
+        }
+        for (size_t i = 0; i < it.size(); i++) Db[i] += it[i];
+        continue;
+      }
       for (int q = 0; q < Q; q++) {
-        double tmp = dot(F.khat[q], r);
+        double tmp = dot(S.khat[q], r);
         cd tk[2] = {std::exp(-IM * mt.k1 * tmp), std::exp(-IM * mt.k2 * tmp)};
         for (int j = 0; j < 2; j++) {
           Db[(0 + j) * Q + q] += Dp[(0 + j) * Q + q] * tk[j];
@@ -1272,6 +1370,12 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
   cd eps_d[2] = {mt.eps1 * IM * mt.omega, mt.eps2 * IM * mt.omega};
   cd my_d[2] = {mt.my1 * IM * mt.omega, mt.my2 * IM * mt.omega};
   cd kd[2] = {mt.k1 * IM, mt.k2 * IM};
+  // The receive rotates the pattern, f_rk = (-f_phi, f_theta) = khat x f.  At the -z
+  // pole the stored components are Cartesian (theta-hat = x, phi-hat = y), for which
+  // khat x f is (f_y, -f_x).  With one K on every level, D is exactly zero there (TRF is
+  // 0 at the poles) and the reference's formula is kept; anterpolated D is not zero.
+  bool level_k = false;
+  for (int l = L0; l < L1; l++) level_k |= F.sl[l].K != F.sl[L1].K;
 #pragma omp parallel for schedule(dynamic, 16)
   for (int j = 0; j < M; j++) {
     long bi = bidx(L1, T.leaf[j]);
@@ -1284,6 +1388,10 @@ static void matvec(const Ctx& C, const cd* x, cd* y, int faithful_lookup) {
       cd kh = 0.0, le = 0.0, ke = 0.0, lh = 0.0;
       for (int q = 0; q < Q; q++) {
         cd rka = -fb[q], rkb = fa[q];
+        if (level_k && q == Q - 1) {
+          rka = fb[q];
+          rkb = -fa[q];
+        }
         le += fa[q] * D[(0 + i) * Q + q] * my_d[i] + fb[q] * D[(4 + i) * Q + q] * my_d[i];
         ke += -rka * D[(0 + i) * Q + q] * kd[i] - rkb * D[(4 + i) * Q + q] * kd[i];
         lh += fa[q] * D[(2 + i) * Q + q] * eps_d[i] + fb[q] * D[(6 + i) * Q + q] * eps_d[i];
@@ -1530,11 +1638,24 @@ int orc_neighbours(long long n, int l, long long* out) {
 }
 
 // near CSR + RT + TL; returns nnz
+// Truncation number per level (index = level, 0 = the context's K), before setup_fmm.
+void orc_set_level_k(void* h, const int* K, int n) {
+  Ctx* C = (Ctx*)h;
+  C->P.level_K.assign(K, K + n);
+}
+
+// Returns the near-field block count, or -1 if the per-level truncation numbers grow
+// toward the leaf (the reference's SS interpolates only up to a larger K, and its RR
+// only down to a smaller one).
 long long orc_setup_fmm(void* h) {
   Ctx* C = (Ctx*)h;
   if (!C->have_tree) build_tree(C->ms, C->P.s_opt, C->T), C->have_tree = true;
-  C->F.K = C->P.K;
-  make_sampling(C->F);
+  std::vector<int> Kl(C->T.l_max + 1, 0);
+  for (int l = C->T.l_min; l <= C->T.l_max; l++)
+    Kl[l] = (l < (int)C->P.level_K.size() && C->P.level_K[l] > 0) ? C->P.level_K[l] : C->P.K;
+  for (int l = C->T.l_min; l < C->T.l_max; l++)
+    if (Kl[l] < Kl[l + 1]) return -1;
+  make_sampling(C->F, Kl);
   make_rt(C->ms, C->mt, C->R, C->T, C->F);
   make_tl(C->mt, C->T, C->F);
   make_near(*C);
@@ -1554,6 +1675,8 @@ void orc_near_csr(void* h, int* ia, int* ja, double* abcd) {
 }
 
 int orc_Q(void* h) { return ((Ctx*)h)->F.Q; }
+
+int orc_level_Q(void* h, int l) { return ((Ctx*)h)->F.sl[l].Q; }
 
 // sampling: khat[3Q], theta[3Q], phi[3Q], trf[Q]
 void orc_sampling(void* h, double* kh, double* th, double* ph, double* trf) {

@@ -5,7 +5,11 @@ The reference has no test of this routine and cannot be run here, so these check
 restatement by its mathematics: it reproduces samples when both samplings are the same,
 it is linear, and it reconstructs band-limited far-field patterns, including the constant
 Cartesian field, which is the case where the rows reflected through the poles carry the
-result (a reflection with the wrong sign or phi shift would give O(1) errors there)."""
+result (a reflection with the wrong sign or phi shift would give O(1) errors there).
+
+The second half checks the whole product with a truncation number per level against the
+product with K = 19 on every level: interpolation up in SS, anterpolation (the transpose)
+down in RR, and the khat x f rotation at the -z pole in the receive."""
 import numpy as np
 import pytest
 
@@ -94,3 +98,60 @@ def test_rows_next_to_the_poles(oracle_lib):
     rows = np.r_[0:2 * kn, (kn - 1) * 2 * kn:kn * 2 * kn]
     assert np.abs(ea[rows]).max() > 0.5
     assert max(np.abs(ga[rows] - ea[rows]).max(), np.abs(gb[rows] - eb[rows]).max()) < 1e-5
+
+
+# ---------------------------------------------------------------------------
+# The product with a truncation number per level (SS interpolation up, RR anterpolation
+# down) against the product with K = 19 on every level.
+
+def _slab_oracle(oracle_lib, k_by_level=None, K=19):
+    from tests import problems as P
+    V, T = P.slab(cells=16, length_wl=4.0, seed=3)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_DIELECTRIC, tree_s_opt=60, threads=8, truncation_number=K)
+    info = o.tree()
+    if k_by_level:
+        o.set_level_truncation(k_by_level)
+    o.setup_fmm()
+    return o, info
+
+
+@pytest.fixture(scope="module")
+def slab_k19(oracle_lib):
+    from tests import problems as P
+    o, info = _slab_oracle(oracle_lib)
+    assert (info["l_min"], info["l_max"]) == (2, 3)  # one SS and one RR step between the levels
+    x = P.random_x(o.N, seed=1)
+    return x, o.matvec(x)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_equal_level_truncation_is_the_uniform_product(oracle_lib, slab_k19):
+    x, y19 = slab_k19
+    o, _ = _slab_oracle(oracle_lib, {2: 19, 3: 19})
+    assert np.array_equal(o.matvec(x), y19)
+
+
+# measured: 1.7e-3, 8.1e-4 and 4.5e-4; K = 12 and 14 on every level give 4.2e-3 and 1.1e-3
+@pytest.mark.parametrize("k_by_level,bound", [({3: 12, 2: 14}, 3e-3), ({3: 14, 2: 16}, 1.5e-3),
+                                              ({3: 16, 2: 19}, 1e-3)])
+def test_level_truncation_product(oracle_lib, slab_k19, k_by_level, bound):
+    x, y19 = slab_k19
+    o, _ = _slab_oracle(oracle_lib, k_by_level)
+    assert _rel(o.matvec(x), y19) < bound
+
+
+def test_larger_upper_truncation_helps(oracle_lib, slab_k19):
+    """Raising K on the upper level only (interpolated up, anterpolated down) makes the
+    product more accurate than the leaf's K on every level."""
+    x, y19 = slab_k19
+    err_uniform = _rel(_slab_oracle(oracle_lib, K=12)[0].matvec(x), y19)
+    err_level = _rel(_slab_oracle(oracle_lib, {3: 12, 2: 14})[0].matvec(x), y19)
+    assert err_level < 0.6 * err_uniform
+
+
+def test_truncation_growing_toward_the_leaf_is_refused(oracle_lib):
+    with pytest.raises(ValueError):
+        _slab_oracle(oracle_lib, {3: 16, 2: 14})
