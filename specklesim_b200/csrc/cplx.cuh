@@ -90,6 +90,23 @@ __device__ __forceinline__ cx<double> ld_stream(const cx<double>* a, unsigned lo
                : "l"(a), "l"(pol));
   return mk<double>(r, i);
 }
+// Loads of data re-read from L2 many times (the SR's level coefficients): evict-last.
+__device__ __forceinline__ unsigned long long l2_evict_last_policy() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ cx<double> ld_keep(const cx<double>* a, unsigned long long pol) {
+  double r, i;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+               : "=d"(r), "=d"(i)
+               : "l"(a), "l"(pol));
+  return mk<double>(r, i);
+}
+// Stores of results read once later (the SR's D): streaming, evict-first.
+__device__ __forceinline__ void st_stream(cx<double>* a, cx<double> v) {
+  asm volatile("st.global.cs.v2.f64 [%0], {%1, %2};\n" ::"l"(a), "d"(v.re), "d"(v.im) : "memory");
+}
 // complex64 streams: a plain load measured faster (8-byte accesses)
 __device__ __forceinline__ cx<float> ld_stream(const cx<float>* a, unsigned long long) { return *a; }
 
