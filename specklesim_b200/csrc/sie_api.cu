@@ -501,7 +501,7 @@ static int build_levels(sie_ctx* c) {
 
 // Gauss-Legendre nodes, ascending (the reference uses the Glaser-Liu-Rokhlin
 // rule, src/Gauss_Quadrature_Fast.f90:424-498; both are exact to rounding).
-static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
   x.assign(n, 0.0);
   w.assign(n, 0.0);
   auto leg = [n](double z, double& pn, double& dpn) {

@@ -295,6 +295,18 @@ int far_matvec64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, cudaEvent_t* e
 int far_matvec32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, cudaEvent_t* ev,
                  cudaEvent_t wait_recv = nullptr, const std::function<int()>* after_agg = nullptr);
 int far_prepare_kernels(sie_ctx* c);
+// Gauss-Legendre nodes and weights on [-1, 1], nodes ascending.
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
+// Sparse real matrix in CSR form.
+struct Csr {
+  int rows = 0, cols = 0;
+  std::vector<int> ptr, col;
+  std::vector<double> val;
+};
+// Local Lagrange interpolation (2p x 2p stencil) of a (theta, phi) pattern pair from the
+// Kc sampling to the Kp sampling: rows 2 Qp (theta values, then phi), columns 2 Qc.
+// With transpose, the anterpolation (its transpose).
+int interp_csr(int p, int Kc, int Kp, bool transpose, Csr& out);
 // Products of a batch of R right-hand sides (internal layout, vector r at offset r * 2M).
 // The near product writes y; the far product adds into it.
 int near_matvec_b64(sie_ctx* c, const zc* x, zc* y, int R, cudaStream_t st);
