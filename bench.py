@@ -30,7 +30,8 @@ WL = 632.8e-9
 EPS = -11.7 - 1.26j  # exp(+iwt) convention of the reference (lossy => Im < 0)
 
 WORKLOADS = {
-    # 10 lambda x 10 lambda rough slab, seed 0, corr 1 lambda, RMS 0.5 lambda, 1 lambda thick
+    # the headline case: 10 lambda x 10 lambda rough slab, seed 0, corr 1 lambda, RMS 0.5 lambda,
+    # 1 lambda thick
     "slab10": dict(length_wl=10.0, rms_wl=0.5, corr_wl=1.0, thickness_wl=1.0, cells=64, seed=0),
     # a small case for quick checks
     "slab4": dict(length_wl=4.0, rms_wl=0.3, corr_wl=1.0, thickness_wl=1.0, cells=24, seed=0),

@@ -162,3 +162,26 @@ def test_faithful_csr_lookup_equals_fast(slab_fmm):
     x = P.random_x(o.N, seed=2)
     a, b = o.matvec(x), o.matvec(x, faithful_lookup=True)
     assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(a)
+
+
+@pytest.mark.parametrize("ngp,diag_bound", [(3, 4e-3), (7, 6e-4)])
+def test_pmchwt_reciprocity(oracle_lib, ngp, diag_bound):
+    """Reciprocity of the Galerkin PMCHWT matrix (blocks of
+    tri_impedance_building_PMCHWT, lib_sie_tri_calculation_mod.f90:1713-1769, assembled
+    at :481-500): with Z = [[A, B], [C, D]] over (J, M) coefficients, the K-operator
+    block B is symmetric to rounding, and C = -B holds exactly because the assembly
+    sets D_mat(2,1) = -D_mat(1,2) (:498).  The L-operator blocks A and D are symmetric
+    up to the singular-pair quadrature (analytic inner integral, ngp x ngp outer rule),
+    so their asymmetry shrinks as ngp grows."""
+    V, T = P.sphere(sub=1)
+    o = oracle_lib.Oracle(V, T, P.WL, P.EPS_DIELECTRIC, formulation="PMCHWT", ngp=ngp, threads=8)
+    Z = o.dense()
+    M = o.M
+    o.close()
+    A, B, C, D = Z[:M, :M], Z[:M, M:], Z[M:, :M], Z[M:, M:]
+    nrm = np.linalg.norm
+    assert nrm(B - B.T) <= 1e-13 * nrm(B)
+    assert nrm(C + B) <= 1e-13 * nrm(B)
+    for X in (A, D):
+        asym = nrm(X - X.T) / nrm(X)
+        assert 0 < asym < diag_bound
