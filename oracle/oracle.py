@@ -62,6 +62,7 @@ def lib():
             "orc_boxes": (None, [vp, C.c_int, lp]),
             "orc_i4": (C.c_int, [vp, C.c_longlong, C.c_int, lp]),
             "orc_neighbours": (C.c_int, [C.c_longlong, C.c_int, lp]),
+            "orc_universal_index": (C.c_longlong, [dp, C.c_int]),
             "orc_setup_fmm": (C.c_longlong, [vp]),
             "orc_set_level_k": (None, [vp, ip, C.c_int]),
             "orc_level_Q": (C.c_int, [vp, C.c_int]),
@@ -247,6 +248,21 @@ class Oracle:
         lib().orc_fn(self.h, e, ot, _d(out))
         return dict(c=out[0:9].reshape(3, 3), area=out[9], length=out[10], df=out[11],
                     mid=out[12:15], nq=out[15:18])
+
+
+def universal_index(point, level):
+    """Box index (Morton, x the most significant bit) at `level` of a point in the unit
+    cube: lib_tree_hf_get_universal_index."""
+    p = np.ascontiguousarray(point, np.float64)
+    return int(lib().orc_universal_index(_d(p), int(level)))
+
+
+def neighbours(n, level):
+    """The up-to-26 level-`level` boxes around box n, x outer, y middle, z inner, n
+    itself left out: lib_tree_hf_get_neighbour_all_xD with k = 1."""
+    out = np.zeros(26, np.int64)
+    k = lib().orc_neighbours(int(n), int(level), _l(out))
+    return out[:k]
 
 
 def hankel2(z, n):

@@ -1631,6 +1631,13 @@ int orc_i4(void* h, long long n, int l, long long* out) {
   return (int)v.size();
 }
 
+// lib_tree_hf_get_universal_index (lib/libtree/src/lib/lib_tree_helper_functions.f90):
+// index of the level-l box holding a point of the unit cube, x the most significant bit
+// of each octal digit.  The same coord_bits + morton3 that build_tree applies.
+long long orc_universal_index(const double* x, int l) {
+  return (long long)morton3(coord_bits(x[0], l), coord_bits(x[1], l), coord_bits(x[2], l), l);
+}
+
 int orc_neighbours(long long n, int l, long long* out) {
   std::vector<uint64_t> v = neighbours((uint64_t)n, l);
   for (size_t i = 0; i < v.size(); i++) out[i] = (long long)v[i];

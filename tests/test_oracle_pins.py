@@ -59,3 +59,24 @@ def test_gmres_tridiagonal_all_ones(oracle_lib):
     x, info = oracle_lib.zgmres(lambda v: A @ v, b, g["restart"], 1e-13, 1000)
     assert info["converged"]
     assert np.allclose(x, np.ones(n), atol=1e-9)
+
+
+def test_tree_universal_index_known_answers(oracle_lib):
+    """lib_tree_helper_functions.f90: test_lib_tree_hf_get_universal_index (3-D branch:
+    (0.75, 0.5, 2^-9 + 2^-8) at level 1 is box 6) and
+    test_lib_tree_hf_get_universal_index_l_max (double points, 8-byte index: every
+    coordinate 1 - 2^-21 at level 21 = int(64 / 3) is box 2^63 - 1)."""
+    assert oracle_lib.universal_index([0.75, 0.5, 2.0 ** -9 + 2.0 ** -8], 1) == 6
+    f = 1.0 - 2.0 ** -21
+    assert oracle_lib.universal_index([f, f, f], 21) == 2 ** 63 - 1
+
+
+def test_tree_neighbours_known_answers(oracle_lib):
+    """lib_tree_helper_functions.f90: test_lib_tree_hf_get_neighbour_all_xD (3-D, k = 1,
+    box 35 at level 2, all 26 neighbours inside the domain) and
+    test_lib_tree_hf_get_neighbour_all_xD_2 (box 5 at level 1, a corner box with 7).
+    The reference lists them in its loop order, which the oracle keeps."""
+    truth = [4, 5, 12, 6, 7, 14, 20, 21, 28, 32, 33, 40, 34, 42, 48, 49, 56,
+             36, 37, 44, 38, 39, 46, 52, 53, 60]
+    assert oracle_lib.neighbours(35, 2).tolist() == truth
+    assert oracle_lib.neighbours(5, 1).tolist() == [0, 1, 2, 3, 4, 6, 7]
