@@ -2,7 +2,8 @@
 
 Run in a container that has the reference source tree (read as text only):
     python tests/golden/make_golden.py /path/to/SpeckleSim
-Writes tests/golden/hankel2_x2.json and tests/golden/gmres_tridiag.json.
+Writes tests/golden/hankel2_x2.json, tests/golden/hankel2_x2p2i.json and
+tests/golden/gmres_tridiag.json.
 """
 import json
 import os
@@ -16,11 +17,11 @@ def fnum(s):
     return float(s.replace("_8", "").replace("d", "e").replace("D", "e"))
 
 
-def hankel(ref):
+def hankel(ref, test="test_lib_math_bessel_spherical_third_kind_2_real"):
     path = os.path.join(ref, "src/lib/libmath/src/math/lib_math_bessel.f90")
     src = open(path).read().splitlines()
-    start = next(i for i, l in enumerate(src) if "function test_lib_math_bessel_spherical_third_kind_2_real" in l)
-    end = next(i for i in range(start + 1, len(src)) if "end function test_lib_math_bessel_spherical_third_kind_2_real" in src[i])
+    start = next(i for i, l in enumerate(src) if "function " + test in l)
+    end = next(i for i in range(start + 1, len(src)) if "end function " + test in src[i])
     vals = {}
     pat = re.compile(r"ground_truth_y\((\d+)\)\s*=\s*cmplx\(([^,]+),\s*([+-]?\s*[^,]+),\s*kind=8\)")
     for i in range(start, end):
@@ -32,10 +33,13 @@ def hankel(ref):
         m = re.search(r"double precision :: x = ([0-9.]+)", src[i])
         if m:
             x = float(m.group(1))
+        m = re.search(r"complex\(kind=8\) :: x = cmplx\(([0-9.]+)_8, ([+-]?[0-9.]+)_8, kind=8\)", src[i])
+        if m:
+            x = [float(m.group(1)), float(m.group(2))]
     n = max(vals)
     return {
         "source": f"src/lib/libmath/src/math/lib_math_bessel.f90:{start + 1}-{end + 1} "
-                  "(test_lib_math_bessel_spherical_third_kind_2_real; values from sageMath)",
+                  f"({test}; values from sageMath)",
         "x": x, "orders": list(range(n)),
         "re": [vals[i + 1][0] for i in range(n)], "im": [vals[i + 1][1] for i in range(n)],
         "tolerance_log": 1e-13,
@@ -58,6 +62,8 @@ if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     with open(os.path.join(HERE, "hankel2_x2.json"), "w") as f:
         json.dump(hankel(ref), f, indent=1)
+    with open(os.path.join(HERE, "hankel2_x2p2i.json"), "w") as f:
+        json.dump(hankel(ref, "test_lib_math_bessel_spherical_third_kind_2_cmplx"), f, indent=1)
     with open(os.path.join(HERE, "gmres_tridiag.json"), "w") as f:
         json.dump(gmres(ref), f, indent=1)
     print("ok")

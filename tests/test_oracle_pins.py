@@ -20,6 +20,19 @@ def test_hankel2_known_answers(oracle_lib):
     assert np.all(np.sign(h.real) == np.sign(re)) and np.all(np.sign(h.imag) == np.sign(im))
 
 
+def test_hankel2_complex_known_answers(oracle_lib):
+    """lib_math_bessel.f90: test_lib_math_bessel_spherical_third_kind_2_cmplx (z = 2 + 2i,
+    orders 0..40, |log|value| - log|truth|| <= 1e-13 for Re and Im, signs equal).  The
+    translation tables evaluate h2 at complex k R in a lossy medium; this pins the
+    recurrence off the real axis."""
+    g = json.load(open(os.path.join(GOLD, "hankel2_x2p2i.json")))
+    h = oracle_lib.hankel2(complex(*g["x"]), len(g["re"]))
+    re, im = np.array(g["re"]), np.array(g["im"])
+    assert np.all(np.abs(np.log(np.abs(h.real)) - np.log(np.abs(re))) <= g["tolerance_log"])
+    assert np.all(np.abs(np.log(np.abs(h.imag)) - np.log(np.abs(im))) <= g["tolerance_log"])
+    assert np.all(np.sign(h.real) == np.sign(re)) and np.all(np.sign(h.imag) == np.sign(im))
+
+
 @pytest.mark.parametrize("z", [3.7 + 0.0j, 12.0 + 0.0j, 25.3 + 0.0j, 5.0 - 0.3j, 9.0 - 1.0j])
 def test_hankel2_vs_scipy(oracle_lib, z):
     from scipy.special import spherical_jn, spherical_yn
