@@ -185,3 +185,38 @@ def test_pmchwt_reciprocity(oracle_lib, ngp, diag_bound):
     for X in (A, D):
         asym = nrm(X - X.T) / nrm(X)
         assert 0 < asym < diag_bound
+
+
+def test_translation_tables_vs_scipy(slab_fmm):
+    """TL_km_ml_fmm (lib_sie_mlfmm.f90:129-188): for the 316 offsets r of the 7 x 7 x 7
+    stencil outside the central 3 x 3 x 3 block (box size D / 2^l), and every k-space
+    direction khat, TL = sum_{l<K} (-i)^(l+1) (2l+1) h2_l(k|r|) P_l(khat . rhat) k / (4 pi)^2,
+    evaluated here with scipy.  The lossy medium's table is kept only at the leaf level
+    (:164-172); coarser levels hold zeros there."""
+    from scipy.special import eval_legendre, spherical_jn, spherical_yn
+    o, info = slab_fmm
+    mat = o.material()
+    kh = o.sampling()[0]
+    for lev in range(info["l_min"], info["l_max"] + 1):
+        TL = o.tl(lev)
+        Q = TL.shape[2]
+        K = int(round(np.sqrt(Q // 2)))
+        assert 2 * K * K + 2 == Q
+        dx = info["D"] / 2 ** lev
+        n = np.arange(K)
+        for t in range(0, 343, 11):
+            i, j, k = t // 49, (t // 7) % 7, t % 7
+            if 2 <= i <= 4 and 2 <= j <= 4 and 2 <= k <= 4:
+                assert not TL[t].any()
+                continue
+            r = dx * (np.array([i, j, k]) - 3.0)
+            rl = np.linalg.norm(r)
+            P = eval_legendre(n[:, None], (kh[:Q] @ (r / rl))[None, :])
+            for med, kk in enumerate([mat["k1"], mat["k2"]]):
+                if med == 1 and lev < info["l_max"] and kk.imag != 0:
+                    assert not TL[t, 1].any()
+                    continue
+                h = spherical_jn(n, kk * rl) - 1j * spherical_yn(n, kk * rl)
+                coef = (-1j) ** (n + 1) * (2 * n + 1) * h * kk / (4 * np.pi) ** 2
+                ref = coef @ P
+                assert np.allclose(TL[t, med], ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
