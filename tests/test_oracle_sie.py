@@ -220,3 +220,32 @@ def test_translation_tables_vs_scipy(slab_fmm):
                 coef = (-1j) ** (n + 1) * (2 * n + 1) * h * kk / (4 * np.pi) ** 2
                 ref = coef @ P
                 assert np.allclose(TL[t, med], ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+
+
+def test_rhs_formulation_scaling_and_magnetic_half(oracle_lib):
+    """get_vector_b_tri (lib_sie_tri_calculation_mod.f90:391-460): PMCHWT takes the
+    tested incident fields (<f_m, E_inc>, <f_m, H_inc>) as they are, ICTF divides the
+    electric half by eta_a and multiplies the magnetic half by it.  The magnetic half is
+    the electric one of the field k_hat x E / (mu_1 c0) (incident_field_tri_general,
+    :939-1002), so it equals the electric half of the PMCHWT right-hand side for that
+    polarisation."""
+    V, T = P.sphere(sub=2)
+    k = np.array([0.3, -0.2, -1.0])
+    k /= np.linalg.norm(k)
+    E = np.cross(k, [0.0, 1.0, 0.0])
+    E = E / np.linalg.norm(E)  # illumination_p%E_in is real(dp)
+    oi = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, formulation="ICTF", ngp=7)
+    op = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, formulation="PMCHWT", ngp=7)
+    M = oi.M
+    mat = oi.material()
+    bi, bp = oi.rhs(k, E), op.rhs(k, E)
+    scale = np.abs(bp).max()
+    assert np.allclose(bi[:M] * mat["eta_a"], bp[:M], rtol=1e-13, atol=1e-14 * scale)
+    assert np.allclose(bi[M:] / mat["eta_a"], bp[M:], rtol=1e-13, atol=1e-14 * scale)
+    # my_1 = my_0 and c0 are unsuffixed literals, so binary32 values held in real(dp)
+    # (lib_sie_constants.f90:9-11); exact SI values would be off by 8e-8 here
+    mu0c0 = float(np.float32(1.2566370614e-6)) * float(np.float32(2.99792458e8))
+    bh = op.rhs(k, np.cross(k, E) / mu0c0)
+    assert np.allclose(bh[:M], bp[M:], rtol=1e-10, atol=1e-12 * np.abs(bp[M:]).max())
+    oi.close()
+    op.close()
