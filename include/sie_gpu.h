@@ -161,6 +161,13 @@ int sie_rhs_planewave(sie_ctx* ctx, const double* k_in, const double* E_in, int 
  * k_dir = calc_p(7).  Writes k_in[3], E_in[3]. */
 int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in);
 
+/* The ngp-point triangle rule the fill kernels use, Quadrature_tri
+ * (src/lib_sie_integration_points.f90:7-143): barycentric points (alpha, beta) and
+ * weights summing to 1, each the binary32 value of the reference's literal.  alpha,
+ * beta, w: room for 12 values; *n = ngp.  Host only; no device is needed.  ngp other
+ * than 1, 3, 4, 6, 7, 12 gives SIE_ERR_ARG. */
+int sie_quadrature_rule(int ngp, double* alpha, double* beta, double* w, int* n);
+
 /* Solve Z x = b for nrhs right-hand sides (stride 2M).  With precision SIE_FP64 each is
  * solved in turn with zgmres semantics; with SIE_MIXED and nrhs > 1 they are solved in
  * batches of up to 16 that advance in lockstep, one batched product per step (restart

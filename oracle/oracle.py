@@ -63,6 +63,7 @@ def lib():
             "orc_i4": (C.c_int, [vp, C.c_longlong, C.c_int, lp]),
             "orc_neighbours": (C.c_int, [C.c_longlong, C.c_int, lp]),
             "orc_universal_index": (C.c_longlong, [dp, C.c_int]),
+            "orc_quad_rule": (C.c_int, [C.c_int, dp, dp, dp]),
             "orc_setup_fmm": (C.c_longlong, [vp]),
             "orc_set_level_k": (None, [vp, ip, C.c_int]),
             "orc_level_Q": (C.c_int, [vp, C.c_int]),
@@ -248,6 +249,14 @@ class Oracle:
         lib().orc_fn(self.h, e, ot, _d(out))
         return dict(c=out[0:9].reshape(3, 3), area=out[9], length=out[10], df=out[11],
                     mid=out[12:15], nq=out[15:18])
+
+
+def quad_rule(ngp):
+    """Barycentric points (alpha, beta) and weights of the ngp-point triangle rule, as the
+    oracle uses them: Quadrature_tri."""
+    a, b, w = np.zeros(12), np.zeros(12), np.zeros(12)
+    n = lib().orc_quad_rule(int(ngp), _d(a), _d(b), _d(w))
+    return a[:n], b[:n], w[:n]
 
 
 def universal_index(point, level):

@@ -1634,6 +1634,14 @@ int orc_i4(void* h, long long n, int l, long long* out) {
 // lib_tree_hf_get_universal_index (lib/libtree/src/lib/lib_tree_helper_functions.f90):
 // index of the level-l box holding a point of the unit cube, x the most significant bit
 // of each octal digit.  The same coord_bits + morton3 that build_tree applies.
+// Quadrature_tri (src/lib_sie_integration_points.f90:7-143) as the oracle holds it;
+// returns the number of points (0 for an ngp the reference does not define).
+int orc_quad_rule(int ngp, double* a, double* b, double* w) {
+  Rule r = make_rule(ngp);
+  for (int i = 0; i < r.n; i++) { a[i] = r.a[i]; b[i] = r.b[i]; w[i] = r.w[i]; }
+  return r.n;
+}
+
 long long orc_universal_index(const double* x, int l) {
   return (long long)morton3(coord_bits(x[0], l), coord_bits(x[1], l), coord_bits(x[2], l), l);
 }

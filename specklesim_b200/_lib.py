@@ -76,7 +76,7 @@ EXPORTS = [
     "sie_get_edges", "sie_get_tree", "sie_get_blocks", "sie_get_near_entries", "sie_get_rt",
     "sie_num_directions", "sie_get_timings", "sie_set_stream", "sie_launch_count", "sie_free",
     "sie_farfield_device_noalloc", "sie_solve_direct", "sie_matvec_adjoint", "sie_matvec_adjoint_device",
-    "sie_grad", "sie_set_inner_operator", "sie_autotune",
+    "sie_grad", "sie_set_inner_operator", "sie_autotune", "sie_quadrature_rule",
 ]
 
 _lib = None
@@ -107,6 +107,7 @@ def load(path=None):
         "sie_matvec_device": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp]),
         "sie_rhs_planewave": (C.c_int, [vp, dp, dp, C.c_int, dp]),
         "sie_incidence": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, dp, dp]),
+        "sie_quadrature_rule": (C.c_int, [C.c_int, dp, dp, dp, C.POINTER(C.c_int)]),
         "sie_solve": (C.c_int, [vp, dp, dp, C.c_int, C.POINTER(SieSolverCfg), C.POINTER(SieStats)]),
         "sie_solve_device": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(SieSolverCfg), C.POINTER(SieStats)]),
         "sie_precondition_left": (C.c_int, [vp, dp, dp]),

@@ -1185,6 +1185,19 @@ int sie_matvec_adjoint(sie_ctx* c, const double* x, double* y, int nrhs) {
   return r;
 }
 
+int sie_quadrature_rule(int ngp, double* alpha, double* beta, double* w, int* n) {
+  if (!alpha || !beta || !w || !n) return fail(SIE_ERR_ARG, "sie_quadrature_rule: null argument");
+  const Rule r = make_rule(ngp);
+  if (r.n == 0) return fail(SIE_ERR_ARG, "sie_quadrature_rule: ngp must be 1, 3, 4, 6, 7 or 12");
+  for (int i = 0; i < r.n; i++) {
+    alpha[i] = r.a[i];
+    beta[i] = r.b[i];
+    w[i] = r.w[i];
+  }
+  *n = r.n;
+  return SIE_OK;
+}
+
 int sie_incidence(double theta, double phi, int pol, int k_dir, double* k_in, double* E_in) {
   if (!k_in || !E_in) return fail(SIE_ERR_ARG, "sie_incidence: null argument");
   if (k_dir != 1 && k_dir != 2) return fail(SIE_ERR_ARG, "sie_incidence: k_dir must be 1 or 2");

@@ -2,8 +2,8 @@
 
 Run in a container that has the reference source tree (read as text only):
     python tests/golden/make_golden.py /path/to/SpeckleSim
-Writes tests/golden/hankel2_x2.json, tests/golden/hankel2_x2p2i.json and
-tests/golden/gmres_tridiag.json.
+Writes tests/golden/hankel2_x2.json, tests/golden/hankel2_x2p2i.json,
+tests/golden/gmres_tridiag.json and tests/golden/quadrature_tri.json.
 """
 import json
 import os
@@ -58,6 +58,34 @@ def gmres(ref):
     }
 
 
+def quadrature(ref):
+    """The triangle rules of Quadrature_tri as written in the source (decimal literals;
+    the compiled reference holds them as binary32 values)."""
+    path = os.path.join(ref, "src/lib_sie_integration_points.f90")
+    lines = open(path).read().splitlines()
+    start = next(i for i, l in enumerate(lines) if "subroutine Quadrature_tri" in l)
+    end = next(i for i in range(start + 1, len(lines)) if lines[i].strip().startswith("end subroutine"))
+    body = "\n".join(lines[start:end + 1])
+    parts = re.split(r"if \(ngp == (\d+)\) then", body)
+    rules = {}
+    for k in range(1, len(parts), 2):
+        n = int(parts[k])
+        rule = {}
+        for name in ("alpha", "beta", "ww"):
+            m = re.search(name + r"\(1:ngp\)\s*=\s*&?\s*(?:\(/(.*?)/\)|([0-9.]+))", parts[k + 1], re.S)
+            if m.group(1) is not None:
+                vals = [float(v.replace("&", "").strip()) for v in m.group(1).split(",")]
+            else:
+                vals = [float(m.group(2))] * n
+            assert len(vals) == n
+            rule[name] = vals
+        rules[str(n)] = rule
+    return {
+        "source": f"src/lib_sie_integration_points.f90:{start + 1}-{end + 1} (Quadrature_tri)",
+        "rules": rules,
+    }
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     with open(os.path.join(HERE, "hankel2_x2.json"), "w") as f:
@@ -66,4 +94,6 @@ if __name__ == "__main__":
         json.dump(hankel(ref, "test_lib_math_bessel_spherical_third_kind_2_cmplx"), f, indent=1)
     with open(os.path.join(HERE, "gmres_tridiag.json"), "w") as f:
         json.dump(gmres(ref), f, indent=1)
+    with open(os.path.join(HERE, "quadrature_tri.json"), "w") as f:
+        json.dump(quadrature(ref), f, indent=1)
     print("ok")

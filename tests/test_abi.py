@@ -52,3 +52,24 @@ def test_argument_errors_without_device(gpu_lib):
     assert gpu_lib.sie_init(C.byref(cfg), _lib.dptr(v), 3, _lib.iptr(t2), 2, C.byref(h)) == _lib.SIE_ERR_ARG
     assert b"ngp" in gpu_lib.sie_last_error()
     assert gpu_lib.sie_matvec(None, None, None, 1, 0) == _lib.SIE_ERR_ARG
+
+
+def test_quadrature_rules_are_the_reference_tables(gpu_lib):
+    """The library's triangle rules (host tables that the fill kernels copy) against the
+    reference's Quadrature_tri literals, as binary32 values, bit for bit."""
+    import json
+    from specklesim_b200 import _lib
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "quadrature_tri.json")))["rules"]
+    a, b, w = np.zeros(12), np.zeros(12), np.zeros(12)
+    n = C.c_int()
+    f32 = lambda v: np.asarray(v, np.float32).astype(np.float64)
+    for ngp, rule in g.items():
+        assert gpu_lib.sie_quadrature_rule(int(ngp), _lib.dptr(a), _lib.dptr(b), _lib.dptr(w),
+                                           C.byref(n)) == _lib.SIE_OK
+        assert n.value == int(ngp)
+        assert np.array_equal(a[:n.value], f32(rule["alpha"]))
+        assert np.array_equal(b[:n.value], f32(rule["beta"]))
+        assert np.array_equal(w[:n.value], f32(rule["ww"]))
+    assert gpu_lib.sie_quadrature_rule(5, _lib.dptr(a), _lib.dptr(b), _lib.dptr(w),
+                                       C.byref(n)) == _lib.SIE_ERR_ARG
+    assert b"ngp" in gpu_lib.sie_last_error()

@@ -93,3 +93,23 @@ def test_tree_neighbours_known_answers(oracle_lib):
              36, 37, 44, 38, 39, 46, 52, 53, 60]
     assert oracle_lib.neighbours(35, 2).tolist() == truth
     assert oracle_lib.neighbours(5, 1).tolist() == [0, 1, 2, 3, 4, 6, 7]
+
+
+@pytest.mark.parametrize("ngp,degree", [(1, 1), (3, 2), (4, 3), (6, 4), (7, 5), (12, 6)])
+def test_triangle_rules_match_the_reference_tables(oracle_lib, ngp, degree):
+    """Quadrature_tri (lib_sie_integration_points.f90:7-143): the oracle holds every
+    point and weight as the binary32 value of the reference's decimal literal (the
+    reference is compiled without real-kind promotion), and each rule integrates the
+    monomials a^i b^j, i + j <= degree, over the unit triangle to binary32 accuracy:
+    sum w a^i b^j = 2 i! j! / (i + j + 2)!."""
+    from math import factorial
+    g = json.load(open(os.path.join(GOLD, "quadrature_tri.json")))["rules"][str(ngp)]
+    a, b, w = oracle_lib.quad_rule(ngp)
+    f32 = lambda v: np.asarray(v, np.float32).astype(np.float64)
+    assert np.array_equal(a, f32(g["alpha"]))
+    assert np.array_equal(b, f32(g["beta"]))
+    assert np.array_equal(w, f32(g["ww"]))
+    for i in range(degree + 1):
+        for j in range(degree + 1 - i):
+            exact = 2.0 * factorial(i) * factorial(j) / factorial(i + j + 2)
+            assert abs(np.sum(w * a ** i * b ** j) - exact) <= 3e-7, (i, j)
