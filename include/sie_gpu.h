@@ -192,7 +192,10 @@ int sie_precondition_left(sie_ctx* ctx, const double* v1, double* v2);
 /* Scattered E and H at observation points (Integration_scattered_field_tri,
  * src/lib_sie_tri_calculation_mod.f90:2782-2825) and the 'rcs' intensity
  * |E|^2 4 pi |r|^2 (src/lib_sie_tri_solver_normal.f90:325-342).
- * pts: npts x 3; E, H: npts x 3 complex (may be NULL); intensity: npts. */
+ * pts: npts x 3; E, H: npts x 3 complex (may be NULL); intensity: npts.
+ * As in the reference, E leaves out the electric scalar-potential term (:2815
+ * multiplies it by 0), so E is right only in its transverse far-zone part; H keeps
+ * every term and is right at any point in the background medium. */
 int sie_farfield(sie_ctx* ctx, const double* x, const double* pts, int npts, double* E,
                  double* H, double* intensity);
 
