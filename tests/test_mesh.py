@@ -70,3 +70,42 @@ def test_iteration_log_format(tmp_path):
     p = tmp_path / "iteration_error.txt"
     io.write_iteration_log(p, [0.5, 1.25e-3])
     assert p.read_text().splitlines()[1] == "         2      1.250000000000E-03     "
+
+
+def test_run_parameters_file_roundtrip(tmp_path):
+    """Calculation_parameters_* (output_file_GMRES, lib_sie_solver_gmres_interface.f90:
+    214-241): the reference's labels in its order, one list-directed line each, and every
+    value read back exactly."""
+    from specklesim_b200 import io
+    keys = io.parameter_keys("surface")
+    assert keys[0] == "object_type" and keys[-1] == "m_pairs" and len(keys) == 25
+    vals = {k: 0 for k in keys}
+    vals.update({
+        "object_type": "surface", "formulation_type": "ICTF", "illumination_type": "Plane",
+        "beam_waist(nm) (Gaussian beam)": 0.0, "Wavelength (nm)": 632.8,
+        "object dimension I (nm)": 6328.0, "object dimension II (nm)": 6328.0,
+        "object centroid (m)": (0.0, 1.5e-9, -3.1640000000000001e-07),
+        "N_el": 20480, "eps_r2": -11.7 - 1.26j, "evaluation_type": "BRDF_p",
+        "evaluation_parameter%dim_a(nm)": (-1.5707963267948966, 1.5707963267948966),
+        "GMRES_time (min.)": 0.0123456789, "convergence_tolerance": 1e-6, "l_max": 4,
+        "dc at l_max": 7.91e-7, "tree_s_opt": 250, "m_pairs": 30720,
+    })
+    p = tmp_path / "Calculation_parameters_tri.txt"
+    io.write_parameters(p, vals)
+    lines = p.read_text().splitlines()
+    assert [ln[1:].split("=")[0] + "=" for ln in lines] == \
+        [lab.split("=")[0] + "=" for lab in io.PARAMETER_LABELS["surface"]]
+    assert lines[0] == " object_type =                  surface"
+    back = io.read_parameters(p)
+    assert list(back) == keys
+    for k in keys:
+        v = io.parse_parameter(back[k])
+        want = vals[k]
+        if isinstance(want, tuple):
+            assert v == want, k
+        elif isinstance(want, str):
+            assert v == want, k
+        else:
+            assert v == want and type(v) is type(want), k
+    with pytest.raises(KeyError):
+        io.write_parameters(tmp_path / "x.txt", {"object_type": "surface"})
