@@ -73,3 +73,24 @@ def test_quadrature_rules_are_the_reference_tables(gpu_lib):
     assert gpu_lib.sie_quadrature_rule(5, _lib.dptr(a), _lib.dptr(b), _lib.dptr(w),
                                        C.byref(n)) == _lib.SIE_ERR_ARG
     assert b"ngp" in gpu_lib.sie_last_error()
+
+
+def test_incidence_matches_the_reference_rotation(gpu_lib):
+    """sie_incidence against kin_and_Ein_calculation and
+    field_rotation_conical_illumination (lib_sie_math.f90:228-293), restated here: k_in =
+    (sin t cos p, sin t sin p, s cos t) with s = +1 / -1 for k_dir 1 / 2, and E_in = Rm
+    (1, 0) for TM, Rm (0, 1) for TE, Rm the 3 x 2 rotation of that routine."""
+    from specklesim_b200 import _lib
+    k = np.zeros(3)
+    e = np.zeros(3)
+    for t in np.linspace(0.0, 1.4, 6):
+        for p in np.linspace(-3.0, 3.0, 7):
+            a, b, c, d = np.sin(t), np.cos(t), np.sin(p), np.cos(p)
+            Rm = np.array([[d * d * b + c * c, c * d * (b - 1)],
+                           [c * d * (b - 1), c * c * b + d * d],
+                           [a * d, a * c]])
+            for pol, e_t in ((1, [1.0, 0.0]), (2, [0.0, 1.0])):
+                for k_dir, s in ((1, 1.0), (2, -1.0)):
+                    assert gpu_lib.sie_incidence(t, p, pol, k_dir, _lib.dptr(k), _lib.dptr(e)) == 0
+                    assert np.allclose(k, [a * d, a * c, s * b], rtol=0, atol=1e-15)
+                    assert np.allclose(e, Rm @ e_t, rtol=0, atol=1e-15)
