@@ -109,3 +109,28 @@ def test_run_parameters_file_roundtrip(tmp_path):
             assert v == want and type(v) is type(want), k
     with pytest.raises(KeyError):
         io.write_parameters(tmp_path / "x.txt", {"object_type": "surface"})
+
+
+def test_evaluation_points_follow_the_reference_layout():
+    """get_evaluation_points (lib_sie_math.f90:295-359): point (i, j) at index (i - 1) n_a + j with
+    the dim_b step outer; 'xy' counts down from the maxima, 'xz' up from the minima; the
+    rcs and BRDF cuts sweep theta over dim_a at phi = dim_b(1) on a sphere of radius
+    dim_c."""
+    from specklesim_b200.observation import evaluation_points
+    p = evaluation_points("xy", (-1.0, 1.0), (-2.0, 2.0), 0.5, 3, 2)
+    assert p.shape == (6, 3)
+    assert np.allclose(p[:3], [[1, 2, 0.5], [0, 2, 0.5], [-1, 2, 0.5]])
+    assert np.allclose(p[3:], [[1, -2, 0.5], [0, -2, 0.5], [-1, -2, 0.5]])
+    p = evaluation_points("yz", (-1.0, 1.0), (0.0, 4.0), 0.25, 2, 3)
+    assert np.allclose(p, [[0.25, 1, 4], [0.25, -1, 4], [0.25, 1, 2], [0.25, -1, 2],
+                           [0.25, 1, 0], [0.25, -1, 0]])
+    p = evaluation_points("xz", (-1.0, 1.0), (0.0, 4.0), -0.3, 3, 2)
+    assert np.allclose(p, [[-1, -0.3, 0], [0, -0.3, 0], [1, -0.3, 0],
+                           [-1, -0.3, 4], [0, -0.3, 4], [1, -0.3, 4]])
+    p = evaluation_points("BRDF_p", (0.0, np.pi / 2), (np.pi / 4, 0.0), 5.0, 5, 64)
+    assert p.shape == (5, 3)
+    assert np.allclose(np.linalg.norm(p, axis=1), 5.0)
+    assert np.allclose(p[0], [0, 0, 5]) and np.allclose(p[-1], [5 / np.sqrt(2), 5 / np.sqrt(2), 0])
+    assert np.allclose(np.arccos(p[:, 2] / 5.0), np.linspace(0, np.pi / 2, 5))
+    with pytest.raises(ValueError):
+        evaluation_points("zz", (0, 1), (0, 1), 0.0, 3, 3)
