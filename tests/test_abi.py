@@ -94,3 +94,45 @@ def test_incidence_matches_the_reference_rotation(gpu_lib):
                     assert gpu_lib.sie_incidence(t, p, pol, k_dir, _lib.dptr(k), _lib.dptr(e)) == 0
                     assert np.allclose(k, [a * d, a * c, s * b], rtol=0, atol=1e-15)
                     assert np.allclose(e, Rm @ e_t, rtol=0, atol=1e-15)
+
+
+def _c_structs(src):
+    """{name: [(type, field), ...]} of the header's typedef structs."""
+    out = {}
+    for body, name in re.findall(r"typedef struct \{(.*?)\}\s*(\w+);", src, re.S):
+        fields = []
+        for decl in re.sub(r"/\*.*?\*/", "", body, flags=re.S).split(";"):
+            m = re.match(r"\s*(int|double)\s+(.+)", decl)
+            if m:
+                fields += [(m.group(1), f.strip()) for f in m.group(2).split(",")]
+        out[name] = fields
+    return out
+
+
+def test_fortran_shim_matches_the_header():
+    """The Fortran shim is not compiled here (no Fortran compiler), so check it against
+    include/sie_gpu.h as text: every bind(C) type has the C struct's fields in the same
+    order with the matching kinds, and every bound procedure names a declared function
+    with the same number of arguments."""
+    hdr = open(os.path.join(ROOT, "include", "sie_gpu.h")).read()
+    shim = open(os.path.join(ROOT, "specklesim_b200", "fortran", "sie_shim.f90")).read()
+    kinds = {"integer(c_int)": "int", "real(c_double)": "double"}
+    structs = _c_structs(hdr)
+    ftypes = re.findall(r"type, bind\(C\) :: (\w+)\n(.*?)end type", shim, re.S)
+    assert {n for n, _ in ftypes} == {"sie_config", "sie_solver_cfg", "sie_stats"}
+    for name, body in ftypes:
+        fields = []
+        for line in body.strip().splitlines():
+            kind, names = line.split("::")
+            fields += [(kinds[kind.strip()], f.strip()) for f in names.split(",")]
+        assert fields == structs[name], name
+    nocomment = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    bound = re.findall(r"(?:function|subroutine) (\w+)\(([^)]*)\)\s*bind\(C, name=\"(\w+)\"\)", shim)
+    assert len(bound) >= 12
+    for fname, args, cname in bound:
+        assert fname == cname
+        m = re.search(r"\b" + cname + r"\s*\(([^)]*)\)\s*;", nocomment)
+        assert m, cname
+        c_args = [a for a in m.group(1).split(",") if a.strip() and a.strip() != "void"]
+        f_args = [a for a in args.split(",") if a.strip()]
+        assert len(f_args) == len(c_args), cname
