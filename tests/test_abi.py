@@ -136,3 +136,15 @@ def test_fortran_shim_matches_the_header():
         c_args = [a for a in m.group(1).split(",") if a.strip() and a.strip() != "void"]
         f_args = [a for a in args.split(",") if a.strip()]
         assert len(f_args) == len(c_args), cname
+
+
+def test_ctypes_structs_match_the_header():
+    """The ctypes mirrors in specklesim_b200/_lib.py have the header structs' fields in
+    order with matching types (Python's reserved 'lambda' is spelled 'lambda_')."""
+    from specklesim_b200 import _lib
+    structs = _c_structs(open(os.path.join(ROOT, "include", "sie_gpu.h")).read())
+    ctype = {C.c_int: "int", C.c_double: "double"}
+    for py, name in ((_lib.SieConfig, "sie_config"), (_lib.SieSolverCfg, "sie_solver_cfg"),
+                     (_lib.SieStats, "sie_stats")):
+        fields = [(ctype[t], f.rstrip("_")) for f, t in py._fields_]
+        assert fields == structs[name], name
