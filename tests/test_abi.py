@@ -148,3 +148,11 @@ def test_ctypes_structs_match_the_header():
                      (_lib.SieStats, "sie_stats")):
         fields = [(ctype[t], f.rstrip("_")) for f, t in py._fields_]
         assert fields == structs[name], name
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """There is no CPU fallback: without libsiegpu.so the loader raises."""
+    import pytest
+    from specklesim_b200 import _lib
+    with pytest.raises(_lib.SieError):
+        _lib.load(str(tmp_path / "libsiegpu.so"))
