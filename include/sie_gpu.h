@@ -48,7 +48,10 @@ typedef struct sie_ctx sie_ctx;
 typedef struct {
   double lambda;                   /* illumination_p%lambda [m] */
   double eps_r1_re, eps_r1_im;     /* background relative permittivity (1, 0) */
-  double eps_r2_re, eps_r2_im;     /* body relative permittivity */
+  double eps_r2_re, eps_r2_im;     /* body relative permittivity.  As in the reference,
+                                      eps_r2_im != 0 keeps the body-medium translations
+                                      at the leaf level only: right for metals, far off
+                                      for weakly lossy dielectrics (use dense = 1) */
   int formulation;                 /* SIE_ICTF (calc_p(3)=3, default) or SIE_PMCHWT */
   int ngp;                         /* triangle rule points, ng = 3 (1,3,4,6,7,12) */
   int tree_s_opt;                  /* tree_s_opt = 250 */
