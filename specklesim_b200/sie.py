@@ -24,6 +24,16 @@ def incidence(theta, phi, pol="TM", k_dir=2):
     return k, e
 
 
+def quadrature_rule(ngp):
+    """(alpha, beta, w) of the ngp-point triangle rule that the fill kernels use
+    (Quadrature_tri, src/lib_sie_integration_points.f90:7-143).  Needs no GPU."""
+    lib = _lib.load()
+    a, b, w = np.zeros(12), np.zeros(12), np.zeros(12)
+    n = C.c_int()
+    check(lib.sie_quadrature_rule(int(ngp), dptr(a), dptr(b), dptr(w), C.byref(n)))
+    return a[:n.value], b[:n.value], w[:n.value]
+
+
 class Sie:
     def __init__(self, verts, tris, wavelength, eps_r2, eps_r1=1.0, formulation="ICTF", ngp=3,
                  tree_s_opt=250, truncation_number=19, normal_convention=2, fix_itbn=False,

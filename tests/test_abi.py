@@ -156,3 +156,13 @@ def test_missing_library_fails_loudly(tmp_path):
     from specklesim_b200 import _lib
     with pytest.raises(_lib.SieError):
         _lib.load(str(tmp_path / "libsiegpu.so"))
+
+
+def test_python_quadrature_rule(gpu_lib):
+    import pytest
+    from specklesim_b200 import SieError
+    from specklesim_b200.sie import quadrature_rule
+    a, b, w = quadrature_rule(12)
+    assert len(a) == len(b) == len(w) == 12 and abs(w.sum() - 1.0) < 1e-6
+    with pytest.raises(SieError):
+        quadrature_rule(2)
