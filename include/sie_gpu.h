@@ -240,7 +240,10 @@ unsigned long long sie_launch_count(void);
  * values per GPU; meshes with more edges get SIE_ERR_ARG.  Calls that may run at
  * the same time on one GPU (other streams, other threads, other contexts) share
  * that array and race: order them on one stream.  The first call on each GPU
- * looks the array up (cudaGetSymbolAddress); make it before any stream capture. */
+ * looks the array up (cudaGetSymbolAddress); make it before any stream capture.
+ * The address is kept for the life of the process: after a cudaDeviceReset it is
+ * stale, so do not call this entry point again once the device has been reset.
+ * The caller's current device is the same after the call as before it. */
 int sie_farfield_device_noalloc(sie_ctx* ctx, const double* d_x, const double* d_pts, int npts,
                                 double* d_E, double* d_H, double* d_I, void* stream);
 

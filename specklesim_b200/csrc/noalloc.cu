@@ -27,9 +27,24 @@ static __device__ __align__(256) zc g_noalloc_x[2 * SIE_NOALLOC_MAX_EDGES];
 
 namespace {
 const int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-cudaError_t g_sym_rc[kMaxDevices];
+// Device address of g_noalloc_x per device ordinal, looked up by the first call on that
+// device that succeeds; a failed lookup is not kept, so the next call tries again.  The
+// address belongs to the module loaded in the device's primary context: after a
+// cudaDeviceReset it is stale, and this entry point must not be called again in the
+// process.
+std::mutex g_sym_mu;
 zc* g_sym_ptr[kMaxDevices];
+
+// Restores the caller's current device when the call returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 }  // namespace
 
 extern "C" int sie_farfield_device_noalloc(sie_ctx* c, const double* d_x, const double* d_pts,
@@ -43,16 +58,20 @@ extern "C" int sie_farfield_device_noalloc(sie_ctx* c, const double* d_x, const 
   if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_farfield_device_noalloc: sie_setup not called");
   if (c->device < 0 || c->device >= kMaxDevices)
     return fail(SIE_ERR_ARG, "sie_farfield_device_noalloc: device ordinal out of range");
+  DeviceGuard keep_device;
   SIE_CUDA(cudaSetDevice(c->device));
-  // The scratch address is looked up once per device, by the first call on it.
-  std::call_once(g_once[c->device], [c] {
-    void* p = nullptr;
-    g_sym_rc[c->device] = cudaGetSymbolAddress(&p, g_noalloc_x);
-    g_sym_ptr[c->device] = (zc*)p;
-  });
-  if (g_sym_rc[c->device] != cudaSuccess)
-    return cuda_fail(g_sym_rc[c->device], "sie_farfield_device_noalloc: cudaGetSymbolAddress");
-  zc* xi = g_sym_ptr[c->device];
+  zc* xi = nullptr;
+  {
+    // the scratch address is looked up once per device, with that device current
+    std::lock_guard<std::mutex> lk(g_sym_mu);
+    if (!g_sym_ptr[c->device]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_x);
+      if (e != cudaSuccess) return cuda_fail(e, "sie_farfield_device_noalloc: cudaGetSymbolAddress");
+      g_sym_ptr[c->device] = (zc*)p;
+    }
+    xi = g_sym_ptr[c->device];
+  }
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   int M = c->M;
   k_gather<<<(M + 255) / 256, 256, 0, st>>>((const zc*)d_x, xi, c->d_perm, M, 1);

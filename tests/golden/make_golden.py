@@ -87,7 +87,9 @@ def quadrature(ref):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <path of the SpeckleSim source tree>")
+    ref = sys.argv[1]
     with open(os.path.join(HERE, "hankel2_x2.json"), "w") as f:
         json.dump(hankel(ref), f, indent=1)
     with open(os.path.join(HERE, "hankel2_x2p2i.json"), "w") as f:
