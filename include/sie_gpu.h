@@ -97,6 +97,21 @@ const char* sie_version(void);
 int sie_init(const sie_config* cfg, const double* verts, int nv, const int* tris, int nt,
              sie_ctx** out);
 
+/* Truncation number of every MLFMM level, truncation_number(l)%n of the reference
+ * (Truncation_number_calculation, src/lib_sie_mlfmm.f90:631-701, which sets
+ * truncation_number_default on every level and leaves its per-level rule commented
+ * out).  K[l] for levels l = 0 .. n-1 (0: cfg->truncation_number); call between sie_init
+ * and sie_setup.  K must not grow from a level to its children.  Where a child level's K
+ * is smaller than its parent's, SS interpolates the child's coefficients to the parent's
+ * sampling (Lagrange_Interpolation_New, src/lib_sie_mlfmm.f90:268-390, 6 x 6 stencil, the
+ * reference's dormant branch at src/lib_sie_tri_mlfmm_interface.f90:486-507) and RR
+ * returns by its transpose.  Three departures from that dormant branch, each needed for
+ * a correct product: SR weights every level by its own quadrature; RR anterpolates (the
+ * reference interpolates, :638-640); the receive takes khat x f at the -z pole in the
+ * pole's Cartesian components.  sie_num_directions then gives the leaf level's Q.  The
+ * transposed product and sie_grad refuse such contexts (SIE_ERR_STATE). */
+int sie_set_level_truncation(sie_ctx* ctx, const int* K, int n);
+
 /* Number of RWG edges M (m_pairs) and the MLFMM levels of the tree. */
 int sie_info(const sie_ctx* ctx, int* n_edges, int* l_min, int* l_max, long long* near_nnz);
 
@@ -188,9 +203,47 @@ int sie_solve_device(sie_ctx* ctx, const double* d_b, double* d_x, int nrhs,
  * LU factors are made on the first call and kept for later right-hand sides. */
 int sie_solve_direct(sie_ctx* ctx, const double* b, double* x, int nrhs);
 
+/* Mixed-precision direct solve of the dense system (context set up with dense = 1): LU
+ * with partial pivoting of the complex64 matrix whose trailing updates run on the tensor
+ * cores as 3xTF32 products (FP32-accurate), then iterative refinement in FP64,
+ * x += U^-1 L^-1 P (b - Z x) with the FP64 dense product, until ||b - Z x|| <= tolerance
+ * ||b|| or max_refinements corrections.  The factors are made on the first call and kept.
+ * Same role as sie_solve_direct (ZGESV of the reference's normal solver,
+ * src/lib_sie_tri_solver_normal.f90:64-217); the refinement converges while cond(Z)
+ * times the FP32 rounding stays below one.  stats (may be NULL): per right-hand side,
+ * iterations = refinement steps, backward_error_true = ||b - Z x|| / ||b|| in FP64,
+ * seconds = wall time (the first includes the factorisation).  SIE_ERR_NOCONV if the
+ * tolerance is not met. */
+int sie_solve_direct_mixed(sie_ctx* ctx, const double* b, double* x, int nrhs, double tolerance,
+                           int max_refinements, sie_stats* stats);
+/* Same on device buffers; the work runs on stream (NULL: the context's stream) and the
+ * call returns when the solutions are in d_x. */
+int sie_solve_direct_mixed_device(sie_ctx* ctx, const double* d_b, double* d_x, int nrhs, double tolerance,
+                                  int max_refinements, sie_stats* stats, void* stream);
+/* Frees the LU factors that sie_solve_direct and sie_solve_direct_mixed keep, so that the
+ * next direct solve factorises again (e.g. after the caller changed nothing but wants the
+ * memory back).  No counterpart in the reference, which factorises in every run. */
+int sie_release_factors(sie_ctx* ctx);
+
 /* Left Jacobi preconditioner, lib_sie_ml_fmm_preconditioner_left
  * (src/lib_sie_tri_mlfmm_interface.f90:323-339): v2 = v1 / diag. */
 int sie_precondition_left(sie_ctx* ctx, const double* v1, double* v2);
+
+#define SIE_PRECOND_NONE 0 /* no preconditioner (the reference default, main.f90:232) */
+#define SIE_PRECOND_NEAR 1 /* near-field restricted additive Schwarz, applied on the right */
+
+/* Preconditioner of every later sie_solve on ctx.  No counterpart in the reference,
+ * whose only option is the left Jacobi scaling of sie_precondition_left (off by
+ * default).  SIE_PRECOND_NEAR builds, from the near matrix alone, one local system per
+ * leaf box A over A and its neighbour boxes (the near panel's columns), factorises it
+ * and keeps the rows of its inverse that belong to A's unknowns: an operator with the
+ * near matrix's sparsity, 64 bytes per 2x2 block (complex64 copy for the mixed solver
+ * made on first use).  The solvers apply it on the right (Z P u = b, x = P u), so the
+ * reported residuals are those of Z x = b.  Set-up costs one LU per leaf box of twice
+ * the box's E2 edge count.  Not for dense contexts.  SIE_PRECOND_NONE frees it. */
+int sie_set_preconditioner(sie_ctx* ctx, int kind);
+/* v2 = P v1 with the preconditioner of sie_set_preconditioner (host vectors). */
+int sie_precondition_right(sie_ctx* ctx, const double* v1, double* v2);
 
 /* Scattered E and H at observation points (Integration_scattered_field_tri,
  * src/lib_sie_tri_calculation_mod.f90:2782-2825) and the 'rcs' intensity
@@ -216,7 +269,9 @@ int sie_num_directions(const sie_ctx* ctx, int* Q);
 /* Device-side timings of the last sie_setup / sie_matvec phases [ms]:
  * fill, RT+TL, set-up, matvec total, near, aggregate, SS, SR, RR, receive; then
  * out[10] = mean Gram-Schmidt passes per Arnoldi step of the last solve; out[11] = inner
- * cycles of the last batched mixed solve replayed from their captured CUDA graph. */
+ * cycles of the last batched mixed solve replayed from their captured CUDA graph;
+ * out[12] = set-up of the near-field preconditioner (host wall time); out[13] = the
+ * complex64 tensor-core LU of sie_solve_direct_mixed (host wall time). */
 int sie_get_timings(const sie_ctx* ctx, double* out, int n);
 
 /* Launch all further work of ctx on the caller's CUDA stream (NULL: back to the

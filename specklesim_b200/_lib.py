@@ -26,6 +26,8 @@ SIE_PMCHWT = 1
 SIE_ICTF = 3
 SIE_FP64 = 0
 SIE_MIXED = 1
+SIE_PRECOND_NONE = 0
+SIE_PRECOND_NEAR = 1
 
 ERR_NAMES = {
     1: "SIE_ERR_ARG", 2: "SIE_ERR_CUDA", 3: "SIE_ERR_STATE", 4: "SIE_ERR_NOMEM",
@@ -77,6 +79,8 @@ EXPORTS = [
     "sie_num_directions", "sie_get_timings", "sie_set_stream", "sie_launch_count", "sie_free",
     "sie_farfield_device_noalloc", "sie_solve_direct", "sie_matvec_adjoint", "sie_matvec_adjoint_device",
     "sie_grad", "sie_set_inner_operator", "sie_autotune", "sie_quadrature_rule",
+    "sie_set_preconditioner", "sie_precondition_right", "sie_set_level_truncation",
+    "sie_solve_direct_mixed", "sie_solve_direct_mixed_device", "sie_release_factors",
 ]
 
 _lib = None
@@ -111,6 +115,9 @@ def load(path=None):
         "sie_solve": (C.c_int, [vp, dp, dp, C.c_int, C.POINTER(SieSolverCfg), C.POINTER(SieStats)]),
         "sie_solve_device": (C.c_int, [vp, vp, vp, C.c_int, C.POINTER(SieSolverCfg), C.POINTER(SieStats)]),
         "sie_precondition_left": (C.c_int, [vp, dp, dp]),
+        "sie_set_preconditioner": (C.c_int, [vp, C.c_int]),
+        "sie_set_level_truncation": (C.c_int, [vp, ip, C.c_int]),
+        "sie_precondition_right": (C.c_int, [vp, dp, dp]),
         "sie_farfield": (C.c_int, [vp, dp, dp, C.c_int, dp, dp, dp]),
         "sie_get_edges": (C.c_int, [vp, ip, ip]),
         "sie_get_tree": (C.c_int, [vp, dp, lp]),
@@ -124,6 +131,10 @@ def load(path=None):
         "sie_free": (C.c_int, [vp]),
         "sie_farfield_device_noalloc": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, vp, vp]),
         "sie_solve_direct": (C.c_int, [vp, dp, dp, C.c_int]),
+        "sie_solve_direct_mixed": (C.c_int, [vp, dp, dp, C.c_int, C.c_double, C.c_int, C.POINTER(SieStats)]),
+        "sie_solve_direct_mixed_device": (C.c_int, [vp, vp, vp, C.c_int, C.c_double, C.c_int,
+                                                    C.POINTER(SieStats), vp]),
+        "sie_release_factors": (C.c_int, [vp]),
         "sie_matvec_adjoint": (C.c_int, [vp, dp, dp, C.c_int]),
         "sie_set_inner_operator": (C.c_int, [vp, vp]),
         "sie_autotune": (C.c_int, [vp, C.c_int, dp, ip]),

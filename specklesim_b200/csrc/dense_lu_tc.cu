@@ -1,0 +1,586 @@
+// Mixed-precision direct solve of the dense system: LU with partial pivoting of the
+// complex64 matrix, its O(N^3) trailing updates on the tensor cores (tc_gemm.cu, 3xTF32,
+// FP32-accurate), then iterative refinement in FP64 against the FP64 dense product.
+//
+// The reference's direct path (lib_sie_tri_solver_normal_I,
+// src/lib_sie_tri_solver_normal.f90:64-217, with ZGESV in solver_LU,
+// src/lib_sie_math.f90:649-676) factorises the FP64 matrix; sie_solve_direct does the
+// same with cuSOLVER.  Here the factorisation runs in FP32 arithmetic and the solution is
+// refined in FP64 (x += U^-1 L^-1 P (b - Z x)) until the true backward error meets the
+// tolerance, which it does while cond(Z) times the factorisation's rounding stays below
+// one.
+//
+// Blocked right-looking LU, panel width NB = 128, on the matrix stored as two FP32
+// planes (real, imaginary), column-major, internal unknown order:
+//   1. panel: for each of its columns, a pivot search (one block), the row swap inside
+//      the panel, then the scaling of the column and the rank-1 update of the panel's
+//      remaining columns (one thread per row);
+//   2. the panel's row swaps applied to every column left and right of it;
+//   3. U12 = L11^-1 A12, a warp per column with L11 in shared memory;
+//   4. A22 -= L21 U12 on the tensor cores.
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "sie_internal.h"
+#include "tc_gemm.cuh"
+
+namespace sie {
+namespace tc {
+int tile_operand(const float* sr, const float* si, size_t ld, int rows, int K, bool trans, char* out,
+                 cudaStream_t st);
+int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, size_t ldc, int m, int n,
+                int* d_err, cudaStream_t st);
+size_t tiled_bytes_host(int rows, int K);
+}  // namespace tc
+
+static const int LU_NB = 128;
+
+// Dense panels (cfg.dense = 1) -> FP32 planes of Z in the internal interleaved order
+// (unknown 2m + a of edge m), column-major.
+__global__ void k_expand_dense32(const long long* base, const int* box_first, const int* box_cnt,
+                                 const int* ncols, int nbox, const zc* va, const zc* vb, const zc* vd, zc cfac,
+                                 int M, float* Zr, float* Zi) {
+  const long long ld = 2LL * M;
+  for (int A = blockIdx.y; A < nbox; A += gridDim.y) {
+    const int nr = box_cnt[A], nc = ncols[A], f = box_first[A];
+    const long long tot = (long long)nr * nc;
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < tot;
+         k += (long long)gridDim.x * blockDim.x) {
+      const int r = (int)(k / nc), j = (int)(k % nc);
+      const long long o = base[A] + k;
+      const long long m = f + r, n = j;
+      const zc a = va[o], b = vb[o], d = vd[o], c = cfac * b;
+      const long long p00 = (2 * n) * ld + 2 * m, p01 = (2 * n + 1) * ld + 2 * m;
+      Zr[p00] = (float)a.re;
+      Zi[p00] = (float)a.im;
+      Zr[p01] = (float)b.re;
+      Zi[p01] = (float)b.im;
+      Zr[p00 + 1] = (float)c.re;
+      Zi[p00 + 1] = (float)c.im;
+      Zr[p01 + 1] = (float)d.re;
+      Zi[p01 + 1] = (float)d.im;
+    }
+  }
+}
+
+// Pivot of column j (rows j .. n-1): the row of largest |a|, first on ties; swaps rows j
+// and p over the panel's columns [c0, c1) and records p.  One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_pivot(float* Ar, float* Ai, size_t ld, int n, int j, int c0, int c1,
+                                                int* ipiv, int* err) {
+  __shared__ float sv[32];
+  __shared__ int si[32];
+  const float* cr = Ar + (size_t)j * ld;
+  const float* ci = Ai + (size_t)j * ld;
+  float best = -1.f;
+  int bi = j;
+  for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+    const float v = cr[i] * cr[i] + ci[i] * ci[i];
+    if (v > best) {
+      best = v;
+      bi = i;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > best || (ov == best && oi < bi)) {
+      best = ov;
+      bi = oi;
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sv[w] = best;
+    si[w] = bi;
+  }
+  __syncthreads();
+  if (w == 0) {
+    best = l < (int)(blockDim.x >> 5) ? sv[l] : -1.f;
+    bi = l < (int)(blockDim.x >> 5) ? si[l] : n;
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (l == 0) {
+      si[0] = bi;
+      sv[0] = best;
+      ipiv[j] = bi;
+      if (!(best > 0.f) || !isfinite(best)) atomicOr(err, 8);  // singular or non-finite column
+    }
+  }
+  __syncthreads();
+  const int p = si[0];
+  if (p != j)
+    for (int c = c0 + (int)threadIdx.x; c < c1; c += blockDim.x) {
+      const size_t a = (size_t)c * ld + j, b = (size_t)c * ld + p;
+      float t = Ar[a];
+      Ar[a] = Ar[b];
+      Ar[b] = t;
+      t = Ai[a];
+      Ai[a] = Ai[b];
+      Ai[b] = t;
+    }
+}
+
+// Column j of the panel [j .. c1): l_i = a_ij / a_jj (i > j), then a_ik -= l_i a_jk for
+// the panel's later columns k.  Thread per row i.
+__global__ void __launch_bounds__(256) k_panel_update(float* Ar, float* Ai, size_t ld, int n, int j, int c1) {
+  __shared__ float ur[LU_NB], ui[LU_NB];
+  const int w = c1 - j - 1;  // later columns of the panel
+  for (int k = threadIdx.x; k < w; k += blockDim.x) {
+    ur[k] = Ar[(size_t)(j + 1 + k) * ld + j];
+    ui[k] = Ai[(size_t)(j + 1 + k) * ld + j];
+  }
+  __syncthreads();
+  const int i = j + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float pr = Ar[(size_t)j * ld + j], pi = Ai[(size_t)j * ld + j];
+  const float den = pr * pr + pi * pi;
+  const float ar = Ar[(size_t)j * ld + i], ai = Ai[(size_t)j * ld + i];
+  const float lr = (ar * pr + ai * pi) / den, li = (ai * pr - ar * pi) / den;
+  Ar[(size_t)j * ld + i] = lr;
+  Ai[(size_t)j * ld + i] = li;
+  for (int k = 0; k < w; k++) {
+    const size_t o = (size_t)(j + 1 + k) * ld + i;
+    Ar[o] -= lr * ur[k] - li * ui[k];
+    Ai[o] -= lr * ui[k] + li * ur[k];
+  }
+}
+
+// Row swaps ipiv[k0 .. k1) applied in order to the columns [c, c + 1) of every thread
+// outside the panel [k0, k1).
+__global__ void k_laswp(float* Ar, float* Ai, size_t ld, int n, int k0, int k1, const int* ipiv) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int outside = n - (k1 - k0);
+  if (c >= outside) return;
+  if (c >= k0) c += k1 - k0;
+  float* cr = Ar + (size_t)c * ld;
+  float* ci = Ai + (size_t)c * ld;
+  for (int j = k0; j < k1; j++) {
+    const int p = ipiv[j];
+    if (p != j) {
+      float t = cr[j];
+      cr[j] = cr[p];
+      cr[p] = t;
+      t = ci[j];
+      ci[j] = ci[p];
+      ci[p] = t;
+    }
+  }
+}
+
+// U12 = L11^-1 A12 in place: L11 the unit lower triangle of the nb x nb diagonal block at
+// (k0, k0), A12 its rows [k0, k0 + nb) in columns [c0, n).  L11 in shared memory; one warp
+// per column, lane l holding rows l, l + 32, l + 64, l + 96.
+__global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld, int n, int k0, int nb, int c0) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* Lr = reinterpret_cast<float*>(smraw);  // [col][row], nb x nb
+  float* Li = Lr + LU_NB * LU_NB;
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int col = e / nb, row = e - col * nb;
+    Lr[col * LU_NB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
+    Li[col * LU_NB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = c0 + blockIdx.x * 8 + warp; c < n; c += gridDim.x * 8) {
+    float* cr = Ar + (size_t)c * ld + k0;
+    float* ci = Ai + (size_t)c * ld + k0;
+    float xr[4], xi[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = lane + 32 * q;
+      xr[q] = r < nb ? cr[r] : 0.f;
+      xi[q] = r < nb ? ci[r] : 0.f;
+    }
+    for (int i = 0; i < nb; i++) {
+      const int q0 = i >> 5;
+      float vr = 0.f, vi = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (q == q0) {
+          vr = __shfl_sync(0xffffffffu, xr[q], i & 31);
+          vi = __shfl_sync(0xffffffffu, xi[q], i & 31);
+        }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = lane + 32 * q;
+        if (r > i && r < nb) {
+          const float lr = Lr[i * LU_NB + r], li = Li[i * LU_NB + r];
+          xr[q] -= lr * vr - li * vi;
+          xi[q] -= lr * vi + li * vr;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = lane + 32 * q;
+      if (r < nb) {
+        cr[r] = xr[q];
+        ci[r] = xi[q];
+      }
+    }
+  }
+}
+
+// Solves with the factors, one vector (complex64, internal order) in place.
+// Forward: x[k0 .. k1) = L11^-1 x[k0 .. k1) (one block), then x[k1 ..) -= L21 x[k0 .. k1).
+__global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
+                                                    int lower, cc* x) {
+  __shared__ float br[LU_NB], bi[LU_NB];
+  for (int r = threadIdx.x; r < nb; r += blockDim.x) {
+    br[r] = x[k0 + r].re;
+    bi[r] = x[k0 + r].im;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    if (lower) {
+      for (int i = 0; i < nb; i++) {
+        const float vr = br[i], vi = bi[i];
+        __syncwarp();
+        for (int r = i + 1 + lane; r < nb; r += 32) {
+          const float lr = Ar[(size_t)(k0 + i) * ld + k0 + r], li = Ai[(size_t)(k0 + i) * ld + k0 + r];
+          br[r] -= lr * vr - li * vi;
+          bi[r] -= lr * vi + li * vr;
+        }
+        __syncwarp();
+      }
+    } else {
+      for (int i = nb - 1; i >= 0; i--) {
+        if (lane == 0) {
+          const float ur = Ar[(size_t)(k0 + i) * ld + k0 + i], ui = Ai[(size_t)(k0 + i) * ld + k0 + i];
+          const float den = ur * ur + ui * ui;
+          const float xr = (br[i] * ur + bi[i] * ui) / den, xi = (bi[i] * ur - br[i] * ui) / den;
+          br[i] = xr;
+          bi[i] = xi;
+        }
+        __syncwarp();
+        const float vr = br[i], vi = bi[i];
+        for (int r = lane; r < i; r += 32) {
+          const float ur = Ar[(size_t)(k0 + i) * ld + k0 + r], ui = Ai[(size_t)(k0 + i) * ld + k0 + r];
+          br[r] -= ur * vr - ui * vi;
+          bi[r] -= ur * vi + ui * vr;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < nb; r += blockDim.x) x[k0 + r] = mk<float>(br[r], bi[r]);
+}
+
+// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb); thread per row.
+__global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
+                                                   int r0, int r1, cc* x) {
+  __shared__ float br[LU_NB], bi[LU_NB];
+  for (int r = threadIdx.x; r < nb; r += blockDim.x) {
+    br[r] = x[k0 + r].re;
+    bi[r] = x[k0 + r].im;
+  }
+  __syncthreads();
+  const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r1) return;
+  float sr = 0.f, si = 0.f;
+  for (int j = 0; j < nb; j++) {
+    const float ar = Ar[(size_t)(k0 + j) * ld + i], ai = Ai[(size_t)(k0 + j) * ld + i];
+    sr += ar * br[j] - ai * bi[j];
+    si += ar * bi[j] + ai * br[j];
+  }
+  x[i].re -= sr;
+  x[i].im -= si;
+}
+
+__global__ void k_apply_pivots(const int* ipiv, int n, cc* x) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int j = 0; j < n; j++) {
+    const int p = ipiv[j];
+    if (p != j) {
+      const cc t = x[j];
+      x[j] = x[p];
+      x[p] = t;
+    }
+  }
+}
+
+__global__ void k_scale_to32(const zc* a, cc* b, int n, double s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = mk<float>((float)(a[i].re * s), (float)(a[i].im * s));
+}
+__global__ void k_add_from32(zc* x, const cc* d, int n, double s) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i].re += (double)d[i].re * s;
+    x[i].im += (double)d[i].im * s;
+  }
+}
+__global__ void k_resid(const zc* b, const zc* ax, zc* r, int n, double* nrm2) {
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const zc v = b[i] - ax[i];
+    r[i] = v;
+    acc += cabs2(v);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(nrm2, acc);
+}
+
+}  // namespace sie
+
+using namespace sie;
+
+// State of the complex64 factorisation, kept in the context between solves.
+struct LuTc {
+  float* Ar = nullptr;
+  float* Ai = nullptr;
+  int* ipiv = nullptr;
+  int n = 0;
+  double factor_s = 0;
+};
+
+static int lu_tc_factor(sie_ctx* c) {
+  if (c->d_lu32) return SIE_OK;
+  const int n = 2 * c->M;
+  const size_t ld = (size_t)n;
+  cudaStream_t s = c->stream;
+  float *Ar = nullptr, *Ai = nullptr;
+  int *ipiv = nullptr, *err = nullptr;
+  char *At = nullptr, *Bt = nullptr;
+  int rc = SIE_OK;
+  auto cleanup = [&]() {
+    if (At) cudaFree(At);
+    if (Bt) cudaFree(Bt);
+    if (err) cudaFree(err);
+  };
+  SIE_CUDA(cudaMalloc(&Ar, ld * n * sizeof(float)));
+  if (cudaMalloc(&Ai, ld * n * sizeof(float)) != cudaSuccess || cudaMalloc(&ipiv, (size_t)n * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&At, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess ||
+      cudaMalloc(&Bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) {
+    cudaFree(Ar);
+    if (Ai) cudaFree(Ai);
+    if (ipiv) cudaFree(ipiv);
+    cleanup();
+    return fail(SIE_ERR_NOMEM, "mixed LU: device memory");
+  }
+  c->d_lu32 = Ar;
+  c->d_lu32i = Ai;
+  c->d_piv32 = ipiv;
+  auto t0 = std::chrono::steady_clock::now();
+  cudaMemsetAsync(err, 0, sizeof(int), s);
+  {
+    dim3 g(64, std::min(c->near.nbox, 1024));
+    k_expand_dense32<<<g, 256, 0, s>>>(c->d_base, c->d_box_first, c->d_box_cnt, c->d_ncols, c->near.nbox, c->d_na,
+                                       c->d_nb, c->d_nd, c->cfac, c->M, Ar, Ai);
+    count_launch();
+  }
+  const size_t trsm_smem = (size_t)2 * LU_NB * LU_NB * sizeof(float);
+  if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
+  for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += LU_NB) {
+    const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
+    for (int j = k0; j < k1; j++) {
+      k_pivot<<<1, 1024, 0, s>>>(Ar, Ai, ld, n, j, k0, k1, ipiv, err);
+      count_launch();
+      if (j + 1 < n) {
+        k_panel_update<<<(n - j - 1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, n, j, k1);
+        count_launch();
+      }
+    }
+    if (n - nb > 0) {
+      k_laswp<<<(n - nb + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, n, k0, k1, ipiv);
+      count_launch();
+    }
+    if (k1 < n) {
+      k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, s>>>(Ar, Ai, ld, n, k0, nb, k1);
+      count_launch();
+      const int m = n - k1;
+      // A22 -= L21 U12 on the tensor cores
+      rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, s);
+      if (rc == SIE_OK) rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, s);
+      if (rc == SIE_OK)
+        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k1, Ai + (size_t)k1 * ld + k1, ld, m, m, err, s);
+    }
+    if (cudaGetLastError() != cudaSuccess && rc == SIE_OK) rc = fail(SIE_ERR_CUDA, "mixed LU: launch");
+  }
+  int herr = 0;
+  if (rc == SIE_OK && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                       cudaStreamSynchronize(s) != cudaSuccess))
+    rc = fail(SIE_ERR_CUDA, "mixed LU: factorisation");
+  if (rc == SIE_OK && (herr & 8)) rc = fail(SIE_ERR_NONFINITE, "mixed LU: singular or non-finite pivot");
+  if (rc == SIE_OK && herr) rc = fail(SIE_ERR_CUDA, "mixed LU: a tensor-core pipeline wait timed out");
+  c->tm.lu_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  cleanup();
+  if (rc != SIE_OK) {
+    cudaFree(c->d_lu32);
+    cudaFree(c->d_lu32i);
+    cudaFree(c->d_piv32);
+    c->d_lu32 = c->d_lu32i = nullptr;
+    c->d_piv32 = nullptr;
+  }
+  return rc;
+}
+
+// x = U^-1 L^-1 P x with the complex64 factors (internal order, in place).
+static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
+  const int n = 2 * c->M;
+  const size_t ld = (size_t)n;
+  const float *Ar = c->d_lu32, *Ai = c->d_lu32i;
+  k_apply_pivots<<<1, 1, 0, s>>>(c->d_piv32, n, x);
+  count_launch();
+  for (int k0 = 0; k0 < n; k0 += LU_NB) {
+    const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
+    k_trsv_block<<<1, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 1, x);
+    count_launch();
+    if (k1 < n) {
+      k_trsv_gemv<<<(n - k1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
+      count_launch();
+    }
+  }
+  for (int k0 = ((n - 1) / LU_NB) * LU_NB; k0 >= 0; k0 -= LU_NB) {
+    const int nb = std::min(LU_NB, n - k0);
+    k_trsv_block<<<1, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, x);
+    count_launch();
+    if (k0 > 0) {
+      k_trsv_gemv<<<(k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
+      count_launch();
+    }
+  }
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+// One or more right-hand sides on device buffers (external order, stride 2M).
+static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, double tolerance,
+                                  int max_refinements, sie_stats* stats, cudaStream_t s) {
+  auto t0 = std::chrono::steady_clock::now();
+  SIE_TRY(lu_tc_factor(c));
+  const int n = 2 * c->M;
+  const size_t bytes = (size_t)n * sizeof(zc);
+  zc *bi = nullptr, *xi = nullptr, *ax = nullptr, *r = nullptr;
+  cc* d32 = nullptr;
+  double* nrm = nullptr;
+  int rc = SIE_OK;
+  if (cudaMalloc(&bi, bytes) != cudaSuccess || cudaMalloc(&xi, bytes) != cudaSuccess ||
+      cudaMalloc(&ax, bytes) != cudaSuccess || cudaMalloc(&r, bytes) != cudaSuccess ||
+      cudaMalloc(&d32, (size_t)n * sizeof(cc)) != cudaSuccess || cudaMalloc(&nrm, sizeof(double)) != cudaSuccess)
+    rc = fail(SIE_ERR_NOMEM, "mixed direct solve: device buffers");
+  for (int k = 0; k < nrhs && rc == SIE_OK; k++) {
+    auto tk = std::chrono::steady_clock::now();
+    const size_t off = (size_t)k * n;
+    double bn2 = 0, rn2 = 0;
+    int steps = 0;
+    rc = gather_ext_to_int(c, d_b + off, bi, 1, s);
+    cudaMemsetAsync(xi, 0, bytes, s);
+    // r = b - Z x in FP64 (x = 0 at the start), then d = LU^-1 r in complex64 (r scaled to
+    // unit norm) and x += d, until ||r|| <= tolerance ||b||
+    for (; rc == SIE_OK; steps++) {
+      if (steps == 0) {
+        cudaMemsetAsync(ax, 0, bytes, s);
+      } else {
+        rc = near_matvec64(c, xi, ax, 1, false, s);
+        if (rc != SIE_OK) break;
+      }
+      cudaMemsetAsync(nrm, 0, sizeof(double), s);
+      k_resid<<<296, 256, 0, s>>>(bi, ax, r, n, nrm);
+      count_launch();
+      if (cudaMemcpyAsync(&rn2, nrm, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        rc = fail(SIE_ERR_CUDA, "mixed direct solve: residual");
+        break;
+      }
+      if (steps == 0) bn2 = rn2;
+      if (!std::isfinite(rn2)) {
+        rc = fail(SIE_ERR_NONFINITE, "mixed direct solve: non-finite residual");
+        break;
+      }
+      if (bn2 == 0.0 || rn2 <= tolerance * tolerance * bn2 || steps > max_refinements) break;
+      const double rn = std::sqrt(rn2);
+      k_scale_to32<<<296, 256, 0, s>>>(r, d32, n, 1.0 / rn);
+      count_launch();
+      rc = lu_tc_solve32(c, d32, s);
+      if (rc != SIE_OK) break;
+      k_add_from32<<<296, 256, 0, s>>>(xi, d32, n, rn);
+      count_launch();
+    }
+    if (rc != SIE_OK) break;
+    rc = scatter_int_to_ext(c, xi, d_x + off, 1, s);
+    if (rc == SIE_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed direct solve");
+    const double be = bn2 > 0 ? std::sqrt(rn2 / bn2) : 0.0;
+    const bool conv = be <= tolerance;
+    if (stats) {
+      stats[k].iterations = steps;
+      stats[k].inner_iterations = 0;
+      stats[k].matvecs = steps;
+      stats[k].converged = conv;
+      stats[k].backward_error_arnoldi = be;
+      stats[k].backward_error_true = be;
+      stats[k].seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - (k == 0 ? t0 : tk)).count();
+    }
+    if (rc == SIE_OK && !conv) rc = fail(SIE_ERR_NOCONV, "mixed direct solve: refinement did not reach the tolerance");
+  }
+  for (void* p : {(void*)bi, (void*)xi, (void*)ax, (void*)r, (void*)d32, (void*)nrm})
+    if (p) cudaFree(p);
+  return rc;
+}
+
+static int check_direct_mixed(sie_ctx* c, int nrhs, double tolerance, int max_refinements, const char* who) {
+  if (!c || nrhs < 1 || !(tolerance > 0) || max_refinements < 0)
+    return fail(SIE_ERR_ARG, std::string(who) + ": bad argument");
+  if (!c->setup_done) return fail(SIE_ERR_STATE, std::string(who) + ": sie_setup not called");
+  if (!c->cfg.dense) return fail(SIE_ERR_STATE, std::string(who) + ": needs a context set up with dense = 1");
+  return SIE_OK;
+}
+
+extern "C" int sie_solve_direct_mixed_device(sie_ctx* c, const double* d_b, double* d_x, int nrhs,
+                                             double tolerance, int max_refinements, sie_stats* stats,
+                                             void* stream) {
+  SIE_TRY(check_direct_mixed(c, nrhs, tolerance, max_refinements, "sie_solve_direct_mixed_device"));
+  if (!d_b || !d_x) return fail(SIE_ERR_ARG, "sie_solve_direct_mixed_device: null buffer");
+  SIE_CUDA(cudaSetDevice(c->device));
+  return solve_direct_mixed_dev(c, (const zc*)d_b, (zc*)d_x, nrhs, tolerance, max_refinements, stats,
+                                stream ? (cudaStream_t)stream : c->stream);
+}
+
+extern "C" int sie_solve_direct_mixed(sie_ctx* c, const double* b, double* x, int nrhs, double tolerance,
+                                      int max_refinements, sie_stats* stats) {
+  SIE_TRY(check_direct_mixed(c, nrhs, tolerance, max_refinements, "sie_solve_direct_mixed"));
+  if (!b || !x) return fail(SIE_ERR_ARG, "sie_solve_direct_mixed: null buffer");
+  SIE_CUDA(cudaSetDevice(c->device));
+  for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
+    if (!std::isfinite(b[i])) return fail(SIE_ERR_NONFINITE, "sie_solve_direct_mixed: non-finite right-hand side");
+  const size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
+  zc *db = nullptr, *dx = nullptr;
+  SIE_CUDA(cudaMalloc(&db, bytes));
+  if (cudaMalloc(&dx, bytes) != cudaSuccess) {
+    cudaFree(db);
+    return fail(SIE_ERR_NOMEM, "sie_solve_direct_mixed: device buffers");
+  }
+  int rc = SIE_OK;
+  if (cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    rc = fail(SIE_ERR_CUDA, "sie_solve_direct_mixed: copy");
+  if (rc == SIE_OK) rc = solve_direct_mixed_dev(c, db, dx, nrhs, tolerance, max_refinements, stats, c->stream);
+  if ((rc == SIE_OK || rc == SIE_ERR_NOCONV) &&
+      (cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+       cudaStreamSynchronize(c->stream) != cudaSuccess))
+    rc = fail(SIE_ERR_CUDA, "sie_solve_direct_mixed: copy back");
+  cudaFree(db);
+  cudaFree(dx);
+  return rc;
+}
+
+extern "C" int sie_release_factors(sie_ctx* c) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_release_factors: null context");
+  SIE_CUDA(cudaSetDevice(c->device));
+  if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
+  for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32})
+    if (p) cudaFree(p);
+  c->d_lu = nullptr;
+  c->d_piv = nullptr;
+  c->d_lu32 = c->d_lu32i = nullptr;
+  c->d_piv32 = nullptr;
+  return SIE_OK;
+}

@@ -170,6 +170,11 @@ __global__ void k_sub(const zc* a, const zc* b, zc* c, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     c[i] = a[i] - b[i];
 }
+// c = a + b
+__global__ void k_add(const zc* a, const zc* b, zc* c, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    c[i] = a[i] + b[i];
+}
 // y = a + V(:, 0:k) coef (coef on the device)
 __global__ void k_combine(const zc* a, const zc* V, const zc* coef, int k, int n, size_t ld, zc* y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -857,6 +862,25 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
     matvecs++;
     return sie_internal_matvec(c, in, out, 1, s, false);
   };
+  // With the near-field preconditioner the Arnoldi process runs on Z P (right
+  // preconditioning): its residual is the true one, and the iterate is x + P V y.
+  const bool pre = c->precond == SIE_PRECOND_NEAR;
+  auto op = [&](const zc* in, zc* out) -> int {
+    if (!pre) return matvec(in, out);
+    SIE_TRY(ras_apply64(c, in, g.r0, s));
+    return matvec(g.r0, out);
+  };
+  // out = x + (P) V(:, 0:k) y; uses g.r0 and g.w as scratch when preconditioned
+  auto update = [&](int k, zc* out) -> int {
+    if (!pre) {
+      k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, k, n, ld, out); sie::count_launch();
+      return SIE_OK;
+    }
+    k_combine<<<RB, RT_, 0, s>>>(nullptr, g.V, g.y, k, n, ld, g.r0); sie::count_launch();
+    SIE_TRY(ras_apply64(c, g.r0, g.w, s));
+    k_add<<<RB, RT_, 0, s>>>(x, g.w, out, n); sie::count_launch();
+    return SIE_OK;
+  };
   auto finish = [&](int code, int iters, double bea, double be, int conv) {
     scatter_int_to_ext(c, x, d_x_ext, 1, s);
     cudaEventRecord(c->ev[13], s);
@@ -924,7 +948,10 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
       compRsd = 1;
       // xCurrent = x + V y
       k_trsv<<<1, 1, 0, s>>>(g.H, m, p + 1, g.y); sie::count_launch();
-      k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, p + 1, n, ld, g.xc); sie::count_launch();
+      {
+        int ru = update(p + 1, g.xc);
+        if (ru != SIE_OK) return -ru;
+      }
       // true residual
       int rr = matvec(g.xc, g.w);
       if (rr != SIE_OK) return -rr;
@@ -947,7 +974,7 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
     int pending = -1;
     for (int jH = 0; jH < m; jH++) {
       // w = A V_jH, then the fused orthogonalisation / Givens step
-      SIE_TRY(matvec(g.V + (size_t)jH * ld, g.w));
+      SIE_TRY(op(g.V + (size_t)jH * ld, g.w));
       SIE_TRY(arnoldi(jH));
       SIE_TRY(post(jH));
       SIE_CUDA(cudaGetLastError());
@@ -977,7 +1004,7 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
     iterOut++;
     if (bea > cfg->tolerance) {
       k_trsv<<<1, 1, 0, s>>>(g.H, m, m, g.y); sie::count_launch();
-      k_combine<<<RB, RT_, 0, s>>>(x, g.V, g.y, m, n, ld, g.xc); sie::count_launch();
+      SIE_TRY(update(m, g.xc));
     }
     k_copy<<<RB, RT_, 0, s>>>(g.xc, x, n); sie::count_launch();
     if (compRsd == 1) {
@@ -1150,8 +1177,17 @@ static int inner_gmres32(sie_ctx* c, Gm32& g, const cc* r, cc* z, double tol, in
     return SIE_OK;
   };
   bool stop = false;
+  // with the near-field preconditioner the inner cycle runs on Z P and returns P (V y);
+  // r is no longer read once V(:, 0) holds it, so c->d_xi32 is the scratch vector
+  const bool pre = c->precond == SIE_PRECOND_NEAR;
+  cc* tmp = c->d_xi32;
   for (int j = 0; j < m && !stop; j++) {
-    SIE_TRY(sie_internal_matvec32(c->inner ? c->inner : c, g.V + (size_t)j * ld, g.w, s, false));
+    const cc* vj = g.V + (size_t)j * ld;
+    if (pre) {
+      SIE_TRY(ras_apply32(c, vj, tmp, s));
+      vj = tmp;
+    }
+    SIE_TRY(sie_internal_matvec32(c->inner ? c->inner : c, vj, g.w, s, false));
     mvs++;
     SIE_TRY(arnoldi_launch32(g, j, beta, s));
     SIE_CUDA(cudaMemcpyAsync(&slots[j & 1], g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
@@ -1160,7 +1196,12 @@ static int inner_gmres32(sie_ctx* c, Gm32& g, const cc* r, cc* z, double tol, in
     if (!stop && j == m - 1) SIE_TRY(check(j, stop));
   }
   k_trsv<<<1, 1, 0, s>>>(g.H, m, k, g.y); sie::count_launch();
-  k_combine_t<float><<<RB, RT_, 0, s>>>(g.V, ld, g.y, k, n, z); sie::count_launch();
+  if (pre) {
+    k_combine_t<float><<<RB, RT_, 0, s>>>(g.V, ld, g.y, k, n, tmp); sie::count_launch();
+    SIE_TRY(ras_apply32(c, tmp, z, s));
+  } else {
+    k_combine_t<float><<<RB, RT_, 0, s>>>(g.V, ld, g.y, k, n, z); sie::count_launch();
+  }
   SIE_CUDA(cudaGetLastError());
   its = k;
   return SIE_OK;
@@ -1172,6 +1213,7 @@ int fgmres_mixed(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solver_cf
     return fail(SIE_ERR_ARG, "mixed solve: bad inner solver settings");
   SIE_TRY(make_f32_tables(c));
   if (c->inner) SIE_TRY(make_f32_tables(c->inner));
+  SIE_TRY(ras_to_f32(c));
   int m = cfg->restart;
   Gm g;
   SIE_TRY(gm_alloc(c, m, g));
@@ -1610,13 +1652,22 @@ static int inner_batch32(sie_ctx* c, GmB& g, double tol) {
   k_bnorm<float><<<grid, RT_, 0, s>>>(g.r32, n, g.pA, g.ldp); sie::count_launch();
   k_binit<float, float><<<grid, RT_, 0, s>>>(g.r32, n, g.pA, g.ldp, g.V32, g.Hi, mi, g.sti, 1, nullptr);
   sie::count_launch();
+  // with the near-field preconditioner the cycle runs on Z P and returns P (V y); r32 is
+  // no longer read once V(:, 0) holds it, so it is the scratch batch
+  const bool pre = c->precond == SIE_PRECOND_NEAR;
   for (int j = 0; j < mi; j++) {
-    SIE_TRY(sie_internal_matvec_b32(c->inner ? c->inner : c, g.V32 + (size_t)j * g.ldj, g.w32, R, s));
+    const cc* vj = g.V32 + (size_t)j * g.ldj;
+    if (pre) {
+      SIE_TRY(ras_apply32(c, vj, g.r32, s, R));
+      vj = g.r32;
+    }
+    SIE_TRY(sie_internal_matvec_b32(c->inner ? c->inner : c, vj, g.w32, R, s));
     SIE_TRY(barnoldi<float>(g.V32, g.ldj, g.w32, n, R, j, g.pA, g.pB, g.ldp, g.Hi, mi, g.rci, g.rsi, g.sti, tol, s));
   }
   k_btrsv<<<R, 32, 0, s>>>(g.Hi, mi, g.sti, g.yi); sie::count_launch();
-  k_bcombine<float, float><<<grid, RT_, 0, s>>>(g.V32, g.ldj, g.yi, mi + 1, g.sti, n, g.z32, 0);
+  k_bcombine<float, float><<<grid, RT_, 0, s>>>(g.V32, g.ldj, g.yi, mi + 1, g.sti, n, pre ? g.r32 : g.z32, 0);
   sie::count_launch();
+  if (pre) SIE_TRY(ras_apply32(c, g.r32, g.z32, s, R));
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }
@@ -1688,6 +1739,7 @@ int fgmres_mixed_batch(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, int R, const 
     return fail(SIE_ERR_ARG, "batched solve: restarts must be 1..63");
   SIE_TRY(make_f32_tables(c));
   if (c->inner) SIE_TRY(make_f32_tables(c->inner));
+  SIE_TRY(ras_to_f32(c));
   GmB g;
   SIE_TRY(gmb_alloc(c, R, mi, mo, g));
   const int n = g.n;

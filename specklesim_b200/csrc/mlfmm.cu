@@ -862,7 +862,17 @@ __global__ void k_rr(const cx<T>* __restrict__ Dp, const int* parent, const int*
 struct RecvConst {
   zc kd[2], my_d[2], eps_d[2];
   zc s1f, s2f;  // ICTF scaling of the two outputs
+  // The receive rotates the pattern, f_rk = (-f_phi, f_theta) = khat x f.  At the -z pole
+  // (the last direction) the stored components are Cartesian (theta-hat = x, phi-hat =
+  // y), for which khat x f = (f_y, -f_x): the k terms change sign.  With one K on every
+  // level D is zero there (TRF is 0 at the poles) and the reference's formula is kept
+  // (pole_fix = 0); anterpolated D is not zero, and per-level truncation sets it.
+  int pole_fix;
 };
+// the k factor of direction q in the receive
+__device__ __forceinline__ zc recv_kd(const RecvConst& rc, int md, int q, int Q) {
+  return (rc.pole_fix && q == Q - 1) ? -rc.kd[md] : rc.kd[md];
+}
 
 template <typename T>
 __global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, const int* box_cnt,
@@ -885,6 +895,7 @@ __global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, co
       for (int k = 0; k < 4; k++) S[md][k] = mk<T>(0, 0);
 #pragma unroll 3
     for (int q = lane; q < Q; q += 32) {
+      const T sg = (rc.pole_fix && q == Q - 1) ? (T)-1 : (T)1;  // k terms at the -z pole
 #pragma unroll
       for (int md = 0; md < 2; md++) {
         cx<T> fa = r[(2 * md) * Q + q], fb = r[(2 * md + 1) * Q + q];
@@ -892,12 +903,12 @@ __global__ void k_receive(const cx<T>* __restrict__ rt, const int* box_first, co
         cx<T> dJp = sD[(4 + md) * Q + q], dMp = sD[(6 + md) * Q + q];
         S[md][0] = cfma(fa, dJt, S[md][0]);
         S[md][0] = cfma(fb, dJp, S[md][0]);
-        S[md][1] = cfma(fb, dJt, S[md][1]);
-        S[md][1] = cfma(-fa, dJp, S[md][1]);
+        S[md][1] = cfma(fb * sg, dJt, S[md][1]);
+        S[md][1] = cfma(-fa * sg, dJp, S[md][1]);
         S[md][2] = cfma(fa, dMt, S[md][2]);
         S[md][2] = cfma(fb, dMp, S[md][2]);
-        S[md][3] = cfma(fa, dMp, S[md][3]);
-        S[md][3] = cfma(-fb, dMt, S[md][3]);
+        S[md][3] = cfma(fa * sg, dMp, S[md][3]);
+        S[md][3] = cfma(-fb * sg, dMt, S[md][3]);
       }
     }
     for (int md = 0; md < 2; md++)
@@ -943,10 +954,11 @@ __global__ void __launch_bounds__(256, 2) k_receive_chunk(const cx<T>* __restric
     for (int md = 0; md < 2; md++) {
       zc dJt = cvt_z(Db[(0 + md) * Q + q]), dMt = cvt_z(Db[(2 + md) * Q + q]);
       zc dJp = cvt_z(Db[(4 + md) * Q + q]), dMp = cvt_z(Db[(6 + md) * Q + q]);
-      zc A1 = (rc.my_d[md] * dJt + rc.kd[md] * dMp) * rc.s1f;
-      zc B1 = (rc.my_d[md] * dJp - rc.kd[md] * dMt) * rc.s1f;
-      zc A2 = (rc.eps_d[md] * dMt - rc.kd[md] * dJp) * rc.s2f;
-      zc B2 = (rc.kd[md] * dJt + rc.eps_d[md] * dMp) * rc.s2f;
+      const zc kd = recv_kd(rc, md, q, Q);
+      zc A1 = (rc.my_d[md] * dJt + kd * dMp) * rc.s1f;
+      zc B1 = (rc.my_d[md] * dJp - kd * dMt) * rc.s1f;
+      zc A2 = (rc.eps_d[md] * dMt - kd * dJp) * rc.s2f;
+      zc B2 = (kd * dJt + rc.eps_d[md] * dMp) * rc.s2f;
       cx<T>* u = sU + (size_t)md * 4 * Q + q;
       u[0] = mk<T>((T)A1.re, (T)A1.im);
       u[Q] = mk<T>((T)B1.re, (T)B1.im);
@@ -1113,14 +1125,15 @@ __global__ void k_ss_b(const cx<T>* __restrict__ Cc, const int* ch_ptr, const in
 // Fold of the eight D items of one (box, vector, direction) into the eight values the
 // receive multiplies the radiation patterns by: per medium A1, B1 (first output) and
 // A2, B2 (second output), as in k_receive_chunk, in FP64.  out[md * 4 + {A1, B1, A2, B2}].
-__device__ __forceinline__ void recv_fold(const zc d[8], const RecvConst& rc, zc u[8]) {
+__device__ __forceinline__ void recv_fold(const zc d[8], const RecvConst& rc, zc u[8], int q, int Q) {
 #pragma unroll
   for (int md = 0; md < 2; md++) {
     const zc dJt = d[0 + md], dMt = d[2 + md], dJp = d[4 + md], dMp = d[6 + md];
-    u[md * 4 + 0] = (rc.my_d[md] * dJt + rc.kd[md] * dMp) * rc.s1f;
-    u[md * 4 + 1] = (rc.my_d[md] * dJp - rc.kd[md] * dMt) * rc.s1f;
-    u[md * 4 + 2] = (rc.eps_d[md] * dMt - rc.kd[md] * dJp) * rc.s2f;
-    u[md * 4 + 3] = (rc.kd[md] * dJt + rc.eps_d[md] * dMp) * rc.s2f;
+    const zc kd = recv_kd(rc, md, q, Q);
+    u[md * 4 + 0] = (rc.my_d[md] * dJt + kd * dMp) * rc.s1f;
+    u[md * 4 + 1] = (rc.my_d[md] * dJp - kd * dMt) * rc.s1f;
+    u[md * 4 + 2] = (rc.eps_d[md] * dMt - kd * dJp) * rc.s2f;
+    u[md * 4 + 3] = (kd * dJt + rc.eps_d[md] * dMp) * rc.s2f;
   }
 }
 
@@ -1154,7 +1167,7 @@ __global__ void k_rr_b(const cx<T>* __restrict__ Dp, const int* parent, const in
     zc dz[8], u[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) dz[i] = cvt_z(d[i]);
-    recv_fold(dz, rc, u);
+    recv_fold(dz, rc, u, q, Q);
 #pragma unroll
     for (int i = 0; i < 8; i++) dst[(size_t)i * Q] = mk<T>((T)u[i].re, (T)u[i].im);
   } else if (p >= 0) {
@@ -1449,18 +1462,20 @@ int far_build_tables(sie_ctx* c, const double* d_boxc) {
     }
     SIE_CUDA(cudaGetLastError());
   }
-  // TL tables per level
+  // TL tables per level, each on its level's sampling
+  int Kmax = K;
+  for (int l = c->l_min; l <= c->l_max; l++) Kmax = std::max(Kmax, c->lv[l].K);
   zc* hk = nullptr;
-  SIE_CUDA(cudaMalloc(&hk, (size_t)343 * 2 * K * sizeof(zc)));
+  SIE_CUDA(cudaMalloc(&hk, (size_t)343 * 2 * Kmax * sizeof(zc)));
   for (int l = c->l_min; l <= c->l_max; l++) {
     Level& L = c->lv[l];
     double dc = ldexp(1.0, -l) * c->D;
     double xmn = -3 * dc, xmx = -xmn;
     double dx = (xmx - xmn) / 6;
-    k_hankel<<<(343 + 63) / 64, 64, 0, st>>>(xmn, dx, c->mt.k1, c->mt.k2, K, L.only_k1, hk); sie::count_launch();
+    k_hankel<<<(343 + 63) / 64, 64, 0, st>>>(xmn, dx, c->mt.k1, c->mt.k2, L.K, L.only_k1, hk); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
-    dim3 g((Q + 127) / 128, 343);
-    k_tl<<<g, 128, 0, st>>>(xmn, dx, hk, c->mt.k1, c->mt.k2, K, Q, c->d_khat, L.tl); sie::count_launch();
+    dim3 g((L.Q + 127) / 128, 343);
+    k_tl<<<g, 128, 0, st>>>(xmn, dx, hk, c->mt.k1, c->mt.k2, L.K, L.Q, L.khat, L.tl); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   SIE_CUDA(cudaStreamSynchronize(st));
@@ -1478,9 +1493,115 @@ template <> const cc* php_up<float>(const Level& L) { return L.ph_up32; }
 template <typename T> static const cx<T>* php_dn(const Level& L);
 template <> const zc* php_dn<double>(const Level& L) { return L.ph_dn; }
 template <> const cc* php_dn<float>(const Level& L) { return L.ph_dn32; }
-template <typename T> static const T* trfp(const sie_ctx* c);
-template <> const double* trfp<double>(const sie_ctx* c) { return c->d_trf; }
-template <> const float* trfp<float>(const sie_ctx* c) { return c->d_trf32; }
+template <typename T> static const T* trfp(const Level& L);
+template <> const double* trfp<double>(const Level& L) { return L.trf; }
+template <> const float* trfp<float>(const Level& L) { return L.trf32; }
+template <typename T> static const T* ivalp(const InterpDev& I);
+template <> const double* ivalp<double>(const InterpDev& I) { return I.val; }
+template <> const float* ivalp<float>(const InterpDev& I) { return I.val32; }
+
+// Interpolation between two levels' samplings on every (theta, phi) item pair of nbox
+// coefficient blocks [8][Q]: out[b][item][q] (+)= sum_k val[k] in[b][...][col[k]], with
+// inputs and outputs ordered (theta values, then phi values) as the CSR rows and
+// columns are.  Thread per (output row, block, item pair).
+template <typename T>
+__global__ void __launch_bounds__(128) k_interp(const int* __restrict__ ptr, const int* __restrict__ col,
+                                                const T* __restrict__ val, int rows,
+                                                const cx<T>* __restrict__ in, int Qi,
+                                                cx<T>* __restrict__ out, int Qo, int accum) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const size_t b = blockIdx.y;
+  const int p = blockIdx.z;
+  const cx<T>* a = in + (b * 8 + p) * (size_t)Qi;       // theta item p
+  const cx<T>* bb = in + (b * 8 + p + 4) * (size_t)Qi;  // its phi item
+  cx<T> acc = mk<T>(0, 0);
+  for (int k = ptr[r]; k < ptr[r + 1]; k++) {
+    const int j = col[k];
+    const cx<T> v = j < Qi ? a[j] : bb[j - Qi];
+    const T w = val[k];
+    acc.re = fma(w, v.re, acc.re);
+    acc.im = fma(w, v.im, acc.im);
+  }
+  const int item = r < Qo ? p : p + 4, q = r < Qo ? r : r - Qo;
+  cx<T>* o = out + (b * 8 + item) * (size_t)Qo + q;
+  if (accum) *o += acc;
+  else *o = acc;
+}
+
+// The same with one block per coefficient block: its 8 x Qi inputs are staged in shared
+// memory once, and the block's threads walk the 4 x rows outputs (the stencil taps then
+// read shared memory, not scattered global words).
+template <typename T>
+__global__ void __launch_bounds__(256) k_interp_s(const int* __restrict__ ptr, const int* __restrict__ col,
+                                                  const T* __restrict__ val, int rows,
+                                                  const cx<T>* __restrict__ in, int Qi,
+                                                  cx<T>* __restrict__ out, int Qo, int accum) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [8][Qi]
+  const size_t b = blockIdx.x;
+  const cx<T>* src = in + b * 8 * (size_t)Qi;
+  for (int i = threadIdx.x; i < 8 * Qi; i += blockDim.x) xs[i] = src[i];
+  __syncthreads();
+  cx<T>* dst = out + b * 8 * (size_t)Qo;
+  for (int t = threadIdx.x; t < 4 * rows; t += blockDim.x) {
+    const int p = t / rows, r = t - p * rows;
+    const cx<T>* a = xs + (size_t)p * Qi;
+    const cx<T>* bb = xs + (size_t)(p + 4) * Qi;
+    cx<T> acc = mk<T>(0, 0);
+    for (int k = ptr[r]; k < ptr[r + 1]; k++) {
+      const int j = col[k];
+      const cx<T> v = j < Qi ? a[j] : bb[j - Qi];
+      const T w = val[k];
+      acc.re = fma(w, v.re, acc.re);
+      acc.im = fma(w, v.im, acc.im);
+    }
+    const int item = r < Qo ? p : p + 4, q = r < Qo ? r : r - Qo;
+    cx<T>* o = dst + (size_t)item * Qo + q;
+    if (accum) *o += acc;
+    else *o = acc;
+  }
+}
+
+// nbox blocks of [8][Qi] through I into blocks of [8][Qo] (Qo = I.rows / 2).
+template <typename T>
+static int interp_run(const InterpDev& I, const cx<T>* in, int Qi, cx<T>* out, size_t nbox, bool accum,
+                      cudaStream_t st) {
+  const size_t smem = (size_t)8 * Qi * sizeof(cx<T>);
+  if (smem <= (size_t)200 * 1024) {
+    SIE_CUDA(raise_smem(k_interp_s<T>, smem));
+    for (size_t b0 = 0; b0 < nbox; b0 += 2147483647u) {
+      const unsigned nb = (unsigned)std::min<size_t>(2147483647u, nbox - b0);
+      k_interp_s<T><<<nb, 256, smem, st>>>(I.ptr, I.col, ivalp<T>(I), I.rows, in + b0 * 8 * Qi, Qi,
+                                           out + b0 * 8 * (I.rows / 2), I.rows / 2, accum ? 1 : 0);
+      sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+    return SIE_OK;
+  }
+  for (size_t b0 = 0; b0 < nbox; b0 += 65535) {
+    const unsigned nb = (unsigned)std::min<size_t>(65535, nbox - b0);
+    dim3 g((I.rows + 127) / 128, nb, 4);
+    k_interp<T><<<g, 128, 0, st>>>(I.ptr, I.col, ivalp<T>(I), I.rows, in + b0 * 8 * Qi, Qi,
+                                   out + b0 * 8 * (I.rows / 2), I.rows / 2, accum ? 1 : 0);
+    sie::count_launch();
+  }
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+// Work buffer for coefficients on another level's sampling, grown on demand.
+static int lvtmp(sie_ctx* c, size_t bytes, void** p) {
+  if (c->lvtmp_bytes < bytes) {
+    if (c->d_lvtmp) cudaFree(c->d_lvtmp);
+    c->d_lvtmp = nullptr;
+    c->lvtmp_bytes = 0;
+    SIE_CUDA(cudaMalloc(&c->d_lvtmp, bytes));
+    c->lvtmp_bytes = bytes;
+  }
+  *p = c->d_lvtmp;
+  return SIE_OK;
+}
 
 // Factors of the final far summation (MLFMM_tri_summation_New,
 // lib_sie_tri_mlfmm.f90:416-497) and the ICTF output scaling (:486-488).
@@ -1500,6 +1621,7 @@ static RecvConst recv_const(const sie_ctx* c) {
     rc.s1f = mk<double>(1, 0);
     rc.s2f = mk<double>(1, 0);
   }
+  rc.pole_fix = c->level_k ? 1 : 0;
   return rc;
 }
 
@@ -1508,16 +1630,24 @@ static RecvConst recv_const(const sie_ctx* c) {
 template <typename T>
 static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
                            const std::function<int()>* after_ss = nullptr) {
-  const int Q = c->Q;
   const int L0 = c->l_min, L1 = c->l_max;
   const bool k2c = c->mt.k2.im != 0.0;
   const int thr = 128;
-  // up 2
+  // up 2: a child level with a smaller sampling is interpolated to the parent's first
+  // (translation_SS, lib_sie_tri_mlfmm_interface.f90:486-507), then shifted on it
   for (int l = L1 - 1; l >= L0; l--) {
     Level& P = c->lv[l];
     Level& Ch = c->lv[l + 1];
+    const int Q = P.Q;
+    const cx<T>* src = (const cx<T>*)Ch.C;
+    if (Ch.Q != Q) {
+      void* tmp = nullptr;
+      SIE_TRY(lvtmp(c, (size_t)Ch.nb * 8 * Q * sizeof(cx<T>), &tmp));
+      SIE_TRY(interp_run<T>(P.up, src, Ch.Q, (cx<T>*)tmp, Ch.nb, false, st));
+      src = (const cx<T>*)tmp;
+    }
     dim3 g((Q + thr - 1) / thr, P.nb);
-    k_ss<T><<<g, thr, 0, st>>>((const cx<T>*)Ch.C, P.ch_ptr, P.ch_idx, P.ch_oct,
+    k_ss<T><<<g, thr, 0, st>>>(src, P.ch_ptr, P.ch_idx, P.ch_oct,
                                php_up<T>(Ch), Q, k2c ? 1 : 2, (cx<T>*)P.C); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
@@ -1526,10 +1656,11 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
   // down 1
   for (int l = L0; l <= L1; l++) {
     Level& L = c->lv[l];
+    const int Q = L.Q;
     if (c->sr_mode == 0) {
       dim3 g((Q + thr - 1) / thr, L.nb);
       k_sr<T><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.i4_ptr, L.i4_src, L.i4_off,
-                                 tlp<T>(L), trfp<T>(c), Q, L.only_k1 ? 1 : 2,
+                                 tlp<T>(L), trfp<T>(L), Q, L.only_k1 ? 1 : 2,
                                  (cx<T>*)L.D); sie::count_launch();
     } else if (c->sr_mode == 5 && L.nb < (1 << 22)) {  // source box and T0 share one int
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
@@ -1539,7 +1670,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
         // SR 0.380 -> 0.360 ms, the same bits); complex64 keeps plain accesses
         constexpr int hint = std::is_same<T, double>::value ? 3 : 0;
         k_sr_warp_ns<T, 1, hint><<<g, 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
-            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D);
+            (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(L), Q, md, nmed == 1, (cx<T>*)L.D);
         sie::count_launch();
       }
     } else if (c->sr_mode >= 4 && L.nb < (1 << 23)) {
@@ -1548,7 +1679,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
       for (int md = 0; md < nmed; md++) {
         k_sr_warp_bf<T><<<g, 32 * SRW_GB, sr_warp_bf_smem<T>(), st>>>(
             (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
-            trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+            trfp<T>(L), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
     } else if (c->sr_mode >= 3 && L.nb < (1 << 23)) {  // source box and slot share one int
       dim3 g((Q + SRW_QT - 1) / SRW_QT, (L.ngrp + SRW_GB - 1) / SRW_GB);
@@ -1556,7 +1687,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
       for (int md = 0; md < nmed; md++) {
         k_sr_warp<T><<<g, 32 * SRW_GB, sr_warp_smem<T>(), st>>>(
             (const cx<T>*)L.C, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L),
-            trfp<T>(c), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
+            trfp<T>(L), Q, md, nmed == 1, (cx<T>*)L.D); sie::count_launch();
       }
     } else if (c->sr_mode == 2) {
       dim3 g((Q + SR_TQ - 1) / SR_TQ, (L.ngrp + SR_GB - 1) / SR_GB);
@@ -1565,7 +1696,7 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
       for (int md = 0; md < nmed; md++) {
         k_sr_group_tl<T><<<g, SR_TQ * SR_GB, smem, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
                                                           L.ngrp, tlp<T>(L),
-                                                          trfp<T>(c), Q, md, nmed == 1,
+                                                          trfp<T>(L), Q, md, nmed == 1,
                                                           (cx<T>*)L.D); sie::count_launch();
       }
     } else {
@@ -1574,21 +1705,36 @@ static int far_translate_t(sie_ctx* c, cudaStream_t st, cudaEvent_t* ev,
       for (int md = 0; md < nmed; md++)
         for (int i0 = 0; i0 < 4; i0 += 2) {
           k_sr_group<T, 2><<<g, thr, 0, st>>>((const cx<T>*)L.C, L.grp_sib, L.grp_src,
-                                              tlp<T>(L), trfp<T>(c), Q, md, i0,
+                                              tlp<T>(L), trfp<T>(L), Q, md, i0,
                                               nmed == 1, (cx<T>*)L.D); sie::count_launch();
         }
     }
     SIE_CUDA(cudaGetLastError());
   }
   if (ev) cudaEventRecord(ev[3], st);
-  // down 2
+  // down 2: a child level with a smaller sampling takes the parent's D shifted on the
+  // parent's sampling, then anterpolated (the transpose of the SS interpolation)
   for (int l = L0 + 1; l <= L1; l++) {
     Level& L = c->lv[l];
     Level& P = c->lv[l - 1];
-    dim3 g((Q + thr - 1) / thr, L.nb);
     int nmed = (k2c && l < L1) ? 1 : 2;
     // D_k2 of the parent is zero when its level only carries k1
     if (k2c) nmed = 1;
+    if (L.Q != P.Q) {
+      const int Qp = P.Q;
+      void* tmp = nullptr;
+      const size_t n = (size_t)L.nb * 8 * Qp;
+      SIE_TRY(lvtmp(c, n * sizeof(cx<T>), &tmp));
+      SIE_CUDA(cudaMemsetAsync(tmp, 0, n * sizeof(cx<T>), st));
+      dim3 g((Qp + thr - 1) / thr, L.nb);
+      k_rr<T><<<g, thr, 0, st>>>((const cx<T>*)P.D, L.parent, L.oct, php_dn<T>(L), Qp, nmed,
+                                 (cx<T>*)tmp); sie::count_launch();
+      SIE_CUDA(cudaGetLastError());
+      SIE_TRY(interp_run<T>(P.dn, (const cx<T>*)tmp, Qp, (cx<T>*)L.D, L.nb, true, st));
+      continue;
+    }
+    const int Q = L.Q;
+    dim3 g((Q + thr - 1) / thr, L.nb);
     k_rr<T><<<g, thr, 0, st>>>((const cx<T>*)P.D, L.parent, L.oct, php_dn<T>(L), Q, nmed,
                                (cx<T>*)L.D); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
@@ -1743,6 +1889,8 @@ __global__ void __launch_bounds__(256, 2) k_adj_out(const zc* __restrict__ rt, c
 
 // y += Z_far^T x (FP64, internal layout); uses the one-vector level buffers C and D.
 int far_matvec_adj64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st) {
+  if (c->level_k)
+    return fail(SIE_ERR_STATE, "transposed product: not available with per-level truncation numbers");
   const int Q = c->Q, L1 = c->l_max;
   Level& L = c->lv[L1];
   {
@@ -1826,7 +1974,7 @@ __global__ void k_fold_leaf(zc* D, int nb, int Q, RecvConst rc) {
   zc* d = D + (size_t)b * 8 * Q + q;
   zc in[8], u[8];
   for (int i = 0; i < 8; i++) in[i] = d[(size_t)i * Q];
-  recv_fold(in, rc, u);
+  recv_fold(in, rc, u, q, Q);
   for (int i = 0; i < 8; i++) d[(size_t)i * Q] = u[i];
 }
 
@@ -1837,6 +1985,7 @@ __global__ void k_conj_copy(const zc* a, zc* b, size_t n) {
 
 // ws: 2 x (leaf boxes x 8 x Q) + 2M complex128.
 int grad_far(sie_ctx* c, const zc* lam, const zc* I, double h, double* grad, void* ws, cudaStream_t st) {
+  if (c->level_k) return fail(SIE_ERR_STATE, "shape gradient: not available with per-level truncation numbers");
   const int Q = c->Q, L1 = c->l_max;
   Level& L = c->lv[L1];
   const size_t nl = (size_t)L.nb * 8 * Q;
@@ -1887,7 +2036,7 @@ template <typename T>
 static int ensure_batch_coeffs(sie_ctx* c, int R) {
   for (int l = c->l_min; l <= c->l_max; l++) {
     Level& L = c->lv[l];
-    size_t need = (size_t)L.nb * 8 * R * c->Q * sizeof(cx<T>);
+    size_t need = (size_t)L.nb * 8 * R * L.Q * sizeof(cx<T>);
     if (L.cdb_bytes >= need) continue;
     if (L.Cb) cudaFree(L.Cb);
     if (L.Db) cudaFree(L.Db);
@@ -1919,18 +2068,28 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
     SIE_CUDA(cudaGetLastError());
   }
   if (after_agg) SIE_TRY((*after_agg)());
+  // the batch layout [box][r][8][Q] is nb * R blocks of [8][Q] for the interpolation
   for (int l = L1 - 1; l >= L0; l--) {
     Level& P = c->lv[l];
     Level& Ch = c->lv[l + 1];
-    dim3 g((Q + thr - 1) / thr, P.nb, R);
-    k_ss_b<T><<<g, thr, 0, st>>>((const cx<T>*)Ch.Cb, P.ch_ptr, P.ch_idx, P.ch_oct, php_up<T>(Ch), Q,
+    const int Qp = P.Q;
+    const cx<T>* src = (const cx<T>*)Ch.Cb;
+    if (Ch.Q != Qp) {
+      void* tmp = nullptr;
+      SIE_TRY(lvtmp(c, (size_t)Ch.nb * R * 8 * Qp * sizeof(cx<T>), &tmp));
+      SIE_TRY(interp_run<T>(P.up, src, Ch.Q, (cx<T>*)tmp, (size_t)Ch.nb * R, false, st));
+      src = (const cx<T>*)tmp;
+    }
+    dim3 g((Qp + thr - 1) / thr, P.nb, R);
+    k_ss_b<T><<<g, thr, 0, st>>>(src, P.ch_ptr, P.ch_idx, P.ch_oct, php_up<T>(Ch), Qp,
                                  k2c ? 1 : 2, R, (cx<T>*)P.Cb); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
   for (int l = L0; l <= L1; l++) {
     Level& L = c->lv[l];
+    const int Ql = L.Q;
     if (L.nb >= (1 << 22)) return fail(SIE_ERR_ARG, "batched far product: too many boxes on a level");
-    const unsigned gx = (Q + SRW_QT - 1) / SRW_QT, gy = (L.ngrp + SRW_GB - 1) / SRW_GB;
+    const unsigned gx = (Ql + SRW_QT - 1) / SRW_QT, gy = (L.ngrp + SRW_GB - 1) / SRW_GB;
     const int nmed = L.only_k1 ? 1 : 2;
     for (int md = 0; md < nmed; md++) {
       // two vectors per source read in FP32; one in FP64, whose accumulators are twice as wide
@@ -1938,27 +2097,48 @@ static int far_matvec_b_t(sie_ctx* c, const cx<T>* rt, const cx<T>* x, cx<T>* y,
       if constexpr (sizeof(T) == 4) {
         if (R % 2 == 0) {
           k_sr_ns_b<T, 2><<<dim3(gx, gy, R / 2), 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
-              (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(c), Q, md, nmed == 1, R,
+              (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(L), Ql, md, nmed == 1, R,
               (cx<T>*)L.Db);
           done = true;
         }
       }
       if (!done)
         k_sr_ns_b<T, 1><<<dim3(gx, gy, R), 32 * SRW_GB, sr_warp_ns_smem<T>(), st>>>(
-            (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(c), Q, md, nmed == 1, R,
+            (const cx<T>*)L.Cb, L.grp_sib, L.grp_src, L.ngrp, tlp<T>(L), trfp<T>(L), Ql, md, nmed == 1, R,
             (cx<T>*)L.Db);
       sie::count_launch();
     }
     SIE_CUDA(cudaGetLastError());
   }
   // RR down to the leaves; the leaf level's kernel also folds D for the receive (with a
-  // single level there is no RR, and the same kernel only folds: every parent is absent)
+  // single level there is no RR, and the same kernel only folds: every parent is absent).
+  // A child level with a smaller sampling takes the parent's D shifted on the parent's
+  // sampling and anterpolated; the leaf level's fold then runs as a pass of its own.
   const RecvConst rcn = recv_const(c);
   for (int l = (L1 > L0 ? L0 + 1 : L1); l <= L1; l++) {
     Level& L = c->lv[l];
     Level& P = c->lv[l > L0 ? l - 1 : l];
-    dim3 g((Q + thr - 1) / thr, L.nb, R);
-    k_rr_b<T><<<g, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), Q, k2c ? 1 : 2, R,
+    if (l > L0 && L.Q != P.Q) {
+      const int Qp = P.Q;
+      void* tmp = nullptr;
+      const size_t n = (size_t)L.nb * R * 8 * Qp;
+      SIE_TRY(lvtmp(c, n * sizeof(cx<T>), &tmp));
+      SIE_CUDA(cudaMemsetAsync(tmp, 0, n * sizeof(cx<T>), st));
+      dim3 g((Qp + thr - 1) / thr, L.nb, R);
+      k_rr_b<T><<<g, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), Qp, k2c ? 1 : 2, R, 0,
+                                   rcn, (cx<T>*)tmp); sie::count_launch();
+      SIE_CUDA(cudaGetLastError());
+      SIE_TRY(interp_run<T>(P.dn, (const cx<T>*)tmp, Qp, (cx<T>*)L.Db, (size_t)L.nb * R, true, st));
+      if (l == L1) {  // fold only: no medium is shifted
+        dim3 gf((L.Q + thr - 1) / thr, L.nb, R);
+        k_rr_b<T><<<gf, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), L.Q, 0, R, 1, rcn,
+                                      (cx<T>*)L.Db); sie::count_launch();
+        SIE_CUDA(cudaGetLastError());
+      }
+      continue;
+    }
+    dim3 g((L.Q + thr - 1) / thr, L.nb, R);
+    k_rr_b<T><<<g, thr, 0, st>>>((const cx<T>*)P.Db, L.parent, L.oct, php_dn<T>(L), L.Q, k2c ? 1 : 2, R,
                                  l == L1, rcn, (cx<T>*)L.Db); sie::count_launch();
     SIE_CUDA(cudaGetLastError());
   }
@@ -2010,13 +2190,23 @@ int make_f32_tables(sie_ctx* c) {
     SIE_CUDA(cudaGetLastError());
     for (int l = c->l_min; l <= c->l_max; l++) {
       Level& L = c->lv[l];
-      size_t ntl = (size_t)343 * 2 * Q, nph = (size_t)8 * 2 * Q;
+      const int Qs = c->lv[l > c->l_min ? l - 1 : l].Q;  // the shift tables' (parent) sampling
+      size_t ntl = (size_t)343 * 2 * L.Q, nph = (size_t)8 * 2 * Qs;
       SIE_CUDA(cudaMalloc(&L.tl32, ntl * sizeof(cc)));
       SIE_CUDA(cudaMalloc(&L.ph_up32, nph * sizeof(cc)));
       SIE_CUDA(cudaMalloc(&L.ph_dn32, nph * sizeof(cc)));
       SIE_TRY(to_c64(L.tl, L.tl32, ntl, st));
       SIE_TRY(to_c64(L.ph_up, L.ph_up32, nph, st));
       SIE_TRY(to_c64(L.ph_dn, L.ph_dn32, nph, st));
+      SIE_CUDA(cudaMalloc(&L.trf32, (size_t)L.Q * sizeof(float)));
+      k_trf_f32<<<(L.Q + 255) / 256, 256, 0, st>>>(L.trf, L.trf32, L.Q); sie::count_launch();
+      for (InterpDev* I : {&L.up, &L.dn})
+        if (I->nnz > 0) {
+          SIE_CUDA(cudaMalloc(&I->val32, (size_t)I->nnz * sizeof(float)));
+          k_trf_f32<<<(unsigned)((I->nnz + 255) / 256), 256, 0, st>>>(I->val, I->val32, (int)I->nnz);
+          sie::count_launch();
+        }
+      SIE_CUDA(cudaGetLastError());
     }
   }
   size_t n = (size_t)2 * c->M;

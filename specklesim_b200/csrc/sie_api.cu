@@ -530,13 +530,17 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
   }
 }
 
-// Khat_and_TRF_ExtendedK (src/lib_sie_mlfmm.f90:190-240)
-static int build_sampling(sie_ctx* c) {
-  int K = c->K, Ns = 2 * K * K, Q = Ns + 2;
-  c->Q = Q;
+// Khat_and_TRF_ExtendedK (src/lib_sie_mlfmm.f90:190-240): directions, transfer vectors
+// and quadrature weights of the K sampling, poles last.
+static void sampling_tables(int K, std::vector<double>& kh, std::vector<double>& th, std::vector<double>& ph,
+                            std::vector<double>& trf) {
+  const int Ns = 2 * K * K, Q = Ns + 2;
   std::vector<double> xx, ww;
   gauss_legendre(K, xx, ww);
-  std::vector<double> kh(3 * Q), th(3 * Q), ph(3 * Q), trf(Q);
+  kh.assign(3 * (size_t)Q, 0.0);
+  th.assign(3 * (size_t)Q, 0.0);
+  ph.assign(3 * (size_t)Q, 0.0);
+  trf.assign(Q, 0.0);
   double dphi = 2 * PI / (2 * K);
   for (int j = 0; j < K; j++)
     for (int k = 0; k < 2 * K; k++) {
@@ -562,6 +566,35 @@ static int build_sampling(sie_ctx* c) {
     ph[3 * i] = 0; ph[3 * i + 1] = 1; ph[3 * i + 2] = 0;
     trf[i] = 0.0;
   }
+}
+
+// Truncation number of level l: the one requested for it, else the configuration's.
+static int level_truncation(const sie_ctx* c, int l) {
+  return (l < (int)c->level_K.size() && c->level_K[l] > 0) ? c->level_K[l] : c->cfg.truncation_number;
+}
+
+// Samplings of every level.  The leaf level's is also the context's own (c->K, c->Q and
+// the d_khat/d_tth/d_tph/d_trf arrays: radiation patterns, aggregate and receive).
+static int build_sampling(sie_ctx* c) {
+  for (int l = c->l_min; l < c->l_max; l++)
+    if (level_truncation(c, l + 1) > level_truncation(c, l))
+      return fail(SIE_ERR_ARG, "per-level truncation numbers must not grow from a level to its children");
+  c->level_k = false;
+  for (int l = c->l_min; l <= c->l_max; l++) {
+    Level& L = c->lv[l];
+    L.K = level_truncation(c, l);
+    L.Q = 2 * L.K * L.K + 2;
+    c->level_k |= L.K != level_truncation(c, c->l_max);
+    std::vector<double> kh, th, ph, trf;
+    sampling_tables(L.K, kh, th, ph, trf);
+    SIE_TRY(upload(&L.khat, kh));
+    SIE_TRY(upload(&L.trf, trf));
+  }
+  int K = level_truncation(c, c->l_max), Ns = 2 * K * K, Q = Ns + 2;
+  c->K = K;
+  c->Q = Q;
+  std::vector<double> kh, th, ph, trf;
+  sampling_tables(K, kh, th, ph, trf);
   // direction of -khat for every direction (used by the transposed product): theta ->
   // pi - theta is Gauss node K-1-j, phi -> phi + pi is k + K, and the two poles swap
   std::vector<int> qp(Q);
@@ -578,6 +611,38 @@ static int build_sampling(sie_ctx* c) {
   SIE_TRY(upload(&c->d_tth, th));
   SIE_TRY(upload(&c->d_tph, ph));
   SIE_TRY(upload(&c->d_trf, trf));
+  return SIE_OK;
+}
+
+// Interpolation (child -> parent) and anterpolation (parent -> child) matrices between
+// level l and level l + 1 when their samplings differ (stencil of 2p x 2p, p = 3, as the
+// reference's Lagrange_Interpolation_New calls use).
+static int upload_interp(const Csr& A, InterpDev& d) {
+  d.rows = A.rows;
+  d.nnz = (long long)A.val.size();
+  SIE_TRY(upload(&d.ptr, A.ptr));
+  SIE_TRY(upload(&d.col, A.col));
+  SIE_TRY(upload(&d.val, A.val));
+  return SIE_OK;
+}
+
+static int build_interp(sie_ctx* c) {
+  size_t tmp = 0;
+  for (int l = c->l_min; l < c->l_max; l++) {
+    Level& P = c->lv[l];
+    Level& Ch = c->lv[l + 1];
+    if (P.K == Ch.K) continue;
+    Csr up, dn;
+    SIE_TRY(interp_csr(3, Ch.K, P.K, false, up));
+    SIE_TRY(interp_csr(3, Ch.K, P.K, true, dn));
+    SIE_TRY(upload_interp(up, P.up));
+    SIE_TRY(upload_interp(dn, P.dn));
+    tmp = std::max(tmp, (size_t)Ch.nb * 8 * P.Q * sizeof(zc));
+  }
+  if (tmp) {
+    SIE_CUDA(cudaMalloc(&c->d_lvtmp, tmp));
+    c->lvtmp_bytes = tmp;
+  }
   return SIE_OK;
 }
 
@@ -907,6 +972,22 @@ int sie_info(const sie_ctx* c, int* n_edges, int* l_min, int* l_max, long long* 
   return SIE_OK;
 }
 
+int sie_set_level_truncation(sie_ctx* c, const int* K, int n) {
+  if (!c || n < 0 || (n > 0 && !K)) return fail(SIE_ERR_ARG, "sie_set_level_truncation: bad argument");
+  if (c->setup_done) return fail(SIE_ERR_STATE, "sie_set_level_truncation: call it before sie_setup");
+  for (int i = 0; i < n; i++)
+    if (K[i] < 0 || K[i] > 200) return fail(SIE_ERR_ARG, "sie_set_level_truncation: truncation number out of range");
+  c->level_K.assign(K, K + n);
+  const int KL = level_truncation(c, c->l_max);
+  for (int l = c->l_min; l < c->l_max; l++)
+    if (level_truncation(c, l + 1) > level_truncation(c, l)) {
+      c->level_K.clear();
+      return fail(SIE_ERR_ARG, "sie_set_level_truncation: truncation numbers must not grow toward the leaf level");
+    }
+  c->K = KL;
+  return SIE_OK;
+}
+
 int sie_num_directions(const sie_ctx* c, int* Q) {
   if (!c || !Q) return fail(SIE_ERR_ARG, "null argument");
   *Q = 2 * c->K * c->K + 2;
@@ -988,13 +1069,16 @@ int sie_setup(sie_ctx* c) {
     SIE_CUDA(cudaMalloc(&c->d_rt, (size_t)M * 4 * Q * sizeof(zc)));
     for (int l = c->l_min; l <= c->l_max; l++) {
       Level& L = c->lv[l];
-      SIE_CUDA(cudaMalloc(&L.C, (size_t)L.nb * 8 * Q * sizeof(zc)));
-      SIE_CUDA(cudaMalloc(&L.D, (size_t)L.nb * 8 * Q * sizeof(zc)));
-      SIE_CUDA(cudaMalloc(&L.tl, (size_t)343 * 2 * Q * sizeof(zc)));
-      SIE_CUDA(cudaMalloc(&L.ph_up, (size_t)8 * 2 * Q * sizeof(zc)));
-      SIE_CUDA(cudaMalloc(&L.ph_dn, (size_t)8 * 2 * Q * sizeof(zc)));
-      SIE_TRY(phase_tables(c, L, l));
+      // the shift tables of level l live on its parent's sampling
+      const Level& S = c->lv[l > c->l_min ? l - 1 : l];
+      SIE_CUDA(cudaMalloc(&L.C, (size_t)L.nb * 8 * L.Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.D, (size_t)L.nb * 8 * L.Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.tl, (size_t)343 * 2 * L.Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.ph_up, (size_t)8 * 2 * S.Q * sizeof(zc)));
+      SIE_CUDA(cudaMalloc(&L.ph_dn, (size_t)8 * 2 * S.Q * sizeof(zc)));
+      SIE_TRY(phase_tables(c, L, l, S.khat, S.Q));
     }
+    SIE_TRY(build_interp(c));
     cudaEventRecord(c->ev[10], c->stream);
     r = far_build_tables(c, d_boxc);
     cudaEventRecord(c->ev[11], c->stream);
@@ -1309,6 +1393,8 @@ static int grad_tables(sie_ctx* c) {
 
 int sie_grad(sie_ctx* c, const double* x, const double* k_in, const double* E_in, const double* pts, int npts,
              const sie_solver_cfg* cfg, double* dJdz, double* J, sie_stats* stats) {
+  if (c && c->level_k)
+    return fail(SIE_ERR_STATE, "sie_grad: not available with per-level truncation numbers");
   if (!c || !x || !k_in || !E_in || !pts || npts < 1 || !cfg || !dJdz)
     return fail(SIE_ERR_ARG, "sie_grad: bad argument");
   if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_grad: sie_setup not called");
@@ -1551,11 +1637,12 @@ int sie_get_rt(sie_ctx* c, const int* edges, int cnt, double* out) {
 
 int sie_get_timings(const sie_ctx* c, double* out, int n) {
   if (!c || !out) return fail(SIE_ERR_ARG, "sie_get_timings: null argument");
-  double v[12] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
+  double v[14] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
                   c->tm.mv_near_ms, c->tm.mv_agg_ms, c->tm.mv_ss_ms, c->tm.mv_sr_ms,
                   c->tm.mv_rr_ms, c->tm.mv_recv_ms,
-                  c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0, c->tm.graph_replays};
-  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
+                  c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0, c->tm.graph_replays,
+                  c->tm.precond_ms, c->tm.lu_factor_ms};
+  for (int i = 0; i < n && i < 14; i++) out[i] = v[i];
   return SIE_OK;
 }
 
@@ -1563,17 +1650,21 @@ int sie_free(sie_ctx* c) {
   if (!c) return SIE_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  ras_release(c);
   void* ptrs[] = {c->d_fn, c->d_rref, c->d_cent, c->d_perm, c->d_box_first, c->d_box_cnt,
                   c->d_nbr_ptr, c->d_nbr_box, c->d_ncols, c->d_base, c->d_edge_box, c->d_rchunk, c->d_na,
                   c->d_nb, c->d_nd, c->d_na32, c->d_nb32, c->d_nd32, c->d_diag, c->d_khat,
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
-                  c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT};
+                  c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT, c->d_lu32, c->d_lu32i, c->d_piv32};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (c->d_lvtmp) cudaFree(c->d_lvtmp);
   for (auto& L : c->lv) {
     void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.tl32, L.ph_up32, L.ph_dn32, L.i4_ptr, L.i4_src, L.i4_off,
-                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src, L.Cb, L.Db};
+                  L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src, L.Cb, L.Db,
+                  L.khat, L.trf, L.trf32, L.up.ptr, L.up.col, L.up.val, L.up.val32, L.dn.ptr, L.dn.col,
+                  L.dn.val, L.dn.val32};
     for (void* p : lp)
       if (p) cudaFree(p);
   }

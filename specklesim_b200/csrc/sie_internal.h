@@ -104,16 +104,37 @@ struct NearLayout {
   long long nnz;
 };
 
+// Interpolation between the k-space samplings of two levels as a sparse real matrix
+// acting on each (theta, phi) item pair of a box's coefficients.
+struct InterpDev {
+  int rows = 0;               // 2 Q_out
+  int* ptr = nullptr;         // rows + 1
+  int* col = nullptr;         // into the 2 Q_in input values (theta values, then phi)
+  double* val = nullptr;
+  float* val32 = nullptr;     // complex64 passes (made with the other complex64 tables)
+  long long nnz = 0;
+};
+
 struct Level {
   int l = 0;
   int nb = 0;
+  // k-space sampling of this level (truncation number K, Q = 2 K^2 + 2 directions)
+  int K = 0, Q = 0;
+  double* khat = nullptr;     // 3 x Q
+  double* trf = nullptr;      // Q quadrature weights
+  float* trf32 = nullptr;
+  // between this level and its children (l + 1) when their samplings differ: up = child
+  // -> this level (SS), dn = this level -> child (RR, the transpose of up)
+  InterpDev up, dn;
   std::vector<uint64_t> box;  // Morton indices, ascending
   // device
   zc* C = nullptr;            // nb x 8 x Q
   zc* D = nullptr;            // nb x 8 x Q
   zc* tl = nullptr;           // 343 x 2 x Q
-  zc* ph_up = nullptr;        // 8 octants x 2 media x Q  exp(+i k khat.(x_child - x_parent))
-  zc* ph_dn = nullptr;        // 8 octants x 2 media x Q  exp(-i k khat.(x_child - x_parent))
+  // on the PARENT level's sampling (Q_{l-1}): the SS shift follows the interpolation to
+  // the parent's sampling, and the RR shift precedes the anterpolation to this level's
+  zc* ph_up = nullptr;        // 8 octants x 2 media x Q_{l-1}  exp(+i k khat.(x_child - x_parent))
+  zc* ph_dn = nullptr;        // 8 octants x 2 media x Q_{l-1}  exp(-i k khat.(x_child - x_parent))
   int* i4_ptr = nullptr;      // nb + 1
   int* i4_src = nullptr;      // source box index (same level)
   int* i4_off = nullptr;      // TL offset index 0..342
@@ -147,6 +168,8 @@ struct Timings {
          mv_rr_ms = 0, mv_recv_ms = 0;
   double gm_passes = 0, gm_steps = 0;  // MGS passes and Arnoldi steps of the last solve
   double graph_replays = 0;            // inner cycles replayed from a CUDA graph, last batched solve
+  double precond_ms = 0;               // set-up of the near-field preconditioner (host wall time)
+  double lu_factor_ms = 0;             // complex64 tensor-core LU of the mixed direct solve
 };
 
 }  // namespace sie
@@ -182,7 +205,13 @@ struct sie_ctx {
   std::vector<int> iperm;         // reference -> internal
   sie::NearLayout near;
   std::vector<sie::Level> lv;     // index = level
+  // K and Q of the leaf level (radiation patterns, aggregate, receive); the other levels
+  // keep theirs in lv[l].K, lv[l].Q
   int K = 0, Q = 0;
+  std::vector<int> level_K;       // requested truncation number per level (0: cfg K)
+  bool level_k = false;           // some level's sampling differs from the leaf's
+  void* d_lvtmp = nullptr;        // coefficients of one level on its parent's sampling
+  size_t lvtmp_bytes = 0;
   bool setup_done = false;
   // SR kernel: 0 one thread per (target box, direction); 1 sibling groups;
   // 2 sibling groups with the translation table staged in shared memory;
@@ -224,6 +253,17 @@ struct sie_ctx {
   cc* d_nb32 = nullptr;
   cc* d_nd32 = nullptr;
   zc cfac;
+  // near-field RAS preconditioner (SIE_PRECOND_NEAR): full 2x2 blocks on the near panels'
+  // layout; complex64 copies for the mixed solver's inner products (made on first use)
+  int precond = SIE_PRECOND_NONE;
+  zc* d_pa = nullptr;
+  zc* d_pb = nullptr;
+  zc* d_pc = nullptr;
+  zc* d_pd = nullptr;
+  cc* d_pa32 = nullptr;
+  cc* d_pb32 = nullptr;
+  cc* d_pc32 = nullptr;
+  cc* d_pd32 = nullptr;
   zc* d_diag = nullptr;           // Jacobi diagonal, internal interleaved (J, M)
   // far field
   double* d_khat = nullptr;       // 3 x Q
@@ -267,6 +307,9 @@ struct sie_ctx {
   size_t io_bytes = 0;
   void* d_lu = nullptr;           // dense LU factors (column-major N x N, internal order)
   int* d_piv = nullptr;           // pivots (N) + info
+  float* d_lu32 = nullptr;        // complex64 LU factors of the mixed direct solve: real plane,
+  float* d_lu32i = nullptr;       // imaginary plane (column-major N x N, internal order)
+  int* d_piv32 = nullptr;         // and their row interchanges
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   void* h_gmb = nullptr;          // pinned host copy of the batched solver's per-system state
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel
@@ -336,8 +379,15 @@ int to_c64(const zc* in, cc* out, size_t n, cudaStream_t st);
 int to_c128(const cc* in, zc* out, size_t n, cudaStream_t st);
 int gather_ext_to_int(sie_ctx* c, const zc* ext, zc* in, int nrhs, cudaStream_t st);
 int scatter_int_to_ext(sie_ctx* c, const zc* in, zc* ext, int nrhs, cudaStream_t st);
-int phase_tables(sie_ctx* c, Level& L, int l);
+int phase_tables(sie_ctx* c, Level& L, int l, const double* khat_parent, int Qp);
 int diag_extract(sie_ctx* c);
+// near-field restricted additive Schwarz preconditioner: build, release, y = P x
+int ras_build(sie_ctx* c);
+void ras_release(sie_ctx* c);
+int ras_to_f32(sie_ctx* c);
+// R vectors at stride 2M
+int ras_apply64(sie_ctx* c, const zc* x, zc* y, cudaStream_t st, int R = 1);
+int ras_apply32(sie_ctx* c, const cc* x, cc* y, cudaStream_t st, int R = 1);
 int jacobi_apply(sie_ctx* c, const zc* v1, zc* v2, cudaStream_t st);
 int rhs_planewave_dev(sie_ctx* c, const double* d_k, const double* d_E, int nrhs, zc* d_b_int);
 int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,

@@ -1,0 +1,225 @@
+// Tensor-core complex GEMM update C -= A B (tcgen05, 3xTF32); layout and scheme in
+// tc_gemm.cuh.  Used by the mixed-precision dense LU (dense_lu_tc.cu) for its trailing
+// updates, the only O(N^3) work of the direct solve.
+#include "sie_internal.h"
+#include "tc_gemm.cuh"
+
+namespace sie {
+namespace tc {
+
+// Pre-tiles rows [0, rows) x K [0, K) of an operand into blocks [tile][chunk] (layout in
+// tc_gemm.cuh), splitting each value into its tf32 pair; rows and K past the operand are
+// zero.  Element (r, k) is src[k * ld + r] (column-major, the A operand: r a row of C)
+// or, with trans, src[r * ld + k] (the B operand read from a column-major K x n matrix: r
+// a column of C).  Grid: (TILE * KC / 256, chunks, tiles), 256 threads.
+__global__ void __launch_bounds__(256) k_tile(const float* __restrict__ sr, const float* __restrict__ si,
+                                              size_t ld, int rows, int K, int trans, int nchunks,
+                                              char* __restrict__ out) {
+  const int c = blockIdx.y, t = blockIdx.z;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;  // element of the block, 0 .. 2047
+  int r, k;
+  if (trans) {  // consecutive threads read consecutive k (contiguous in src)
+    k = e % KC;
+    r = e / KC;
+  } else {
+    r = e % TILE;
+    k = e / TILE;
+  }
+  const int gr = t * TILE + r, gk = c * KC + k;
+  float vr = 0.f, vi = 0.f;
+  if (gr < rows && gk < K) {
+    const size_t o = trans ? (size_t)gr * ld + gk : (size_t)gk * ld + gr;
+    vr = sr[o];
+    vi = si[o];
+  }
+  float rh, rl, ih, il;
+  tf32_split(vr, rh, rl);
+  tf32_split(vi, ih, il);
+  char* blk = out + ((size_t)t * nchunks + c) * BLOCK_BYTES + plane_offset(r, k);
+  *(float*)(blk) = rh;
+  *(float*)(blk + PLANE_BYTES) = rl;
+  *(float*)(blk + 2 * PLANE_BYTES) = ih;
+  *(float*)(blk + 3 * PLANE_BYTES) = il;
+}
+
+// C tile (blockIdx.x, blockIdx.y) -= A tile row blockIdx.x times B tile row blockIdx.y.
+__global__ void __launch_bounds__(256, 1) k_gemm(const char* __restrict__ At, const char* __restrict__ Bt,
+                                                 int nchunks, float* __restrict__ Cr, float* __restrict__ Ci,
+                                                 size_t ldc, int m, int n, int* err) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 127) & ~(uintptr_t)127);
+  uint64_t* full = (uint64_t*)(sm + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tslot = (uint32_t*)(done + 1);
+  __shared__ int fail;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mt = blockIdx.x, nt = blockIdx.y;
+  if (threadIdx.x == 0) {
+    fail = 0;
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    // 256 columns: the real accumulator in 0..127, the imaginary one in 128..255
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+
+  if (warp == 0 && lane == 0) {
+    // producer: one A block and one B block per stage
+    const char* a0 = At + (size_t)mt * nchunks * BLOCK_BYTES;
+    const char* b0 = Bt + (size_t)nt * nchunks * BLOCK_BYTES;
+    for (int c = 0; c < nchunks; c++) {
+      const int s = c % STAGES;
+      if (c >= STAGES && !mbar_wait(&empty[s], ((c / STAGES) - 1) & 1)) {
+        atomicOr(err, 1);
+        fail = 1;
+        break;
+      }
+      unsigned char* st = sm + s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      bulk_g2s(st, a0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
+      bulk_g2s(st + BLOCK_BYTES, b0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idp = idesc_tf32(false), idn = idesc_tf32(true);
+    const uint32_t dr = tmem, di = tmem + TILE;
+    bool first = true;
+    for (int c = 0; c < nchunks; c++) {
+      const int s = c % STAGES;
+      if (!mbar_wait(&full[s], (c / STAGES) & 1)) {
+        atomicOr(err, 2);
+        fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t sa = smem_u32(sm + s * STAGE_BYTES), sb = sa + BLOCK_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < KC / 8; ks++) {
+        const uint32_t o = ks * 2 * 2048;  // two 4-element core columns per MMA of K = 8
+        const uint64_t arh = smem_desc(sa + o), arl = smem_desc(sa + PLANE_BYTES + o);
+        const uint64_t aih = smem_desc(sa + 2 * PLANE_BYTES + o), ail = smem_desc(sa + 3 * PLANE_BYTES + o);
+        const uint64_t brh = smem_desc(sb + o), brl = smem_desc(sb + PLANE_BYTES + o);
+        const uint64_t bih = smem_desc(sb + 2 * PLANE_BYTES + o), bil = smem_desc(sb + 3 * PLANE_BYTES + o);
+        // Re += Ar Br - Ai Bi
+        mma_tf32(dr, arh, brh, idp, !first);
+        mma_tf32(dr, arh, brl, idp, true);
+        mma_tf32(dr, arl, brh, idp, true);
+        mma_tf32(dr, aih, bih, idn, true);
+        mma_tf32(dr, aih, bil, idn, true);
+        mma_tf32(dr, ail, bih, idn, true);
+        // Im += Ar Bi + Ai Br
+        mma_tf32(di, arh, bih, idp, !first);
+        mma_tf32(di, arh, bil, idp, true);
+        mma_tf32(di, arl, bih, idp, true);
+        mma_tf32(di, aih, brh, idp, true);
+        mma_tf32(di, aih, brl, idp, true);
+        mma_tf32(di, ail, brh, idp, true);
+        first = false;
+      }
+      mma_commit(&empty[s]);
+    }
+    // arrives once every MMA issued above has completed
+    mma_commit(done);
+  }
+  __syncwarp();
+  const bool ok = mbar_wait(done, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (!ok) atomicOr(err, 4);
+  __syncthreads();
+  if (ok && !fail) {
+    // eight warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows of C) for the column
+    // half w / 4, so twice the loads are in flight
+    const int wl = warp & 3, half = warp >> 2;
+    const int row = mt * TILE + wl * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+#pragma unroll 1
+    for (int j0 = half * (TILE / 2); j0 < (half + 1) * (TILE / 2); j0 += 32) {
+      uint32_t vr[32], vi[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]),
+            "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]),
+            "=r"(vr[14]), "=r"(vr[15]), "=r"(vr[16]), "=r"(vr[17]), "=r"(vr[18]), "=r"(vr[19]), "=r"(vr[20]),
+            "=r"(vr[21]), "=r"(vr[22]), "=r"(vr[23]), "=r"(vr[24]), "=r"(vr[25]), "=r"(vr[26]), "=r"(vr[27]),
+            "=r"(vr[28]), "=r"(vr[29]), "=r"(vr[30]), "=r"(vr[31])
+          : "r"(lane_base + j0));
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]),
+            "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]),
+            "=r"(vi[14]), "=r"(vi[15]), "=r"(vi[16]), "=r"(vi[17]), "=r"(vi[18]), "=r"(vi[19]), "=r"(vi[20]),
+            "=r"(vi[21]), "=r"(vi[22]), "=r"(vi[23]), "=r"(vi[24]), "=r"(vi[25]), "=r"(vi[26]), "=r"(vi[27]),
+            "=r"(vi[28]), "=r"(vi[29]), "=r"(vi[30]), "=r"(vi[31])
+          : "r"(lane_base + TILE + j0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < m) {
+        // 32 loads of C first, then their stores: independent requests in flight
+        const int ncol = min(32, n - (nt * TILE + j0));
+        float* pr = Cr + (size_t)(nt * TILE + j0) * ldc + row;
+        float* pi = Ci + (size_t)(nt * TILE + j0) * ldc + row;
+#pragma unroll
+        for (int h = 0; h < 32; h += 16) {
+          float cr[16], ci[16];
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            if (h + j < ncol) {
+              cr[j] = pr[(size_t)(h + j) * ldc];
+              ci[j] = pi[(size_t)(h + j) * ldc];
+            }
+#pragma unroll
+          for (int j = 0; j < 16; j++)
+            if (h + j < ncol) {
+              pr[(size_t)(h + j) * ldc] = cr[j] - __uint_as_float(vr[h + j]);
+              pi[(size_t)(h + j) * ldc] = ci[j] - __uint_as_float(vi[h + j]);
+            }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+}
+
+// Host side: number of 128-row tiles and 16-wide K chunks of an operand.
+inline int tiles(int rows) { return (rows + TILE - 1) / TILE; }
+inline int chunks(int K) { return (K + KC - 1) / KC; }
+inline size_t tiled_bytes(int rows, int K) { return (size_t)tiles(rows) * chunks(K) * BLOCK_BYTES; }
+
+size_t tiled_bytes_host(int rows, int K) { return tiled_bytes(rows, K); }
+
+int tile_operand(const float* sr, const float* si, size_t ld, int rows, int K, bool trans, char* out,
+                 cudaStream_t st) {
+  dim3 g(TILE * KC / 256, chunks(K), tiles(rows));
+  k_tile<<<g, 256, 0, st>>>(sr, si, ld, rows, K, trans ? 1 : 0, chunks(K), out);
+  count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+// C (m x n, planes Cr / Ci, leading dimension ldc) -= A B from pre-tiled operands.
+int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, size_t ldc, int m, int n,
+                int* d_err, cudaStream_t st) {
+  SIE_CUDA(raise_smem(k_gemm, SMEM_BYTES));
+  dim3 g(tiles(m), tiles(n));
+  k_gemm<<<g, 256, SMEM_BYTES, st>>>(At, Bt, chunks(K), Cr, Ci, ldc, m, n, d_err);
+  count_launch();
+  SIE_CUDA(cudaGetLastError());
+  return SIE_OK;
+}
+
+}  // namespace tc
+}  // namespace sie

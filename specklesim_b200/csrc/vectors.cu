@@ -59,10 +59,12 @@ __global__ void k_phase(double h, zc k1, zc k2, const double* khat, int Q, zc* u
   }
 }
 
-int phase_tables(sie_ctx* c, Level& L, int l) {
+// Shift tables of level l's boxes from and to their parents, on the parent's sampling
+// (khat_parent, Qp directions).
+int phase_tables(sie_ctx* c, Level& L, int l, const double* khat_parent, int Qp) {
   double h = ldexp(1.0, -(l + 1)) * c->D;
-  dim3 g((c->Q + 127) / 128, 8);
-  k_phase<<<g, 128, 0, c->stream>>>(h, c->mt.k1, c->mt.k2, c->d_khat, c->Q, L.ph_up, L.ph_dn); sie::count_launch();
+  dim3 g((Qp + 127) / 128, 8);
+  k_phase<<<g, 128, 0, c->stream>>>(h, c->mt.k1, c->mt.k2, khat_parent, Qp, L.ph_up, L.ph_dn); sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
 }

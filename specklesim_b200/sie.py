@@ -37,7 +37,7 @@ def quadrature_rule(ngp):
 class Sie:
     def __init__(self, verts, tris, wavelength, eps_r2, eps_r1=1.0, formulation="ICTF", ngp=3,
                  tree_s_opt=250, truncation_number=19, normal_convention=2, fix_itbn=False,
-                 device=0, dense=False):
+                 device=0, dense=False, level_truncation=None):
         lib = _lib.load()
         cfg = SieConfig()
         lib.sie_config_default(C.byref(cfg))
@@ -66,6 +66,12 @@ class Sie:
         self.l_min, self.l_max = l0.value, l1.value
         self.near_nnz = nnz.value
         self._setup = False
+        if level_truncation:
+            # {level: K}: truncation number per MLFMM level (others keep truncation_number)
+            kl = np.zeros(max(level_truncation) + 1, np.int32)
+            for l, k in level_truncation.items():
+                kl[l] = int(k)
+            check(lib.sie_set_level_truncation(self._h, iptr(kl), len(kl)))
 
     # --- set-up -----------------------------------------------------------
     def setup(self):
@@ -181,6 +187,40 @@ class Sie:
         x = x.T
         return x[:, 0] if b.ndim == 1 else x
 
+    def set_preconditioner(self, kind="near"):
+        """Preconditioner of later solves: "near" (near-field restricted additive Schwarz,
+        applied on the right) or None."""
+        kinds = {None: _lib.SIE_PRECOND_NONE, "none": _lib.SIE_PRECOND_NONE, "near": _lib.SIE_PRECOND_NEAR}
+        check(self._lib.sie_set_preconditioner(self._h, kinds[kind]))
+        return self
+
+    def precondition_right(self, v1):
+        """P v1 with the preconditioner of set_preconditioner."""
+        v1 = _lib.as_c128(v1)
+        v2 = np.zeros_like(v1)
+        check(self._lib.sie_precondition_right(self._h, dptr(v1.view(np.float64)), dptr(v2.view(np.float64))))
+        return v2
+
+    def solve_direct_mixed(self, b, tolerance=1e-10, max_refinements=30, raise_on_noconv=True):
+        """Direct solve with a complex64 tensor-core LU and FP64 iterative refinement
+        (context made with dense=True); returns the currents and the per-vector stats."""
+        b = _lib.as_c128(b)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bb = np.ascontiguousarray(b.reshape(self.n, nrhs).T)
+        x = np.zeros_like(bb)
+        stats = (SieStats * nrhs)()
+        code = self._lib.sie_solve_direct_mixed(self._h, dptr(bb.view(np.float64)), dptr(x.view(np.float64)), nrhs,
+                                                float(tolerance), int(max_refinements), stats)
+        if code != _lib.SIE_OK and not (code == _lib.SIE_ERR_NOCONV and not raise_on_noconv):
+            check(code)
+        st = [{f: getattr(s, f) for f, _ in SieStats._fields_} for s in stats]
+        x = x.T
+        return (x[:, 0], st[0]) if b.ndim == 1 else (x, st)
+
+    def release_factors(self):
+        """Drop the kept LU factors (the next direct solve factorises again)."""
+        check(self._lib.sie_release_factors(self._h))
+
     def precondition_left(self, v1):
         v1 = _lib.as_c128(v1)
         v2 = np.zeros_like(v1)
@@ -241,10 +281,11 @@ class Sie:
         return out
 
     def timings(self):
-        v = np.zeros(12)
-        check(self._lib.sie_get_timings(self._h, dptr(v), 12))
+        v = np.zeros(14)
+        check(self._lib.sie_get_timings(self._h, dptr(v), 14))
         keys = ["fill_ms", "rt_tl_ms", "setup_ms", "mv_total_ms", "mv_near_ms", "mv_agg_ms",
-                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step", "graph_replays"]
+                "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step", "graph_replays",
+                "precond_ms", "lu_factor_ms"]
         return dict(zip(keys, v))
 
     def close(self):
