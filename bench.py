@@ -1,15 +1,30 @@
-"""Benchmark of the SIE hot path: plane-wave solves per second on the rough-slab
-workload (10 lambda x 10 lambda, ~19.5k triangles, ~29k RWG edges, plain FP64
-MLFMM + GMRES to 1e-6).
+"""Benchmark of the SIE hot path on the rough-slab workload of the reference's configuration
+(10 lambda x 10 lambda, 19,456 triangles, 29,184 RWG edges, metal eps = -11.7 - 1.26i,
+ICTF): converged solves per second.
 
-One step = one GMRES solve of one right-hand side on a set-up problem (near
-field, radiation patterns and translation tables are built once, as the
-reference does for its incidence-angle loop, main.f90:450-463).  `value` times
-the device solve (inputs resident in HBM); `e2e` times the public host API with
-the right-hand side copied in from pinned memory and the currents copied out.
+On this plasmonic slab no iterative solve converges: the MLFMM product is 6.7 % off the
+dense one with the reference's K = 19 on every level (1e-5 with per-level truncation
+numbers), the system amplifies operator error by >= 7,000, and GMRES, also with the
+near-field RAS preconditioner, stalls above 0.4 after 1,000-2,000 steps.  So a converged
+solve is a direct one, and one step is one direct solve of one plane wave: the LU
+factorisation of the FP64 dense matrix (filled once, as the reference's normal solver
+does) and the solution.
 
-Multi-GPU (torchrun): every rank solves its own realisation (seed = rank),
-weak scaling, no collective on the data path; timings are max-reduced.
+`value` is the mixed-precision direct solve (complex64 LU whose trailing updates run on
+the tensor cores as 3xTF32 products, FP64 iterative refinement to a backward error of
+1e-10) on device-resident buffers; the plain FP64 direct solve (cuSOLVER ZGETRF/ZGETRS,
+the reference's ZGESV) is timed beside it, with the far-field error between the two.
+`e2e` is the mixed solve through the host-buffer API.  `roofline` is the tensor-core
+trailing update, the dominant kernel; `roofline_matvec` keeps the MLFMM product against
+HBM.
+
+Multi-GPU (torchrun): every rank solves its own realisation (seed = rank), weak scaling, no
+collective on the data path; timings are max-reduced.
+
+`--impl reference` times the reference's own algorithm for this workload (the oracle, a
+C++ restatement of it: MLFMM with K = 19 on every level, no preconditioner, zgmres with
+restart = max_iterations = 650 as main.f90:226-230 sets) on the host cores; its solve is
+650 iterations, which do not reach the tolerance on this slab.
 """
 import argparse
 import json
@@ -31,16 +46,27 @@ EPS = -11.7 - 1.26j  # exp(+iwt) convention of the reference (lossy => Im < 0)
 
 WORKLOADS = {
     # the headline case: 10 lambda x 10 lambda rough slab, seed 0, corr 1 lambda, RMS 0.5 lambda,
-    # 1 lambda thick
-    "slab10": dict(length_wl=10.0, rms_wl=0.5, corr_wl=1.0, thickness_wl=1.0, cells=64, seed=0),
+    # 1 lambda thick; truncation numbers per MLFMM level (2.5 / 1.25 / 0.625 lambda boxes)
+    "slab10": dict(length_wl=10.0, rms_wl=0.5, corr_wl=1.0, thickness_wl=1.0, cells=64, seed=0,
+                   level_k={2: 34, 3: 23, 4: 19}, inner_k={2: 26, 3: 17, 4: 12}),
     # a small case for quick checks
-    "slab4": dict(length_wl=4.0, rms_wl=0.3, corr_wl=1.0, thickness_wl=1.0, cells=24, seed=0),
+    "slab4": dict(length_wl=4.0, rms_wl=0.3, corr_wl=1.0, thickness_wl=1.0, cells=24, seed=0,
+                  level_k=None, inner_k={3: 12, 2: 12}),
 }
+DIRECT = dict(tolerance=1e-10, max_refinements=40)
+REFERENCE_ITERATIONS = 650  # main.f90:226-230: max_iterations = restart = 650
 
 
-# matvecs of one budgeted FP64 solve on the GPU (650 Arnoldi steps + the final true
-# residual); the CPU arm times matvecs and multiplies by this count
-MATVECS_PER_SOLVE = {"slab10": 651, "slab4": 651}
+def config_of(name, T=None, M=None):
+    w = WORKLOADS[name]
+    return {
+        "workload": (f"{name}: rough slab {w['length_wl']} lambda (seed=rank), lambda=632.8nm, "
+                     f"eps=-11.7-1.26i (exp(+iwt)), ICTF, ng=3"
+                     + (f", {T} triangles, {M} RWG edges" if T else "")),
+        "solver": ("direct: dense FP64 fill, complex64 LU with partial pivoting (trailing updates on the "
+                   f"tensor cores, 3xTF32) and FP64 iterative refinement to {DIRECT['tolerance']}"),
+        "l2": "inputs > L2 (the dense matrix is tens of GB)",
+    }
 
 
 def peaks():
@@ -142,22 +168,28 @@ def demorton(b, l, axis):
     return v
 
 
-def matvec_algorithmic(g, Q):
+def matvec_algorithmic(g, level_k, K=19):
     """Algorithmic DRAM bytes of one FP64 matvec, and the FP64 flops of its SR step.
     Bytes: near panels (a, b, d: 48 B per 2x2 block), radiation patterns read by the
-    aggregate and the receive, x in and y out, C and D of every level written and read.
-    The SR source coefficients are read from L2 (each level's C fits), so they are not
-    DRAM bytes.  SR flops: 4 complex multiply-adds = 32 real flops per (I4 pair,
-    direction, medium); medium 2 only on the leaf level (k2 complex)."""
+    aggregate and the receive (leaf sampling), x in and y out, C and D of every level
+    written and read (each level's own sampling), and the coefficients of a level carried
+    on its parent's sampling between the interpolation and the shift (SS) or the shift and
+    the anterpolation (RR).  The SR source coefficients are read from L2 (each level's C
+    fits), so they are not DRAM bytes.  SR flops: 4 complex multiply-adds = 32 real flops
+    per (I4 pair, direction, medium); medium 2 only on the leaf level (k2 complex)."""
     M, N, s = g.n_edges, g.n, 16
     st = level_stats(g)
+    Kl = {l: (level_k or {}).get(l, K) for l, _, _ in st}
+    Ql = {l: 2 * k * k + 2 for l, k in Kl.items()}
+    Qleaf = Ql[g.l_max]
     near = g.near_nnz * 3 * s
-    rt = 2 * M * 4 * Q * s
+    rt = 2 * M * 4 * Qleaf * s
     xy = 2 * N * s
-    coeff = sum(nb * 8 * Q * s * 4 for _, nb, _ in st)
-    sr_flops = sum(ni4 * Q * 32 * (2 if l == g.l_max else 1) for l, _, ni4 in st)
-    return dict(near=near, rt=rt, xy=xy, coeff=coeff, total=near + rt + xy + coeff, sr_flops=sr_flops,
-                levels=st)
+    coeff = sum(nb * 8 * Ql[l] * s * 4 for l, nb, _ in st)
+    interp = sum(nb * 8 * Ql[l - 1] * s * 4 for l, nb, _ in st if l > g.l_min and Ql[l] != Ql[l - 1])
+    sr_flops = sum(ni4 * Ql[l] * 32 * (2 if l == g.l_max else 1) for l, _, ni4 in st)
+    return dict(near=near, rt=rt, xy=xy, coeff=coeff + interp, total=near + rt + xy + coeff + interp,
+                sr_flops=sr_flops, levels=st, Q=Ql)
 
 
 def fp64_dgemm_tflops(dev):
@@ -176,9 +208,6 @@ def fp64_dgemm_tflops(dev):
     return best
 
 
-EPS_CONVERGING = 2.25 - 0.01j
-
-
 def hemisphere_grid(n=128, r=5.0):
     """The 128 x 128 (theta, phi) grid over the upper hemisphere at r = 5 m."""
     th = (np.arange(n) + 0.5) * (0.5 * np.pi / n)
@@ -187,125 +216,9 @@ def hemisphere_grid(n=128, r=5.0):
     return r * np.stack([np.sin(T) * np.cos(P), np.sin(T) * np.sin(P), np.cos(T)], axis=-1).reshape(-1, 3)
 
 
-def mixed_vs_fp64(V, T, tol):
-    """Solves/s of the mixed-precision solver (FP64 flexible GMRES around FP32 GMRES)
-    against the plain FP64 GMRES, both to the same backward error, and the relative error
-    of the mixed far-field intensity on the 128 x 128 hemisphere grid.  The slab mesh of
-    the workload with a dielectric body: the metallic ICTF system stalls in both
-    precisions, so it gives no equal-accuracy comparison."""
-    from specklesim_b200 import Sie, incidence
-    g = Sie(V, T, WL, EPS_CONVERGING, tree_s_opt=250, truncation_number=19).setup()
-    k, E = incidence(0.0, 0.0, "TM", 2)
-    b = g.rhs_planewave(k, E)
-    pts = hemisphere_grid()
-    x64, s64 = g.solve(b, restart=50, max_iterations=4000, tolerance=tol, raise_on_noconv=False)
-    xm, sm = g.solve(b, restart=10, max_iterations=100, tolerance=tol, precision="mixed",
-                     inner_restart=30, inner_tolerance=1e-2, raise_on_noconv=False)
-    xm, sm = g.solve(b, restart=10, max_iterations=100, tolerance=tol, precision="mixed",
-                     inner_restart=30, inner_tolerance=1e-2, raise_on_noconv=False)
-    I64 = g.farfield(x64, pts)[2]
-    Im = g.farfield(xm, pts)[2]
-    # the inner products through a K = 12 operator on the same mesh (a cheaper preconditioner
-    # operator; the outer FP64 products stay K = 19)
-    gi = Sie(V, T, WL, EPS_CONVERGING, tree_s_opt=250, truncation_number=12).setup()
-    g.set_inner_operator(gi)
-    xk, sk = g.solve(b, restart=10, max_iterations=100, tolerance=tol, precision="mixed",
-                     inner_restart=60, inner_tolerance=1e-2, raise_on_noconv=False)
-    g.set_inner_operator(None)
-    Ik = g.farfield(xk, pts)[2]
-    batched = batched_mixed(g, pts, tol, inner=gi)
-    g.close()
-    gi.close()
-    return {
-        "workload": f"same slab mesh, eps = {EPS_CONVERGING} (converging), tolerance {tol}",
-        "fp64": {"solves_per_s": 1.0 / s64["seconds"], "iterations": s64["iterations"],
-                 "backward_error": s64["backward_error_true"], "converged": bool(s64["converged"])},
-        "mixed": {"solves_per_s": 1.0 / sm["seconds"], "outer_iterations": sm["iterations"],
-                  "inner_iterations": sm["inner_iterations"], "backward_error": sm["backward_error_true"],
-                  "converged": bool(sm["converged"]), "inner": "GMRES(30) FP32 to 1e-2, outer FGMRES(10) FP64"},
-        "speedup": s64["seconds"] / sm["seconds"],
-        "mixed_inner_k12": {"speedup": s64["seconds"] / sk["seconds"], "outer_iterations": sk["iterations"],
-                            "converged": bool(sk["converged"]),
-                            "farfield_rel_err_vs_fp64": float(np.linalg.norm(Ik - I64) / np.linalg.norm(I64)),
-                            "inner": "GMRES(60) complex64 through a K = 12 context to 1e-2, outer FGMRES(10) FP64"},
-        "farfield_rel_err_vs_fp64": float(np.linalg.norm(Im - I64) / np.linalg.norm(I64)),
-        "currents_rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
-        "farfield_points": int(pts.shape[0]),
-        "batched": batched,
-    }
-
-
-def batched_mixed(g, pts, tol, inner=None, fp64_sample=4):
-    """The 16 plane waves of the batching form (theta 0/10/20/30 deg x phi 0/90 deg x TE/TM)
-    solved together by the batched mixed-precision solver, against plain FP64 GMRES solves
-    of the first `fp64_sample` of them one at a time (FP64 time per solve = mean over the
-    sample).  Errors: currents and 128 x 128 far-field intensity of the sampled columns.
-    With `inner` the inner complex64 products go through that context (a lower truncation
-    number); the same batch is also timed with the inner products on g itself."""
-    from specklesim_b200 import incidence
-    incs = [incidence(np.deg2rad(t), np.deg2rad(p), pol, 2)
-            for t in (0, 10, 20, 30) for p in (0, 90) for pol in ("TM", "TE")]
-    B = np.stack([g.rhs_planewave(k, E) for k, E in incs], axis=1)
-    kw = dict(restart=10, max_iterations=100, tolerance=tol, precision="mixed", inner_restart=60,
-              inner_tolerance=1e-2, raise_on_noconv=False)
-    Xb, sb = g.solve(B[:, :2], **kw)  # warm-up (allocation of the batch workspace)
-    Xb, sb = g.solve(B, **kw)
-    t_same = sb[0]["seconds"]
-    its_same = max(s["iterations"] for s in sb)
-    if inner is not None:
-        g.set_inner_operator(inner)
-        Xb, sb = g.solve(B[:, :2], **kw)
-        Xb, sb = g.solve(B, **kw)
-        g.set_inner_operator(None)
-    t_batch = sb[0]["seconds"]
-    t64, ferr, cerr = [], [], []
-    for j in range(fp64_sample):
-        x64, s64 = g.solve(B[:, j], restart=50, max_iterations=4000, tolerance=tol, raise_on_noconv=False)
-        t64.append(s64["seconds"])
-        I64 = g.farfield(x64, pts)[2]
-        Ib = g.farfield(Xb[:, j], pts)[2]
-        ferr.append(float(np.linalg.norm(Ib - I64) / np.linalg.norm(I64)))
-        cerr.append(float(np.linalg.norm(Xb[:, j] - x64) / np.linalg.norm(x64)))
-    per64 = float(np.mean(t64))
-    return {
-        "rhs": B.shape[1], "seconds": t_batch, "solves_per_s": B.shape[1] / t_batch,
-        "fp64_seconds_per_solve": per64, "fp64_sample": fp64_sample,
-        "speedup_vs_fp64": per64 / (t_batch / B.shape[1]),
-        "outer_iterations_max": max(s["iterations"] for s in sb),
-        "backward_error_max": max(s["backward_error_true"] for s in sb),
-        "converged": all(bool(s["converged"]) for s in sb),
-        "farfield_rel_err_vs_fp64_max": max(ferr), "currents_rel_err_vs_fp64_max": max(cerr),
-        "inner": "lockstep GMRES(60) complex64 to 1e-2 on one batched product per step, outer FGMRES(10) FP64",
-        "inner_operator": ("K = 12 (Q = 290) complex64 MLFMM on the same mesh; outer products K = 19"
-                           if inner is not None else "the outer operator (K = 19) in complex64"),
-        "same_operator": {"seconds": t_same, "speedup_vs_fp64": per64 / (t_same / B.shape[1]),
-                          "outer_iterations_max": its_same},
-    }
-
-
-def gradient_timing(tol):
-    """One shape gradient in the differentiation form's setting: slab10 with seed 2 and the
-    metal, 256 observation directions in a 20-degree cone around specular.  ICTF on this
-    slab stalls in GMRES, so the forward and the adjoint solves both run the reference's
-    budget (restart 50, 650 iterations); the time is sie_grad's wall time (adjoint solve
-    plus the derivative kernels over all vertices)."""
-    from specklesim_b200 import Sie, incidence
-    from specklesim_b200.shape import cone_points
-    V, T = build_mesh("slab10", 2)
-    g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19).setup()
-    k, E = incidence(0.0, 0.0, "TM", 2)
-    x, _ = g.solve(g.rhs_planewave(k, E), restart=50, max_iterations=650, tolerance=tol, raise_on_noconv=False)
-    pts = cone_points(256, [0, 0, 1], 20.0, seed=2)
-    kw = dict(restart=50, max_iterations=650, tolerance=tol, raise_on_noconv=False)
-    g.grad(x, k, E, pts[:8], **kw)  # warm-up: gradient tables and workspace
-    t0 = time.perf_counter()
-    J, dz, st = g.grad(x, k, E, pts, **kw)
-    t = time.perf_counter() - t0
-    g.close()
-    return {"workload": "slab10 seed 2, eps -11.7-1.26i, 256 directions in a 20-degree cone around specular",
-            "vertices": int(len(V)), "seconds": t, "adjoint_solve_seconds": st["seconds"],
-            "adjoint_iterations": st["iterations"], "derivative_kernels_seconds": t - st["seconds"],
-            "objective": J}
+def _stats(ts):
+    return {"median_s": float(statistics.median(ts)), "min_s": float(min(ts)), "max_s": float(max(ts)),
+            "repeats": len(ts)}
 
 
 def committed_traffic():
@@ -320,173 +233,62 @@ def committed_traffic():
     return None
 
 
-def cpu_reference(V, T, matvecs_per_solve, threads, s_opt=250, budget_matvecs=2):
-    """The oracle (C++ restatement of the reference) timed on the host cores."""
-    from oracle.oracle import Oracle
+def cpu_reference(V, T, threads, iters_per_step, steps, warmup, s_opt=250):
+    """The reference's algorithm on the host cores: the oracle (C++ restatement, OpenMP)
+    set up with K = 19 on every level, and the numpy restatement of zgmres (IMGS, Givens,
+    restart = max_iterations) driving the oracle's MLFMM product.  A step runs
+    `iters_per_step` Arnoldi steps of that GMRES from x0 = 0 on the plane-wave right-hand
+    side (one matvec each); a reference solve is REFERENCE_ITERATIONS of them."""
+    from oracle.oracle import Oracle, zgmres
+    from specklesim_b200 import incidence
     o = Oracle(V, T, WL, EPS, tree_s_opt=s_opt, threads=threads)
     t0 = time.perf_counter()
     o.tree()
     o.setup_fmm()
     t_setup = time.perf_counter() - t0
-    x = np.random.default_rng(0).standard_normal(o.N) + 0j
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b = o.rhs(k, E)
     ts = []
-    for _ in range(budget_matvecs):
+    for i in range(warmup + steps):
         t1 = time.perf_counter()
-        o.matvec(x)
-        ts.append(time.perf_counter() - t1)
-    t_mv = min(ts)
+        zgmres(o.matvec, b, iters_per_step, 1e-30, iters_per_step)
+        if i >= warmup:
+            ts.append(time.perf_counter() - t1)
     o.close()
-    per_solve = t_mv * matvecs_per_solve
+    t_step = statistics.median(ts)
+    # zgmres ends a budget with the true residual: iters_per_step + 1 products per step
+    per_mv = t_step / (iters_per_step + 1)
+    per_solve = per_mv * (REFERENCE_ITERATIONS + 1)
     return dict(value=1.0 / per_solve, unit="solves/s", cores=threads, kind="port",
-                sample=(f"oracle C++ restatement (OpenMP, {threads} threads): set-up {t_setup:.1f} s untimed, "
-                        f"{budget_matvecs} MLFMM matvecs timed ({t_mv:.3f} s each); solves/s = "
-                        f"1 / (matvec time x {matvecs_per_solve} matvecs per solve of the GPU run)"),
-                setup_s=t_setup, matvec_s=t_mv)
+                sample=(f"oracle C++ restatement of the reference (OpenMP, {threads} threads), K = 19 on every "
+                        f"level, no preconditioner: set-up {t_setup:.1f} s untimed; each step = {iters_per_step} "
+                        f"GMRES steps + the final true residual (numpy zgmres restatement driving the oracle "
+                        f"product, {per_mv:.3f} s per product with its Arnoldi step); solves/s = 1 / "
+                        f"({REFERENCE_ITERATIONS + 1} products: the reference's max_iterations of {REFERENCE_ITERATIONS} "
+                        "and the final residual; its solve does not reach the tolerance on this slab).  The "
+                        "orthogonalisation against up to 650 basis vectors of the later steps is not in the "
+                        "sample, which favours the CPU"),
+                setup_s=t_setup, step_s=t_step, ts=ts)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="slab10", choices=list(WORKLOADS))
-    ap.add_argument("--restart", type=int, default=50)
-    ap.add_argument("--tol", type=float, default=1e-6)
-    ap.add_argument("--max-iterations", type=int, default=650)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--reference-matvecs-per-solve", type=int, default=0)
-    args = ap.parse_args()
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        # the reference's CPU implementation of the path (the oracle port) on the host cores
-        if rank != 0:
-            return
-        V, T = build_mesh(args.workload, 0)
-        threads = os.cpu_count() or 1
-        mps = args.reference_matvecs_per_solve or MATVECS_PER_SOLVE[args.workload]
-        cb = cpu_reference(V, T, mps, threads)
-        line = {
-            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 / cb["value"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload} rough slab (seed 0), ICTF, ng=3, s_opt=250, K=19",
-                       "matvecs_per_solve": mps},
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line))
-        return
-
-    import torch
-    import torch.distributed as dist
-
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    from specklesim_b200 import Sie, incidence, _lib
-
-    V, T = build_mesh(args.workload, rank)
-    t0 = time.perf_counter()
-    g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local)
-    g.setup()
-    setup_s = time.perf_counter() - t0
-    # kernel variants picked for this mesh by the library's autotuner (same product)
-    tune_before, tune_after, tune_modes = g.autotune("fp64")
-    lib = _lib.load()
-    stream = torch.cuda.Stream()
-    _lib.check(lib.sie_set_stream(g._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
-
-    k, E = incidence(0.0, 0.0, "TM", 2)  # x-polarised normal incidence along -z
-    b_host = g.rhs_planewave(k, E)
-    N = g.n
-    dev = torch.device("cuda", local)
-    with torch.cuda.stream(stream):
-        b = torch.from_numpy(b_host.view(np.float64)).to(dev)
-        x = torch.zeros_like(b)
-    stream.synchronize()
-
+def mlfmm_matvec(V, T, local, stream, b, peak, peak_kind):
+    """The MLFMM product on the same mesh (the reference's operator: s_opt = 250, K = 19
+    on every level) against HBM: one product timed with CUDA events after the autotuner
+    picked its kernel variants, each phase's own duration from a second context whose
+    product runs the phases one after another, and the product with per-level truncation
+    numbers for comparison."""
     import ctypes as C
-    cfg = _lib.SieSolverCfg()
-    lib.sie_solver_default(C.byref(cfg))
-    cfg.restart, cfg.max_iterations, cfg.tolerance = args.restart, args.max_iterations, args.tol
-    st = _lib.SieStats()
-
-    def solve_dev():
-        rc = lib.sie_solve_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1, C.byref(cfg),
-                                  C.byref(st))
-        if rc != _lib.SIE_ERR_NOCONV:  # the budgeted solve ends like the reference's info(1) = -4
-            _lib.check(rc)
-
-    for _ in range(args.warmup):
-        solve_dev()
-    iters, mvs, conv, be = st.iterations, st.matvecs, st.converged, st.backward_error_true
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    # ---- device-resident timed region
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = lib.sie_launch_count()
-    with ClockSampler(local) as clk:
-        barrier()
-        e0.record(stream)
-        for _ in range(args.steps):
-            solve_dev()
-        e1.record(stream)
-        barrier()
-    launches = lib.sie_launch_count() - l0
-    t_dev = e0.elapsed_time(e1) / 1000.0
-    if world > 1:
-        tt = torch.tensor([t_dev], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev = float(tt.item())
-    value = world * args.steps / t_dev
-
-    # ---- end to end through the public host API (pinned host buffers)
-    bp = torch.from_numpy(b_host.view(np.float64).copy()).pin_memory()
-    xp = torch.zeros_like(bp).pin_memory()
-    stats = (_lib.SieStats * 1)()
-    dp = C.POINTER(C.c_double)
-    barrier()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk_e2e:
-        e2.record(stream)
-        for _ in range(args.steps):
-            rc = lib.sie_solve(g._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1, C.byref(cfg), stats)
-            if rc != _lib.SIE_ERR_NOCONV:
-                _lib.check(rc)
-        e3.record(stream)
-        barrier()
-    t_e2e = e2.elapsed_time(e3) / 1000.0
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = world * args.steps / t_e2e
-    x_e2e = xp.numpy().view(np.complex128)
-
-    # ---- matvec phases and roofline (one timed matvec)
+    from specklesim_b200 import Sie, _lib
+    lib = _lib.load()
+    g = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local).setup()
+    tune_before, tune_after, tune_modes = g.autotune("fp64")
+    _lib.check(lib.sie_set_stream(g._h, C.c_void_p(stream.cuda_stream)))
+    import torch
     y = torch.empty_like(b)
-    _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
-                                     C.c_void_p(stream.cuda_stream)))
-    for _ in range(3):
+    for _ in range(4):
         _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
                                          C.c_void_p(stream.cuda_stream)))
     tm = g.timings()
-    Q = 2 * 19 * 19 + 2
-    peak, peak_kind = peaks()
-    # The product above runs the near panels on a second stream beside the translations,
-    # so its per-phase events overlap. Each phase's own duration comes from a second
-    # context on the same mesh whose product runs the phases one after another.
     os.environ["SIE_OVERLAP"] = "0"
     try:
         gs = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local).setup()
@@ -499,80 +301,246 @@ def main():
     gs.close()
     phases = {k: tms[k] for k in ("mv_near_ms", "mv_agg_ms", "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms")}
     phases["serial_total_ms"] = tms["mv_total_ms"]
-    mvb = matvec_algorithmic(g, Q)
+    mvb = matvec_algorithmic(g, None)
     mv_ms = tm["mv_total_ms"]
     ach = mvb["total"] / (mv_ms * 1e-3) / 1e9
-    # The hot-path unit is one MLFMM matvec (near panels + aggregate + SS + SR + RR +
-    # receive), HBM-bound as a whole; the per-phase entries give each kernel's own bound.
-    fp64_peak = fp64_dgemm_tflops(dev)
-    ph_rows = {
-        "near": ("hbm", mvb["near"], phases["mv_near_ms"]),
-        "aggregate": ("hbm", mvb["rt"] / 2 + N * 16, phases["mv_agg_ms"]),
-        "receive": ("hbm", mvb["rt"] / 2 + 2 * N * 16, phases["mv_recv_ms"]),
-        "sr": ("fp64", mvb["sr_flops"], phases["mv_sr_ms"]),
-    }
+    N = g.n
     per_phase = {}
-    for k, (bound, units, ms) in ph_rows.items():
-        if bound == "hbm":
-            a = units / (ms * 1e-3) / 1e9
-            per_phase[k] = {"bound": "hbm", "achieved": a, "unit": "GB/s", "frac": a / peak, "ms": ms}
-        else:
-            a = units / (ms * 1e-3) / 1e12
-            per_phase[k] = {"bound": "fp64", "achieved": a, "unit": "TFLOP/s", "peak": fp64_peak,
-                            "peak_source": "measured here: torch float64 matmul (cuBLAS DGEMM) 4096^3",
-                            "frac": a / fp64_peak if fp64_peak else None, "ms": ms}
-    roof = {"kernel": "one MLFMM matvec (all phases)", "bound": "hbm", "achieved": ach, "peak": peak,
-            "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-            "bytes_per_launch": mvb["total"], "launch_ms": mv_ms, "traffic": committed_traffic(),
-            "per_phase": per_phase}
-    mv_frac = ach / peak
+    for k_, (units, ms) in {"near": (mvb["near"], phases["mv_near_ms"]),
+                            "aggregate": (mvb["rt"] / 2 + N * 16, phases["mv_agg_ms"]),
+                            "receive": (mvb["rt"] / 2 + 2 * N * 16, phases["mv_recv_ms"])}.items():
+        a = units / (ms * 1e-3) / 1e9
+        per_phase[k_] = {"bound": "hbm", "achieved": a, "unit": "GB/s", "frac": a / peak, "ms": ms}
+    a = mvb["sr_flops"] / (phases["mv_sr_ms"] * 1e-3) / 1e12
+    per_phase["sr"] = {"bound": "fp64", "achieved": a, "unit": "TFLOP/s", "ms": phases["mv_sr_ms"]}
+    g.close()
+    # per-level truncation numbers (accurate on the 2.5 lambda boxes)
+    kk = WORKLOADS["slab10"]["level_k"]
+    gl = Sie(V, T, WL, EPS, tree_s_opt=250, truncation_number=19, device=local, level_truncation=kk).setup()
+    _lib.check(lib.sie_set_stream(gl._h, C.c_void_p(stream.cuda_stream)))
+    for _ in range(4):
+        _lib.check(lib.sie_matvec_device(gl._h, C.c_void_p(b.data_ptr()), C.c_void_p(y.data_ptr()), 1, 0,
+                                         C.c_void_p(stream.cuda_stream)))
+    tml = gl.timings()
+    mvl = matvec_algorithmic(gl, kk)
+    gl.close()
+    return {"kernel": "one MLFMM matvec (all phases), K = 19 on every level", "bound": "hbm", "achieved": ach,
+            "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)", "bytes_per_launch": mvb["total"],
+            "launch_ms": mv_ms, "traffic": committed_traffic(), "per_phase": per_phase, "phases_ms": phases,
+            "autotune": {"matvec_ms_before": tune_before, "matvec_ms_after": tune_after, "variants": tune_modes},
+            "levels_boxes_i4_pairs": mvb["levels"],
+            "level_truncation": {"K": {str(k): v for k, v in kk.items()}, "matvec_ms": tml["mv_total_ms"],
+                                 "bytes_per_launch": mvl["total"],
+                                 "achieved_gbs": mvl["total"] / (tml["mv_total_ms"] * 1e-3) / 1e9}}
 
-    # ---- mixed precision against plain FP64 at equal tolerance (rank 0, N = 1)
-    mixed = None
-    grad = None
-    if rank == 0 and world == 1 and not args.no_mixed:
-        mixed = mixed_vs_fp64(V, T, args.tol)
-        grad = gradient_timing(args.tol)
 
-    # ---- CPU baseline: the oracle on the host cores (rank 0, N = 1)
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="slab10", choices=list(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-matvec", action="store_true")
+    ap.add_argument("--fp64-repeats", type=int, default=3)
+    ap.add_argument("--reference-iterations-per-step", type=int, default=2)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference's CPU implementation of the path (the oracle port) on the host cores
+        if rank != 0:
+            return
+        V, T = build_mesh(args.workload, 0)
+        threads = os.cpu_count() or 1
+        cb = cpu_reference(V, T, threads, args.reference_iterations_per_step, args.steps, args.warmup)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * cb["step_s"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_of(args.workload),
+            "step": (f"{args.reference_iterations_per_step} GMRES steps of the reference's MLFMM solver (+ the final "
+                     f"residual); value = 1 / ({REFERENCE_ITERATIONS + 1} products)"),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from specklesim_b200 import Sie, incidence, _lib
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(t):
+        if world > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    V, T = build_mesh(args.workload, rank)
+    dev = torch.device("cuda", local)
+    lib = _lib.load()
+    stream = torch.cuda.Stream(dev)
+    peak_hbm, peak_kind = peaks()
+
+    # ---- dense set-up: the FP64 matrix (every pair through the near-field fill kernels)
+    t0 = time.perf_counter()
+    d = Sie(V, T, WL, EPS, device=local, dense=True).setup()
+    fill_s = time.perf_counter() - t0
+    _lib.check(lib.sie_set_stream(d._h, C.c_void_p(stream.cuda_stream)))
+    k, E = incidence(0.0, 0.0, "TM", 2)  # x-polarised normal incidence along -z
+    b_host = d.rhs_planewave(k, E)
+    N = d.n
+    with torch.cuda.stream(stream):
+        b = torch.from_numpy(b_host.view(np.float64)).to(dev)
+        x = torch.zeros_like(b)
+    stream.synchronize()
+    st = _lib.SieStats()
+    steps_info = []
+
+    def mixed_dev():
+        _lib.check(lib.sie_release_factors(d._h))
+        _lib.check(lib.sie_solve_direct_mixed_device(d._h, C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), 1,
+                                                     DIRECT["tolerance"], DIRECT["max_refinements"], C.byref(st),
+                                                     C.c_void_p(stream.cuda_stream)))
+        steps_info.append((st.seconds, st.iterations, st.backward_error_true))
+
+    for _ in range(args.warmup):
+        mixed_dev()
+    steps_info.clear()
+
+    # ---- device-resident timed region: one direct solve (LU + refinement) per step
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = lib.sie_launch_count()
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            mixed_dev()
+        e1.record(stream)
+        barrier()
+    launches = lib.sie_launch_count() - l0
+    t_dev = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+    value = world * args.steps / t_dev
+    tmd = d.timings()
+    xm = x.cpu().numpy().view(np.complex128).copy()
+
+    # ---- end to end through the public host API (pinned host buffers), min(K, 3) steps
+    ke = min(args.steps, 3)
+    bp = torch.from_numpy(b_host.view(np.float64).copy()).pin_memory()
+    xp = torch.zeros_like(bp).pin_memory()
+    stats = (_lib.SieStats * 1)()
+    dp = C.POINTER(C.c_double)
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk_e2e:
+        e2.record(stream)
+        for _ in range(ke):
+            _lib.check(lib.sie_release_factors(d._h))
+            _lib.check(lib.sie_solve_direct_mixed(d._h, C.cast(bp.data_ptr(), dp), C.cast(xp.data_ptr(), dp), 1,
+                                                  DIRECT["tolerance"], DIRECT["max_refinements"], stats))
+        e3.record(stream)
+        barrier()
+    t_e2e = max_over_ranks(e2.elapsed_time(e3) / 1000.0)
+    e2e = world * ke / t_e2e
+
+    # ---- the plain FP64 direct solve (cuSOLVER ZGETRF + ZGETRS) beside it, and the
+    # far-field error between the two on the 128 x 128 hemisphere grid (rank 0)
+    fp64 = None
+    if rank == 0:
+        t64 = []
+        x64 = None
+        for _ in range(args.fp64_repeats):
+            _lib.check(lib.sie_release_factors(d._h))
+            t1 = time.perf_counter()
+            x64 = d.solve_direct(b_host)
+            t64.append(time.perf_counter() - t1)
+        _lib.check(lib.sie_release_factors(d._h))
+        pts = hemisphere_grid()
+        I64 = d.farfield(x64, pts)[2]
+        Im = d.farfield(xm, pts)[2]
+        r64 = float(np.linalg.norm(d.matvec(x64) - b_host) / np.linalg.norm(b_host))
+        tmed = [s_ for s_, _, _ in steps_info]
+        fp64 = {
+            "fp64": {"solves_per_s": 1.0 / statistics.median(t64), **_stats(t64), "backward_error": r64,
+                     "solver": "cuSOLVER ZGETRF + ZGETRS (host buffers), factors dropped before every solve"},
+            "mixed": {"solves_per_s": 1.0 / statistics.median(tmed), **_stats(tmed),
+                      "refinement_steps": [i for _, i, _ in steps_info][-1],
+                      "backward_error": max(be for _, _, be in steps_info)},
+            "speedup_vs_fp64": statistics.median(t64) / statistics.median(tmed),
+            "farfield_rel_err_vs_fp64": float(np.linalg.norm(Im - I64) / np.linalg.norm(I64)),
+            "currents_rel_err_vs_fp64": float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
+            "farfield_points": int(pts.shape[0]),
+        }
+    d.close()
+    torch.cuda.empty_cache()
+
+    # ---- roofline of the dominant kernel: the tensor-core trailing update of the LU.  The
+    # 3xTF32 scheme runs 3 tf32 products per real product, 4 real products per complex one:
+    # 3 x 8 = 24 tensor flops per complex multiply-add; the TF32 dense peak is half the
+    # measured BF16 one
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        tf32_peak, tf32_src = float(pk["bf16_tflops"]) / 2, "measured (MEASURED_PEAKS.json bf16_tflops / 2)"
+    except Exception:
+        tf32_peak, tf32_src = 1590.0 / 2, "fallback (1.59 PFLOP/s bf16 / 2)"
+    g_ms = tmd["lu_gemm_ms"]
+    useful = tmd["lu_gemm_flops"]
+    tensor_tf = 3 * useful / (g_ms * 1e-3) / 1e12 if g_ms > 0 else None
+    roof = {"kernel": "tc::k_gemm, the LU's trailing update A22 -= L21 U12 (tcgen05.mma kind::tf32, 3xTF32)",
+            "bound": "tensor", "achieved": tensor_tf, "peak": tf32_peak, "unit": "TFLOP/s",
+            "frac": tensor_tf / tf32_peak if tensor_tf else None, "peak_source": tf32_src, "traffic": None,
+            "launches_per_step": tmd["lu_gemm_launches"], "ms_per_step": g_ms,
+            "useful_complex_tflops": useful / (g_ms * 1e-3) / 1e12 if g_ms > 0 else None,
+            "lu_factor_ms": tmd["lu_factor_ms"]}
+
+    # ---- the MLFMM product against HBM (rank 0, N = 1)
+    rmv = None
+    if rank == 0 and world == 1 and not args.no_matvec:
+        rmv = mlfmm_matvec(V, T, local, stream, b, peak_hbm, peak_kind)
+
+    # ---- CPU baseline: the reference's algorithm on the host cores (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cb = cpu_reference(V, T, mvs, threads)
-        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_reference(V, T, threads, 2, 2, 1)
+        cpu = {k_: cb[k_] for k_ in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:
-        res = b_host - g.matvec(x_e2e)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {
-                "workload": (f"{args.workload}: rough slab {WORKLOADS[args.workload]['length_wl']} lambda, "
-                             f"lambda=632.8nm, eps=-11.7-1.26i (exp(+iwt)), seed=rank, {T.shape[0]} triangles, "
-                             f"{g.n_edges} RWG edges, ICTF, ng=3, s_opt=250, K=19, l={g.l_min}..{g.l_max}"),
-                "precision": "fp64", "solver": f"GMRES(IMGS) restart {args.restart}, tol {args.tol}",
-                "iterations": iters, "matvecs_per_solve": mvs, "converged": bool(conv),
-                "backward_error": be, "max_iterations": args.max_iterations, "setup_s": setup_s,
-                "near_nnz_blocks": g.near_nnz, "matvec_ms": tm["mv_total_ms"],
-                "autotune": {"matvec_ms_before": tune_before, "matvec_ms_after": tune_after, "variants": tune_modes},
-                "matvec_phases_ms": phases, "matvec_phases_note": "phases timed one after another; "
-                "matvec_ms runs the near panels concurrently with the translations",
-                "levels_boxes_i4_pairs": mvb["levels"], "gs_passes_per_arnoldi_step": tm["gm_passes_per_step"],
-                "matvec_hbm_frac": mv_frac, "fill_ms": tm["fill_ms"],
-                "residual_e2e": float(np.linalg.norm(res) / np.linalg.norm(b_host)),
-                "mixed_vs_fp64": mixed, "shape_gradient": grad,
-                "l2": "inputs > L2 (near panels and radiation patterns are GBs)",
-            },
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64+f64", "data": "synthetic",
+            "config": config_of(args.workload, T.shape[0], N // 2),
+            "details": {"unknowns": N, "fill_s": fill_s, "mixed_vs_fp64": fp64,
+                        "step": "one direct solve of one plane wave: LU of the dense matrix (factors dropped "
+                                "before every step) and FP64 refinement"},
             "roofline": roof,
+            "roofline_matvec": rmv,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16,
-                    "clocks": clk_e2e.summary()},
+                    "steps": ke, "clocks": clk_e2e.summary()},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
-    g.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -271,7 +271,11 @@ int sie_num_directions(const sie_ctx* ctx, int* Q);
  * out[10] = mean Gram-Schmidt passes per Arnoldi step of the last solve; out[11] = inner
  * cycles of the last batched mixed solve replayed from their captured CUDA graph;
  * out[12] = set-up of the near-field preconditioner (host wall time); out[13] = the
- * complex64 tensor-core LU of sie_solve_direct_mixed (host wall time). */
+ * complex64 tensor-core LU of sie_solve_direct_mixed (host wall time), out[14] its
+ * tensor-core trailing updates (CUDA events on the launching stream, summed), out[15]
+ * their complex flops (8 per complex multiply-add), out[16] their launches; out[17..20]
+ * with SIE_LU_PHASES=1 in the environment, the device time of the LU's panels, row swaps,
+ * L11 solves and operand tiling. */
 int sie_get_timings(const sie_ctx* ctx, double* out, int n);
 
 /* Launch all further work of ctx on the caller's CUDA stream (NULL: back to the

@@ -12,12 +12,14 @@
 //
 // Blocked right-looking LU, panel width NB = 128, on the matrix stored as two FP32
 // planes (real, imaginary), column-major, internal unknown order:
-//   1. panel: for each of its columns, a pivot search (one block), the row swap inside
-//      the panel, then the scaling of the column and the rank-1 update of the panel's
-//      remaining columns (one thread per row);
+//   1. panel, in sub-panels of 16 columns: for each column a pivot search (one block), the
+//      row swap across the panel, the scaling of the column and the rank-1 update of the
+//      sub-panel (one thread per row); then the sub-panel's U rows (L11^-1) and one rank-16
+//      update of the panel's later columns;
 //   2. the panel's row swaps applied to every column left and right of it;
 //   3. U12 = L11^-1 A12, a warp per column with L11 in shared memory;
-//   4. A22 -= L21 U12 on the tensor cores.
+//   4. A22 -= L21 U12 on the tensor cores: first the next panel's columns, then, on a
+//      second (low-priority) stream, the rest, which runs beside the next panel (look-ahead).
 #include <chrono>
 #include <cmath>
 #include <vector>
@@ -34,7 +36,8 @@ int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, siz
 size_t tiled_bytes_host(int rows, int K);
 }  // namespace tc
 
-static const int LU_NB = 128;
+static const int LU_NB = 128;  // panel width (the tensor-core update's K)
+static const int LU_SB = 16;   // sub-panel width inside a panel
 
 // Dense panels (cfg.dense = 1) -> FP32 planes of Z in the internal interleaved order
 // (unknown 2m + a of edge m), column-major.
@@ -152,6 +155,64 @@ __global__ void __launch_bounds__(256) k_panel_update(float* Ar, float* Ai, size
   }
 }
 
+// Sub-panel [s0, s1) of a panel ending at k1: its rows of the panel's later columns,
+// U = L11^-1 A (L11 the unit lower triangle of the sub-panel's diagonal block).  Thread
+// per column c in [s1, k1).
+__global__ void k_sub_trsm(float* Ar, float* Ai, size_t ld, int s0, int s1, int k1) {
+  const int c = s1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= k1) return;
+  const int w = s1 - s0;
+  float xr[LU_SB], xi[LU_SB];
+  for (int i = 0; i < w; i++) {
+    xr[i] = Ar[(size_t)c * ld + s0 + i];
+    xi[i] = Ai[(size_t)c * ld + s0 + i];
+  }
+  for (int i = 1; i < w; i++)
+    for (int t = 0; t < i; t++) {
+      const float lr = Ar[(size_t)(s0 + t) * ld + s0 + i], li = Ai[(size_t)(s0 + t) * ld + s0 + i];
+      xr[i] -= lr * xr[t] - li * xi[t];
+      xi[i] -= lr * xi[t] + li * xr[t];
+    }
+  for (int i = 1; i < w; i++) {
+    Ar[(size_t)c * ld + s0 + i] = xr[i];
+    Ai[(size_t)c * ld + s0 + i] = xi[i];
+  }
+}
+
+// Rank-w update of the panel's later columns by a factored sub-panel [s0, s1):
+// a_rc -= sum_t l_rt u_tc for rows r >= s1 and columns c in [s1, k1).  The sub-panel's U
+// rows in shared memory; thread per row.
+__global__ void __launch_bounds__(256) k_sub_update(float* Ar, float* Ai, size_t ld, int n, int s0, int s1,
+                                                    int k1) {
+  __shared__ float ur[LU_SB][LU_NB], ui[LU_SB][LU_NB];
+  const int w = s1 - s0, nc = k1 - s1;
+  for (int e = threadIdx.x; e < w * nc; e += blockDim.x) {
+    const int t = e / nc, c = e - t * nc;
+    ur[t][c] = Ar[(size_t)(s1 + c) * ld + s0 + t];
+    ui[t][c] = Ai[(size_t)(s1 + c) * ld + s0 + t];
+  }
+  __syncthreads();
+  const int r = s1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  float lr[LU_SB], li[LU_SB];
+  for (int t = 0; t < w; t++) {
+    lr[t] = Ar[(size_t)(s0 + t) * ld + r];
+    li[t] = Ai[(size_t)(s0 + t) * ld + r];
+  }
+  for (int c = 0; c < nc; c++) {
+    float sr = 0.f, si = 0.f;
+#pragma unroll
+    for (int t = 0; t < LU_SB; t++)
+      if (t < w) {
+        sr += lr[t] * ur[t][c] - li[t] * ui[t][c];
+        si += lr[t] * ui[t][c] + li[t] * ur[t][c];
+      }
+    const size_t o = (size_t)(s1 + c) * ld + r;
+    Ar[o] -= sr;
+    Ai[o] -= si;
+  }
+}
+
 // Row swaps ipiv[k0 .. k1) applied in order to the columns [c, c + 1) of every thread
 // outside the panel [k0, k1).
 __global__ void k_laswp(float* Ar, float* Ai, size_t ld, int n, int k0, int k1, const int* ipiv) {
@@ -228,11 +289,20 @@ __global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld,
   }
 }
 
-// Solves with the factors, one vector (complex64, internal order) in place.
-// Forward: x[k0 .. k1) = L11^-1 x[k0 .. k1) (one block), then x[k1 ..) -= L21 x[k0 .. k1).
+// Solves with the factors, one vector (complex64, internal order) in place.  Diagonal
+// block: x[k0 .. k0 + nb) = L11^-1 x (lower, unit diagonal) or U11^-1 x (upper), with the
+// block staged in shared memory first (coalesced), then one warp runs the substitution.
 __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
                                                     int lower, cc* x) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
+  float* Di = Dr + LU_NB * LU_NB;
   __shared__ float br[LU_NB], bi[LU_NB];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int col = e / nb, row = e - col * nb;
+    Dr[col * LU_NB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
+    Di[col * LU_NB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
+  }
   for (int r = threadIdx.x; r < nb; r += blockDim.x) {
     br[r] = x[k0 + r].re;
     bi[r] = x[k0 + r].im;
@@ -245,7 +315,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
         const float vr = br[i], vi = bi[i];
         __syncwarp();
         for (int r = i + 1 + lane; r < nb; r += 32) {
-          const float lr = Ar[(size_t)(k0 + i) * ld + k0 + r], li = Ai[(size_t)(k0 + i) * ld + k0 + r];
+          const float lr = Dr[i * LU_NB + r], li = Di[i * LU_NB + r];
           br[r] -= lr * vr - li * vi;
           bi[r] -= lr * vi + li * vr;
         }
@@ -254,7 +324,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
     } else {
       for (int i = nb - 1; i >= 0; i--) {
         if (lane == 0) {
-          const float ur = Ar[(size_t)(k0 + i) * ld + k0 + i], ui = Ai[(size_t)(k0 + i) * ld + k0 + i];
+          const float ur = Dr[i * LU_NB + i], ui = Di[i * LU_NB + i];
           const float den = ur * ur + ui * ui;
           const float xr = (br[i] * ur + bi[i] * ui) / den, xi = (bi[i] * ur - br[i] * ui) / den;
           br[i] = xr;
@@ -263,7 +333,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
         __syncwarp();
         const float vr = br[i], vi = bi[i];
         for (int r = lane; r < i; r += 32) {
-          const float ur = Ar[(size_t)(k0 + i) * ld + k0 + r], ui = Ai[(size_t)(k0 + i) * ld + k0 + r];
+          const float ur = Dr[i * LU_NB + r], ui = Di[i * LU_NB + r];
           br[r] -= ur * vr - ui * vi;
           bi[r] -= ur * vi + ui * vr;
         }
@@ -296,16 +366,9 @@ __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float*
   x[i].im -= si;
 }
 
-__global__ void k_apply_pivots(const int* ipiv, int n, cc* x) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int j = 0; j < n; j++) {
-    const int p = ipiv[j];
-    if (p != j) {
-      const cc t = x[j];
-      x[j] = x[p];
-      x[p] = t;
-    }
-  }
+// y[i] = x[perm[i]]: the factorisation's row interchanges as one gather
+__global__ void k_permute(const int* perm, int n, const cc* x, cc* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = x[perm[i]];
 }
 
 __global__ void k_scale_to32(const zc* a, cc* b, int n, double s) {
@@ -378,48 +441,179 @@ static int lu_tc_factor(sie_ctx* c) {
                                        c->d_nb, c->d_nd, c->cfac, c->M, Ar, Ai);
     count_launch();
   }
+  // CUDA events around every trailing update, read once the factorisation has finished
+  std::vector<cudaEvent_t> evs;
+  auto new_event = [&]() {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) == cudaSuccess) evs.push_back(e);
+    return e;
+  };
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_ev;
+  double gemm_flops = 0;
   const size_t trsm_smem = (size_t)2 * LU_NB * LU_NB * sizeof(float);
   if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
+  // optional per-phase device times (SIE_LU_PHASES=1): panel, swaps, L11 solve, tiling
+  const char* pe = getenv("SIE_LU_PHASES");
+  const bool phases = pe && atoi(pe) != 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ph_ev[4];
+  auto mark = [&](int which, bool start, cudaEvent_t& keep) {
+    if (!phases) return;
+    cudaEvent_t e = new_event();
+    if (!e) return;
+    cudaEventRecord(e, s);
+    if (start) keep = e;
+    else ph_ev[which].push_back({keep, e});
+  };
+  cudaEvent_t pk = nullptr;
+  // Look-ahead: the panel chain runs on a high-priority stream sp.  After a panel's
+  // update, the columns of the next panel are updated first (on sp), and the rest of the
+  // trailing update goes to a low-priority stream sg, where it runs beside the next
+  // panel's factorisation (disjoint columns).  The next row swaps and operand tiling wait
+  // for it.
+  cudaStream_t sp = nullptr, sg = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_tiled = nullptr, ev_rest = nullptr, ev_sp = nullptr, ev_sg = nullptr;
+  {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    if (cudaStreamCreateWithPriority(&sp, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&sg, cudaStreamNonBlocking, lo) != cudaSuccess)
+      rc = fail(SIE_ERR_CUDA, "mixed LU: streams");
+    for (cudaEvent_t* e : {&ev_start, &ev_tiled, &ev_rest, &ev_sp, &ev_sg})
+      if (rc == SIE_OK && cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(SIE_ERR_CUDA, "mixed LU: events");
+    if (rc == SIE_OK) {
+      cudaEventRecord(ev_start, s);
+      cudaStreamWaitEvent(sp, ev_start, 0);
+      cudaStreamWaitEvent(sg, ev_start, 0);
+    }
+  }
+  const cudaStream_t s_main = s;
+  s = sp;  // the phase marks and the panel chain
+  bool rest_pending = false;
   for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += LU_NB) {
     const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
-    for (int j = k0; j < k1; j++) {
-      k_pivot<<<1, 1024, 0, s>>>(Ar, Ai, ld, n, j, k0, k1, ipiv, err);
-      count_launch();
-      if (j + 1 < n) {
-        k_panel_update<<<(n - j - 1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, n, j, k1);
+    mark(0, true, pk);
+    // the panel in sub-panels of LU_SB columns: column steps inside the sub-panel, then
+    // one rank-LU_SB update of the panel's later columns
+    for (int s0 = k0; s0 < k1; s0 += LU_SB) {
+      const int s1 = std::min(s0 + LU_SB, k1);
+      for (int j = s0; j < s1; j++) {
+        k_pivot<<<1, 1024, 0, sp>>>(Ar, Ai, ld, n, j, k0, k1, ipiv, err);
         count_launch();
+        if (j + 1 < n) {
+          k_panel_update<<<(n - j - 1 + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, j, s1);
+          count_launch();
+        }
+      }
+      if (s1 < k1) {
+        k_sub_trsm<<<1, 128, 0, sp>>>(Ar, Ai, ld, s0, s1, k1);
+        count_launch();
+        if (s1 < n) {
+          k_sub_update<<<(n - s1 + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, s0, s1, k1);
+          count_launch();
+        }
       }
     }
+    mark(0, false, pk);
+    if (rest_pending) cudaStreamWaitEvent(sp, ev_rest, 0);  // the previous trailing update
+    mark(1, true, pk);
     if (n - nb > 0) {
-      k_laswp<<<(n - nb + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, n, k0, k1, ipiv);
+      k_laswp<<<(n - nb + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, k0, k1, ipiv);
       count_launch();
     }
+    mark(1, false, pk);
     if (k1 < n) {
-      k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, s>>>(Ar, Ai, ld, n, k0, nb, k1);
+      mark(2, true, pk);
+      k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, sp>>>(Ar, Ai, ld, n, k0, nb, k1);
       count_launch();
-      const int m = n - k1;
+      mark(2, false, pk);
+      const int m = n - k1, nn = std::min(LU_NB, m);
       // A22 -= L21 U12 on the tensor cores
-      rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, s);
-      if (rc == SIE_OK) rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, s);
+      mark(3, true, pk);
+      rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, sp);
+      if (rc == SIE_OK) rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, sp);
+      mark(3, false, pk);
+      cudaEventRecord(ev_tiled, sp);
+      if (rc == SIE_OK && m > nn) {
+        // the columns past the next panel, on sg
+        cudaStreamWaitEvent(sg, ev_tiled, 0);
+        cudaEvent_t e0 = new_event(), e1 = new_event();
+        if (e0) cudaEventRecord(e0, sg);
+        const size_t boff = (size_t)((nb + tc::KC - 1) / tc::KC) * tc::BLOCK_BYTES;  // B tile 1
+        rc = tc::gemm_update(At, Bt + boff, nb, Ar + (size_t)(k1 + nn) * ld + k1, Ai + (size_t)(k1 + nn) * ld + k1,
+                             ld, m, m - nn, err, sg);
+        if (e1) cudaEventRecord(e1, sg);
+        if (e0 && e1) gemm_ev.push_back({e0, e1});
+        cudaEventRecord(ev_rest, sg);
+        rest_pending = true;
+        gemm_flops += 8.0 * m * (double)(m - nn) * nb;
+      }
+      // the next panel's columns, on sp
+      cudaEvent_t e0 = new_event(), e1 = new_event();
+      if (e0) cudaEventRecord(e0, sp);
       if (rc == SIE_OK)
-        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k1, Ai + (size_t)k1 * ld + k1, ld, m, m, err, s);
+        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k1, Ai + (size_t)k1 * ld + k1, ld, m, nn, err, sp);
+      if (e1) cudaEventRecord(e1, sp);
+      if (e0 && e1) gemm_ev.push_back({e0, e1});
+      gemm_flops += 8.0 * m * (double)nn * nb;
     }
     if (cudaGetLastError() != cudaSuccess && rc == SIE_OK) rc = fail(SIE_ERR_CUDA, "mixed LU: launch");
+  }
+  s = s_main;
+  if (ev_sp && ev_sg) {
+    cudaEventRecord(ev_sp, sp);
+    cudaEventRecord(ev_sg, sg);
+    cudaStreamWaitEvent(s, ev_sp, 0);
+    cudaStreamWaitEvent(s, ev_sg, 0);
   }
   int herr = 0;
   if (rc == SIE_OK && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                        cudaStreamSynchronize(s) != cudaSuccess))
     rc = fail(SIE_ERR_CUDA, "mixed LU: factorisation");
+  if (rc == SIE_OK) {
+    // the interchanges as one permutation, for the solves
+    std::vector<int> piv(n), perm(n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    if (cudaMemcpy(piv.data(), ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(SIE_ERR_CUDA, "mixed LU: pivots");
+    for (int j = 0; j < n && rc == SIE_OK; j++) std::swap(perm[j], perm[piv[j]]);
+    if (rc == SIE_OK && (cudaMalloc(&c->d_perm32, (size_t)n * sizeof(int)) != cudaSuccess ||
+                         cudaMalloc(&c->d_tmp32, (size_t)n * sizeof(cc)) != cudaSuccess ||
+                         cudaMemcpy(c->d_perm32, perm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice) !=
+                             cudaSuccess))
+      rc = fail(SIE_ERR_NOMEM, "mixed LU: permutation");
+  }
   if (rc == SIE_OK && (herr & 8)) rc = fail(SIE_ERR_NONFINITE, "mixed LU: singular or non-finite pivot");
   if (rc == SIE_OK && herr) rc = fail(SIE_ERR_CUDA, "mixed LU: a tensor-core pipeline wait timed out");
   c->tm.lu_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  double gms = 0;
+  for (auto& pe : gemm_ev) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, pe.first, pe.second) == cudaSuccess) gms += ms;
+  }
+  c->tm.lu_gemm_ms = gms;
+  for (int q = 0; q < 4; q++) {
+    double t = 0;
+    for (auto& pe2 : ph_ev[q]) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, pe2.first, pe2.second) == cudaSuccess) t += ms;
+    }
+    c->tm.lu_phase_ms[q] = t;
+  }
+  c->tm.lu_gemm_flops = gemm_flops;
+  c->tm.lu_gemm_launches = (int)gemm_ev.size();
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  for (cudaEvent_t e : {ev_start, ev_tiled, ev_rest, ev_sp, ev_sg})
+    if (e) cudaEventDestroy(e);
+  if (sp) cudaStreamDestroy(sp);
+  if (sg) cudaStreamDestroy(sg);
   cleanup();
   if (rc != SIE_OK) {
-    cudaFree(c->d_lu32);
-    cudaFree(c->d_lu32i);
-    cudaFree(c->d_piv32);
+    for (void* p : {(void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32, (void*)c->d_perm32, (void*)c->d_tmp32})
+      if (p) cudaFree(p);
     c->d_lu32 = c->d_lu32i = nullptr;
-    c->d_piv32 = nullptr;
+    c->d_piv32 = c->d_perm32 = nullptr;
+    c->d_tmp32 = nullptr;
   }
   return rc;
 }
@@ -429,11 +623,14 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   const int n = 2 * c->M;
   const size_t ld = (size_t)n;
   const float *Ar = c->d_lu32, *Ai = c->d_lu32i;
-  k_apply_pivots<<<1, 1, 0, s>>>(c->d_piv32, n, x);
+  k_permute<<<148, 256, 0, s>>>(c->d_perm32, n, x, c->d_tmp32);
   count_launch();
+  SIE_CUDA(cudaMemcpyAsync(x, c->d_tmp32, (size_t)n * sizeof(cc), cudaMemcpyDeviceToDevice, s));
+  const size_t dsm = (size_t)2 * LU_NB * LU_NB * sizeof(float);
+  SIE_CUDA(raise_smem(k_trsv_block, dsm));
   for (int k0 = 0; k0 < n; k0 += LU_NB) {
     const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
-    k_trsv_block<<<1, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 1, x);
+    k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 1, x);
     count_launch();
     if (k1 < n) {
       k_trsv_gemv<<<(n - k1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
@@ -442,7 +639,7 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   }
   for (int k0 = ((n - 1) / LU_NB) * LU_NB; k0 >= 0; k0 -= LU_NB) {
     const int nb = std::min(LU_NB, n - k0);
-    k_trsv_block<<<1, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, x);
+    k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 0, x);
     count_launch();
     if (k0 > 0) {
       k_trsv_gemv<<<(k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
@@ -576,11 +773,13 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   if (!c) return fail(SIE_ERR_ARG, "sie_release_factors: null context");
   SIE_CUDA(cudaSetDevice(c->device));
   if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
-  for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32})
+  for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32,
+                  (void*)c->d_perm32, (void*)c->d_tmp32})
     if (p) cudaFree(p);
   c->d_lu = nullptr;
   c->d_piv = nullptr;
   c->d_lu32 = c->d_lu32i = nullptr;
-  c->d_piv32 = nullptr;
+  c->d_piv32 = c->d_perm32 = nullptr;
+  c->d_tmp32 = nullptr;
   return SIE_OK;
 }

@@ -170,6 +170,10 @@ struct Timings {
   double graph_replays = 0;            // inner cycles replayed from a CUDA graph, last batched solve
   double precond_ms = 0;               // set-up of the near-field preconditioner (host wall time)
   double lu_factor_ms = 0;             // complex64 tensor-core LU of the mixed direct solve
+  double lu_gemm_ms = 0;               // of which its tensor-core trailing updates (CUDA events)
+  double lu_gemm_flops = 0;            // complex flops of those updates (8 per multiply-add)
+  int lu_gemm_launches = 0;
+  double lu_phase_ms[4] = {0, 0, 0, 0};  // panel, row swaps, L11 solve, operand tiling (SIE_LU_PHASES=1)
 };
 
 }  // namespace sie
@@ -309,7 +313,9 @@ struct sie_ctx {
   int* d_piv = nullptr;           // pivots (N) + info
   float* d_lu32 = nullptr;        // complex64 LU factors of the mixed direct solve: real plane,
   float* d_lu32i = nullptr;       // imaginary plane (column-major N x N, internal order)
-  int* d_piv32 = nullptr;         // and their row interchanges
+  int* d_piv32 = nullptr;         // and their row interchanges,
+  int* d_perm32 = nullptr;        // the same as one permutation (row i of P A is row perm[i] of A)
+  cc* d_tmp32 = nullptr;          // work vector of the triangular solves
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   void* h_gmb = nullptr;          // pinned host copy of the batched solver's per-system state
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) k_tile(const float* __restrict__ sr, cons
 }
 
 // C tile (blockIdx.x, blockIdx.y) -= A tile row blockIdx.x times B tile row blockIdx.y.
-__global__ void __launch_bounds__(256, 1) k_gemm(const char* __restrict__ At, const char* __restrict__ Bt,
+__global__ void __launch_bounds__(256, 2) k_gemm(const char* __restrict__ At, const char* __restrict__ Bt,
                                                  int nchunks, float* __restrict__ Cr, float* __restrict__ Ci,
                                                  size_t ldc, int m, int n, int* err) {
   extern __shared__ __align__(1024) unsigned char smraw[];
@@ -144,43 +144,39 @@ __global__ void __launch_bounds__(256, 1) k_gemm(const char* __restrict__ At, co
     const int row = mt * TILE + wl * 32 + lane;
     const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
 #pragma unroll 1
-    for (int j0 = half * (TILE / 2); j0 < (half + 1) * (TILE / 2); j0 += 32) {
-      uint32_t vr[32], vi[32];
+    for (int j0 = half * (TILE / 2); j0 < (half + 1) * (TILE / 2); j0 += 16) {
+      uint32_t vr[16], vi[16];
       asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
           : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]),
             "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]),
-            "=r"(vr[14]), "=r"(vr[15]), "=r"(vr[16]), "=r"(vr[17]), "=r"(vr[18]), "=r"(vr[19]), "=r"(vr[20]),
-            "=r"(vr[21]), "=r"(vr[22]), "=r"(vr[23]), "=r"(vr[24]), "=r"(vr[25]), "=r"(vr[26]), "=r"(vr[27]),
-            "=r"(vr[28]), "=r"(vr[29]), "=r"(vr[30]), "=r"(vr[31])
+            "=r"(vr[14]), "=r"(vr[15])
           : "r"(lane_base + j0));
       asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
           : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]),
             "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]),
-            "=r"(vi[14]), "=r"(vi[15]), "=r"(vi[16]), "=r"(vi[17]), "=r"(vi[18]), "=r"(vi[19]), "=r"(vi[20]),
-            "=r"(vi[21]), "=r"(vi[22]), "=r"(vi[23]), "=r"(vi[24]), "=r"(vi[25]), "=r"(vi[26]), "=r"(vi[27]),
-            "=r"(vi[28]), "=r"(vi[29]), "=r"(vi[30]), "=r"(vi[31])
+            "=r"(vi[14]), "=r"(vi[15])
           : "r"(lane_base + TILE + j0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (row < m) {
-        // 32 loads of C first, then their stores: independent requests in flight
-        const int ncol = min(32, n - (nt * TILE + j0));
+        // 16 loads of C first, then their stores: independent requests in flight
+        const int ncol = min(16, n - (nt * TILE + j0));
         float* pr = Cr + (size_t)(nt * TILE + j0) * ldc + row;
         float* pi = Ci + (size_t)(nt * TILE + j0) * ldc + row;
 #pragma unroll
-        for (int h = 0; h < 32; h += 16) {
-          float cr[16], ci[16];
+        for (int h = 0; h < 16; h += 8) {
+          float cr[8], ci[8];
 #pragma unroll
-          for (int j = 0; j < 16; j++)
+          for (int j = 0; j < 8; j++)
             if (h + j < ncol) {
               cr[j] = pr[(size_t)(h + j) * ldc];
               ci[j] = pi[(size_t)(h + j) * ldc];
             }
 #pragma unroll
-          for (int j = 0; j < 16; j++)
+          for (int j = 0; j < 8; j++)
             if (h + j < ncol) {
               pr[(size_t)(h + j) * ldc] = cr[j] - __uint_as_float(vr[h + j]);
               pi[(size_t)(h + j) * ldc] = ci[j] - __uint_as_float(vi[h + j]);

@@ -10,16 +10,17 @@
 //
 // Operands are pre-tiled in global memory in the shape the MMA reads from shared memory,
 // so each pipeline stage is one contiguous bulk (TMA) copy:
-//   block (tile t of 128 rows, K chunk c of 16): 4 planes (re hi, re lo, im hi, im lo),
-//   each 128 rows x 16 tf32 in the K-major no-swizzle canonical layout: core matrices of
+//   block (tile t of 128 rows, K chunk c of 8): 4 planes (re hi, re lo, im hi, im lo),
+//   each 128 rows x 8 tf32 in the K-major no-swizzle canonical layout: core matrices of
 //   8 rows x 16 bytes (4 tf32), core (k/4, r/8) at byte ((k/4) * 16 + r/8) * 128, row r%8
 //   at +16 (r%8), element k%4 at +4 (k%4).  LBO (next 4 k) = 2048 B, SBO (next 8 rows) =
-//   128 B.  One block = 32 KB; blocks ordered [tile][chunk].
+//   128 B.  One block = 16 KB; blocks ordered [tile][chunk].
 // A's rows are C's rows (M); B is tiled by C's columns (the MMA's N rows), K-major too.
 //
-// Kernel: one CTA (8 warps) per 128 x 128 tile of C.  Warp 0 lane 0 issues the bulk copies
-// into a 3-stage ring (64 KB per stage: one A block, one B block); warp 1 lane 0 issues
-// the MMAs (M = 128, N = 128, K = 8, 24 per stage) and commits each stage back to the
+// Kernel: one CTA (8 warps) per 128 x 128 tile of C, two CTAs per SM so that one's
+// epilogue overlaps the other's MMAs.  Warp 0 lane 0 issues the bulk copies into a
+// 3-stage ring (32 KB per stage: one A block, one B block); warp 1 lane 0 issues the MMAs
+// (M = 128, N = 128, K = 8, 12 per stage) and commits each stage back to the
 // producer; then all four warps read the accumulators (warp w owns TMEM lanes 32w..32w+31
 // = rows of C) and subtract them from C.  Every wait on an mbarrier is bounded: a wait
 // that runs out sets *err and the CTA skips the rest of its work, waiting (also bounded)
@@ -32,12 +33,13 @@ namespace sie {
 namespace tc {
 
 constexpr int TILE = 128;                 // rows of an operand tile; C tile is TILE x TILE
-constexpr int KC = 16;                    // K per pipeline stage (two MMAs of K = 8)
-constexpr int PLANE_BYTES = TILE * KC * 4;  // 8 KB
-constexpr int BLOCK_BYTES = 4 * PLANE_BYTES;  // 32 KB: re hi, re lo, im hi, im lo
+constexpr int KC = 8;                     // K per pipeline stage (one MMA of K = 8)
+constexpr int PLANE_BYTES = TILE * KC * 4;  // 4 KB
+constexpr int BLOCK_BYTES = 4 * PLANE_BYTES;  // 16 KB: re hi, re lo, im hi, im lo
 constexpr int STAGES = 3;
 constexpr int STAGE_BYTES = 2 * BLOCK_BYTES;  // A block + B block
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + barriers, alignment slack
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + barriers, alignment slack: 97 KB,
+                                                         // two CTAs per SM (TMEM 2 x 256 columns)
 constexpr unsigned WAIT_LIMIT = 1u << 26;   // polls of one mbarrier before giving up
 
 // byte offset of element (r, k) inside one plane of a block
