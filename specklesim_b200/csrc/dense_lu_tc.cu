@@ -10,14 +10,15 @@
 // tolerance, which it does while cond(Z) times the factorisation's rounding stays below
 // one.
 //
-// Blocked right-looking LU, panel width NB = 128, on the matrix stored as two FP32
+// Blocked right-looking LU, panel width NB = 256, on the matrix stored as two FP32
 // planes (real, imaginary), column-major, internal unknown order:
-//   1. panel, in sub-panels of 16 columns: for each column a pivot search (one block), the
-//      row swap across the panel, the scaling of the column and the rank-1 update of the
-//      sub-panel (one thread per row); then the sub-panel's U rows (L11^-1) and one rank-16
-//      update of the panel's later columns;
+//   1. panel, in sub-panels of 16 columns: each sub-panel is one cooperative launch that,
+//      column by column, agrees on the pivot, swaps rows across the panel, scales the
+//      column and updates the sub-panel (two bounded grid barriers per column); then the
+//      sub-panel's U rows (L11^-1) and one rank-16 update of the panel's later columns;
 //   2. the panel's row swaps applied to every column left and right of it;
-//   3. U12 = L11^-1 A12, a warp per column with L11 in shared memory;
+//   3. U12 = L11^-1 A12 by 128-row diagonal blocks: a warp per column with the block in
+//      shared memory, the rows below it updated on the tensor cores;
 //   4. A22 -= L21 U12 on the tensor cores: first the next panel's columns, then, on a
 //      second (low-priority) stream, the rest, which runs beside the next panel (look-ahead).
 #include <chrono>
@@ -32,12 +33,15 @@ namespace tc {
 int tile_operand(const float* sr, const float* si, size_t ld, int rows, int K, bool trans, char* out,
                  cudaStream_t st);
 int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, size_t ldc, int m, int n,
-                int* d_err, cudaStream_t st);
+                int* d_err, cudaStream_t st, int max_ctas = 0);
 size_t tiled_bytes_host(int rows, int K);
 }  // namespace tc
 
-static const int LU_NB = 128;  // panel width (the tensor-core update's K)
+static const int LU_NB = 256;  // panel width (the tensor-core update's K)
 static const int LU_SB = 16;   // sub-panel width inside a panel
+static const int LU_TB = 128;  // diagonal blocks of the triangular solves
+static const int LU_FREE_SMS = 12;  // multiprocessors the look-ahead update leaves to the panels
+static const int PANEL_MAX_BLOCKS = 256;  // largest grid of the cooperative panel kernel
 
 // Dense panels (cfg.dense = 1) -> FP32 planes of Z in the internal interleaved order
 // (unknown 2m + a of edge m), column-major.
@@ -67,92 +71,157 @@ __global__ void k_expand_dense32(const long long* base, const int* box_first, co
   }
 }
 
-// Pivot of column j (rows j .. n-1): the row of largest |a|, first on ties; swaps rows j
-// and p over the panel's columns [c0, c1) and records p.  One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_pivot(float* Ar, float* Ai, size_t ld, int n, int j, int c0, int c1,
-                                                int* ipiv, int* err) {
-  __shared__ float sv[32];
-  __shared__ int si[32];
-  const float* cr = Ar + (size_t)j * ld;
-  const float* ci = Ai + (size_t)j * ld;
-  float best = -1.f;
-  int bi = j;
-  for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
-    const float v = cr[i] * cr[i] + ci[i] * ci[i];
-    if (v > best) {
-      best = v;
-      bi = i;
-    }
+// Pivot comparison: larger |a|^2 first, the smaller row index on ties (the first maximum,
+// as izamax).
+__device__ __forceinline__ void argmax_pair(float& best, int& bi, float ov, int oi) {
+  if (ov > best || (ov == best && oi < bi)) {
+    best = ov;
+    bi = oi;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ov > best || (ov == best && oi < bi)) {
-      best = ov;
-      bi = oi;
-    }
-  }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) {
-    sv[w] = best;
-    si[w] = bi;
-  }
-  __syncthreads();
-  if (w == 0) {
-    best = l < (int)(blockDim.x >> 5) ? sv[l] : -1.f;
-    bi = l < (int)(blockDim.x >> 5) ? si[l] : n;
-    for (int o = 16; o > 0; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
-    }
-    if (l == 0) {
-      si[0] = bi;
-      sv[0] = best;
-      ipiv[j] = bi;
-      if (!(best > 0.f) || !isfinite(best)) atomicOr(err, 8);  // singular or non-finite column
-    }
-  }
-  __syncthreads();
-  const int p = si[0];
-  if (p != j)
-    for (int c = c0 + (int)threadIdx.x; c < c1; c += blockDim.x) {
-      const size_t a = (size_t)c * ld + j, b = (size_t)c * ld + p;
-      float t = Ar[a];
-      Ar[a] = Ar[b];
-      Ar[b] = t;
-      t = Ai[a];
-      Ai[a] = Ai[b];
-      Ai[b] = t;
-    }
 }
 
-// Column j of the panel [j .. c1): l_i = a_ij / a_jj (i > j), then a_ik -= l_i a_jk for
-// the panel's later columns k.  Thread per row i.
-__global__ void __launch_bounds__(256) k_panel_update(float* Ar, float* Ai, size_t ld, int n, int j, int c1) {
-  __shared__ float ur[LU_NB], ui[LU_NB];
-  const int w = c1 - j - 1;  // later columns of the panel
-  for (int k = threadIdx.x; k < w; k += blockDim.x) {
-    ur[k] = Ar[(size_t)(j + 1 + k) * ld + j];
-    ui[k] = Ai[(size_t)(j + 1 + k) * ld + j];
+// Grid barrier of the cooperative sub-panel kernel (all its blocks are resident).  The
+// wait is bounded: a block that sees no progress for about a second records the failure
+// in st[2] and stops waiting; later barriers then pass straight through, and the host
+// reports the error.  st = {arrival count, generation, error}.
+__device__ void lu_grid_bar(unsigned* st, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &st[1];
+    volatile unsigned* bad = &st[2];
+    if (*bad == 0) {
+      const unsigned g = *gen;
+      __threadfence();
+      const unsigned arrived = atomicAdd(&st[0], 1u) + 1u;
+      if (arrived == nblocks) {
+        atomicExch(&st[0], 0u);
+        __threadfence();
+        atomicAdd(&st[1], 1u);
+      } else {
+        long long it = 0;
+        while (*gen == g && *bad == 0) {
+          if (++it > (1LL << 24)) {
+            atomicExch(&st[2], 1u);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+    }
+    __threadfence();
   }
   __syncthreads();
-  const int i = j + 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float pr = Ar[(size_t)j * ld + j], pi = Ai[(size_t)j * ld + j];
-  const float den = pr * pr + pi * pi;
-  const float ar = Ar[(size_t)j * ld + i], ai = Ai[(size_t)j * ld + i];
-  const float lr = (ar * pr + ai * pi) / den, li = (ai * pr - ar * pi) / den;
-  Ar[(size_t)j * ld + i] = lr;
-  Ai[(size_t)j * ld + i] = li;
-  for (int k = 0; k < w; k++) {
-    const size_t o = (size_t)(j + 1 + k) * ld + i;
-    Ar[o] -= lr * ur[k] - li * ui[k];
-    Ai[o] -= lr * ui[k] + li * ur[k];
+}
+
+// One sub-panel [s0, s1) of the panel [k0, k1) factorised by one cooperative launch: for
+// each column j, every block reduces the published maxima of column j to the same pivot
+// p, block 0 swaps rows j and p across the panel and records p; after a grid barrier every
+// thread scales its rows of column j by the pivot and updates them in the sub-panel's
+// later columns with row j, and publishes its maximum of the updated column j + 1; a
+// second barrier ends the step.  Matrix reads bypass L1 (__ldcg): rows written by other
+// blocks are seen through L2.  pmax / pidx: one slot per block.
+__global__ void __launch_bounds__(256) k_subpanel(float* Ar, float* Ai, size_t ld, int n, int s0, int s1, int k0,
+                                                  int k1, int* ipiv, int* err, float* pmax, int* pidx,
+                                                  unsigned* bar) {
+  __shared__ float sv[8];
+  __shared__ int si[8];
+  __shared__ int piv_s;
+  const unsigned G = gridDim.x;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  auto publish = [&](float best, int bi) {
+    for (int o = 16; o > 0; o >>= 1)
+      argmax_pair(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+    if (l == 0) {
+      sv[w] = best;
+      si[w] = bi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 1; k < (int)(blockDim.x >> 5); k++) argmax_pair(best, bi, sv[k], si[k]);
+      pmax[blockIdx.x] = best;
+      pidx[blockIdx.x] = bi;
+    }
+  };
+  {  // maxima of the first column
+    float best = -1.f;
+    int bi = n;
+    for (int r = s0 + gtid; r < n; r += gstride) {
+      const float a = __ldcg(Ar + (size_t)s0 * ld + r), b = __ldcg(Ai + (size_t)s0 * ld + r);
+      argmax_pair(best, bi, a * a + b * b, r);
+    }
+    publish(best, bi);
   }
+  lu_grid_bar(bar, G);
+  for (int j = s0; j < s1; j++) {
+    if (threadIdx.x < 32) {
+      float best = -1.f;
+      int bi = n;
+      for (int k = threadIdx.x; k < (int)G; k += 32) argmax_pair(best, bi, __ldcg(pmax + k), __ldcg(pidx + k));
+      for (int o = 16; o > 0; o >>= 1)
+        argmax_pair(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+      if (threadIdx.x == 0) {
+        piv_s = bi;
+        if (blockIdx.x == 0) {
+          ipiv[j] = bi;
+          if (!(best > 0.f) || !isfinite(best) || bi >= n) atomicOr(err, 8);  // singular or non-finite
+        }
+      }
+    }
+    __syncthreads();
+    const int p = piv_s;
+    if (blockIdx.x == 0 && p != j && p < n)
+      for (int c = k0 + (int)threadIdx.x; c < k1; c += blockDim.x) {
+        const size_t a = (size_t)c * ld + j, b = (size_t)c * ld + p;
+        const float tr = __ldcg(Ar + a), ti = __ldcg(Ai + a);
+        Ar[a] = __ldcg(Ar + b);
+        Ai[a] = __ldcg(Ai + b);
+        Ar[b] = tr;
+        Ai[b] = ti;
+      }
+    lu_grid_bar(bar, G);
+    // row j is final: its pivot and its values in the sub-panel's later columns
+    const float pr = __ldcg(Ar + (size_t)j * ld + j), pi = __ldcg(Ai + (size_t)j * ld + j);
+    const float den = pr * pr + pi * pi;
+    const int wj = s1 - j - 1;
+    float ur[LU_SB], ui[LU_SB];
+#pragma unroll
+    for (int k = 0; k < LU_SB; k++)
+      if (k < wj) {
+        ur[k] = __ldcg(Ar + (size_t)(j + 1 + k) * ld + j);
+        ui[k] = __ldcg(Ai + (size_t)(j + 1 + k) * ld + j);
+      }
+    float best = -1.f;
+    int bi = n;
+    for (int r = j + 1 + gtid; r < n; r += gstride) {
+      // every load of the row first (one round trip to L2), then the arithmetic and stores
+      float ar = __ldcg(Ar + (size_t)j * ld + r), ai = __ldcg(Ai + (size_t)j * ld + r);
+      float xr[LU_SB], xi[LU_SB];
+#pragma unroll
+      for (int k = 0; k < LU_SB; k++)
+        if (k < wj) {
+          const size_t o = (size_t)(j + 1 + k) * ld + r;
+          xr[k] = __ldcg(Ar + o);
+          xi[k] = __ldcg(Ai + o);
+        }
+      const float lr = (ar * pr + ai * pi) / den, li = (ai * pr - ar * pi) / den;
+      Ar[(size_t)j * ld + r] = lr;
+      Ai[(size_t)j * ld + r] = li;
+#pragma unroll
+      for (int k = 0; k < LU_SB; k++)
+        if (k < wj) {
+          const size_t o = (size_t)(j + 1 + k) * ld + r;
+          xr[k] -= lr * ur[k] - li * ui[k];
+          xi[k] -= lr * ui[k] + li * ur[k];
+          Ar[o] = xr[k];
+          Ai[o] = xi[k];
+        }
+      if (wj > 0) argmax_pair(best, bi, xr[0] * xr[0] + xi[0] * xi[0], r);
+    }
+    if (j + 1 < s1) publish(best, bi);
+    lu_grid_bar(bar, G);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bar + 2) != 0) atomicOr(err, 16);  // a barrier gave up
 }
 
 // Sub-panel [s0, s1) of a panel ending at k1: its rows of the panel's later columns,
@@ -235,17 +304,17 @@ __global__ void k_laswp(float* Ar, float* Ai, size_t ld, int n, int k0, int k1, 
   }
 }
 
-// U12 = L11^-1 A12 in place: L11 the unit lower triangle of the nb x nb diagonal block at
-// (k0, k0), A12 its rows [k0, k0 + nb) in columns [c0, n).  L11 in shared memory; one warp
-// per column, lane l holding rows l, l + 32, l + 64, l + 96.
+// X = L^-1 X in place for a diagonal block of the factors: L the unit lower triangle of
+// the nb x nb block at (k0, k0) (nb <= LU_TB), X its rows [k0, k0 + nb) in columns [c0, n).
+// L in shared memory; one warp per column, lane l holding rows l, l + 32, l + 64, l + 96.
 __global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld, int n, int k0, int nb, int c0) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float* Lr = reinterpret_cast<float*>(smraw);  // [col][row], nb x nb
-  float* Li = Lr + LU_NB * LU_NB;
+  float* Li = Lr + LU_TB * LU_TB;
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     const int col = e / nb, row = e - col * nb;
-    Lr[col * LU_NB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
-    Li[col * LU_NB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
+    Lr[col * LU_TB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
+    Li[col * LU_TB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -272,7 +341,7 @@ __global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld,
       for (int q = 0; q < 4; q++) {
         const int r = lane + 32 * q;
         if (r > i && r < nb) {
-          const float lr = Lr[i * LU_NB + r], li = Li[i * LU_NB + r];
+          const float lr = Lr[i * LU_TB + r], li = Li[i * LU_TB + r];
           xr[q] -= lr * vr - li * vi;
           xi[q] -= lr * vi + li * vr;
         }
@@ -296,12 +365,12 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
                                                     int lower, cc* x) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
-  float* Di = Dr + LU_NB * LU_NB;
-  __shared__ float br[LU_NB], bi[LU_NB];
+  float* Di = Dr + LU_TB * LU_TB;
+  __shared__ float br[LU_TB], bi[LU_TB];
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     const int col = e / nb, row = e - col * nb;
-    Dr[col * LU_NB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
-    Di[col * LU_NB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
+    Dr[col * LU_TB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
+    Di[col * LU_TB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
   }
   for (int r = threadIdx.x; r < nb; r += blockDim.x) {
     br[r] = x[k0 + r].re;
@@ -315,7 +384,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
         const float vr = br[i], vi = bi[i];
         __syncwarp();
         for (int r = i + 1 + lane; r < nb; r += 32) {
-          const float lr = Dr[i * LU_NB + r], li = Di[i * LU_NB + r];
+          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
           br[r] -= lr * vr - li * vi;
           bi[r] -= lr * vi + li * vr;
         }
@@ -324,7 +393,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
     } else {
       for (int i = nb - 1; i >= 0; i--) {
         if (lane == 0) {
-          const float ur = Dr[i * LU_NB + i], ui = Di[i * LU_NB + i];
+          const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
           const float den = ur * ur + ui * ui;
           const float xr = (br[i] * ur + bi[i] * ui) / den, xi = (bi[i] * ur - br[i] * ui) / den;
           br[i] = xr;
@@ -333,7 +402,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
         __syncwarp();
         const float vr = br[i], vi = bi[i];
         for (int r = lane; r < i; r += 32) {
-          const float ur = Dr[i * LU_NB + r], ui = Di[i * LU_NB + r];
+          const float ur = Dr[i * LU_TB + r], ui = Di[i * LU_TB + r];
           br[r] -= ur * vr - ui * vi;
           bi[r] -= ur * vi + ui * vr;
         }
@@ -348,7 +417,7 @@ __global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float
 // x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb); thread per row.
 __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
                                                    int r0, int r1, cc* x) {
-  __shared__ float br[LU_NB], bi[LU_NB];
+  __shared__ float br[LU_TB], bi[LU_TB];
   for (int r = threadIdx.x; r < nb; r += blockDim.x) {
     br[r] = x[k0 + r].re;
     bi[r] = x[k0 + r].im;
@@ -413,17 +482,20 @@ static int lu_tc_factor(sie_ctx* c) {
   float *Ar = nullptr, *Ai = nullptr;
   int *ipiv = nullptr, *err = nullptr;
   char *At = nullptr, *Bt = nullptr;
+  void* pscr = nullptr;  // pivot search: per-block maxima and indices, and the block counter
   int rc = SIE_OK;
   auto cleanup = [&]() {
     if (At) cudaFree(At);
     if (Bt) cudaFree(Bt);
     if (err) cudaFree(err);
+    if (pscr) cudaFree(pscr);
   };
   SIE_CUDA(cudaMalloc(&Ar, ld * n * sizeof(float)));
   if (cudaMalloc(&Ai, ld * n * sizeof(float)) != cudaSuccess || cudaMalloc(&ipiv, (size_t)n * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
       cudaMalloc(&At, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess ||
-      cudaMalloc(&Bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) {
+      cudaMalloc(&Bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess ||
+      cudaMalloc(&pscr, (size_t)PANEL_MAX_BLOCKS * 8 + 64) != cudaSuccess) {
     cudaFree(Ar);
     if (Ai) cudaFree(Ai);
     if (ipiv) cudaFree(ipiv);
@@ -435,6 +507,10 @@ static int lu_tc_factor(sie_ctx* c) {
   c->d_piv32 = ipiv;
   auto t0 = std::chrono::steady_clock::now();
   cudaMemsetAsync(err, 0, sizeof(int), s);
+  float* pmax = (float*)pscr;
+  int* pidx = (int*)((char*)pscr + (size_t)PANEL_MAX_BLOCKS * 4);
+  unsigned* pbar = (unsigned*)((char*)pscr + (size_t)PANEL_MAX_BLOCKS * 8);  // count, generation, error
+  cudaMemsetAsync(pbar, 0, 4 * sizeof(unsigned), s);
   {
     dim3 g(64, std::min(c->near.nbox, 1024));
     k_expand_dense32<<<g, 256, 0, s>>>(c->d_base, c->d_box_first, c->d_box_cnt, c->d_ncols, c->near.nbox, c->d_na,
@@ -450,7 +526,7 @@ static int lu_tc_factor(sie_ctx* c) {
   };
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_ev;
   double gemm_flops = 0;
-  const size_t trsm_smem = (size_t)2 * LU_NB * LU_NB * sizeof(float);
+  const size_t trsm_smem = (size_t)2 * LU_TB * LU_TB * sizeof(float);
   if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
   // optional per-phase device times (SIE_LU_PHASES=1): panel, swaps, L11 solve, tiling
   const char* pe = getenv("SIE_LU_PHASES");
@@ -488,6 +564,21 @@ static int lu_tc_factor(sie_ctx* c) {
     }
   }
   const cudaStream_t s_main = s;
+  // the look-ahead update leaves LU_FREE_SMS multiprocessors to the panel chain (two
+  // persistent CTAs per multiprocessor)
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  int free_sms = LU_FREE_SMS;
+  if (const char* e = getenv("SIE_LU_FREE_SMS")) free_sms = std::max(0, std::min(nsm - 1, atoi(e)));
+  const int rest_ctas = 2 * std::max(1, nsm - free_sms);
+  // SIE_LU_LOOKAHEAD=0 runs the whole trailing update on the panel stream (same work)
+  const char* la = getenv("SIE_LU_LOOKAHEAD");
+  const bool lookahead = !(la && atoi(la) == 0);
+  // the cooperative panel kernel: blocks that fit on the multiprocessors the look-ahead
+  // update leaves free (all of them resident at once)
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpanel, 256, 0) != cudaSuccess) per_sm = 1;
+  const int panel_blocks = std::max(1, std::min(PANEL_MAX_BLOCKS, std::min(per_sm, 4) * std::max(free_sms, 1)));
   s = sp;  // the phase marks and the panel chain
   bool rest_pending = false;
   for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += LU_NB) {
@@ -497,16 +588,19 @@ static int lu_tc_factor(sie_ctx* c) {
     // one rank-LU_SB update of the panel's later columns
     for (int s0 = k0; s0 < k1; s0 += LU_SB) {
       const int s1 = std::min(s0 + LU_SB, k1);
-      for (int j = s0; j < s1; j++) {
-        k_pivot<<<1, 1024, 0, sp>>>(Ar, Ai, ld, n, j, k0, k1, ipiv, err);
-        count_launch();
-        if (j + 1 < n) {
-          k_panel_update<<<(n - j - 1 + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, j, s1);
-          count_launch();
+      {
+        int ns0 = s0, ns1 = s1, nn0 = n, kk0 = k0, kk1 = k1;
+        size_t ldd = ld;
+        void* args[] = {&Ar, &Ai, &ldd, &nn0, &ns0, &ns1, &kk0, &kk1, &ipiv, &err, &pmax, &pidx, &pbar};
+        if (cudaLaunchCooperativeKernel((const void*)k_subpanel, dim3(panel_blocks), dim3(256), args, 0, sp) !=
+            cudaSuccess) {
+          rc = fail(SIE_ERR_CUDA, "mixed LU: cooperative panel launch");
+          break;
         }
+        count_launch();
       }
       if (s1 < k1) {
-        k_sub_trsm<<<1, 128, 0, sp>>>(Ar, Ai, ld, s0, s1, k1);
+        k_sub_trsm<<<1, LU_NB, 0, sp>>>(Ar, Ai, ld, s0, s1, k1);
         count_launch();
         if (s1 < n) {
           k_sub_update<<<(n - s1 + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, s0, s1, k1);
@@ -524,8 +618,22 @@ static int lu_tc_factor(sie_ctx* c) {
     mark(1, false, pk);
     if (k1 < n) {
       mark(2, true, pk);
-      k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, sp>>>(Ar, Ai, ld, n, k0, nb, k1);
-      count_launch();
+      // U12 = L11^-1 A12 by diagonal blocks of LU_TB: each block's rows are solved, then the
+      // rows below it in the panel lose L21-block times them (a tensor-core update)
+      for (int d0 = k0; d0 < k1 && rc == SIE_OK; d0 += LU_TB) {
+        const int db = std::min(LU_TB, k1 - d0), d1 = d0 + db;
+        k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, sp>>>(Ar, Ai, ld, n, d0, db, k1);
+        count_launch();
+        if (d1 < k1) {
+          const int mb = k1 - d1;
+          rc = tc::tile_operand(Ar + (size_t)d0 * ld + d1, Ai + (size_t)d0 * ld + d1, ld, mb, db, false, At, sp);
+          if (rc == SIE_OK)
+            rc = tc::tile_operand(Ar + (size_t)k1 * ld + d0, Ai + (size_t)k1 * ld + d0, ld, n - k1, db, true, Bt, sp);
+          if (rc == SIE_OK)
+            rc = tc::gemm_update(At, Bt, db, Ar + (size_t)k1 * ld + d1, Ai + (size_t)k1 * ld + d1, ld, mb, n - k1,
+                                 err, sp);
+        }
+      }
       mark(2, false, pk);
       const int m = n - k1, nn = std::min(LU_NB, m);
       // A22 -= L21 U12 on the tensor cores
@@ -534,17 +642,19 @@ static int lu_tc_factor(sie_ctx* c) {
       if (rc == SIE_OK) rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, sp);
       mark(3, false, pk);
       cudaEventRecord(ev_tiled, sp);
+      const cudaStream_t srest = lookahead ? sg : sp;
       if (rc == SIE_OK && m > nn) {
         // the columns past the next panel, on sg
         cudaStreamWaitEvent(sg, ev_tiled, 0);
         cudaEvent_t e0 = new_event(), e1 = new_event();
-        if (e0) cudaEventRecord(e0, sg);
-        const size_t boff = (size_t)((nb + tc::KC - 1) / tc::KC) * tc::BLOCK_BYTES;  // B tile 1
+        if (e0) cudaEventRecord(e0, srest);
+        // the B tiles past the next panel's nn columns
+        const size_t boff = (size_t)(nn / tc::TILE) * ((nb + tc::KC - 1) / tc::KC) * tc::BLOCK_BYTES;
         rc = tc::gemm_update(At, Bt + boff, nb, Ar + (size_t)(k1 + nn) * ld + k1, Ai + (size_t)(k1 + nn) * ld + k1,
-                             ld, m, m - nn, err, sg);
-        if (e1) cudaEventRecord(e1, sg);
+                             ld, m, m - nn, err, srest, lookahead ? rest_ctas : 0);
+        if (e1) cudaEventRecord(e1, srest);
         if (e0 && e1) gemm_ev.push_back({e0, e1});
-        cudaEventRecord(ev_rest, sg);
+        cudaEventRecord(ev_rest, srest);
         rest_pending = true;
         gemm_flops += 8.0 * m * (double)(m - nn) * nb;
       }
@@ -584,6 +694,7 @@ static int lu_tc_factor(sie_ctx* c) {
       rc = fail(SIE_ERR_NOMEM, "mixed LU: permutation");
   }
   if (rc == SIE_OK && (herr & 8)) rc = fail(SIE_ERR_NONFINITE, "mixed LU: singular or non-finite pivot");
+  if (rc == SIE_OK && (herr & 16)) rc = fail(SIE_ERR_CUDA, "mixed LU: a grid barrier of the panel kernel timed out");
   if (rc == SIE_OK && herr) rc = fail(SIE_ERR_CUDA, "mixed LU: a tensor-core pipeline wait timed out");
   c->tm.lu_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   double gms = 0;
@@ -626,10 +737,10 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   k_permute<<<148, 256, 0, s>>>(c->d_perm32, n, x, c->d_tmp32);
   count_launch();
   SIE_CUDA(cudaMemcpyAsync(x, c->d_tmp32, (size_t)n * sizeof(cc), cudaMemcpyDeviceToDevice, s));
-  const size_t dsm = (size_t)2 * LU_NB * LU_NB * sizeof(float);
+  const size_t dsm = (size_t)2 * LU_TB * LU_TB * sizeof(float);
   SIE_CUDA(raise_smem(k_trsv_block, dsm));
-  for (int k0 = 0; k0 < n; k0 += LU_NB) {
-    const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
+  for (int k0 = 0; k0 < n; k0 += LU_TB) {
+    const int nb = std::min(LU_TB, n - k0), k1 = k0 + nb;
     k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 1, x);
     count_launch();
     if (k1 < n) {
@@ -637,8 +748,8 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
       count_launch();
     }
   }
-  for (int k0 = ((n - 1) / LU_NB) * LU_NB; k0 >= 0; k0 -= LU_NB) {
-    const int nb = std::min(LU_NB, n - k0);
+  for (int k0 = ((n - 1) / LU_TB) * LU_TB; k0 >= 0; k0 -= LU_TB) {
+    const int nb = std::min(LU_TB, n - k0);
     k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 0, x);
     count_launch();
     if (k0 > 0) {

@@ -1544,22 +1544,30 @@ __global__ void __launch_bounds__(256) k_interp_s(const int* __restrict__ ptr, c
   for (int i = threadIdx.x; i < 8 * Qi; i += blockDim.x) xs[i] = src[i];
   __syncthreads();
   cx<T>* dst = out + b * 8 * (size_t)Qo;
-  for (int t = threadIdx.x; t < 4 * rows; t += blockDim.x) {
-    const int p = t / rows, r = t - p * rows;
-    const cx<T>* a = xs + (size_t)p * Qi;
-    const cx<T>* bb = xs + (size_t)(p + 4) * Qi;
-    cx<T> acc = mk<T>(0, 0);
+  // thread per output row: each stencil tap is read once and applied to the four item
+  // pairs (theta item p and its phi item p + 4)
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    cx<T> acc[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) acc[p] = mk<T>(0, 0);
     for (int k = ptr[r]; k < ptr[r + 1]; k++) {
       const int j = col[k];
-      const cx<T> v = j < Qi ? a[j] : bb[j - Qi];
       const T w = val[k];
-      acc.re = fma(w, v.re, acc.re);
-      acc.im = fma(w, v.im, acc.im);
+      const cx<T>* src = j < Qi ? xs + j : xs + (size_t)4 * Qi + (j - Qi);
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const cx<T> v = src[(size_t)p * Qi];
+        acc[p].re = fma(w, v.re, acc[p].re);
+        acc[p].im = fma(w, v.im, acc[p].im);
+      }
     }
-    const int item = r < Qo ? p : p + 4, q = r < Qo ? r : r - Qo;
-    cx<T>* o = dst + (size_t)item * Qo + q;
-    if (accum) *o += acc;
-    else *o = acc;
+    const int q = r < Qo ? r : r - Qo, i0 = r < Qo ? 0 : 4;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      cx<T>* o = dst + (size_t)(i0 + p) * Qo + q;
+      if (accum) *o += acc[p];
+      else *o = acc[p];
+    }
   }
 }
 

@@ -42,7 +42,22 @@ __global__ void __launch_bounds__(256) k_tile(const float* __restrict__ sr, cons
   *(float*)(blk + 3 * PLANE_BYTES) = il;
 }
 
-// C tile (blockIdx.x, blockIdx.y) -= A tile row blockIdx.x times B tile row blockIdx.y.
+// C tile (mt, nt) -= A tile row mt times B tile row nt.  Persistent: CTA b takes tiles b,
+// b + gridDim.x, ...; the stage ring's phases run on across tiles (chunk counter g), the
+// done barrier flips once per tile, and a CTA barrier after each epilogue frees the
+// accumulators before the next tile's first MMA.
+__device__ __forceinline__ void tile_coords(int tile, int m, int n, int& mt, int& nt) {
+  // groups of GROUP_M row tiles, each swept across the column tiles, so the CTAs in flight
+  // share a few A and B tiles in L2 (a row-tile-fastest order would cycle every A tile of
+  // the operand through L2 for each column tile)
+  const int tm = (m + TILE - 1) / TILE, tn = (n + TILE - 1) / TILE;
+  const int per = GROUP_M * tn;
+  const int g = tile / per, r = tile - g * per;
+  const int gm = min(GROUP_M, tm - g * GROUP_M);
+  nt = r / gm;
+  mt = g * GROUP_M + (r - nt * gm);
+}
+
 __global__ void __launch_bounds__(256, 2) k_gemm(const char* __restrict__ At, const char* __restrict__ Bt,
                                                  int nchunks, float* __restrict__ Cr, float* __restrict__ Ci,
                                                  size_t ldc, int m, int n, int* err) {
@@ -54,7 +69,7 @@ __global__ void __launch_bounds__(256, 2) k_gemm(const char* __restrict__ At, co
   uint32_t* tslot = (uint32_t*)(done + 1);
   __shared__ int fail;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int mt = blockIdx.x, nt = blockIdx.y;
+  const int ntiles = ((m + TILE - 1) / TILE) * ((n + TILE - 1) / TILE);
   if (threadIdx.x == 0) {
     fail = 0;
     for (int s = 0; s < STAGES; s++) {
@@ -73,117 +88,129 @@ __global__ void __launch_bounds__(256, 2) k_gemm(const char* __restrict__ At, co
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
-
-  if (warp == 0 && lane == 0) {
-    // producer: one A block and one B block per stage
-    const char* a0 = At + (size_t)mt * nchunks * BLOCK_BYTES;
-    const char* b0 = Bt + (size_t)nt * nchunks * BLOCK_BYTES;
-    for (int c = 0; c < nchunks; c++) {
-      const int s = c % STAGES;
-      if (c >= STAGES && !mbar_wait(&empty[s], ((c / STAGES) - 1) & 1)) {
-        atomicOr(err, 1);
-        fail = 1;
-        break;
+  int it = 0;
+  unsigned g0 = 0;  // chunks of the earlier tiles of this CTA
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++, g0 += nchunks) {
+    int mt, nt;
+    tile_coords(tile, m, n, mt, nt);
+    if (!fail && warp == 0 && lane == 0) {
+      // producer: one A block and one B block per stage
+      const char* a0 = At + (size_t)mt * nchunks * BLOCK_BYTES;
+      const char* b0 = Bt + (size_t)nt * nchunks * BLOCK_BYTES;
+      for (int c = 0; c < nchunks; c++) {
+        const unsigned g = g0 + c;
+        const int s = g % STAGES;
+        if (g >= STAGES && !mbar_wait(&empty[s], ((g / STAGES) - 1) & 1)) {
+          atomicOr(err, 1);
+          fail = 1;
+          break;
+        }
+        unsigned char* st = sm + s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        bulk_g2s(st, a0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
+        bulk_g2s(st + BLOCK_BYTES, b0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
       }
-      unsigned char* st = sm + s * STAGE_BYTES;
-      mbar_expect_tx(&full[s], STAGE_BYTES);
-      bulk_g2s(st, a0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
-      bulk_g2s(st + BLOCK_BYTES, b0 + (size_t)c * BLOCK_BYTES, BLOCK_BYTES, &full[s]);
-    }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer
-    const uint32_t idp = idesc_tf32(false), idn = idesc_tf32(true);
-    const uint32_t dr = tmem, di = tmem + TILE;
-    bool first = true;
-    for (int c = 0; c < nchunks; c++) {
-      const int s = c % STAGES;
-      if (!mbar_wait(&full[s], (c / STAGES) & 1)) {
-        atomicOr(err, 2);
-        fail = 1;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t sa = smem_u32(sm + s * STAGE_BYTES), sb = sa + BLOCK_BYTES;
+    } else if (!fail && warp == 1 && lane == 0) {
+      // MMA issuer
+      const uint32_t idp = idesc_tf32(false), idn = idesc_tf32(true);
+      const uint32_t dr = tmem, di = tmem + TILE;
+      bool first = true;
+      for (int c = 0; c < nchunks; c++) {
+        const unsigned g = g0 + c;
+        const int s = g % STAGES;
+        if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+          atomicOr(err, 2);
+          fail = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa = smem_u32(sm + s * STAGE_BYTES), sb = sa + BLOCK_BYTES;
 #pragma unroll
-      for (int ks = 0; ks < KC / 8; ks++) {
-        const uint32_t o = ks * 2 * 2048;  // two 4-element core columns per MMA of K = 8
-        const uint64_t arh = smem_desc(sa + o), arl = smem_desc(sa + PLANE_BYTES + o);
-        const uint64_t aih = smem_desc(sa + 2 * PLANE_BYTES + o), ail = smem_desc(sa + 3 * PLANE_BYTES + o);
-        const uint64_t brh = smem_desc(sb + o), brl = smem_desc(sb + PLANE_BYTES + o);
-        const uint64_t bih = smem_desc(sb + 2 * PLANE_BYTES + o), bil = smem_desc(sb + 3 * PLANE_BYTES + o);
-        // Re += Ar Br - Ai Bi
-        mma_tf32(dr, arh, brh, idp, !first);
-        mma_tf32(dr, arh, brl, idp, true);
-        mma_tf32(dr, arl, brh, idp, true);
-        mma_tf32(dr, aih, bih, idn, true);
-        mma_tf32(dr, aih, bil, idn, true);
-        mma_tf32(dr, ail, bih, idn, true);
-        // Im += Ar Bi + Ai Br
-        mma_tf32(di, arh, bih, idp, !first);
-        mma_tf32(di, arh, bil, idp, true);
-        mma_tf32(di, arl, bih, idp, true);
-        mma_tf32(di, aih, brh, idp, true);
-        mma_tf32(di, aih, brl, idp, true);
-        mma_tf32(di, ail, brh, idp, true);
-        first = false;
+        for (int ks = 0; ks < KC / 8; ks++) {
+          const uint32_t o = ks * 2 * 2048;  // two 4-element core columns per MMA of K = 8
+          const uint64_t arh = smem_desc(sa + o), arl = smem_desc(sa + PLANE_BYTES + o);
+          const uint64_t aih = smem_desc(sa + 2 * PLANE_BYTES + o), ail = smem_desc(sa + 3 * PLANE_BYTES + o);
+          const uint64_t brh = smem_desc(sb + o), brl = smem_desc(sb + PLANE_BYTES + o);
+          const uint64_t bih = smem_desc(sb + 2 * PLANE_BYTES + o), bil = smem_desc(sb + 3 * PLANE_BYTES + o);
+          // Re += Ar Br - Ai Bi
+          mma_tf32(dr, arh, brh, idp, !first);
+          mma_tf32(dr, arh, brl, idp, true);
+          mma_tf32(dr, arl, brh, idp, true);
+          mma_tf32(dr, aih, bih, idn, true);
+          mma_tf32(dr, aih, bil, idn, true);
+          mma_tf32(dr, ail, bih, idn, true);
+          // Im += Ar Bi + Ai Br
+          mma_tf32(di, arh, bih, idp, !first);
+          mma_tf32(di, arh, bil, idp, true);
+          mma_tf32(di, arl, bih, idp, true);
+          mma_tf32(di, aih, brh, idp, true);
+          mma_tf32(di, aih, brl, idp, true);
+          mma_tf32(di, ail, brh, idp, true);
+          first = false;
+        }
+        mma_commit(&empty[s]);
       }
-      mma_commit(&empty[s]);
+      // arrives once every MMA issued above has completed
+      mma_commit(done);
     }
-    // arrives once every MMA issued above has completed
-    mma_commit(done);
-  }
-  __syncwarp();
-  const bool ok = mbar_wait(done, 0);
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  if (!ok) atomicOr(err, 4);
-  __syncthreads();
-  if (ok && !fail) {
-    // eight warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows of C) for the column
-    // half w / 4, so twice the loads are in flight
-    const int wl = warp & 3, half = warp >> 2;
-    const int row = mt * TILE + wl * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
+    __syncwarp();
+    const bool ok = mbar_wait(done, it & 1);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok) atomicOr(err, 4);
+    __syncthreads();
+    if (ok && !fail) {
+      // eight warps: warp w reads TMEM lanes 32 (w % 4) .. (its rows of C) for the column
+      // half w / 4, so twice the loads are in flight
+      const int wl = warp & 3, half = warp >> 2;
+      const int row = mt * TILE + wl * 32 + lane;
+      const uint32_t lane_base = tmem + ((uint32_t)(wl * 32) << 16);
 #pragma unroll 1
-    for (int j0 = half * (TILE / 2); j0 < (half + 1) * (TILE / 2); j0 += 16) {
-      uint32_t vr[16], vi[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15}, [%16];"
-          : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]),
-            "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]),
-            "=r"(vr[14]), "=r"(vr[15])
-          : "r"(lane_base + j0));
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15}, [%16];"
-          : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]),
-            "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]),
-            "=r"(vi[14]), "=r"(vi[15])
-          : "r"(lane_base + TILE + j0));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < m) {
-        // 16 loads of C first, then their stores: independent requests in flight
-        const int ncol = min(16, n - (nt * TILE + j0));
-        float* pr = Cr + (size_t)(nt * TILE + j0) * ldc + row;
-        float* pi = Ci + (size_t)(nt * TILE + j0) * ldc + row;
+      for (int j0 = half * (TILE / 2); j0 < (half + 1) * (TILE / 2); j0 += 16) {
+        uint32_t vr[16], vi[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]),
+              "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]),
+              "=r"(vr[14]), "=r"(vr[15])
+            : "r"(lane_base + j0));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]),
+              "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]),
+              "=r"(vi[14]), "=r"(vi[15])
+            : "r"(lane_base + TILE + j0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < m) {
+          // 16 loads of C first, then their stores: independent requests in flight
+          const int ncol = min(16, n - (nt * TILE + j0));
+          float* pr = Cr + (size_t)(nt * TILE + j0) * ldc + row;
+          float* pi = Ci + (size_t)(nt * TILE + j0) * ldc + row;
 #pragma unroll
-        for (int h = 0; h < 16; h += 8) {
-          float cr[8], ci[8];
+          for (int h = 0; h < 16; h += 8) {
+            float cr[8], ci[8];
 #pragma unroll
-          for (int j = 0; j < 8; j++)
-            if (h + j < ncol) {
-              cr[j] = pr[(size_t)(h + j) * ldc];
-              ci[j] = pi[(size_t)(h + j) * ldc];
-            }
+            for (int j = 0; j < 8; j++)
+              if (h + j < ncol) {
+                cr[j] = pr[(size_t)(h + j) * ldc];
+                ci[j] = pi[(size_t)(h + j) * ldc];
+              }
 #pragma unroll
-          for (int j = 0; j < 8; j++)
-            if (h + j < ncol) {
-              pr[(size_t)(h + j) * ldc] = cr[j] - __uint_as_float(vr[h + j]);
-              pi[(size_t)(h + j) * ldc] = ci[j] - __uint_as_float(vi[h + j]);
-            }
+            for (int j = 0; j < 8; j++)
+              if (h + j < ncol) {
+                pr[(size_t)(h + j) * ldc] = cr[j] - __uint_as_float(vr[h + j]);
+                pi[(size_t)(h + j) * ldc] = ci[j] - __uint_as_float(vi[h + j]);
+              }
+          }
         }
       }
     }
+    // every warp has read its accumulators before the next tile's MMAs overwrite them
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (fail || !ok) break;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -206,12 +233,15 @@ int tile_operand(const float* sr, const float* si, size_t ld, int rows, int K, b
   return SIE_OK;
 }
 
-// C (m x n, planes Cr / Ci, leading dimension ldc) -= A B from pre-tiled operands.
+// C (m x n, planes Cr / Ci, leading dimension ldc) -= A B from pre-tiled operands, on at
+// most max_ctas persistent CTAs (0: one per tile).
 int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, size_t ldc, int m, int n,
-                int* d_err, cudaStream_t st) {
+                int* d_err, cudaStream_t st, int max_ctas = 0) {
   SIE_CUDA(raise_smem(k_gemm, SMEM_BYTES));
-  dim3 g(tiles(m), tiles(n));
-  k_gemm<<<g, 256, SMEM_BYTES, st>>>(At, Bt, chunks(K), Cr, Ci, ldc, m, n, d_err);
+  long long nt = (long long)tiles(m) * tiles(n);
+  if (nt > 2147483647LL) return fail(SIE_ERR_ARG, "tensor-core update: too many tiles");
+  if (max_ctas > 0 && nt > max_ctas) nt = max_ctas;
+  k_gemm<<<(unsigned)nt, 256, SMEM_BYTES, st>>>(At, Bt, chunks(K), Cr, Ci, ldc, m, n, d_err);
   count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;

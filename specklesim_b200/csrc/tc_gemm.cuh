@@ -41,6 +41,7 @@ constexpr int STAGE_BYTES = 2 * BLOCK_BYTES;  // A block + B block
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + barriers, alignment slack: 97 KB,
                                                          // two CTAs per SM (TMEM 2 x 256 columns)
 constexpr unsigned WAIT_LIMIT = 1u << 26;   // polls of one mbarrier before giving up
+constexpr int GROUP_M = 16;               // row tiles swept together across the column tiles
 
 // byte offset of element (r, k) inside one plane of a block
 __host__ __device__ __forceinline__ int plane_offset(int r, int k) {
