@@ -8,8 +8,10 @@
 //
 // All vectors and the Hessenberg matrix stay on the device; the host only reads
 // a few scalars per Arnoldi step to steer the iteration.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -32,8 +34,19 @@ struct GmState {
   int passes;       // MGS passes of the last Arnoldi step
   unsigned bar_count, bar_gen;  // grid barrier of the fused Arnoldi kernel
   int bar_err;      // set if a grid barrier wait gave up
-  int pad;
+  int spin_limit;   // polls before a barrier or exchange wait gives up (<= 0: the default)
 };
+
+// Polls of one grid-barrier or exchange wait before it gives up: about a second by
+// default; SIE_GRID_SPIN_LIMIT in the environment sets it (a test makes the waits run out).
+static int grid_spin_limit_host() {
+  const char* e = getenv("SIE_GRID_SPIN_LIMIT");
+  return e ? std::max(1, atoi(e)) : 0;
+}
+__device__ __forceinline__ long long spin_limit(const GmState* gs, long long dflt) {
+  const int v = *(volatile const int*)&gs->spin_limit;
+  return v > 0 ? (long long)v : dflt;
+}
 
 __device__ __forceinline__ zc warp_sum(zc v) {
   for (int o = 16; o > 0; o >>= 1) {
@@ -246,8 +259,9 @@ __device__ void grid_bar(GmState* gs, unsigned nblocks) {
         atomicAdd(&gs->bar_gen, 1u);
       } else {
         long long it = 0;
+        const long long lim = spin_limit(gs, 1LL << 24);
         while (*gen == g && *err == 0) {
-          if (++it > (1LL << 24)) {
+          if (++it > lim) {
             atomicExch(&gs->bar_err, 1);
             break;
           }
@@ -369,9 +383,10 @@ __device__ zc ar_allreduce(zc v, ArSlot* slots, unsigned round, unsigned tag, in
     for (int i = threadIdx.x; i < nb; i += 32) {
       volatile unsigned* pt = &buf[i].tag;
       long long it = 0;
+      const long long lim = spin_limit(gs, 1LL << 22);
       while (*pt != tag) {
         if (*(volatile int*)&gs->bar_err) break;
-        if (++it > (1LL << 22)) {
+        if (++it > lim) {
           atomicExch(&gs->bar_err, 1);
           break;
         }
@@ -845,6 +860,10 @@ int sie::gmres_solve(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solve
   c->tm.gm_passes = c->tm.gm_steps = 0;
   // grid barrier state (bar_count, bar_gen, bar_err) starts clean for every solve
   SIE_CUDA(cudaMemsetAsync(&g.gs->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), s));
+  {
+    const int lim = grid_spin_limit_host();
+    SIE_CUDA(cudaMemcpyAsync(&g.gs->spin_limit, &lim, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
   cudaEventRecord(c->ev[12], s);
   // internal layout: b -> d_yi (kept), x -> d_xi
   zc* b = c->d_yi;
@@ -1151,6 +1170,10 @@ static int inner_gmres32(sie_ctx* c, Gm32& g, const cc* r, cc* z, double tol, in
   k_norm2_t<float><<<RB, RT_, 0, s>>>(r, n, g.part); sie::count_launch();
   k_norm_final<<<1, RT_, 0, s>>>(g.part, RB, g.gs); sie::count_launch();
   SIE_CUDA(cudaMemsetAsync(&g.gs->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), s));
+  {
+    const int lim = grid_spin_limit_host();
+    SIE_CUDA(cudaMemcpyAsync(&g.gs->spin_limit, &lim, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
   GmState h;
   SIE_CUDA(cudaMemcpyAsync(&h, g.gs, sizeof(GmState), cudaMemcpyDeviceToHost, s));
   SIE_CUDA(cudaStreamSynchronize(s));
@@ -1232,6 +1255,10 @@ int fgmres_mixed(sie_ctx* c, const zc* d_b_ext, zc* d_x_ext, const sie_solver_cf
   zc* Z = (zc*)c->d_gmz;
   c->tm.gm_passes = c->tm.gm_steps = 0;
   SIE_CUDA(cudaMemsetAsync(&g.gs->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), s));
+  {
+    const int lim = grid_spin_limit_host();
+    SIE_CUDA(cudaMemcpyAsync(&g.gs->spin_limit, &lim, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
   cudaEventRecord(c->ev[12], s);
   zc* b = c->d_yi;
   zc* x = c->d_xi;

@@ -22,6 +22,7 @@ module sie_gpu_c
   integer(c_int), parameter :: SIE_PMCHWT = 1
   integer(c_int), parameter :: SIE_ICTF = 3
   integer(c_int), parameter :: SIE_FP64 = 0
+  integer(c_int), parameter :: SIE_PRECOND_NEAR = 1
 
   type, bind(C) :: sie_config
     real(c_double) :: lambda
@@ -128,6 +129,21 @@ module sie_gpu_c
       type(c_ptr), value :: ctx, inner
       integer(c_int) :: rc
     end function
+    function sie_solve(ctx, b, x, nrhs, cfg, stats) bind(C, name="sie_solve") result(rc)
+      import :: c_int, c_ptr, sie_solver_cfg, sie_stats
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: b, x
+      integer(c_int), value :: nrhs
+      type(sie_solver_cfg), intent(in) :: cfg
+      type(sie_stats), intent(out) :: stats
+      integer(c_int) :: rc
+    end function
+    function sie_set_preconditioner(ctx, kind) bind(C, name="sie_set_preconditioner") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: kind
+      integer(c_int) :: rc
+    end function
     function sie_free(ctx) bind(C, name="sie_free") result(rc)
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
@@ -176,10 +192,17 @@ module lib_sie_tri_mlfmm_interface
   ! shape gradient of the far-field intensity
   public :: lib_sie_ml_fmm_adjoint_tri
   public :: lib_sie_ml_fmm_grad_z_tri
+  ! the library context, for the GMRES-interface shim (sie_gmres_shim.f90)
+  public :: sie_shim_context
 
   type(c_ptr), save :: m_ctx = c_null_ptr
 
 contains
+
+  function sie_shim_context() result(ctx)
+    type(c_ptr) :: ctx
+    ctx = m_ctx
+  end function sie_shim_context
 
   ! lib_sie_ml_fmm_precalculation_tri (:59-92): mesh, tree, near field, RT, TL, diagonal.
   subroutine lib_sie_ml_fmm_precalculation_tri()

@@ -138,6 +138,24 @@ def test_fortran_shim_matches_the_header():
         assert len(f_args) == len(c_args), cname
 
 
+def test_fortran_gmres_shim_exports_the_reference_procedures():
+    """sie_gmres_shim.f90 stands in for the reference's lib_sie_solver_gmres_interface: it
+    declares the same module and the same public procedures
+    (src/lib_sie_solver_gmres_interface.f90:27-29), and every library function it calls is
+    bound in sie_shim.f90's interface block."""
+    shim2 = open(os.path.join(ROOT, "specklesim_b200", "fortran", "sie_gmres_shim.f90")).read()
+    shim = open(os.path.join(ROOT, "specklesim_b200", "fortran", "sie_shim.f90")).read()
+    assert re.search(r"^module lib_sie_solver_gmres_interface$", shim2, re.M)
+    public = set(re.findall(r"public :: (\w+)", shim2))
+    assert public == {"run_ml_fmm_GMRES_tri", "lib_sie_solver_GMRES_run",
+                      "prerun_ml_fmm_GMRES_tri_conical_planewaves"}
+    for name in public:
+        assert re.search(r"subroutine " + name + r"\(\)", shim2, re.I)
+    bound = set(re.findall(r"bind\(C, name=\"(\w+)\"\)", shim))
+    called = set(re.findall(r"\b(sie_\w+)\(", shim2)) - {"sie_check", "sie_shim_context"}
+    assert called and called <= bound, called - bound
+
+
 def test_ctypes_structs_match_the_header():
     """The ctypes mirrors in specklesim_b200/_lib.py have the header structs' fields in
     order with matching types (Python's reserved 'lambda' is spelled 'lambda_')."""
