@@ -56,7 +56,7 @@ class SpeckleProblem:
     system by LU (exact); otherwise FP64 MLFMM GMRES to `tolerance`."""
 
     def __init__(self, V0, T, top, spline, wavelength, eps_r2, k_in, E_in, pts, dense=False,
-                 tree_s_opt=250, tolerance=1e-10, restart=50, max_iterations=4000):
+                 tree_s_opt=250, tolerance=1e-10, restart=50, max_iterations=4000, mixed_direct=False):
         self.V0 = np.asarray(V0, dtype=float)
         self.T = np.asarray(T)
         self.top = np.asarray(top)
@@ -64,6 +64,10 @@ class SpeckleProblem:
         self.wl, self.eps = wavelength, eps_r2
         self.k_in, self.E_in, self.pts = np.asarray(k_in, float), np.asarray(E_in, float), np.asarray(pts, float)
         self.dense, self.s_opt = dense, tree_s_opt
+        # dense=True with mixed_direct: objective() solves with the complex64 tensor-core LU
+        # and FP64 refinement to `tolerance`; value_and_grad() keeps the FP64 LU, whose
+        # factors also give the adjoint solve
+        self.mixed_direct = mixed_direct
         self.solver = dict(restart=restart, max_iterations=max_iterations, tolerance=tolerance)
 
     def vertices(self, c):
@@ -77,8 +81,11 @@ class SpeckleProblem:
             return Sie(V, self.T, self.wl, self.eps, dense=True).setup()
         return Sie(V, self.T, self.wl, self.eps, tree_s_opt=self.s_opt).setup()
 
-    def _solve(self, g):
+    def _solve(self, g, mixed=True):
         b = g.rhs_planewave(self.k_in, self.E_in)
+        if self.dense and self.mixed_direct and mixed:
+            x, _ = g.solve_direct_mixed(b, tolerance=self.solver["tolerance"])
+            return x
         if self.dense:
             return g.solve_direct(b)
         x, _ = g.solve(b, **self.solver)
@@ -97,7 +104,7 @@ class SpeckleProblem:
         """J and dJ/dc (one forward solve, one adjoint solve)."""
         g = self._context(self.vertices(c))
         try:
-            x = self._solve(g)
+            x = self._solve(g, mixed=False)
             J, dz, _ = g.grad(x, self.k_in, self.E_in, self.pts, **self.solver)
             return J, self.B.T @ dz[self.top]
         finally:
