@@ -224,6 +224,10 @@ int sie_solve_direct_mixed_device(sie_ctx* ctx, const double* d_b, double* d_x, 
  * next direct solve factorises again (e.g. after the caller changed nothing but wants the
  * memory back).  No counterpart in the reference, which factorises in every run. */
 int sie_release_factors(sie_ctx* ctx);
+/* Marks the kept LU factors out of date and keeps their device memory: the next direct
+ * solve factorises again into the same buffers, without allocating.  For a caller that
+ * refactorises the same context repeatedly; sie_release_factors frees the memory. */
+int sie_invalidate_factors(sie_ctx* ctx);
 
 /* Left Jacobi preconditioner, lib_sie_ml_fmm_preconditioner_left
  * (src/lib_sie_tri_mlfmm_interface.f90:323-339): v2 = v1 / diag. */

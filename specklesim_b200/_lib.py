@@ -80,7 +80,7 @@ EXPORTS = [
     "sie_farfield_device_noalloc", "sie_solve_direct", "sie_matvec_adjoint", "sie_matvec_adjoint_device",
     "sie_grad", "sie_set_inner_operator", "sie_autotune", "sie_quadrature_rule",
     "sie_set_preconditioner", "sie_precondition_right", "sie_set_level_truncation",
-    "sie_solve_direct_mixed", "sie_solve_direct_mixed_device", "sie_release_factors",
+    "sie_solve_direct_mixed", "sie_solve_direct_mixed_device", "sie_release_factors", "sie_invalidate_factors",
 ]
 
 _lib = None
@@ -135,6 +135,7 @@ def load(path=None):
         "sie_solve_direct_mixed_device": (C.c_int, [vp, vp, vp, C.c_int, C.c_double, C.c_int,
                                                     C.POINTER(SieStats), vp]),
         "sie_release_factors": (C.c_int, [vp]),
+        "sie_invalidate_factors": (C.c_int, [vp]),
         "sie_matvec_adjoint": (C.c_int, [vp, dp, dp, C.c_int]),
         "sie_set_inner_operator": (C.c_int, [vp, vp]),
         "sie_autotune": (C.c_int, [vp, C.c_int, dp, ip]),

@@ -38,11 +38,11 @@ __global__ void k_expand_dense(const long long* base, const int* box_first, cons
 using namespace sie;
 
 static int lu_factor(sie_ctx* c) {
-  if (c->d_lu) return SIE_OK;
+  if (c->d_lu && c->lu64_valid) return SIE_OK;
   int n = 2 * c->M;
   size_t bytes = (size_t)n * n * sizeof(zc);
-  SIE_CUDA(cudaMalloc(&c->d_lu, bytes));
-  SIE_CUDA(cudaMalloc(&c->d_piv, (size_t)(n + 1) * sizeof(int)));
+  if (!c->d_lu) SIE_CUDA(cudaMalloc(&c->d_lu, bytes));
+  if (!c->d_piv) SIE_CUDA(cudaMalloc(&c->d_piv, (size_t)(n + 1) * sizeof(int)));
   dim3 g(64, std::min(c->near.nbox, 1024));
   k_expand_dense<<<g, 256, 0, c->stream>>>(c->d_base, c->d_box_first, c->d_box_cnt, c->d_ncols,
                                             c->near.nbox, c->d_na, c->d_nb, c->d_nd, c->cfac,
@@ -78,6 +78,7 @@ static int lu_factor(sie_ctx* c) {
     c->d_lu = nullptr;
     c->d_piv = nullptr;
   }
+  c->lu64_valid = rc == SIE_OK;
   return rc;
 }
 

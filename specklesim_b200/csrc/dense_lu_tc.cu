@@ -80,32 +80,40 @@ __device__ __forceinline__ void argmax_pair(float& best, int& bi, float ov, int 
   }
 }
 
-// Grid barrier of the cooperative sub-panel kernel (all its blocks are resident).  The
-// wait is bounded: a block that sees no progress for about a second records the failure
-// in st[2] and stops waiting; later barriers then pass straight through, and the host
-// reports the error.  st = {arrival count, generation, error}.
-__device__ void lu_grid_bar(unsigned* st, unsigned nblocks) {
+// Per-block slot of the panel kernel's pivot search: the block's largest |a|^2 in the
+// column being searched, its row, and that row's values in the sub-panel's columns from
+// the searched column on (the pivot row, if it wins).
+struct PanelSlot {
+  float mx;
+  int ix;
+  float2 row[LU_SB];
+};
+// the panel scratch: error word, two generations of slots, then one barrier counter per
+// sub-panel launch and the barrier's give-up flag
+static const size_t PANEL_SLOTS_OFF = 256;
+static const size_t PANEL_CNT_OFF = PANEL_SLOTS_OFF + 2 * PANEL_MAX_BLOCKS * sizeof(PanelSlot);
+static size_t panel_cnt_bytes(int n) { return ((size_t)n / LU_SB + 2) * sizeof(unsigned); }
+// then the swap plan of the latest panel: {count, src[2 LU_NB], dst[2 LU_NB]}
+static size_t panel_plan_off(int n) { return (PANEL_CNT_OFF + panel_cnt_bytes(n) + 255) / 256 * 256; }
+static size_t panel_scratch_bytes(int n) { return panel_plan_off(n) + (1 + 4 * LU_NB) * sizeof(int); }
+
+// Grid barrier of the cooperative sub-panel kernel (all its blocks are resident) on a
+// counter that only grows within one launch: the m-th barrier waits for m * gridDim.x
+// arrivals.  The wait is bounded: a block that sees no progress for about a second sets
+// *bad and stops waiting; later barriers then pass straight through, and the host reports
+// the error.
+__device__ __forceinline__ void panel_bar(unsigned* cnt, unsigned* bad, unsigned target) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = &st[1];
-    volatile unsigned* bad = &st[2];
-    if (*bad == 0) {
-      const unsigned g = *gen;
-      __threadfence();
-      const unsigned arrived = atomicAdd(&st[0], 1u) + 1u;
-      if (arrived == nblocks) {
-        atomicExch(&st[0], 0u);
-        __threadfence();
-        atomicAdd(&st[1], 1u);
-      } else {
-        long long it = 0;
-        while (*gen == g && *bad == 0) {
-          if (++it > (1LL << 24)) {
-            atomicExch(&st[2], 1u);
-            break;
-          }
-          __nanosleep(64);
-        }
+    __threadfence();
+    atomicAdd(cnt, 1u);
+    volatile unsigned* vc = cnt;
+    volatile unsigned* vb = bad;
+    long long it = 0;
+    while (*vc < target && *vb == 0) {
+      if (++it > (1LL << 21)) {
+        atomicExch(bad, 1u);
+        break;
       }
     }
     __threadfence();
@@ -113,65 +121,125 @@ __device__ void lu_grid_bar(unsigned* st, unsigned nblocks) {
   __syncthreads();
 }
 
-// One sub-panel [s0, s1) of the panel [k0, k1) factorised by one cooperative launch: for
-// each column j, every block reduces the published maxima of column j to the same pivot
-// p, block 0 swaps rows j and p across the panel and records p; after a grid barrier every
-// thread scales its rows of column j by the pivot and updates them in the sub-panel's
-// later columns with row j, and publishes its maximum of the updated column j + 1; a
-// second barrier ends the step.  Matrix reads bypass L1 (__ldcg): rows written by other
-// blocks are seen through L2.  pmax / pidx: one slot per block.
-__global__ void __launch_bounds__(256) k_subpanel(float* Ar, float* Ai, size_t ld, int n, int s0, int s1, int k0,
-                                                  int k1, int* ipiv, int* err, float* pmax, int* pidx,
-                                                  unsigned* bar) {
+// Block-wide argmax of (value, row) pairs (ties to the smaller row); returns the winner to
+// every thread, and whether the calling thread holds it (the lowest such thread).
+__device__ __forceinline__ void block_argmax(float v, int i, float* sv, int* si, int* st, float& bv, int& bi,
+                                             bool& mine) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  float best = v;
+  int idx = i, who = threadIdx.x;
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, idx, o), ow = __shfl_xor_sync(0xffffffffu, who, o);
+    if (ov > best || (ov == best && (oi < idx || (oi == idx && ow < who)))) {
+      best = ov;
+      idx = oi;
+      who = ow;
+    }
+  }
+  if (l == 0) {
+    sv[w] = best;
+    si[w] = idx;
+    st[w] = who;
+  }
+  __syncthreads();
+  best = sv[0];
+  idx = si[0];
+  who = st[0];
+  for (int k = 1; k < (int)(blockDim.x >> 5); k++)
+    if (sv[k] > best || (sv[k] == best && (si[k] < idx || (si[k] == idx && st[k] < who)))) {
+      best = sv[k];
+      idx = si[k];
+      who = st[k];
+    }
+  __syncthreads();  // sv/si/st are reused by the next call
+  bv = best;
+  bi = idx;
+  mine = who == (int)threadIdx.x;
+}
+
+// One sub-panel [s0, s1) of the panel [k0, k1) factorised by one cooperative launch, one
+// grid barrier per column.  Before the barrier that ends column j - 1, every block has
+// published its candidate for column j in slots[gen]: the largest |a|^2 among its rows and
+// that row's values in columns [j, s1).  After it, every block reduces the slots to the
+// same pivot p (the first maximum, as izamax) and takes the pivot row from the winning
+// slot, so nobody reads row p from the matrix.  Row j and row p trade places logically:
+// the thread that owns row p reads the old row j, writes the pivot row into row j and the
+// updated old row j into row p; block 0 swaps the two rows in the panel's other columns,
+// which no other block touches during the launch.  Each row r > j is then scaled and
+// updated, and the block's best candidate for column j + 1 goes to the other generation of
+// slots.  Matrix and slot reads bypass L1 (__ldcg): other blocks' writes are seen through L2.
+__global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_t ld, int n, int s0, int s1, int k0,
+                                                     int k1, int* ipiv, int* err, PanelSlot* slots, unsigned* cnt,
+                                                     unsigned* bad) {
   __shared__ float sv[8];
-  __shared__ int si[8];
-  __shared__ int piv_s;
+  __shared__ int si[8], st[8];
+  __shared__ float2 urow[LU_SB];
+  __shared__ int piv_s, win_s;
   const unsigned G = gridDim.x;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  auto publish = [&](float best, int bi) {
-    for (int o = 16; o > 0; o >>= 1)
-      argmax_pair(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
-    if (l == 0) {
-      sv[w] = best;
-      si[w] = bi;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int k = 1; k < (int)(blockDim.x >> 5); k++) argmax_pair(best, bi, sv[k], si[k]);
-      pmax[blockIdx.x] = best;
-      pidx[blockIdx.x] = bi;
+  unsigned nbar = 0;
+  // publish the block's candidate (row bi, of the column c) into slot generation gen
+  auto publish = [&](float best, int bi, int c, int gen) {
+    float bv;
+    int brow;
+    bool mine;
+    block_argmax(best, bi, sv, si, st, bv, brow, mine);
+    PanelSlot* sl = slots + (size_t)gen * PANEL_MAX_BLOCKS + blockIdx.x;
+    if (mine) {
+      sl->mx = bv;
+      sl->ix = brow;
+      if (brow < n)  // the winner wrote this row itself: its own writes are visible to it
+        for (int k = 0; k < s1 - c; k++)
+          sl->row[k] = make_float2(__ldcg(Ar + (size_t)(c + k) * ld + brow), __ldcg(Ai + (size_t)(c + k) * ld + brow));
     }
   };
-  {  // maxima of the first column
+  {  // candidates of the first column
     float best = -1.f;
     int bi = n;
     for (int r = s0 + gtid; r < n; r += gstride) {
       const float a = __ldcg(Ar + (size_t)s0 * ld + r), b = __ldcg(Ai + (size_t)s0 * ld + r);
       argmax_pair(best, bi, a * a + b * b, r);
     }
-    publish(best, bi);
+    publish(best, bi, s0, 0);
   }
-  lu_grid_bar(bar, G);
+  panel_bar(cnt, bad, ++nbar * G);
   for (int j = s0; j < s1; j++) {
-    if (threadIdx.x < 32) {
-      float best = -1.f;
-      int bi = n;
-      for (int k = threadIdx.x; k < (int)G; k += 32) argmax_pair(best, bi, __ldcg(pmax + k), __ldcg(pidx + k));
-      for (int o = 16; o > 0; o >>= 1)
-        argmax_pair(best, bi, __shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bi, o));
+    const int gen = (j - s0) & 1, wj = s1 - j;
+    // the pivot: every block reduces the same slots in the same way
+    {
+      const PanelSlot* sl = slots + (size_t)gen * PANEL_MAX_BLOCKS;
+      float v = -1.f;
+      int i = n;
+      if (threadIdx.x < G) {
+        v = __ldcg(&sl[threadIdx.x].mx);
+        i = __ldcg(&sl[threadIdx.x].ix);
+      }
+      float bv;
+      int bi;
+      bool mine;
+      block_argmax(v, i, sv, si, st, bv, bi, mine);
+      if (mine) win_s = threadIdx.x;  // the winning block
+      __syncthreads();
+      const int wb = win_s;
+      if (threadIdx.x < wj) {
+        const float2* rw = &sl[wb].row[threadIdx.x];
+        urow[threadIdx.x] = make_float2(__ldcg(&rw->x), __ldcg(&rw->y));
+      }
       if (threadIdx.x == 0) {
         piv_s = bi;
         if (blockIdx.x == 0) {
           ipiv[j] = bi;
-          if (!(best > 0.f) || !isfinite(best) || bi >= n) atomicOr(err, 8);  // singular or non-finite
+          if (!(bv > 0.f) || !isfinite(bv) || bi >= n) atomicOr(err, 8);  // singular or non-finite
         }
       }
+      __syncthreads();
     }
-    __syncthreads();
-    const int p = piv_s;
-    if (blockIdx.x == 0 && p != j && p < n)
+    const int p = piv_s < n ? piv_s : j;
+    // rows j and p in the panel's columns outside [j, s1)
+    if (blockIdx.x == 0 && p != j)
       for (int c = k0 + (int)threadIdx.x; c < k1; c += blockDim.x) {
+        if (c >= j && c < s1) continue;
         const size_t a = (size_t)c * ld + j, b = (size_t)c * ld + p;
         const float tr = __ldcg(Ar + a), ti = __ldcg(Ai + a);
         Ar[a] = __ldcg(Ar + b);
@@ -179,146 +247,279 @@ __global__ void __launch_bounds__(256) k_subpanel(float* Ar, float* Ai, size_t l
         Ar[b] = tr;
         Ai[b] = ti;
       }
-    lu_grid_bar(bar, G);
-    // row j is final: its pivot and its values in the sub-panel's later columns
-    const float pr = __ldcg(Ar + (size_t)j * ld + j), pi = __ldcg(Ai + (size_t)j * ld + j);
-    const float den = pr * pr + pi * pi;
-    const int wj = s1 - j - 1;
-    float ur[LU_SB], ui[LU_SB];
-#pragma unroll
-    for (int k = 0; k < LU_SB; k++)
-      if (k < wj) {
-        ur[k] = __ldcg(Ar + (size_t)(j + 1 + k) * ld + j);
-        ui[k] = __ldcg(Ai + (size_t)(j + 1 + k) * ld + j);
-      }
+    const float2 pv = urow[0];
+    const float den = pv.x * pv.x + pv.y * pv.y;
     float best = -1.f;
     int bi = n;
     for (int r = j + 1 + gtid; r < n; r += gstride) {
-      // every load of the row first (one round trip to L2), then the arithmetic and stores
-      float ar = __ldcg(Ar + (size_t)j * ld + r), ai = __ldcg(Ai + (size_t)j * ld + r);
+      const int src = r == p ? j : r;  // logical row r lives in physical row j until now
       float xr[LU_SB], xi[LU_SB];
 #pragma unroll
       for (int k = 0; k < LU_SB; k++)
         if (k < wj) {
-          const size_t o = (size_t)(j + 1 + k) * ld + r;
+          const size_t o = (size_t)(j + k) * ld + src;
           xr[k] = __ldcg(Ar + o);
           xi[k] = __ldcg(Ai + o);
         }
-      const float lr = (ar * pr + ai * pi) / den, li = (ai * pr - ar * pi) / den;
+      if (r == p) {  // row j becomes the pivot row
+#pragma unroll
+        for (int k = 0; k < LU_SB; k++)
+          if (k < wj) {
+            const size_t o = (size_t)(j + k) * ld + j;
+            Ar[o] = urow[k].x;
+            Ai[o] = urow[k].y;
+          }
+      }
+      const float lr = (xr[0] * pv.x + xi[0] * pv.y) / den, li = (xi[0] * pv.x - xr[0] * pv.y) / den;
       Ar[(size_t)j * ld + r] = lr;
       Ai[(size_t)j * ld + r] = li;
 #pragma unroll
-      for (int k = 0; k < LU_SB; k++)
+      for (int k = 1; k < LU_SB; k++)
         if (k < wj) {
-          const size_t o = (size_t)(j + 1 + k) * ld + r;
-          xr[k] -= lr * ur[k] - li * ui[k];
-          xi[k] -= lr * ui[k] + li * ur[k];
+          const float ur = urow[k].x, ui = urow[k].y;
+          xr[k] -= lr * ur - li * ui;
+          xi[k] -= lr * ui + li * ur;
+          const size_t o = (size_t)(j + k) * ld + r;
           Ar[o] = xr[k];
           Ai[o] = xi[k];
         }
-      if (wj > 0) argmax_pair(best, bi, xr[0] * xr[0] + xi[0] * xi[0], r);
+      if (wj > 1) argmax_pair(best, bi, xr[1] * xr[1] + xi[1] * xi[1], r);
     }
-    if (j + 1 < s1) publish(best, bi);
-    lu_grid_bar(bar, G);
+    if (j + 1 < s1) {
+      publish(best, bi, j + 1, gen ^ 1);
+      panel_bar(cnt, bad, ++nbar * G);
+    }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bar + 2) != 0) atomicOr(err, 16);  // a barrier gave up
+  if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bad) != 0) atomicOr(err, 16);  // a barrier gave up
 }
 
 // Sub-panel [s0, s1) of a panel ending at k1: its rows of the panel's later columns,
-// U = L11^-1 A (L11 the unit lower triangle of the sub-panel's diagonal block).  Thread
-// per column c in [s1, k1).
-__global__ void k_sub_trsm(float* Ar, float* Ai, size_t ld, int s0, int s1, int k1) {
+// U = L11^-1 A (L11 the unit lower triangle of the sub-panel's diagonal block).  L11 in
+// shared memory; thread per column c in [s1, k1), its w values loaded together.
+__global__ void __launch_bounds__(LU_NB) k_sub_trsm(float* Ar, float* Ai, size_t ld, int s0, int s1, int k1) {
+  __shared__ float Lr[LU_SB][LU_SB], Li[LU_SB][LU_SB];  // [column t][row i]
+  const int w = s1 - s0;
+  for (int e = threadIdx.x; e < LU_SB * LU_SB; e += blockDim.x) {
+    const int t = e / LU_SB, i = e - t * LU_SB;
+    const bool in = t < w && i < w;
+    Lr[t][i] = in ? Ar[(size_t)(s0 + t) * ld + s0 + i] : 0.f;
+    Li[t][i] = in ? Ai[(size_t)(s0 + t) * ld + s0 + i] : 0.f;
+  }
+  __syncthreads();
   const int c = s1 + blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= k1) return;
-  const int w = s1 - s0;
   float xr[LU_SB], xi[LU_SB];
-  for (int i = 0; i < w; i++) {
-    xr[i] = Ar[(size_t)c * ld + s0 + i];
-    xi[i] = Ai[(size_t)c * ld + s0 + i];
+#pragma unroll
+  for (int i = 0; i < LU_SB; i++) {
+    xr[i] = i < w ? Ar[(size_t)c * ld + s0 + i] : 0.f;
+    xi[i] = i < w ? Ai[(size_t)c * ld + s0 + i] : 0.f;
   }
-  for (int i = 1; i < w; i++)
+#pragma unroll
+  for (int i = 1; i < LU_SB; i++)
+#pragma unroll
     for (int t = 0; t < i; t++) {
-      const float lr = Ar[(size_t)(s0 + t) * ld + s0 + i], li = Ai[(size_t)(s0 + t) * ld + s0 + i];
+      const float lr = Lr[t][i], li = Li[t][i];
       xr[i] -= lr * xr[t] - li * xi[t];
       xi[i] -= lr * xi[t] + li * xr[t];
     }
-  for (int i = 1; i < w; i++) {
-    Ar[(size_t)c * ld + s0 + i] = xr[i];
-    Ai[(size_t)c * ld + s0 + i] = xi[i];
-  }
+#pragma unroll
+  for (int i = 1; i < LU_SB; i++)
+    if (i < w) {
+      Ar[(size_t)c * ld + s0 + i] = xr[i];
+      Ai[(size_t)c * ld + s0 + i] = xi[i];
+    }
 }
 
 // Rank-w update of the panel's later columns by a factored sub-panel [s0, s1):
 // a_rc -= sum_t l_rt u_tc for rows r >= s1 and columns c in [s1, k1).  The sub-panel's U
-// rows in shared memory; thread per row.
-__global__ void __launch_bounds__(256) k_sub_update(float* Ar, float* Ai, size_t ld, int n, int s0, int s1,
+// rows in shared memory; thread per row, its w L values in registers, the columns in
+// groups of 8 whose loads are issued together.
+static const int LU_UPD_CG = 8;
+__global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, size_t ld, int n, int s0, int s1,
                                                     int k1) {
   __shared__ float ur[LU_SB][LU_NB], ui[LU_SB][LU_NB];
   const int w = s1 - s0, nc = k1 - s1;
-  for (int e = threadIdx.x; e < w * nc; e += blockDim.x) {
-    const int t = e / nc, c = e - t * nc;
-    ur[t][c] = Ar[(size_t)(s1 + c) * ld + s0 + t];
-    ui[t][c] = Ai[(size_t)(s1 + c) * ld + s0 + t];
+  for (int e0 = threadIdx.x; e0 < LU_SB * LU_NB; e0 += 4 * blockDim.x) {
+    float vr[4], vi[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = e0 + q * blockDim.x, t = e / LU_NB, c = e - t * LU_NB;
+      const bool in = e < LU_SB * LU_NB && t < w && c < nc;
+      vr[q] = in ? Ar[(size_t)(s1 + c) * ld + s0 + t] : 0.f;
+      vi[q] = in ? Ai[(size_t)(s1 + c) * ld + s0 + t] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int e = e0 + q * blockDim.x, t = e / LU_NB, c = e - t * LU_NB;
+      if (e < LU_SB * LU_NB) {
+        ur[t][c] = vr[q];
+        ui[t][c] = vi[q];
+      }
+    }
   }
   __syncthreads();
   const int r = s1 + blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
   float lr[LU_SB], li[LU_SB];
-  for (int t = 0; t < w; t++) {
-    lr[t] = Ar[(size_t)(s0 + t) * ld + r];
-    li[t] = Ai[(size_t)(s0 + t) * ld + r];
-  }
-  for (int c = 0; c < nc; c++) {
-    float sr = 0.f, si = 0.f;
 #pragma unroll
-    for (int t = 0; t < LU_SB; t++)
-      if (t < w) {
-        sr += lr[t] * ur[t][c] - li[t] * ui[t][c];
-        si += lr[t] * ui[t][c] + li[t] * ur[t][c];
+  for (int t = 0; t < LU_SB; t++) {
+    lr[t] = t < w ? Ar[(size_t)(s0 + t) * ld + r] : 0.f;
+    li[t] = t < w ? Ai[(size_t)(s0 + t) * ld + r] : 0.f;
+  }
+#pragma unroll 1
+  for (int c0 = 0; c0 < nc; c0 += LU_UPD_CG) {
+    float cr[LU_UPD_CG], ci[LU_UPD_CG];
+#pragma unroll
+    for (int g = 0; g < LU_UPD_CG; g++) {
+      const size_t o = (size_t)(s1 + c0 + g) * ld + r;
+      cr[g] = c0 + g < nc ? Ar[o] : 0.f;
+      ci[g] = c0 + g < nc ? Ai[o] : 0.f;
+    }
+#pragma unroll
+    for (int t = 0; t < LU_SB; t++) {  // rows t >= w of ur/ui are zero
+      const float l_r = lr[t], l_i = li[t];
+#pragma unroll
+      for (int g = 0; g < LU_UPD_CG; g++) {
+        const float a = ur[t][c0 + g], b = ui[t][c0 + g];
+        cr[g] -= l_r * a - l_i * b;
+        ci[g] -= l_r * b + l_i * a;
       }
-    const size_t o = (size_t)(s1 + c) * ld + r;
-    Ar[o] -= sr;
-    Ai[o] -= si;
+    }
+#pragma unroll
+    for (int g = 0; g < LU_UPD_CG; g++)
+      if (c0 + g < nc) {
+        const size_t o = (size_t)(s1 + c0 + g) * ld + r;
+        Ar[o] = cr[g];
+        Ai[o] = ci[g];
+      }
   }
 }
 
-// Row swaps ipiv[k0 .. k1) applied in order to the columns [c, c + 1) of every thread
-// outside the panel [k0, k1).
-__global__ void k_laswp(float* Ar, float* Ai, size_t ld, int n, int k0, int k1, const int* ipiv) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
+// The row swaps ipiv[k0 .. k1) of one panel (applied in order, as LAPACK's laswp) as one
+// gather: after them, row dst[i] holds the old row src[i], for the nb positions of the
+// panel and the rows outside it that the swaps reach (at most nb more).  One block; the
+// swaps are followed in order, the lookup of a row outside the panel searched by all
+// threads.  plan = {count, src[2 LU_NB], dst[2 LU_NB]}.
+__global__ void __launch_bounds__(256) k_swap_plan(const int* ipiv, int k0, int k1, int* plan) {
+  __shared__ int pos[2 * LU_NB], cont[2 * LU_NB], ip[LU_NB];
+  __shared__ int nx, found;
+  const int nb = k1 - k0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    pos[i] = cont[i] = k0 + i;
+    ip[i] = ipiv[k0 + i];
+  }
+  if (threadIdx.x == 0) nx = 0;
+  __syncthreads();
+  for (int j = 0; j < nb; j++) {
+    const int p = ip[j];
+    if (p == k0 + j) continue;  // uniform: every thread reads the same ip[j]
+    int idx = p - k0;
+    if (p >= k1) {
+      if (threadIdx.x == 0) found = -1;
+      __syncthreads();
+      for (int t = threadIdx.x; t < nx; t += blockDim.x)
+        if (pos[nb + t] == p) found = nb + t;
+      __syncthreads();
+      if (threadIdx.x == 0 && found < 0) {
+        pos[nb + nx] = cont[nb + nx] = p;
+        found = nb + nx;
+        nx++;
+      }
+      __syncthreads();
+      idx = found;
+    }
+    if (threadIdx.x == 0) {
+      const int t = cont[j];
+      cont[j] = cont[idx];
+      cont[idx] = t;
+    }
+    __syncthreads();
+  }
+  const int cnt = nb + nx;
+  for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+    plan[1 + i] = cont[i];
+    plan[1 + 2 * LU_NB + i] = pos[i];
+  }
+  if (threadIdx.x == 0) plan[0] = cnt;
+}
+
+// The plan applied to every column outside the panel [k0, k1): a block per tile of
+// LU_SWAP_TC columns, a thread per plan entry; all of a tile's reads happen before any
+// of its writes.
+static const int LU_SWAP_TC = 8;
+__global__ void __launch_bounds__(512) k_swap_apply(float* Ar, float* Ai, size_t ld, int n, int k0, int k1,
+                                                    const int* plan) {
+  const int cnt = plan[0];
+  const int i = threadIdx.x;
   const int outside = n - (k1 - k0);
-  if (c >= outside) return;
-  if (c >= k0) c += k1 - k0;
-  float* cr = Ar + (size_t)c * ld;
-  float* ci = Ai + (size_t)c * ld;
-  for (int j = k0; j < k1; j++) {
-    const int p = ipiv[j];
-    if (p != j) {
-      float t = cr[j];
-      cr[j] = cr[p];
-      cr[p] = t;
-      t = ci[j];
-      ci[j] = ci[p];
-      ci[p] = t;
+  int src = 0, dst = 0;
+  if (i < cnt) {
+    src = plan[1 + i];
+    dst = plan[1 + 2 * LU_NB + i];
+  }
+  float vr[LU_SWAP_TC], vi[LU_SWAP_TC];
+  const int c0 = blockIdx.x * LU_SWAP_TC;
+#pragma unroll
+  for (int t = 0; t < LU_SWAP_TC; t++) {
+    int c = c0 + t;
+    vr[t] = vi[t] = 0.f;
+    if (i < cnt && c < outside) {
+      if (c >= k0) c += k1 - k0;
+      vr[t] = Ar[(size_t)c * ld + src];
+      vi[t] = Ai[(size_t)c * ld + src];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int t = 0; t < LU_SWAP_TC; t++) {
+    int c = c0 + t;
+    if (i < cnt && c < outside) {
+      if (c >= k0) c += k1 - k0;
+      Ar[(size_t)c * ld + dst] = vr[t];
+      Ai[(size_t)c * ld + dst] = vi[t];
+    }
+  }
+}
+
+// Copies the nb x nb diagonal block at (k0, k0) of the two planes into shared memory
+// ([col][row], leading dimension LU_TB), eight loads in flight per thread.
+__device__ __forceinline__ void stage_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb, float* Dr,
+                                            float* Di) {
+  const int tot = nb * nb;
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 8 * blockDim.x) {
+    float vr[8], vi[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * blockDim.x;
+      const int col = e / nb, row = e - col * nb;
+      vr[q] = e < tot ? Ar[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
+      vi[q] = e < tot ? Ai[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * blockDim.x;
+      const int col = e / nb, row = e - col * nb;
+      if (e < tot) {
+        Dr[col * LU_TB + row] = vr[q];
+        Di[col * LU_TB + row] = vi[q];
+      }
     }
   }
 }
 
 // X = L^-1 X in place for a diagonal block of the factors: L the unit lower triangle of
 // the nb x nb block at (k0, k0) (nb <= LU_TB), X its rows [k0, k0 + nb) in columns [c0, n).
-// L in shared memory; one warp per column, lane l holding rows l, l + 32, l + 64, l + 96.
-__global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld, int n, int k0, int nb, int c0) {
+// L in shared memory (staged once per block: the grid is one block per multiprocessor, 16
+// warps each); one warp per column, lane l holding rows l, l + 32, l + 64, l + 96.
+__global__ void __launch_bounds__(512) k_trsm_l(float* Ar, float* Ai, size_t ld, int n, int k0, int nb, int c0) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float* Lr = reinterpret_cast<float*>(smraw);  // [col][row], nb x nb
   float* Li = Lr + LU_TB * LU_TB;
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int col = e / nb, row = e - col * nb;
-    Lr[col * LU_TB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
-    Li[col * LU_TB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
-  }
+  stage_block(Ar, Ai, ld, k0, nb, Lr, Li);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = c0 + blockIdx.x * 8 + warp; c < n; c += gridDim.x * 8) {
+  const int nw = blockDim.x >> 5;
+  for (int c = c0 + blockIdx.x * nw + warp; c < n; c += gridDim.x * nw) {
     float* cr = Ar + (size_t)c * ld + k0;
     float* ci = Ai + (size_t)c * ld + k0;
     float xr[4], xi[4];
@@ -360,76 +561,79 @@ __global__ void __launch_bounds__(256) k_trsm_l(float* Ar, float* Ai, size_t ld,
 
 // Solves with the factors, one vector (complex64, internal order) in place.  Diagonal
 // block: x[k0 .. k0 + nb) = L11^-1 x (lower, unit diagonal) or U11^-1 x (upper), with the
-// block staged in shared memory first (coalesced), then one warp runs the substitution.
-__global__ void __launch_bounds__(256) k_trsv_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
-                                                    int lower, cc* x) {
+// block staged in shared memory first; thread r < nb owns x_r, one barrier per step.
+__global__ void __launch_bounds__(LU_TB) k_trsv_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
+                                                      int lower, cc* x) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
   float* Di = Dr + LU_TB * LU_TB;
-  __shared__ float br[LU_TB], bi[LU_TB];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int col = e / nb, row = e - col * nb;
-    Dr[col * LU_TB + row] = Ar[(size_t)(k0 + col) * ld + k0 + row];
-    Di[col * LU_TB + row] = Ai[(size_t)(k0 + col) * ld + k0 + row];
-  }
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) {
+  __shared__ float br[LU_TB], bi[LU_TB], yr[LU_TB], yi[LU_TB];
+  stage_block(Ar, Ai, ld, k0, nb, Dr, Di);
+  const int r = threadIdx.x;
+  if (r < nb) {
     br[r] = x[k0 + r].re;
     bi[r] = x[k0 + r].im;
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    if (lower) {
-      for (int i = 0; i < nb; i++) {
-        const float vr = br[i], vi = bi[i];
-        __syncwarp();
-        for (int r = i + 1 + lane; r < nb; r += 32) {
-          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
-          br[r] -= lr * vr - li * vi;
-          bi[r] -= lr * vi + li * vr;
-        }
-        __syncwarp();
+  if (lower) {
+    // step i: x_i is final; every row below it loses L_ri x_i
+    for (int i = 0; i < nb; i++) {
+      const float vr = br[i], vi = bi[i];
+      if (r > i && r < nb) {
+        const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+        br[r] -= lr * vr - li * vi;
+        bi[r] -= lr * vi + li * vr;
       }
-    } else {
-      for (int i = nb - 1; i >= 0; i--) {
-        if (lane == 0) {
-          const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
-          const float den = ur * ur + ui * ui;
-          const float xr = (br[i] * ur + bi[i] * ui) / den, xi = (bi[i] * ur - br[i] * ui) / den;
-          br[i] = xr;
-          bi[i] = xi;
-        }
-        __syncwarp();
-        const float vr = br[i], vi = bi[i];
-        for (int r = lane; r < i; r += 32) {
-          const float ur = Dr[i * LU_TB + r], ui = Di[i * LU_TB + r];
-          br[r] -= ur * vr - ui * vi;
-          bi[r] -= ur * vi + ui * vr;
-        }
-        __syncwarp();
-      }
+      __syncthreads();
     }
+    if (r < nb) x[k0 + r] = mk<float>(br[r], bi[r]);
+  } else {
+    // step i (downward): y_i = x_i / U_ii (every thread forms it; thread i keeps it), and
+    // every row above loses U_ri y_i
+    for (int i = nb - 1; i >= 0; i--) {
+      const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
+      const float den = ur * ur + ui * ui;
+      const float vr = (br[i] * ur + bi[i] * ui) / den, vi = (bi[i] * ur - br[i] * ui) / den;
+      if (r == i) {
+        yr[i] = vr;
+        yi[i] = vi;
+      } else if (r < i) {
+        const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+        br[r] -= lr * vr - li * vi;
+        bi[r] -= lr * vi + li * vr;
+      }
+      __syncthreads();
+    }
+    if (r < nb) x[k0 + r] = mk<float>(yr[r], yi[r]);
   }
-  __syncthreads();
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) x[k0 + r] = mk<float>(br[r], bi[r]);
 }
 
-// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb); thread per row.
+// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb); thread per row, 16
+// columns' loads in flight at a time.
 __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
                                                    int r0, int r1, cc* x) {
   __shared__ float br[LU_TB], bi[LU_TB];
-  for (int r = threadIdx.x; r < nb; r += blockDim.x) {
-    br[r] = x[k0 + r].re;
-    bi[r] = x[k0 + r].im;
+  for (int r = threadIdx.x; r < LU_TB; r += blockDim.x) {
+    br[r] = r < nb ? x[k0 + r].re : 0.f;
+    bi[r] = r < nb ? x[k0 + r].im : 0.f;
   }
   __syncthreads();
   const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r1) return;
   float sr = 0.f, si = 0.f;
-  for (int j = 0; j < nb; j++) {
-    const float ar = Ar[(size_t)(k0 + j) * ld + i], ai = Ai[(size_t)(k0 + j) * ld + i];
-    sr += ar * br[j] - ai * bi[j];
-    si += ar * bi[j] + ai * br[j];
+  for (int j0 = 0; j0 < nb; j0 += 16) {
+    float ar[16], ai[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const size_t o = (size_t)(k0 + j0 + q) * ld + i;
+      ar[q] = j0 + q < nb ? Ar[o] : 0.f;
+      ai[q] = j0 + q < nb ? Ai[o] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      sr += ar[q] * br[j0 + q] - ai[q] * bi[j0 + q];
+      si += ar[q] * bi[j0 + q] + ai[q] * br[j0 + q];
+    }
   }
   x[i].re -= sr;
   x[i].im -= si;
@@ -475,42 +679,41 @@ struct LuTc {
 };
 
 static int lu_tc_factor(sie_ctx* c) {
-  if (c->d_lu32) return SIE_OK;
+  if (c->d_lu32 && c->lu32_valid) return SIE_OK;
+  c->lu32_valid = false;
   const int n = 2 * c->M;
   const size_t ld = (size_t)n;
   cudaStream_t s = c->stream;
-  float *Ar = nullptr, *Ai = nullptr;
-  int *ipiv = nullptr, *err = nullptr;
-  char *At = nullptr, *Bt = nullptr;
-  void* pscr = nullptr;  // pivot search: per-block maxima and indices, and the block counter
-  int rc = SIE_OK;
-  auto cleanup = [&]() {
-    if (At) cudaFree(At);
-    if (Bt) cudaFree(Bt);
-    if (err) cudaFree(err);
-    if (pscr) cudaFree(pscr);
-  };
-  SIE_CUDA(cudaMalloc(&Ar, ld * n * sizeof(float)));
-  if (cudaMalloc(&Ai, ld * n * sizeof(float)) != cudaSuccess || cudaMalloc(&ipiv, (size_t)n * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&err, sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&At, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess ||
-      cudaMalloc(&Bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess ||
-      cudaMalloc(&pscr, (size_t)PANEL_MAX_BLOCKS * 8 + 64) != cudaSuccess) {
-    cudaFree(Ar);
-    if (Ai) cudaFree(Ai);
-    if (ipiv) cudaFree(ipiv);
-    cleanup();
+  // the factors and the workspace stay allocated until sie_release_factors (a later
+  // factorisation of the same context reuses them)
+  const size_t scr_bytes = panel_scratch_bytes(n);
+  if (!c->d_lu32 && cudaMalloc(&c->d_lu32, ld * n * sizeof(float)) != cudaSuccess) c->d_lu32 = nullptr;
+  if (!c->d_lu32i && cudaMalloc(&c->d_lu32i, ld * n * sizeof(float)) != cudaSuccess) c->d_lu32i = nullptr;
+  if (!c->d_piv32 && cudaMalloc(&c->d_piv32, (size_t)n * sizeof(int)) != cudaSuccess) c->d_piv32 = nullptr;
+  if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_at = nullptr;
+  if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_bt = nullptr;
+  if (!c->d_lu_scr || c->lu_scr_bytes < scr_bytes) {
+    if (c->d_lu_scr) cudaFree(c->d_lu_scr);
+    if (cudaMalloc(&c->d_lu_scr, scr_bytes) != cudaSuccess) c->d_lu_scr = nullptr;
+    c->lu_scr_bytes = c->d_lu_scr ? scr_bytes : 0;
+  }
+  if (!c->d_lu32 || !c->d_lu32i || !c->d_piv32 || !c->d_lu_at || !c->d_lu_bt || !c->d_lu_scr) {
+    cudaGetLastError();
     return fail(SIE_ERR_NOMEM, "mixed LU: device memory");
   }
-  c->d_lu32 = Ar;
-  c->d_lu32i = Ai;
-  c->d_piv32 = ipiv;
+  float* Ar = c->d_lu32;
+  float* Ai = c->d_lu32i;
+  int* ipiv = c->d_piv32;
+  char* At = c->d_lu_at;
+  char* Bt = c->d_lu_bt;
+  int* err = (int*)c->d_lu_scr;
+  PanelSlot* slots = (PanelSlot*)((char*)c->d_lu_scr + PANEL_SLOTS_OFF);
+  unsigned* pcnt = (unsigned*)((char*)c->d_lu_scr + PANEL_CNT_OFF);  // one counter per sub-panel launch
+  unsigned* pbad = pcnt + (n / LU_SB + 1);
+  int* plan = (int*)((char*)c->d_lu_scr + panel_plan_off(n));
+  int rc = SIE_OK;
   auto t0 = std::chrono::steady_clock::now();
-  cudaMemsetAsync(err, 0, sizeof(int), s);
-  float* pmax = (float*)pscr;
-  int* pidx = (int*)((char*)pscr + (size_t)PANEL_MAX_BLOCKS * 4);
-  unsigned* pbar = (unsigned*)((char*)pscr + (size_t)PANEL_MAX_BLOCKS * 8);  // count, generation, error
-  cudaMemsetAsync(pbar, 0, 4 * sizeof(unsigned), s);
+  cudaMemsetAsync(c->d_lu_scr, 0, scr_bytes, s);
   {
     dim3 g(64, std::min(c->near.nbox, 1024));
     k_expand_dense32<<<g, 256, 0, s>>>(c->d_base, c->d_box_first, c->d_box_cnt, c->d_ncols, c->near.nbox, c->d_na,
@@ -575,10 +778,14 @@ static int lu_tc_factor(sie_ctx* c) {
   const char* la = getenv("SIE_LU_LOOKAHEAD");
   const bool lookahead = !(la && atoi(la) == 0);
   // the cooperative panel kernel: blocks that fit on the multiprocessors the look-ahead
-  // update leaves free (all of them resident at once)
+  // update leaves free, or on all of them without look-ahead (all resident at once)
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpanel, 256, 0) != cudaSuccess) per_sm = 1;
-  const int panel_blocks = std::max(1, std::min(PANEL_MAX_BLOCKS, std::min(per_sm, 4) * std::max(free_sms, 1)));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_subpanel, 256, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int panel_sms = lookahead ? std::max(free_sms, 1) : nsm;
+  int panel_blocks = std::max(1, std::min(PANEL_MAX_BLOCKS, std::min(per_sm, 4) * panel_sms));
+  if (const char* e = getenv("SIE_LU_PANEL_BLOCKS"))
+    panel_blocks = std::max(1, std::min(panel_blocks, atoi(e)));
   s = sp;  // the phase marks and the panel chain
   bool rest_pending = false;
   for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += LU_NB) {
@@ -591,7 +798,8 @@ static int lu_tc_factor(sie_ctx* c) {
       {
         int ns0 = s0, ns1 = s1, nn0 = n, kk0 = k0, kk1 = k1;
         size_t ldd = ld;
-        void* args[] = {&Ar, &Ai, &ldd, &nn0, &ns0, &ns1, &kk0, &kk1, &ipiv, &err, &pmax, &pidx, &pbar};
+        unsigned* cnt = pcnt + s0 / LU_SB;  // a fresh (zeroed) counter for every launch
+        void* args[] = {&Ar, &Ai, &ldd, &nn0, &ns0, &ns1, &kk0, &kk1, &ipiv, &err, &slots, &cnt, &pbad};
         if (cudaLaunchCooperativeKernel((const void*)k_subpanel, dim3(panel_blocks), dim3(256), args, 0, sp) !=
             cudaSuccess) {
           rc = fail(SIE_ERR_CUDA, "mixed LU: cooperative panel launch");
@@ -612,7 +820,9 @@ static int lu_tc_factor(sie_ctx* c) {
     if (rest_pending) cudaStreamWaitEvent(sp, ev_rest, 0);  // the previous trailing update
     mark(1, true, pk);
     if (n - nb > 0) {
-      k_laswp<<<(n - nb + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, k0, k1, ipiv);
+      k_swap_plan<<<1, 256, 0, sp>>>(ipiv, k0, k1, plan);
+      count_launch();
+      k_swap_apply<<<(n - nb + LU_SWAP_TC - 1) / LU_SWAP_TC, 2 * LU_NB, 0, sp>>>(Ar, Ai, ld, n, k0, k1, plan);
       count_launch();
     }
     mark(1, false, pk);
@@ -622,7 +832,7 @@ static int lu_tc_factor(sie_ctx* c) {
       // rows below it in the panel lose L21-block times them (a tensor-core update)
       for (int d0 = k0; d0 < k1 && rc == SIE_OK; d0 += LU_TB) {
         const int db = std::min(LU_TB, k1 - d0), d1 = d0 + db;
-        k_trsm_l<<<std::min(1184, (n - k1 + 7) / 8), 256, trsm_smem, sp>>>(Ar, Ai, ld, n, d0, db, k1);
+        k_trsm_l<<<std::min(nsm, (n - k1 + 15) / 16), 512, trsm_smem, sp>>>(Ar, Ai, ld, n, d0, db, k1);
         count_launch();
         if (d1 < k1) {
           const int mb = k1 - d1;
@@ -687,8 +897,8 @@ static int lu_tc_factor(sie_ctx* c) {
     if (cudaMemcpy(piv.data(), ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
       rc = fail(SIE_ERR_CUDA, "mixed LU: pivots");
     for (int j = 0; j < n && rc == SIE_OK; j++) std::swap(perm[j], perm[piv[j]]);
-    if (rc == SIE_OK && (cudaMalloc(&c->d_perm32, (size_t)n * sizeof(int)) != cudaSuccess ||
-                         cudaMalloc(&c->d_tmp32, (size_t)n * sizeof(cc)) != cudaSuccess ||
+    if (rc == SIE_OK && ((!c->d_perm32 && cudaMalloc(&c->d_perm32, (size_t)n * sizeof(int)) != cudaSuccess) ||
+                         (!c->d_tmp32 && cudaMalloc(&c->d_tmp32, (size_t)n * sizeof(cc)) != cudaSuccess) ||
                          cudaMemcpy(c->d_perm32, perm.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice) !=
                              cudaSuccess))
       rc = fail(SIE_ERR_NOMEM, "mixed LU: permutation");
@@ -718,14 +928,7 @@ static int lu_tc_factor(sie_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (sp) cudaStreamDestroy(sp);
   if (sg) cudaStreamDestroy(sg);
-  cleanup();
-  if (rc != SIE_OK) {
-    for (void* p : {(void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32, (void*)c->d_perm32, (void*)c->d_tmp32})
-      if (p) cudaFree(p);
-    c->d_lu32 = c->d_lu32i = nullptr;
-    c->d_piv32 = c->d_perm32 = nullptr;
-    c->d_tmp32 = nullptr;
-  }
+  c->lu32_valid = rc == SIE_OK;
   return rc;
 }
 
@@ -741,7 +944,7 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   SIE_CUDA(raise_smem(k_trsv_block, dsm));
   for (int k0 = 0; k0 < n; k0 += LU_TB) {
     const int nb = std::min(LU_TB, n - k0), k1 = k0 + nb;
-    k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 1, x);
+    k_trsv_block<<<1, LU_TB, dsm, s>>>(Ar, Ai, ld, k0, nb, 1, x);
     count_launch();
     if (k1 < n) {
       k_trsv_gemv<<<(n - k1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
@@ -750,7 +953,7 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   }
   for (int k0 = ((n - 1) / LU_TB) * LU_TB; k0 >= 0; k0 -= LU_TB) {
     const int nb = std::min(LU_TB, n - k0);
-    k_trsv_block<<<1, 256, dsm, s>>>(Ar, Ai, ld, k0, nb, 0, x);
+    k_trsv_block<<<1, LU_TB, dsm, s>>>(Ar, Ai, ld, k0, nb, 0, x);
     count_launch();
     if (k0 > 0) {
       k_trsv_gemv<<<(k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
@@ -885,12 +1088,24 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   SIE_CUDA(cudaSetDevice(c->device));
   if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
   for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32,
-                  (void*)c->d_perm32, (void*)c->d_tmp32})
+                  (void*)c->d_perm32, (void*)c->d_tmp32, (void*)c->d_lu_at, (void*)c->d_lu_bt, c->d_lu_scr})
     if (p) cudaFree(p);
   c->d_lu = nullptr;
   c->d_piv = nullptr;
   c->d_lu32 = c->d_lu32i = nullptr;
   c->d_piv32 = c->d_perm32 = nullptr;
   c->d_tmp32 = nullptr;
+  c->d_lu_at = c->d_lu_bt = nullptr;
+  c->d_lu_scr = nullptr;
+  c->lu_scr_bytes = 0;
+  c->lu64_valid = c->lu32_valid = false;
+  return SIE_OK;
+}
+
+extern "C" int sie_invalidate_factors(sie_ctx* c) {
+  if (!c) return fail(SIE_ERR_ARG, "sie_invalidate_factors: null context");
+  SIE_CUDA(cudaSetDevice(c->device));
+  if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
+  c->lu64_valid = c->lu32_valid = false;
   return SIE_OK;
 }

