@@ -63,10 +63,31 @@ def config_of(name, T=None, M=None):
         "workload": (f"{name}: rough slab {w['length_wl']} lambda (seed=rank), lambda=632.8nm, "
                      f"eps=-11.7-1.26i (exp(+iwt)), ICTF, ng=3"
                      + (f", {T} triangles, {M} RWG edges" if T else "")),
-        "solver": ("direct: dense FP64 fill, complex64 LU with partial pivoting (trailing updates on the "
-                   f"tensor cores, 3xTF32) and FP64 iterative refinement to {DIRECT['tolerance']}"),
-        "l2": "inputs > L2 (the dense matrix is tens of GB)",
+        "l2": "inputs > L2 (the dense matrix is tens of GB; the MLFMM tables are GBs)",
     }
+
+
+SOLVER_OURS = ("direct: dense FP64 fill, complex64 LU with partial pivoting (trailing updates on the tensor "
+               "cores, split-FP16 with a 3xTF32 fallback) and FP64 iterative refinement to "
+               f"{DIRECT['tolerance']}")
+
+
+def mesh_edges(T):
+    from specklesim_b200 import mesh
+    return mesh.edge_count(T)
+
+
+def host_cpu():
+    """nproc and the CPU model of this host."""
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
 
 
 def peaks():
@@ -335,6 +356,59 @@ def mlfmm_matvec(V, T, local, stream, b, peak, peak_kind):
                                  "achieved_gbs": mvl["total"] / (tml["mv_total_ms"] * 1e-3) / 1e9}}
 
 
+def c3_record(local, stream, peak, s_opt=250):
+    """The 30 lambda x 30 lambda slab of the C2 recipe with seed 1 at its stated size (the
+    precision configuration's mesh).  On this metal no iterative solve converges (as on
+    slab10) and the dense matrix would take N^2 x 16 B, terabytes, so the record is what
+    the library does at this size: the set-up, the K = 19 product against HBM, and budgeted
+    FP64 GMRES steps (n > 65,536: the Arnoldi step leaves the single-cluster kernel)."""
+    import ctypes as C
+    import torch
+    from specklesim_b200 import Sie, _lib, incidence, mesh
+    lib = _lib.load()
+    t0 = time.perf_counter()
+    V, T = mesh.slab_config(30.0, WL, 0.5, 1.0, 1, thickness_wl=1.0)
+    mesh_s = time.perf_counter() - t0
+    free0 = torch.cuda.mem_get_info(local)[0]
+    t0 = time.perf_counter()
+    g = Sie(V, T, WL, EPS, tree_s_opt=s_opt, truncation_number=19, device=local).setup()
+    setup_s = time.perf_counter() - t0
+    used_gb = (free0 - torch.cuda.mem_get_info(local)[0]) / 1e9
+    _lib.check(lib.sie_set_stream(g._h, C.c_void_p(stream.cuda_stream)))
+    k, E = incidence(0.0, 0.0, "TM", 2)
+    b_host = g.rhs_planewave(k, E)
+    with torch.cuda.stream(stream):
+        bd = torch.from_numpy(b_host.view(np.float64)).to(f"cuda:{local}")
+        yd = torch.empty_like(bd)
+    for _ in range(3):
+        _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(bd.data_ptr()), C.c_void_p(yd.data_ptr()), 1, 0,
+                                         C.c_void_p(stream.cuda_stream)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(stream)
+    for _ in range(reps):
+        _lib.check(lib.sie_matvec_device(g._h, C.c_void_p(bd.data_ptr()), C.c_void_p(yd.data_ptr()), 1, 0,
+                                         C.c_void_p(stream.cuda_stream)))
+    e1.record(stream)
+    e1.synchronize()
+    mv_ms = e0.elapsed_time(e1) / reps
+    mvb = matvec_algorithmic(g, None)
+    ach = mvb["total"] / (mv_ms * 1e-3) / 1e9
+    t0 = time.perf_counter()
+    x, st = g.solve(b_host, restart=30, max_iterations=30, tolerance=1e-12, raise_on_noconv=False)
+    gm_s = time.perf_counter() - t0
+    out = {"workload": "slab30: rough slab 30 lambda, seed 1, RMS 0.5 lambda, corr 1 lambda, 1 lambda thick, "
+                       "metal, ICTF, s_opt 250, K = 19",
+           "triangles": int(T.shape[0]), "edges": g.n_edges, "unknowns": g.n,
+           "levels_boxes_i4_pairs": mvb["levels"], "mesh_s": mesh_s, "setup_s": setup_s,
+           "device_gb": used_gb, "near_blocks": g.near_nnz,
+           "matvec_ms": mv_ms, "matvec_bytes": mvb["total"], "matvec_gbs": ach, "matvec_frac_hbm": ach / peak,
+           "gmres30": {"iterations": st["iterations"], "backward_error": st["backward_error_true"], "seconds": gm_s,
+                       "ms_per_iteration": 1e3 * gm_s / max(st["iterations"], 1)}}
+    g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +418,7 @@ def main():
     ap.add_argument("--workload", default="slab10", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-matvec", action="store_true")
+    ap.add_argument("--no-c3", action="store_true", help="skip the 30 lambda record")
     ap.add_argument("--fp64-repeats", type=int, default=3)
     ap.add_argument("--reference-iterations-per-step", type=int, default=2)
     args = ap.parse_args()
@@ -364,10 +439,11 @@ def main():
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * cb["step_s"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_of(args.workload),
+            "config": config_of(args.workload, T.shape[0], mesh_edges(T)),
+            "solver": "the reference's: MLFMM (K = 19 on every level) + zgmres, restart = max_iterations = 650",
             "step": (f"{args.reference_iterations_per_step} GMRES steps of the reference's MLFMM solver (+ the final "
                      f"residual); value = 1 / ({REFERENCE_ITERATIONS + 1} products)"),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "cpu_baseline": {**{k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}, "host": host_cpu()},
             "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line))
@@ -496,36 +572,44 @@ def main():
     d.close()
     torch.cuda.empty_cache()
 
-    # ---- roofline of the dominant kernel: the tensor-core trailing update of the LU.  The
-    # 3xTF32 scheme runs 3 tf32 products per real product, 4 real products per complex one:
-    # 3 x 8 = 24 tensor flops per complex multiply-add; the TF32 dense peak is half the
-    # measured BF16 one
+    # ---- roofline of the dominant kernel: the tensor-core trailing update of the LU.  Both
+    # splits run 3 tensor products per real product, 4 real products per complex one: 3 x 8 =
+    # 24 tensor flops per complex multiply-add.  Split-FP16 (kind::f16) runs at the dense
+    # f16/bf16 peak; 3xTF32 (kind::tf32) at half of it
+    f16 = bool(tmd["lu_f16"])
     try:
         pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        tf32_peak, tf32_src = float(pk["bf16_tflops"]) / 2, "measured (MEASURED_PEAKS.json bf16_tflops / 2)"
+        bf = float(pk["bf16_tflops"])
+        peak_t, peak_src = (bf, "measured (MEASURED_PEAKS.json bf16_tflops, the dense f16 rate)") if f16 else \
+            (bf / 2, "measured (MEASURED_PEAKS.json bf16_tflops / 2, the dense tf32 rate)")
     except Exception:
-        tf32_peak, tf32_src = 1590.0 / 2, "fallback (1.59 PFLOP/s bf16 / 2)"
+        peak_t, peak_src = (1590.0, "fallback (1.59 PFLOP/s)") if f16 else (795.0, "fallback (1.59 PFLOP/s / 2)")
     g_ms = tmd["lu_gemm_ms"]
     useful = tmd["lu_gemm_flops"]
     tensor_tf = 3 * useful / (g_ms * 1e-3) / 1e12 if g_ms > 0 else None
-    roof = {"kernel": "tc::k_gemm, the LU's trailing update A22 -= L21 U12 (tcgen05.mma kind::tf32, 3xTF32)",
-            "bound": "tensor", "achieved": tensor_tf, "peak": tf32_peak, "unit": "TFLOP/s",
-            "frac": tensor_tf / tf32_peak if tensor_tf else None, "peak_source": tf32_src, "traffic": None,
+    roof = {"kernel": ("tc::k_gemm, the LU's trailing update A22 -= L21 U12 " +
+                       ("(tcgen05.mma kind::f16, split-FP16 with power-of-two operand scaling)" if f16 else
+                        "(tcgen05.mma kind::tf32, 3xTF32)")),
+            "bound": "tensor", "achieved": tensor_tf, "peak": peak_t, "unit": "TFLOP/s",
+            "frac": tensor_tf / peak_t if tensor_tf else None, "peak_source": peak_src, "traffic": None,
             "launches_per_step": tmd["lu_gemm_launches"], "ms_per_step": g_ms,
             "useful_complex_tflops": useful / (g_ms * 1e-3) / 1e12 if g_ms > 0 else None,
-            "lu_factor_ms": tmd["lu_factor_ms"]}
+            "lu_factor_ms": tmd["lu_factor_ms"], "factorizations_last_step": tmd["lu_factorizations"]}
 
     # ---- the MLFMM product against HBM (rank 0, N = 1)
     rmv = None
     if rank == 0 and world == 1 and not args.no_matvec:
         rmv = mlfmm_matvec(V, T, local, stream, b, peak_hbm, peak_kind)
+    c3 = None
+    if rank == 0 and world == 1 and not args.no_c3:
+        c3 = c3_record(local, stream, peak_hbm)
 
     # ---- CPU baseline: the reference's algorithm on the host cores (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cb = cpu_reference(V, T, threads, 2, 2, 1)
-        cpu = {k_: cb[k_] for k_ in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {**{k_: cb[k_] for k_ in ("value", "unit", "cores", "kind", "sample")}, "host": host_cpu()}
 
     if rank == 0:
         line = {
@@ -533,11 +617,13 @@ def main():
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64+f64", "data": "synthetic",
             "config": config_of(args.workload, T.shape[0], N // 2),
+            "solver": SOLVER_OURS,
             "details": {"unknowns": N, "fill_s": fill_s, "mixed_vs_fp64": fp64,
                         "step": "one direct solve of one plane wave: LU of the dense matrix (refactorised every "
                                 "step into memory kept from the first) and FP64 refinement"},
             "roofline": roof,
             "roofline_matvec": rmv,
+            "slab30": c3,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": N * 16, "d2h_bytes_per_step": N * 16,
                     "steps": ke, "clocks": clk_e2e.summary()},

@@ -279,7 +279,9 @@ int sie_num_directions(const sie_ctx* ctx, int* Q);
  * tensor-core trailing updates (CUDA events on the launching stream, summed), out[15]
  * their complex flops (8 per complex multiply-add), out[16] their launches; out[17..20]
  * with SIE_LU_PHASES=1 in the environment, the device time of the LU's panels, row swaps,
- * L11 solves and operand tiling. */
+ * L11 solves and operand tiling; out[21] = 1 if the last factorisation's trailing updates
+ * ran in split-FP16, 0 for 3xTF32; out[22] = factorisations in the last mixed direct solve
+ * (2 when the split-FP16 factors stalled the refinement and it factorised again). */
 int sie_get_timings(const sie_ctx* ctx, double* out, int n);
 
 /* Launch all further work of ctx on the caller's CUDA stream (NULL: back to the

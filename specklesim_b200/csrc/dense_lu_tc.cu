@@ -31,9 +31,9 @@
 namespace sie {
 namespace tc {
 int tile_operand(const float* sr, const float* si, size_t ld, int rows, int K, bool trans, char* out,
-                 cudaStream_t st);
+                 cudaStream_t st, bool f16, unsigned* amax);
 int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, size_t ldc, int m, int n,
-                int* d_err, cudaStream_t st, int max_ctas = 0);
+                int* d_err, cudaStream_t st, int max_ctas, bool f16, const unsigned* amax);
 size_t tiled_bytes_host(int rows, int K);
 }  // namespace tc
 
@@ -95,7 +95,9 @@ static const size_t PANEL_CNT_OFF = PANEL_SLOTS_OFF + 2 * PANEL_MAX_BLOCKS * siz
 static size_t panel_cnt_bytes(int n) { return ((size_t)n / LU_SB + 2) * sizeof(unsigned); }
 // then the swap plan of the latest panel: {count, src[2 LU_NB], dst[2 LU_NB]}
 static size_t panel_plan_off(int n) { return (PANEL_CNT_OFF + panel_cnt_bytes(n) + 255) / 256 * 256; }
-static size_t panel_scratch_bytes(int n) { return panel_plan_off(n) + (1 + 4 * LU_NB) * sizeof(int); }
+// and the two operand maxima of the split-FP16 updates
+static size_t panel_amax_off(int n) { return (panel_plan_off(n) + (1 + 4 * LU_NB) * sizeof(int) + 15) / 16 * 16; }
+static size_t panel_scratch_bytes(int n) { return panel_amax_off(n) + 2 * sizeof(unsigned); }
 
 // Grid barrier of the cooperative sub-panel kernel (all its blocks are resident) on a
 // counter that only grows within one launch: the m-th barrier waits for m * gridDim.x
@@ -559,57 +561,120 @@ __global__ void __launch_bounds__(512) k_trsm_l(float* Ar, float* Ai, size_t ld,
   }
 }
 
-// Solves with the factors, one vector (complex64, internal order) in place.  Diagonal
-// block: x[k0 .. k0 + nb) = L11^-1 x (lower, unit diagonal) or U11^-1 x (upper), with the
-// block staged in shared memory first; thread r < nb owns x_r, one barrier per step.
-__global__ void __launch_bounds__(LU_TB) k_trsv_block(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
-                                                      int lower, cc* x) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
-  float* Di = Dr + LU_TB * LU_TB;
-  __shared__ float br[LU_TB], bi[LU_TB], yr[LU_TB], yi[LU_TB];
-  stage_block(Ar, Ai, ld, k0, nb, Dr, Di);
-  const int r = threadIdx.x;
-  if (r < nb) {
-    br[r] = x[k0 + r].re;
-    bi[r] = x[k0 + r].im;
-  }
-  __syncthreads();
-  if (lower) {
-    // step i: x_i is final; every row below it loses L_ri x_i
-    for (int i = 0; i < nb; i++) {
-      const float vr = br[i], vi = bi[i];
-      if (r > i && r < nb) {
-        const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
-        br[r] -= lr * vr - li * vi;
-        bi[r] -= lr * vi + li * vr;
-      }
-      __syncthreads();
+// The diagonal blocks of the factors, copied once after the factorisation into one
+// contiguous 128 KB slab each ([plane][col][row], LU_TB x LU_TB, zero past a ragged last
+// block), so that a triangular solve stages a block with one bulk copy.
+__global__ void __launch_bounds__(256) k_copy_diag(const float* Ar, const float* Ai, size_t ld, int n,
+                                                   float* out) {
+  const int k0 = blockIdx.x * LU_TB, nb = min(LU_TB, n - k0);
+  float* o = out + (size_t)blockIdx.x * 2 * LU_TB * LU_TB;
+  for (int e0 = threadIdx.x; e0 < LU_TB * LU_TB; e0 += 8 * blockDim.x) {
+    float vr[8], vi[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * blockDim.x, col = e / LU_TB, row = e - col * LU_TB;
+      const bool in = col < nb && row < nb;
+      vr[q] = in ? Ar[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
+      vi[q] = in ? Ai[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
     }
-    if (r < nb) x[k0 + r] = mk<float>(br[r], bi[r]);
-  } else {
-    // step i (downward): y_i = x_i / U_ii (every thread forms it; thread i keeps it), and
-    // every row above loses U_ri y_i
-    for (int i = nb - 1; i >= 0; i--) {
-      const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
-      const float den = ur * ur + ui * ui;
-      const float vr = (br[i] * ur + bi[i] * ui) / den, vi = (bi[i] * ur - br[i] * ui) / den;
-      if (r == i) {
-        yr[i] = vr;
-        yi[i] = vi;
-      } else if (r < i) {
-        const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
-        br[r] -= lr * vr - li * vi;
-        bi[r] -= lr * vi + li * vr;
-      }
-      __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * blockDim.x;
+      o[e] = vr[q];
+      o[LU_TB * LU_TB + e] = vi[q];
     }
-    if (r < nb) x[k0 + r] = mk<float>(yr[r], yi[r]);
   }
 }
 
-// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb); thread per row, 16
-// columns' loads in flight at a time.
+// Solves with the factors, one vector (complex64, internal order) in place.  Diagonal
+// block: x[k0 .. k0 + nb) = L11^-1 x (lower, unit diagonal) or U11^-1 x (upper).  The block
+// arrives by one bulk copy on an mbarrier (bounded wait: on give-up the kernel records
+// bit 32 in *err, waits once more, bounded, for the copy, and leaves x alone); one warp
+// then runs the substitution with lane l holding rows l, l + 32, l + 64, l + 96.
+__global__ void __launch_bounds__(32) k_trsv_diag(const float* diag, int k0, int nb, int lower, cc* x, int* err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t bar;
+  float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
+  float* Di = Dr + LU_TB * LU_TB;
+  const int lane = threadIdx.x;
+  const unsigned bytes = 2u * LU_TB * LU_TB * sizeof(float);
+  if (lane == 0) {
+    tc::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (lane == 0) {
+    tc::mbar_expect_tx(&bar, bytes);
+    tc::bulk_g2s(Dr, diag, bytes, &bar);
+  }
+  float xr[4], xi[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = lane + 32 * q;
+    xr[q] = r < nb ? x[k0 + r].re : 0.f;
+    xi[q] = r < nb ? x[k0 + r].im : 0.f;
+  }
+  if (!tc::mbar_wait(&bar, 0)) {
+    if (lane == 0) atomicOr(err, 32);
+    tc::mbar_wait(&bar, 0);
+    return;
+  }
+  if (lower) {
+    for (int i = 0; i < nb; i++) {
+      const int q0 = i >> 5;
+      float vr = 0.f, vi = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (q == q0) {
+          vr = __shfl_sync(0xffffffffu, xr[q], i & 31);
+          vi = __shfl_sync(0xffffffffu, xi[q], i & 31);
+        }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = lane + 32 * q;
+        if (r > i) {
+          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+          xr[q] -= lr * vr - li * vi;
+          xi[q] -= lr * vi + li * vr;
+        }
+      }
+    }
+  } else {
+    for (int i = nb - 1; i >= 0; i--) {
+      const int q0 = i >> 5;
+      float br = 0.f, bi = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (q == q0) {
+          br = __shfl_sync(0xffffffffu, xr[q], i & 31);
+          bi = __shfl_sync(0xffffffffu, xi[q], i & 31);
+        }
+      const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
+      const float den = ur * ur + ui * ui;
+      const float vr = (br * ur + bi * ui) / den, vi = (bi * ur - br * ui) / den;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = lane + 32 * q;
+        if (r == i) {
+          xr[q] = vr;
+          xi[q] = vi;
+        } else if (r < i) {
+          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+          xr[q] -= lr * vr - li * vi;
+          xi[q] -= lr * vi + li * vr;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = lane + 32 * q;
+    if (r < nb) x[k0 + r] = mk<float>(xr[q], xi[q]);
+  }
+}
+
+// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb): four threads per row,
+// each a quarter of the columns with its 16 loads in flight, summed by shuffles.
 __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
                                                    int r0, int r1, cc* x) {
   __shared__ float br[LU_TB], bi[LU_TB];
@@ -618,25 +683,36 @@ __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float*
     bi[r] = r < nb ? x[k0 + r].im : 0.f;
   }
   __syncthreads();
-  const int i = r0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r1) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = r0 + (t >> 2), part = t & 3;
+  const bool live = i < r1;
   float sr = 0.f, si = 0.f;
-  for (int j0 = 0; j0 < nb; j0 += 16) {
-    float ar[16], ai[16];
+  if (live) {
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const size_t o = (size_t)(k0 + j0 + q) * ld + i;
-      ar[q] = j0 + q < nb ? Ar[o] : 0.f;
-      ai[q] = j0 + q < nb ? Ai[o] : 0.f;
-    }
+    for (int h = 0; h < LU_TB / 4; h += 16) {
+      float ar[16], ai[16];
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      sr += ar[q] * br[j0 + q] - ai[q] * bi[j0 + q];
-      si += ar[q] * bi[j0 + q] + ai[q] * br[j0 + q];
+      for (int q = 0; q < 16; q++) {
+        const int j = part * (LU_TB / 4) + h + q;
+        ar[q] = j < nb ? Ar[(size_t)(k0 + j) * ld + i] : 0.f;
+        ai[q] = j < nb ? Ai[(size_t)(k0 + j) * ld + i] : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        const int j = part * (LU_TB / 4) + h + q;
+        sr += ar[q] * br[j] - ai[q] * bi[j];
+        si += ar[q] * bi[j] + ai[q] * br[j];
+      }
     }
   }
-  x[i].re -= sr;
-  x[i].im -= si;
+  sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+  si += __shfl_xor_sync(0xffffffffu, si, 1);
+  sr += __shfl_xor_sync(0xffffffffu, sr, 2);
+  si += __shfl_xor_sync(0xffffffffu, si, 2);
+  if (live && part == 0) {
+    x[i].re -= sr;
+    x[i].im -= si;
+  }
 }
 
 // y[i] = x[perm[i]]: the factorisation's row interchanges as one gather
@@ -692,12 +768,15 @@ static int lu_tc_factor(sie_ctx* c) {
   if (!c->d_piv32 && cudaMalloc(&c->d_piv32, (size_t)n * sizeof(int)) != cudaSuccess) c->d_piv32 = nullptr;
   if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_at = nullptr;
   if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_bt = nullptr;
+  const int ndiag = (n + LU_TB - 1) / LU_TB;
+  if (!c->d_lu_diag && cudaMalloc(&c->d_lu_diag, (size_t)ndiag * 2 * LU_TB * LU_TB * sizeof(float)) != cudaSuccess)
+    c->d_lu_diag = nullptr;
   if (!c->d_lu_scr || c->lu_scr_bytes < scr_bytes) {
     if (c->d_lu_scr) cudaFree(c->d_lu_scr);
     if (cudaMalloc(&c->d_lu_scr, scr_bytes) != cudaSuccess) c->d_lu_scr = nullptr;
     c->lu_scr_bytes = c->d_lu_scr ? scr_bytes : 0;
   }
-  if (!c->d_lu32 || !c->d_lu32i || !c->d_piv32 || !c->d_lu_at || !c->d_lu_bt || !c->d_lu_scr) {
+  if (!c->d_lu32 || !c->d_lu32i || !c->d_piv32 || !c->d_lu_at || !c->d_lu_bt || !c->d_lu_scr || !c->d_lu_diag) {
     cudaGetLastError();
     return fail(SIE_ERR_NOMEM, "mixed LU: device memory");
   }
@@ -711,6 +790,7 @@ static int lu_tc_factor(sie_ctx* c) {
   unsigned* pcnt = (unsigned*)((char*)c->d_lu_scr + PANEL_CNT_OFF);  // one counter per sub-panel launch
   unsigned* pbad = pcnt + (n / LU_SB + 1);
   int* plan = (int*)((char*)c->d_lu_scr + panel_plan_off(n));
+  unsigned* amax = (unsigned*)((char*)c->d_lu_scr + panel_amax_off(n));
   int rc = SIE_OK;
   auto t0 = std::chrono::steady_clock::now();
   cudaMemsetAsync(c->d_lu_scr, 0, scr_bytes, s);
@@ -777,6 +857,12 @@ static int lu_tc_factor(sie_ctx* c) {
   // SIE_LU_LOOKAHEAD=0 runs the whole trailing update on the panel stream (same work)
   const char* la = getenv("SIE_LU_LOOKAHEAD");
   const bool lookahead = !(la && atoi(la) == 0);
+  // trailing updates in split-FP16 unless this context's refinement needed 3xTF32 before
+  // (or SIE_LU_GEMM=tf32 asks for it)
+  const char* gp = getenv("SIE_LU_GEMM");
+  const bool gh = c->lu_f16_ok && !(gp && std::string(gp) == "tf32");
+  c->tm.lu_f16 = gh ? 1 : 0;
+  c->tm.lu_factorizations += 1;
   // the cooperative panel kernel: blocks that fit on the multiprocessors the look-ahead
   // update leaves free, or on all of them without look-ahead (all resident at once)
   int per_sm = 0;
@@ -836,20 +922,24 @@ static int lu_tc_factor(sie_ctx* c) {
         count_launch();
         if (d1 < k1) {
           const int mb = k1 - d1;
-          rc = tc::tile_operand(Ar + (size_t)d0 * ld + d1, Ai + (size_t)d0 * ld + d1, ld, mb, db, false, At, sp);
+          rc = tc::tile_operand(Ar + (size_t)d0 * ld + d1, Ai + (size_t)d0 * ld + d1, ld, mb, db, false, At, sp, gh,
+                                amax);
           if (rc == SIE_OK)
-            rc = tc::tile_operand(Ar + (size_t)k1 * ld + d0, Ai + (size_t)k1 * ld + d0, ld, n - k1, db, true, Bt, sp);
+            rc = tc::tile_operand(Ar + (size_t)k1 * ld + d0, Ai + (size_t)k1 * ld + d0, ld, n - k1, db, true, Bt, sp,
+                                  gh, amax + 1);
           if (rc == SIE_OK)
             rc = tc::gemm_update(At, Bt, db, Ar + (size_t)k1 * ld + d1, Ai + (size_t)k1 * ld + d1, ld, mb, n - k1,
-                                 err, sp);
+                                 err, sp, 0, gh, amax);
         }
       }
       mark(2, false, pk);
       const int m = n - k1, nn = std::min(LU_NB, m);
       // A22 -= L21 U12 on the tensor cores
       mark(3, true, pk);
-      rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, sp);
-      if (rc == SIE_OK) rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, sp);
+      rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, sp, gh, amax);
+      if (rc == SIE_OK)
+        rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, m, nb, true, Bt, sp, gh,
+                              amax + 1);
       mark(3, false, pk);
       cudaEventRecord(ev_tiled, sp);
       const cudaStream_t srest = lookahead ? sg : sp;
@@ -859,9 +949,10 @@ static int lu_tc_factor(sie_ctx* c) {
         cudaEvent_t e0 = new_event(), e1 = new_event();
         if (e0) cudaEventRecord(e0, srest);
         // the B tiles past the next panel's nn columns
-        const size_t boff = (size_t)(nn / tc::TILE) * ((nb + tc::KC - 1) / tc::KC) * tc::BLOCK_BYTES;
+        const int kc = gh ? tc::KC_F16 : tc::KC;
+        const size_t boff = (size_t)(nn / tc::TILE) * ((nb + kc - 1) / kc) * tc::BLOCK_BYTES;
         rc = tc::gemm_update(At, Bt + boff, nb, Ar + (size_t)(k1 + nn) * ld + k1, Ai + (size_t)(k1 + nn) * ld + k1,
-                             ld, m, m - nn, err, srest, lookahead ? rest_ctas : 0);
+                             ld, m, m - nn, err, srest, lookahead ? rest_ctas : 0, gh, amax);
         if (e1) cudaEventRecord(e1, srest);
         if (e0 && e1) gemm_ev.push_back({e0, e1});
         cudaEventRecord(ev_rest, srest);
@@ -872,7 +963,8 @@ static int lu_tc_factor(sie_ctx* c) {
       cudaEvent_t e0 = new_event(), e1 = new_event();
       if (e0) cudaEventRecord(e0, sp);
       if (rc == SIE_OK)
-        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k1, Ai + (size_t)k1 * ld + k1, ld, m, nn, err, sp);
+        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k1, Ai + (size_t)k1 * ld + k1, ld, m, nn, err, sp, 0,
+                             gh, amax);
       if (e1) cudaEventRecord(e1, sp);
       if (e0 && e1) gemm_ev.push_back({e0, e1});
       gemm_flops += 8.0 * m * (double)nn * nb;
@@ -885,6 +977,10 @@ static int lu_tc_factor(sie_ctx* c) {
     cudaEventRecord(ev_sg, sg);
     cudaStreamWaitEvent(s, ev_sp, 0);
     cudaStreamWaitEvent(s, ev_sg, 0);
+  }
+  if (rc == SIE_OK) {
+    k_copy_diag<<<ndiag, 256, 0, s>>>(Ar, Ai, ld, n, c->d_lu_diag);
+    count_launch();
   }
   int herr = 0;
   if (rc == SIE_OK && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -937,26 +1033,28 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   const int n = 2 * c->M;
   const size_t ld = (size_t)n;
   const float *Ar = c->d_lu32, *Ai = c->d_lu32i;
+  int* err = (int*)c->d_lu_scr;
   k_permute<<<148, 256, 0, s>>>(c->d_perm32, n, x, c->d_tmp32);
   count_launch();
   SIE_CUDA(cudaMemcpyAsync(x, c->d_tmp32, (size_t)n * sizeof(cc), cudaMemcpyDeviceToDevice, s));
   const size_t dsm = (size_t)2 * LU_TB * LU_TB * sizeof(float);
-  SIE_CUDA(raise_smem(k_trsv_block, dsm));
+  SIE_CUDA(raise_smem(k_trsv_diag, dsm));
+  const size_t blk = (size_t)2 * LU_TB * LU_TB;
   for (int k0 = 0; k0 < n; k0 += LU_TB) {
     const int nb = std::min(LU_TB, n - k0), k1 = k0 + nb;
-    k_trsv_block<<<1, LU_TB, dsm, s>>>(Ar, Ai, ld, k0, nb, 1, x);
+    k_trsv_diag<<<1, 32, dsm, s>>>(c->d_lu_diag + (size_t)(k0 / LU_TB) * blk, k0, nb, 1, x, err);
     count_launch();
     if (k1 < n) {
-      k_trsv_gemv<<<(n - k1 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
+      k_trsv_gemv<<<(4 * (n - k1) + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
       count_launch();
     }
   }
   for (int k0 = ((n - 1) / LU_TB) * LU_TB; k0 >= 0; k0 -= LU_TB) {
     const int nb = std::min(LU_TB, n - k0);
-    k_trsv_block<<<1, LU_TB, dsm, s>>>(Ar, Ai, ld, k0, nb, 0, x);
+    k_trsv_diag<<<1, 32, dsm, s>>>(c->d_lu_diag + (size_t)(k0 / LU_TB) * blk, k0, nb, 0, x, err);
     count_launch();
     if (k0 > 0) {
-      k_trsv_gemv<<<(k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
+      k_trsv_gemv<<<(4 * k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
       count_launch();
     }
   }
@@ -968,6 +1066,7 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
 static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, double tolerance,
                                   int max_refinements, sie_stats* stats, cudaStream_t s) {
   auto t0 = std::chrono::steady_clock::now();
+  c->tm.lu_factorizations = 0;
   SIE_TRY(lu_tc_factor(c));
   const int n = 2 * c->M;
   const size_t bytes = (size_t)n * sizeof(zc);
@@ -982,8 +1081,10 @@ static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, 
   for (int k = 0; k < nrhs && rc == SIE_OK; k++) {
     auto tk = std::chrono::steady_clock::now();
     const size_t off = (size_t)k * n;
-    double bn2 = 0, rn2 = 0;
+    double bn2 = 0, rn2 = 0, prev2 = 0;
     int steps = 0;
+    bool stalled = false;  // split-FP16 factors that do not contract the residual
+    const bool h_factors = c->tm.lu_f16 != 0;
     rc = gather_ext_to_int(c, d_b + off, bi, 1, s);
     cudaMemsetAsync(xi, 0, bytes, s);
     // r = b - Z x in FP64 (x = 0 at the start), then d = LU^-1 r in complex64 (r scaled to
@@ -998,17 +1099,31 @@ static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, 
       cudaMemsetAsync(nrm, 0, sizeof(double), s);
       k_resid<<<296, 256, 0, s>>>(bi, ax, r, n, nrm);
       count_launch();
+      int herr = 0;
       if (cudaMemcpyAsync(&rn2, nrm, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+          cudaMemcpyAsync(&herr, c->d_lu_scr, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaStreamSynchronize(s) != cudaSuccess) {
         rc = fail(SIE_ERR_CUDA, "mixed direct solve: residual");
         break;
       }
+      if (herr & 32) {
+        rc = fail(SIE_ERR_CUDA, "mixed direct solve: a triangular solve's block copy timed out");
+        break;
+      }
       if (steps == 0) bn2 = rn2;
+      const bool done = std::isfinite(rn2) && (bn2 == 0.0 || rn2 <= tolerance * tolerance * bn2);
+      // each correction must at least halve the residual (the factors' error times cond(Z)
+      // well below one); split-FP16 factors that do not are replaced by 3xTF32 ones
+      if (h_factors && !done && steps >= 2 && (!std::isfinite(rn2) || rn2 > 0.25 * prev2)) {
+        stalled = true;
+        break;
+      }
+      prev2 = rn2;
       if (!std::isfinite(rn2)) {
         rc = fail(SIE_ERR_NONFINITE, "mixed direct solve: non-finite residual");
         break;
       }
-      if (bn2 == 0.0 || rn2 <= tolerance * tolerance * bn2 || steps > max_refinements) break;
+      if (done || steps > max_refinements) break;
       const double rn = std::sqrt(rn2);
       k_scale_to32<<<296, 256, 0, s>>>(r, d32, n, 1.0 / rn);
       count_launch();
@@ -1018,6 +1133,14 @@ static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, 
       count_launch();
     }
     if (rc != SIE_OK) break;
+    if (stalled) {  // factorise again with 3xTF32 updates and redo this right-hand side
+      c->lu_f16_ok = false;
+      c->lu32_valid = false;
+      rc = lu_tc_factor(c);
+      if (rc != SIE_OK) break;
+      k--;
+      continue;
+    }
     rc = scatter_int_to_ext(c, xi, d_x + off, 1, s);
     if (rc == SIE_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed direct solve");
     const double be = bn2 > 0 ? std::sqrt(rn2 / bn2) : 0.0;
@@ -1088,7 +1211,8 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   SIE_CUDA(cudaSetDevice(c->device));
   if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
   for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32,
-                  (void*)c->d_perm32, (void*)c->d_tmp32, (void*)c->d_lu_at, (void*)c->d_lu_bt, c->d_lu_scr})
+                  (void*)c->d_perm32, (void*)c->d_tmp32, (void*)c->d_lu_at, (void*)c->d_lu_bt, c->d_lu_scr,
+                  (void*)c->d_lu_diag})
     if (p) cudaFree(p);
   c->d_lu = nullptr;
   c->d_piv = nullptr;
@@ -1097,6 +1221,7 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   c->d_tmp32 = nullptr;
   c->d_lu_at = c->d_lu_bt = nullptr;
   c->d_lu_scr = nullptr;
+  c->d_lu_diag = nullptr;
   c->lu_scr_bytes = 0;
   c->lu64_valid = c->lu32_valid = false;
   return SIE_OK;

@@ -1637,14 +1637,15 @@ int sie_get_rt(sie_ctx* c, const int* edges, int cnt, double* out) {
 
 int sie_get_timings(const sie_ctx* c, double* out, int n) {
   if (!c || !out) return fail(SIE_ERR_ARG, "sie_get_timings: null argument");
-  double v[21] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
+  double v[23] = {c->tm.fill_ms, c->tm.rt_ms, c->tm.setup_ms, c->tm.mv_total_ms,
                   c->tm.mv_near_ms, c->tm.mv_agg_ms, c->tm.mv_ss_ms, c->tm.mv_sr_ms,
                   c->tm.mv_rr_ms, c->tm.mv_recv_ms,
                   c->tm.gm_steps > 0 ? c->tm.gm_passes / c->tm.gm_steps : 0.0, c->tm.graph_replays,
                   c->tm.precond_ms, c->tm.lu_factor_ms, c->tm.lu_gemm_ms, c->tm.lu_gemm_flops,
                   (double)c->tm.lu_gemm_launches, c->tm.lu_phase_ms[0], c->tm.lu_phase_ms[1],
-                  c->tm.lu_phase_ms[2], c->tm.lu_phase_ms[3]};
-  for (int i = 0; i < n && i < 21; i++) out[i] = v[i];
+                  c->tm.lu_phase_ms[2], c->tm.lu_phase_ms[3], (double)c->tm.lu_f16,
+                  (double)c->tm.lu_factorizations};
+  for (int i = 0; i < n && i < 23; i++) out[i] = v[i];
   return SIE_OK;
 }
 
@@ -1659,7 +1660,8 @@ int sie_free(sie_ctx* c) {
                   c->d_tth, c->d_tph, c->d_trf, c->d_rt, c->d_rt32, c->d_trf32, c->d_xi32, c->d_yi32, c->d_xi, c->d_yi, c->d_gm, c->d_gm32, c->d_gmz, c->d_lu, c->d_piv, c->d_io,
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
                   c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT, c->d_lu32, c->d_lu32i, c->d_piv32,
-                  c->d_perm32, c->d_tmp32, c->d_lu_at, c->d_lu_bt, c->d_lu_scr};
+                  c->d_perm32, c->d_tmp32, c->d_lu_at, c->d_lu_bt, c->d_lu_scr,
+                  c->d_lu_diag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->d_lvtmp) cudaFree(c->d_lvtmp);

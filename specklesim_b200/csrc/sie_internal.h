@@ -174,6 +174,8 @@ struct Timings {
   double lu_gemm_flops = 0;            // complex flops of those updates (8 per multiply-add)
   int lu_gemm_launches = 0;
   double lu_phase_ms[4] = {0, 0, 0, 0};  // panel, row swaps, L11 solve, operand tiling (SIE_LU_PHASES=1)
+  int lu_f16 = 0;                      // the last factorisation's trailing updates: 1 split-FP16, 0 3xTF32
+  int lu_factorizations = 0;           // factorisations of the last mixed direct solve
 };
 
 }  // namespace sie
@@ -319,11 +321,15 @@ struct sie_ctx {
   char* d_lu_at = nullptr;        // mixed LU workspace: the pre-tiled A and B operands of the
   char* d_lu_bt = nullptr;        // trailing updates,
   void* d_lu_scr = nullptr;       // the panel kernel's slots, barrier counters and error word
+  float* d_lu_diag = nullptr;     // the factors' diagonal blocks, contiguous, for the solves
   size_t lu_scr_bytes = 0;
   // the factors above are current (sie_invalidate_factors clears these and keeps the memory,
   // sie_release_factors frees it)
   bool lu64_valid = false;
   bool lu32_valid = false;
+  // the mixed LU's trailing updates may run in split-FP16: cleared when the refinement on
+  // such factors stalls, after which this context factorises with 3xTF32
+  bool lu_f16_ok = true;
   void* h_gm = nullptr;           // pinned host slots for the solver's scalars
   void* h_gmb = nullptr;          // pinned host copy of the batched solver's per-system state
   int ar_blocks = 0;              // co-resident grid of the fused Arnoldi kernel

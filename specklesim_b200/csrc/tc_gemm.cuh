@@ -1,12 +1,18 @@
 // Complex GEMM update on the 5th-generation tensor cores (tcgen05, sm_100a):
 //
-//     C -= A B        A: m x K, B: K x n, C: m x n, complex, FP32-accurate
+//     C -= A B        A: m x K, B: K x n, C: m x n, complex
 //
 // C is complex64 stored as two real planes (Cr, Ci), column-major.  The operands are
-// split into tf32 pairs (x = hi + lo, hi rounded to tf32, lo the exact remainder) and
-// every complex product is formed from the three products hi*hi + hi*lo + lo*hi of each
-// real product ("3xTF32"): Cr -= Ar Br - Ai Bi, Ci -= Ar Bi + Ai Br, accumulated in FP32 in
-// tensor memory.  The error of one product is ~2^-21 relative, FP32-level.
+// split into pairs x = hi + lo and every complex product is formed from the three products
+// hi*hi + hi*lo + lo*hi of each real product: Cr -= Ar Br - Ai Bi, Ci -= Ar Bi + Ai Br,
+// accumulated in FP32 in tensor memory.  Two splits:
+//   3xTF32 (kind::tf32): hi rounded to tf32, lo the exact remainder; ~2^-21 relative,
+//     FP32-level; 8 K per MMA.
+//   split-FP16 (kind::f16, both operands f16): each operand scaled by a power of two s
+//     that puts its largest magnitude below 2^14, hi = f16(s x), lo = f16(s x - hi), the
+//     accumulator multiplied back by 1 / (s_A s_B), exact; hi and lo keep 11 bits each, so
+//     the products are as accurate as 3xTF32 relative to the operands' largest entries, and
+//     an MMA takes 16 K at the same issue rate: twice the tf32 throughput.
 //
 // Operands are pre-tiled in global memory in the shape the MMA reads from shared memory,
 // so each pipeline stage is one contiguous bulk (TMA) copy:
@@ -46,6 +52,13 @@ constexpr int GROUP_M = 16;               // row tiles swept together across the
 // byte offset of element (r, k) inside one plane of a block
 __host__ __device__ __forceinline__ int plane_offset(int r, int k) {
   return (((k >> 2) * 16 + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 3) << 2);
+}
+// the same for the f16 planes: a block covers KC_F16 = 16 K; core matrices of 8 rows x
+// 16 bytes (8 f16), so the byte layout, LBO and SBO are those of the tf32 planes
+constexpr int KC_F16 = 16;
+constexpr int F16_TOP = 14;  // scaled operands stay below 2^14 (f16 overflows at 65504)
+__host__ __device__ __forceinline__ int plane_offset_f16(int r, int k) {
+  return (((k >> 3) * 16 + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1);
 }
 
 // hi = x rounded to tf32 (low 13 mantissa bits zero), lo = x - hi exactly
@@ -106,6 +119,18 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate ? 1u : 0u));
+}
+// instruction descriptor for kind::f16: D f32, A and B f16, both K-major, M = N = 128
+__host__ __device__ constexpr uint32_t idesc_f16(bool neg_a) {
+  return (1u << 4) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         bool accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(idesc), "r"(accumulate ? 1u : 0u));
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {

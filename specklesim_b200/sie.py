@@ -286,12 +286,12 @@ class Sie:
         return out
 
     def timings(self):
-        v = np.zeros(21)
-        check(self._lib.sie_get_timings(self._h, dptr(v), 21))
+        v = np.zeros(23)
+        check(self._lib.sie_get_timings(self._h, dptr(v), 23))
         keys = ["fill_ms", "rt_tl_ms", "setup_ms", "mv_total_ms", "mv_near_ms", "mv_agg_ms",
                 "mv_ss_ms", "mv_sr_ms", "mv_rr_ms", "mv_recv_ms", "gm_passes_per_step", "graph_replays",
                 "precond_ms", "lu_factor_ms", "lu_gemm_ms", "lu_gemm_flops", "lu_gemm_launches",
-                "lu_panel_ms", "lu_swap_ms", "lu_trsm_ms", "lu_tile_ms"]
+                "lu_panel_ms", "lu_swap_ms", "lu_trsm_ms", "lu_tile_ms", "lu_f16", "lu_factorizations"]
         return dict(zip(keys, v))
 
     def close(self):

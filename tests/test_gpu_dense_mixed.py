@@ -33,6 +33,9 @@ def test_mixed_direct_solve_matches_fp64_and_oracle(oracle_lib, gpu_lib, case):
     assert st["converged"] and st["backward_error_true"] <= 1e-12
     assert 1 <= st["iterations"] <= 30
     assert _rel(xm, x64) < 1e-9
+    # these systems need no fallback: one factorisation, its updates in split-FP16
+    tt = g.timings()
+    assert tt["lu_f16"] == 1 and tt["lu_factorizations"] == 1, tt
     # the currents solve the oracle's own dense system (its blocks agree with the fill
     # kernels' to 1e-9 of the block scale; measured 1.2e-10 on the small sphere)
     o = oracle_lib.Oracle(V, T, P.WL, P.EPS_METAL, threads=8)
@@ -58,3 +61,23 @@ def test_mixed_direct_solve_refuses_mlfmm_contexts(gpu_lib):
         g.solve_direct_mixed(np.ones(g.n, complex))
     assert e.value.code == _lib.SIE_ERR_STATE
     g.close()
+
+
+def test_mixed_direct_solve_with_tf32_updates(gpu_lib, monkeypatch):
+    """SIE_LU_GEMM=tf32 runs the trailing updates as 3xTF32 products: the same solution,
+    in no more refinement steps."""
+    from specklesim_b200 import Sie, incidence
+    V, T = P.sphere(3)
+    g = Sie(V, T, P.WL, P.EPS_METAL, dense=True).setup()
+    b = g.rhs_planewave(*incidence(0.3, 0.2, "TM", 2))
+    x_bf, st_bf = g.solve_direct_mixed(b, tolerance=1e-12)
+    assert g.timings()["lu_f16"] == 1
+    monkeypatch.setenv("SIE_LU_GEMM", "tf32")
+    g.invalidate_factors()
+    x_tf, st_tf = g.solve_direct_mixed(b, tolerance=1e-12)
+    tt = g.timings()
+    assert tt["lu_f16"] == 0 and tt["lu_factorizations"] == 1
+    assert st_tf["converged"] and st_tf["iterations"] <= st_bf["iterations"]
+    assert _rel(x_tf, x_bf) < 1e-10
+    g.close()
+
