@@ -107,18 +107,20 @@ static size_t panel_scratch_bytes(int n) { return panel_amax_off(n) + 2 * sizeof
 __device__ __forceinline__ void panel_bar(unsigned* cnt, unsigned* bad, unsigned target) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(cnt, 1u);
-    volatile unsigned* vc = cnt;
+    // release: the block's writes (ordered before by the CTA barrier) are visible to any
+    // block that acquires the count
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
     volatile unsigned* vb = bad;
     long long it = 0;
-    while (*vc < target && *vb == 0) {
+    while (true) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+      if (v >= target || *vb != 0) break;
       if (++it > (1LL << 21)) {
         atomicExch(bad, 1u);
         break;
       }
     }
-    __threadfence();
   }
   __syncthreads();
 }
@@ -126,7 +128,7 @@ __device__ __forceinline__ void panel_bar(unsigned* cnt, unsigned* bad, unsigned
 // Block-wide argmax of (value, row) pairs (ties to the smaller row); returns the winner to
 // every thread, and whether the calling thread holds it (the lowest such thread).
 __device__ __forceinline__ void block_argmax(float v, int i, float* sv, int* si, int* st, float& bv, int& bi,
-                                             bool& mine) {
+                                             bool& mine, int* winner = nullptr) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   float best = v;
   int idx = i, who = threadIdx.x;
@@ -158,6 +160,7 @@ __device__ __forceinline__ void block_argmax(float v, int i, float* sv, int* si,
   bv = best;
   bi = idx;
   mine = who == (int)threadIdx.x;
+  if (winner) *winner = who;
 }
 
 // One sub-panel [s0, s1) of the panel [k0, k1) factorised by one cooperative launch, one
@@ -165,18 +168,21 @@ __device__ __forceinline__ void block_argmax(float v, int i, float* sv, int* si,
 // published its candidate for column j in slots[gen]: the largest |a|^2 among its rows and
 // that row's values in columns [j, s1).  After it, every block reduces the slots to the
 // same pivot p (the first maximum, as izamax) and takes the pivot row from the winning
-// slot, so nobody reads row p from the matrix.  Row j and row p trade places logically:
-// the thread that owns row p reads the old row j, writes the pivot row into row j and the
-// updated old row j into row p; block 0 swaps the two rows in the panel's other columns,
-// which no other block touches during the launch.  Each row r > j is then scaled and
-// updated, and the block's best candidate for column j + 1 goes to the other generation of
-// slots.  Matrix and slot reads bypass L1 (__ldcg): other blocks' writes are seen through L2.
+// slot, so nobody reads row p from the matrix.  Row j and row p trade places logically in
+// the sub-panel's columns [j, s1): the thread that owns row p reads the old row j, writes
+// the pivot row into row j and the updated old row j into row p.  The two rows' values in
+// the panel's other columns are swapped after the launch (k_sub_finish), as nothing here
+// reads them.  Each row r > j is then scaled and updated, and the block's best candidate
+// for column j + 1 goes to the other generation of slots: every thread keeps the values of
+// its best row in shared memory, so the winner's row is published without a reload.
+// Matrix and slot reads bypass L1 (__ldcg): other blocks' writes are seen through L2.
 __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_t ld, int n, int s0, int s1, int k0,
                                                      int k1, int* ipiv, int* err, PanelSlot* slots, unsigned* cnt,
                                                      unsigned* bad) {
   __shared__ float sv[8];
   __shared__ int si[8], st[8];
   __shared__ float2 urow[LU_SB];
+  __shared__ float2 cand[LU_SB - 1][256];  // each thread's best row, columns j + 1 .. s1 - 1
   __shared__ int piv_s, win_s;
   const unsigned G = gridDim.x;
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = G * blockDim.x;
@@ -238,17 +244,6 @@ __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_
       __syncthreads();
     }
     const int p = piv_s < n ? piv_s : j;
-    // rows j and p in the panel's columns outside [j, s1)
-    if (blockIdx.x == 0 && p != j)
-      for (int c = k0 + (int)threadIdx.x; c < k1; c += blockDim.x) {
-        if (c >= j && c < s1) continue;
-        const size_t a = (size_t)c * ld + j, b = (size_t)c * ld + p;
-        const float tr = __ldcg(Ar + a), ti = __ldcg(Ai + a);
-        Ar[a] = __ldcg(Ar + b);
-        Ai[a] = __ldcg(Ai + b);
-        Ar[b] = tr;
-        Ai[b] = ti;
-      }
     const float2 pv = urow[0];
     const float den = pv.x * pv.x + pv.y * pv.y;
     float best = -1.f;
@@ -285,22 +280,99 @@ __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_
           Ar[o] = xr[k];
           Ai[o] = xi[k];
         }
-      if (wj > 1) argmax_pair(best, bi, xr[1] * xr[1] + xi[1] * xi[1], r);
+      if (wj > 1) {
+        const float v = xr[1] * xr[1] + xi[1] * xi[1];
+        if (v > best || (v == best && r < bi)) {
+          best = v;
+          bi = r;
+#pragma unroll
+          for (int k = 1; k < LU_SB; k++)
+            if (k < wj) cand[k - 1][threadIdx.x] = make_float2(xr[k], xi[k]);
+        }
+      }
     }
     if (j + 1 < s1) {
-      publish(best, bi, j + 1, gen ^ 1);
+      float bv;
+      int brow, who;
+      bool mine;
+      block_argmax(best, bi, sv, si, st, bv, brow, mine, &who);
+      PanelSlot* sl = slots + (size_t)(gen ^ 1) * PANEL_MAX_BLOCKS + blockIdx.x;
+      if (threadIdx.x == 0) {
+        sl->mx = bv;
+        sl->ix = brow;
+      }
+      if (brow < n && (int)threadIdx.x < wj - 1) sl->row[threadIdx.x] = cand[threadIdx.x][who];
       panel_bar(cnt, bad, ++nbar * G);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bad) != 0) atomicOr(err, 16);  // a barrier gave up
 }
 
-// Sub-panel [s0, s1) of a panel ending at k1: its rows of the panel's later columns,
-// U = L11^-1 A (L11 the unit lower triangle of the sub-panel's diagonal block).  L11 in
-// shared memory; thread per column c in [s1, k1), its w values loaded together.
-__global__ void __launch_bounds__(LU_NB) k_sub_trsm(float* Ar, float* Ai, size_t ld, int s0, int s1, int k1) {
+// After the sub-panel [s0, s1) of the panel [k0, k1): its row interchanges applied to the
+// panel's other columns (in order; a column c of the sub-panel takes those of its later
+// columns j > c), then its rows of the panel's later columns, U = L11^-1 A (L11 the unit
+// lower triangle of the sub-panel's diagonal block).  One block, a thread per panel
+// column: the rows the swaps reach (the sub-panel's rows and the pivot rows below it, at
+// most 2 LU_SB) are loaded together into shared memory, swapped there and written back.
+__global__ void __launch_bounds__(LU_NB) k_sub_finish(float* Ar, float* Ai, size_t ld, int k0, int s0, int s1, int k1,
+                                                      const int* ipiv) {
+  __shared__ int srow[2 * LU_SB], slot[LU_SB];
+  __shared__ int nslot;
   __shared__ float Lr[LU_SB][LU_SB], Li[LU_SB][LU_SB];  // [column t][row i]
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2(*vals)[LU_NB] = reinterpret_cast<float2(*)[LU_NB]>(smraw);  // [2 LU_SB][LU_NB], 64 KB
+  __shared__ int pv[LU_SB];
   const int w = s1 - s0;
+  if ((int)threadIdx.x < w) pv[threadIdx.x] = ipiv[s0 + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    // slots 0 .. w - 1: rows s0 .. s1 - 1; then each distinct pivot row below s1
+    int ns = w;
+    for (int i = 0; i < w; i++) srow[i] = s0 + i;
+    for (int j = 0; j < w; j++) {
+      const int p = pv[j];
+      int q = p - s0;
+      if (p >= s1) {
+        q = -1;
+        for (int t = w; t < ns; t++)
+          if (srow[t] == p) q = t;
+        if (q < 0) {
+          srow[ns] = p;
+          q = ns++;
+        }
+      }
+      slot[j] = q;
+    }
+    nslot = ns;
+  }
+  __syncthreads();
+  const int c = k0 + threadIdx.x;
+  const int ns = nslot;
+  if (c < k1) {
+    const int jlo = (c >= s0 && c < s1) ? c + 1 - s0 : 0;
+    if (jlo < w) {
+#pragma unroll
+      for (int q = 0; q < 2 * LU_SB; q++)
+        if (q < ns) vals[q][threadIdx.x] = make_float2(Ar[(size_t)c * ld + srow[q]], Ai[(size_t)c * ld + srow[q]]);
+      for (int j = jlo; j < w; j++) {
+        const int q = slot[j];
+        if (q != j) {
+          const float2 t = vals[j][threadIdx.x];
+          vals[j][threadIdx.x] = vals[q][threadIdx.x];
+          vals[q][threadIdx.x] = t;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 2 * LU_SB; q++)
+        if (q < ns) {
+          Ar[(size_t)c * ld + srow[q]] = vals[q][threadIdx.x].x;
+          Ai[(size_t)c * ld + srow[q]] = vals[q][threadIdx.x].y;
+        }
+    }
+  }
+  __syncthreads();
+  if (s1 >= k1) return;
+  // U rows of the later columns: L11 (now in its final rows) staged, thread per column
   for (int e = threadIdx.x; e < LU_SB * LU_SB; e += blockDim.x) {
     const int t = e / LU_SB, i = e - t * LU_SB;
     const bool in = t < w && i < w;
@@ -308,8 +380,7 @@ __global__ void __launch_bounds__(LU_NB) k_sub_trsm(float* Ar, float* Ai, size_t
     Li[t][i] = in ? Ai[(size_t)(s0 + t) * ld + s0 + i] : 0.f;
   }
   __syncthreads();
-  const int c = s1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= k1) return;
+  if (c < s1 || c >= k1) return;
   float xr[LU_SB], xi[LU_SB];
 #pragma unroll
   for (int i = 0; i < LU_SB; i++) {
@@ -337,6 +408,7 @@ __global__ void __launch_bounds__(LU_NB) k_sub_trsm(float* Ar, float* Ai, size_t
 // rows in shared memory; thread per row, its w L values in registers, the columns in
 // groups of 8 whose loads are issued together.
 static const int LU_UPD_CG = 8;
+static const int LU_UPD_SLICE = 64;  // columns per block of the grid's second dimension
 __global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, size_t ld, int n, int s0, int s1,
                                                     int k1) {
   __shared__ float ur[LU_SB][LU_NB], ui[LU_SB][LU_NB];
@@ -368,14 +440,16 @@ __global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, siz
     lr[t] = t < w ? Ar[(size_t)(s0 + t) * ld + r] : 0.f;
     li[t] = t < w ? Ai[(size_t)(s0 + t) * ld + r] : 0.f;
   }
+  // this block's slice of LU_UPD_SLICE columns
+  const int cend = min(nc, (int)(blockIdx.y + 1) * LU_UPD_SLICE);
 #pragma unroll 1
-  for (int c0 = 0; c0 < nc; c0 += LU_UPD_CG) {
+  for (int c0 = blockIdx.y * LU_UPD_SLICE; c0 < cend; c0 += LU_UPD_CG) {
     float cr[LU_UPD_CG], ci[LU_UPD_CG];
 #pragma unroll
     for (int g = 0; g < LU_UPD_CG; g++) {
       const size_t o = (size_t)(s1 + c0 + g) * ld + r;
-      cr[g] = c0 + g < nc ? Ar[o] : 0.f;
-      ci[g] = c0 + g < nc ? Ai[o] : 0.f;
+      cr[g] = c0 + g < cend ? Ar[o] : 0.f;
+      ci[g] = c0 + g < cend ? Ai[o] : 0.f;
     }
 #pragma unroll
     for (int t = 0; t < LU_SB; t++) {  // rows t >= w of ur/ui are zero
@@ -389,7 +463,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, siz
     }
 #pragma unroll
     for (int g = 0; g < LU_UPD_CG; g++)
-      if (c0 + g < nc) {
+      if (c0 + g < cend) {
         const size_t o = (size_t)(s1 + c0 + g) * ld + r;
         Ar[o] = cr[g];
         Ai[o] = ci[g];
@@ -561,120 +635,134 @@ __global__ void __launch_bounds__(512) k_trsm_l(float* Ar, float* Ai, size_t ld,
   }
 }
 
-// The diagonal blocks of the factors, copied once after the factorisation into one
-// contiguous 128 KB slab each ([plane][col][row], LU_TB x LU_TB, zero past a ragged last
-// block), so that a triangular solve stages a block with one bulk copy.
-__global__ void __launch_bounds__(256) k_copy_diag(const float* Ar, const float* Ai, size_t ld, int n,
-                                                   float* out) {
+// The inverses of the factors' diagonal blocks, formed once after the factorisation:
+// block b (rows [128 b, 128 b + nb)) gives L11^-1 (unit lower) in slab 2 b and U11^-1 in
+// slab 2 b + 1, each 128 KB ([plane][col][row], LU_TB x LU_TB, zero past a ragged last
+// block), so that a triangular solve applies a diagonal block as one matrix-vector
+// product instead of a 128-step substitution.  Grid (blocks, 2), 16 warps: the block in
+// shared memory, a warp per column of the inverse (column c solves against e_c).
+__global__ void __launch_bounds__(512) k_diag_inverse(const float* Ar, const float* Ai, size_t ld, int n,
+                                                      float* out) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
+  float* Di = Dr + LU_TB * LU_TB;
   const int k0 = blockIdx.x * LU_TB, nb = min(LU_TB, n - k0);
-  float* o = out + (size_t)blockIdx.x * 2 * LU_TB * LU_TB;
-  for (int e0 = threadIdx.x; e0 < LU_TB * LU_TB; e0 += 8 * blockDim.x) {
-    float vr[8], vi[8];
+  const bool lower = blockIdx.y == 0;
+  stage_block(Ar, Ai, ld, k0, nb, Dr, Di);
+  __syncthreads();
+  float* o = out + ((size_t)blockIdx.x * 2 + (lower ? 0 : 1)) * 2 * LU_TB * LU_TB;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int c = warp; c < LU_TB; c += nw) {
+    float xr[4], xi[4];
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const int e = e0 + q * blockDim.x, col = e / LU_TB, row = e - col * LU_TB;
-      const bool in = col < nb && row < nb;
-      vr[q] = in ? Ar[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
-      vi[q] = in ? Ai[(size_t)(k0 + col) * ld + k0 + row] : 0.f;
+    for (int q = 0; q < 4; q++) {
+      xr[q] = (lane + 32 * q == c && c < nb) ? 1.f : 0.f;
+      xi[q] = 0.f;
+    }
+    if (c < nb) {
+      if (lower) {
+        for (int i = c; i < nb; i++) {
+          const int q0 = i >> 5;
+          float vr = 0.f, vi = 0.f;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (q == q0) {
+              vr = __shfl_sync(0xffffffffu, xr[q], i & 31);
+              vi = __shfl_sync(0xffffffffu, xi[q], i & 31);
+            }
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int r = lane + 32 * q;
+            if (r > i && r < nb) {
+              const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+              xr[q] -= lr * vr - li * vi;
+              xi[q] -= lr * vi + li * vr;
+            }
+          }
+        }
+      } else {
+        for (int i = c; i >= 0; i--) {
+          const int q0 = i >> 5;
+          float br = 0.f, bi = 0.f;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (q == q0) {
+              br = __shfl_sync(0xffffffffu, xr[q], i & 31);
+              bi = __shfl_sync(0xffffffffu, xi[q], i & 31);
+            }
+          const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
+          const float den = ur * ur + ui * ui;
+          const float vr = (br * ur + bi * ui) / den, vi = (bi * ur - br * ui) / den;
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int r = lane + 32 * q;
+            if (r == i) {
+              xr[q] = vr;
+              xi[q] = vi;
+            } else if (r < i) {
+              const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
+              xr[q] -= lr * vr - li * vi;
+              xi[q] -= lr * vi + li * vr;
+            }
+          }
+        }
+      }
     }
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const int e = e0 + q * blockDim.x;
-      o[e] = vr[q];
-      o[LU_TB * LU_TB + e] = vi[q];
+    for (int q = 0; q < 4; q++) {
+      o[c * LU_TB + lane + 32 * q] = xr[q];
+      o[LU_TB * LU_TB + c * LU_TB + lane + 32 * q] = xi[q];
     }
   }
 }
 
 // Solves with the factors, one vector (complex64, internal order) in place.  Diagonal
-// block: x[k0 .. k0 + nb) = L11^-1 x (lower, unit diagonal) or U11^-1 x (upper).  The block
-// arrives by one bulk copy on an mbarrier (bounded wait: on give-up the kernel records
-// bit 32 in *err, waits once more, bounded, for the copy, and leaves x alone); one warp
-// then runs the substitution with lane l holding rows l, l + 32, l + 64, l + 96.
-__global__ void __launch_bounds__(32) k_trsv_diag(const float* diag, int k0, int nb, int lower, cc* x, int* err) {
+// block: x[k0 .. k0 + nb) = D^-1 x with D^-1 the block's precomputed inverse (L11^-1 or
+// U11^-1).  The inverse arrives by one bulk copy on an mbarrier (bounded wait: on give-up
+// the kernel records bit 32 in *err, waits once more, bounded, for the copy, and leaves x
+// alone); two threads per row then form the product from shared memory.
+__global__ void __launch_bounds__(256) k_trsv_diag(const float* dinv, int k0, int nb, cc* x, int* err) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ float br[LU_TB], bi[LU_TB];
   float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
   float* Di = Dr + LU_TB * LU_TB;
-  const int lane = threadIdx.x;
   const unsigned bytes = 2u * LU_TB * LU_TB * sizeof(float);
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     tc::mbar_init(&bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  __syncwarp();
-  if (lane == 0) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
     tc::mbar_expect_tx(&bar, bytes);
-    tc::bulk_g2s(Dr, diag, bytes, &bar);
+    tc::bulk_g2s(Dr, dinv, bytes, &bar);
   }
-  float xr[4], xi[4];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int r = lane + 32 * q;
-    xr[q] = r < nb ? x[k0 + r].re : 0.f;
-    xi[q] = r < nb ? x[k0 + r].im : 0.f;
+  if (threadIdx.x < LU_TB) {
+    const int r = threadIdx.x;
+    br[r] = r < nb ? x[k0 + r].re : 0.f;
+    bi[r] = r < nb ? x[k0 + r].im : 0.f;
   }
+  __syncthreads();
   if (!tc::mbar_wait(&bar, 0)) {
-    if (lane == 0) atomicOr(err, 32);
+    if (threadIdx.x == 0) atomicOr(err, 32);
     tc::mbar_wait(&bar, 0);
     return;
   }
-  if (lower) {
-    for (int i = 0; i < nb; i++) {
-      const int q0 = i >> 5;
-      float vr = 0.f, vi = 0.f;
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (q == q0) {
-          vr = __shfl_sync(0xffffffffu, xr[q], i & 31);
-          vi = __shfl_sync(0xffffffffu, xi[q], i & 31);
-        }
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int r = lane + 32 * q;
-        if (r > i) {
-          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
-          xr[q] -= lr * vr - li * vi;
-          xi[q] -= lr * vi + li * vr;
-        }
-      }
-    }
-  } else {
-    for (int i = nb - 1; i >= 0; i--) {
-      const int q0 = i >> 5;
-      float br = 0.f, bi = 0.f;
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (q == q0) {
-          br = __shfl_sync(0xffffffffu, xr[q], i & 31);
-          bi = __shfl_sync(0xffffffffu, xi[q], i & 31);
-        }
-      const float ur = Dr[i * LU_TB + i], ui = Di[i * LU_TB + i];
-      const float den = ur * ur + ui * ui;
-      const float vr = (br * ur + bi * ui) / den, vi = (bi * ur - br * ui) / den;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int r = lane + 32 * q;
-        if (r == i) {
-          xr[q] = vr;
-          xi[q] = vi;
-        } else if (r < i) {
-          const float lr = Dr[i * LU_TB + r], li = Di[i * LU_TB + r];
-          xr[q] -= lr * vr - li * vi;
-          xi[q] -= lr * vi + li * vr;
-        }
-      }
-    }
+  const int r = threadIdx.x >> 1, h = threadIdx.x & 1;
+  float sr = 0.f, si = 0.f;
+#pragma unroll 8
+  for (int c = h * (LU_TB / 2); c < (h + 1) * (LU_TB / 2); c++) {
+    const float ar = Dr[c * LU_TB + r], ai = Di[c * LU_TB + r];
+    sr += ar * br[c] - ai * bi[c];
+    si += ar * bi[c] + ai * br[c];
   }
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int r = lane + 32 * q;
-    if (r < nb) x[k0 + r] = mk<float>(xr[q], xi[q]);
-  }
+  sr += __shfl_xor_sync(0xffffffffu, sr, 1);
+  si += __shfl_xor_sync(0xffffffffu, si, 1);
+  if (h == 0 && r < nb) x[k0 + r] = mk<float>(sr, si);
 }
 
-// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb): four threads per row,
-// each a quarter of the columns with its 16 loads in flight, summed by shuffles.
+// x[rows r0 .. r1) -= A[r0 .. r1, k0 .. k0 + nb) x[k0 .. k0 + nb): eight threads per row,
+// each 16 columns with their loads in flight together, summed by shuffles.
 __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
                                                    int r0, int r1, cc* x) {
   __shared__ float br[LU_TB], bi[LU_TB];
@@ -684,31 +772,29 @@ __global__ void __launch_bounds__(256) k_trsv_gemv(const float* Ar, const float*
   }
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = r0 + (t >> 2), part = t & 3;
+  const int i = r0 + (t >> 3), part = t & 7;
   const bool live = i < r1;
   float sr = 0.f, si = 0.f;
   if (live) {
+    float ar[16], ai[16];
 #pragma unroll
-    for (int h = 0; h < LU_TB / 4; h += 16) {
-      float ar[16], ai[16];
+    for (int q = 0; q < 16; q++) {
+      const int j = part * 16 + q;
+      ar[q] = j < nb ? Ar[(size_t)(k0 + j) * ld + i] : 0.f;
+      ai[q] = j < nb ? Ai[(size_t)(k0 + j) * ld + i] : 0.f;
+    }
 #pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int j = part * (LU_TB / 4) + h + q;
-        ar[q] = j < nb ? Ar[(size_t)(k0 + j) * ld + i] : 0.f;
-        ai[q] = j < nb ? Ai[(size_t)(k0 + j) * ld + i] : 0.f;
-      }
-#pragma unroll
-      for (int q = 0; q < 16; q++) {
-        const int j = part * (LU_TB / 4) + h + q;
-        sr += ar[q] * br[j] - ai[q] * bi[j];
-        si += ar[q] * bi[j] + ai[q] * br[j];
-      }
+    for (int q = 0; q < 16; q++) {
+      const int j = part * 16 + q;
+      sr += ar[q] * br[j] - ai[q] * bi[j];
+      si += ar[q] * bi[j] + ai[q] * br[j];
     }
   }
-  sr += __shfl_xor_sync(0xffffffffu, sr, 1);
-  si += __shfl_xor_sync(0xffffffffu, si, 1);
-  sr += __shfl_xor_sync(0xffffffffu, sr, 2);
-  si += __shfl_xor_sync(0xffffffffu, si, 2);
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    si += __shfl_xor_sync(0xffffffffu, si, o);
+  }
   if (live && part == 0) {
     x[i].re -= sr;
     x[i].im -= si;
@@ -769,7 +855,7 @@ static int lu_tc_factor(sie_ctx* c) {
   if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_at = nullptr;
   if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_bt = nullptr;
   const int ndiag = (n + LU_TB - 1) / LU_TB;
-  if (!c->d_lu_diag && cudaMalloc(&c->d_lu_diag, (size_t)ndiag * 2 * LU_TB * LU_TB * sizeof(float)) != cudaSuccess)
+  if (!c->d_lu_diag && cudaMalloc(&c->d_lu_diag, (size_t)ndiag * 4 * LU_TB * LU_TB * sizeof(float)) != cudaSuccess)
     c->d_lu_diag = nullptr;
   if (!c->d_lu_scr || c->lu_scr_bytes < scr_bytes) {
     if (c->d_lu_scr) cudaFree(c->d_lu_scr);
@@ -810,7 +896,9 @@ static int lu_tc_factor(sie_ctx* c) {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_ev;
   double gemm_flops = 0;
   const size_t trsm_smem = (size_t)2 * LU_TB * LU_TB * sizeof(float);
-  if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess) rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
+  const size_t finish_smem = (size_t)2 * LU_SB * LU_NB * sizeof(float2);
+  if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess || raise_smem(k_sub_finish, finish_smem) != cudaSuccess)
+    rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
   // optional per-phase device times (SIE_LU_PHASES=1): panel, swaps, L11 solve, tiling
   const char* pe = getenv("SIE_LU_PHASES");
   const bool phases = pe && atoi(pe) != 0;
@@ -893,11 +981,12 @@ static int lu_tc_factor(sie_ctx* c) {
         }
         count_launch();
       }
+      k_sub_finish<<<1, LU_NB, finish_smem, sp>>>(Ar, Ai, ld, k0, s0, s1, k1, ipiv);
+      count_launch();
       if (s1 < k1) {
-        k_sub_trsm<<<1, LU_NB, 0, sp>>>(Ar, Ai, ld, s0, s1, k1);
-        count_launch();
         if (s1 < n) {
-          k_sub_update<<<(n - s1 + 255) / 256, 256, 0, sp>>>(Ar, Ai, ld, n, s0, s1, k1);
+          k_sub_update<<<dim3((n - s1 + 255) / 256, (k1 - s1 + LU_UPD_SLICE - 1) / LU_UPD_SLICE), 256, 0, sp>>>(
+              Ar, Ai, ld, n, s0, s1, k1);
           count_launch();
         }
       }
@@ -979,8 +1068,13 @@ static int lu_tc_factor(sie_ctx* c) {
     cudaStreamWaitEvent(s, ev_sg, 0);
   }
   if (rc == SIE_OK) {
-    k_copy_diag<<<ndiag, 256, 0, s>>>(Ar, Ai, ld, n, c->d_lu_diag);
-    count_launch();
+    const size_t ism = (size_t)2 * LU_TB * LU_TB * sizeof(float);
+    if (raise_smem(k_diag_inverse, ism) != cudaSuccess) {
+      rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
+    } else {
+      k_diag_inverse<<<dim3(ndiag, 2), 512, ism, s>>>(Ar, Ai, ld, n, c->d_lu_diag);
+      count_launch();
+    }
   }
   int herr = 0;
   if (rc == SIE_OK && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -1039,22 +1133,22 @@ static int lu_tc_solve32(sie_ctx* c, cc* x, cudaStream_t s) {
   SIE_CUDA(cudaMemcpyAsync(x, c->d_tmp32, (size_t)n * sizeof(cc), cudaMemcpyDeviceToDevice, s));
   const size_t dsm = (size_t)2 * LU_TB * LU_TB * sizeof(float);
   SIE_CUDA(raise_smem(k_trsv_diag, dsm));
-  const size_t blk = (size_t)2 * LU_TB * LU_TB;
+  const size_t slab = (size_t)2 * LU_TB * LU_TB;
   for (int k0 = 0; k0 < n; k0 += LU_TB) {
     const int nb = std::min(LU_TB, n - k0), k1 = k0 + nb;
-    k_trsv_diag<<<1, 32, dsm, s>>>(c->d_lu_diag + (size_t)(k0 / LU_TB) * blk, k0, nb, 1, x, err);
+    k_trsv_diag<<<1, 256, dsm, s>>>(c->d_lu_diag + (size_t)(2 * (k0 / LU_TB)) * slab, k0, nb, x, err);
     count_launch();
     if (k1 < n) {
-      k_trsv_gemv<<<(4 * (n - k1) + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
+      k_trsv_gemv<<<(8 * (n - k1) + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, k1, n, x);
       count_launch();
     }
   }
   for (int k0 = ((n - 1) / LU_TB) * LU_TB; k0 >= 0; k0 -= LU_TB) {
     const int nb = std::min(LU_TB, n - k0);
-    k_trsv_diag<<<1, 32, dsm, s>>>(c->d_lu_diag + (size_t)(k0 / LU_TB) * blk, k0, nb, 0, x, err);
+    k_trsv_diag<<<1, 256, dsm, s>>>(c->d_lu_diag + (size_t)(2 * (k0 / LU_TB) + 1) * slab, k0, nb, x, err);
     count_launch();
     if (k0 > 0) {
-      k_trsv_gemv<<<(4 * k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
+      k_trsv_gemv<<<(8 * k0 + 255) / 256, 256, 0, s>>>(Ar, Ai, ld, k0, nb, 0, k0, x);
       count_launch();
     }
   }
