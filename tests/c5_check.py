@@ -19,13 +19,10 @@ c - h and c + h.  A control passes when the central difference agrees with the a
 to 1e-4 relative; a control with flipped triples is reported as across a jump, with its
 one-sided differences.
 
-The solves themselves set a floor under the differences: the refinement stops at a
-backward error of 1e-12, near the FP64 residual's own rounding (eps * ||Z|| ||x|| / ||b||,
-with ||Z|| ||x|| / ||b|| about 7e3 on this slab), so each J carries a relative error of
-about 1e-8, which a step of 1e-4 lambda turns into an absolute error of about 6e-4 in the
-difference.  A smooth control that misses 1e-4 relative is therefore also differenced
-with a step of 1e-3 lambda (ten times less of that noise), which the report gives beside
-it.
+A smooth control that misses 1e-4 relative is also differenced with a step of 1e-3
+lambda, which the report gives beside it with that step's flipped triples.  The report
+also gives J from the FP64 LU and from the mixed solve: their difference bounds the part
+of the solves in the differences.
 
 Run: python -m tests.c5_check  (prints one JSON line; exit status 1 if a control without
 flipped triples is off by more than 1e-4 relative)."""
