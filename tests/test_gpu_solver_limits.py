@@ -7,7 +7,9 @@
 - The grid-wide waits of the Arnoldi kernel are bounded: with the limit set to one poll
   (SIE_GRID_SPIN_LIMIT) a solve returns SIE_ERR_CUDA instead of waiting, and the context
   solves normally afterwards.  No GPU fault is involved: the kernel records the failed wait
-  and returns."""
+  and returns.
+- A device allocation that cannot succeed (the dense matrix of a mesh whose near panels
+  exceed the GPU's memory) ends the set-up with SIE_ERR_NOMEM, and the next context works."""
 import numpy as np
 import pytest
 
@@ -65,3 +67,29 @@ def test_bounded_grid_wait_reports_and_recovers(gpu_lib, monkeypatch):
     assert st["iterations"] == 10
     assert np.linalg.norm(x - x_ref) <= 1e-12 * np.linalg.norm(x_ref)
     g.close()
+
+
+def test_allocation_failure_reports_nomem(gpu_lib):
+    import torch
+    from specklesim_b200 import Sie, SieError, _lib, incidence, mesh
+    total = torch.cuda.get_device_properties(0).total_memory
+    # a dense context stores 48 bytes per pair of RWG edges: pick a slab whose pairs need more
+    # than the whole device
+    cells = 64
+    while True:
+        V, T = mesh.slab_config(cells / 6.4, P.WL, 0.3, 1.0, 4, cells=cells, thickness_wl=1.0)
+        M = mesh.edge_count(T)
+        if 48.0 * M * M > 1.05 * total:
+            break
+        cells += 8
+    big = Sie(V, T, P.WL, P.EPS_METAL, dense=True)
+    with pytest.raises(SieError) as e:
+        big.setup()
+    assert e.value.code == _lib.SIE_ERR_NOMEM
+    big.close()  # frees whatever the failed set-up had allocated
+    V, T = P.sphere(2)
+    g = Sie(V, T, P.WL, P.EPS_METAL, dense=True).setup()
+    x, st = g.solve_direct_mixed(g.rhs_planewave(*incidence(0.0, 0.0, "TM", 2)), tolerance=1e-12)
+    assert st["converged"]
+    g.close()
+
