@@ -1499,6 +1499,12 @@ template <> const float* trfp<float>(const Level& L) { return L.trf32; }
 template <typename T> static const T* ivalp(const InterpDev& I);
 template <> const double* ivalp<double>(const InterpDev& I) { return I.val; }
 template <> const float* ivalp<float>(const InterpDev& I) { return I.val32; }
+template <typename T> static const T* ievalp(const InterpDev& I);
+template <> const double* ievalp<double>(const InterpDev& I) { return I.eval; }
+template <> const float* ievalp<float>(const InterpDev& I) { return I.eval32; }
+template <typename T> static const T* iovalp(const InterpDev& I);
+template <> const double* iovalp<double>(const InterpDev& I) { return I.oval; }
+template <> const float* iovalp<float>(const InterpDev& I) { return I.oval32; }
 
 // Interpolation between two levels' samplings on every (theta, phi) item pair of nbox
 // coefficient blocks [8][Q]: out[b][item][q] (+)= sum_k val[k] in[b][...][col[k]], with
@@ -1571,11 +1577,85 @@ __global__ void __launch_bounds__(256) k_interp_s(const int* __restrict__ ptr, c
   }
 }
 
+// The same on the tap-major stencil: the block's 8 x Qi inputs staged in shared memory,
+// a thread per output row, four taps' (column, weight) pairs loaded together (coalesced
+// across the warp's rows) before their shared-memory reads and multiply-adds; the long
+// rows' remaining taps from the CSR overflow.
+template <typename T>
+__global__ void __launch_bounds__(256) k_interp_e(const int* __restrict__ ecol, const T* __restrict__ eval, int ew,
+                                                  const int* __restrict__ optr, const int* __restrict__ ocol,
+                                                  const T* __restrict__ oval, int rows,
+                                                  const cx<T>* __restrict__ in, int Qi,
+                                                  cx<T>* __restrict__ out, int Qo, int accum) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [8][Qi]
+  const size_t b = blockIdx.x;
+  const cx<T>* src = in + b * 8 * (size_t)Qi;
+  for (int i = threadIdx.x; i < 8 * Qi; i += blockDim.x) xs[i] = src[i];
+  __syncthreads();
+  cx<T>* dst = out + b * 8 * (size_t)Qo;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    cx<T> acc[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) acc[p] = mk<T>(0, 0);
+    for (int t0 = 0; t0 < ew; t0 += 4) {
+      int j[4];
+      T w[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const bool in_ = t0 + u < ew;
+        j[u] = in_ ? ecol[(size_t)(t0 + u) * rows + r] : 0;
+        w[u] = in_ ? eval[(size_t)(t0 + u) * rows + r] : (T)0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const cx<T>* sp = j[u] < Qi ? xs + j[u] : xs + (size_t)4 * Qi + (j[u] - Qi);
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+          const cx<T> v = sp[(size_t)p * Qi];
+          acc[p].re = fma(w[u], v.re, acc[p].re);
+          acc[p].im = fma(w[u], v.im, acc[p].im);
+        }
+      }
+    }
+    for (int k = optr[r]; k < optr[r + 1]; k++) {
+      const int j = ocol[k];
+      const T w = oval[k];
+      const cx<T>* sp = j < Qi ? xs + j : xs + (size_t)4 * Qi + (j - Qi);
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const cx<T> v = sp[(size_t)p * Qi];
+        acc[p].re = fma(w, v.re, acc[p].re);
+        acc[p].im = fma(w, v.im, acc[p].im);
+      }
+    }
+    const int q = r < Qo ? r : r - Qo, i0 = r < Qo ? 0 : 4;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      cx<T>* o = dst + (size_t)(i0 + p) * Qo + q;
+      if (accum) *o += acc[p];
+      else *o = acc[p];
+    }
+  }
+}
+
 // nbox blocks of [8][Qi] through I into blocks of [8][Qo] (Qo = I.rows / 2).
 template <typename T>
 static int interp_run(const InterpDev& I, const cx<T>* in, int Qi, cx<T>* out, size_t nbox, bool accum,
                       cudaStream_t st) {
   const size_t smem = (size_t)8 * Qi * sizeof(cx<T>);
+  if (smem <= (size_t)200 * 1024 && ievalp<T>(I)) {
+    SIE_CUDA(raise_smem(k_interp_e<T>, smem));
+    for (size_t b0 = 0; b0 < nbox; b0 += 2147483647u) {
+      const unsigned nb = (unsigned)std::min<size_t>(2147483647u, nbox - b0);
+      k_interp_e<T><<<nb, 256, smem, st>>>(I.ecol, ievalp<T>(I), I.ew, I.optr, I.ocol, iovalp<T>(I), I.rows,
+                                           in + b0 * 8 * Qi, Qi, out + b0 * 8 * (I.rows / 2), I.rows / 2,
+                                           accum ? 1 : 0);
+      sie::count_launch();
+    }
+    SIE_CUDA(cudaGetLastError());
+    return SIE_OK;
+  }
   if (smem <= (size_t)200 * 1024) {
     SIE_CUDA(raise_smem(k_interp_s<T>, smem));
     for (size_t b0 = 0; b0 < nbox; b0 += 2147483647u) {
@@ -2212,6 +2292,15 @@ int make_f32_tables(sie_ctx* c) {
         if (I->nnz > 0) {
           SIE_CUDA(cudaMalloc(&I->val32, (size_t)I->nnz * sizeof(float)));
           k_trf_f32<<<(unsigned)((I->nnz + 255) / 256), 256, 0, st>>>(I->val, I->val32, (int)I->nnz);
+          sie::count_launch();
+          const int ne = I->ew * I->rows;
+          SIE_CUDA(cudaMalloc(&I->eval32, (size_t)std::max(ne, 1) * sizeof(float)));
+          if (ne > 0) {
+            k_trf_f32<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(I->eval, I->eval32, ne);
+            sie::count_launch();
+          }
+          SIE_CUDA(cudaMalloc(&I->oval32, (size_t)I->onnz * sizeof(float)));
+          k_trf_f32<<<(unsigned)((I->onnz + 255) / 256), 256, 0, st>>>(I->oval, I->oval32, (int)I->onnz);
           sie::count_launch();
         }
       SIE_CUDA(cudaGetLastError());

@@ -623,6 +623,40 @@ static int upload_interp(const Csr& A, InterpDev& d) {
   SIE_TRY(upload(&d.ptr, A.ptr));
   SIE_TRY(upload(&d.col, A.col));
   SIE_TRY(upload(&d.val, A.val));
+  // ELL width: the row length that covers 99.5 % of the rows, a multiple of 4
+  std::vector<int> len(A.rows);
+  for (int r = 0; r < A.rows; r++) len[r] = A.ptr[r + 1] - A.ptr[r];
+  std::vector<int> sorted_len = len;
+  std::sort(sorted_len.begin(), sorted_len.end());
+  int ew = A.rows ? sorted_len[std::min(A.rows - 1, (int)(0.995 * A.rows))] : 0;
+  ew = (ew + 3) / 4 * 4;
+  std::vector<int> ec((size_t)ew * A.rows, 0), op(A.rows + 1, 0), oc;
+  std::vector<double> ev((size_t)ew * A.rows, 0.0), ov;
+  for (int r = 0; r < A.rows; r++) {
+    for (int k = A.ptr[r]; k < A.ptr[r + 1]; k++) {
+      const int t = k - A.ptr[r];
+      if (t < ew) {
+        const size_t o = (size_t)t * A.rows + r;
+        ec[o] = A.col[k];
+        ev[o] = A.val[k];
+      } else {
+        oc.push_back(A.col[k]);
+        ov.push_back(A.val[k]);
+      }
+    }
+    op[r + 1] = (int)oc.size();
+  }
+  if (oc.empty()) {  // keep the overflow arrays non-empty
+    oc.push_back(0);
+    ov.push_back(0.0);
+  }
+  d.ew = ew;
+  d.onnz = (long long)ov.size();
+  SIE_TRY(upload(&d.ecol, ec));
+  SIE_TRY(upload(&d.eval, ev));
+  SIE_TRY(upload(&d.optr, op));
+  SIE_TRY(upload(&d.ocol, oc));
+  SIE_TRY(upload(&d.oval, ov));
   return SIE_OK;
 }
 
@@ -1669,7 +1703,9 @@ int sie_free(sie_ctx* c) {
     void* lp[] = {L.C, L.D, L.tl, L.ph_up, L.ph_dn, L.tl32, L.ph_up32, L.ph_dn32, L.i4_ptr, L.i4_src, L.i4_off,
                   L.ch_ptr, L.ch_idx, L.ch_oct, L.parent, L.oct, L.grp_sib, L.grp_src, L.Cb, L.Db,
                   L.khat, L.trf, L.trf32, L.up.ptr, L.up.col, L.up.val, L.up.val32, L.dn.ptr, L.dn.col,
-                  L.dn.val, L.dn.val32};
+                  L.dn.val, L.dn.val32, L.up.ecol, L.up.eval, L.up.eval32, L.dn.ecol, L.dn.eval,
+                  L.dn.eval32, L.up.optr, L.up.ocol, L.up.oval, L.up.oval32, L.dn.optr, L.dn.ocol,
+                  L.dn.oval, L.dn.oval32};
     for (void* p : lp)
       if (p) cudaFree(p);
   }

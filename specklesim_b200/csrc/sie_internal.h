@@ -113,6 +113,18 @@ struct InterpDev {
   double* val = nullptr;
   float* val32 = nullptr;     // complex64 passes (made with the other complex64 tables)
   long long nnz = 0;
+  // the same stencil tap-major (ELL): tap t of row r at [t * rows + r], rows padded to
+  // ew taps with weight 0, so a warp's 32 rows read each tap coalesced; the taps of the
+  // few longer rows (the poles of the anterpolation) past ew in a CSR overflow
+  int ew = 0;
+  int* ecol = nullptr;
+  double* eval = nullptr;
+  float* eval32 = nullptr;
+  int* optr = nullptr;
+  int* ocol = nullptr;
+  double* oval = nullptr;
+  float* oval32 = nullptr;
+  long long onnz = 0;
 };
 
 struct Level {
