@@ -95,9 +95,9 @@ static const size_t PANEL_CNT_OFF = PANEL_SLOTS_OFF + 2 * PANEL_MAX_BLOCKS * siz
 static size_t panel_cnt_bytes(int n) { return ((size_t)n / LU_SB + 2) * sizeof(unsigned); }
 // then the swap plan of the latest panel: {count, src[2 LU_NB], dst[2 LU_NB]}
 static size_t panel_plan_off(int n) { return (PANEL_CNT_OFF + panel_cnt_bytes(n) + 255) / 256 * 256; }
-// and the two operand maxima of the split-FP16 updates
+// and the operand maxima of the split-FP16 updates (the trailing ones, then the panel's own)
 static size_t panel_amax_off(int n) { return (panel_plan_off(n) + (1 + 4 * LU_NB) * sizeof(int) + 15) / 16 * 16; }
-static size_t panel_scratch_bytes(int n) { return panel_amax_off(n) + 2 * sizeof(unsigned); }
+static size_t panel_scratch_bytes(int n) { return panel_amax_off(n) + 4 * sizeof(unsigned); }
 
 // Grid barrier of the cooperative sub-panel kernel (all its blocks are resident) on a
 // counter that only grows within one launch: the m-th barrier waits for m * gridDim.x
@@ -169,10 +169,10 @@ __device__ __forceinline__ void block_argmax(float v, int i, float* sv, int* si,
 // that row's values in columns [j, s1).  After it, every block reduces the slots to the
 // same pivot p (the first maximum, as izamax) and takes the pivot row from the winning
 // slot, so nobody reads row p from the matrix.  Row j and row p trade places logically in
-// the sub-panel's columns [j, s1): the thread that owns row p reads the old row j, writes
-// the pivot row into row j and the updated old row j into row p.  The two rows' values in
-// the panel's other columns are swapped after the launch (k_sub_finish), as nothing here
-// reads them.  Each row r > j is then scaled and updated, and the block's best candidate
+// the sub-panel's columns: the thread that owns row p reads the old row j, writes the
+// pivot row into row j and the updated old row j into row p, and swaps the two rows' L
+// values in the columns [s0, j).  Their values in the panel's other columns are swapped
+// after the launch (k_sub_finish), as nothing here reads them.  Each row r > j is then scaled and updated, and the block's best candidate
 // for column j + 1 goes to the other generation of slots: every thread keeps the values of
 // its best row in shared memory, so the winner's row is published without a reload.
 // Matrix and slot reads bypass L1 (__ldcg): other blocks' writes are seen through L2.
@@ -290,6 +290,29 @@ __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_
             if (k < wj) cand[k - 1][threadIdx.x] = make_float2(xr[k], xi[k]);
         }
       }
+      if (r == p) {  // rows j and p also trade their L values in the columns [s0, j), in
+                     // two halves whose loads are issued together
+#pragma unroll
+        for (int h = 0; h < LU_SB; h += LU_SB / 2) {
+          float er[LU_SB / 2], ei[LU_SB / 2], fr[LU_SB / 2], fi[LU_SB / 2];
+#pragma unroll
+          for (int k = 0; k < LU_SB / 2; k++)
+            if (s0 + h + k < j) {
+              er[k] = __ldcg(Ar + (size_t)(s0 + h + k) * ld + j);
+              ei[k] = __ldcg(Ai + (size_t)(s0 + h + k) * ld + j);
+              fr[k] = __ldcg(Ar + (size_t)(s0 + h + k) * ld + p);
+              fi[k] = __ldcg(Ai + (size_t)(s0 + h + k) * ld + p);
+            }
+#pragma unroll
+          for (int k = 0; k < LU_SB / 2; k++)
+            if (s0 + h + k < j) {
+              Ar[(size_t)(s0 + h + k) * ld + j] = fr[k];
+              Ai[(size_t)(s0 + h + k) * ld + j] = fi[k];
+              Ar[(size_t)(s0 + h + k) * ld + p] = er[k];
+              Ai[(size_t)(s0 + h + k) * ld + p] = ei[k];
+            }
+        }
+      }
     }
     if (j + 1 < s1) {
       float bv;
@@ -308,90 +331,97 @@ __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_
   if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bad) != 0) atomicOr(err, 16);  // a barrier gave up
 }
 
-// After the sub-panel [s0, s1) of the panel [k0, k1): its row interchanges applied to the
-// panel's other columns (in order; a column c of the sub-panel takes those of its later
-// columns j > c), then its rows of the panel's later columns, U = L11^-1 A (L11 the unit
-// lower triangle of the sub-panel's diagonal block).  One block, a thread per panel
-// column: the rows the swaps reach (the sub-panel's rows and the pivot rows below it, at
-// most 2 LU_SB) are loaded together into shared memory, swapped there and written back.
-__global__ void __launch_bounds__(LU_NB) k_sub_finish(float* Ar, float* Ai, size_t ld, int k0, int s0, int s1, int k1,
-                                                      const int* ipiv) {
-  __shared__ int srow[2 * LU_SB], slot[LU_SB];
+// After the sub-panel [s0, s1) of the panel [k0, k1): its row interchanges applied, in
+// order, to the panel's columns outside the sub-panel (the sub-panel's own columns were
+// swapped by k_subpanel), then its rows of the later columns of its 64-column block
+// [s1, uend), U = L11^-1 A (L11 the unit lower triangle of the sub-panel's diagonal
+// block).  A thread per panel column, LU_FIN_T columns per block: the rows the swaps reach
+// (the sub-panel's rows and the pivot rows below it, at most 2 LU_SB) are loaded together
+// into shared memory, swapped there and written back.  No block writes the sub-panel's
+// columns, so every block reads L11 from memory without waiting on the others.
+static const int LU_FIN_T = 64;
+__global__ void __launch_bounds__(LU_FIN_T) k_sub_finish(float* Ar, float* Ai, size_t ld, int k0, int s0, int s1,
+                                                         int k1, int uend, const int* ipiv) {
+  __shared__ int pv[LU_SB], slot[LU_SB], first[LU_SB], srow[2 * LU_SB];
   __shared__ int nslot;
-  __shared__ float Lr[LU_SB][LU_SB], Li[LU_SB][LU_SB];  // [column t][row i]
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float2(*vals)[LU_NB] = reinterpret_cast<float2(*)[LU_NB]>(smraw);  // [2 LU_SB][LU_NB], 64 KB
-  __shared__ int pv[LU_SB];
-  const int w = s1 - s0;
-  if ((int)threadIdx.x < w) pv[threadIdx.x] = ipiv[s0 + threadIdx.x];
+  __shared__ float2 vals[2 * LU_SB][LU_FIN_T];
+  __shared__ float2 L11[LU_SB][LU_SB];  // [column t][row i]
+  const int w = s1 - s0, tid = threadIdx.x;
+  if (tid < w) pv[tid] = ipiv[s0 + tid];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // slots 0 .. w - 1: rows s0 .. s1 - 1; then each distinct pivot row below s1
-    int ns = w;
-    for (int i = 0; i < w; i++) srow[i] = s0 + i;
-    for (int j = 0; j < w; j++) {
-      const int p = pv[j];
-      int q = p - s0;
-      if (p >= s1) {
-        q = -1;
-        for (int t = w; t < ns; t++)
-          if (srow[t] == p) q = t;
-        if (q < 0) {
-          srow[ns] = p;
-          q = ns++;
+  // slots 0 .. w - 1: rows s0 .. s1 - 1; then each distinct pivot row below s1, in order of
+  // its first appearance (thread j finds pivot j's slot)
+  if (tid < w) {
+    const int p = pv[tid];
+    int f = tid;
+    if (p >= s1)
+      for (int j = 0; j < tid; j++)
+        if (pv[j] == p) {
+          f = j;
+          break;
         }
-      }
-      slot[j] = q;
-    }
-    nslot = ns;
+    first[tid] = f;
   }
   __syncthreads();
-  const int c = k0 + threadIdx.x;
+  if (tid < w) {
+    const int p = pv[tid];
+    if (p < s1) {
+      slot[tid] = p - s0;
+    } else {
+      int rank = 0;  // first appearances below s1 before this pivot's
+      for (int j = 0; j < first[tid]; j++) rank += (pv[j] >= s1 && first[j] == j) ? 1 : 0;
+      slot[tid] = w + rank;
+      if (first[tid] == tid) srow[w + rank] = p;
+    }
+    srow[tid] = s0 + tid;
+  }
+  if (tid == 0) {
+    int cnt = 0;
+    for (int j = 0; j < w; j++) cnt += (pv[j] >= s1 && first[j] == j) ? 1 : 0;
+    nslot = w + cnt;
+  }
+  __syncthreads();
   const int ns = nslot;
-  if (c < k1) {
-    const int jlo = (c >= s0 && c < s1) ? c + 1 - s0 : 0;
-    if (jlo < w) {
+  const int c = k0 + blockIdx.x * LU_FIN_T + tid;
+  if (c < k1 && (c < s0 || c >= s1)) {
 #pragma unroll
-      for (int q = 0; q < 2 * LU_SB; q++)
-        if (q < ns) vals[q][threadIdx.x] = make_float2(Ar[(size_t)c * ld + srow[q]], Ai[(size_t)c * ld + srow[q]]);
-      for (int j = jlo; j < w; j++) {
-        const int q = slot[j];
-        if (q != j) {
-          const float2 t = vals[j][threadIdx.x];
-          vals[j][threadIdx.x] = vals[q][threadIdx.x];
-          vals[q][threadIdx.x] = t;
-        }
+    for (int q = 0; q < 2 * LU_SB; q++)
+      if (q < ns) vals[q][tid] = make_float2(Ar[(size_t)c * ld + srow[q]], Ai[(size_t)c * ld + srow[q]]);
+    for (int j = 0; j < w; j++) {
+      const int q = slot[j];
+      if (q != j) {
+        const float2 t = vals[j][tid];
+        vals[j][tid] = vals[q][tid];
+        vals[q][tid] = t;
       }
-#pragma unroll
-      for (int q = 0; q < 2 * LU_SB; q++)
-        if (q < ns) {
-          Ar[(size_t)c * ld + srow[q]] = vals[q][threadIdx.x].x;
-          Ai[(size_t)c * ld + srow[q]] = vals[q][threadIdx.x].y;
-        }
     }
+#pragma unroll
+    for (int q = 0; q < 2 * LU_SB; q++)
+      if (q < ns) {
+        Ar[(size_t)c * ld + srow[q]] = vals[q][tid].x;
+        Ai[(size_t)c * ld + srow[q]] = vals[q][tid].y;
+      }
+  }
+  // U rows of the block's columns in [s1, uend)
+  const int cb0 = k0 + blockIdx.x * LU_FIN_T;
+  if (s1 >= uend || cb0 + LU_FIN_T <= s1 || cb0 >= uend) return;  // uniform over the block
+  for (int e = tid; e < w * w; e += blockDim.x) {
+    const int t = e / w, i = e - t * w;
+    L11[t][i] = make_float2(Ar[(size_t)(s0 + t) * ld + s0 + i], Ai[(size_t)(s0 + t) * ld + s0 + i]);
   }
   __syncthreads();
-  if (s1 >= k1) return;
-  // U rows of the later columns: L11 (now in its final rows) staged, thread per column
-  for (int e = threadIdx.x; e < LU_SB * LU_SB; e += blockDim.x) {
-    const int t = e / LU_SB, i = e - t * LU_SB;
-    const bool in = t < w && i < w;
-    Lr[t][i] = in ? Ar[(size_t)(s0 + t) * ld + s0 + i] : 0.f;
-    Li[t][i] = in ? Ai[(size_t)(s0 + t) * ld + s0 + i] : 0.f;
-  }
-  __syncthreads();
-  if (c < s1 || c >= k1) return;
+  if (c < s1 || c >= uend) return;
   float xr[LU_SB], xi[LU_SB];
 #pragma unroll
-  for (int i = 0; i < LU_SB; i++) {
-    xr[i] = i < w ? Ar[(size_t)c * ld + s0 + i] : 0.f;
-    xi[i] = i < w ? Ai[(size_t)c * ld + s0 + i] : 0.f;
+  for (int i = 0; i < LU_SB; i++) {  // rows s0 .. s1 - 1 of column c, after the swaps above
+    xr[i] = i < w ? vals[i][tid].x : 0.f;
+    xi[i] = i < w ? vals[i][tid].y : 0.f;
   }
 #pragma unroll
   for (int i = 1; i < LU_SB; i++)
 #pragma unroll
     for (int t = 0; t < i; t++) {
-      const float lr = Lr[t][i], li = Li[t][i];
+      const float lr = t < w && i < w ? L11[t][i].x : 0.f, li = t < w && i < w ? L11[t][i].y : 0.f;
       xr[i] -= lr * xr[t] - li * xi[t];
       xi[i] -= lr * xi[t] + li * xr[t];
     }
@@ -403,16 +433,67 @@ __global__ void __launch_bounds__(LU_NB) k_sub_finish(float* Ar, float* Ai, size
     }
 }
 
-// Rank-w update of the panel's later columns by a factored sub-panel [s0, s1):
-// a_rc -= sum_t l_rt u_tc for rows r >= s1 and columns c in [s1, k1).  The sub-panel's U
+// U rows [b0, b1) of the panel's columns [c0, c1): x = L^-1 x with L the unit lower
+// triangle of the 64-column block's diagonal (b1 - b0 <= LU_BB).  A block per LU_BB
+// columns, a thread per column; L and the columns in shared memory (dynamic, 64 KB).
+static const int LU_BB = 64;
+__global__ void __launch_bounds__(LU_BB) k_blk_trsm(float* Ar, float* Ai, size_t ld, int b0, int b1, int c0,
+                                                    int c1) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2(*L)[LU_BB] = reinterpret_cast<float2(*)[LU_BB]>(smraw);                      // [col t][row i]
+  float2(*X)[LU_BB] = reinterpret_cast<float2(*)[LU_BB]>(smraw + LU_BB * LU_BB * 8);  // [row i][thread]
+  const int w = b1 - b0, t = threadIdx.x;
+  for (int e0 = t; e0 < w * w; e0 += 8 * LU_BB) {
+    float2 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * LU_BB, col = e / w, row = e - col * w;
+      v[q] = e < w * w ? make_float2(Ar[(size_t)(b0 + col) * ld + b0 + row], Ai[(size_t)(b0 + col) * ld + b0 + row])
+                       : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int e = e0 + q * LU_BB, col = e / w, row = e - col * w;
+      if (e < w * w) L[col][row] = v[q];
+    }
+  }
+  const int c = c0 + blockIdx.x * LU_BB + t;
+  const bool live = c < c1;
+  for (int i0 = 0; i0 < w; i0 += 16) {
+    float2 v[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      v[q] = live && i0 + q < w ? make_float2(Ar[(size_t)c * ld + b0 + i0 + q], Ai[(size_t)c * ld + b0 + i0 + q])
+                                : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      if (i0 + q < w) X[i0 + q][t] = v[q];
+  }
+  __syncthreads();
+  if (!live) return;
+  for (int i = 1; i < w; i++) {
+    float2 x = X[i][t];
+    for (int k = 0; k < i; k++) {
+      const float2 l = L[k][i], y = X[k][t];
+      x.x -= l.x * y.x - l.y * y.y;
+      x.y -= l.x * y.y + l.y * y.x;
+    }
+    X[i][t] = x;
+    Ar[(size_t)c * ld + b0 + i] = x.x;
+    Ai[(size_t)c * ld + b0 + i] = x.y;
+  }
+}
+
+// Rank-w update of the later columns of the sub-panel's 64-column block by a factored
+// sub-panel [s0, s1): a_rc -= sum_t l_rt u_tc for rows r >= s1 and columns c in [s1, uend).  The sub-panel's U
 // rows in shared memory; thread per row, its w L values in registers, the columns in
 // groups of 8 whose loads are issued together.
 static const int LU_UPD_CG = 8;
 static const int LU_UPD_SLICE = 64;  // columns per block of the grid's second dimension
 __global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, size_t ld, int n, int s0, int s1,
-                                                    int k1) {
+                                                    int uend) {
   __shared__ float ur[LU_SB][LU_NB], ui[LU_SB][LU_NB];
-  const int w = s1 - s0, nc = k1 - s1;
+  const int w = s1 - s0, nc = uend - s1;
   for (int e0 = threadIdx.x; e0 < LU_SB * LU_NB; e0 += 4 * blockDim.x) {
     float vr[4], vi[4];
 #pragma unroll
@@ -583,70 +664,20 @@ __device__ __forceinline__ void stage_block(const float* Ar, const float* Ai, si
   }
 }
 
-// X = L^-1 X in place for a diagonal block of the factors: L the unit lower triangle of
-// the nb x nb block at (k0, k0) (nb <= LU_TB), X its rows [k0, k0 + nb) in columns [c0, n).
-// L in shared memory (staged once per block: the grid is one block per multiprocessor, 16
-// warps each); one warp per column, lane l holding rows l, l + 32, l + 64, l + 96.
-__global__ void __launch_bounds__(512) k_trsm_l(float* Ar, float* Ai, size_t ld, int n, int k0, int nb, int c0) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float* Lr = reinterpret_cast<float*>(smraw);  // [col][row], nb x nb
-  float* Li = Lr + LU_TB * LU_TB;
-  stage_block(Ar, Ai, ld, k0, nb, Lr, Li);
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nw = blockDim.x >> 5;
-  for (int c = c0 + blockIdx.x * nw + warp; c < n; c += gridDim.x * nw) {
-    float* cr = Ar + (size_t)c * ld + k0;
-    float* ci = Ai + (size_t)c * ld + k0;
-    float xr[4], xi[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int r = lane + 32 * q;
-      xr[q] = r < nb ? cr[r] : 0.f;
-      xi[q] = r < nb ? ci[r] : 0.f;
-    }
-    for (int i = 0; i < nb; i++) {
-      const int q0 = i >> 5;
-      float vr = 0.f, vi = 0.f;
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (q == q0) {
-          vr = __shfl_sync(0xffffffffu, xr[q], i & 31);
-          vi = __shfl_sync(0xffffffffu, xi[q], i & 31);
-        }
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int r = lane + 32 * q;
-        if (r > i && r < nb) {
-          const float lr = Lr[i * LU_TB + r], li = Li[i * LU_TB + r];
-          xr[q] -= lr * vr - li * vi;
-          xi[q] -= lr * vi + li * vr;
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int r = lane + 32 * q;
-      if (r < nb) {
-        cr[r] = xr[q];
-        ci[r] = xi[q];
-      }
-    }
-  }
-}
-
-// The inverses of the factors' diagonal blocks, formed once after the factorisation:
-// block b (rows [128 b, 128 b + nb)) gives L11^-1 (unit lower) in slab 2 b and U11^-1 in
-// slab 2 b + 1, each 128 KB ([plane][col][row], LU_TB x LU_TB, zero past a ragged last
-// block), so that a triangular solve applies a diagonal block as one matrix-vector
-// product instead of a 128-step substitution.  Grid (blocks, 2), 16 warps: the block in
-// shared memory, a warp per column of the inverse (column c solves against e_c).
-__global__ void __launch_bounds__(512) k_diag_inverse(const float* Ar, const float* Ai, size_t ld, int n,
+// The inverses of diagonal blocks of the factors: grid block b covers rows
+// [128 (blk0 + b), min(128 (blk0 + b + 1), n)) and gives its unit lower triangle's inverse
+// in slab 2 b and (with a second grid row) its upper triangle's in slab 2 b + 1, each
+// 128 KB ([plane][col][row], LU_TB x LU_TB, zero past a ragged block).  Formed for all
+// blocks once after the factorisation, so that a triangular solve applies a diagonal
+// block as one matrix-vector product instead of a 128-step substitution, and for the two
+// blocks of each panel's L11.  16 warps: the block in shared memory, a warp per column of
+// the inverse (column c solves against e_c).
+__global__ void __launch_bounds__(512) k_diag_inverse(const float* Ar, const float* Ai, size_t ld, int n, int blk0,
                                                       float* out) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float* Dr = reinterpret_cast<float*>(smraw);  // [col][row]
   float* Di = Dr + LU_TB * LU_TB;
-  const int k0 = blockIdx.x * LU_TB, nb = min(LU_TB, n - k0);
+  const int k0 = (blk0 + blockIdx.x) * LU_TB, nb = min(LU_TB, n - k0);  // rows [k0, min(k0 + 128, n))
   const bool lower = blockIdx.y == 0;
   stage_block(Ar, Ai, ld, k0, nb, Dr, Di);
   __syncthreads();
@@ -712,6 +743,67 @@ __global__ void __launch_bounds__(512) k_diag_inverse(const float* Ar, const flo
     for (int q = 0; q < 4; q++) {
       o[c * LU_TB + lane + 32 * q] = xr[q];
       o[LU_TB * LU_TB + c * LU_TB + lane + 32 * q] = xi[q];
+    }
+  }
+}
+
+// M = I - L11^-1 for a panel's unit lower diagonal block of nb <= 256 rows, made of the
+// 128-row blocks A (top) and B (bottom) and the block C below A: from the inverses of A
+// and B (slabs 0 and 2 of inv), M11 = I - A^-1, M22 = I - B^-1, M21 = B^-1 C A^-1 and
+// M12 = 0, column-major with leading dimension LU_NB.  Then U12 = L11^-1 A12 is the
+// in-place update A12 -= M A12, a tensor-core GEMM.  Grid: a block per column j of M,
+// 128 threads.
+__global__ void __launch_bounds__(LU_TB) k_l11_m(const float* Ar, const float* Ai, size_t ld, int k0, int nb,
+                                                 const float* inv, float* Mr, float* Mi) {
+  __shared__ float tr[LU_TB], ti[LU_TB];
+  const int j = blockIdx.x, r = threadIdx.x;
+  const int n1 = min(LU_TB, nb), n2 = nb - n1;
+  const size_t sl = (size_t)LU_TB * LU_TB;
+  const float *Ar_inv = inv, *Ai_inv = inv + sl;              // A^-1: [col][row]
+  const float *Br_inv = inv + 4 * sl, *Bi_inv = inv + 5 * sl;  // B^-1 (slab 2)
+  float* mr = Mr + (size_t)j * LU_NB;
+  float* mi = Mi + (size_t)j * LU_NB;
+  if (j < n1) {
+    if (r < n1) {
+      mr[r] = (r == j ? 1.f : 0.f) - Ar_inv[(size_t)j * LU_TB + r];
+      mi[r] = -Ai_inv[(size_t)j * LU_TB + r];
+    }
+    if (n2 > 0) {
+      // t = C A^-1[:, j], C(r, k) = L11(n1 + r, k)
+      float sr = 0.f, si = 0.f;
+      if (r < n2) {
+#pragma unroll 16
+        for (int k = 0; k < n1; k++) {
+          const float cr = Ar[(size_t)(k0 + k) * ld + k0 + n1 + r], ci = Ai[(size_t)(k0 + k) * ld + k0 + n1 + r];
+          const float ar = Ar_inv[(size_t)j * LU_TB + k], ai = Ai_inv[(size_t)j * LU_TB + k];
+          sr += cr * ar - ci * ai;
+          si += cr * ai + ci * ar;
+        }
+      }
+      tr[r] = sr;
+      ti[r] = si;
+      __syncthreads();
+      if (r < n2) {  // M21[:, j] = B^-1 t
+        float ur = 0.f, ui = 0.f;
+#pragma unroll 16
+        for (int k = 0; k < n2; k++) {
+          const float br = Br_inv[(size_t)k * LU_TB + r], bi = Bi_inv[(size_t)k * LU_TB + r];
+          ur += br * tr[k] - bi * ti[k];
+          ui += br * ti[k] + bi * tr[k];
+        }
+        mr[n1 + r] = ur;
+        mi[n1 + r] = ui;
+      }
+    }
+  } else {
+    const int jj = j - n1;
+    if (r < n1) {
+      mr[r] = 0.f;
+      mi[r] = 0.f;
+    }
+    if (r < n2) {
+      mr[n1 + r] = (r == jj ? 1.f : 0.f) - Br_inv[(size_t)jj * LU_TB + r];
+      mi[n1 + r] = -Bi_inv[(size_t)jj * LU_TB + r];
     }
   }
 }
@@ -854,6 +946,15 @@ static int lu_tc_factor(sie_ctx* c) {
   if (!c->d_piv32 && cudaMalloc(&c->d_piv32, (size_t)n * sizeof(int)) != cudaSuccess) c->d_piv32 = nullptr;
   if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_at = nullptr;
   if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_bt = nullptr;
+  // the panel's own updates (beside the previous trailing update, which still reads At, Bt)
+  if (!c->d_lu_at2 && cudaMalloc(&c->d_lu_at2, tc::tiled_bytes_host(n, LU_BB) + tc::tiled_bytes_host(LU_NB, LU_BB)) !=
+                          cudaSuccess)
+    c->d_lu_at2 = nullptr;
+  // a panel's L11 work: two blocks' inverse slabs (4 x 128 KB with the unused upper ones),
+  // then M = I - L11^-1 in two LU_NB x LU_NB planes
+  if (!c->d_lu_minv &&
+      cudaMalloc(&c->d_lu_minv, (8 * (size_t)LU_TB * LU_TB + 2 * (size_t)LU_NB * LU_NB) * sizeof(float)) != cudaSuccess)
+    c->d_lu_minv = nullptr;
   const int ndiag = (n + LU_TB - 1) / LU_TB;
   if (!c->d_lu_diag && cudaMalloc(&c->d_lu_diag, (size_t)ndiag * 4 * LU_TB * LU_TB * sizeof(float)) != cudaSuccess)
     c->d_lu_diag = nullptr;
@@ -862,7 +963,8 @@ static int lu_tc_factor(sie_ctx* c) {
     if (cudaMalloc(&c->d_lu_scr, scr_bytes) != cudaSuccess) c->d_lu_scr = nullptr;
     c->lu_scr_bytes = c->d_lu_scr ? scr_bytes : 0;
   }
-  if (!c->d_lu32 || !c->d_lu32i || !c->d_piv32 || !c->d_lu_at || !c->d_lu_bt || !c->d_lu_scr || !c->d_lu_diag) {
+  if (!c->d_lu32 || !c->d_lu32i || !c->d_piv32 || !c->d_lu_at || !c->d_lu_bt || !c->d_lu_scr || !c->d_lu_diag ||
+      !c->d_lu_minv || !c->d_lu_at2) {
     cudaGetLastError();
     return fail(SIE_ERR_NOMEM, "mixed LU: device memory");
   }
@@ -871,6 +973,8 @@ static int lu_tc_factor(sie_ctx* c) {
   int* ipiv = c->d_piv32;
   char* At = c->d_lu_at;
   char* Bt = c->d_lu_bt;
+  char* At2 = c->d_lu_at2;
+  char* Bt2 = At2 + tc::tiled_bytes_host(n, LU_BB);
   int* err = (int*)c->d_lu_scr;
   PanelSlot* slots = (PanelSlot*)((char*)c->d_lu_scr + PANEL_SLOTS_OFF);
   unsigned* pcnt = (unsigned*)((char*)c->d_lu_scr + PANEL_CNT_OFF);  // one counter per sub-panel launch
@@ -896,8 +1000,8 @@ static int lu_tc_factor(sie_ctx* c) {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_ev;
   double gemm_flops = 0;
   const size_t trsm_smem = (size_t)2 * LU_TB * LU_TB * sizeof(float);
-  const size_t finish_smem = (size_t)2 * LU_SB * LU_NB * sizeof(float2);
-  if (raise_smem(k_trsm_l, trsm_smem) != cudaSuccess || raise_smem(k_sub_finish, finish_smem) != cudaSuccess)
+  const size_t blk_smem = (size_t)2 * LU_BB * LU_BB * sizeof(float2);
+  if (raise_smem(k_diag_inverse, trsm_smem) != cudaSuccess || raise_smem(k_blk_trsm, blk_smem) != cudaSuccess)
     rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
   // optional per-phase device times (SIE_LU_PHASES=1): panel, swaps, L11 solve, tiling
   const char* pe = getenv("SIE_LU_PHASES");
@@ -947,6 +1051,10 @@ static int lu_tc_factor(sie_ctx* c) {
   const bool lookahead = !(la && atoi(la) == 0);
   // trailing updates in split-FP16 unless this context's refinement needed 3xTF32 before
   // (or SIE_LU_GEMM=tf32 asks for it)
+  // the panel's block width: LU_BB, or the whole panel (SIE_LU_BLOCK=256: every sub-panel
+  // updates all of the panel's later columns on the CUDA cores)
+  int pbb = LU_BB;
+  if (const char* e = getenv("SIE_LU_BLOCK")) pbb = atoi(e) >= LU_NB ? LU_NB : LU_BB;
   const char* gp = getenv("SIE_LU_GEMM");
   const bool gh = c->lu_f16_ok && !(gp && std::string(gp) == "tf32");
   c->tm.lu_f16 = gh ? 1 : 0;
@@ -967,8 +1075,12 @@ static int lu_tc_factor(sie_ctx* c) {
     mark(0, true, pk);
     // the panel in sub-panels of LU_SB columns: column steps inside the sub-panel, then
     // one rank-LU_SB update of the panel's later columns
+    // the panel in 64-column blocks of 16-column sub-panels: inside a block, each
+    // sub-panel updates the block's later columns (CUDA cores); after a block, its U rows
+    // of the panel's remaining columns and one tensor-core update of those columns
     for (int s0 = k0; s0 < k1; s0 += LU_SB) {
       const int s1 = std::min(s0 + LU_SB, k1);
+      const int b0 = k0 + (s0 - k0) / pbb * pbb, b1 = std::min(b0 + pbb, k1);
       {
         int ns0 = s0, ns1 = s1, nn0 = n, kk0 = k0, kk1 = k1;
         size_t ldd = ld;
@@ -981,14 +1093,25 @@ static int lu_tc_factor(sie_ctx* c) {
         }
         count_launch();
       }
-      k_sub_finish<<<1, LU_NB, finish_smem, sp>>>(Ar, Ai, ld, k0, s0, s1, k1, ipiv);
+      k_sub_finish<<<(k1 - k0 + LU_FIN_T - 1) / LU_FIN_T, LU_FIN_T, 0, sp>>>(Ar, Ai, ld, k0, s0, s1, k1, b1, ipiv);
       count_launch();
-      if (s1 < k1) {
-        if (s1 < n) {
-          k_sub_update<<<dim3((n - s1 + 255) / 256, (k1 - s1 + LU_UPD_SLICE - 1) / LU_UPD_SLICE), 256, 0, sp>>>(
-              Ar, Ai, ld, n, s0, s1, k1);
-          count_launch();
-        }
+      if (s1 < b1 && s1 < n) {
+        k_sub_update<<<dim3((n - s1 + 255) / 256, (b1 - s1 + LU_UPD_SLICE - 1) / LU_UPD_SLICE), 256, 0, sp>>>(
+            Ar, Ai, ld, n, s0, s1, b1);
+        count_launch();
+      }
+      if (s1 == b1 && b1 < k1 && rc == SIE_OK) {
+        const int w = b1 - b0;
+        k_blk_trsm<<<(k1 - b1 + LU_BB - 1) / LU_BB, LU_BB, blk_smem, sp>>>(Ar, Ai, ld, b0, b1, b1, k1);
+        count_launch();
+        rc = tc::tile_operand(Ar + (size_t)b0 * ld + b1, Ai + (size_t)b0 * ld + b1, ld, n - b1, w, false, At2, sp, gh,
+                              amax + 2);
+        if (rc == SIE_OK)
+          rc = tc::tile_operand(Ar + (size_t)b1 * ld + b0, Ai + (size_t)b1 * ld + b0, ld, k1 - b1, w, true, Bt2, sp,
+                                gh, amax + 3);
+        if (rc == SIE_OK)
+          rc = tc::gemm_update(At2, Bt2, w, Ar + (size_t)b1 * ld + b1, Ai + (size_t)b1 * ld + b1, ld, n - b1, k1 - b1,
+                               err, sp, 0, gh, amax + 2);
       }
     }
     mark(0, false, pk);
@@ -1003,24 +1126,22 @@ static int lu_tc_factor(sie_ctx* c) {
     mark(1, false, pk);
     if (k1 < n) {
       mark(2, true, pk);
-      // U12 = L11^-1 A12 by diagonal blocks of LU_TB: each block's rows are solved, then the
-      // rows below it in the panel lose L21-block times them (a tensor-core update)
-      for (int d0 = k0; d0 < k1 && rc == SIE_OK; d0 += LU_TB) {
-        const int db = std::min(LU_TB, k1 - d0), d1 = d0 + db;
-        k_trsm_l<<<std::min(nsm, (n - k1 + 15) / 16), 512, trsm_smem, sp>>>(Ar, Ai, ld, n, d0, db, k1);
-        count_launch();
-        if (d1 < k1) {
-          const int mb = k1 - d1;
-          rc = tc::tile_operand(Ar + (size_t)d0 * ld + d1, Ai + (size_t)d0 * ld + d1, ld, mb, db, false, At, sp, gh,
-                                amax);
-          if (rc == SIE_OK)
-            rc = tc::tile_operand(Ar + (size_t)k1 * ld + d0, Ai + (size_t)k1 * ld + d0, ld, n - k1, db, true, Bt, sp,
-                                  gh, amax + 1);
-          if (rc == SIE_OK)
-            rc = tc::gemm_update(At, Bt, db, Ar + (size_t)k1 * ld + d1, Ai + (size_t)k1 * ld + d1, ld, mb, n - k1,
-                                 err, sp, 0, gh, amax);
-        }
-      }
+      // U12 = L11^-1 A12 as the in-place tensor-core update A12 -= (I - L11^-1) A12: the
+      // inverses of L11's two 128-row blocks, then M = I - L11^-1 (k_l11_m), then the GEMM
+      float* inv = c->d_lu_minv;
+      float* Mr = inv + 8 * (size_t)LU_TB * LU_TB;
+      float* Mi = Mr + (size_t)LU_NB * LU_NB;
+      k_diag_inverse<<<dim3((nb + LU_TB - 1) / LU_TB, 1), 512, trsm_smem, sp>>>(Ar, Ai, ld, k1, k0 / LU_TB, inv);
+      count_launch();
+      k_l11_m<<<nb, LU_TB, 0, sp>>>(Ar, Ai, ld, k0, nb, inv, Mr, Mi);
+      count_launch();
+      rc = tc::tile_operand(Mr, Mi, LU_NB, nb, nb, false, At, sp, gh, amax);
+      if (rc == SIE_OK)
+        rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, n - k1, nb, true, Bt, sp, gh,
+                              amax + 1);
+      if (rc == SIE_OK)
+        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, nb, n - k1, err, sp,
+                             0, gh, amax);
       mark(2, false, pk);
       const int m = n - k1, nn = std::min(LU_NB, m);
       // A22 -= L21 U12 on the tensor cores
@@ -1072,7 +1193,7 @@ static int lu_tc_factor(sie_ctx* c) {
     if (raise_smem(k_diag_inverse, ism) != cudaSuccess) {
       rc = fail(SIE_ERR_CUDA, "mixed LU: shared memory");
     } else {
-      k_diag_inverse<<<dim3(ndiag, 2), 512, ism, s>>>(Ar, Ai, ld, n, c->d_lu_diag);
+      k_diag_inverse<<<dim3(ndiag, 2), 512, ism, s>>>(Ar, Ai, ld, n, 0, c->d_lu_diag);
       count_launch();
     }
   }
@@ -1306,7 +1427,7 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
   for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32,
                   (void*)c->d_perm32, (void*)c->d_tmp32, (void*)c->d_lu_at, (void*)c->d_lu_bt, c->d_lu_scr,
-                  (void*)c->d_lu_diag})
+                  (void*)c->d_lu_diag, (void*)c->d_lu_minv, (void*)c->d_lu_at2})
     if (p) cudaFree(p);
   c->d_lu = nullptr;
   c->d_piv = nullptr;
@@ -1316,6 +1437,8 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   c->d_lu_at = c->d_lu_bt = nullptr;
   c->d_lu_scr = nullptr;
   c->d_lu_diag = nullptr;
+  c->d_lu_minv = nullptr;
+  c->d_lu_at2 = nullptr;
   c->lu_scr_bytes = 0;
   c->lu64_valid = c->lu32_valid = false;
   return SIE_OK;

@@ -1577,21 +1577,27 @@ __global__ void __launch_bounds__(256) k_interp_s(const int* __restrict__ ptr, c
   }
 }
 
-// The same on the tap-major stencil: the block's 8 x Qi inputs staged in shared memory,
-// a thread per output row, four taps' (column, weight) pairs loaded together (coalesced
-// across the warp's rows) before their shared-memory reads and multiply-adds; the long
-// rows' remaining taps from the CSR overflow.
+// The same on the tap-major stencil: the block's inputs staged in shared memory, a thread
+// per output row, four taps' (column, weight) pairs loaded together (coalesced across the
+// warp's rows) before their shared-memory reads and multiply-adds; the long rows' remaining
+// taps from the CSR overflow.  A block takes np of the four item pairs (pairs
+// blockIdx.y * np ..), so that a sampling too large for all eight items in shared memory
+// runs as two blocks of two pairs.
 template <typename T>
 __global__ void __launch_bounds__(256) k_interp_e(const int* __restrict__ ecol, const T* __restrict__ eval, int ew,
                                                   const int* __restrict__ optr, const int* __restrict__ ocol,
                                                   const T* __restrict__ oval, int rows,
                                                   const cx<T>* __restrict__ in, int Qi,
-                                                  cx<T>* __restrict__ out, int Qo, int accum) {
+                                                  cx<T>* __restrict__ out, int Qo, int accum, int np) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [8][Qi]
+  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [theta items p0 .. p0 + np, then phi items][Qi]
   const size_t b = blockIdx.x;
+  const int p0 = blockIdx.y * np;
   const cx<T>* src = in + b * 8 * (size_t)Qi;
-  for (int i = threadIdx.x; i < 8 * Qi; i += blockDim.x) xs[i] = src[i];
+  for (int i = threadIdx.x; i < 2 * np * Qi; i += blockDim.x) {
+    const int h = i / (np * Qi), rem = i - h * np * Qi;  // h: 0 theta, 1 phi
+    xs[i] = src[(size_t)(4 * h + p0) * Qi + rem];
+  }
   __syncthreads();
   cx<T>* dst = out + b * 8 * (size_t)Qo;
   for (int r = threadIdx.x; r < rows; r += blockDim.x) {
@@ -1609,33 +1615,36 @@ __global__ void __launch_bounds__(256) k_interp_e(const int* __restrict__ ecol, 
       }
 #pragma unroll
       for (int u = 0; u < 4; u++) {
-        const cx<T>* sp = j[u] < Qi ? xs + j[u] : xs + (size_t)4 * Qi + (j[u] - Qi);
+        const cx<T>* sp = j[u] < Qi ? xs + j[u] : xs + (size_t)np * Qi + (j[u] - Qi);
 #pragma unroll
-        for (int p = 0; p < 4; p++) {
-          const cx<T> v = sp[(size_t)p * Qi];
-          acc[p].re = fma(w[u], v.re, acc[p].re);
-          acc[p].im = fma(w[u], v.im, acc[p].im);
-        }
+        for (int p = 0; p < 4; p++)
+          if (p < np) {
+            const cx<T> v = sp[(size_t)p * Qi];
+            acc[p].re = fma(w[u], v.re, acc[p].re);
+            acc[p].im = fma(w[u], v.im, acc[p].im);
+          }
       }
     }
     for (int k = optr[r]; k < optr[r + 1]; k++) {
       const int j = ocol[k];
       const T w = oval[k];
-      const cx<T>* sp = j < Qi ? xs + j : xs + (size_t)4 * Qi + (j - Qi);
+      const cx<T>* sp = j < Qi ? xs + j : xs + (size_t)np * Qi + (j - Qi);
 #pragma unroll
-      for (int p = 0; p < 4; p++) {
-        const cx<T> v = sp[(size_t)p * Qi];
-        acc[p].re = fma(w, v.re, acc[p].re);
-        acc[p].im = fma(w, v.im, acc[p].im);
-      }
+      for (int p = 0; p < 4; p++)
+        if (p < np) {
+          const cx<T> v = sp[(size_t)p * Qi];
+          acc[p].re = fma(w, v.re, acc[p].re);
+          acc[p].im = fma(w, v.im, acc[p].im);
+        }
     }
     const int q = r < Qo ? r : r - Qo, i0 = r < Qo ? 0 : 4;
 #pragma unroll
-    for (int p = 0; p < 4; p++) {
-      cx<T>* o = dst + (size_t)(i0 + p) * Qo + q;
-      if (accum) *o += acc[p];
-      else *o = acc[p];
-    }
+    for (int p = 0; p < 4; p++)
+      if (p < np) {
+        cx<T>* o = dst + (size_t)(i0 + p0 + p) * Qo + q;
+        if (accum) *o += acc[p];
+        else *o = acc[p];
+      }
   }
 }
 
@@ -1644,13 +1653,18 @@ template <typename T>
 static int interp_run(const InterpDev& I, const cx<T>* in, int Qi, cx<T>* out, size_t nbox, bool accum,
                       cudaStream_t st) {
   const size_t smem = (size_t)8 * Qi * sizeof(cx<T>);
-  if (smem <= (size_t)200 * 1024 && ievalp<T>(I)) {
-    SIE_CUDA(raise_smem(k_interp_e<T>, smem));
-    for (size_t b0 = 0; b0 < nbox; b0 += 2147483647u) {
-      const unsigned nb = (unsigned)std::min<size_t>(2147483647u, nbox - b0);
-      k_interp_e<T><<<nb, 256, smem, st>>>(I.ecol, ievalp<T>(I), I.ew, I.optr, I.ocol, iovalp<T>(I), I.rows,
-                                           in + b0 * 8 * Qi, Qi, out + b0 * 8 * (I.rows / 2), I.rows / 2,
-                                           accum ? 1 : 0);
+  // all four item pairs per block; a sampling too large for eight items in shared memory
+  // takes the CSR kernel on global memory below (many more blocks in flight, which measured
+  // faster than two staged blocks of two pairs)
+  const int np = smem <= (size_t)200 * 1024 ? 4 : 0;
+  if (np > 0 && ievalp<T>(I)) {
+    const size_t sm = smem * np / 4;
+    SIE_CUDA(raise_smem(k_interp_e<T>, sm));
+    for (size_t b0 = 0; b0 < nbox; b0 += 65535u) {
+      const unsigned nb = (unsigned)std::min<size_t>(65535u, nbox - b0);
+      k_interp_e<T><<<dim3(nb, 4 / np), 256, sm, st>>>(I.ecol, ievalp<T>(I), I.ew, I.optr, I.ocol, iovalp<T>(I),
+                                                       I.rows, in + b0 * 8 * Qi, Qi, out + b0 * 8 * (I.rows / 2),
+                                                       I.rows / 2, accum ? 1 : 0, np);
       sie::count_launch();
     }
     SIE_CUDA(cudaGetLastError());

@@ -24,7 +24,13 @@ int fail(int code, const std::string& msg) {
 }
 int cuda_fail(cudaError_t e, const char* what) {
   g_err = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
-  return e == cudaErrorMemoryAllocation ? SIE_ERR_NOMEM : SIE_ERR_CUDA;
+  if (e == cudaErrorMemoryAllocation) {
+    // a failed allocation is not sticky: clear it, so that the next check of the runtime's
+    // last error (after a later launch) does not report it again
+    cudaGetLastError();
+    return SIE_ERR_NOMEM;
+  }
+  return SIE_ERR_CUDA;
 }
 
 // src/lib_sie_integration_points.f90:7-141; the literals are binary32.
@@ -1695,7 +1701,7 @@ int sie_free(sie_ctx* c) {
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
                   c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT, c->d_lu32, c->d_lu32i, c->d_piv32,
                   c->d_perm32, c->d_tmp32, c->d_lu_at, c->d_lu_bt, c->d_lu_scr,
-                  c->d_lu_diag};
+                  c->d_lu_diag, c->d_lu_minv, c->d_lu_at2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->d_lvtmp) cudaFree(c->d_lvtmp);

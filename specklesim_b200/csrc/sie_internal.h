@@ -333,7 +333,9 @@ struct sie_ctx {
   char* d_lu_at = nullptr;        // mixed LU workspace: the pre-tiled A and B operands of the
   char* d_lu_bt = nullptr;        // trailing updates,
   void* d_lu_scr = nullptr;       // the panel kernel's slots, barrier counters and error word
-  float* d_lu_diag = nullptr;     // the factors' diagonal blocks, contiguous, for the solves
+  float* d_lu_diag = nullptr;     // the inverses of the factors' diagonal blocks, for the solves
+  float* d_lu_minv = nullptr;     // a panel's I - L11^-1 and its blocks' inverses
+  char* d_lu_at2 = nullptr;       // the panel's own tensor-core updates: tiled L and U blocks
   size_t lu_scr_bytes = 0;
   // the factors above are current (sie_invalidate_factors clears these and keeps the memory,
   // sie_release_factors frees it)
