@@ -37,7 +37,8 @@ int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, siz
 size_t tiled_bytes_host(int rows, int K);
 }  // namespace tc
 
-static const int LU_NB = 256;  // panel width (the tensor-core update's K)
+static const int LU_NB = 256;  // default panel width (the tensor-core update's K); L11 blocks of U12
+static const int LU_NBX = 512;  // largest panel width (SIE_LU_NB=512)
 static const int LU_SB = 16;   // sub-panel width inside a panel
 static const int LU_TB = 128;  // diagonal blocks of the triangular solves
 static const int LU_FREE_SMS = 12;  // multiprocessors the look-ahead update leaves to the panels
@@ -93,10 +94,10 @@ struct PanelSlot {
 static const size_t PANEL_SLOTS_OFF = 256;
 static const size_t PANEL_CNT_OFF = PANEL_SLOTS_OFF + 2 * PANEL_MAX_BLOCKS * sizeof(PanelSlot);
 static size_t panel_cnt_bytes(int n) { return ((size_t)n / LU_SB + 2) * sizeof(unsigned); }
-// then the swap plan of the latest panel: {count, src[2 LU_NB], dst[2 LU_NB]}
+// then the swap plan of the latest panel: {count, src[2 LU_NBX], dst[2 LU_NBX]}
 static size_t panel_plan_off(int n) { return (PANEL_CNT_OFF + panel_cnt_bytes(n) + 255) / 256 * 256; }
 // and the operand maxima of the split-FP16 updates (the trailing ones, then the panel's own)
-static size_t panel_amax_off(int n) { return (panel_plan_off(n) + (1 + 4 * LU_NB) * sizeof(int) + 15) / 16 * 16; }
+static size_t panel_amax_off(int n) { return (panel_plan_off(n) + (1 + 4 * LU_NBX) * sizeof(int) + 15) / 16 * 16; }
 static size_t panel_scratch_bytes(int n) { return panel_amax_off(n) + 4 * sizeof(unsigned); }
 
 // Grid barrier of the cooperative sub-panel kernel (all its blocks are resident) on a
@@ -556,9 +557,9 @@ __global__ void __launch_bounds__(256, 2) k_sub_update(float* Ar, float* Ai, siz
 // gather: after them, row dst[i] holds the old row src[i], for the nb positions of the
 // panel and the rows outside it that the swaps reach (at most nb more).  One block; the
 // swaps are followed in order, the lookup of a row outside the panel searched by all
-// threads.  plan = {count, src[2 LU_NB], dst[2 LU_NB]}.
+// threads.  plan = {count, src[2 LU_NBX], dst[2 LU_NBX]}.
 __global__ void __launch_bounds__(256) k_swap_plan(const int* ipiv, int k0, int k1, int* plan) {
-  __shared__ int pos[2 * LU_NB], cont[2 * LU_NB], ip[LU_NB];
+  __shared__ int pos[2 * LU_NBX], cont[2 * LU_NBX], ip[LU_NBX];
   __shared__ int nx, found;
   const int nb = k1 - k0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) {
@@ -595,7 +596,7 @@ __global__ void __launch_bounds__(256) k_swap_plan(const int* ipiv, int k0, int 
   const int cnt = nb + nx;
   for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
     plan[1 + i] = cont[i];
-    plan[1 + 2 * LU_NB + i] = pos[i];
+    plan[1 + 2 * LU_NBX + i] = pos[i];
   }
   if (threadIdx.x == 0) plan[0] = cnt;
 }
@@ -612,7 +613,7 @@ __global__ void __launch_bounds__(512) k_swap_apply(float* Ar, float* Ai, size_t
   int src = 0, dst = 0;
   if (i < cnt) {
     src = plan[1 + i];
-    dst = plan[1 + 2 * LU_NB + i];
+    dst = plan[1 + 2 * LU_NBX + i];
   }
   float vr[LU_SWAP_TC], vi[LU_SWAP_TC];
   const int c0 = blockIdx.x * LU_SWAP_TC;
@@ -944,10 +945,10 @@ static int lu_tc_factor(sie_ctx* c) {
   if (!c->d_lu32 && cudaMalloc(&c->d_lu32, ld * n * sizeof(float)) != cudaSuccess) c->d_lu32 = nullptr;
   if (!c->d_lu32i && cudaMalloc(&c->d_lu32i, ld * n * sizeof(float)) != cudaSuccess) c->d_lu32i = nullptr;
   if (!c->d_piv32 && cudaMalloc(&c->d_piv32, (size_t)n * sizeof(int)) != cudaSuccess) c->d_piv32 = nullptr;
-  if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_at = nullptr;
-  if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NB)) != cudaSuccess) c->d_lu_bt = nullptr;
+  if (!c->d_lu_at && cudaMalloc(&c->d_lu_at, tc::tiled_bytes_host(n, LU_NBX)) != cudaSuccess) c->d_lu_at = nullptr;
+  if (!c->d_lu_bt && cudaMalloc(&c->d_lu_bt, tc::tiled_bytes_host(n, LU_NBX)) != cudaSuccess) c->d_lu_bt = nullptr;
   // the panel's own updates (beside the previous trailing update, which still reads At, Bt)
-  if (!c->d_lu_at2 && cudaMalloc(&c->d_lu_at2, tc::tiled_bytes_host(n, LU_BB) + tc::tiled_bytes_host(LU_NB, LU_BB)) !=
+  if (!c->d_lu_at2 && cudaMalloc(&c->d_lu_at2, tc::tiled_bytes_host(n, LU_BB) + tc::tiled_bytes_host(LU_NBX, LU_BB)) !=
                           cudaSuccess)
     c->d_lu_at2 = nullptr;
   // a panel's L11 work: two blocks' inverse slabs (4 x 128 KB with the unused upper ones),
@@ -1055,6 +1056,10 @@ static int lu_tc_factor(sie_ctx* c) {
   // updates all of the panel's later columns on the CUDA cores)
   int pbb = LU_BB;
   if (const char* e = getenv("SIE_LU_BLOCK")) pbb = atoi(e) >= LU_NB ? LU_NB : LU_BB;
+  // panel width: LU_NB, or LU_NBX (SIE_LU_NB=512: trailing updates of K = 512, which read
+  // and write the trailing matrix half as often per flop)
+  int pnb = LU_NB;
+  if (const char* e = getenv("SIE_LU_NB")) pnb = atoi(e) >= LU_NBX ? LU_NBX : LU_NB;
   const char* gp = getenv("SIE_LU_GEMM");
   const bool gh = c->lu_f16_ok && !(gp && std::string(gp) == "tf32");
   c->tm.lu_f16 = gh ? 1 : 0;
@@ -1070,8 +1075,8 @@ static int lu_tc_factor(sie_ctx* c) {
     panel_blocks = std::max(1, std::min(panel_blocks, atoi(e)));
   s = sp;  // the phase marks and the panel chain
   bool rest_pending = false;
-  for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += LU_NB) {
-    const int nb = std::min(LU_NB, n - k0), k1 = k0 + nb;
+  for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += pnb) {
+    const int nb = std::min(pnb, n - k0), k1 = k0 + nb;
     mark(0, true, pk);
     // the panel in sub-panels of LU_SB columns: column steps inside the sub-panel, then
     // one rank-LU_SB update of the panel's later columns
@@ -1120,30 +1125,46 @@ static int lu_tc_factor(sie_ctx* c) {
     if (n - nb > 0) {
       k_swap_plan<<<1, 256, 0, sp>>>(ipiv, k0, k1, plan);
       count_launch();
-      k_swap_apply<<<(n - nb + LU_SWAP_TC - 1) / LU_SWAP_TC, 2 * LU_NB, 0, sp>>>(Ar, Ai, ld, n, k0, k1, plan);
+      k_swap_apply<<<(n - nb + LU_SWAP_TC - 1) / LU_SWAP_TC, 2 * nb, 0, sp>>>(Ar, Ai, ld, n, k0, k1, plan);
       count_launch();
     }
     mark(1, false, pk);
     if (k1 < n) {
       mark(2, true, pk);
-      // U12 = L11^-1 A12 as the in-place tensor-core update A12 -= (I - L11^-1) A12: the
-      // inverses of L11's two 128-row blocks, then M = I - L11^-1 (k_l11_m), then the GEMM
+      // U12 = L11^-1 A12, in halves of at most LU_NB rows: each half as the in-place
+      // tensor-core update A12 -= (I - L11^-1) A12 (the inverses of L11's two 128-row
+      // blocks, then M = I - L11^-1 by k_l11_m, then the GEMM); a second half first loses
+      // L(h, first half) times the first half's U rows
       float* inv = c->d_lu_minv;
       float* Mr = inv + 8 * (size_t)LU_TB * LU_TB;
       float* Mi = Mr + (size_t)LU_NB * LU_NB;
-      k_diag_inverse<<<dim3((nb + LU_TB - 1) / LU_TB, 1), 512, trsm_smem, sp>>>(Ar, Ai, ld, k1, k0 / LU_TB, inv);
-      count_launch();
-      k_l11_m<<<nb, LU_TB, 0, sp>>>(Ar, Ai, ld, k0, nb, inv, Mr, Mi);
-      count_launch();
-      rc = tc::tile_operand(Mr, Mi, LU_NB, nb, nb, false, At, sp, gh, amax);
-      if (rc == SIE_OK)
-        rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, n - k1, nb, true, Bt, sp, gh,
-                              amax + 1);
-      if (rc == SIE_OK)
-        rc = tc::gemm_update(At, Bt, nb, Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, nb, n - k1, err, sp,
-                             0, gh, amax);
+      for (int h0 = k0; h0 < k1 && rc == SIE_OK; h0 += LU_NB) {
+        const int hb = std::min(LU_NB, k1 - h0), h1 = h0 + hb;
+        if (h0 > k0) {
+          rc = tc::tile_operand(Ar + (size_t)k0 * ld + h0, Ai + (size_t)k0 * ld + h0, ld, hb, h0 - k0, false, At, sp,
+                                gh, amax);
+          if (rc == SIE_OK)
+            rc = tc::tile_operand(Ar + (size_t)k1 * ld + k0, Ai + (size_t)k1 * ld + k0, ld, n - k1, h0 - k0, true, Bt,
+                                  sp, gh, amax + 1);
+          if (rc == SIE_OK)
+            rc = tc::gemm_update(At, Bt, h0 - k0, Ar + (size_t)k1 * ld + h0, Ai + (size_t)k1 * ld + h0, ld, hb, n - k1,
+                                 err, sp, 0, gh, amax);
+          if (rc != SIE_OK) break;
+        }
+        k_diag_inverse<<<dim3((hb + LU_TB - 1) / LU_TB, 1), 512, trsm_smem, sp>>>(Ar, Ai, ld, h1, h0 / LU_TB, inv);
+        count_launch();
+        k_l11_m<<<hb, LU_TB, 0, sp>>>(Ar, Ai, ld, h0, hb, inv, Mr, Mi);
+        count_launch();
+        rc = tc::tile_operand(Mr, Mi, LU_NB, hb, hb, false, At, sp, gh, amax);
+        if (rc == SIE_OK)
+          rc = tc::tile_operand(Ar + (size_t)k1 * ld + h0, Ai + (size_t)k1 * ld + h0, ld, n - k1, hb, true, Bt, sp, gh,
+                                amax + 1);
+        if (rc == SIE_OK)
+          rc = tc::gemm_update(At, Bt, hb, Ar + (size_t)k1 * ld + h0, Ai + (size_t)k1 * ld + h0, ld, hb, n - k1, err,
+                               sp, 0, gh, amax);
+      }
       mark(2, false, pk);
-      const int m = n - k1, nn = std::min(LU_NB, m);
+      const int m = n - k1, nn = std::min(pnb, m);
       // A22 -= L21 U12 on the tensor cores
       mark(3, true, pk);
       rc = tc::tile_operand(Ar + (size_t)k0 * ld + k1, Ai + (size_t)k0 * ld + k1, ld, m, nb, false, At, sp, gh, amax);
