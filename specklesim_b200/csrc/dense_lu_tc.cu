@@ -605,7 +605,7 @@ __global__ void __launch_bounds__(256) k_swap_plan(const int* ipiv, int k0, int 
 // LU_SWAP_TC columns, a thread per plan entry; all of a tile's reads happen before any
 // of its writes.
 static const int LU_SWAP_TC = 8;
-__global__ void __launch_bounds__(512) k_swap_apply(float* Ar, float* Ai, size_t ld, int n, int k0, int k1,
+__global__ void __launch_bounds__(2 * LU_NBX) k_swap_apply(float* Ar, float* Ai, size_t ld, int n, int k0, int k1,
                                                     const int* plan) {
   const int cnt = plan[0];
   const int i = threadIdx.x;
