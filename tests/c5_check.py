@@ -52,8 +52,11 @@ def singular_flips(Vm, Vp, T, et):
     cm, cp = Vm[T].mean(axis=1), Vp[T].mean(axis=1)
     rm = np.linalg.norm(cm[et[:, 0]] - cm[et[:, 1]], axis=1)
     rp = np.linalg.norm(cp[et[:, 0]] - cp[et[:, 1]], axis=1)
-    moved_t = np.nonzero(np.any(cm != cp, axis=1))[0]
-    moved_e = np.nonzero(rm != rp)[0]
+    moved = np.any(cm != cp, axis=1)
+    moved_t = np.nonzero(moved)[0]
+    # edges whose own triangles moved (possibly together, keeping r_m) or whose r_m changed:
+    # all their pairs are checked below
+    moved_e = np.nonzero((rm != rp) | moved[et[:, 0]] | moved[et[:, 1]])[0]
     flips = 0
     # every edge side against the moved triangles (edges with a changed r_m come next)
     keep = np.ones(len(et), bool)
