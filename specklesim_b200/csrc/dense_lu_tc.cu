@@ -37,8 +37,8 @@ int gemm_update(const char* At, const char* Bt, int K, float* Cr, float* Ci, siz
 size_t tiled_bytes_host(int rows, int K);
 }  // namespace tc
 
-static const int LU_NB = 256;  // default panel width (the tensor-core update's K); L11 blocks of U12
-static const int LU_NBX = 512;  // largest panel width (SIE_LU_NB=512)
+static const int LU_NB = 256;  // the narrower panel width (SIE_LU_NB=256); L11 blocks of U12
+static const int LU_NBX = 512;  // the default panel width (the trailing updates' K)
 static const int LU_SB = 16;   // sub-panel width inside a panel
 static const int LU_TB = 128;  // diagonal blocks of the triangular solves
 static const int LU_FREE_SMS = 12;  // multiprocessors the look-ahead update leaves to the panels
@@ -1056,9 +1056,10 @@ static int lu_tc_factor(sie_ctx* c) {
   // updates all of the panel's later columns on the CUDA cores)
   int pbb = LU_BB;
   if (const char* e = getenv("SIE_LU_BLOCK")) pbb = atoi(e) >= LU_NB ? LU_NB : LU_BB;
-  // panel width: LU_NB, or LU_NBX (SIE_LU_NB=512: trailing updates of K = 512, which read
-  // and write the trailing matrix half as often per flop)
-  int pnb = LU_NB;
+  // panel width: LU_NBX (trailing updates of K = 512, which read and write the trailing
+  // matrix half as often per flop as K = 256: 2.60 s against 2.90 s for the slab10 solve),
+  // or LU_NB with SIE_LU_NB=256
+  int pnb = LU_NBX;
   if (const char* e = getenv("SIE_LU_NB")) pnb = atoi(e) >= LU_NBX ? LU_NBX : LU_NB;
   const char* gp = getenv("SIE_LU_GEMM");
   const bool gh = c->lu_f16_ok && !(gp && std::string(gp) == "tf32");
