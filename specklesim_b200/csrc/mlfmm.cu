@@ -1535,48 +1535,6 @@ __global__ void __launch_bounds__(128) k_interp(const int* __restrict__ ptr, con
   else *o = acc;
 }
 
-// The same with one block per coefficient block: its 8 x Qi inputs are staged in shared
-// memory once, and the block's threads walk the 4 x rows outputs (the stencil taps then
-// read shared memory, not scattered global words).
-template <typename T>
-__global__ void __launch_bounds__(256) k_interp_s(const int* __restrict__ ptr, const int* __restrict__ col,
-                                                  const T* __restrict__ val, int rows,
-                                                  const cx<T>* __restrict__ in, int Qi,
-                                                  cx<T>* __restrict__ out, int Qo, int accum) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cx<T>* xs = reinterpret_cast<cx<T>*>(smraw);  // [8][Qi]
-  const size_t b = blockIdx.x;
-  const cx<T>* src = in + b * 8 * (size_t)Qi;
-  for (int i = threadIdx.x; i < 8 * Qi; i += blockDim.x) xs[i] = src[i];
-  __syncthreads();
-  cx<T>* dst = out + b * 8 * (size_t)Qo;
-  // thread per output row: each stencil tap is read once and applied to the four item
-  // pairs (theta item p and its phi item p + 4)
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    cx<T> acc[4];
-#pragma unroll
-    for (int p = 0; p < 4; p++) acc[p] = mk<T>(0, 0);
-    for (int k = ptr[r]; k < ptr[r + 1]; k++) {
-      const int j = col[k];
-      const T w = val[k];
-      const cx<T>* src = j < Qi ? xs + j : xs + (size_t)4 * Qi + (j - Qi);
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        const cx<T> v = src[(size_t)p * Qi];
-        acc[p].re = fma(w, v.re, acc[p].re);
-        acc[p].im = fma(w, v.im, acc[p].im);
-      }
-    }
-    const int q = r < Qo ? r : r - Qo, i0 = r < Qo ? 0 : 4;
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      cx<T>* o = dst + (size_t)(i0 + p) * Qo + q;
-      if (accum) *o += acc[p];
-      else *o = acc[p];
-    }
-  }
-}
-
 // The same on the tap-major stencil: the block's inputs staged in shared memory, a thread
 // per output row, four taps' (column, weight) pairs loaded together (coalesced across the
 // warp's rows) before their shared-memory reads and multiply-adds; the long rows' remaining
@@ -1665,17 +1623,6 @@ static int interp_run(const InterpDev& I, const cx<T>* in, int Qi, cx<T>* out, s
       k_interp_e<T><<<dim3(nb, 4 / np), 256, sm, st>>>(I.ecol, ievalp<T>(I), I.ew, I.optr, I.ocol, iovalp<T>(I),
                                                        I.rows, in + b0 * 8 * Qi, Qi, out + b0 * 8 * (I.rows / 2),
                                                        I.rows / 2, accum ? 1 : 0, np);
-      sie::count_launch();
-    }
-    SIE_CUDA(cudaGetLastError());
-    return SIE_OK;
-  }
-  if (smem <= (size_t)200 * 1024) {
-    SIE_CUDA(raise_smem(k_interp_s<T>, smem));
-    for (size_t b0 = 0; b0 < nbox; b0 += 2147483647u) {
-      const unsigned nb = (unsigned)std::min<size_t>(2147483647u, nbox - b0);
-      k_interp_s<T><<<nb, 256, smem, st>>>(I.ptr, I.col, ivalp<T>(I), I.rows, in + b0 * 8 * Qi, Qi,
-                                           out + b0 * 8 * (I.rows / 2), I.rows / 2, accum ? 1 : 0);
       sie::count_launch();
     }
     SIE_CUDA(cudaGetLastError());
