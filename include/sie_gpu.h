@@ -220,8 +220,9 @@ int sie_solve_direct_mixed(sie_ctx* ctx, const double* b, double* x, int nrhs, d
  * call returns when the solutions are in d_x. */
 int sie_solve_direct_mixed_device(sie_ctx* ctx, const double* d_b, double* d_x, int nrhs, double tolerance,
                                   int max_refinements, sie_stats* stats, void* stream);
-/* Frees the LU factors that sie_solve_direct and sie_solve_direct_mixed keep, so that the
- * next direct solve factorises again (e.g. after the caller changed nothing but wants the
+/* Frees the LU factors that sie_solve_direct and sie_solve_direct_mixed keep, with their
+ * workspace (tiled operands, the solves' vectors and staging buffers), so that the next
+ * direct solve factorises again (e.g. after the caller changed nothing but wants the
  * memory back).  No counterpart in the reference, which factorises in every run. */
 int sie_release_factors(sie_ctx* ctx);
 /* Marks the kept LU factors out of date and keeps their device memory: the next direct

@@ -1307,14 +1307,20 @@ static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, 
   SIE_TRY(lu_tc_factor(c));
   const int n = 2 * c->M;
   const size_t bytes = (size_t)n * sizeof(zc);
-  zc *bi = nullptr, *xi = nullptr, *ax = nullptr, *r = nullptr;
-  cc* d32 = nullptr;
-  double* nrm = nullptr;
+  // the refinement's vectors: allocated with the first solve and kept with the factors
+  // (a cudaMalloc / cudaFree pair per solve cost up to 0.7 s now and then on a device with
+  // tens of GB allocated)
   int rc = SIE_OK;
-  if (cudaMalloc(&bi, bytes) != cudaSuccess || cudaMalloc(&xi, bytes) != cudaSuccess ||
-      cudaMalloc(&ax, bytes) != cudaSuccess || cudaMalloc(&r, bytes) != cudaSuccess ||
-      cudaMalloc(&d32, (size_t)n * sizeof(cc)) != cudaSuccess || cudaMalloc(&nrm, sizeof(double)) != cudaSuccess)
+  if (!c->d_lu_ref &&
+      cudaMalloc(&c->d_lu_ref, 4 * bytes + (size_t)n * sizeof(cc) + 2 * sizeof(double)) != cudaSuccess) {
+    c->d_lu_ref = nullptr;
+    cudaGetLastError();
     rc = fail(SIE_ERR_NOMEM, "mixed direct solve: device buffers");
+  }
+  zc* bi = (zc*)c->d_lu_ref;
+  zc *xi = bi + n, *ax = bi + 2 * (size_t)n, *r = bi + 3 * (size_t)n;
+  cc* d32 = (cc*)(bi + 4 * (size_t)n);
+  double* nrm = (double*)(d32 + n);
   for (int k = 0; k < nrhs && rc == SIE_OK; k++) {
     auto tk = std::chrono::steady_clock::now();
     const size_t off = (size_t)k * n;
@@ -1393,8 +1399,6 @@ static int solve_direct_mixed_dev(sie_ctx* c, const zc* d_b, zc* d_x, int nrhs, 
     }
     if (rc == SIE_OK && !conv) rc = fail(SIE_ERR_NOCONV, "mixed direct solve: refinement did not reach the tolerance");
   }
-  for (void* p : {(void*)bi, (void*)xi, (void*)ax, (void*)r, (void*)d32, (void*)nrm})
-    if (p) cudaFree(p);
   return rc;
 }
 
@@ -1424,12 +1428,20 @@ extern "C" int sie_solve_direct_mixed(sie_ctx* c, const double* b, double* x, in
   for (size_t i = 0; i < (size_t)4 * c->M * nrhs; i++)
     if (!std::isfinite(b[i])) return fail(SIE_ERR_NONFINITE, "sie_solve_direct_mixed: non-finite right-hand side");
   const size_t bytes = (size_t)2 * c->M * nrhs * sizeof(zc);
-  zc *db = nullptr, *dx = nullptr;
-  SIE_CUDA(cudaMalloc(&db, bytes));
-  if (cudaMalloc(&dx, bytes) != cudaSuccess) {
-    cudaFree(db);
-    return fail(SIE_ERR_NOMEM, "sie_solve_direct_mixed: device buffers");
+  // device copies of b and x, kept with the factors and grown when nrhs grows
+  if (c->lu_io_bytes < 2 * bytes) {
+    if (c->d_lu_io) cudaFree(c->d_lu_io);
+    c->d_lu_io = nullptr;
+    c->lu_io_bytes = 0;
+    if (cudaMalloc(&c->d_lu_io, 2 * bytes) != cudaSuccess) {
+      c->d_lu_io = nullptr;
+      cudaGetLastError();
+      return fail(SIE_ERR_NOMEM, "sie_solve_direct_mixed: device buffers");
+    }
+    c->lu_io_bytes = 2 * bytes;
   }
+  zc* db = (zc*)c->d_lu_io;
+  zc* dx = (zc*)((char*)c->d_lu_io + bytes);
   int rc = SIE_OK;
   if (cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
     rc = fail(SIE_ERR_CUDA, "sie_solve_direct_mixed: copy");
@@ -1438,8 +1450,6 @@ extern "C" int sie_solve_direct_mixed(sie_ctx* c, const double* b, double* x, in
       (cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
        cudaStreamSynchronize(c->stream) != cudaSuccess))
     rc = fail(SIE_ERR_CUDA, "sie_solve_direct_mixed: copy back");
-  cudaFree(db);
-  cudaFree(dx);
   return rc;
 }
 
@@ -1449,7 +1459,7 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   if (c->stream) SIE_CUDA(cudaStreamSynchronize(c->stream));
   for (void* p : {(void*)c->d_lu, (void*)c->d_piv, (void*)c->d_lu32, (void*)c->d_lu32i, (void*)c->d_piv32,
                   (void*)c->d_perm32, (void*)c->d_tmp32, (void*)c->d_lu_at, (void*)c->d_lu_bt, c->d_lu_scr,
-                  (void*)c->d_lu_diag, (void*)c->d_lu_minv, (void*)c->d_lu_at2})
+                  (void*)c->d_lu_diag, (void*)c->d_lu_minv, (void*)c->d_lu_at2, (void*)c->d_lu_ref, c->d_lu_io})
     if (p) cudaFree(p);
   c->d_lu = nullptr;
   c->d_piv = nullptr;
@@ -1461,6 +1471,9 @@ extern "C" int sie_release_factors(sie_ctx* c) {
   c->d_lu_diag = nullptr;
   c->d_lu_minv = nullptr;
   c->d_lu_at2 = nullptr;
+  c->d_lu_ref = nullptr;
+  c->d_lu_io = nullptr;
+  c->lu_io_bytes = 0;
   c->lu_scr_bytes = 0;
   c->lu64_valid = c->lu32_valid = false;
   return SIE_OK;

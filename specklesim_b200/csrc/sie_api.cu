@@ -1701,7 +1701,7 @@ int sie_free(sie_ctx* c) {
                   c->d_xb32, c->d_yb32, c->d_gmb, c->d_qperm, c->d_boxc, c->d_side, c->d_vert,
                   c->d_grad_ws, c->d_tri_verts, c->d_naT, c->d_nbT, c->d_ndT, c->d_lu32, c->d_lu32i, c->d_piv32,
                   c->d_perm32, c->d_tmp32, c->d_lu_at, c->d_lu_bt, c->d_lu_scr,
-                  c->d_lu_diag, c->d_lu_minv, c->d_lu_at2};
+                  c->d_lu_diag, c->d_lu_minv, c->d_lu_at2, c->d_lu_ref, c->d_lu_io};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->d_lvtmp) cudaFree(c->d_lvtmp);

@@ -336,6 +336,9 @@ struct sie_ctx {
   float* d_lu_diag = nullptr;     // the inverses of the factors' diagonal blocks, for the solves
   float* d_lu_minv = nullptr;     // a panel's I - L11^-1 and its blocks' inverses
   char* d_lu_at2 = nullptr;       // the panel's own tensor-core updates: tiled L and U blocks
+  void* d_lu_ref = nullptr;       // the refinement's vectors (b, x, Zx, r, the complex64 step, norms)
+  void* d_lu_io = nullptr;        // device copies of b and x for the host-buffer direct solve
+  size_t lu_io_bytes = 0;
   size_t lu_scr_bytes = 0;
   // the factors above are current (sie_invalidate_factors clears these and keeps the memory,
   // sie_release_factors frees it)
