@@ -31,7 +31,7 @@ extern "C" {
 #define SIE_ERR_STATE 3     /* call order violated (e.g. matvec before setup) */
 #define SIE_ERR_NOMEM 4     /* device or host allocation failed */
 #define SIE_ERR_MESH 5      /* mesh is not a valid triangle surface */
-#define SIE_ERR_NOCONV 6    /* GMRES did not reach the tolerance */
+#define SIE_ERR_NOCONV 6    /* GMRES, or a mixed direct solve's refinement, did not reach the tolerance */
 #define SIE_ERR_TIMEOUT 7   /* host-side time limit reached */
 #define SIE_ERR_NONFINITE 8 /* NaN/Inf met in an input or a result */
 
@@ -205,9 +205,12 @@ int sie_solve_direct(sie_ctx* ctx, const double* b, double* x, int nrhs);
 
 /* Mixed-precision direct solve of the dense system (context set up with dense = 1): LU
  * with partial pivoting of the complex64 matrix whose trailing updates run on the tensor
- * cores as 3xTF32 products (FP32-accurate), then iterative refinement in FP64,
- * x += U^-1 L^-1 P (b - Z x) with the FP64 dense product, until ||b - Z x|| <= tolerance
- * ||b|| or max_refinements corrections.  The factors are made on the first call and kept.
+ * cores as split-FP16 products (each operand block scaled by a power of two and split
+ * into two FP16 parts, three products accumulated in FP32), then iterative refinement in
+ * FP64, x += U^-1 L^-1 P (b - Z x) with the FP64 dense product, until ||b - Z x|| <=
+ * tolerance ||b|| or max_refinements corrections.  If a refinement step fails to halve
+ * the residual, the matrix is factorised again with 3xTF32 updates (FP32-accurate) and the
+ * refinement restarts.  The factors are made on the first call and kept.
  * Same role as sie_solve_direct (ZGESV of the reference's normal solver,
  * src/lib_sie_tri_solver_normal.f90:64-217); the refinement converges while cond(Z)
  * times the FP32 rounding stays below one.  stats (may be NULL): per right-hand side,

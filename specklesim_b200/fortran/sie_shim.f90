@@ -144,6 +144,27 @@ module sie_gpu_c
       integer(c_int), value :: kind
       integer(c_int) :: rc
     end function
+    function sie_solve_direct(ctx, b, x, nrhs) bind(C, name="sie_solve_direct") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, b, x
+      integer(c_int), value :: nrhs
+      integer(c_int) :: rc
+    end function
+    function sie_solve_direct_mixed(ctx, b, x, nrhs, tolerance, &
+        max_refinements, stats) bind(C, name="sie_solve_direct_mixed") result(rc)
+      import :: c_int, c_double, c_ptr, sie_stats
+      type(c_ptr), value :: ctx, b, x
+      integer(c_int), value :: nrhs
+      real(c_double), value :: tolerance
+      integer(c_int), value :: max_refinements
+      type(sie_stats), intent(out) :: stats
+      integer(c_int) :: rc
+    end function
+    function sie_release_factors(ctx) bind(C, name="sie_release_factors") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int) :: rc
+    end function
     function sie_free(ctx) bind(C, name="sie_free") result(rc)
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
@@ -192,6 +213,8 @@ module lib_sie_tri_mlfmm_interface
   ! shape gradient of the far-field intensity
   public :: lib_sie_ml_fmm_adjoint_tri
   public :: lib_sie_ml_fmm_grad_z_tri
+  ! the fill and dense LU solve of the reference's normal solver, on the GPU
+  public :: lib_sie_ml_fmm_solve_direct_tri
   ! the library context, for the GMRES-interface shim (sie_gmres_shim.f90)
   public :: sie_shim_context
 
@@ -204,8 +227,11 @@ contains
     ctx = m_ctx
   end function sie_shim_context
 
-  ! lib_sie_ml_fmm_precalculation_tri (:59-92): mesh, tree, near field, RT, TL, diagonal.
-  subroutine lib_sie_ml_fmm_precalculation_tri()
+  ! The library's settings and mesh from the reference's module globals, as the
+  ! precalculation (:59-92) takes them; dense = 1 asks for the assembled matrix.
+  subroutine shim_open(dense, ctx)
+    integer(c_int), intent(in) :: dense
+    type(c_ptr), intent(inout) :: ctx
     type(sie_config) :: cfg
     real(c_double), allocatable :: verts(:)
     integer(c_int), allocatable :: tris(:)
@@ -231,9 +257,15 @@ contains
     cfg%tree_s_opt = tree_s_opt
     cfg%truncation_number = truncation_number_default
     cfg%normal_convention = calc_p(7)
-    if (c_associated(m_ctx)) call sie_check(sie_free(m_ctx), 'sie_free')
-    call sie_check(sie_init(cfg, verts, nv, tris, nt, m_ctx), 'sie_init')
-    call sie_check(sie_setup(m_ctx), 'sie_setup')
+    cfg%dense = dense
+    if (c_associated(ctx)) call sie_check(sie_free(ctx), 'sie_free')
+    call sie_check(sie_init(cfg, verts, nv, tris, nt, ctx), 'sie_init')
+    call sie_check(sie_setup(ctx), 'sie_setup')
+  end subroutine shim_open
+
+  ! lib_sie_ml_fmm_precalculation_tri (:59-92): mesh, tree, near field, RT, TL, diagonal.
+  subroutine lib_sie_ml_fmm_precalculation_tri()
+    call shim_open(0_c_int, m_ctx)
   end subroutine lib_sie_ml_fmm_precalculation_tri
 
   subroutine run_MLFMM_one_forward_tri()
@@ -323,5 +355,42 @@ contains
                   c_loc(dJdz), J, st)
     if (rc /= SIE_ERR_NOCONV) call sie_check(rc, 'sie_grad')
   end subroutine lib_sie_ml_fmm_grad_z_tri
+
+  ! The impedance fill and solver_LU of lib_sie_tri_solver_normal_I
+  ! (src/lib_sie_tri_solver_normal.f90:87-138, ZGESV at src/lib_sie_math.f90:649-676) on
+  ! the GPU: a dense context from the same module globals, the plane-wave right-hand side
+  ! and the direct solve.  mixed = .false. factorises the FP64 matrix; mixed = .true.
+  ! factorises it in complex64 on the tensor cores and refines in FP64 until
+  ! ||b - Z x|| <= tolerance ||b||.  On return vector_b holds the solution, as VV_EH of
+  ! solver_LU does; the context and its factors are freed.
+  subroutine lib_sie_ml_fmm_solve_direct_tri(vector_b, mixed, tolerance)
+    double complex, dimension(:), allocatable, target, intent(inout) :: vector_b
+    logical, intent(in) :: mixed
+    double precision, intent(in) :: tolerance
+    double complex, dimension(:), allocatable, target :: vector_x
+    type(c_ptr) :: ctx
+    type(sie_stats) :: st
+    integer(c_int) :: rc
+    ctx = c_null_ptr
+    call shim_open(1_c_int, ctx)
+    if (allocated(vector_b)) deallocate(vector_b)
+    allocate(vector_b(2 * m_pairs), vector_x(2 * m_pairs))
+    call sie_check(sie_rhs_planewave(ctx, illumination_p%k_in, illumination_p%E_in, 1_c_int, &
+                                     c_loc(vector_b)), 'sie_rhs_planewave')
+    if (mixed) then
+      rc = sie_solve_direct_mixed(ctx, c_loc(vector_b), c_loc(vector_x), 1_c_int, &
+                                  real(tolerance, c_double), 30_c_int, st)
+      if (rc == SIE_ERR_NOCONV) then
+        print *, 'B200 SIE library: refinement stopped at backward error ', st%backward_error_true
+      else
+        call sie_check(rc, 'sie_solve_direct_mixed')
+      end if
+    else
+      call sie_check(sie_solve_direct(ctx, c_loc(vector_b), c_loc(vector_x), 1_c_int), &
+                     'sie_solve_direct')
+    end if
+    vector_b = vector_x
+    call sie_check(sie_free(ctx), 'sie_free')
+  end subroutine lib_sie_ml_fmm_solve_direct_tri
 
 end module lib_sie_tri_mlfmm_interface

@@ -156,6 +156,27 @@ def test_fortran_gmres_shim_exports_the_reference_procedures():
     assert called and called <= bound, called - bound
 
 
+def test_fortran_shim_defines_its_public_procedures():
+    """Every public procedure of sie_shim.f90's lib_sie_tri_mlfmm_interface is defined in
+    the module, the reference's eight (src/lib_sie_tri_mlfmm_interface.f90:18-26) among
+    them, and every library function the module calls is bound in the interface block
+    (the direct solve's included)."""
+    shim = open(os.path.join(ROOT, "specklesim_b200", "fortran", "sie_shim.f90")).read()
+    body = shim[shim.index("module lib_sie_tri_mlfmm_interface"):]
+    public = set(re.findall(r"public :: (\w+)", body))
+    assert {"lib_sie_ml_fmm_calculate_vector_b_tri", "lib_sie_ml_fmm_get_vector_b_tri",
+            "lib_sie_ml_fmm_get_init_vector_x_tri", "lib_sie_ml_fmm_precalculation_tri",
+            "lib_sie_ml_fmm_run_tri", "lib_sie_ml_fmm_save_vector_x_tri",
+            "run_MLFMM_one_forward_tri", "lib_sie_ml_fmm_preconditioner_left",
+            "lib_sie_ml_fmm_solve_direct_tri"} <= public
+    for name in public:
+        assert re.search(r"(subroutine|function) " + name + r"\(", body), name
+    bound = set(re.findall(r"bind\(C, name=\"(\w+)\"\)", shim))
+    called = set(re.findall(r"\b(sie_\w+)\(", body)) - {"sie_check", "sie_shim_context"}
+    assert {"sie_solve_direct", "sie_solve_direct_mixed"} <= called
+    assert called <= bound, called - bound
+
+
 def test_ctypes_structs_match_the_header():
     """The ctypes mirrors in specklesim_b200/_lib.py have the header structs' fields in
     order with matching types (Python's reserved 'lambda' is spelled 'lambda_')."""
