@@ -1,6 +1,7 @@
 // Mixed-precision direct solve of the dense system: LU with partial pivoting of the
-// complex64 matrix, its O(N^3) trailing updates on the tensor cores (tc_gemm.cu, 3xTF32,
-// FP32-accurate), then iterative refinement in FP64 against the FP64 dense product.
+// complex64 matrix, its O(N^3) trailing updates on the tensor cores (tc_gemm.cu: split-FP16
+// products with power-of-two operand scaling, or 3xTF32), then iterative refinement in
+// FP64 against the FP64 dense product.
 //
 // The reference's direct path (lib_sie_tri_solver_normal_I,
 // src/lib_sie_tri_solver_normal.f90:64-217, with ZGESV in solver_LU,
@@ -10,15 +11,17 @@
 // tolerance, which it does while cond(Z) times the factorisation's rounding stays below
 // one.
 //
-// Blocked right-looking LU, panel width NB = 256, on the matrix stored as two FP32
-// planes (real, imaginary), column-major, internal unknown order:
-//   1. panel, in sub-panels of 16 columns: each sub-panel is one cooperative launch that,
-//      column by column, agrees on the pivot, swaps rows across the panel, scales the
-//      column and updates the sub-panel (two bounded grid barriers per column); then the
-//      sub-panel's U rows (L11^-1) and one rank-16 update of the panel's later columns;
+// Blocked right-looking LU, panel width 512 (256 with SIE_LU_NB=256), on the matrix
+// stored as two FP32 planes (real, imaginary), column-major, internal unknown order:
+//   1. panel, in 64-column blocks of 8-column sub-panels: each sub-panel is one
+//      cooperative launch that, column by column, agrees on the pivot (one bounded grid
+//      barrier per column), moves the pivot row, scales the column and updates the
+//      sub-panel; then its row swaps for the panel's other columns, its U
+//      rows and a rank-8 update of its block's later columns; after each block, its U
+//      rows of the panel's later columns and one tensor-core update of those columns;
 //   2. the panel's row swaps applied to every column left and right of it;
-//   3. U12 = L11^-1 A12 by 128-row diagonal blocks: a warp per column with the block in
-//      shared memory, the rows below it updated on the tensor cores;
+//   3. U12 = L11^-1 A12 in 256-row halves, each an in-place tensor-core update with
+//      M = I - L11^-1 of the half's diagonal block;
 //   4. A22 -= L21 U12 on the tensor cores: first the next panel's columns, then, on a
 //      second (low-priority) stream, the rest, which runs beside the next panel (look-ahead).
 #include <chrono>
@@ -39,9 +42,16 @@ size_t tiled_bytes_host(int rows, int K);
 
 static const int LU_NB = 256;  // the narrower panel width (SIE_LU_NB=256); L11 blocks of U12
 static const int LU_NBX = 512;  // the default panel width (the trailing updates' K)
-static const int LU_SB = 16;   // sub-panel width inside a panel
+// sub-panel width inside a panel: each column step of the panel kernel streams the
+// sub-panel's remaining columns through L2, so narrower sub-panels move fewer bytes per
+// column (slab10 factorisation 2.23 s with 8 against 2.35 s with 16)
+static const int LU_SB = 8;
 static const int LU_TB = 128;  // diagonal blocks of the triangular solves
-static const int LU_FREE_SMS = 12;  // multiprocessors the look-ahead update leaves to the panels
+// multiprocessors the look-ahead update leaves to the panels: the panel chain is the
+// factorisation's critical path, and its sub-panel kernel, which streams the sub-panel
+// through L2 once per column, speeds up with more of them (slab10: 2.37-2.40 s with 24
+// against 2.43-2.45 s with 12, 2.41-2.42 s with 36)
+static const int LU_FREE_SMS = 24;
 static const int PANEL_MAX_BLOCKS = 256;  // largest grid of the cooperative panel kernel
 
 // Dense panels (cfg.dense = 1) -> FP32 planes of Z in the internal interleaved order
@@ -330,6 +340,35 @@ __global__ void __launch_bounds__(256, 4) k_subpanel(float* Ar, float* Ai, size_
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && __ldcg(bad) != 0) atomicOr(err, 16);  // a barrier gave up
+}
+
+
+__device__ __forceinline__ void ll_put(unsigned long long* p, unsigned tag, unsigned bits) {
+  const unsigned long long w = ((unsigned long long)tag << 32) | bits;
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+__device__ __forceinline__ unsigned long long ll_ld(const unsigned long long* p) {
+  unsigned long long w;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+  return w;
+}
+// The payload of *p once it carries tag (w: a first load of it).  Bounded: after about
+// two million reloads without the tag, or once another thread gave up, it sets *bad and
+// returns whatever it holds; the host reports the error.
+__device__ __forceinline__ unsigned ll_wait(const unsigned long long* p, unsigned long long w, unsigned tag,
+                                            unsigned* bad) {
+  long long it = 0;
+  while ((unsigned)(w >> 32) != tag) {
+    if ((++it & 63) == 0) {
+      if (*(volatile unsigned*)bad != 0) break;
+      if (it > (1LL << 21)) {
+        atomicExch(bad, 1u);
+        break;
+      }
+    }
+    w = ll_ld(p);
+  }
+  return (unsigned)w;
 }
 
 // After the sub-panel [s0, s1) of the panel [k0, k1): its row interchanges applied, in
@@ -1052,15 +1091,16 @@ static int lu_tc_factor(sie_ctx* c) {
   const bool lookahead = !(la && atoi(la) == 0);
   // trailing updates in split-FP16 unless this context's refinement needed 3xTF32 before
   // (or SIE_LU_GEMM=tf32 asks for it)
-  // the panel's block width: LU_BB, or the whole panel (SIE_LU_BLOCK=256: every sub-panel
-  // updates all of the panel's later columns on the CUDA cores)
-  int pbb = LU_BB;
-  if (const char* e = getenv("SIE_LU_BLOCK")) pbb = atoi(e) >= LU_NB ? LU_NB : LU_BB;
   // panel width: LU_NBX (trailing updates of K = 512, which read and write the trailing
   // matrix half as often per flop as K = 256: 2.60 s against 2.90 s for the slab10 solve),
   // or LU_NB with SIE_LU_NB=256
   int pnb = LU_NBX;
   if (const char* e = getenv("SIE_LU_NB")) pnb = atoi(e) >= LU_NBX ? LU_NBX : LU_NB;
+  // the panel's block width: LU_BB, or with 256-column panels the whole panel
+  // (SIE_LU_BLOCK=256: every sub-panel updates all of the panel's later columns on the CUDA
+  // cores; k_sub_update holds at most LU_NB columns of U, so 512-column panels keep LU_BB)
+  int pbb = LU_BB;
+  if (const char* e = getenv("SIE_LU_BLOCK")) pbb = atoi(e) >= LU_NB && pnb <= LU_NB ? pnb : LU_BB;
   const char* gp = getenv("SIE_LU_GEMM");
   const bool gh = c->lu_f16_ok && !(gp && std::string(gp) == "tf32");
   c->tm.lu_f16 = gh ? 1 : 0;
@@ -1079,9 +1119,7 @@ static int lu_tc_factor(sie_ctx* c) {
   for (int k0 = 0; k0 < n && rc == SIE_OK; k0 += pnb) {
     const int nb = std::min(pnb, n - k0), k1 = k0 + nb;
     mark(0, true, pk);
-    // the panel in sub-panels of LU_SB columns: column steps inside the sub-panel, then
-    // one rank-LU_SB update of the panel's later columns
-    // the panel in 64-column blocks of 16-column sub-panels: inside a block, each
+    // the panel in 64-column blocks of LU_SB-column sub-panels: inside a block, each
     // sub-panel updates the block's later columns (CUDA cores); after a block, its U rows
     // of the panel's remaining columns and one tensor-core update of those columns
     for (int s0 = k0; s0 < k1; s0 += LU_SB) {
@@ -1102,12 +1140,20 @@ static int lu_tc_factor(sie_ctx* c) {
       k_sub_finish<<<(k1 - k0 + LU_FIN_T - 1) / LU_FIN_T, LU_FIN_T, 0, sp>>>(Ar, Ai, ld, k0, s0, s1, k1, b1, ipiv);
       count_launch();
       if (s1 < b1 && s1 < n) {
+        if (b1 - s1 > LU_NB) {  // k_sub_update holds LU_NB columns of U in shared memory
+          rc = fail(SIE_ERR_ARG, "mixed LU: block wider than the sub-panel update's tile");
+          break;
+        }
         k_sub_update<<<dim3((n - s1 + 255) / 256, (b1 - s1 + LU_UPD_SLICE - 1) / LU_UPD_SLICE), 256, 0, sp>>>(
             Ar, Ai, ld, n, s0, s1, b1);
         count_launch();
       }
       if (s1 == b1 && b1 < k1 && rc == SIE_OK) {
         const int w = b1 - b0;
+        if (w > LU_BB) {  // k_blk_trsm holds LU_BB columns of L in shared memory
+          rc = fail(SIE_ERR_ARG, "mixed LU: block wider than the triangular solve's tile");
+          break;
+        }
         k_blk_trsm<<<(k1 - b1 + LU_BB - 1) / LU_BB, LU_BB, blk_smem, sp>>>(Ar, Ai, ld, b0, b1, b1, k1);
         count_launch();
         rc = tc::tile_operand(Ar + (size_t)b0 * ld + b1, Ai + (size_t)b0 * ld + b1, ld, n - b1, w, false, At2, sp, gh,

@@ -1,6 +1,7 @@
 """Mixed-precision direct solve (sie_solve_direct_mixed: complex64 LU whose trailing
-updates run on the tensor cores as 3xTF32 products, FP64 iterative refinement) against the
-FP64 direct solve and the oracle's dense matrix (needs a B200).
+updates run on the tensor cores as split-FP16 products, 3xTF32 as the fallback, then FP64
+iterative refinement) against the FP64 direct solve and the oracle's dense matrix (needs a
+B200).
 
 The reference's direct path is the dense fill plus ZGESV (lib_sie_tri_solver_normal_I,
 src/lib_sie_tri_solver_normal.f90:64-217; solver_LU, src/lib_sie_math.f90:649-676)."""
@@ -81,3 +82,30 @@ def test_mixed_direct_solve_with_tf32_updates(gpu_lib, monkeypatch):
     assert _rel(x_tf, x_bf) < 1e-10
     g.close()
 
+
+
+@pytest.mark.parametrize("env", [
+    {"SIE_LU_LOOKAHEAD": "0"},                              # 256 blocks, every multiprocessor
+    {"SIE_LU_PANEL_BLOCKS": "1"},                           # a single block
+    {"SIE_LU_PANEL_BLOCKS": "3", "SIE_LU_NB": "256", "SIE_LU_BLOCK": "256"},  # 3 blocks, whole-panel blocks
+], ids=["all_sms", "one_block", "three_blocks"])
+def test_panel_grids_agree(gpu_lib, monkeypatch, env):
+    """The cooperative panel kernel with 256 blocks (no look-ahead), with 1 block and with
+    3 blocks (256-column panels as one block each) factorises the same matrix to solutions
+    that agree with the FP64 solve, in the same number of refinement steps (within one) as
+    the default grid."""
+    from specklesim_b200 import Sie, incidence
+    V, T = P.slab(cells=10, length_wl=2.0, seed=3)
+    g = Sie(V, T, P.WL, P.EPS_METAL, dense=True).setup()
+    b = g.rhs_planewave(*incidence(0.3, 0.2, "TM", 2))
+    x64 = g.solve_direct(b)
+    x0, st0 = g.solve_direct_mixed(b, tolerance=1e-12, max_refinements=30)
+    for key, val in env.items():
+        monkeypatch.setenv(key, val)
+    g.invalidate_factors()
+    x1, st1 = g.solve_direct_mixed(b, tolerance=1e-12, max_refinements=30)
+    assert st0["converged"] and st1["converged"]
+    assert _rel(x0, x64) < 1e-9 and _rel(x1, x64) < 1e-9
+    assert abs(st1["iterations"] - st0["iterations"]) <= 1
+    assert g.timings()["lu_factorizations"] == 1
+    g.close()
