@@ -263,6 +263,18 @@ int sie_precondition_right(sie_ctx* ctx, const double* v1, double* v2);
 int sie_farfield(sie_ctx* ctx, const double* x, const double* pts, int npts, double* E,
                  double* H, double* intensity);
 
+/* E and H at npts points inside the body, Integration_scattered_field_tri_within_medium
+ * (src/lib_sie_tri_calculation_mod.f90:2829-2877): the field that the negated currents
+ * radiate into the medium of relative permittivity eps_r (the reference passes the
+ * evaluation point's medium, eps_r2 inside the body) with the wavenumber k0 sqrt(eps_r),
+ * mu_0 and eps_0 eps_r, the scalar-potential term of E included, on the 3-point rule of
+ * sie_farfield.  x: the 2M currents in sie_farfield's layout; E, H: npts x 3 complex
+ * (either may be NULL).  It is the total field there; the caller (the reference's
+ * lib_sie_tri_observation_field_calculation, src/lib_sie_tri_solver_normal.f90:385-407)
+ * adds no incident field to it. */
+int sie_field_interior(sie_ctx* ctx, const double* x, const double* pts, int npts, double eps_r_re,
+                       double eps_r_im, double* E, double* H);
+
 /* Introspection for parity tests. */
 int sie_get_edges(const sie_ctx* ctx, int* elem, int* corner);
 int sie_get_tree(const sie_ctx* ctx, double* D_xmin, long long* leaf_box);

@@ -75,6 +75,9 @@ def lib():
             "orc_matvec": (None, [vp, dp, dp, C.c_int]),
             "orc_rhs": (None, [vp, dp, dp, dp]),
             "orc_field": (None, [vp, dp, dp, C.c_int, dp, dp]),
+            "orc_field_interior": (None, [vp, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp]),
+            "orc_field_medium": (None, [vp, dp, dp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, dp, dp]),
             "orc_hankel2": (None, [C.c_double, C.c_double, C.c_int, dp]),
             "orc_gauss_legendre": (None, [C.c_int, dp, dp]),
             "orc_lagrange_interp": (None, [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]),
@@ -238,6 +241,31 @@ class Oracle:
                         _d(H.view(np.float64)))
         I = np.sum(np.abs(E) ** 2, axis=1) * 4 * np.pi * np.sum(p * p, axis=1)
         return E, H, I
+
+    def field_interior(self, x, pts, eps_r):
+        """E, H at points inside the body (Integration_scattered_field_tri_within_medium,
+        src/lib_sie_tri_calculation_mod.f90:2829-2877) in the medium of relative
+        permittivity eps_r."""
+        x = np.ascontiguousarray(x, np.complex128)
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        E = np.zeros((p.shape[0], 3), np.complex128)
+        H = np.zeros((p.shape[0], 3), np.complex128)
+        er = complex(eps_r)
+        lib().orc_field_interior(self.h, _d(x.view(np.float64)), _d(p), p.shape[0], er.real, er.imag,
+                                 _d(E.view(np.float64)), _d(H.view(np.float64)))
+        return E, H
+
+    def field_medium(self, x, pts, k, my, eps):
+        """The exterior routine (Integration_scattered_field_tri) with the medium's
+        wavenumber k, permeability my and permittivity eps replaced."""
+        x = np.ascontiguousarray(x, np.complex128)
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        E = np.zeros((p.shape[0], 3), np.complex128)
+        H = np.zeros((p.shape[0], 3), np.complex128)
+        k, eps = complex(k), complex(eps)
+        lib().orc_field_medium(self.h, _d(x.view(np.float64)), _d(p), p.shape[0], k.real, k.imag, float(my),
+                               eps.real, eps.imag, _d(E.view(np.float64)), _d(H.view(np.float64)))
+        return E, H
 
     def hanninen(self, m, tt, n, ll, ia, q):
         out = np.zeros(13)

@@ -1465,10 +1465,67 @@ static void rhs_planewave(const Ctx& C, const double* kin, const double* Ein, cd
   }
 }
 
-// Integration_scattered_field_tri :2782-2825 (E and H at observation points)
+// Integration_scattered_field_tri :2782-2825 (E and H at observation points), in the
+// medium mt (the context's background medium, or another one for the decomposition check
+// of the interior field below)
+static void scattered_field_in(const Ctx& C, const Material& mt, const cd* x, const double* pts, int npts, cd* E,
+                               cd* H);
 static void scattered_field(const Ctx& C, const cd* x, const double* pts, int npts, cd* E, cd* H) {
+  scattered_field_in(C, C.mt, x, pts, npts, E, H);
+}
+
+// Integration_scattered_field_tri_within_medium :2829-2877: E and H at points inside the
+// body, radiated into the medium of relative permittivity eps_r (km = k0 sqrt(eps_r),
+// eps_2 = eps_0 eps_r, mu_0) by the negated equivalent currents (SE = -SEH(m), SH =
+// -SEH(m + M)), with the scalar-potential term of E kept (the exterior routine multiplies
+// it by zero).  The same 3-point rule as the exterior routine.
+static void scattered_field_interior(const Ctx& C, const cd* x, const double* pts, int npts, cd eps_r, cd* E,
+                                     cd* H) {
   int M = (int)C.ms.edge_mid.size();
   const Material& mt = C.mt;
+  const cd eps2 = EPS0 * eps_r, km = mt.k0 * std::sqrt(eps_r);
+  Rule R = make_rule(3);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int p = 0; p < npts; p++) {
+    V3 ra = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
+    C3 Es = c3zero(), Hs = c3zero();
+    for (int m = 0; m < M; m++) {
+      const cd SE = -x[m], SH = -x[m + M];
+      for (int t = 0; t < 2; t++) {
+        const Fn& f = C.ms.fn[2 * m + t];
+        double dfm = f.sign * f.length;
+        for (int i = 0; i < R.n; i++) {
+          V3 rq = simplex(R.a[i], R.b[i], f.c);
+          V3 fm = (rq - f.c[2]) * 0.5 * dfm;
+          V3 d = ra - rq;
+          double Rn = vlen(d);
+          cd G, DG;
+          green(km, Rn, G, DG);
+          C3 gG = (d / Rn) * DG;
+          C3 Hf = fm * SH;
+          C3 cHg{Hf.y * gG.z - Hf.z * gG.y, Hf.z * gG.x - Hf.x * gG.z, Hf.x * gG.y - Hf.y * gG.x};
+          C3 fg{fm.y * gG.z - fm.z * gG.y, fm.z * gG.x - fm.x * gG.z, fm.x * gG.y - fm.y * gG.x};
+          cd a1 = IM * mt.omega * MU0 * SE * G;
+          cd a4 = 1.0 / (IM * mt.omega * eps2) * SE * dfm;
+          C3 Ke{a1 * fm.x - cHg.x - a4 * gG.x, a1 * fm.y - cHg.y - a4 * gG.y, a1 * fm.z - cHg.z - a4 * gG.z};
+          double w = R.w[i];
+          Es = Es + Ke * cd(-w);
+          cd a2 = IM * mt.omega * eps2 * SH * G;
+          cd a3 = 1.0 / (IM * mt.omega * MU0) * SH * dfm;
+          C3 Kh{a2 * fm.x - a3 * gG.x + SE * fg.x, a2 * fm.y - a3 * gG.y + SE * fg.y,
+                a2 * fm.z - a3 * gG.z + SE * fg.z};
+          Hs = Hs + Kh * cd(-w);
+        }
+      }
+    }
+    E[3 * p] = Es.x; E[3 * p + 1] = Es.y; E[3 * p + 2] = Es.z;
+    H[3 * p] = Hs.x; H[3 * p + 1] = Hs.y; H[3 * p + 2] = Hs.z;
+  }
+}
+
+static void scattered_field_in(const Ctx& C, const Material& mt, const cd* x, const double* pts, int npts, cd* E,
+                               cd* H) {
+  int M = (int)C.ms.edge_mid.size();
   Rule R = make_rule(3);
 #pragma omp parallel for schedule(dynamic, 4)
   for (int p = 0; p < npts; p++) {
@@ -1725,6 +1782,20 @@ void orc_rhs(void* h, const double* kin, const double* Ein, double* b) {
 
 void orc_field(void* h, const double* x, const double* pts, int npts, double* E, double* H) {
   scattered_field(*(Ctx*)h, (const cd*)x, pts, npts, (cd*)E, (cd*)H);
+}
+void orc_field_interior(void* h, const double* x, const double* pts, int npts, double er_re, double er_im, double* E,
+                        double* H) {
+  scattered_field_interior(*(Ctx*)h, (const cd*)x, pts, npts, cd(er_re, er_im), (cd*)E, (cd*)H);
+}
+// the exterior routine in a medium given by its wavenumber, permeability and permittivity
+void orc_field_medium(void* h, const double* x, const double* pts, int npts, double k_re, double k_im, double my,
+                      double eps_re, double eps_im, double* E, double* H) {
+  const Ctx& C = *(Ctx*)h;
+  Material mt = C.mt;
+  mt.k1 = cd(k_re, k_im);
+  mt.my1 = my;
+  mt.eps1 = cd(eps_re, eps_im);
+  scattered_field_in(C, mt, (const cd*)x, pts, npts, (cd*)E, (cd*)H);
 }
 
 // special functions exposed for the pins

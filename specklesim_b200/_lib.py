@@ -81,6 +81,7 @@ EXPORTS = [
     "sie_grad", "sie_set_inner_operator", "sie_autotune", "sie_quadrature_rule",
     "sie_set_preconditioner", "sie_precondition_right", "sie_set_level_truncation",
     "sie_solve_direct_mixed", "sie_solve_direct_mixed_device", "sie_release_factors", "sie_invalidate_factors",
+    "sie_field_interior",
 ]
 
 _lib = None
@@ -119,6 +120,7 @@ def load(path=None):
         "sie_set_level_truncation": (C.c_int, [vp, ip, C.c_int]),
         "sie_precondition_right": (C.c_int, [vp, dp, dp]),
         "sie_farfield": (C.c_int, [vp, dp, dp, C.c_int, dp, dp, dp]),
+        "sie_field_interior": (C.c_int, [vp, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp]),
         "sie_get_edges": (C.c_int, [vp, ip, ip]),
         "sie_get_tree": (C.c_int, [vp, dp, lp]),
         "sie_get_blocks": (C.c_int, [vp, ip, ip, C.c_int, dp]),

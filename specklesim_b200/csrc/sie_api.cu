@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <map>
 #include <string>
@@ -1551,6 +1552,84 @@ int sie_farfield(sie_ctx* c, const double* x, const double* pts, int npts, doubl
     if (intensity) cudaMemcpy(intensity, dI, (size_t)npts * sizeof(double), cudaMemcpyDeviceToHost);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) r = cuda_fail(e, "sie_farfield copies");
+  }
+  cudaFree(dx);
+  cudaFree(dp);
+  cudaFree(dE);
+  cudaFree(dH);
+  cudaFree(dI);
+  return r;
+}
+
+// Integration_scattered_field_tri_within_medium (:2829-2877) as two passes of the
+// exterior field kernel in the interior medium (km = k0 sqrt(eps_r), mu_0,
+// eps_2 = eps_0 eps_r): the negated currents give H and E without its scalar-potential
+// term; the currents (J, M) = (0, -J / eps_2) with permeability 1 and permittivity 0 give,
+// as their H, that term, -(1/(i w eps_2)) SE dfm grad G summed and negated like the rest.
+int sie_field_interior(sie_ctx* c, const double* x, const double* pts, int npts, double eps_r_re, double eps_r_im,
+                       double* E, double* H) {
+  if (!c || !x || !pts || npts < 1) return fail(SIE_ERR_ARG, "sie_field_interior: bad argument");
+  if (!std::isfinite(eps_r_re) || !std::isfinite(eps_r_im) || (eps_r_re == 0.0 && eps_r_im == 0.0))
+    return fail(SIE_ERR_ARG, "sie_field_interior: eps_r must be finite and non-zero");
+  SIE_CUDA(cudaSetDevice(c->device));
+  if (!c->setup_done) return fail(SIE_ERR_STATE, "sie_field_interior: sie_setup not called");
+  SIE_TRY(ensure_work(c, 1));
+  const int M = c->M;
+  const std::complex<double> km = c->mt.k0 * std::sqrt(std::complex<double>(eps_r_re, eps_r_im));
+  const zc eps2 = mk<double>(eps_r_re, eps_r_im) * EPS0;
+  Material m1 = c->mt;
+  m1.k1 = mk<double>(km.real(), km.imag());
+  m1.my1 = MU0;
+  m1.eps1 = eps2;
+  Material m2 = m1;
+  m2.my1 = 1.0;
+  m2.eps1 = mk<double>(0, 0);
+  const zc* xz = reinterpret_cast<const zc*>(x);
+  std::vector<zc> xab((size_t)4 * M);  // the two passes' currents, external order
+  for (int m = 0; m < M; m++) {
+    xab[m] = -xz[m];
+    xab[(size_t)M + m] = -xz[(size_t)M + m];
+    xab[(size_t)2 * M + m] = mk<double>(0, 0);
+    xab[(size_t)3 * M + m] = -(xz[m] / eps2);
+  }
+  const size_t vb = (size_t)2 * M * sizeof(zc), fb = 3 * (size_t)npts * sizeof(zc);
+  zc *dx = nullptr, *dE = nullptr, *dH = nullptr;
+  double *dp = nullptr, *dI = nullptr;
+  int r = SIE_OK;
+  if (cudaMalloc(&dx, 2 * vb) != cudaSuccess || cudaMalloc(&dp, 3 * (size_t)npts * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&dE, 2 * fb) != cudaSuccess || cudaMalloc(&dH, 2 * fb) != cudaSuccess ||
+      cudaMalloc(&dI, (size_t)npts * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    r = fail(SIE_ERR_NOMEM, "sie_field_interior: device memory");
+  }
+  if (r == SIE_OK && (h2d(dx, xab.data(), 2 * vb) != cudaSuccess ||
+                      h2d(dp, pts, 3 * (size_t)npts * sizeof(double)) != cudaSuccess))
+    r = fail(SIE_ERR_CUDA, "sie_field_interior: copies");
+  // pass 1 into (dE, dH), pass 2 into the second halves; the gathers and kernels share
+  // the context's stream, so pass 2's gather waits for pass 1's kernel
+  if (r == SIE_OK) r = gather_ext_to_int(c, dx, c->d_xi, 1, c->stream);
+  if (r == SIE_OK) r = farfield_dev(c, m1, c->d_xi, dp, npts, dE, dH, dI);
+  if (r == SIE_OK) r = gather_ext_to_int(c, dx + 2 * (size_t)M, c->d_xi, 1, c->stream);
+  if (r == SIE_OK) r = farfield_dev(c, m2, c->d_xi, dp, npts, dE + 3 * (size_t)npts, dH + 3 * (size_t)npts, dI);
+  if (r == SIE_OK) {
+    std::vector<zc> hE(6 * (size_t)npts), hH(6 * (size_t)npts);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+        cudaMemcpy(hE.data(), dE, 2 * fb, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hH.data(), dH, 2 * fb, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      r = cuda_fail(cudaGetLastError(), "sie_field_interior");
+    } else {
+      for (size_t i = 0; i < 3 * (size_t)npts; i++) {
+        const zc e = hE[i] + hH[3 * (size_t)npts + i];
+        if (E) {
+          E[2 * i] = e.re;
+          E[2 * i + 1] = e.im;
+        }
+        if (H) {
+          H[2 * i] = hH[i].re;
+          H[2 * i + 1] = hH[i].im;
+        }
+      }
+    }
   }
   cudaFree(dx);
   cudaFree(dp);

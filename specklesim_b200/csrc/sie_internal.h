@@ -429,6 +429,9 @@ int jacobi_apply(sie_ctx* c, const zc* v1, zc* v2, cudaStream_t st);
 int rhs_planewave_dev(sie_ctx* c, const double* d_k, const double* d_E, int nrhs, zc* d_b_int);
 int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
                  double* d_I);
+// the same in the medium mt (wavenumber k1, permeability my1, permittivity eps1)
+int farfield_dev(sie_ctx* c, const Material& mt, const zc* d_x_int, const double* d_pts, int npts, zc* d_E,
+                 zc* d_H, double* d_I);
 int gmres_solve(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
 int fgmres_mixed(sie_ctx* c, const zc* d_b, zc* d_x, const sie_solver_cfg* cfg, sie_stats* st);
 // Z^H y = g in place (dense contexts, LU factors made on first use)

@@ -235,11 +235,15 @@ __global__ void k_field(const FnD* fn, const zc* x, int M, Material mt, const do
   }
 }
 
-int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
-                 double* d_I) {
-  k_field<<<npts, 256, 0, c->stream>>>(c->d_fn, d_x_int, c->M, c->mt, d_pts, npts, d_E, d_H, d_I); sie::count_launch();
+int farfield_dev(sie_ctx* c, const Material& mt, const zc* d_x_int, const double* d_pts, int npts, zc* d_E,
+                 zc* d_H, double* d_I) {
+  k_field<<<npts, 256, 0, c->stream>>>(c->d_fn, d_x_int, c->M, mt, d_pts, npts, d_E, d_H, d_I); sie::count_launch();
   SIE_CUDA(cudaGetLastError());
   return SIE_OK;
+}
+int farfield_dev(sie_ctx* c, const zc* d_x_int, const double* d_pts, int npts, zc* d_E, zc* d_H,
+                 double* d_I) {
+  return farfield_dev(c, c->mt, d_x_int, d_pts, npts, d_E, d_H, d_I);
 }
 
 __global__ void k_z2c(const zc* a, cc* b, size_t n) {

@@ -243,6 +243,61 @@ class Sie:
                                      dptr(E.view(np.float64)), dptr(H.view(np.float64)), dptr(I)))
         return E, H, I
 
+    def field_interior(self, x, pts, eps_r=None):
+        """E, H at points inside the body (Integration_scattered_field_tri_within_medium,
+        src/lib_sie_tri_calculation_mod.f90:2829-2877): the total field there, in the
+        medium of relative permittivity eps_r (the body's, eps_r2, by default)."""
+        x = _lib.as_c128(x)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        npts = p.shape[0]
+        er = complex(self.cfg.eps_r2_re, self.cfg.eps_r2_im) if eps_r is None else complex(eps_r)
+        E = np.zeros((npts, 3), np.complex128)
+        H = np.zeros((npts, 3), np.complex128)
+        check(self._lib.sie_field_interior(self._h, dptr(x.view(np.float64)), dptr(p), npts, er.real, er.imag,
+                                           dptr(E.view(np.float64)), dptr(H.view(np.float64))))
+        return E, H
+
+    def near_field(self, x, pts, inside, k_in=None, E_in=None):
+        """E, H of a near-field map, as the plane-wave branch of
+        lib_sie_tri_observation_field_calculation (src/lib_sie_tri_solver_normal.f90:
+        385-420): points with inside[i] true get the interior field (eps_r2), with a
+        component of E below 1e-20 in modulus set to zero together with the same
+        component of H, as the reference does; the others get the scattered field plus,
+        when k_in and E_in are given (the reference's total_field), the incident plane
+        wave of lib_sie_tri_input_field_calculation (src/lib_sie_tri_calculation_mod.f90:
+        2604-2609): E_in exp(-i k1 k_in . r), H = k1 k_in x E / (mu_1 omega).  Every point
+        uses the 3-point rule; the reference raises it near the surface
+        (ngp_near_field_distance_tri)."""
+        x = _lib.as_c128(x)
+        p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        inside = np.asarray(inside, dtype=bool).reshape(-1)
+        if inside.size != p.shape[0]:
+            raise ValueError("near_field: inside must have one entry per point")
+        E = np.zeros((p.shape[0], 3), np.complex128)
+        H = np.zeros((p.shape[0], 3), np.complex128)
+        if inside.any():
+            Ei, Hi = self.field_interior(x, p[inside])
+            small = np.abs(Ei) < 1e-20
+            Ei[small] = 0
+            Hi[small] = 0
+            E[inside], H[inside] = Ei, Hi
+        out = ~inside
+        if out.any():
+            Es, Hs, _ = self.farfield(x, p[out])
+            if k_in is not None:
+                mu0 = float(np.float32(1.2566370614e-6))
+                c0 = float(np.float32(2.99792458e8))
+                lam = float(self.cfg.lambda_)
+                k1 = 2 * np.pi / lam * np.sqrt(complex(self.cfg.eps_r1_re, self.cfg.eps_r1_im))
+                omega = 2 * np.pi * c0 / lam
+                kv = np.asarray(k_in, dtype=np.float64).reshape(3)
+                Einc = np.asarray(E_in, dtype=np.complex128).reshape(1, 3) * np.exp(-1j * k1 * (p[out] @ kv))[:, None]
+                Hinc = np.cross(k1 * kv[None, :], Einc) / (mu0 * omega)
+                Es = Es + Einc
+                Hs = Hs + Hinc
+            E[out], H[out] = Es, Hs
+        return E, H
+
     def farfield_device_noalloc(self, d_x, d_pts, npts, d_E, d_H, d_I, stream=0):
         """Far field on device buffers (raw addresses) with no device allocation; the
         work is queued on `stream` and not waited for."""
