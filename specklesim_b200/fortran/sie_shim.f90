@@ -165,6 +165,22 @@ module sie_gpu_c
       type(c_ptr), value :: ctx
       integer(c_int) :: rc
     end function
+    function sie_farfield(ctx, x, pts, npts, E, H, intensity) bind(C, name="sie_farfield") result(rc)
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx, x, pts
+      integer(c_int), value :: npts
+      type(c_ptr), value :: E, H, intensity
+      integer(c_int) :: rc
+    end function
+    function sie_field_interior(ctx, x, pts, npts, eps_r_re, eps_r_im, &
+        E, H) bind(C, name="sie_field_interior") result(rc)
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: ctx, x, pts
+      integer(c_int), value :: npts
+      real(c_double), value :: eps_r_re, eps_r_im
+      type(c_ptr), value :: E, H
+      integer(c_int) :: rc
+    end function
     function sie_free(ctx) bind(C, name="sie_free") result(rc)
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
@@ -215,6 +231,8 @@ module lib_sie_tri_mlfmm_interface
   public :: lib_sie_ml_fmm_grad_z_tri
   ! the fill and dense LU solve of the reference's normal solver, on the GPU
   public :: lib_sie_ml_fmm_solve_direct_tri
+  ! the fields at observation points, outside and inside the body, on the GPU
+  public :: lib_sie_ml_fmm_fields_tri
   ! the library context, for the GMRES-interface shim (sie_gmres_shim.f90)
   public :: sie_shim_context
 
@@ -392,5 +410,55 @@ contains
     vector_b = vector_x
     call sie_check(sie_free(ctx), 'sie_free')
   end subroutine lib_sie_ml_fmm_solve_direct_tri
+
+  ! E(3, n) and H(3, n) at the points pts(3, n) for the currents vector_x: where media(i)
+  ! is 2, the field inside the body (Integration_scattered_field_tri_within_medium,
+  ! src/lib_sie_tri_calculation_mod.f90:2829-2877, in eps_r2), elsewhere the scattered
+  ! field (Integration_scattered_field_tri, :2782-2825); all points in two library calls,
+  ! for the point loops of lib_sie_tri_observation_field_calculation
+  ! (src/lib_sie_tri_solver_normal.f90:325-420), which add the incident field and zero
+  ! vanishing interior components as before.
+  subroutine lib_sie_ml_fmm_fields_tri(vector_x, pts, media, E, H)
+    double complex, dimension(:), allocatable, target, intent(in) :: vector_x
+    real(c_double), dimension(:, :), intent(in) :: pts
+    integer, dimension(:), intent(in) :: media
+    double complex, dimension(:, :), intent(out) :: E, H
+    real(c_double), allocatable, target :: p_in(:, :), p_out(:, :), intens(:)
+    double complex, allocatable, target :: e_in(:, :), h_in(:, :), e_out(:, :), h_out(:, :)
+    integer :: i, n_in, n_out, a, b
+    n_in = count(media == 2)
+    n_out = size(media) - n_in
+    allocate(p_in(3, max(n_in, 1)), p_out(3, max(n_out, 1)), intens(max(n_out, 1)))
+    allocate(e_in(3, max(n_in, 1)), h_in(3, max(n_in, 1)), e_out(3, max(n_out, 1)), h_out(3, max(n_out, 1)))
+    a = 0
+    b = 0
+    do i = 1, size(media)
+      if (media(i) == 2) then
+        a = a + 1
+        p_in(:, a) = pts(:, i)
+      else
+        b = b + 1
+        p_out(:, b) = pts(:, i)
+      end if
+    end do
+    if (n_in > 0) call sie_check(sie_field_interior(m_ctx, c_loc(vector_x), c_loc(p_in), int(n_in, c_int), &
+                                 real(eps_r2, c_double), real(aimag(eps_r2), c_double), c_loc(e_in), &
+                                 c_loc(h_in)), 'sie_field_interior')
+    if (n_out > 0) call sie_check(sie_farfield(m_ctx, c_loc(vector_x), c_loc(p_out), int(n_out, c_int), &
+                                  c_loc(e_out), c_loc(h_out), c_loc(intens)), 'sie_farfield')
+    a = 0
+    b = 0
+    do i = 1, size(media)
+      if (media(i) == 2) then
+        a = a + 1
+        E(:, i) = e_in(:, a)
+        H(:, i) = h_in(:, a)
+      else
+        b = b + 1
+        E(:, i) = e_out(:, b)
+        H(:, i) = h_out(:, b)
+      end if
+    end do
+  end subroutine lib_sie_ml_fmm_fields_tri
 
 end module lib_sie_tri_mlfmm_interface
