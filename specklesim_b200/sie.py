@@ -266,8 +266,8 @@ class Sie:
         when k_in and E_in are given (the reference's total_field), the incident plane
         wave of lib_sie_tri_input_field_calculation (src/lib_sie_tri_calculation_mod.f90:
         2604-2609): E_in exp(-i k1 k_in . r), H = k1 k_in x E / (mu_1 omega).  Every point
-        uses the 3-point rule; the reference raises it near the surface
-        (ngp_near_field_distance_tri)."""
+        uses the 3-point rule, as the reference does for rough surfaces; for spheres it
+        raises it near the surface (ngp_near_field_distance_tri, :2627-2670)."""
         x = _lib.as_c128(x)
         p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
         inside = np.asarray(inside, dtype=bool).reshape(-1)
