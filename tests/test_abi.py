@@ -52,6 +52,9 @@ def test_argument_errors_without_device(gpu_lib):
     assert gpu_lib.sie_init(C.byref(cfg), _lib.dptr(v), 3, _lib.iptr(t2), 2, C.byref(h)) == _lib.SIE_ERR_ARG
     assert b"ngp" in gpu_lib.sie_last_error()
     assert gpu_lib.sie_matvec(None, None, None, 1, 0) == _lib.SIE_ERR_ARG
+    p = np.zeros(3)
+    assert gpu_lib.sie_field_interior(None, _lib.dptr(p), _lib.dptr(p), 1, 2.25, 0.0, None, None) == _lib.SIE_ERR_ARG
+    assert gpu_lib.sie_solve_direct_mixed(None, None, None, 1, 1e-10, 30, None) == _lib.SIE_ERR_ARG
 
 
 def test_quadrature_rules_are_the_reference_tables(gpu_lib):
