@@ -75,6 +75,7 @@ def lib():
             "orc_matvec": (None, [vp, dp, dp, C.c_int]),
             "orc_rhs": (None, [vp, dp, dp, dp]),
             "orc_field": (None, [vp, dp, dp, C.c_int, dp, dp]),
+            "orc_set_xnt_binary32": (None, [C.c_int]),
             "orc_field_interior": (None, [vp, dp, dp, C.c_int, C.c_double, C.c_double, dp, dp]),
             "orc_field_medium": (None, [vp, dp, dp, C.c_int, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_double, dp, dp]),
@@ -277,6 +278,12 @@ class Oracle:
         lib().orc_fn(self.h, e, ot, _d(out))
         return dict(c=out[0:9].reshape(3, 3), area=out[9], length=out[10], df=out[11],
                     mid=out[12:15], nq=out[15:18])
+
+
+def set_xnt_binary32(on):
+    """Round the x_nt term of the singular outer integrals to binary32 as the reference
+    does (True, the default) or keep it in FP64 (False), for every later fill."""
+    lib().orc_set_xnt_binary32(1 if on else 0)
 
 
 def quad_rule(ngp):

@@ -44,6 +44,11 @@ static const cd IM(0.0, 1.0);
 // Unsuffixed Fortran literals are binary32 (no real-kind promotion flag in the
 // reference build); src/lib_sie_constants.f90:9-11.
 static inline double f32(double x) { return (double)(float)x; }
+// The reference adds the x_nt term of the singular outer integrals as cmplx(x_nt, 0.0),
+// i.e. rounded to binary32, a staircase in the vertex coordinates.  Tests that study the
+// smoothness of J in the vertices switch the rounding off (orc_set_xnt_binary32).
+static bool g_xnt_binary32 = true;
+static inline double xnt_term(double x) { return g_xnt_binary32 ? f32(x) : x; }
 static const double C0 = (double)2.99792458e+8f;
 static const double EPS0 = (double)8.854187817e-12f;
 static const double MU0 = (double)1.2566370614e-6f;
@@ -420,7 +425,7 @@ static Outer outer_regular(const Fn& fm, const Fn& fn, const Rule& R, int md, cd
   }
   double sg = (md == 1) ? -0.5 : 0.5;  // 0.5*(-1)**md
   o.Kn += sg * f32(xnn);                // cmplx(x_nn, 0.0) is binary32
-  o.Kt += sg * f32(xnt);
+  o.Kt += sg * xnt_term(xnt);
   return o;
 }
 
@@ -448,7 +453,7 @@ static Outer outer_singular(const Fn& fm, const Fn& fn, const Rule& R, int md, c
   }
   double sg = (md == 1) ? -0.5 : 0.5;
   o.Kn += sg * f32(xnn);
-  o.Kt += sg * f32(xnt);
+  o.Kt += sg * xnt_term(xnt);
   return o;
 }
 
@@ -476,7 +481,7 @@ static cd outer_edge_adjacent(const Fn& fm, const Fn& fn, int md, cd k) {
     xnt -= dot(rfn, cross(fm.nq, rfm)) * trf;
   }
   double sg = (md == 1) ? -0.5 : 0.5;
-  return Kt + sg * f32(xnt);
+  return Kt + sg * xnt_term(xnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -1783,6 +1788,7 @@ void orc_rhs(void* h, const double* kin, const double* Ein, double* b) {
 void orc_field(void* h, const double* x, const double* pts, int npts, double* E, double* H) {
   scattered_field(*(Ctx*)h, (const cd*)x, pts, npts, (cd*)E, (cd*)H);
 }
+void orc_set_xnt_binary32(int on) { g_xnt_binary32 = on != 0; }
 void orc_field_interior(void* h, const double* x, const double* pts, int npts, double er_re, double er_im, double* E,
                         double* H) {
   scattered_field_interior(*(Ctx*)h, (const cd*)x, pts, npts, cd(er_re, er_im), (cd*)E, (cd*)H);
