@@ -41,3 +41,49 @@ def test_singular_flips_match_a_brute_force_count():
         v = rng.integers(0, 49)  # a vertex of the rough top face
         Vp[v, 2] += step * P.WL
         assert singular_flips(V, Vp, T, et) == _brute_flips(V, Vp, T, et)
+
+
+def _brute_crossings(Vm, Vp, T, et):
+    from tests.c5_check import _RULE3
+    n = 0
+    singular = []
+    for V in (Vm, Vp):
+        c = V[T].mean(axis=1)
+        rm = np.zeros(len(T))
+        for a, b in et:
+            r = np.linalg.norm(c[a] - c[b])
+            rm[a], rm[b] = max(rm[a], r), max(rm[b], r)
+        singular.append(np.linalg.norm(c[:, None, :] - c[None, :, :], axis=2) <= 1.5 * rm[:, None])
+    S = singular[0] | singular[1]
+    for p, q in zip(*np.nonzero(S)):
+        if p == q:
+            continue
+        for V_a, V_b in ((Vm, Vp),):
+            hs = []
+            for V in (V_a, V_b):
+                P, Q = V[T[p]], V[T[q]]
+                nq = np.cross(Q[1] - Q[0], Q[2] - Q[0])
+                hs.append((_RULE3 @ P - Q[0]) @ nq)
+            n += int(np.count_nonzero(np.sign(hs[0]) != np.sign(hs[1])))
+    return n
+
+
+def test_plane_crossings_match_a_brute_force_count():
+    """Outer quadrature points of singular pairs that cross the source triangle's plane
+    between two vertex sets (the kink of the unsigned solid angle), against a count over
+    every pair of the mesh."""
+    from tests.c5_check import plane_crossings
+    V, T = P.slab(cells=6, length_wl=1.5, seed=2, rms_wl=0.2, corr_wl=0.5, thickness_wl=0.5)
+    T = np.asarray(T)
+    et = _edge_triangles(T)
+    assert plane_crossings(V, V.copy(), T, et) == 0
+    rng = np.random.default_rng(1)
+    seen = 0
+    for step in (1e-3, 3e-2, 1e-1, 3e-1):
+        Vp = V.copy()
+        v = rng.integers(0, 49)  # a vertex of the rough top face
+        Vp[v, 2] += step * P.WL
+        n = plane_crossings(V, Vp, T, et)
+        assert n == _brute_crossings(V, Vp, T, et)
+        seen += n
+    assert seen > 0  # the larger steps carry points across planes
