@@ -50,3 +50,27 @@ def evaluation_points(evaluation_type, dim_a, dim_b, dim_c, n_a, n_b=1):
     else:
         out[:, 0], out[:, 1], out[:, 2] = a0 + dx_a * jj, c, b0 + dx_b * ii
     return out
+
+
+def energy_scat(evaluation_type, E, pts, theta_in=0.0, dim_a=None, n_a=None):
+    """The scattered energy the reference reports beside E_out
+    (lib_sie_tri_observation_field_calculation, src/lib_sie_tri_solver_normal.f90:325-360):
+    for 'rcs_p'/'rcs_n', |E|^2 4 pi |r|^2 (the intensity of sie_farfield); for
+    'BRDF_p'/'BRDF_n', |E|^2 |r|^2 / (cos theta_in cos theta_s), with theta_s the cut's
+    angles dim_a[0] + j (dim_a[1] - dim_a[0]) / (n_a - 1) (:316-322).  E: (n, 3) complex
+    fields at the points pts (n, 3)."""
+    E = np.asarray(E)
+    p = np.asarray(pts, dtype=np.float64).reshape(-1, 3)
+    e2 = np.sum(np.abs(E) ** 2, axis=1)
+    r2 = np.sum(p * p, axis=1)
+    if evaluation_type in ("rcs_p", "rcs_n"):
+        return e2 * 4 * np.pi * r2
+    if evaluation_type in ("BRDF_p", "BRDF_n"):
+        if dim_a is None or n_a is None:
+            raise ValueError("energy_scat: BRDF needs the cut's dim_a and n_a")
+        a0, a1 = float(dim_a[0]), float(dim_a[1])
+        theta_s = a0 + (a1 - a0) / (n_a - 1) * np.arange(n_a)
+        if theta_s.size != e2.size:
+            raise ValueError("energy_scat: one field per angle of the cut")
+        return e2 * r2 / (np.cos(theta_in) * np.cos(theta_s))
+    raise ValueError(f"energy_scat: no energy for evaluation type {evaluation_type!r}")

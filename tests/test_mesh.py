@@ -134,3 +134,19 @@ def test_evaluation_points_follow_the_reference_layout():
     assert np.allclose(np.arccos(p[:, 2] / 5.0), np.linspace(0, np.pi / 2, 5))
     with pytest.raises(ValueError):
         evaluation_points("zz", (0, 1), (0, 1), 0.0, 3, 3)
+
+
+def test_energy_scat_follows_the_reference_formulas():
+    """rcs: |E|^2 4 pi |r|^2; BRDF: |E|^2 |r|^2 / (cos theta_in cos theta_s) on the cut's
+    angles (lib_sie_tri_solver_normal.f90:316-360), from fields on the cut's points."""
+    from specklesim_b200.observation import energy_scat, evaluation_points
+    rng = np.random.default_rng(4)
+    pts = evaluation_points("BRDF_p", (0.0, 1.2), (0.3, 0.0), 5.0, 7)
+    E = rng.normal(size=(7, 3)) + 1j * rng.normal(size=(7, 3))
+    e2 = np.array([np.vdot(e, e).real for e in E])
+    assert np.allclose(energy_scat("rcs_p", E, pts), e2 * 4 * np.pi * 25.0)
+    th = np.linspace(0.0, 1.2, 7)
+    assert np.allclose(energy_scat("BRDF_n", E, pts, theta_in=0.2, dim_a=(0.0, 1.2), n_a=7),
+                       e2 * 25.0 / (np.cos(0.2) * np.cos(th)))
+    with pytest.raises(ValueError):
+        energy_scat("xy", E, pts)
