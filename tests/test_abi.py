@@ -208,3 +208,51 @@ def test_python_quadrature_rule(gpu_lib):
     assert len(a) == len(b) == len(w) == 12 and abs(w.sum() - 1.0) < 1e-6
     with pytest.raises(SieError):
         quadrature_rule(2)
+
+
+def _fortran_blocks_balanced(src):
+    """Every module, interface, derived type, procedure, DO and IF-THEN block of a free-form
+    Fortran source is closed by the matching END (continuation lines joined, comments
+    dropped); returns the first problem or None."""
+    lines, buf = [], ""
+    for raw in src.splitlines():
+        line = raw.split("!")[0].rstrip()
+        if buf:
+            line, buf = buf + " " + line.strip(), ""
+        if line.endswith("&"):
+            buf = line[:-1]
+            continue
+        lines.append(line.strip().lower())
+    stack = []
+    for line in lines:
+        if not line:
+            continue
+        m = re.match(r"^end\s*(subroutine|function|module|interface|type|do|if|select)?\b", line)
+        if m and (line == "end" or m.group(1)):
+            if not stack:
+                return "unmatched " + line
+            top = stack.pop()
+            if m.group(1) and m.group(1) != top:
+                return f"{top} closed by {line}"
+            continue
+        if line.startswith("module "):
+            stack.append("module")
+        elif line == "interface":
+            stack.append("interface")
+        elif re.match(r"^type\s*,|^type\s+\w", line):
+            stack.append("type")
+        elif re.search(r"\b(subroutine|function)\s+\w+\s*\(", line):
+            stack.append("subroutine" if "subroutine" in line.split("(")[0] else "function")
+        elif re.match(r"^do\b", line):
+            stack.append("do")
+        elif re.match(r"^if\s*\(.*\)\s*then$", line):
+            stack.append("if")
+    return f"left open: {stack}" if stack else None
+
+
+def test_fortran_shims_have_balanced_blocks():
+    """No Fortran compiler here: a structural check that each shim's blocks are closed."""
+    for name in ("sie_shim.f90", "sie_gmres_shim.f90"):
+        src = open(os.path.join(ROOT, "specklesim_b200", "fortran", name)).read()
+        assert _fortran_blocks_balanced(src) is None, (name, _fortran_blocks_balanced(src))
+    assert _fortran_blocks_balanced("module a\ncontains\nsubroutine b()\nend subroutine b\n") is not None
