@@ -119,34 +119,75 @@ def test_extinction_theorem_inside_the_sphere(oracle_lib, eps, formulation, boun
         assert err < bound, (r, err)
 
 
-def mie_d1(m, x):
-    """d_1 of the field inside a sphere (Bohren & Huffman eq. 4.52, equal permeabilities),
-    in their exp(-i w t) convention; at the centre the internal field is d_1 E0 x_hat."""
-    n = 1
+def mie_internal(m, x, k, pts):
+    """The field inside the sphere (Bohren & Huffman eqs. 4.50 and 4.52, equal
+    permeabilities): E1 = sum_n E_n (c_n M_o1n - i d_n N_e1n) with spherical Bessel radial
+    functions of m k r, E_n = i^n (2n + 1) / (n (n + 1)), for their x-polarised unit wave
+    along +z in the exp(-i w t) convention; pts (n, 3) in their frame."""
+    nmax = int(x + 4 * x ** (1 / 3) + 2) + 10
+    n = np.arange(1, nmax + 1)
     j = spherical_jn(n, x)
-    h = spherical_jn(n, x) + 1j * spherical_yn(n, x)
-    dxi = h + x * (spherical_jn(n, x, derivative=True) + 1j * spherical_yn(n, x, derivative=True))
-    dpsi_x = j + x * spherical_jn(n, x, derivative=True)
+    h = j + 1j * spherical_yn(n, x)
+    dxh = h + x * (spherical_jn(n, x, derivative=True) + 1j * spherical_yn(n, x, derivative=True))
+    dxj = j + x * spherical_jn(n, x, derivative=True)
     mx = m * x
-    dpsi_mx = spherical_jn(n, mx) + mx * spherical_jn(n, mx, derivative=True)
-    return m * (j * dxi - h * dpsi_x) / (m * m * spherical_jn(n, mx) * dxi - h * dpsi_mx)
+    jm = spherical_jn(n, mx)
+    dmj = jm + mx * spherical_jn(n, mx, derivative=True)
+    cn = (j * dxh - h * dxj) / (jm * dxh - h * dmj)
+    dn = (m * j * dxh - m * h * dxj) / (m * m * jm * dxh - h * dmj)
+    En = 1j ** n * (2 * n + 1) / (n * (n + 1))
+    out = []
+    for p in pts:
+        r = np.linalg.norm(p)
+        th, ph = np.arccos(p[2] / r), np.arctan2(p[1], p[0])
+        u = np.cos(th)
+        pi = np.zeros(nmax + 1)
+        tau = np.zeros(nmax + 1)
+        pi[1], tau[1] = 1.0, u
+        pi[2] = 3 * u
+        tau[2] = 2 * u * pi[2] - 3 * pi[1]
+        for i in range(3, nmax + 1):
+            pi[i] = (2 * i - 1) / (i - 1) * u * pi[i - 1] - i / (i - 1) * pi[i - 2]
+            tau[i] = i * u * pi[i] - (i + 1) * pi[i - 1]
+        pi, tau = pi[1:], tau[1:]
+        rho = m * k * r
+        z = spherical_jn(n, rho)
+        dz = (z + rho * spherical_jn(n, rho, derivative=True)) / rho  # [rho z_n]' / rho
+        Er = np.sum(En * -1j * dn * np.cos(ph) * n * (n + 1) * np.sin(th) * pi * z / rho)
+        Et = np.sum(En * (cn * np.cos(ph) * pi * z - 1j * dn * np.cos(ph) * tau * dz))
+        Ep = np.sum(En * (-cn * np.sin(ph) * tau * z + 1j * dn * np.sin(ph) * pi * dz))
+        er = np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+        et = np.array([np.cos(th) * np.cos(ph), np.cos(th) * np.sin(ph), -np.sin(th)])
+        ep = np.array([-np.sin(ph), np.cos(ph), 0.0])
+        out.append(Er * er + Et * et + Ep * ep)
+    return np.array(out)
 
 
 @pytest.mark.parametrize("formulation", ["ICTF", "PMCHWT"])
-def test_interior_field_at_the_sphere_centre_matches_mie(oracle_lib, formulation):
+def test_interior_field_matches_mie(oracle_lib, formulation):
     """Integration_scattered_field_tri_within_medium (lib_sie_tri_calculation_mod.f90:
-    2829-2877) at the centre of the dielectric sphere against the Mie internal field
-    there, d_1 E0 x_hat (amplitude and phase); the SIE code's exp(+i w t) convention makes
-    it the complex conjugate of Bohren & Huffman's value with m = conj(sqrt(eps)).
-    Measured 0.6 % for both formulations."""
+    2829-2877) inside the dielectric sphere against the Mie internal field, amplitude and
+    phase, at 12 random directions on radii 0.1-0.4 lambda (radius 0.5 lambda).  The SIE
+    wave travels along -z in exp(+i w t): the Mie field at the point mirrored in z, its z
+    component negated, complex-conjugated, with m = conj(sqrt(eps)).  Measured 0.6-1.1 %
+    (ICTF) and 0.55-0.9 % (PMCHWT); at the centre the field is d_1 E0 x_hat (0.6 %)."""
     eps = P.EPS_DIELECTRIC
     o, x = solved_sphere(oracle_lib, eps, formulation)
     k = 2 * np.pi / P.WL
     a = 0.5 * P.WL
-    ref = np.conj(mie_d1(np.sqrt(np.conj(eps)), k * a)) * E_IN
-    E, _ = o.field_interior(x, np.zeros((1, 3)), eps)
-    err = np.linalg.norm(E[0] - ref) / np.linalg.norm(ref)
-    assert err < 0.03, err
+    m = np.sqrt(np.conj(eps))
+    flip = np.array([1.0, 1.0, -1.0])
+    d = np.random.default_rng(3).normal(size=(12, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    for r in (0.1, 0.2, 0.3, 0.4):
+        pts = d * r * P.WL
+        E, _ = o.field_interior(x, pts, eps)
+        ref = np.conj(mie_internal(m, k * a, k, pts * flip) * flip)
+        err = np.linalg.norm(E - ref) / np.linalg.norm(ref)
+        assert err < 0.02, (r, err)
+    E0, _ = o.field_interior(x, np.zeros((1, 3)), eps)
+    ref0 = np.conj(mie_internal(m, k * a, k, np.array([[0.0, 0.0, 1e-9 * P.WL]]))[0])
+    assert np.linalg.norm(E0[0] - ref0) / np.linalg.norm(ref0) < 0.02
 
 
 @pytest.mark.parametrize("formulation", ["ICTF", "PMCHWT"])
