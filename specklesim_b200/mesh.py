@@ -168,3 +168,33 @@ def edge_count(tris):
     e = np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]]), axis=1)
     _, cnt = np.unique(e, axis=0, return_counts=True)
     return int((cnt >= 2).sum())
+
+
+def winding_number(verts, tris, pts, chunk=2048):
+    """Generalised winding number of the closed triangle surface at each point: the sum of
+    the signed solid angles of its triangles (Van Oosterom and Strackee, IEEE Trans.
+    Biomed. Eng. 30 (1983) 125) over 4 pi.  +-1 inside (the sign follows the triangles'
+    orientation), 0 outside."""
+    V = np.asarray(verts, dtype=np.float64)
+    T = np.asarray(tris)
+    P = np.asarray(pts, dtype=np.float64).reshape(-1, 3)
+    A, B, C = V[T[:, 0]], V[T[:, 1]], V[T[:, 2]]
+    out = np.empty(len(P))
+    for s in range(0, len(P), chunk):
+        p = P[s:s + chunk, None, :]
+        a, b, c = A[None] - p, B[None] - p, C[None] - p
+        la, lb, lc = (np.linalg.norm(v, axis=2) for v in (a, b, c))
+        num = np.einsum("ijk,ijk->ij", a, np.cross(b, c))
+        den = (la * lb * lc + np.einsum("ijk,ijk->ij", a, b) * lc + np.einsum("ijk,ijk->ij", a, c) * lb
+               + np.einsum("ijk,ijk->ij", b, c) * la)
+        out[s:s + chunk] = 2 * np.arctan2(num, den).sum(axis=1) / (4 * np.pi)
+    return out
+
+
+def inside(verts, tris, pts):
+    """True for points inside the closed triangle surface (|winding number| > 1/2): the
+    medium-2 points of a near-field map.  The reference classifies map points by its
+    analytic shapes (sphere radius, grating profile, rough-surface boundary file;
+    get_evaluation_points_domain_new, src/lib_sie_math.f90:360-530); this uses the
+    meshed surface itself."""
+    return np.abs(winding_number(verts, tris, pts)) > 0.5

@@ -56,6 +56,7 @@ class Sie:
         self.cfg = cfg
         v = np.ascontiguousarray(verts, dtype=np.float64)
         t = np.ascontiguousarray(tris, dtype=np.int32)
+        self.verts, self.tris = v, t
         self._h = C.c_void_p()
         check(lib.sie_init(C.byref(cfg), dptr(v), v.shape[0], iptr(t), t.shape[0], C.byref(self._h)))
         self._lib = lib
@@ -257,10 +258,11 @@ class Sie:
                                            dptr(E.view(np.float64)), dptr(H.view(np.float64))))
         return E, H
 
-    def near_field(self, x, pts, inside, k_in=None, E_in=None):
+    def near_field(self, x, pts, inside=None, k_in=None, E_in=None):
         """E, H of a near-field map, as the plane-wave branch of
         lib_sie_tri_observation_field_calculation (src/lib_sie_tri_solver_normal.f90:
-        385-420): points with inside[i] true get the interior field (eps_r2), with a
+        385-420): points with inside[i] true (by default: inside the context's closed
+        mesh, mesh.inside) get the interior field (eps_r2), with a
         component of E below 1e-20 in modulus set to zero together with the same
         component of H, as the reference does; the others get the scattered field plus,
         when k_in and E_in are given (the reference's total_field), the incident plane
@@ -270,6 +272,9 @@ class Sie:
         raises it near the surface (ngp_near_field_distance_tri, :2627-2670)."""
         x = _lib.as_c128(x)
         p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+        if inside is None:
+            from .mesh import inside as inside_mesh
+            inside = inside_mesh(self.verts, self.tris, p)
         inside = np.asarray(inside, dtype=bool).reshape(-1)
         if inside.size != p.shape[0]:
             raise ValueError("near_field: inside must have one entry per point")

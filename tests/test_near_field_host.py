@@ -64,3 +64,31 @@ def test_near_field_zeroes_vanishing_interior_components(oracle_lib):
     assert np.array_equal(E, [[0, 1.0, 0], [2.0, 1e-19, 0]])
     assert np.array_equal(H, [[0, 6.0, 0], [8.0, 9.0, 0]])
     o.close()
+
+
+def test_default_media_from_the_mesh(oracle_lib):
+    """Without an inside mask, the map's medium-2 points are those inside the closed mesh
+    (generalised winding number): the same result as the explicit mask."""
+    V, T = P.sphere(1)
+    eps = complex(P.EPS_DIELECTRIC)
+    o = oracle_lib.Oracle(V, T, P.WL, eps, threads=4)
+    g = _host_only(o, eps)
+    g.verts, g.tris = np.asarray(V), np.asarray(T)
+    x = P.random_x(o.N, seed=7)
+    d = np.random.default_rng(3).normal(size=(20, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    pts = np.concatenate([d * 0.3 * P.WL, d * 0.8 * P.WL])
+    mask = np.arange(40) < 20
+    E1, H1 = g.near_field(x, pts)
+    E2, H2 = g.near_field(x, pts, mask)
+    assert np.array_equal(E1, E2) and np.array_equal(H1, H2)
+    o.close()
+
+
+def test_winding_number_of_closed_meshes():
+    from specklesim_b200 import mesh
+    for V, T in (P.sphere(2), P.slab(cells=10, length_wl=2.0, seed=3)):
+        c = np.asarray(V).mean(axis=0)
+        far = c + np.array([0.0, 0.0, 10.0 * P.WL])
+        w = mesh.winding_number(V, T, np.stack([c, far]))
+        assert abs(abs(w[0]) - 1) < 1e-9 and abs(w[1]) < 1e-9
